@@ -1,0 +1,363 @@
+"""Benchmark of the B200 anti-aliased fill (one JSON line on rank 0).
+
+Workload (default): the glyph-dense text page — 150,000 quadratic glyph paths
+(2 contours on average, 12-60 quadratic segments each, 8-12 pt em at 300 dpi)
+on 60 baselines of one 2550x3300 u8 page initialised to 255, seed 0. A step
+renders the whole page: fill the page with 255, flatten every path in FP64,
+build the AA rows, bin paths to tiles and composite them in order.
+
+  value  Mpixel/s with the path inputs already resident in device memory
+         (rrb_batch_upload once, rrb_record_batch per step), timed with CUDA
+         events on the backend's own stream, max over ranks.
+  e2e    the same metric through rrb_render_pages_host with pinned HOST
+         buffers: the path arrays and the page go host->device and the page
+         comes back every step.
+
+Multi-GPU: pages are independent, so N ranks render N page replicas with no
+collective on the data path (weak scaling); only the timing barrier and the
+max-over-ranks reduction use torch.distributed.
+
+`--impl reference` times the reference CPU scanline rasterizer's
+restatement (oracle/, the reference itself is Rust and cannot be built here)
+on the host cores: each step renders one copy of the page per thread.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "pdf-raster_b200"), str(ROOT / "oracle")]
+
+METRIC = "bit-exact Mpixel/s & edges/s, batched vs plain per-path GPU; p99 page latency"
+WORKLOADS = {
+    "glyphs": (dict(kind=1, seed=0),
+               "glyph-dense text page: 150,000 quadratic glyph paths (2 contours avg, 12-60 quads each, "
+               "8-12 pt em @300 dpi, 60 baselines) on one 2550x3300 u8 page (Letter @300 dpi), NZ, gray 0, alpha 255"),
+    "polygons": (dict(kind=0, seed=0),
+                 "polygon page: 2,000 closed paths (1-3 contours x 4-32 line/cubic segments, jittered circles, "
+                 "log-normal radius) on one 2550x3300 u8 page, NZ 70% / EO 30%, opaque"),
+}
+CLOCK_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), ws
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.path = device, None, None
+
+    def start(self):
+        try:
+            self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"rrb_clocks_{os.getpid()}.csv"
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={CLOCK_FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def oracle_page(scene, threads=1):
+    import rr_oracle
+    rr_oracle.build()
+    a = scene.blank_arena()
+    t = time.perf_counter()
+    st = rr_oracle.render_scene(scene, a, threads=threads)
+    return a, time.perf_counter() - t, st
+
+
+def run_reference(args, rank, world):
+    """The reference CPU path (its restatement) on the host cores."""
+    if rank != 0:
+        return
+    import rr_oracle
+    import rrb
+    rr_oracle.build()
+    kw, desc = WORKLOADS[args.workload]
+    scene = rrb.Scene(**kw)
+    cores = os.cpu_count() or 1
+    threads = max(1, min(cores, args.ref_threads))
+    arenas = [scene.blank_arena() for _ in range(threads)]
+
+    def step():
+        for a in arenas:
+            a.fill(255)
+        ts = [threading.Thread(target=rr_oracle.render_scene, args=(scene, a), kwargs=dict(threads=1))
+              for a in arenas]
+        t = time.perf_counter()
+        for x in ts:
+            x.start()
+        for x in ts:
+            x.join()
+        return time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    total = sum(times)
+    mpx = scene.pixels * threads * args.steps / total / 1e6
+    sample = f"{threads} copies of the page per step, one per host thread (page-parallel, as the reference's per-page workers)"
+    line = {"impl": "reference", "metric": METRIC, "value": mpx, "unit": "Mpixel/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded)", "config": {"workload": desc, "pages_per_step": threads},
+            "cpu_baseline": {"value": mpx, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": mpx, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_copy(backend, arr, keep):
+    arr = np.ascontiguousarray(arr)
+    buf = backend.alloc_host_pinned(max(1, arr.nbytes))
+    v = buf.array()[: arr.nbytes].view(arr.dtype)
+    v[:] = arr.reshape(-1)
+    keep.append(buf)
+    return v
+
+
+def run_rrb(args, rank, local, world):
+    import rrb
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = tdist
+    import torch
+
+    kw, desc = WORKLOADS[args.workload]
+    scene = rrb.Scene(**kw)
+    backend = rrb.B200Backend(local)
+    tuning = backend.get_tuning()
+    pages = backend.alloc_device(scene.arena_bytes)
+    scene.view.pages = None
+    batch = backend.batch_upload(scene.view)
+    stream = torch.cuda.ExternalStream(backend.stream, device=torch.device("cuda", local))
+
+    def step():
+        backend.begin_page()
+        backend.record_fill_buffer(pages, 255)
+        batch.record(pages, args.rowmap)
+        backend.wait_page(backend.submit_page())
+
+    for _ in range(args.warmup):
+        step()
+    # ---- timed region: resident inputs, per-stage events inside the library
+    backend.set_profiling(True)
+    stage_acc, launches, step_ms = {}, 0, []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(local)
+    clocks.start()
+    ev[0].record(stream)
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record(stream)
+        st = backend.last_batch_stats()
+        launches += st["kernel_launches"]
+        for name, (ms, nl) in backend.stage_times().items():
+            a = stage_acc.setdefault(name, [0.0, 0])
+            a[0] += ms
+            a[1] += nl
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    backend.set_profiling(False)
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    stats = backend.last_batch_stats()
+    ms_per_step = total_ms / args.steps
+    px = scene.pixels
+    value = px * world * args.steps / (total_ms / 1e3) / 1e6
+    edges_s = stats["segments"] * world * args.steps / (total_ms / 1e3)
+
+    # ---- roofline of the dominant kernel (HBM-bound integer work)
+    peak, peak_kind = measured_peak()
+    stage_ms = {k: v[0] / args.steps for k, v in stage_acc.items()}
+    dom = max(stage_ms, key=stage_ms.get)
+    alg = {
+        # page read + written once, each span (4 B) and AA-row index entry (8 B) read once
+        "composite": 2 * px + 4 * stats["spans"] + 8 * stats["aa_rows"],
+        # each edge record (32 B) read once, row index (8 B/row) and spans (4 B) written once
+        "rows": 32 * stats["segments"] + 8 * stats["aa_rows"] + 4 * stats["spans"],
+        # path points (16 B) + flags read, edge records written
+        "seg_write": 17 * scene.n_pts + 32 * stats["segments"],
+        "seg_count": 17 * scene.n_pts + 4 * scene.n_pts,
+    }
+    alg_b = alg.get(dom)
+    roofline = None
+    if alg_b:
+        dur = stage_ms[dom] / max(1, stage_acc[dom][1] / args.steps) / 1e3
+        ach = alg_b / dur / 1e9
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
+                    "algorithmic_bytes_per_launch": alg_b}
+
+    # ---- plain per-path form on a sample of paths (one record_path_fill per path)
+    plain = None
+    if args.plain_sample > 0 and rank == 0:
+        W, H = int(scene.page_width[0]), int(scene.page_height[0])
+        n = min(args.plain_sample, scene.n_paths)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        backend.begin_page()
+        backend.record_fill_buffer(pages, 255)
+        t0.record(stream)
+        for p in range(n):
+            a, b = int(scene.path_pt_off[p]), int(scene.path_pt_off[p + 1])
+            backend.record_path_fill(scene.pts[a:b], scene.flags[a:b], pages, W, H,
+                                     fill_rule=int(scene.fill_rule[p]), gray=int(scene.gray[p]),
+                                     alpha=int(scene.alpha[p]), rowmap=args.rowmap)
+        t1.record(stream)
+        backend.wait_page(backend.submit_page())
+        torch.cuda.synchronize(local)
+        per_path = t0.elapsed_time(t1) / n
+        plain_mpx = px / (per_path * scene.n_paths / 1e3) / 1e6
+        plain = {"mpixel_s": plain_mpx, "sample_paths": n, "ms_per_path": per_path,
+                 "batched_speedup": value / world / plain_mpx}
+
+    # ---- end to end through the public API with pinned host buffers
+    keep = []
+    h = {k: pinned_copy(backend, getattr(scene, k), keep) for k in (
+        "pts", "flags", "path_pt_off", "fill_rule", "gray", "alpha", "path_page", "page_width", "page_height",
+        "page_offset")}
+    params = rrb.batch_params(h["pts"], h["flags"], h["path_pt_off"], h["fill_rule"], h["gray"], h["alpha"],
+                              h["path_page"], h["page_width"], h["page_height"], h["page_offset"], pages,
+                              rowmap=args.rowmap)
+    host_page = pinned_copy(backend, scene.blank_arena(), keep)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    host_page[:] = 255
+    backend.render_pages_host(params, host_page)  # warm
+    if dist:
+        dist.barrier()
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        host_page[:] = 255
+        backend.render_pages_host(params, host_page)
+    e2e_s = time.perf_counter() - t
+    if dist:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = sum(int(h[k].nbytes) for k in h) + int(host_page.nbytes)
+    e2e = {"value": px * world * e2e_steps / e2e_s / 1e6, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": int(host_page.nbytes), "steps": e2e_steps,
+           "api": "rrb_render_pages_host (C ABI), pinned host buffers"}
+
+    # ---- parity check and CPU baseline (rank 0, N = 1)
+    gpu_page = np.empty(scene.arena_bytes, np.uint8)
+    backend.wait_download(backend.download_async(pages, gpu_page))
+    cpu = None
+    bit_exact = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref, secs, ost = oracle_page(scene, threads=1)
+        bit_exact = bool(np.array_equal(ref, np.asarray(host_page)) and np.array_equal(ref, gpu_page))
+        cpu = {"value": px / secs / 1e6, "unit": "Mpixel/s", "cores": 1, "kind": "port",
+               "sample": "the whole page (all paths), 1 host thread, C++ restatement of the reference CPU path",
+               "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"]}
+    batch.free()
+    if rank == 0:
+        p50, p99 = (float(np.percentile(step_ms, q)) for q in (50, 99))
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator, seed 0; no public dataset for this path)",
+            "config": {"workload": desc, "paths": scene.n_paths, "pages": scene.n_pages,
+                       "rowmap": ["documented", "as_shipped"][args.rowmap],
+                       "tile": f"{tuning.tile_w}x{tuning.tile_h}",
+                       "l2": f"inputs larger than L2 ({16 * scene.n_pts / 1e6:.0f} MB of path points)",
+                       "parallelism": f"replicas x{world} (one page per GPU)"},
+            "edges_per_s": edges_s, "segments_per_step": stats["segments"],
+            "input_segments_per_step": scene.n_lines + scene.n_cubics,
+            "p50_page_ms": p50, "p99_page_ms": p99,
+            "plain_per_path": plain, "bit_exact": bit_exact,
+            "roofline": roofline, "stages_ms": stage_ms,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    backend.free_device(pages)
+    backend.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["rrb", "reference"], default="rrb")
+    ap.add_argument("--workload", choices=list(WORKLOADS), default="glyphs")
+    ap.add_argument("--rowmap", type=int, default=0)
+    ap.add_argument("--plain-sample", type=int, default=2000)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--ref-threads", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local, world = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_rrb(args, rank, local, world)
+
+
+if __name__ == "__main__":
+    main()

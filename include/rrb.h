@@ -1,0 +1,268 @@
+/*
+ * rrb.h — C ABI of the B200 anti-aliased fill backend ("rrb").
+ *
+ * This is the drop-in boundary beside the reference's CUDA / Vulkan / CPU
+ * backends: every entry point mirrors one method of the reference trait
+ * `GpuBackend` (crates/gpu/src/backend/mod.rs:216-503) or one of its
+ * parameter structs (crates/gpu/src/backend/params.rs), with plain pointers,
+ * sizes and an int status instead of Rust types. A Rust `impl GpuBackend for
+ * B200Backend` binds these symbols one to one.
+ *
+ * Status codes mirror `BackendError` (mod.rs:35-72) plus a timeout and a
+ * device error. The text of the last failure is available from
+ * rrb_last_error_message(ctx).
+ *
+ * Pixels written by rrb_record_path_fill / rrb_record_path_batch are bit-exact
+ * with the reference CPU scanline rasterizer (crates/raster fill_impl with
+ * vector_antialias = true, Gray8 page, div255 source-over).
+ */
+#ifndef RRB_H
+#define RRB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (BackendError, crates/gpu/src/backend/mod.rs:35-72) ---- */
+#define RRB_OK 0
+#define RRB_ERR_ZERO_SIZE_ALLOC 1     /* BackendError::ZeroSizeAlloc */
+#define RRB_ERR_UNALIGNED_FILL 2      /* BackendError::UnalignedFill */
+#define RRB_ERR_POOL_EXHAUSTED 3      /* BackendError::DescriptorPoolExhausted */
+#define RRB_ERR_INVARIANT 4           /* BackendError::InvariantViolation (validate()) */
+#define RRB_ERR_OTHER 5               /* BackendError::Other */
+#define RRB_ERR_TIMEOUT 6             /* wait_page / wait_transfer exceeded timeout_ns */
+#define RRB_ERR_DEVICE 7              /* CUDA runtime / kernel error */
+#define RRB_ERR_OUT_OF_MEMORY 8       /* allocation beyond the device memory budget */
+#define RRB_ERR_STATE 9               /* begin/record/submit called out of order */
+
+/* Fill rules (AaFillParams::fill_rule, params.rs:90-103). */
+#define RRB_FILL_NONZERO 0
+#define RRB_FILL_EVEN_ODD 1
+
+/* Row map of the AA driver loop (crates/raster/src/fill/mod.rs:176-203). */
+#define RRB_ROWMAP_DOCUMENTED 0 /* pixel row y <- AA rows 4y..4y+3 (module docs, Splash) */
+#define RRB_ROWMAP_AS_SHIPPED 1 /* the literal loop: pixel row y <- AA rows 16y+12..16y+15 */
+
+/* PathFlags (crates/raster/src/path/mod.rs:70-79). */
+#define RRB_PATH_FIRST 0x01u
+#define RRB_PATH_LAST 0x02u
+#define RRB_PATH_CLOSED 0x04u
+#define RRB_PATH_CURVE 0x08u
+
+typedef struct rrb_ctx rrb_ctx;       /* one backend = one device + one stream */
+typedef struct rrb_buf rrb_buf;       /* opaque device buffer (GpuBackend::DeviceBuffer) */
+typedef struct rrb_host_buf rrb_host_buf; /* opaque pinned host buffer (GpuBackend::HostBuffer) */
+typedef uint64_t rrb_fence;           /* GpuBackend::PageFence; 0 is never a valid fence */
+
+/* VramBudget (crates/gpu/src/backend/mod.rs, detect_vram_budget). */
+typedef struct {
+    uint64_t total_bytes;
+    uint64_t free_bytes;
+    uint64_t budget_bytes; /* the limit passed to rrb_init (0 = whole device) */
+    uint64_t used_bytes;   /* bytes this backend holds now */
+} rrb_vram_budget;
+
+/* ---- lifetime ----------------------------------------------------------- */
+/* CudaBackend::new equivalent: bind `device`, create the stream, cap this
+ * backend's device allocations at mem_budget_bytes (0 = no cap). */
+int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out);
+int rrb_destroy(rrb_ctx* ctx);
+const char* rrb_last_error_message(const rrb_ctx* ctx);
+const char* rrb_status_name(int status);
+/* Library build identifier (kernel arch, version). */
+const char* rrb_version(void);
+
+/* ---- memory: GpuBackend::{alloc_device, alloc_device_zeroed, device_buffer_len,
+ *      free_device, alloc_host_pinned, free_host_pinned} (mod.rs:235-295) ---- */
+int rrb_alloc_device(rrb_ctx* ctx, size_t size, rrb_buf** out);
+int rrb_alloc_device_zeroed(rrb_ctx* ctx, size_t size, rrb_buf** out);
+size_t rrb_device_buffer_len(const rrb_buf* buf);
+/* Raw device address of a buffer (for interop with other CUDA code). */
+void* rrb_device_ptr(const rrb_buf* buf);
+int rrb_free_device(rrb_ctx* ctx, rrb_buf* buf);
+int rrb_alloc_host_pinned(rrb_ctx* ctx, size_t size, rrb_host_buf** out);
+void* rrb_host_ptr(const rrb_host_buf* buf);
+int rrb_free_host_pinned(rrb_ctx* ctx, rrb_host_buf* buf);
+
+/* ---- transfers: GpuBackend::{upload_async, download_async, wait_download,
+ *      submit_transfer, wait_transfer} (mod.rs:405-480) ---- */
+int rrb_upload_async(rrb_ctx* ctx, const rrb_buf* dst, size_t dst_offset, const void* src,
+                     size_t len, rrb_fence* out_fence);
+int rrb_download_async(rrb_ctx* ctx, const rrb_buf* src, size_t src_offset, void* dst, size_t len,
+                       rrb_fence* out_fence);
+int rrb_wait_download(rrb_ctx* ctx, rrb_fence fence);
+int rrb_submit_transfer(rrb_ctx* ctx, rrb_fence* out_fence);
+int rrb_wait_transfer(rrb_ctx* ctx, rrb_fence fence, uint64_t timeout_ns);
+int rrb_detect_vram_budget(rrb_ctx* ctx, rrb_vram_budget* out);
+
+/* ---- per-page state machine: begin_page -> record_* -> submit_page ->
+ *      wait_page (mod.rs:195-204, 306, 400-405) ---- */
+int rrb_begin_page(rrb_ctx* ctx);
+/* GpuBackend::record_zero_buffer (mod.rs:378-395). */
+int rrb_record_zero_buffer(rrb_ctx* ctx, const rrb_buf* buf);
+int rrb_submit_page(rrb_ctx* ctx, rrb_fence* out_fence);
+/* Blocks until the fence completes or timeout_ns elapses (0 = no limit). */
+int rrb_wait_page(rrb_ctx* ctx, rrb_fence fence, uint64_t timeout_ns);
+
+/* ---- the anti-aliased path fill ------------------------------------------
+ * A page is a device-resident u8 Gray8 bitmap of width*height bytes, row
+ * stride `width`, no alpha plane (the renderer's page: pdf_interp
+ * renderer/page/mod.rs:479-480 filled with 255).
+ *
+ * One path (replaces raster::fill / raster::eo_fill, crates/raster/src/fill/
+ * mod.rs:55-104, called from PageRenderer::fill_path, crates/pdf_interp/src/
+ * renderer/page/mod.rs:1061-1138, with DEVICE_MATRIX, page clip and
+ * vector_antialias = true). `pts` holds n_pts (x,y) f64 pairs and `flags`
+ * n_pts PathFlags bytes, both HOST memory, exactly as Path::{pts,flags}. The
+ * path is flattened in FP64 and rasterised on the device; nothing comes back
+ * to the host. */
+typedef struct {
+    const double* pts;     /* host, [n_pts*2] */
+    const uint8_t* flags;  /* host, [n_pts]   */
+    uint32_t n_pts;
+    double matrix[6];      /* XPath::new matrix; identity in the renderer */
+    double flatness;       /* max(gs.flatness, 0.1) in the renderer */
+    uint8_t fill_rule;     /* RRB_FILL_NONZERO / RRB_FILL_EVEN_ODD */
+    uint8_t gray;          /* solid source gray */
+    uint8_t alpha;         /* PipeState::a_input (fill_alpha * 255) */
+    uint8_t rowmap;        /* RRB_ROWMAP_* */
+    const rrb_buf* page;   /* device Gray8 page */
+    uint64_t page_offset;  /* byte offset of the page inside `page` */
+    uint32_t width, height;
+} rrb_path_fill_params;
+int rrb_record_path_fill(rrb_ctx* ctx, const rrb_path_fill_params* p);
+
+/* Many paths over many pages in one submission (the batched form). All
+ * arrays are HOST memory; the backend uploads them and renders every path,
+ * in index order per page, into device pages. Paths on different pages are
+ * independent; paths on one page composite in index order. */
+typedef struct {
+    const double* pts;          /* [n_pts*2] */
+    const uint8_t* flags;       /* [n_pts] */
+    uint64_t n_pts;
+    const uint64_t* path_pt_off;/* [n_paths+1], offsets into pts/flags */
+    const uint8_t* fill_rule;   /* [n_paths] */
+    const uint8_t* gray;        /* [n_paths] */
+    const uint8_t* alpha;       /* [n_paths] */
+    const uint32_t* path_page;  /* [n_paths] page index */
+    uint64_t n_paths;
+    const uint32_t* page_width; /* [n_pages] */
+    const uint32_t* page_height;/* [n_pages] */
+    const uint64_t* page_offset;/* [n_pages] byte offset of each page in `pages` */
+    uint32_t n_pages;
+    const rrb_buf* pages;       /* device arena holding every page */
+    double matrix[6];
+    double flatness;
+    uint8_t rowmap;
+} rrb_path_batch_params;
+int rrb_record_path_batch(rrb_ctx* ctx, const rrb_path_batch_params* p);
+
+/* Device-resident batches: the inputs of a path batch are validated and
+ * uploaded once, then rendered any number of times into device pages with no
+ * further host-to-device traffic (the serving loop keeps them resident).
+ * rrb_record_path_batch is rrb_batch_upload + rrb_record_batch on a
+ * context-owned batch. */
+typedef struct rrb_batch rrb_batch;
+int rrb_batch_upload(rrb_ctx* ctx, const rrb_path_batch_params* p, rrb_batch** out);
+int rrb_record_batch(rrb_ctx* ctx, rrb_batch* batch, const rrb_buf* pages, int rowmap);
+int rrb_batch_free(rrb_ctx* ctx, rrb_batch* batch);
+
+/* Fill `len` bytes of `buf` at `off` with `value` inside the current page
+ * (record_zero_buffer generalised: pages start white, 255). */
+int rrb_record_fill_buffer(rrb_ctx* ctx, const rrb_buf* buf, size_t off, size_t len, uint8_t value);
+
+/* Per-stage device time of the last batch, measured with CUDA events on the
+ * backend's stream while profiling is enabled. */
+typedef struct {
+    char name[24];
+    float ms;
+    uint32_t launches;
+} rrb_stage_time;
+int rrb_set_profiling(rrb_ctx* ctx, int enable);
+/* The cudaStream_t every call of this context is ordered on (for callers
+ * that time or order their own work against the backend). */
+void* rrb_stream(rrb_ctx* ctx);
+int rrb_last_stage_times(rrb_ctx* ctx, rrb_stage_time* out, int cap, int* n);
+
+/* Host-side validation of a batch without a device (the params validate()
+ * step, crates/gpu/src/backend/params.rs:57,334; FakeBackend pattern,
+ * params.rs:978-1075). pages_len is the byte size of the page arena. The
+ * first violated invariant is written to msg. */
+int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, char* msg, size_t msg_len);
+
+/* Per-batch tuning knobs (tile shape etc.); 0 fields keep the defaults.
+ * Tile shapes accepted: 16x16, 32x32, 64x16. */
+typedef struct {
+    uint32_t tile_w, tile_h;
+    uint32_t rows_per_chunk;    /* AA rows per row-kernel work item: 32 */
+    uint32_t reserved[5];
+} rrb_tuning;
+int rrb_set_tuning(rrb_ctx* ctx, const rrb_tuning* t);
+int rrb_get_tuning(rrb_ctx* ctx, rrb_tuning* t);
+
+/* Counters of the last recorded batch (filled after the page fence). */
+typedef struct {
+    uint64_t paths, pieces, segments;       /* input paths, walk pieces, flattened segments */
+    uint64_t aa_rows, spans, row_overflows; /* AA rows built, spans emitted, rows on the slow path */
+    uint64_t tiles, tile_pairs;             /* tiles with work, (tile, path) pairs */
+    uint64_t nonterminating_rows;           /* rows whose winding never returns to 0 */
+    uint64_t kernel_launches;               /* kernels launched by the last record call */
+} rrb_batch_stats;
+int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
+
+/* Host-side convenience for a user holding host pages: uploads the pages,
+ * records the batch, downloads the pages and waits (one call, end to end). */
+int rrb_render_pages_host(rrb_ctx* ctx, const rrb_path_batch_params* p, uint8_t* host_pages,
+                          size_t host_pages_len);
+
+/* ---- path construction on the host (A1, A2) --------------------------------
+ * PathBuilder::{move_to, line_to, curve_to, close} (crates/raster/src/path/
+ * mod.rs:310-448) and conic_to_cubic (crates/font/src/outline.rs:106-112). */
+typedef struct rrb_path rrb_path;
+rrb_path* rrb_path_new(void);
+void rrb_path_free(rrb_path* p);
+void rrb_path_clear(rrb_path* p);
+int rrb_path_move_to(rrb_path* p, double x, double y);       /* 0, or 1 NoCurPt / 2 BogusPath */
+int rrb_path_line_to(rrb_path* p, double x, double y);
+int rrb_path_curve_to(rrb_path* p, double x1, double y1, double x2, double y2, double x3, double y3);
+int rrb_path_conic_to(rrb_path* p, double xc, double yc, double x3, double y3);
+int rrb_path_close(rrb_path* p, int force);
+uint64_t rrb_path_len(const rrb_path* p);
+const double* rrb_path_pts(const rrb_path* p);
+const uint8_t* rrb_path_flags(const rrb_path* p);
+void rrb_conic_to_cubic(double p0x, double p0y, double pcx, double pcy, double p3x, double p3y,
+                        double out[4]);
+
+/* ---- seeded synthetic scenes (the benchmark workloads) ----------------------
+ * kind 0: polygon page (2,000 paths of 1-3 contours x 4-32 line/cubic
+ *         segments on jittered circles, NZ 70% / EO 30%, opaque);
+ * kind 1: glyph-dense text page (150,000 quadratic glyphs on 60 baselines);
+ * kind 2: mixed pages of uneven size (30% glyphs, 40% polygons, 30% rects,
+ *         alpha 32-255). Zero fields take the defaults of each kind. */
+typedef struct {
+    uint32_t kind;
+    uint64_t seed;
+    uint32_t n_pages;      /* kind 2 (default 64); kinds 0/1 always 1 */
+    uint32_t n_paths;      /* kinds 0/1: paths on the page; kind 2: 0 = log-normal count */
+    uint32_t page_w, page_h; /* kinds 0/1 page size (default 2550x3300) */
+    double page_scale;     /* kind 2: page dimensions multiplied by this (default 1) */
+    double paths_scale;    /* kind 2: median path count multiplied by this (default 1) */
+    uint32_t path_cap;     /* kind 2: max paths per page (default 50,000) */
+    uint32_t reserved;
+} rrb_scene_params;
+typedef struct rrb_scene rrb_scene;
+int rrb_scene_generate(const rrb_scene_params* p, rrb_scene** out);
+void rrb_scene_free(rrb_scene* s);
+/* Fills a batch view of the scene (pages = NULL, caller binds a device arena). */
+void rrb_scene_view(const rrb_scene* s, rrb_path_batch_params* out);
+uint64_t rrb_scene_arena_bytes(const rrb_scene* s);
+/* Input segment counts of the scene: [lines, cubics, points]. */
+void rrb_scene_counts(const rrb_scene* s, uint64_t out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RRB_H */

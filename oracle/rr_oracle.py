@@ -1,0 +1,307 @@
+"""ctypes binding of the CPU oracle (oracle/rr_oracle.{h,cpp}).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline / reference legs of bench.py, never by the product package.
+`build()` compiles it with oracle/Makefile into oracle/_build/.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "librr_oracle.so"
+
+ROWMAP_DOCUMENTED = 0
+ROWMAP_AS_SHIPPED = 1
+
+
+class Seg(C.Structure):
+    _fields_ = [("x0", C.c_double), ("y0", C.c_double), ("x1", C.c_double), ("y1", C.c_double),
+                ("dxdy", C.c_double), ("dxdy_fp", C.c_int32), ("flags", C.c_uint32)]
+
+
+class Intersect(C.Structure):
+    _fields_ = [("x0", C.c_int32), ("x1", C.c_int32), ("count", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("paths", "segments", "aa_rows", "intersects", "unpinned_tie_rows",
+                                          "nonterminating_rows")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+XF_HORIZ, XF_VERT, XF_FLIPPED = 1, 2, 4
+PF_FIRST, PF_LAST, PF_CLOSED, PF_CURVE = 1, 2, 4, 8
+IDENTITY = (1.0, 0.0, 0.0, 1.0, 0.0, 0.0)
+
+_LIB = None
+
+
+def build(arch: str | None = None) -> Path:
+    """Compile the oracle if needed. `arch` overrides -march (default x86-64-v3, portable to any AVX2 host)."""
+    src = HERE / "rr_oracle.cpp"
+    if LIB_PATH.exists() and LIB_PATH.stat().st_mtime >= max(src.stat().st_mtime,
+                                                              (HERE / "rr_oracle.h").stat().st_mtime):
+        return LIB_PATH
+    env = dict(os.environ)
+    cmd = ["make", "-C", str(HERE), f"ARCHFLAGS=-march={arch or 'x86-64-v3'}"]
+    subprocess.run(cmd, check=True, env=env, stdout=subprocess.DEVNULL)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        D, I32, U8, I64, VP = C.c_double, C.c_int32, C.c_uint8, C.c_int64, C.c_void_p
+        sig = {
+            "or_path_new": (VP, []), "or_path_free": (None, [VP]),
+            "or_path_move_to": (C.c_int, [VP, D, D]), "or_path_line_to": (C.c_int, [VP, D, D]),
+            "or_path_curve_to": (C.c_int, [VP, D, D, D, D, D, D]), "or_path_close": (C.c_int, [VP, C.c_int]),
+            "or_path_len": (I64, [VP]), "or_path_pts": (C.POINTER(D), [VP]), "or_path_flags": (C.POINTER(U8), [VP]),
+            "or_conic_to_cubic": (None, [D] * 6 + [C.POINTER(D)]),
+            "or_transform": (None, [C.POINTER(D), D, D, C.POINTER(D)]),
+            "or_flatten_curve": (I32, [C.POINTER(D), D, C.POINTER(D), I32]),
+            "or_add_segment": (None, [D, D, D, D, C.POINTER(Seg)]),
+            "or_xpath_new": (I64, [C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D), D, C.c_int, C.POINTER(Seg), I64]),
+            "or_xpath_aa_scale": (None, [C.POINTER(Seg), I64]),
+            "or_scanner_new": (VP, [C.POINTER(Seg), I64, C.c_int, I32, I32, C.POINTER(Stats)]),
+            "or_scanner_free": (None, [VP]),
+            "or_scanner_bounds": (None, [VP, C.POINTER(I32)]),
+            "or_scanner_row": (I64, [VP, I32, C.POINTER(Intersect), I64]),
+            "or_scanner_test": (C.c_int, [VP, I32, I32]),
+            "or_count_crossings": (None, [C.POINTER(Intersect), I64, I32, C.POINTER(I32)]),
+            "or_add_intersection": (I64, [C.POINTER(Intersect), I64, I32, I32, I32]),
+            "or_render_aa_line": (None, [VP, C.POINTER(U8), I64, I32, C.POINTER(I32), C.POINTER(Stats)]),
+            "or_aabuf_set_span": (None, [C.POINTER(U8), I64, I64, I64, I64]),
+            "or_aa_coverage_span": (None, [C.POINTER(U8), I64, I64, C.POINTER(U8), I64]),
+            "or_aa_gamma": (C.POINTER(U8), []),
+            "or_div255": (U8, [C.c_uint32]),
+            "or_render_span_aa_gray": (None, [C.POINTER(U8), C.POINTER(U8), I64, U8, U8]),
+            "or_composite_aa_rgb8_opaque": (None, [C.POINTER(U8), C.POINTER(U8), U8, C.POINTER(U8), I64]),
+            "or_rgb_to_gray": (None, [C.POINTER(U8), C.POINTER(U8), I64]),
+            "or_fill_path": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D), D,
+                                    C.c_int, U8, U8, C.c_int, C.POINTER(Stats)]),
+            "or_render_scene": (None, [C.POINTER(U8), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(D), C.POINTER(U8),
+                                       C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
+                                       C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D), D, C.c_int, C.c_int,
+                                       C.POINTER(Stats)]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(L, n)
+            f.restype, f.argtypes = r, a
+        _LIB = L
+    return _LIB
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _mat(m):
+    return (C.c_double * 6)(*m)
+
+
+# ---- A1/A2 --------------------------------------------------------------------
+class OraclePath:
+    """PathBuilder restatement; build() returns (pts[n,2], flags[n])."""
+
+    def __init__(self):
+        self.h = lib().or_path_new()
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_path_free(self.h)
+            self.h = None
+
+    def move_to(self, x, y):
+        return lib().or_path_move_to(self.h, x, y)
+
+    def line_to(self, x, y):
+        return lib().or_path_line_to(self.h, x, y)
+
+    def curve_to(self, *a):
+        return lib().or_path_curve_to(self.h, *a)
+
+    def close(self, force=False):
+        return lib().or_path_close(self.h, int(force))
+
+    def build(self):
+        n = lib().or_path_len(self.h)
+        if n == 0:
+            return np.zeros((0, 2)), np.zeros(0, np.uint8)
+        pts = np.ctypeslib.as_array(lib().or_path_pts(self.h), shape=(n * 2,)).reshape(n, 2).copy()
+        return pts, np.ctypeslib.as_array(lib().or_path_flags(self.h), shape=(n,)).copy()
+
+
+def conic_to_cubic(p0, pc, p3):
+    o = (C.c_double * 4)()
+    lib().or_conic_to_cubic(p0[0], p0[1], pc[0], pc[1], p3[0], p3[1], o)
+    return (o[0], o[1]), (o[2], o[3])
+
+
+# ---- A3-A6 -----------------------------------------------------------------------
+def transform(m, x, y):
+    o = (C.c_double * 2)()
+    lib().or_transform(_mat(m), x, y, o)
+    return o[0], o[1]
+
+
+def flatten_curve(p0, p1, p2, p3, flatness_sq):
+    cp = (C.c_double * 8)(*p0, *p1, *p2, *p3)
+    out = np.zeros(2 * 1025, np.float64)
+    n = lib().or_flatten_curve(cp, flatness_sq, _p(out, C.c_double), 1025)
+    return out[: 2 * n].reshape(n, 2)
+
+
+def add_segment(x0, y0, x1, y1) -> Seg:
+    s = Seg()
+    lib().or_add_segment(x0, y0, x1, y1, C.byref(s))
+    return s
+
+
+def xpath_new(pts, flags, matrix=IDENTITY, flatness=0.1, close=True, aa_scale=False):
+    pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    n = flags.size
+    need = lib().or_xpath_new(_p(pts, C.c_double), _p(flags, C.c_uint8), n, _mat(matrix), flatness, int(close),
+                              None, 0)
+    segs = (Seg * max(1, need))()
+    lib().or_xpath_new(_p(pts, C.c_double), _p(flags, C.c_uint8), n, _mat(matrix), flatness, int(close), segs, need)
+    if aa_scale:
+        lib().or_xpath_aa_scale(segs, need)
+    return list(segs)[:need]
+
+
+# ---- A7/A8 -----------------------------------------------------------------------
+class Scanner:
+    def __init__(self, segs, eo=False, clip_y_min=0, clip_y_max=1 << 20):
+        arr = (Seg * max(1, len(segs)))(*segs)
+        self.stats = Stats()
+        self.h = lib().or_scanner_new(arr, len(segs), int(eo), clip_y_min, clip_y_max, C.byref(self.stats))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_scanner_free(self.h)
+            self.h = None
+
+    def bounds(self):
+        o = (C.c_int32 * 5)()
+        lib().or_scanner_bounds(self.h, o)
+        return dict(y_min=o[0], y_max=o[1], x_min=o[2], x_max=o[3], empty=bool(o[4]))
+
+    def row(self, y):
+        n = lib().or_scanner_row(self.h, y, None, 0)
+        buf = (Intersect * max(1, n))()
+        lib().or_scanner_row(self.h, y, buf, n)
+        return [(b.x0, b.x1, b.count) for b in list(buf)[:n]]
+
+    def test(self, x, y) -> bool:
+        return bool(lib().or_scanner_test(self.h, x, y))
+
+    def render_aa_line(self, aa_width, y):
+        rb = (aa_width + 7) // 8
+        buf = np.zeros(rb * 4, np.uint8)
+        o = (C.c_int32 * 2)()
+        st = Stats()
+        lib().or_render_aa_line(self.h, _p(buf, C.c_uint8), aa_width, y, o, C.byref(st))
+        return buf.reshape(4, rb), (o[0], o[1]), st
+
+
+def count_crossings(row, x):
+    arr = (Intersect * max(1, len(row)))(*[Intersect(*r) for r in row])
+    o = (C.c_int32 * 2)()
+    lib().or_count_crossings(arr, len(row), x, o)
+    return o[0], bool(o[1])
+
+
+def add_intersection(row, x0, x1, count):
+    arr = (Intersect * (len(row) + 1))(*[Intersect(*r) for r in row])
+    n = lib().or_add_intersection(arr, len(row), x0, x1, count)
+    return [(a.x0, a.x1, a.count) for a in list(arr)[:n]]
+
+
+def aabuf_set_span(buf, width, row, x0, x1):
+    lib().or_aabuf_set_span(_p(buf, C.c_uint8), width, row, x0, x1)
+
+
+# ---- A10-A12 -----------------------------------------------------------------------
+def aa_coverage_span(rows4: np.ndarray, x0: int, n: int) -> np.ndarray:
+    rows4 = np.ascontiguousarray(rows4, np.uint8)
+    out = np.zeros(n, np.uint8)
+    lib().or_aa_coverage_span(_p(rows4, C.c_uint8), rows4.shape[1], x0, _p(out, C.c_uint8), n)
+    return out
+
+
+def aa_gamma():
+    g = lib().or_aa_gamma()
+    return [g[i] for i in range(17)]
+
+
+def div255(x: int) -> int:
+    return int(lib().or_div255(x))
+
+
+def render_span_aa_gray(dst: np.ndarray, shape: np.ndarray, a_input: int, gray: int):
+    shape = np.ascontiguousarray(shape, np.uint8)
+    lib().or_render_span_aa_gray(_p(dst, C.c_uint8), _p(shape, C.c_uint8), shape.size, a_input, gray)
+
+
+def composite_aa_rgb8_opaque(dst: np.ndarray, src, a_input: int, shape: np.ndarray):
+    s = np.asarray(src, np.uint8)
+    shape = np.ascontiguousarray(shape, np.uint8)
+    lib().or_composite_aa_rgb8_opaque(_p(dst, C.c_uint8), _p(s, C.c_uint8), a_input, _p(shape, C.c_uint8), shape.size)
+
+
+def rgb_to_gray(rgb: np.ndarray) -> np.ndarray:
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    out = np.zeros(rgb.size // 3, np.uint8)
+    lib().or_rgb_to_gray(_p(rgb, C.c_uint8), _p(out, C.c_uint8), out.size)
+    return out
+
+
+# ---- A9 + scenes -----------------------------------------------------------------
+def fill_path(page: np.ndarray, pts, flags, eo=False, gray=0, alpha=255, rowmap=ROWMAP_DOCUMENTED, matrix=IDENTITY,
+              flatness=0.1) -> dict:
+    """fill_impl on a (H, W) u8 page in place; returns the oracle counters."""
+    assert page.dtype == np.uint8 and page.flags["C_CONTIGUOUS"] and page.ndim == 2
+    pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    st = Stats()
+    lib().or_fill_path(_p(page, C.c_uint8), page.shape[1], page.shape[0], _p(pts, C.c_double),
+                       _p(flags, C.c_uint8), flags.size, _mat(matrix), flatness, int(eo), gray, alpha, rowmap,
+                       C.byref(st))
+    return st.as_dict()
+
+
+def render_arrays(arena, page_offset, page_width, page_height, pts, flags, path_pt_off, fill_rule, gray, alpha,
+                  path_page, rowmap=ROWMAP_DOCUMENTED, threads=1, matrix=IDENTITY, flatness=0.1) -> dict:
+    """Render every path in order onto an arena of pages (in place)."""
+    a = [np.ascontiguousarray(x, t) for x, t in (
+        (page_offset, np.uint64), (page_width, np.uint32), (page_height, np.uint32),
+        (np.reshape(pts, -1), np.float64), (flags, np.uint8), (path_pt_off, np.uint64), (fill_rule, np.uint8),
+        (gray, np.uint8), (alpha, np.uint8), (path_page, np.uint32))]
+    st = Stats()
+    lib().or_render_scene(_p(arena, C.c_uint8), _p(a[0], C.c_uint64), _p(a[1], C.c_uint32), _p(a[2], C.c_uint32),
+                          a[1].size, _p(a[3], C.c_double), _p(a[4], C.c_uint8), _p(a[5], C.c_uint64),
+                          _p(a[6], C.c_uint8), _p(a[7], C.c_uint8), _p(a[8], C.c_uint8), _p(a[9], C.c_uint32),
+                          a[6].size, _mat(matrix), flatness, rowmap, threads, C.byref(st))
+    return st.as_dict()
+
+
+def render_scene(scene, arena: np.ndarray, rowmap=ROWMAP_DOCUMENTED, threads=1) -> dict:
+    """Render an rrb.Scene (its numpy views) with the oracle into `arena` in place."""
+    return render_arrays(arena, scene.page_offset, scene.page_width, scene.page_height, scene.pts, scene.flags,
+                         scene.path_pt_off, scene.fill_rule, scene.gray, scene.alpha, scene.path_page,
+                         rowmap=rowmap, threads=threads)

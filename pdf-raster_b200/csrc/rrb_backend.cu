@@ -1,0 +1,934 @@
+// rrb_backend.cu — the C ABI (include/rrb.h): context, device memory,
+// transfers, the per-page state machine of GpuBackend
+// (crates/gpu/src/backend/mod.rs:216-503) and the path-fill batch driver.
+//
+// One rrb_ctx = one device + one non-blocking stream, as GpuCtx serialises
+// every call on one stream (crates/gpu/src/lib.rs:197-208). Scratch buffers
+// for a batch are owned by the context and grow on demand, so repeated
+// batches of similar size allocate nothing.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/rrb.h"
+#include "rrb_kernels.cuh"
+
+using namespace rrb;
+
+struct rrb_buf {
+    void* p = nullptr;
+    size_t len = 0;
+};
+struct rrb_host_buf {
+    void* p = nullptr;
+    size_t len = 0;
+};
+
+namespace {
+
+struct Scratch {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+constexpr int KCAP = 24;        // merged Intersect entries per AA row kept in shared memory
+constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
+
+}  // namespace
+
+struct rrb_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t used = 0;
+    std::string err;
+    bool in_page = false;
+    rrb_tuning tuning{};
+    rrb_batch_stats stats{};
+    uint64_t next_fence = 1;
+    std::unordered_map<uint64_t, cudaEvent_t> fences;
+    std::vector<cudaEvent_t> free_events;
+    // Batch scratch.
+    Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
+    Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
+    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats;
+    uint32_t* h_read = nullptr;  // pinned readback area
+    uint64_t launches = 0;
+    struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
+    struct StageTimer* timer = nullptr;
+    float stage_ms[16] = {};
+    uint32_t stage_launches[16] = {};
+};
+
+namespace {
+
+int set_err(rrb_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_err(rrb_ctx* c, cudaError_t e, const char* what) {
+    return set_err(c, RRB_ERR_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define RRB_CUDA(ctx, call)                                   \
+    do {                                                      \
+        cudaError_t e__ = (call);                             \
+        if (e__ != cudaSuccess) return cuda_err(ctx, e__, #call); \
+    } while (0)
+
+int dev_alloc(rrb_ctx* c, size_t bytes, void** out) {
+    if (c->budget && c->used + bytes > c->budget)
+        return set_err(c, RRB_ERR_OUT_OF_MEMORY,
+                       "device allocation of " + std::to_string(bytes) + " bytes exceeds the budget");
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(c, RRB_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c->used += bytes;
+    return RRB_OK;
+}
+
+void dev_free(rrb_ctx* c, void* p, size_t bytes) {
+    if (!p) return;
+    cudaFree(p);
+    c->used -= std::min<uint64_t>(c->used, bytes);
+}
+
+// Grow a scratch buffer to at least `bytes` (x1.25 headroom); contents are not kept.
+int ensure(rrb_ctx* c, Scratch& s, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (s.cap >= bytes) return RRB_OK;
+    if (s.p) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamSynchronize");
+        dev_free(c, s.p, s.cap);
+        s.p = nullptr;
+        s.cap = 0;
+    }
+    size_t want = bytes + bytes / 4;
+    want = (want + 255) & ~size_t(255);
+    int rc = dev_alloc(c, want, &s.p);
+    if (rc) return rc;
+    s.cap = want;
+    return RRB_OK;
+}
+
+template <typename T>
+T* as(Scratch& s) {
+    return static_cast<T*>(s.p);
+}
+
+int grid_for(rrb_ctx* c, uint64_t n, int threads, int per_sm = 8) {
+    uint64_t need = (n + threads - 1) / threads;
+    uint64_t cap = static_cast<uint64_t>(c->sm_count) * per_sm;
+    return static_cast<int>(std::max<uint64_t>(1, std::min(need, cap)));
+}
+
+// Exclusive scan of n u32 at d_in into d_out[0..n] (d_out[n] = total).
+int scan_u32(rrb_ctx* c, const uint32_t* d_in, uint32_t* d_out, uint32_t n) {
+    uint32_t* bs = as<uint32_t>(c->s_block);
+    if (n == 0) {
+        RRB_CUDA(c, cudaMemsetAsync(d_out, 0, sizeof(uint32_t), c->stream));
+        return RRB_OK;
+    }
+    uint32_t nb = std::min<uint32_t>(SCAN_MAX_BLOCKS, std::max<uint32_t>(1, (n + 4095) / 4096));
+    uint32_t per = (n + nb - 1) / nb;
+    nb = (n + per - 1) / per;
+    k_scan_reduce<<<nb, SCAN_THREADS, 0, c->stream>>>(d_in, n, per, bs);
+    k_scan_blocks<<<1, 1024, 0, c->stream>>>(bs, nb);
+    k_scan_down<<<nb, SCAN_THREADS, 0, c->stream>>>(d_in, d_out, n, per, bs);
+    c->launches += 3;
+    RRB_CUDA(c, cudaGetLastError());
+    return RRB_OK;
+}
+
+template <typename T>
+int upload(rrb_ctx* c, Scratch& s, const T* src, size_t count) {
+    int rc = ensure(c, s, count * sizeof(T));
+    if (rc) return rc;
+    if (count) RRB_CUDA(c, cudaMemcpyAsync(s.p, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return RRB_OK;
+}
+
+int read_back(rrb_ctx* c, const void* dev, size_t bytes) {
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+    RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RRB_OK;
+}
+
+bool valid_tile(uint32_t w, uint32_t h) {
+    return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16);
+}
+
+int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
+                     uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
+                     const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, uint8_t* arena,
+                     int rowmap, const BatchCounters* ctr) {
+#define RRB_COMP(TW, TH)                                                                                 \
+    k_composite<TW, TH><<<grid, COMP_THREADS, 0, c->stream>>>(info, geom, n_pages, n_tiles, SUPER, SUPER, \
+                                                              super_off, super_list, row_off, row_idx,    \
+                                                              spans, arena, rowmap, ctr)
+    if (tw == 64 && th == 16) RRB_COMP(64, 16);
+    else if (tw == 32 && th == 32) RRB_COMP(32, 32);
+    else RRB_COMP(16, 16);
+#undef RRB_COMP
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    return RRB_OK;
+}
+
+// Host-side checks of a batch (the params.validate() of the reference,
+// crates/gpu/src/backend/params.rs:57,334), plus the page geometry the
+// kernels need. No device access.
+int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw, uint32_t th,
+                   std::vector<PageGeom>& geom, uint64_t& tiles, uint64_t& supers, std::string& msg) {
+    const uint64_t n_paths = h->n_paths, n_pts = h->n_pts;
+    const uint32_t n_pages = h->n_pages;
+    tiles = supers = 0;
+    if (h->rowmap > 1) return msg = "rowmap must be 0 or 1", RRB_ERR_INVARIANT;
+    if (!(h->flatness >= 0.0)) return msg = "flatness must be >= 0", RRB_ERR_INVARIANT;
+    for (int i = 0; i < 6; ++i)
+        if (!std::isfinite(h->matrix[i])) return msg = "matrix must be finite", RRB_ERR_INVARIANT;
+    if (!valid_tile(tw, th)) return msg = "tile shape must be 16x16, 32x32 or 64x16", RRB_ERR_INVARIANT;
+    if (n_paths == 0) return RRB_OK;
+    if (!h->pts || !h->flags || !h->path_pt_off || !h->fill_rule || !h->gray || !h->alpha || !h->path_page ||
+        !h->page_width || !h->page_height || !h->page_offset || !n_pages)
+        return msg = "null array in path batch", RRB_ERR_INVARIANT;
+    if (n_pts >= (1ull << 30) || n_paths >= (1ull << 31))
+        return msg = "batch exceeds 2^30 points or 2^31 paths", RRB_ERR_INVARIANT;
+    if (h->path_pt_off[0] != 0 || h->path_pt_off[n_paths] != n_pts)
+        return msg = "path_pt_off must start at 0 and end at n_pts", RRB_ERR_INVARIANT;
+    for (uint64_t p = 0; p < n_paths; ++p)
+        if (h->path_pt_off[p + 1] < h->path_pt_off[p]) return msg = "path_pt_off must be non-decreasing", RRB_ERR_INVARIANT;
+    geom.assign(n_pages, PageGeom{});
+    for (uint32_t pg = 0; pg < n_pages; ++pg) {
+        uint32_t w = h->page_width[pg], ht = h->page_height[pg];
+        if (w == 0 || ht == 0 || w > 16383 || ht > (1u << 28))
+            return msg = "page width must be 1..16383 and height 1..2^28", RRB_ERR_INVARIANT;
+        if (h->page_offset[pg] + static_cast<uint64_t>(w) * ht > arena_len)
+            return msg = "page extends past the page buffer", RRB_ERR_INVARIANT;
+        PageGeom& G = geom[pg];
+        G.w = w;
+        G.h = ht;
+        G.offset = h->page_offset[pg];
+        G.ntx = (w + tw - 1) / tw;
+        G.nsx = (w + SUPER - 1) / SUPER;
+        G.tile_base = static_cast<uint32_t>(tiles);
+        G.super_base = static_cast<uint32_t>(supers);
+        tiles += static_cast<uint64_t>(G.ntx) * ((ht + th - 1) / th);
+        supers += static_cast<uint64_t>(G.nsx) * ((ht + SUPER - 1) / SUPER);
+    }
+    uint32_t prev = 0;
+    for (uint64_t p = 0; p < n_paths; ++p) {
+        uint32_t pg = h->path_page[p];
+        if (pg >= n_pages || pg < prev)
+            return msg = "path_page must be < n_pages and non-decreasing", RRB_ERR_INVARIANT;
+        if (h->fill_rule[p] > 1) return msg = "fill_rule must be 0 or 1", RRB_ERR_INVARIANT;
+        prev = pg;
+    }
+    uint64_t p = 0;
+    for (uint32_t pg = 0; pg < n_pages; ++pg) {
+        geom[pg].path_begin = static_cast<uint32_t>(p);
+        while (p < n_paths && h->path_page[p] == pg) ++p;
+        geom[pg].path_end = static_cast<uint32_t>(p);
+    }
+    if (tiles >= (1ull << 31) || supers >= (1ull << 31)) return msg = "too many tiles", RRB_ERR_INVARIANT;
+    return RRB_OK;
+}
+
+// Recompute per-tile geometry for tile shape (tw, th).
+void set_tiles(std::vector<PageGeom>& geom, uint32_t tw, uint32_t th, uint64_t& tiles) {
+    tiles = 0;
+    for (PageGeom& G : geom) {
+        G.ntx = (G.w + tw - 1) / tw;
+        G.tile_base = static_cast<uint32_t>(tiles);
+        tiles += static_cast<uint64_t>(G.ntx) * ((G.h + th - 1) / th);
+    }
+}
+
+}  // namespace
+
+// A batch whose inputs live in device memory: uploaded once, rendered any
+// number of times (the serving loop keeps these resident).
+struct rrb_batch {
+    Scratch pts, flags, off, rule, gray, alpha, page, geom, pw, ph, mtx;
+    std::vector<PageGeom> geom_h;
+    uint64_t supers = 0, arena_need = 0;
+    uint64_t n_paths = 0, n_pts = 0;
+    uint32_t n_pages = 0;
+    double flat_sq = 0.0;
+    uint8_t rowmap = 0;
+};
+
+namespace {
+
+// Stage names for the optional per-stage event timing.
+const char* const kStageNames[] = {"walk",   "seg_count",   "scan_edges", "seg_write", "path_bbox",
+                                   "scan_rows_chunks", "super_count", "scan_super", "super_write", "rows",
+                                   "rows_slow", "composite"};
+constexpr int kStages = sizeof(kStageNames) / sizeof(kStageNames[0]);
+
+}  // namespace
+
+struct StageTimer {
+    bool on = false;
+    cudaEvent_t begin[kStages] = {}, end[kStages] = {};
+    bool used[kStages] = {};
+    uint32_t launches[kStages] = {};
+    uint64_t launch_mark = 0;
+};
+
+namespace {
+
+// Per-stage CUDA events on the launching stream (profiling mode only).
+void stage(rrb_ctx* c, int k) {
+    StageTimer* t = c->timer;
+    if (!t || !t->on || k >= kStages) return;
+    cudaEventRecord(t->begin[k], c->stream);
+    t->used[k] = true;
+    t->launch_mark = c->launches;
+}
+
+void stage_end(rrb_ctx* c, int k) {
+    StageTimer* t = c->timer;
+    if (!t || !t->on || k >= kStages) return;
+    cudaEventRecord(t->end[k], c->stream);
+    t->launches[k] = static_cast<uint32_t>(c->launches - t->launch_mark);
+}
+
+void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
+    Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
+                      &B->mtx};
+    for (Scratch* s : all) {
+        dev_free(c, s->p, s->cap);
+        s->p = nullptr;
+        s->cap = 0;
+    }
+}
+
+int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
+    std::string msg;
+    uint64_t tiles = 0;
+    int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg);
+    if (v) return set_err(c, v, msg);
+    B->n_paths = h->n_paths;
+    B->n_pts = h->n_pts;
+    B->n_pages = h->n_pages;
+    B->flat_sq = h->flatness * h->flatness;
+    B->rowmap = h->rowmap;
+    B->arena_need = 0;
+    for (const PageGeom& G : B->geom_h)
+        B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(G.w) * G.h);
+    if (B->n_paths == 0) return RRB_OK;
+    int rc;
+    if ((rc = upload(c, B->pts, h->pts, 2 * h->n_pts))) return rc;
+    if ((rc = upload(c, B->flags, h->flags, h->n_pts))) return rc;
+    if ((rc = upload(c, B->off, h->path_pt_off, h->n_paths + 1))) return rc;
+    if ((rc = upload(c, B->rule, h->fill_rule, h->n_paths))) return rc;
+    if ((rc = upload(c, B->gray, h->gray, h->n_paths))) return rc;
+    if ((rc = upload(c, B->alpha, h->alpha, h->n_paths))) return rc;
+    if ((rc = upload(c, B->page, h->path_page, h->n_paths))) return rc;
+    if ((rc = upload(c, B->pw, h->page_width, h->n_pages))) return rc;
+    if ((rc = upload(c, B->ph, h->page_height, h->n_pages))) return rc;
+    if ((rc = ensure(c, B->geom, h->n_pages * sizeof(PageGeom)))) return rc;
+    if ((rc = upload(c, B->mtx, h->matrix, 6))) return rc;
+    return RRB_OK;
+}
+
+// The pipeline over a device-resident batch into the device page arena.
+int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
+    c->launches = 0;
+    std::memset(&c->stats, 0, sizeof c->stats);
+    if (B->n_paths == 0) return RRB_OK;
+    if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
+    if (rowmap < 0 || rowmap > 1) return set_err(c, RRB_ERR_INVARIANT, "rowmap must be 0 or 1");
+    const uint32_t tw = c->tuning.tile_w ? c->tuning.tile_w : 64;
+    const uint32_t th = c->tuning.tile_h ? c->tuning.tile_h : 16;
+    uint64_t tiles = 0;
+    set_tiles(B->geom_h, tw, th, tiles);
+    if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
+    const uint64_t n_paths = B->n_paths, n_pts = B->n_pts, supers = B->supers;
+    const uint32_t n_pages = B->n_pages;
+    const uint32_t NP = static_cast<uint32_t>(n_paths), NS = static_cast<uint32_t>(n_pts);
+    const double flat_sq = B->flat_sq;
+    int rc;
+    RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
+                                c->stream));
+    // ---- stage 1: walk, flatten counts, edge offsets
+    if ((rc = ensure(c, c->s_pieces, n_pts * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_clip, n_pts * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_edge_off, (n_pts + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_block, (SCAN_MAX_BLOCKS + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
+    RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
+    stage(c, 0);
+    k_walk<<<grid_for(c, n_paths, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
+                                                             as<uint64_t>(B->off), NP, as<double>(B->mtx),
+                                                             as<uint32_t>(B->page), as<uint32_t>(B->ph),
+                                                             as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip));
+    c->launches += 1;
+    stage_end(c, 0);
+    stage(c, 1);
+    k_seg_count<<<grid_for(c, n_pts, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NS,
+                                                                as<double>(B->mtx), flat_sq,
+                                                                as<uint32_t>(c->s_edge_off));
+    c->launches += 1;
+    stage_end(c, 1);
+    RRB_CUDA(c, cudaGetLastError());
+    stage(c, 2);
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_edge_off), as<uint32_t>(c->s_edge_off), NS))) return rc;
+    stage_end(c, 2);
+    if ((rc = read_back(c, as<uint32_t>(c->s_edge_off) + NS, sizeof(uint32_t)))) return rc;
+    const uint64_t n_edges = c->h_read[0];
+    // ---- stage 2: edges, path boxes, row/chunk offsets, supertile bins
+    if ((rc = ensure(c, c->s_edges, std::max<uint64_t>(1, n_edges) * sizeof(Edge)))) return rc;
+    if ((rc = ensure(c, c->s_info, n_paths * sizeof(PathInfo)))) return rc;
+    if ((rc = ensure(c, c->s_rows, (n_paths + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_chunks, (n_paths + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
+    stage(c, 3);
+    k_seg_write<<<grid_for(c, n_pts, 128), 128, 0, c->stream>>>(
+        as<double>(B->pts), as<uint2>(c->s_pieces), NS, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
+        static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip));
+    c->launches += 1;
+    stage_end(c, 3);
+    const int chunk_rows = 32;
+    stage(c, 4);
+    k_path_bbox<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(
+        as<uint64_t>(B->off), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
+        as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
+        as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
+        chunk_rows, as<BatchCounters>(c->s_ctr));
+    c->launches += 1;
+    stage_end(c, 4);
+    RRB_CUDA(c, cudaGetLastError());
+    stage(c, 5);
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_rows), as<uint32_t>(c->s_rows), NP))) return rc;
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_chunks), NP))) return rc;
+    stage_end(c, 5);
+    const uint32_t NSUP = static_cast<uint32_t>(supers);
+    stage(c, 6);
+    k_super_bin<false><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
+        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, as<uint32_t>(c->s_super_cnt),
+        nullptr, nullptr);
+    c->launches += 1;
+    stage_end(c, 6);
+    RRB_CUDA(c, cudaGetLastError());
+    stage(c, 7);
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_cnt), NSUP))) return rc;
+    stage_end(c, 7);
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 0, as<uint32_t>(c->s_rows) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 1, as<uint32_t>(c->s_chunks) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 2, as<uint32_t>(c->s_super_cnt) + NSUP, 4, cudaMemcpyDeviceToHost,
+                                c->stream));
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 4, &as<BatchCounters>(c->s_ctr)->raw_entries, 8, cudaMemcpyDeviceToHost,
+                                c->stream));
+    RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    const uint64_t n_rows = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
+    uint64_t raw_entries;
+    std::memcpy(&raw_entries, c->h_read + 4, 8);
+    // ---- stage 3: rows. A row with m merged entries yields at most m/2 + 1
+    // spans (every span consumes an opening and a closing entry, except the
+    // last one of a row whose winding never returns to zero).
+    uint64_t span_cap = raw_entries / 2 + n_rows + 1024;
+    if (span_cap > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 spans");
+    if (n_rows > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 rows");
+    if ((rc = ensure(c, c->s_row_idx, std::max<uint64_t>(1, n_rows) * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_spans, span_cap * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_ovf, std::max<uint64_t>(1, n_rows) * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
+    stage(c, 8);
+    k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
+        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, nullptr,
+        as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list));
+    c->launches += 1;
+    stage_end(c, 8);
+    stage(c, 9);
+    if (n_chunks) {
+        int g = grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16);
+        k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
+            as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
+            as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+            static_cast<uint32_t>(span_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_rows)),
+            as<BatchCounters>(c->s_ctr), chunk_rows);
+        c->launches += 1;
+    }
+    stage_end(c, 9);
+    RRB_CUDA(c, cudaGetLastError());
+    // Slow rows, if any: read the overflow count.
+    if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+    BatchCounters hc;
+    std::memcpy(&hc, c->h_read, sizeof hc);
+    uint64_t slow_rows = std::min<uint64_t>(hc.ovf_count, n_rows);
+    if (slow_rows) {
+        uint64_t need = std::min<uint64_t>(slow_rows * 256 + n_edges, 0x7FFFFFFFull);
+        stage(c, 10);
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            if ((rc = ensure(c, c->s_scratch, need * sizeof(int3)))) return rc;
+            uint32_t zero = 0;
+            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &zero, 4, cudaMemcpyHostToDevice,
+                                        c->stream));
+            k_rows_slow<<<grid_for(c, slow_rows, 128), 128, 0, c->stream>>>(
+                as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), as<uint32_t>(B->pw),
+                as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_rows)), as<int3>(c->s_scratch),
+                static_cast<uint32_t>(c->s_scratch.cap / sizeof(int3)), as<uint2>(c->s_row_idx),
+                as<uint32_t>(c->s_spans), static_cast<uint32_t>(span_cap), as<BatchCounters>(c->s_ctr));
+            c->launches += 1;
+            RRB_CUDA(c, cudaGetLastError());
+            if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+            std::memcpy(&hc, c->h_read, sizeof hc);
+            if (!(hc.err & ERR_SCRATCH_CAP)) break;
+            // Not enough scratch: grow to what was asked for and run again.
+            need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + n_edges, 0x7FFFFFFFull);
+            uint32_t e0 = hc.err & ~ERR_SCRATCH_CAP;
+            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->err, &e0, 4, cudaMemcpyHostToDevice, c->stream));
+        }
+        stage_end(c, 10);
+    }
+    // ---- stage 4: composite
+    stage(c, 11);
+    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 8),
+                               as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
+                               as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
+                               as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), arena, rowmap,
+                               as<BatchCounters>(c->s_ctr))))
+        return rc;
+    stage_end(c, 11);
+    if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+    std::memcpy(&hc, c->h_read, sizeof hc);
+    c->stats.paths = n_paths;
+    c->stats.pieces = n_pts;
+    c->stats.segments = n_edges;
+    c->stats.aa_rows = n_rows;
+    c->stats.spans = hc.span_cursor;
+    c->stats.row_overflows = hc.ovf_count;
+    c->stats.tiles = tiles;
+    c->stats.tile_pairs = n_pairs;
+    c->stats.nonterminating_rows = hc.nonterminating;
+    c->stats.kernel_launches = c->launches;
+    if (c->timer && c->timer->on) {
+        // The final read_back synchronised the stream: every event is complete.
+        for (int k = 0; k < kStages; ++k) {
+            float ms = 0.f;
+            if (c->timer->used[k]) cudaEventElapsedTime(&ms, c->timer->begin[k], c->timer->end[k]);
+            c->stage_ms[k] = ms;
+            c->stage_launches[k] = c->timer->used[k] ? c->timer->launches[k] : 0;
+        }
+    }
+    if (hc.err) {
+        char buf[128];
+        std::snprintf(buf, sizeof buf, "batch capacity exceeded (error bits 0x%x); pages left untouched", hc.err);
+        return set_err(c, RRB_ERR_POOL_EXHAUSTED, buf);
+    }
+    return RRB_OK;
+}
+
+int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len) {
+    rrb_batch* B = c->tmp_batch;
+    int rc = batch_upload(c, h, B);
+    if (rc) return rc;
+    return run_resident(c, B, arena, arena_len, h->rowmap);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rrb_version(void) { return "rrb 0.1 sm_100a"; }
+
+const char* rrb_status_name(int s) {
+    switch (s) {
+        case RRB_OK: return "ok";
+        case RRB_ERR_ZERO_SIZE_ALLOC: return "ZeroSizeAlloc";
+        case RRB_ERR_UNALIGNED_FILL: return "UnalignedFill";
+        case RRB_ERR_POOL_EXHAUSTED: return "PoolExhausted";
+        case RRB_ERR_INVARIANT: return "InvariantViolation";
+        case RRB_ERR_OTHER: return "Other";
+        case RRB_ERR_TIMEOUT: return "Timeout";
+        case RRB_ERR_DEVICE: return "DeviceError";
+        case RRB_ERR_OUT_OF_MEMORY: return "OutOfMemory";
+        case RRB_ERR_STATE: return "StateError";
+        default: return "unknown";
+    }
+}
+
+int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
+    if (!out) return RRB_ERR_INVARIANT;
+    *out = nullptr;
+    rrb_ctx* c = new rrb_ctx();
+    c->device = device;
+    c->budget = mem_budget_bytes;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        return RRB_ERR_DEVICE;
+    }
+    int sm = 0;
+    if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sm > 0)
+        c->sm_count = sm;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return RRB_ERR_DEVICE;
+    }
+    e = cudaMallocHost(reinterpret_cast<void**>(&c->h_read), 4096);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return RRB_ERR_DEVICE;
+    }
+    c->tmp_batch = new rrb_batch();
+    c->tuning.tile_w = 64;
+    c->tuning.tile_h = 16;
+    c->tuning.rows_per_chunk = 32;
+    *out = c;
+    return RRB_OK;
+}
+
+int rrb_destroy(rrb_ctx* c) {
+    if (!c) return RRB_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    Scratch* all[] = {&c->s_pts, &c->s_flags, &c->s_off, &c->s_rule, &c->s_gray, &c->s_alpha, &c->s_page,
+                      &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
+                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
+                      &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats};
+    for (Scratch* s : all) dev_free(c, s->p, s->cap);
+    if (c->tmp_batch) {
+        free_batch_bufs(c, c->tmp_batch);
+        delete c->tmp_batch;
+    }
+    if (c->timer) {
+        for (int k = 0; k < kStages; ++k) {
+            cudaEventDestroy(c->timer->begin[k]);
+            cudaEventDestroy(c->timer->end[k]);
+        }
+        delete c->timer;
+    }
+    for (auto& kv : c->fences) cudaEventDestroy(kv.second);
+    for (cudaEvent_t ev : c->free_events) cudaEventDestroy(ev);
+    if (c->h_read) cudaFreeHost(c->h_read);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return RRB_OK;
+}
+
+const char* rrb_last_error_message(const rrb_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+int rrb_alloc_device(rrb_ctx* c, size_t size, rrb_buf** out) {
+    if (!c || !out) return RRB_ERR_INVARIANT;
+    if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_device called with size = 0");
+    cudaSetDevice(c->device);
+    void* p = nullptr;
+    int rc = dev_alloc(c, size, &p);
+    if (rc) return rc;
+    *out = new rrb_buf{p, size};
+    return RRB_OK;
+}
+
+int rrb_alloc_device_zeroed(rrb_ctx* c, size_t size, rrb_buf** out) {
+    if (!c || !out) return RRB_ERR_INVARIANT;
+    if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_device_zeroed called with size = 0");
+    int rc = rrb_alloc_device(c, size, out);
+    if (rc) return rc;
+    RRB_CUDA(c, cudaMemsetAsync((*out)->p, 0, size, c->stream));
+    RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    return RRB_OK;
+}
+
+size_t rrb_device_buffer_len(const rrb_buf* b) { return b ? b->len : 0; }
+void* rrb_device_ptr(const rrb_buf* b) { return b ? b->p : nullptr; }
+
+int rrb_free_device(rrb_ctx* c, rrb_buf* b) {
+    if (!c || !b) return RRB_ERR_INVARIANT;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    dev_free(c, b->p, b->len);
+    delete b;
+    return RRB_OK;
+}
+
+int rrb_alloc_host_pinned(rrb_ctx* c, size_t size, rrb_host_buf** out) {
+    if (!c || !out) return RRB_ERR_INVARIANT;
+    if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_host_pinned called with size = 0");
+    void* p = nullptr;
+    RRB_CUDA(c, cudaMallocHost(&p, size));
+    *out = new rrb_host_buf{p, size};
+    return RRB_OK;
+}
+
+void* rrb_host_ptr(const rrb_host_buf* b) { return b ? b->p : nullptr; }
+
+int rrb_free_host_pinned(rrb_ctx* c, rrb_host_buf* b) {
+    if (!c || !b) return RRB_ERR_INVARIANT;
+    cudaStreamSynchronize(c->stream);
+    cudaFreeHost(b->p);
+    delete b;
+    return RRB_OK;
+}
+
+static int record_fence(rrb_ctx* c, rrb_fence* out) {
+    cudaEvent_t ev;
+    if (!c->free_events.empty()) {
+        ev = c->free_events.back();
+        c->free_events.pop_back();
+    } else {
+        RRB_CUDA(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    RRB_CUDA(c, cudaEventRecord(ev, c->stream));
+    uint64_t id = c->next_fence++;
+    c->fences[id] = ev;
+    if (out) *out = id;
+    return RRB_OK;
+}
+
+static int wait_fence(rrb_ctx* c, rrb_fence f, uint64_t timeout_ns) {
+    auto it = c->fences.find(f);
+    if (it == c->fences.end()) return set_err(c, RRB_ERR_INVARIANT, "unknown fence");
+    cudaEvent_t ev = it->second;
+    auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_err(c, e, "cudaEventQuery");
+        if (timeout_ns) {
+            auto dt = std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0);
+            if (static_cast<uint64_t>(dt.count()) > timeout_ns)
+                return set_err(c, RRB_ERR_TIMEOUT, "fence not signalled within timeout");
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+    c->fences.erase(it);
+    c->free_events.push_back(ev);
+    return RRB_OK;
+}
+
+int rrb_upload_async(rrb_ctx* c, const rrb_buf* dst, size_t off, const void* src, size_t len, rrb_fence* out) {
+    if (!c || !dst || (!src && len)) return RRB_ERR_INVARIANT;
+    if (off > dst->len || len > dst->len - off)
+        return set_err(c, RRB_ERR_INVARIANT, "upload exceeds the device buffer");
+    cudaSetDevice(c->device);
+    if (len) RRB_CUDA(c, cudaMemcpyAsync(static_cast<char*>(dst->p) + off, src, len, cudaMemcpyHostToDevice, c->stream));
+    return record_fence(c, out);
+}
+
+int rrb_download_async(rrb_ctx* c, const rrb_buf* src, size_t off, void* dst, size_t len, rrb_fence* out) {
+    if (!c || !src || (!dst && len)) return RRB_ERR_INVARIANT;
+    if (off > src->len || len > src->len - off)
+        return set_err(c, RRB_ERR_INVARIANT, "download exceeds the device buffer");
+    cudaSetDevice(c->device);
+    if (len) RRB_CUDA(c, cudaMemcpyAsync(dst, static_cast<const char*>(src->p) + off, len, cudaMemcpyDeviceToHost, c->stream));
+    return record_fence(c, out);
+}
+
+int rrb_wait_download(rrb_ctx* c, rrb_fence f) { return c ? wait_fence(c, f, 0) : RRB_ERR_INVARIANT; }
+int rrb_submit_transfer(rrb_ctx* c, rrb_fence* out) { return c ? record_fence(c, out) : RRB_ERR_INVARIANT; }
+int rrb_wait_transfer(rrb_ctx* c, rrb_fence f, uint64_t t) { return c ? wait_fence(c, f, t) : RRB_ERR_INVARIANT; }
+
+int rrb_detect_vram_budget(rrb_ctx* c, rrb_vram_budget* out) {
+    if (!c || !out) return RRB_ERR_INVARIANT;
+    cudaSetDevice(c->device);
+    size_t fr = 0, tot = 0;
+    RRB_CUDA(c, cudaMemGetInfo(&fr, &tot));
+    out->total_bytes = tot;
+    out->free_bytes = fr;
+    out->budget_bytes = c->budget;
+    out->used_bytes = c->used;
+    return RRB_OK;
+}
+
+int rrb_begin_page(rrb_ctx* c) {
+    if (!c) return RRB_ERR_INVARIANT;
+    if (c->in_page) return set_err(c, RRB_ERR_STATE, "begin_page while a page is open");
+    c->in_page = true;
+    return RRB_OK;
+}
+
+int rrb_record_zero_buffer(rrb_ctx* c, const rrb_buf* b) {
+    if (!c || !b) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    RRB_CUDA(c, cudaMemsetAsync(b->p, 0, b->len, c->stream));
+    return RRB_OK;
+}
+
+int rrb_submit_page(rrb_ctx* c, rrb_fence* out) {
+    if (!c) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "submit_page without begin_page");
+    c->in_page = false;
+    return record_fence(c, out);
+}
+
+int rrb_wait_page(rrb_ctx* c, rrb_fence f, uint64_t timeout_ns) {
+    return c ? wait_fence(c, f, timeout_ns) : RRB_ERR_INVARIANT;
+}
+
+int rrb_set_tuning(rrb_ctx* c, const rrb_tuning* t) {
+    if (!c || !t) return RRB_ERR_INVARIANT;
+    uint32_t w = t->tile_w ? t->tile_w : c->tuning.tile_w, h = t->tile_h ? t->tile_h : c->tuning.tile_h;
+    if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32 or 64x16");
+    c->tuning.tile_w = w;
+    c->tuning.tile_h = h;
+    return RRB_OK;
+}
+
+int rrb_get_tuning(rrb_ctx* c, rrb_tuning* t) {
+    if (!c || !t) return RRB_ERR_INVARIANT;
+    *t = c->tuning;
+    return RRB_OK;
+}
+
+int rrb_last_batch_stats(rrb_ctx* c, rrb_batch_stats* out) {
+    if (!c || !out) return RRB_ERR_INVARIANT;
+    *out = c->stats;
+    return RRB_OK;
+}
+
+int rrb_record_path_batch(rrb_ctx* c, const rrb_path_batch_params* p) {
+    if (!c || !p) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
+    cudaSetDevice(c->device);
+    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len);
+}
+
+int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, char* msg, size_t msg_len) {
+    if (!p) return RRB_ERR_INVARIANT;
+    std::vector<PageGeom> geom;
+    uint64_t tiles = 0, supers = 0;
+    std::string m;
+    int rc = validate_batch(p, pages_len, 64, 16, geom, tiles, supers, m);
+    if (msg && msg_len) {
+        std::snprintf(msg, msg_len, "%s", m.c_str());
+    }
+    return rc;
+}
+
+int rrb_record_path_fill(rrb_ctx* c, const rrb_path_fill_params* p) {
+    if (!c || !p) return RRB_ERR_INVARIANT;
+    if (!p->page) return set_err(c, RRB_ERR_INVARIANT, "page buffer is null");
+    if (p->n_pts && (!p->pts || !p->flags)) return set_err(c, RRB_ERR_INVARIANT, "null path arrays");
+    if (p->fill_rule > 1) return set_err(c, RRB_ERR_INVARIANT, "fill_rule must be 0 or 1");
+    rrb_path_batch_params b;
+    std::memset(&b, 0, sizeof b);
+    uint64_t off[2] = {0, p->n_pts};
+    uint32_t page = 0, w = p->width, h = p->height;
+    uint64_t po = p->page_offset;
+    b.pts = p->pts;
+    b.flags = p->flags;
+    b.n_pts = p->n_pts;
+    b.path_pt_off = off;
+    b.fill_rule = &p->fill_rule;
+    b.gray = &p->gray;
+    b.alpha = &p->alpha;
+    b.path_page = &page;
+    b.n_paths = p->n_pts ? 1 : 0;
+    b.page_width = &w;
+    b.page_height = &h;
+    b.page_offset = &po;
+    b.n_pages = 1;
+    b.pages = p->page;
+    std::memcpy(b.matrix, p->matrix, sizeof b.matrix);
+    b.flatness = p->flatness;
+    b.rowmap = p->rowmap;
+    return rrb_record_path_batch(c, &b);
+}
+
+int rrb_batch_upload(rrb_ctx* c, const rrb_path_batch_params* p, rrb_batch** out) {
+    if (!c || !p || !out) return RRB_ERR_INVARIANT;
+    cudaSetDevice(c->device);
+    rrb_batch* B = new rrb_batch();
+    int rc = batch_upload(c, p, B);
+    if (rc) {
+        free_batch_bufs(c, B);
+        delete B;
+        return rc;
+    }
+    RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    *out = B;
+    return RRB_OK;
+}
+
+int rrb_record_batch(rrb_ctx* c, rrb_batch* B, const rrb_buf* pages, int rowmap) {
+    if (!c || !B || !pages) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    cudaSetDevice(c->device);
+    return run_resident(c, B, static_cast<uint8_t*>(pages->p), pages->len, rowmap);
+}
+
+int rrb_batch_free(rrb_ctx* c, rrb_batch* B) {
+    if (!c || !B) return RRB_ERR_INVARIANT;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_batch_bufs(c, B);
+    delete B;
+    return RRB_OK;
+}
+
+int rrb_record_fill_buffer(rrb_ctx* c, const rrb_buf* b, size_t off, size_t len, uint8_t value) {
+    if (!c || !b) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    if (off > b->len || len > b->len - off) return set_err(c, RRB_ERR_INVARIANT, "fill exceeds the device buffer");
+    RRB_CUDA(c, cudaMemsetAsync(static_cast<char*>(b->p) + off, value, len, c->stream));
+    return RRB_OK;
+}
+
+void* rrb_stream(rrb_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+int rrb_set_profiling(rrb_ctx* c, int enable) {
+    if (!c) return RRB_ERR_INVARIANT;
+    if (!c->timer) {
+        c->timer = new StageTimer();
+        for (int k = 0; k < kStages; ++k) {
+            RRB_CUDA(c, cudaEventCreate(&c->timer->begin[k]));
+            RRB_CUDA(c, cudaEventCreate(&c->timer->end[k]));
+        }
+    }
+    c->timer->on = enable != 0;
+    return RRB_OK;
+}
+
+int rrb_last_stage_times(rrb_ctx* c, rrb_stage_time* out, int cap, int* n) {
+    if (!c || !n) return RRB_ERR_INVARIANT;
+    int m = 0;
+    for (int k = 0; k < kStages; ++k) {
+        if (m < cap && out) {
+            std::snprintf(out[m].name, sizeof out[m].name, "%s", kStageNames[k]);
+            out[m].ms = c->stage_ms[k];
+            out[m].launches = c->stage_launches[k];
+        }
+        ++m;
+    }
+    *n = m;
+    return RRB_OK;
+}
+
+int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len) {
+    if (!c || !p || !host_pages || !p->pages) return RRB_ERR_INVARIANT;
+    if (len > p->pages->len) return set_err(c, RRB_ERR_INVARIANT, "host pages larger than the device arena");
+    cudaSetDevice(c->device);
+    RRB_CUDA(c, cudaMemcpyAsync(p->pages->p, host_pages, len, cudaMemcpyHostToDevice, c->stream));
+    int rc = rrb_begin_page(c);
+    if (rc) return rc;
+    rc = rrb_record_path_batch(c, p);
+    rrb_fence f = 0;
+    int rc2 = rrb_submit_page(c, &f);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    RRB_CUDA(c, cudaMemcpyAsync(host_pages, p->pages->p, len, cudaMemcpyDeviceToHost, c->stream));
+    return rrb_wait_page(c, f, 0) ? RRB_ERR_DEVICE : (cudaStreamSynchronize(c->stream) == cudaSuccess ? RRB_OK : RRB_ERR_DEVICE);
+}
+
+}  // extern "C"

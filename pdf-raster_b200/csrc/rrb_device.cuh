@@ -1,0 +1,298 @@
+// rrb_device.cuh — device-side arithmetic of the AA fill path.
+//
+// Every FP64 operation that the reference performs as a single IEEE op is
+// written with an explicit round-to-nearest intrinsic (__dadd_rn, __dmul_rn,
+// ...) so nvcc cannot contract it into an FMA; every f64::mul_add of the
+// reference is __fma_rn. That keeps flattening and segment set-up bit-exact
+// with the reference CPU rasterizer independently of -fmad.
+#pragma once
+
+#include <cstdint>
+
+namespace rrb {
+
+constexpr int AA = 4;                     // AA_SIZE (crates/raster/src/types.rs:27)
+constexpr int MAX_CURVE_SPLITS = 1024;    // types.rs:36
+constexpr int FLATTEN_STACK = 10;         // log2(MAX_CURVE_SPLITS) pending right halves
+
+// PathFlags (crates/raster/src/path/mod.rs:70-79).
+constexpr uint8_t PF_FIRST = 0x01, PF_LAST = 0x02, PF_CLOSED = 0x04, PF_CURVE = 0x08;
+
+// Edge kinds of the int32 edge record.
+constexpr int EK_HORIZ = 0, EK_VERT = 1, EK_SLOPED = 2;
+constexpr int EF_KIND_MASK = 3, EF_POSITIVE = 4, EF_FIRST_ZERO = 8, EF_EMPTY = 16;
+
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// f64::midpoint (Rust std): (a+b)/2 when both |a|,|b| <= f64::MAX/2.
+__device__ __forceinline__ double midpoint(double a, double b) {
+    const double HI = 8.98846567431157854e+307;   // f64::MAX / 2
+    const double LO = 4.45014771701440277e-308;   // f64::MIN_POSITIVE * 2
+    double aa = fabs(a), ab = fabs(b);
+    if (aa <= HI && ab <= HI) return ddiv(dadd(a, b), 2.0);
+    if (aa < LO) return dadd(a, ddiv(b, 2.0));
+    if (ab < LO) return dadd(ddiv(a, 2.0), b);
+    return dadd(ddiv(a, 2.0), ddiv(b, 2.0));
+}
+
+// saturate_f64_to_i32 / splash_floor (crates/color/src/convert.rs:221-265).
+__device__ __forceinline__ int32_t sat_i32_of_integral(double x) {
+    if (!isfinite(x)) return x == __longlong_as_double(0x7ff0000000000000LL) ? INT32_MAX : INT32_MIN;
+    if (x >= 2147483647.0) return INT32_MAX;
+    if (x <= -2147483648.0) return INT32_MIN;
+    return static_cast<int32_t>(x);
+}
+__device__ __forceinline__ int32_t splash_floor(double x) { return sat_i32_of_integral(floor(x)); }
+
+// fp_from_f64 (crates/raster/src/scanner/mod.rs:51-66): truncating 16.16.
+__device__ __forceinline__ int32_t fp_from_f64(double x) {
+    double fp = dmul(x, 65536.0);
+    if (fp >= 2147483647.0) return INT32_MAX;
+    if (fp <= -2147483648.0) return INT32_MIN;
+    if (isnan(fp)) return 0;
+    return __double2int_rz(fp);
+}
+
+__device__ __forceinline__ int32_t sat_i64_to_i32(long long v) {
+    return v > INT32_MAX ? INT32_MAX : (v < INT32_MIN ? INT32_MIN : static_cast<int32_t>(v));
+}
+
+// transform (crates/raster/src/xpath.rs:421-426).
+__device__ __forceinline__ void transform(const double* m, double x, double y, double& ox, double& oy) {
+    ox = dfma(x, m[0], dfma(y, m[2], m[4]));
+    oy = dfma(x, m[1], dfma(y, m[3], m[5]));
+}
+
+// The int32 edge record: everything fill_intersections (scanner/mod.rs:511-587)
+// derives from one AA-scaled XPathSeg, so the row stage needs no FP64.
+//   row0,row1  clipped AA row range (EF_EMPTY when none)
+//   flags      kind | EF_POSITIVE (FLIPPED: count +1, else -1) | EF_FIRST_ZERO
+//              (row0 is not strictly below seg_y_min: count 0 on row0)
+//   a          HORIZ: floor(min x); VERT: floor(x0); SLOPED: px0 of row0
+//   b          HORIZ: floor(max x); SLOPED: xx1_fp of row0 (16.16)
+//   dfp        SLOPED: dxdy_fp; cmin/cmax: SLOPED 16.16 clamp bounds
+struct __align__(16) Edge {
+    int32_t row0, row1, flags, a, b, dfp, cmin, cmax;
+};
+
+// add_segment (xpath.rs:324-402) + aa_scale (xpath.rs:283-303) + the
+// per-segment set-up of count/fill_intersections, clipped to AA rows
+// [clip_lo, clip_hi].
+__device__ __forceinline__ Edge make_edge(double x0, double y0, double x1, double y1, int32_t clip_lo,
+                                          int32_t clip_hi) {
+    Edge e;
+    e.dfp = 0;
+    e.cmin = 0;
+    e.cmax = 0;
+    e.b = 0;
+    unsigned long long by0 = __double_as_longlong(y0), by1 = __double_as_longlong(y1);
+    unsigned long long bx0 = __double_as_longlong(x0), bx1 = __double_as_longlong(x1);
+    if (by0 == by1) {
+        // HORIZ: never flipped, dxdy = 0; aa_scale then multiplies by 4.
+        double sx0 = dmul(x0, 4.0), sx1 = dmul(x1, 4.0), sy = dmul(y0, 4.0);
+        e.flags = EK_HORIZ;
+        if (isnan(sx0) || isnan(sy)) {
+            e.flags |= EF_EMPTY;
+            e.row0 = 1;
+            e.row1 = 0;
+            e.a = 0;
+            return e;
+        }
+        int32_t row = splash_floor(sy);
+        if (row >= clip_lo && row <= clip_hi) {
+            e.row0 = row;
+            e.row1 = row;
+        } else {
+            e.flags |= EF_EMPTY;
+            e.row0 = 1;
+            e.row1 = 0;
+        }
+        e.a = splash_floor(fmin(sx0, sx1));
+        e.b = splash_floor(fmax(sx0, sx1));
+        return e;
+    }
+    bool vert = bx0 == bx1;
+    double dxdy = vert ? 0.0 : ddiv(dsub(x1, x0), dsub(y1, y0));
+    bool flipped = false;
+    if (y0 > y1) {
+        double t = x0; x0 = x1; x1 = t;
+        t = y0; y0 = y1; y1 = t;
+        flipped = true;
+    }
+    int32_t dxdy_fp;
+    {
+        double fp = dmul(dxdy, 65536.0);
+        if (fp >= 2147483647.0) dxdy_fp = INT32_MAX;
+        else if (fp <= -2147483648.0) dxdy_fp = INT32_MIN;
+        else if (isnan(fp)) dxdy_fp = 0;
+        else dxdy_fp = static_cast<int32_t>(round(fp));
+    }
+    x0 = dmul(x0, 4.0);
+    y0 = dmul(y0, 4.0);
+    x1 = dmul(x1, 4.0);
+    y1 = dmul(y1, 4.0);
+    e.flags = (vert ? EK_VERT : EK_SLOPED) | (flipped ? EF_POSITIVE : 0);
+    if (isnan(x0) || isnan(y0)) {
+        e.flags |= EF_EMPTY;
+        e.row0 = 1;
+        e.row1 = 0;
+        e.a = 0;
+        return e;
+    }
+    double sy_min = fmin(y0, y1), sy_max = fmax(y0, y1);
+    int32_t r0 = max(splash_floor(sy_min), clip_lo);
+    int32_t r1 = min(splash_floor(sy_max), clip_hi);
+    e.row0 = r0;
+    e.row1 = r1;
+    if (r0 > r1) e.flags |= EF_EMPTY;
+    if (!(sy_min < static_cast<double>(r0))) e.flags |= EF_FIRST_ZERO;
+    if (vert) {
+        e.a = splash_floor(x0);
+        return e;
+    }
+    double x_base = dfma(y0, -dxdy, x0);
+    double sxmin = fmin(x0, x1), sxmax = fmax(x0, x1);
+    e.cmin = fp_from_f64(sxmin);
+    e.cmax = fp_from_f64(sxmax);
+    double r0d = static_cast<double>(r0);
+    double xx_init = r0d > y0 ? dfma(r0d, dxdy, x_base) : x0;
+    double xc = xx_init;
+    if (xc < sxmin) xc = sxmin;
+    if (xc > sxmax) xc = sxmax;
+    e.a = splash_floor(xc);
+    e.b = fp_from_f64(dfma(dadd(r0d, 1.0), dxdy, x_base));
+    e.dfp = dxdy_fp;
+    return e;
+}
+
+// Intersect entry of edge `e` on AA row r (row0 <= r <= row1): the closed form
+// of fill_intersections' stepping. The saturating accumulator
+// xx1_fp += dxdy_fp is monotone, so after k steps it equals the exact sum
+// clamped to the i32 range.
+__device__ __forceinline__ void edge_entry(const Edge& e, int32_t r, int32_t& lo, int32_t& hi, int32_t& c) {
+    int kind = e.flags & EF_KIND_MASK;
+    if (kind == EK_HORIZ) {
+        lo = e.a;
+        hi = e.b;
+        c = 0;
+        return;
+    }
+    c = ((e.flags & EF_FIRST_ZERO) && r == e.row0) ? 0 : ((e.flags & EF_POSITIVE) ? 1 : -1);
+    if (kind == EK_VERT) {
+        lo = e.a;
+        hi = e.a;
+        return;
+    }
+    long long k = static_cast<long long>(r) - e.row0;
+    int32_t x1v = sat_i64_to_i32(static_cast<long long>(e.b) + k * e.dfp);
+    int32_t px1 = min(max(x1v, e.cmin), e.cmax) >> 16;
+    int32_t px0;
+    if (k == 0) {
+        px0 = e.a;
+    } else {
+        int32_t x0v = sat_i64_to_i32(static_cast<long long>(e.b) + (k - 1) * e.dfp);
+        px0 = min(max(x0v, e.cmin), e.cmax) >> 16;
+    }
+    lo = min(px0, px1);
+    hi = max(px0, px1);
+}
+
+// AA column range [lo, hi] of the entries an edge can produce.
+__device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo, int32_t& hi) {
+    int kind = e.flags & EF_KIND_MASK;
+    if (kind == EK_HORIZ) {
+        lo = e.a;
+        hi = e.b;
+    } else if (kind == EK_VERT) {
+        lo = e.a;
+        hi = e.a;
+    } else {
+        lo = min(e.a, e.cmin >> 16);
+        hi = max(e.a, e.cmax >> 16);
+    }
+}
+
+// flatten_curve (crates/raster/src/path/flatten.rs:109-215) with the slot
+// arrays replaced by the chain of pending right halves: slot p's data is
+// (start, c1, c2) and its endpoint is the start of the next pending slot (or
+// p3 when that is slot MAX_CURVE_SPLITS). Splitting [pp1,pp2] pushes slot
+// pp3 = (pp1+pp2)/2; emitting pops. Interval lengths halve per push, so at
+// most log2(1024) = 10 halves are pending. Same operations in the same
+// order as the reference, hence the same points.
+template <typename Emit>
+__device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                             double p2y, double p3x, double p3y, double flat_sq,
+                                             Emit emit) {
+    double sx[FLATTEN_STACK][6];
+    int sidx[FLATTEN_STACK];
+    int top = 0;
+    double c0x = p0x, c0y = p0y, c1x = p1x, c1y = p1y, c2x = p2x, c2y = p2y;
+    int pp1 = 0;
+    int count = 0;
+    while (pp1 < MAX_CURVE_SPLITS) {
+        int pp2;
+        double xr3, yr3;
+        if (top > 0) {
+            pp2 = sidx[top - 1];
+            xr3 = sx[top - 1][0];
+            yr3 = sx[top - 1][1];
+        } else {
+            pp2 = MAX_CURVE_SPLITS;
+            xr3 = p3x;
+            yr3 = p3y;
+        }
+        double mx = midpoint(c0x, xr3), my = midpoint(c0y, yr3);
+        double dx1 = dsub(c1x, mx), dy1 = dsub(c1y, my);
+        double dx2 = dsub(c2x, mx), dy2 = dsub(c2y, my);
+        double d1 = dfma(dx1, dx1, dmul(dy1, dy1));
+        double d2 = dfma(dx2, dx2, dmul(dy2, dy2));
+        if (pp2 - pp1 == 1 || (d1 <= flat_sq && d2 <= flat_sq)) {
+            emit(xr3, yr3);
+            ++count;
+            pp1 = pp2;
+            if (top > 0) {
+                --top;
+                c0x = sx[top][0];
+                c0y = sx[top][1];
+                c1x = sx[top][2];
+                c1y = sx[top][3];
+                c2x = sx[top][4];
+                c2y = sx[top][5];
+            }
+        } else {
+            double xl1 = midpoint(c0x, c1x), yl1 = midpoint(c0y, c1y);
+            double xh = midpoint(c1x, c2x), yh = midpoint(c1y, c2y);
+            double xl2 = midpoint(xl1, xh), yl2 = midpoint(yl1, yh);
+            double xr2 = midpoint(c2x, xr3), yr2 = midpoint(c2y, yr3);
+            double xr1 = midpoint(xh, xr2), yr1 = midpoint(yh, yr2);
+            double xr0 = midpoint(xl2, xr1), yr0 = midpoint(yl2, yr1);
+            int pp3 = (pp1 + pp2) >> 1;
+            // pp2 - pp1 >= 2 here, so fewer than FLATTEN_STACK halves are pending.
+            sx[top][0] = xr0;
+            sx[top][1] = yr0;
+            sx[top][2] = xr1;
+            sx[top][3] = yr1;
+            sx[top][4] = xr2;
+            sx[top][5] = yr2;
+            sidx[top] = pp3;
+            ++top;
+            c1x = xl1;
+            c1y = yl1;
+            c2x = xl2;
+            c2y = yl2;
+        }
+    }
+    return count;
+}
+
+// div255 (crates/color/src/convert.rs:50-58).
+__device__ __forceinline__ uint32_t div255(uint32_t x) {
+    uint32_t s = (x + (x >> 8) + 0x80u) >> 8;
+    return s > 255u ? 255u : s;
+}
+
+}  // namespace rrb

@@ -1,0 +1,840 @@
+// rrb_kernels.cuh — the AA fill pipeline kernels.
+//
+// Stage map onto the reference CPU path (crates/raster):
+//   k_walk          XPath::new subpath walk (xpath.rs:162-260), incl. the
+//                   curve-branch LAST quirk and the 1e-10 closing test
+//   k_seg_count     flatten_curve pass 1 (path/flatten.rs:109-215): counts
+//   k_seg_write     flatten_curve pass 2 + add_segment + aa_scale + the
+//                   per-segment set-up of fill_intersections -> Edge records
+//   k_path_bbox     XPathScanner::new bounding box (scanner/mod.rs:131-180)
+//   k_super_*       per-page tile binning: ordered path lists per supertile
+//   k_rows          fill_intersections + write_intersect merge + per-row sort
+//                   + render_aa_line winding walk (scanner/mod.rs:393-642),
+//                   one warp per 32 AA rows of one path
+//   k_rows_slow     the same for rows whose merged list exceeds shared memory
+//   k_composite     draw_aa_line coverage + AA_GAMMA + render_span_aa div255
+//                   source-over (fill/mod.rs:344-401, pipe/aa.rs:192-208),
+//                   one CTA per page tile, paths in index order
+#pragma once
+
+#include <cstdint>
+
+#include "rrb_device.cuh"
+
+namespace rrb {
+
+// Piece slots: one per input point. kind in bits 30-31 of .y.
+constexpr uint32_t PK_NONE = 0, PK_LINE = 1, PK_CURVE = 2, PK_CLOSE = 3;
+
+struct PathInfo {
+    int32_t y0, y1;          // AA rows [y0, y1] (y0 > y1: no rows)
+    int32_t px0, px1;        // pixel columns touched (px0 > px1: none)
+    int32_t py0, py1;        // pixel rows touched under the row map
+    uint32_t e_begin, e_end; // edge range
+    uint32_t paint;          // gray | alpha << 8 | rule << 16
+    uint32_t page;
+    uint32_t pad0, pad1;
+};
+
+// Error / status word bits shared by all kernels of a batch.
+constexpr uint32_t ERR_EDGE_CAP = 1, ERR_ROW_CAP = 2, ERR_SPAN_CAP = 4, ERR_OVF_CAP = 8,
+                   ERR_SCRATCH_CAP = 16, ERR_SUPER_CAP = 32;
+
+// Device counters of a batch.
+struct BatchCounters {
+    uint32_t err;
+    uint32_t span_cursor;
+    uint32_t ovf_count;
+    uint32_t scratch_cursor;
+    uint32_t nonterminating;
+    uint32_t pad[3];
+    unsigned long long raw_entries;  // sum over edges of the rows they cover
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// XPath::new walk, one thread per path. Pieces are written at the path's
+// point slots [off, off+n); unused slots get PK_NONE. Point indices are global.
+// ---------------------------------------------------------------------------
+__global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict__ flags,
+                       const uint64_t* __restrict__ path_pt_off, uint32_t n_paths,
+                       const double* __restrict__ mtx, const uint32_t* __restrict__ path_page,
+                       const uint32_t* __restrict__ page_h, uint2* __restrict__ pieces,
+                       uint32_t* __restrict__ slot_clip_hi) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        uint32_t off = static_cast<uint32_t>(path_pt_off[p]);
+        uint32_t n = static_cast<uint32_t>(path_pt_off[p + 1]) - off;
+        uint32_t slot = off;
+        const uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u;
+        for (uint32_t k = 0; k < n; ++k) slot_clip_hi[off + k] = clip_hi;
+        uint32_t i = 0;
+        while (i < n) {
+            if (flags[off + i] & PF_FIRST) {
+                uint32_t sp = i, cur = i;
+                ++i;
+                while (i < n) {
+                    uint8_t f = flags[off + i];
+                    if (f & PF_CURVE) {
+                        if (i + 2 >= n) break;
+                        pieces[slot++] = make_uint2(off + cur, (PK_CURVE << 30) | (off + i));
+                        cur = i + 2;
+                        i += 3;
+                    } else {
+                        pieces[slot++] = make_uint2(off + cur, (PK_LINE << 30) | (off + i));
+                        cur = i;
+                        ++i;
+                        if (f & PF_LAST) break;
+                    }
+                }
+                double sx, sy, cx, cy;
+                transform(m, pts[2 * (off + sp)], pts[2 * (off + sp) + 1], sx, sy);
+                transform(m, pts[2 * (off + cur)], pts[2 * (off + cur) + 1], cx, cy);
+                if (fabs(dsub(cx, sx)) > 1e-10 || fabs(dsub(cy, sy)) > 1e-10)
+                    pieces[slot++] = make_uint2(off + cur, (PK_CLOSE << 30) | (off + sp));
+            } else {
+                ++i;
+            }
+        }
+        for (; slot < off + n; ++slot) pieces[slot] = make_uint2(0u, PK_NONE << 30);
+    }
+}
+
+__device__ __forceinline__ void load_tpt(const double* pts, const double* m, uint32_t i, double& x, double& y) {
+    transform(m, pts[2 * i], pts[2 * i + 1], x, y);
+}
+
+// Segments per piece slot.
+__global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
+                            const double* __restrict__ mtx, double flat_sq, uint32_t* __restrict__ counts) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
+        uint2 pc = pieces[s];
+        uint32_t kind = pc.y >> 30;
+        uint32_t c = 0;
+        if (kind == PK_LINE || kind == PK_CLOSE) {
+            c = 1;
+        } else if (kind == PK_CURVE) {
+            uint32_t i = pc.y & 0x3fffffffu;
+            double x0, y0, x1, y1, x2, y2, x3, y3;
+            load_tpt(pts, m, pc.x, x0, y0);
+            load_tpt(pts, m, i, x1, y1);
+            load_tpt(pts, m, i + 1, x2, y2);
+            load_tpt(pts, m, i + 2, x3, y3);
+            c = flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [](double, double) {});
+        }
+        counts[s] = c;
+    }
+}
+
+// Edge records per piece slot, at edge_off[slot].
+__global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
+                            const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
+                            uint32_t edge_cap, Edge* __restrict__ edges,
+                            const uint32_t* __restrict__ slot_clip_hi) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
+        uint2 pc = pieces[s];
+        uint32_t kind = pc.y >> 30;
+        if (kind == PK_NONE) continue;
+        uint32_t base = edge_off[s];
+        int32_t chi = static_cast<int32_t>(slot_clip_hi[s]);
+        uint32_t j = pc.y & 0x3fffffffu;
+        double x0, y0;
+        load_tpt(pts, m, pc.x, x0, y0);
+        if (kind == PK_LINE || kind == PK_CLOSE) {
+            double x1, y1;
+            load_tpt(pts, m, j, x1, y1);
+            if (base < edge_cap) edges[base] = make_edge(x0, y0, x1, y1, 0, chi);
+        } else {
+            double x1, y1, x2, y2, x3, y3;
+            load_tpt(pts, m, j, x1, y1);
+            load_tpt(pts, m, j + 1, x2, y2);
+            load_tpt(pts, m, j + 2, x3, y3);
+            double cx = x0, cy = y0;
+            uint32_t k = base;
+            flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [&](double fx, double fy) {
+                if (k < edge_cap) edges[k] = make_edge(cx, cy, fx, fy, 0, chi);
+                ++k;
+                cx = fx;
+                cy = fy;
+            });
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan of u32 (three phases, host-known n).
+// out[i] = sum(in[0..i)), out[n] = total. in and out may alias.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_MAX_BLOCKS = 1024;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    int nw = blockDim.x >> 5;
+    if (warp == 0) {
+        uint32_t w = lane < nw ? sh[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) sh[lane] = w;
+    }
+    __syncthreads();
+    uint32_t wp = warp ? sh[warp - 1] : 0u;
+    total = sh[nw - 1];
+    __syncthreads();
+    return wp + x - v;
+}
+
+__global__ void k_scan_reduce(const uint32_t* __restrict__ in, uint32_t n, uint32_t per_block,
+                              uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t sh[32];
+    uint32_t b0 = blockIdx.x * per_block;
+    uint32_t b1 = min(n, b0 + per_block);
+    uint32_t acc = 0;
+    for (uint32_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += in[i];
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_scan_blocks(uint32_t* __restrict__ block_sums, uint32_t nb) {
+    __shared__ uint32_t sh[32];
+    uint32_t v = threadIdx.x < nb ? block_sums[threadIdx.x] : 0u;
+    uint32_t total;
+    uint32_t ex = block_excl_scan(v, sh, total);
+    if (threadIdx.x < nb) block_sums[threadIdx.x] = ex;
+    if (threadIdx.x == 0) block_sums[SCAN_MAX_BLOCKS] = total;
+}
+
+__global__ void k_scan_down(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
+                            uint32_t per_block, const uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t sh[32];
+    uint32_t b0 = blockIdx.x * per_block;
+    uint32_t b1 = min(n, b0 + per_block);
+    uint32_t carry = block_sums[blockIdx.x];
+    for (uint32_t t0 = b0; t0 < b1; t0 += blockDim.x) {
+        uint32_t i = t0 + threadIdx.x;
+        uint32_t v = i < b1 ? in[i] : 0u;
+        uint32_t total;
+        uint32_t ex = block_excl_scan(v, sh, total);
+        if (i < b1) out[i] = carry + ex;
+        carry += total;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = block_sums[SCAN_MAX_BLOCKS];
+}
+
+// ---------------------------------------------------------------------------
+// Path bounding box (XPathScanner::new, scanner/mod.rs:131-180): one warp per
+// path reduces its edges to the AA row range and AA column range, then maps
+// them to the pixel rectangle the row map can touch.
+// ---------------------------------------------------------------------------
+__global__ void k_path_bbox(const uint64_t* __restrict__ path_pt_off, const uint32_t* __restrict__ edge_off,
+                            const Edge* __restrict__ edges, uint32_t n_paths, const uint8_t* __restrict__ rule,
+                            const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha,
+                            const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
+                            const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
+                            uint32_t* __restrict__ path_rows, uint32_t* __restrict__ path_chunks,
+                            int chunk_rows, BatchCounters* __restrict__ ctr) {
+    int lane = threadIdx.x & 31;
+    uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = warp_g; p < n_paths; p += nwarps) {
+        uint32_t eb = edge_off[path_pt_off[p]], ee = edge_off[path_pt_off[p + 1]];
+        int32_t y0 = INT32_MAX, y1 = INT32_MIN, xl = INT32_MAX, xh = INT32_MIN;
+        unsigned long long raw = 0;
+        for (uint32_t j = eb + lane; j < ee; j += 32) {
+            Edge e = edges[j];
+            if (e.flags & EF_EMPTY) continue;
+            int32_t lo, hi;
+            edge_xrange(e, lo, hi);
+            raw += static_cast<unsigned long long>(e.row1 - e.row0 + 1);
+            y0 = min(y0, e.row0);
+            y1 = max(y1, e.row1);
+            xl = min(xl, lo);
+            xh = max(xh, hi);
+        }
+        for (int o = 16; o; o >>= 1) {
+            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+            xl = min(xl, __shfl_xor_sync(0xffffffffu, xl, o));
+            xh = max(xh, __shfl_xor_sync(0xffffffffu, xh, o));
+            raw += __shfl_xor_sync(0xffffffffu, raw, o);
+        }
+        if (lane == 0) {
+            if (raw) atomicAdd(&ctr->raw_entries, raw);
+            uint32_t pg = path_page[p];
+            int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
+            PathInfo pi;
+            pi.e_begin = eb;
+            pi.e_end = ee;
+            pi.paint = uint32_t(gray[p]) | (uint32_t(alpha[p]) << 8) | (uint32_t(rule[p] ? 1 : 0) << 16);
+            pi.page = pg;
+            pi.pad0 = pi.pad1 = 0;
+            uint32_t rows = 0;
+            if (y0 <= y1) {
+                pi.y0 = y0;
+                pi.y1 = y1;
+                rows = static_cast<uint32_t>(y1 - y0 + 1);
+                // Pixel columns: spans cover AA columns [max(x0,0), min(x1+1, 4W)).
+                int32_t cl = max(xl, 0), ch = min(xh, 4 * W - 1);
+                pi.px0 = cl >> 2;
+                pi.px1 = ch >> 2;
+                if (xh < 0 || xl >= 4 * W) {
+                    pi.px0 = 1;
+                    pi.px1 = 0;
+                }
+                // Pixel rows under the row map.
+                if (rowmap == 0) {
+                    pi.py0 = y0 >> 2;
+                    pi.py1 = y1 >> 2;
+                } else {
+                    pi.py0 = y0 >> 2;
+                    int32_t t = y1 - 12;
+                    pi.py1 = t >= 0 ? (t >> 4) : -1;
+                }
+                pi.py0 = max(pi.py0, 0);
+                pi.py1 = min(pi.py1, H - 1);
+            } else {
+                pi.y0 = 1;
+                pi.y1 = 0;
+                pi.px0 = 1;
+                pi.px1 = 0;
+                pi.py0 = 1;
+                pi.py1 = 0;
+            }
+            info[p] = pi;
+            path_rows[p] = rows;
+            path_chunks[p] = (rows + chunk_rows - 1) / chunk_rows;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Supertile binning: for each supertile of a page, the ordered list of paths
+// of that page whose pixel rectangle overlaps it. One warp per supertile
+// ballots over 32 paths at a time, so list order is path order.
+// ---------------------------------------------------------------------------
+struct PageGeom {
+    uint32_t w, h;
+    uint32_t path_begin, path_end;
+    uint32_t tile_base, ntx;       // tiles of this page start at tile_base, ntx per row
+    uint32_t super_base, nsx;      // supertiles start at super_base, nsx per row
+    uint64_t offset;               // page byte offset in the arena
+};
+
+__device__ __forceinline__ uint32_t find_page_by(const PageGeom* pg, uint32_t n_pages, uint32_t idx, bool super) {
+    uint32_t lo = 0, hi = n_pages;  // last page with base <= idx
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t b = super ? pg[mid].super_base : pg[mid].tile_base;
+        if (b <= idx) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <bool WRITE>
+__global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages,
+                            uint32_t n_super, int stw, int sth, uint32_t* __restrict__ super_count,
+                            const uint32_t* __restrict__ super_off, uint32_t* __restrict__ super_list) {
+    int lane = threadIdx.x & 31;
+    uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t s = warp_g; s < n_super; s += nwarps) {
+        uint32_t pg = find_page_by(pages, n_pages, s, true);
+        PageGeom G = pages[pg];
+        uint32_t local = s - G.super_base;
+        int32_t sx = static_cast<int32_t>(local % G.nsx), sy = static_cast<int32_t>(local / G.nsx);
+        int32_t x0 = sx * stw, x1 = x0 + stw - 1, y0 = sy * sth, y1 = y0 + sth - 1;
+        uint32_t cnt = 0;
+        uint32_t base = WRITE ? super_off[s] : 0u;
+        for (uint32_t j = G.path_begin; j < G.path_end; j += 32) {
+            uint32_t q = j + lane;
+            bool hit = false;
+            if (q < G.path_end) {
+                const PathInfo& P = info[q];
+                hit = P.px0 <= P.px1 && P.py0 <= P.py1 && P.px0 <= x1 && P.px1 >= x0 && P.py0 <= y1 && P.py1 >= y0;
+            }
+            uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (WRITE && hit) super_list[base + cnt + __popc(m & lanemask_lt())] = q;
+            cnt += __popc(m);
+        }
+        if (!WRITE && lane == 0) super_count[s] = cnt;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row stage: one warp per chunk of 32 consecutive AA rows of one path; lane =
+// row. The path's edges are visited in order, 32 at a time: a ballot selects
+// those overlapping the chunk and the set bits are walked in ascending order,
+// so each row sees its entries in segment order and the write_intersect merge
+// (merge only with the last entry written to the row) is reproduced exactly.
+// The merged list lives in shared memory (KCAP entries per row); rows that
+// overflow go to k_rows_slow.
+// ---------------------------------------------------------------------------
+constexpr int ROWS_WARPS = 4;
+
+__device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? v : v + 1; }
+
+// Winding walk of render_aa_line (scanner/mod.rs:393-467) for one AA row over
+// its sorted entries, emitting the union of the covered spans clamped to
+// [0, aa_width) in place over the entry arrays. Returns the span count.
+template <typename Get, typename Put>
+__device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, Get get, Put put, uint32_t& nonterm) {
+    int32_t count = 0, xx = 0;
+    int i = 0, ns = 0;
+    bool have = false;
+    int32_t cs = 0, ce = 0;
+    while (i < n || (count & mask) != 0) {
+        if ((count & mask) == 0) {
+            if (i >= n) break;
+            int32_t x0, x1, c;
+            get(i, x0, x1, c);
+            xx = x0;
+            count = static_cast<int32_t>(static_cast<uint32_t>(count) + static_cast<uint32_t>(c));
+            ++i;
+            continue;
+        }
+        int32_t span_x1;
+        bool ran_out = false;
+        for (;;) {
+            if (i >= n) {
+                span_x1 = aa_width;
+                ran_out = true;
+                break;
+            }
+            int32_t x0, x1, c;
+            get(i, x0, x1, c);
+            count = static_cast<int32_t>(static_cast<uint32_t>(count) + static_cast<uint32_t>(c));
+            int32_t end = static_cast<int32_t>(static_cast<uint32_t>(x1) + 1u);
+            ++i;
+            if ((count & mask) == 0) {
+                span_x1 = end;
+                break;
+            }
+        }
+        int32_t bx0 = max(xx, 0);
+        int32_t bx1 = max(min(span_x1, aa_width), 0);
+        if (bx0 < bx1) {
+            if (have && bx0 <= ce) {
+                ce = max(ce, bx1);
+            } else {
+                if (have) put(ns++, cs, ce);
+                cs = bx0;
+                ce = bx1;
+                have = true;
+            }
+        }
+        xx = span_x1;
+        if (ran_out) {
+            ++nonterm;
+            break;
+        }
+    }
+    if (have) put(ns++, cs, ce);
+    return ns;
+}
+
+template <int KCAP>
+__global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
+    const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ row_off,
+    const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w, uint32_t n_paths,
+    uint2* __restrict__ row_idx, uint32_t* __restrict__ spans, uint32_t span_cap, uint2* __restrict__ ovf,
+    uint32_t ovf_cap, BatchCounters* __restrict__ ctr, int chunk_rows) {
+    __shared__ int32_t sx0[ROWS_WARPS][KCAP][32];
+    __shared__ int32_t sx1[ROWS_WARPS][KCAP][32];
+    __shared__ int32_t scn[ROWS_WARPS][KCAP][32];
+    __shared__ Edge sedge[ROWS_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t total_chunks = chunk_off[n_paths];
+    uint32_t nonterm = 0;
+    for (uint32_t c = blockIdx.x * ROWS_WARPS + w; c < total_chunks; c += gridDim.x * ROWS_WARPS) {
+        // Path owning chunk c: last p with chunk_off[p] <= c.
+        uint32_t lo = 0, hi = n_paths;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (chunk_off[mid] <= c) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t p = lo;
+        const PathInfo P = info[p];
+        const int32_t chunk_lo = P.y0 + static_cast<int32_t>(c - chunk_off[p]) * chunk_rows;
+        const int32_t chunk_hi = min(chunk_lo + chunk_rows - 1, P.y1);
+        const int32_t r = chunk_lo + lane;
+        const bool valid = lane < chunk_rows && r <= chunk_hi;
+        const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
+        const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        int n = 0;
+        bool has_last = false;
+        int32_t lx0 = 0, lx1 = 0, lc = 0;
+        for (uint32_t eb = P.e_begin; eb < P.e_end; eb += 32) {
+            uint32_t j = eb + lane;
+            Edge e;
+            bool hit = false;
+            if (j < P.e_end) {
+                e = edges[j];
+                hit = !(e.flags & EF_EMPTY) && e.row0 <= chunk_hi && e.row1 >= chunk_lo;
+            }
+            uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (!m) continue;
+            if (hit) sedge[w][lane] = e;
+            __syncwarp();
+            while (m) {
+                int b = __ffs(m) - 1;
+                m &= m - 1;
+                const Edge E = sedge[w][b];
+                if (valid && E.row0 <= r && r <= E.row1) {
+                    int32_t elo, ehi, ec;
+                    edge_entry(E, r, elo, ehi, ec);
+                    if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
+                        lc = static_cast<int32_t>(static_cast<uint32_t>(lc) + static_cast<uint32_t>(ec));
+                        lx0 = min(lx0, elo);
+                        lx1 = max(lx1, ehi);
+                    } else {
+                        if (has_last) {
+                            if (n < KCAP) {
+                                sx0[w][n][lane] = lx0;
+                                sx1[w][n][lane] = lx1;
+                                scn[w][n][lane] = lc;
+                            }
+                            ++n;
+                        }
+                        lx0 = elo;
+                        lx1 = ehi;
+                        lc = ec;
+                        has_last = true;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        if (has_last) {
+            if (n < KCAP) {
+                sx0[w][n][lane] = lx0;
+                sx1[w][n][lane] = lx1;
+                scn[w][n][lane] = lc;
+            }
+            ++n;
+        }
+        const bool overflow = valid && n > KCAP;
+        int ns = 0;
+        if (valid && !overflow) {
+            // sort_unstable_by_key(x0) on <= KCAP (<= 20 in practice) entries:
+            // stable insertion sort, as Rust std sorts short slices.
+            for (int a = 1; a < n; ++a) {
+                int32_t t0 = sx0[w][a][lane], t1 = sx1[w][a][lane], tc = scn[w][a][lane];
+                int b = a;
+                while (b > 0 && t0 < sx0[w][b - 1][lane]) {
+                    sx0[w][b][lane] = sx0[w][b - 1][lane];
+                    sx1[w][b][lane] = sx1[w][b - 1][lane];
+                    scn[w][b][lane] = scn[w][b - 1][lane];
+                    --b;
+                }
+                sx0[w][b][lane] = t0;
+                sx1[w][b][lane] = t1;
+                scn[w][b][lane] = tc;
+            }
+            ns = walk_row(
+                n, mask, aa_width,
+                [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
+                    x0 = sx0[w][i][lane];
+                    x1 = sx1[w][i][lane];
+                    cc = scn[w][i][lane];
+                },
+                [&](int k, int32_t s, int32_t e) {
+                    sx0[w][k][lane] = s;
+                    sx1[w][k][lane] = e;
+                },
+                nonterm);
+        }
+        // Allocate span storage for the whole warp with one atomic.
+        uint32_t incl = ns;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t base = 0;
+        if (lane == 31 && total) base = atomicAdd(&ctr->span_cursor, total);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        const bool fits = static_cast<uint64_t>(base) + total <= span_cap;
+        if (lane == 0 && total && !fits) atomicOr(&ctr->err, ERR_SPAN_CAP);
+        if (valid) {
+            uint32_t ri = row_off[p] + static_cast<uint32_t>(r - P.y0);
+            if (overflow) {
+                uint32_t k = atomicAdd(&ctr->ovf_count, 1u);
+                if (k < ovf_cap) ovf[k] = make_uint2(p, static_cast<uint32_t>(r));
+                else atomicOr(&ctr->err, ERR_OVF_CAP);
+                row_idx[ri] = make_uint2(0u, 0u);
+            } else if (fits) {
+                uint32_t o0 = base + incl - ns;
+                for (int k = 0; k < ns; ++k)
+                    spans[o0 + k] = static_cast<uint32_t>(sx0[w][k][lane]) | (static_cast<uint32_t>(sx1[w][k][lane]) << 16);
+                row_idx[ri] = make_uint2(o0, static_cast<uint32_t>(ns));
+            } else {
+                row_idx[ri] = make_uint2(0u, 0u);
+            }
+        }
+        __syncwarp();
+    }
+    if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
+}
+
+// Rows whose merged list exceeded KCAP: one thread per row, the list in a
+// global scratch slice sized by the path's edge count.
+__global__ void k_rows_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ row_off,
+                            const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w,
+                            const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
+                            uint32_t scratch_cap, uint2* __restrict__ row_idx, uint32_t* __restrict__ spans,
+                            uint32_t span_cap, BatchCounters* __restrict__ ctr) {
+    uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);
+    uint32_t nonterm = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_ovf; k += gridDim.x * blockDim.x) {
+        uint32_t p = ovf[k].x;
+        int32_t r = static_cast<int32_t>(ovf[k].y);
+        const PathInfo P = info[p];
+        uint32_t ne = P.e_end - P.e_begin;
+        uint32_t sb = atomicAdd(&ctr->scratch_cursor, ne);
+        if (static_cast<uint64_t>(sb) + ne > scratch_cap) {
+            atomicOr(&ctr->err, ERR_SCRATCH_CAP);
+            continue;
+        }
+        int3* L = scratch + sb;
+        int n = 0;
+        for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
+            Edge E = edges[j];
+            if ((E.flags & EF_EMPTY) || r < E.row0 || r > E.row1) continue;
+            int32_t elo, ehi, ec;
+            edge_entry(E, r, elo, ehi, ec);
+            if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
+                L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
+                L[n - 1].x = min(L[n - 1].x, elo);
+                L[n - 1].y = max(L[n - 1].y, ehi);
+            } else {
+                L[n++] = make_int3(elo, ehi, ec);
+            }
+        }
+        // Stable sort by x0 (rows > 20 entries: see the tie note in the oracle).
+        for (int a = 1; a < n; ++a) {
+            int3 t = L[a];
+            int b = a;
+            while (b > 0 && t.x < L[b - 1].x) {
+                L[b] = L[b - 1];
+                --b;
+            }
+            L[b] = t;
+        }
+        const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
+        const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        int ns = walk_row(
+            n, mask, aa_width,
+            [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
+                x0 = L[i].x;
+                x1 = L[i].y;
+                cc = L[i].z;
+            },
+            [&](int q, int32_t s, int32_t e) {
+                L[q].x = s;
+                L[q].y = e;
+            },
+            nonterm);
+        uint32_t ri = row_off[p] + static_cast<uint32_t>(r - P.y0);
+        uint32_t o0 = ns ? atomicAdd(&ctr->span_cursor, static_cast<uint32_t>(ns)) : 0u;
+        if (static_cast<uint64_t>(o0) + ns > span_cap) {
+            atomicOr(&ctr->err, ERR_SPAN_CAP);
+            row_idx[ri] = make_uint2(0u, 0u);
+            continue;
+        }
+        for (int q = 0; q < ns; ++q)
+            spans[o0 + q] = static_cast<uint32_t>(L[q].x) | (static_cast<uint32_t>(L[q].y) << 16);
+        row_idx[ri] = make_uint2(o0, static_cast<uint32_t>(ns));
+    }
+    if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
+}
+
+// ---------------------------------------------------------------------------
+// Composite: one CTA per TW x TH page tile. The tile's bytes are loaded once
+// into registers, every path of the tile's supertile list whose rectangle
+// overlaps the tile is applied in path order (coverage from its four AA
+// sub-row span lists -> AA_GAMMA -> div255 source-over), and the tile is
+// stored once.
+// ---------------------------------------------------------------------------
+constexpr int COMP_THREADS = 256;
+constexpr int COMP_CHUNK = 256;
+
+__constant__ uint8_t c_gamma[17] = {0, 4, 11, 21, 32, 45, 59, 74, 90, 108, 126, 145, 166, 187, 209, 231, 255};
+
+struct HitInfo {
+    int32_t y0, y1, py0, py1;
+    uint32_t row_off, paint;
+};
+
+template <int TW, int TH>
+__device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap, int tile_x0, int tile_y0, int W,
+                                                    int H, const uint2* __restrict__ row_idx,
+                                                    const uint32_t* __restrict__ spans, const uint8_t* gamma,
+                                                    uint32_t (&pix)[TH * TW / COMP_THREADS]) {
+    constexpr int LPR = TW < 32 ? TW : 32;            // lanes per pixel row
+    constexpr int PX = TW / LPR;                      // pixels per lane
+    constexpr int RPW = 32 / LPR;                     // rows per warp step
+    constexpr int NW = COMP_THREADS / 32;
+    constexpr int ITERS = TH / (NW * RPW);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int col = (lane % LPR) * PX;
+    const int32_t g = static_cast<int32_t>(h.paint & 0xff);
+    const uint32_t alpha = (h.paint >> 8) & 0xff;
+    const int32_t c_tile0 = 4 * tile_x0, c_tile1 = 4 * (tile_x0 + TW);
+#pragma unroll
+    for (int it = 0; it < ITERS; ++it) {
+        const int ry = (w * RPW + lane / LPR) + it * NW * RPW;
+        const int y = tile_y0 + ry;
+        if (y < h.py0 || y > h.py1 || y >= H) continue;
+        const int32_t base = rowmap ? 16 * y + 12 : 4 * y;
+        int32_t cov[PX];
+#pragma unroll
+        for (int q = 0; q < PX; ++q) cov[q] = 0;
+#pragma unroll
+        for (int sub = 0; sub < 4; ++sub) {
+            const int32_t r = base + sub;
+            if (r < h.y0 || r > h.y1) continue;
+            const uint2 ix = row_idx[h.row_off + static_cast<uint32_t>(r - h.y0)];
+            for (uint32_t j = 0; j < ix.y; ++j) {
+                const uint32_t sp = spans[ix.x + j];
+                const int32_t s = static_cast<int32_t>(sp & 0xffffu), e = static_cast<int32_t>(sp >> 16);
+                if (e <= c_tile0) continue;
+                if (s >= c_tile1) break;
+#pragma unroll
+                for (int q = 0; q < PX; ++q) {
+                    const int32_t pc = 4 * (tile_x0 + col + q);
+                    cov[q] += max(0, min(e, pc + 4) - max(s, pc));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PX; ++q) {
+            if (cov[q] == 0) continue;
+            const uint32_t shape = gamma[min(cov[q], 16)];
+            const uint32_t a_src = div255(alpha * shape);
+            const int k = it * PX + q;
+            const uint32_t d = pix[k];
+            pix[k] = div255((255u - a_src) * d + a_src * static_cast<uint32_t>(g));
+        }
+    }
+}
+
+template <int TW, int TH>
+__global__ void __launch_bounds__(COMP_THREADS) k_composite(
+    const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
+    int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
+    const uint32_t* __restrict__ row_off, const uint2* __restrict__ row_idx, const uint32_t* __restrict__ spans,
+    uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr) {
+    constexpr int LPR = TW < 32 ? TW : 32;
+    constexpr int PX = TW / LPR;
+    constexpr int RPW = 32 / LPR;
+    constexpr int NW = COMP_THREADS / 32;
+    constexpr int ITERS = TH / (NW * RPW);
+    constexpr int NPIX = TH * TW / COMP_THREADS;
+    static_assert(ITERS * PX == NPIX, "tile shape must cover the CTA exactly");
+    __shared__ HitInfo hits[COMP_CHUNK];
+    __shared__ uint32_t wcnt[NW];
+    __shared__ uint8_t gamma[17];
+    if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
+    if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int col = (lane % LPR) * PX;
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const uint32_t pg = find_page_by(pages, n_pages, t, false);
+        const PageGeom G = pages[pg];
+        const uint32_t lt = t - G.tile_base;
+        const int tx = static_cast<int>(lt % G.ntx), ty = static_cast<int>(lt / G.ntx);
+        const int X0 = tx * TW, Y0 = ty * TH;
+        const int W = static_cast<int>(G.w), H = static_cast<int>(G.h);
+        uint8_t* page = arena + G.offset;
+        uint32_t pix[NPIX];
+#pragma unroll
+        for (int it = 0; it < ITERS; ++it) {
+            const int y = Y0 + (w * RPW + lane / LPR) + it * NW * RPW;
+#pragma unroll
+            for (int q = 0; q < PX; ++q) {
+                const int x = X0 + col + q;
+                pix[it * PX + q] = (y < H && x < W) ? page[static_cast<size_t>(y) * W + x] : 0u;
+            }
+        }
+        const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
+        const uint32_t s = G.super_base + sy * G.nsx + sx;
+        const uint32_t l0 = super_off[s], l1 = super_off[s + 1];
+        for (uint32_t c0 = l0; c0 < l1; c0 += COMP_CHUNK) {
+            const uint32_t q = c0 + threadIdx.x;
+            bool hit = false;
+            PathInfo P;
+            if (q < l1) {
+                P = info[super_list[q]];
+                hit = P.px0 <= X0 + TW - 1 && P.px1 >= X0 && P.py0 <= Y0 + TH - 1 && P.py1 >= Y0 && P.px0 <= P.px1;
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) wcnt[w] = __popc(m);
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const uint32_t v = wcnt[k];
+                before += k < w ? v : 0u;
+                total += v;
+            }
+            if (hit) {
+                const uint32_t pos = before + __popc(m & lanemask_lt());
+                HitInfo hi;
+                hi.y0 = P.y0;
+                hi.y1 = P.y1;
+                hi.py0 = P.py0;
+                hi.py1 = P.py1;
+                hi.row_off = row_off[super_list[q]];
+                hi.paint = P.paint;
+                hits[pos] = hi;
+            }
+            __syncthreads();
+            for (uint32_t k = 0; k < total; ++k) {
+                HitInfo h = hits[k];
+                composite_path_rows<TW, TH>(h, rowmap, X0, Y0, W, H, row_idx, spans, gamma, pix);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int it = 0; it < ITERS; ++it) {
+            const int y = Y0 + (w * RPW + lane / LPR) + it * NW * RPW;
+#pragma unroll
+            for (int q = 0; q < PX; ++q) {
+                const int x = X0 + col + q;
+                if (y < H && x < W) page[static_cast<size_t>(y) * W + x] = static_cast<uint8_t>(pix[it * PX + q]);
+            }
+        }
+    }
+}
+
+}  // namespace rrb

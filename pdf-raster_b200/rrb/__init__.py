@@ -1,0 +1,409 @@
+"""rrb — B200-native anti-aliased path fill behind the reference's GpuBackend surface.
+
+`B200Backend` mirrors the reference trait `GpuBackend`
+(crates/gpu/src/backend/mod.rs:216-503): alloc_device / alloc_device_zeroed /
+free_device / upload_async / download_async / begin_page / record_* /
+submit_page / wait_page / detect_vram_budget, with status codes mapped to
+`BackendError`-named exceptions. Every call goes through the C ABI of
+librrb.so (include/rrb.h); there is no CPU fallback: without the library, or
+without a CUDA device, calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import (RRB_FILL_EVEN_ODD, RRB_FILL_NONZERO, RRB_ROWMAP_AS_SHIPPED,  # noqa: F401
+                   RRB_ROWMAP_DOCUMENTED, BatchStats, PathBatchParams, PathFillParams, SceneParams, StageTime,
+                   Tuning, VramBudget)
+
+__all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "lib",
+           "conic_to_cubic", "RRB_FILL_NONZERO", "RRB_FILL_EVEN_ODD", "RRB_ROWMAP_DOCUMENTED",
+           "RRB_ROWMAP_AS_SHIPPED"]
+
+IDENTITY = (1.0, 0.0, 0.0, 1.0, 0.0, 0.0)
+
+
+def lib() -> C.CDLL:
+    return _abi.load()
+
+
+class BackendError(RuntimeError):
+    """A non-zero rrb status; `.kind` is the BackendError variant name."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.kind = lib().rrb_status_name(status).decode()
+        super().__init__(f"{self.kind}: {message}")
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+@dataclass
+class DeviceBuffer:
+    handle: int
+    size: int
+
+    @property
+    def ptr(self) -> int:
+        return lib().rrb_device_ptr(self.handle) or 0
+
+
+@dataclass
+class PinnedBuffer:
+    handle: int
+    size: int
+
+    def array(self) -> np.ndarray:
+        p = lib().rrb_host_ptr(self.handle)
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), shape=(self.size,))
+
+
+class PathBuilder:
+    """PathBuilder::{move_to,line_to,curve_to,close} (crates/raster/src/path/mod.rs:310-448)."""
+
+    ERRORS = {1: "NoCurPt", 2: "BogusPath"}
+
+    def __init__(self):
+        self._h = lib().rrb_path_new()
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().rrb_path_free(h)
+
+    def _chk(self, rc: int):
+        if rc:
+            raise ValueError(self.ERRORS.get(rc, str(rc)))
+
+    def move_to(self, x, y):
+        self._chk(lib().rrb_path_move_to(self._h, x, y))
+
+    def line_to(self, x, y):
+        self._chk(lib().rrb_path_line_to(self._h, x, y))
+
+    def curve_to(self, x1, y1, x2, y2, x3, y3):
+        self._chk(lib().rrb_path_curve_to(self._h, x1, y1, x2, y2, x3, y3))
+
+    def conic_to(self, xc, yc, x3, y3):
+        self._chk(lib().rrb_path_conic_to(self._h, xc, yc, x3, y3))
+
+    def close(self, force: bool = False):
+        self._chk(lib().rrb_path_close(self._h, int(force)))
+
+    def build(self):
+        """Return copies of (pts[n,2] f64, flags[n] u8)."""
+        n = lib().rrb_path_len(self._h)
+        if n == 0:
+            return np.zeros((0, 2)), np.zeros(0, np.uint8)
+        pts = np.ctypeslib.as_array(lib().rrb_path_pts(self._h), shape=(n * 2,)).reshape(n, 2).copy()
+        fl = np.ctypeslib.as_array(lib().rrb_path_flags(self._h), shape=(n,)).copy()
+        return pts, fl
+
+
+def conic_to_cubic(p0, pc, p3):
+    out = (C.c_double * 4)()
+    lib().rrb_conic_to_cubic(p0[0], p0[1], pc[0], pc[1], p3[0], p3[1], out)
+    return (out[0], out[1]), (out[2], out[3])
+
+
+class Scene:
+    """A seeded synthetic workload (kind 0 polygons, 1 glyphs, 2 mixed pages).
+
+    Arrays are numpy views of the generator's memory (valid while the Scene lives).
+    """
+
+    def __init__(self, kind: int, seed: int = 0, **kw):
+        p = SceneParams(kind=kind, seed=seed)
+        for k, v in kw.items():
+            setattr(p, k, v)
+        h = C.c_void_p()
+        rc = lib().rrb_scene_generate(C.byref(p), C.byref(h))
+        if rc:
+            raise BackendError(rc, "scene generation failed")
+        self._h = h.value
+        self.view = PathBatchParams()
+        lib().rrb_scene_view(self._h, C.byref(self.view))
+        v = self.view
+        self.n_paths = int(v.n_paths)
+        self.n_pts = int(v.n_pts)
+        self.n_pages = int(v.n_pages)
+        asa = np.ctypeslib.as_array
+        self.pts = asa(v.pts, shape=(self.n_pts * 2,)).reshape(self.n_pts, 2) if self.n_pts else np.zeros((0, 2))
+        self.flags = asa(v.flags, shape=(self.n_pts,)) if self.n_pts else np.zeros(0, np.uint8)
+        self.path_pt_off = asa(v.path_pt_off, shape=(self.n_paths + 1,))
+        self.fill_rule = asa(v.fill_rule, shape=(self.n_paths,))
+        self.gray = asa(v.gray, shape=(self.n_paths,))
+        self.alpha = asa(v.alpha, shape=(self.n_paths,))
+        self.path_page = asa(v.path_page, shape=(self.n_paths,))
+        self.page_width = asa(v.page_width, shape=(self.n_pages,))
+        self.page_height = asa(v.page_height, shape=(self.n_pages,))
+        self.page_offset = asa(v.page_offset, shape=(self.n_pages,))
+        self.arena_bytes = int(lib().rrb_scene_arena_bytes(self._h))
+        cnt = (C.c_uint64 * 3)()
+        lib().rrb_scene_counts(self._h, cnt)
+        self.n_lines, self.n_cubics = int(cnt[0]), int(cnt[1])
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().rrb_scene_free(h)
+
+    @property
+    def pixels(self) -> int:
+        return int(np.sum(self.page_width.astype(np.int64) * self.page_height.astype(np.int64)))
+
+    def blank_arena(self, value: int = 255) -> np.ndarray:
+        """Host page arena initialised to `value` (white pages)."""
+        return np.full(self.arena_bytes, value, dtype=np.uint8)
+
+    def page(self, arena: np.ndarray, i: int) -> np.ndarray:
+        o, w, h = int(self.page_offset[i]), int(self.page_width[i]), int(self.page_height[i])
+        return arena[o:o + w * h].reshape(h, w)
+
+
+def batch_params(pts, flags, path_pt_off, fill_rule, gray, alpha, path_page, page_width, page_height,
+                 page_offset, pages: DeviceBuffer | None, matrix=IDENTITY, flatness=0.1,
+                 rowmap=RRB_ROWMAP_DOCUMENTED, keep=None) -> PathBatchParams:
+    """Build a PathBatchParams over numpy arrays (kept alive through `keep`)."""
+    arrs = dict(
+        pts=np.ascontiguousarray(pts, np.float64).reshape(-1),
+        flags=np.ascontiguousarray(flags, np.uint8),
+        path_pt_off=np.ascontiguousarray(path_pt_off, np.uint64),
+        fill_rule=np.ascontiguousarray(fill_rule, np.uint8),
+        gray=np.ascontiguousarray(gray, np.uint8),
+        alpha=np.ascontiguousarray(alpha, np.uint8),
+        path_page=np.ascontiguousarray(path_page, np.uint32),
+        page_width=np.ascontiguousarray(page_width, np.uint32),
+        page_height=np.ascontiguousarray(page_height, np.uint32),
+        page_offset=np.ascontiguousarray(page_offset, np.uint64),
+    )
+    if keep is not None:
+        keep.extend(arrs.values())
+    p = PathBatchParams()
+    p.pts = _ptr(arrs["pts"], C.c_double)
+    p.flags = _ptr(arrs["flags"], C.c_uint8)
+    p.n_pts = arrs["flags"].size
+    p.path_pt_off = _ptr(arrs["path_pt_off"], C.c_uint64)
+    p.fill_rule = _ptr(arrs["fill_rule"], C.c_uint8)
+    p.gray = _ptr(arrs["gray"], C.c_uint8)
+    p.alpha = _ptr(arrs["alpha"], C.c_uint8)
+    p.path_page = _ptr(arrs["path_page"], C.c_uint32)
+    p.n_paths = arrs["fill_rule"].size
+    p.page_width = _ptr(arrs["page_width"], C.c_uint32)
+    p.page_height = _ptr(arrs["page_height"], C.c_uint32)
+    p.page_offset = _ptr(arrs["page_offset"], C.c_uint64)
+    p.n_pages = arrs["page_width"].size
+    p.pages = pages.handle if pages is not None else None
+    for i in range(6):
+        p.matrix[i] = matrix[i]
+    p.flatness = flatness
+    p.rowmap = rowmap
+    return p
+
+
+class B200Backend:
+    """The B200 backend: one device, one stream (GpuBackend, mod.rs:216-503)."""
+
+    def __init__(self, device: int = 0, mem_budget: int = 0):
+        h = C.c_void_p()
+        rc = lib().rrb_init(device, mem_budget, C.byref(h))
+        if rc:
+            raise BackendError(rc, f"rrb_init(device={device}) failed")
+        self._h = h.value
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().rrb_destroy(h)
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def _chk(self, rc: int):
+        if rc:
+            raise BackendError(rc, lib().rrb_last_error_message(self._h).decode())
+
+    # ---- memory
+    def alloc_device(self, size: int) -> DeviceBuffer:
+        h = C.c_void_p()
+        self._chk(lib().rrb_alloc_device(self._h, size, C.byref(h)))
+        return DeviceBuffer(h.value, size)
+
+    def alloc_device_zeroed(self, size: int) -> DeviceBuffer:
+        h = C.c_void_p()
+        self._chk(lib().rrb_alloc_device_zeroed(self._h, size, C.byref(h)))
+        return DeviceBuffer(h.value, size)
+
+    def device_buffer_len(self, buf: DeviceBuffer) -> int:
+        return int(lib().rrb_device_buffer_len(buf.handle))
+
+    def free_device(self, buf: DeviceBuffer):
+        self._chk(lib().rrb_free_device(self._h, buf.handle))
+
+    def alloc_host_pinned(self, size: int) -> PinnedBuffer:
+        h = C.c_void_p()
+        self._chk(lib().rrb_alloc_host_pinned(self._h, size, C.byref(h)))
+        return PinnedBuffer(h.value, size)
+
+    def free_host_pinned(self, buf: PinnedBuffer):
+        self._chk(lib().rrb_free_host_pinned(self._h, buf.handle))
+
+    # ---- transfers
+    def upload_async(self, dst: DeviceBuffer, src: np.ndarray, offset: int = 0) -> int:
+        src = np.ascontiguousarray(src)
+        f = C.c_uint64()
+        self._chk(lib().rrb_upload_async(self._h, dst.handle, offset, src.ctypes.data, src.nbytes, C.byref(f)))
+        return f.value
+
+    def download_async(self, src: DeviceBuffer, dst: np.ndarray, offset: int = 0) -> int:
+        assert dst.flags["C_CONTIGUOUS"]
+        f = C.c_uint64()
+        self._chk(lib().rrb_download_async(self._h, src.handle, offset, dst.ctypes.data, dst.nbytes, C.byref(f)))
+        return f.value
+
+    def wait_download(self, fence: int):
+        self._chk(lib().rrb_wait_download(self._h, fence))
+
+    def submit_transfer(self) -> int:
+        f = C.c_uint64()
+        self._chk(lib().rrb_submit_transfer(self._h, C.byref(f)))
+        return f.value
+
+    def wait_transfer(self, fence: int, timeout_ns: int = 0):
+        self._chk(lib().rrb_wait_transfer(self._h, fence, timeout_ns))
+
+    def detect_vram_budget(self) -> VramBudget:
+        b = VramBudget()
+        self._chk(lib().rrb_detect_vram_budget(self._h, C.byref(b)))
+        return b
+
+    # ---- page state machine
+    def begin_page(self):
+        self._chk(lib().rrb_begin_page(self._h))
+
+    def record_zero_buffer(self, buf: DeviceBuffer):
+        self._chk(lib().rrb_record_zero_buffer(self._h, buf.handle))
+
+    def submit_page(self) -> int:
+        f = C.c_uint64()
+        self._chk(lib().rrb_submit_page(self._h, C.byref(f)))
+        return f.value
+
+    def wait_page(self, fence: int, timeout_ns: int = 0):
+        self._chk(lib().rrb_wait_page(self._h, fence, timeout_ns))
+
+    def record_path_fill(self, pts, flags, page: DeviceBuffer, width: int, height: int, *, fill_rule=0,
+                         gray=0, alpha=255, rowmap=RRB_ROWMAP_DOCUMENTED, matrix=IDENTITY, flatness=0.1,
+                         page_offset=0):
+        pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+        flags = np.ascontiguousarray(flags, np.uint8)
+        p = PathFillParams()
+        p.pts = _ptr(pts, C.c_double)
+        p.flags = _ptr(flags, C.c_uint8)
+        p.n_pts = flags.size
+        for i in range(6):
+            p.matrix[i] = matrix[i]
+        p.flatness = flatness
+        p.fill_rule, p.gray, p.alpha, p.rowmap = fill_rule, gray, alpha, rowmap
+        p.page = page.handle
+        p.page_offset = page_offset
+        p.width, p.height = width, height
+        self._chk(lib().rrb_record_path_fill(self._h, C.byref(p)))
+
+    def record_path_batch(self, params: PathBatchParams):
+        self._chk(lib().rrb_record_path_batch(self._h, C.byref(params)))
+
+    def render_pages_host(self, params: PathBatchParams, host_pages: np.ndarray):
+        assert host_pages.dtype == np.uint8 and host_pages.flags["C_CONTIGUOUS"]
+        self._chk(lib().rrb_render_pages_host(self._h, C.byref(params), host_pages.ctypes.data, host_pages.nbytes))
+
+    def record_fill_buffer(self, buf: DeviceBuffer, value: int, offset: int = 0, length: int | None = None):
+        n = buf.size - offset if length is None else length
+        self._chk(lib().rrb_record_fill_buffer(self._h, buf.handle, offset, n, value))
+
+    # ---- device-resident batches
+    def batch_upload(self, params: PathBatchParams) -> "ResidentBatch":
+        h = C.c_void_p()
+        self._chk(lib().rrb_batch_upload(self._h, C.byref(params), C.byref(h)))
+        return ResidentBatch(self, h.value)
+
+    def record_batch(self, batch: "ResidentBatch", pages: DeviceBuffer, rowmap: int = RRB_ROWMAP_DOCUMENTED):
+        self._chk(lib().rrb_record_batch(self._h, batch.handle, pages.handle, rowmap))
+
+    # ---- profiling
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this backend (every call is ordered on it)."""
+        return int(lib().rrb_stream(self._h) or 0)
+
+    def set_profiling(self, enable: bool = True):
+        self._chk(lib().rrb_set_profiling(self._h, int(enable)))
+
+    def stage_times(self) -> dict:
+        buf = (StageTime * 32)()
+        n = C.c_int()
+        self._chk(lib().rrb_last_stage_times(self._h, buf, 32, C.byref(n)))
+        return {buf[i].name.decode(): (float(buf[i].ms), int(buf[i].launches)) for i in range(min(n.value, 32))}
+
+    # ---- tuning / stats
+    def set_tuning(self, tile_w: int = 0, tile_h: int = 0):
+        t = Tuning(tile_w=tile_w, tile_h=tile_h)
+        self._chk(lib().rrb_set_tuning(self._h, C.byref(t)))
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        self._chk(lib().rrb_get_tuning(self._h, C.byref(t)))
+        return t
+
+    def last_batch_stats(self) -> dict:
+        s = BatchStats()
+        self._chk(lib().rrb_last_batch_stats(self._h, C.byref(s)))
+        return {n: int(getattr(s, n)) for n, _ in BatchStats._fields_}
+
+    # ---- convenience: render a Scene into a host arena, end to end
+    def render_scene(self, scene: Scene, host_arena: np.ndarray, pages: DeviceBuffer | None = None,
+                     rowmap=RRB_ROWMAP_DOCUMENTED):
+        """Upload `host_arena`, render every path of `scene` into it on the device, download it."""
+        own = pages is None
+        if own:
+            pages = self.alloc_device(max(1, scene.arena_bytes))
+        scene.view.pages = pages.handle
+        scene.view.rowmap = rowmap
+        try:
+            self.render_pages_host(scene.view, host_arena)
+        finally:
+            scene.view.pages = None
+            if own:
+                self.free_device(pages)
+
+
+class ResidentBatch:
+    """A path batch whose inputs stay in device memory (rrb_batch_upload)."""
+
+    def __init__(self, backend: B200Backend, handle: int):
+        self.backend, self.handle = backend, handle
+
+    def record(self, pages: DeviceBuffer, rowmap: int = RRB_ROWMAP_DOCUMENTED):
+        self.backend.record_batch(self, pages, rowmap)
+
+    def free(self):
+        h, self.handle = self.handle, None
+        if h and self.backend.handle:
+            self.backend._chk(lib().rrb_batch_free(self.backend.handle, h))

@@ -1,0 +1,184 @@
+"""ctypes declarations of the C ABI in include/rrb.h.
+
+Struct layouts here must match the header field for field; tests check the
+sizes against offsets computed by the C compiler through rrb_abi_sizes-free
+means (ctypes alignment rules equal the C ABI rules on x86-64).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "librrb.so"
+
+# status codes (include/rrb.h)
+RRB_OK = 0
+RRB_ERR_ZERO_SIZE_ALLOC = 1
+RRB_ERR_UNALIGNED_FILL = 2
+RRB_ERR_POOL_EXHAUSTED = 3
+RRB_ERR_INVARIANT = 4
+RRB_ERR_OTHER = 5
+RRB_ERR_TIMEOUT = 6
+RRB_ERR_DEVICE = 7
+RRB_ERR_OUT_OF_MEMORY = 8
+RRB_ERR_STATE = 9
+
+RRB_FILL_NONZERO = 0
+RRB_FILL_EVEN_ODD = 1
+RRB_ROWMAP_DOCUMENTED = 0
+RRB_ROWMAP_AS_SHIPPED = 1
+
+
+class VramBudget(C.Structure):
+    _fields_ = [("total_bytes", C.c_uint64), ("free_bytes", C.c_uint64),
+                ("budget_bytes", C.c_uint64), ("used_bytes", C.c_uint64)]
+
+
+class PathFillParams(C.Structure):
+    _fields_ = [
+        ("pts", C.POINTER(C.c_double)),
+        ("flags", C.POINTER(C.c_uint8)),
+        ("n_pts", C.c_uint32),
+        ("matrix", C.c_double * 6),
+        ("flatness", C.c_double),
+        ("fill_rule", C.c_uint8),
+        ("gray", C.c_uint8),
+        ("alpha", C.c_uint8),
+        ("rowmap", C.c_uint8),
+        ("page", C.c_void_p),
+        ("page_offset", C.c_uint64),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+    ]
+
+
+class PathBatchParams(C.Structure):
+    _fields_ = [
+        ("pts", C.POINTER(C.c_double)),
+        ("flags", C.POINTER(C.c_uint8)),
+        ("n_pts", C.c_uint64),
+        ("path_pt_off", C.POINTER(C.c_uint64)),
+        ("fill_rule", C.POINTER(C.c_uint8)),
+        ("gray", C.POINTER(C.c_uint8)),
+        ("alpha", C.POINTER(C.c_uint8)),
+        ("path_page", C.POINTER(C.c_uint32)),
+        ("n_paths", C.c_uint64),
+        ("page_width", C.POINTER(C.c_uint32)),
+        ("page_height", C.POINTER(C.c_uint32)),
+        ("page_offset", C.POINTER(C.c_uint64)),
+        ("n_pages", C.c_uint32),
+        ("pages", C.c_void_p),
+        ("matrix", C.c_double * 6),
+        ("flatness", C.c_double),
+        ("rowmap", C.c_uint8),
+    ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("rows_per_chunk", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles", "tile_pairs",
+        "nonterminating_rows", "kernel_launches")]
+
+
+class StageTime(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("ms", C.c_float), ("launches", C.c_uint32)]
+
+
+class SceneParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("seed", C.c_uint64),
+        ("n_pages", C.c_uint32),
+        ("n_paths", C.c_uint32),
+        ("page_w", C.c_uint32),
+        ("page_h", C.c_uint32),
+        ("page_scale", C.c_double),
+        ("paths_scale", C.c_double),
+        ("path_cap", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+# Every exported symbol of include/rrb.h with its signature: (restype, argtypes).
+VP = C.c_void_p
+SIGNATURES = {
+    "rrb_init": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(VP)]),
+    "rrb_destroy": (C.c_int, [VP]),
+    "rrb_last_error_message": (C.c_char_p, [VP]),
+    "rrb_status_name": (C.c_char_p, [C.c_int]),
+    "rrb_version": (C.c_char_p, []),
+    "rrb_alloc_device": (C.c_int, [VP, C.c_size_t, C.POINTER(VP)]),
+    "rrb_alloc_device_zeroed": (C.c_int, [VP, C.c_size_t, C.POINTER(VP)]),
+    "rrb_device_buffer_len": (C.c_size_t, [VP]),
+    "rrb_device_ptr": (VP, [VP]),
+    "rrb_free_device": (C.c_int, [VP, VP]),
+    "rrb_alloc_host_pinned": (C.c_int, [VP, C.c_size_t, C.POINTER(VP)]),
+    "rrb_host_ptr": (VP, [VP]),
+    "rrb_free_host_pinned": (C.c_int, [VP, VP]),
+    "rrb_upload_async": (C.c_int, [VP, VP, C.c_size_t, VP, C.c_size_t, C.POINTER(C.c_uint64)]),
+    "rrb_download_async": (C.c_int, [VP, VP, C.c_size_t, VP, C.c_size_t, C.POINTER(C.c_uint64)]),
+    "rrb_wait_download": (C.c_int, [VP, C.c_uint64]),
+    "rrb_submit_transfer": (C.c_int, [VP, C.POINTER(C.c_uint64)]),
+    "rrb_wait_transfer": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
+    "rrb_detect_vram_budget": (C.c_int, [VP, C.POINTER(VramBudget)]),
+    "rrb_begin_page": (C.c_int, [VP]),
+    "rrb_record_zero_buffer": (C.c_int, [VP, VP]),
+    "rrb_submit_page": (C.c_int, [VP, C.POINTER(C.c_uint64)]),
+    "rrb_wait_page": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
+    "rrb_record_path_fill": (C.c_int, [VP, C.POINTER(PathFillParams)]),
+    "rrb_record_path_batch": (C.c_int, [VP, C.POINTER(PathBatchParams)]),
+    "rrb_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
+    "rrb_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
+    "rrb_last_batch_stats": (C.c_int, [VP, C.POINTER(BatchStats)]),
+    "rrb_batch_upload": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(VP)]),
+    "rrb_record_batch": (C.c_int, [VP, VP, VP, C.c_int]),
+    "rrb_batch_free": (C.c_int, [VP, VP]),
+    "rrb_record_fill_buffer": (C.c_int, [VP, VP, C.c_size_t, C.c_size_t, C.c_uint8]),
+    "rrb_set_profiling": (C.c_int, [VP, C.c_int]),
+    "rrb_stream": (VP, [VP]),
+    "rrb_last_stage_times": (C.c_int, [VP, C.POINTER(StageTime), C.c_int, C.POINTER(C.c_int)]),
+    "rrb_validate_path_batch": (C.c_int, [C.POINTER(PathBatchParams), C.c_size_t, C.c_char_p, C.c_size_t]),
+    "rrb_render_pages_host": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t]),
+    "rrb_path_new": (VP, []),
+    "rrb_path_free": (None, [VP]),
+    "rrb_path_clear": (None, [VP]),
+    "rrb_path_move_to": (C.c_int, [VP, C.c_double, C.c_double]),
+    "rrb_path_line_to": (C.c_int, [VP, C.c_double, C.c_double]),
+    "rrb_path_curve_to": (C.c_int, [VP] + [C.c_double] * 6),
+    "rrb_path_conic_to": (C.c_int, [VP] + [C.c_double] * 4),
+    "rrb_path_close": (C.c_int, [VP, C.c_int]),
+    "rrb_path_len": (C.c_uint64, [VP]),
+    "rrb_path_pts": (C.POINTER(C.c_double), [VP]),
+    "rrb_path_flags": (C.POINTER(C.c_uint8), [VP]),
+    "rrb_conic_to_cubic": (None, [C.c_double] * 6 + [C.POINTER(C.c_double)]),
+    "rrb_scene_generate": (C.c_int, [C.POINTER(SceneParams), C.POINTER(VP)]),
+    "rrb_scene_free": (None, [VP]),
+    "rrb_scene_view": (None, [VP, C.POINTER(PathBatchParams)]),
+    "rrb_scene_arena_bytes": (C.c_uint64, [VP]),
+    "rrb_scene_counts": (None, [VP, C.POINTER(C.c_uint64)]),
+}
+
+_LIB = None
+
+
+def load() -> C.CDLL:
+    """Load librrb.so (raising if it was not built) and declare every signature."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python pdf-raster_b200/rrb/build.py` "
+                "(the AA fill has no CPU fallback)")
+        lib = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
