@@ -178,6 +178,9 @@ def run_rrb(args, rank, local, world):
     import torch
 
     kw, desc = WORKLOADS[args.workload]
+    if args.paths:
+        kw = dict(kw, n_paths=args.paths)
+        desc += f" [reduced to {args.paths} paths]"
     scene = rrb.Scene(**kw)
     backend = rrb.B200Backend(local)
     tuning = backend.get_tuning()
@@ -351,6 +354,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-threads", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
     args = ap.parse_args()
     rank, local, world = dist_env()
     if args.impl == "reference":

@@ -62,7 +62,7 @@ struct rrb_ctx {
     // Batch scratch.
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
-    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats;
+    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups;
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
@@ -239,13 +239,19 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
         if (h->fill_rule[p] > 1) return msg = "fill_rule must be 0 or 1", RRB_ERR_INVARIANT;
         prev = pg;
     }
-    uint64_t p = 0;
+    uint64_t p = 0, work = 0;
     for (uint32_t pg = 0; pg < n_pages; ++pg) {
-        geom[pg].path_begin = static_cast<uint32_t>(p);
+        PageGeom& G = geom[pg];
+        G.path_begin = static_cast<uint32_t>(p);
         while (p < n_paths && h->path_page[p] == pg) ++p;
-        geom[pg].path_end = static_cast<uint32_t>(p);
+        G.path_end = static_cast<uint32_t>(p);
+        G.nblk = std::max<uint32_t>(1, (G.path_end - G.path_begin + BIN_BLOCK - 1) / BIN_BLOCK);
+        G.work_base = static_cast<uint32_t>(work);
+        work += static_cast<uint64_t>(G.nsx) * ((G.h + SUPER - 1) / SUPER) * G.nblk;
     }
-    if (tiles >= (1ull << 31) || supers >= (1ull << 31)) return msg = "too many tiles", RRB_ERR_INVARIANT;
+    if (tiles >= (1ull << 31) || supers >= (1ull << 31) || work >= (1ull << 31))
+        return msg = "too many tiles", RRB_ERR_INVARIANT;
+    supers = work;  // binning work items
     return RRB_OK;
 }
 
@@ -399,6 +405,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_rows, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_chunks, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_groups, ((n_edges + 31) / 32 + 1) * sizeof(int2)))) return rc;
     stage(c, 3);
     k_seg_write<<<grid_for(c, n_pts, 128), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NS, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
@@ -412,7 +419,9 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
         chunk_rows, as<BatchCounters>(c->s_ctr));
-    c->launches += 1;
+    k_edge_groups<<<grid_for(c, (n_edges + 31) / 32, 128), 128, 0, c->stream>>>(
+        as<Edge>(c->s_edges), static_cast<uint32_t>(n_edges), as<int2>(c->s_groups));
+    c->launches += 2;
     stage_end(c, 4);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 5);
@@ -461,7 +470,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         int g = grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16);
         k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
-            as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+            as<int2>(c->s_groups), as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
             static_cast<uint32_t>(span_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_rows)),
             as<BatchCounters>(c->s_ctr), chunk_rows);
         c->launches += 1;
@@ -605,7 +614,8 @@ int rrb_destroy(rrb_ctx* c) {
     Scratch* all[] = {&c->s_pts, &c->s_flags, &c->s_off, &c->s_rule, &c->s_gray, &c->s_alpha, &c->s_page,
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
-                      &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats};
+                      &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
+                      &c->s_groups};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);

@@ -17,6 +17,7 @@
 //                   one CTA per page tile, paths in index order
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #include "rrb_device.cuh"
@@ -26,10 +27,11 @@ namespace rrb {
 // Piece slots: one per input point. kind in bits 30-31 of .y.
 constexpr uint32_t PK_NONE = 0, PK_LINE = 1, PK_CURVE = 2, PK_CLOSE = 3;
 
-struct PathInfo {
-    int32_t y0, y1;          // AA rows [y0, y1] (y0 > y1: no rows)
+// 48 bytes, 16-byte aligned; the pixel rectangle leads so it loads as one int4.
+struct __align__(16) PathInfo {
     int32_t px0, px1;        // pixel columns touched (px0 > px1: none)
     int32_t py0, py1;        // pixel rows touched under the row map
+    int32_t y0, y1;          // AA rows [y0, y1] (y0 > y1: no rows)
     uint32_t e_begin, e_end; // edge range
     uint32_t paint;          // gray | alpha << 8 | rule << 16
     uint32_t page;
@@ -345,8 +347,11 @@ struct PageGeom {
     uint32_t path_begin, path_end;
     uint32_t tile_base, ntx;       // tiles of this page start at tile_base, ntx per row
     uint32_t super_base, nsx;      // supertiles start at super_base, nsx per row
+    uint32_t work_base, nblk;      // binning work items: (supertile, block of BIN_BLOCK paths)
     uint64_t offset;               // page byte offset in the arena
 };
+
+constexpr uint32_t BIN_BLOCK = 2048;  // paths per binning work item
 
 __device__ __forceinline__ uint32_t find_page_by(const PageGeom* pg, uint32_t n_pages, uint32_t idx, bool super) {
     uint32_t lo = 0, hi = n_pages;  // last page with base <= idx
@@ -359,33 +364,51 @@ __device__ __forceinline__ uint32_t find_page_by(const PageGeom* pg, uint32_t n_
     return lo;
 }
 
+__device__ __forceinline__ uint32_t find_page_work(const PageGeom* pg, uint32_t n_pages, uint32_t q) {
+    uint32_t lo = 0, hi = n_pages;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (pg[mid].work_base <= q) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// One warp per work item (supertile s, block b of the page's paths): the
+// paths of block b that overlap s, in path order. Work items of one
+// supertile are consecutive, so after an exclusive scan of the counts the
+// supertile's list is the contiguous range [off(s,0), off(s,nblk)).
 template <bool WRITE>
 __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages,
-                            uint32_t n_super, int stw, int sth, uint32_t* __restrict__ super_count,
-                            const uint32_t* __restrict__ super_off, uint32_t* __restrict__ super_list) {
+                            uint32_t n_work, int stw, int sth, uint32_t* __restrict__ work_count,
+                            const uint32_t* __restrict__ work_off, uint32_t* __restrict__ super_list) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t s = warp_g; s < n_super; s += nwarps) {
-        uint32_t pg = find_page_by(pages, n_pages, s, true);
+    for (uint32_t q = warp_g; q < n_work; q += nwarps) {
+        uint32_t pg = find_page_work(pages, n_pages, q);
         PageGeom G = pages[pg];
-        uint32_t local = s - G.super_base;
-        int32_t sx = static_cast<int32_t>(local % G.nsx), sy = static_cast<int32_t>(local / G.nsx);
+        uint32_t local = q - G.work_base;
+        uint32_t sl = local / G.nblk, blk = local % G.nblk;
+        int32_t sx = static_cast<int32_t>(sl % G.nsx), sy = static_cast<int32_t>(sl / G.nsx);
         int32_t x0 = sx * stw, x1 = x0 + stw - 1, y0 = sy * sth, y1 = y0 + sth - 1;
+        uint32_t pb = G.path_begin + blk * BIN_BLOCK;
+        uint32_t pe = min(G.path_end, pb + BIN_BLOCK);
         uint32_t cnt = 0;
-        uint32_t base = WRITE ? super_off[s] : 0u;
-        for (uint32_t j = G.path_begin; j < G.path_end; j += 32) {
-            uint32_t q = j + lane;
+        uint32_t base = WRITE ? work_off[q] : 0u;
+        for (uint32_t j = pb; j < pe; j += 32) {
+            uint32_t qq = j + lane;
             bool hit = false;
-            if (q < G.path_end) {
-                const PathInfo& P = info[q];
-                hit = P.px0 <= P.px1 && P.py0 <= P.py1 && P.px0 <= x1 && P.px1 >= x0 && P.py0 <= y1 && P.py1 >= y0;
+            if (qq < pe) {
+                static_assert(sizeof(PathInfo) % 16 == 0 && offsetof(PathInfo, px0) == 0, "int4 load of the rectangle");
+                const int4 r = *reinterpret_cast<const int4*>(&info[qq]);  // px0, px1, py0, py1
+                hit = r.x <= r.y && r.z <= r.w && r.x <= x1 && r.y >= x0 && r.z <= y1 && r.w >= y0;
             }
             uint32_t m = __ballot_sync(0xffffffffu, hit);
-            if (WRITE && hit) super_list[base + cnt + __popc(m & lanemask_lt())] = q;
+            if (WRITE && hit) super_list[base + cnt + __popc(m & lanemask_lt())] = qq;
             cnt += __popc(m);
         }
-        if (!WRITE && lane == 0) super_count[s] = cnt;
+        if (!WRITE && lane == 0) work_count[q] = cnt;
     }
 }
 
@@ -461,16 +484,35 @@ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, G
     return ns;
 }
 
+// Row range [min row0, max row1] of each aligned group of 32 edges (empty
+// edges excluded), so a chunk can skip whole groups with one load.
+__global__ void k_edge_groups(const Edge* __restrict__ edges, uint32_t n_edges, int2* __restrict__ groups) {
+    const uint32_t n_groups = (n_edges + 31) / 32;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
+        int32_t lo = INT32_MAX, hi = INT32_MIN;
+        const uint32_t e1 = min(n_edges, g * 32 + 32);
+        for (uint32_t j = g * 32; j < e1; ++j) {
+            const Edge e = edges[j];
+            if (e.flags & EF_EMPTY) continue;
+            lo = min(lo, e.row0);
+            hi = max(hi, e.row1);
+        }
+        groups[g] = make_int2(lo, hi);
+    }
+}
+
 template <int KCAP>
 __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ row_off,
-    const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w, uint32_t n_paths,
-    uint2* __restrict__ row_idx, uint32_t* __restrict__ spans, uint32_t span_cap, uint2* __restrict__ ovf,
-    uint32_t ovf_cap, BatchCounters* __restrict__ ctr, int chunk_rows) {
+    const Edge* __restrict__ edges, const int2* __restrict__ groups, const uint32_t* __restrict__ page_w,
+    uint32_t n_paths, uint2* __restrict__ row_idx, uint32_t* __restrict__ spans, uint32_t span_cap,
+    uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr, int chunk_rows) {
     __shared__ int32_t sx0[ROWS_WARPS][KCAP][32];
     __shared__ int32_t sx1[ROWS_WARPS][KCAP][32];
     __shared__ int32_t scn[ROWS_WARPS][KCAP][32];
-    __shared__ Edge sedge[ROWS_WARPS][32];
+    // Edge records of the current batch, field-major so that lanes reading
+    // different edges hit different banks.
+    __shared__ int32_t sedge[ROWS_WARPS][8][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
@@ -493,23 +535,50 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
         int n = 0;
         bool has_last = false;
         int32_t lx0 = 0, lx1 = 0, lc = 0;
-        for (uint32_t eb = P.e_begin; eb < P.e_end; eb += 32) {
-            uint32_t j = eb + lane;
+        for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
+            const int2 grp = groups[eb >> 5];
+            if (grp.x > chunk_hi || grp.y < chunk_lo) continue;  // no edge of this group touches the chunk
+            const uint32_t j = eb + lane;
             Edge e;
             bool hit = false;
-            if (j < P.e_end) {
+            if (j >= P.e_begin && j < P.e_end) {
                 e = edges[j];
                 hit = !(e.flags & EF_EMPTY) && e.row0 <= chunk_hi && e.row1 >= chunk_lo;
             }
             uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (!m) continue;
-            if (hit) sedge[w][lane] = e;
+            if (hit) {
+                sedge[w][0][lane] = e.row0;
+                sedge[w][1][lane] = e.row1;
+                sedge[w][2][lane] = e.flags;
+                sedge[w][3][lane] = e.a;
+                sedge[w][4][lane] = e.b;
+                sedge[w][5][lane] = e.dfp;
+                sedge[w][6][lane] = e.cmin;
+                sedge[w][7][lane] = e.cmax;
+            }
             __syncwarp();
+            // Edges of this batch covering this lane's row, in edge order.
+            uint32_t mine = 0;
             while (m) {
-                int b = __ffs(m) - 1;
+                const int b = __ffs(m) - 1;
                 m &= m - 1;
-                const Edge E = sedge[w][b];
-                if (valid && E.row0 <= r && r <= E.row1) {
+                if (sedge[w][0][b] <= r && r <= sedge[w][1][b]) mine |= 1u << b;
+            }
+            if (!valid) mine = 0;
+            while (mine) {
+                const int b = __ffs(mine) - 1;
+                mine &= mine - 1;
+                Edge E;
+                E.row0 = sedge[w][0][b];
+                E.row1 = sedge[w][1][b];
+                E.flags = sedge[w][2][b];
+                E.a = sedge[w][3][b];
+                E.b = sedge[w][4][b];
+                E.dfp = sedge[w][5][b];
+                E.cmin = sedge[w][6][b];
+                E.cmax = sedge[w][7][b];
+                {
                     int32_t elo, ehi, ec;
                     edge_entry(E, r, elo, ehi, ec);
                     if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
@@ -787,8 +856,8 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
             }
         }
         const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
-        const uint32_t s = G.super_base + sy * G.nsx + sx;
-        const uint32_t l0 = super_off[s], l1 = super_off[s + 1];
+        const uint32_t q0 = G.work_base + (sy * G.nsx + sx) * G.nblk;
+        const uint32_t l0 = super_off[q0], l1 = super_off[q0 + G.nblk];
         for (uint32_t c0 = l0; c0 < l1; c0 += COMP_CHUNK) {
             const uint32_t q = c0 + threadIdx.x;
             bool hit = false;
