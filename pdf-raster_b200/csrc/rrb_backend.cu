@@ -41,7 +41,7 @@ struct Scratch {
     size_t cap = 0;
 };
 
-constexpr int KCAP = 24;        // merged Intersect entries per AA row kept in shared memory
+constexpr int KCAP = 16;        // merged Intersect entries per AA row kept in shared memory
 constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
 
 }  // namespace
@@ -62,7 +62,7 @@ struct rrb_ctx {
     // Batch scratch.
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
-    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups;
+    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces;
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
@@ -368,15 +368,14 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
     const uint64_t n_paths = B->n_paths, n_pts = B->n_pts, supers = B->supers;
     const uint32_t n_pages = B->n_pages;
-    const uint32_t NP = static_cast<uint32_t>(n_paths), NS = static_cast<uint32_t>(n_pts);
+    const uint32_t NP = static_cast<uint32_t>(n_paths);
     const double flat_sq = B->flat_sq;
     int rc;
     RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
                                 c->stream));
-    // ---- stage 1: walk, flatten counts, edge offsets
-    if ((rc = ensure(c, c->s_pieces, n_pts * sizeof(uint2)))) return rc;
-    if ((rc = ensure(c, c->s_clip, n_pts * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_edge_off, (n_pts + 1) * sizeof(uint32_t)))) return rc;
+    // ---- stage 1: walk, compact pieces, flatten counts, edge offsets
+    if ((rc = ensure(c, c->s_slots, n_pts * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_path_pieces, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_block, (SCAN_MAX_BLOCKS + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
     RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
@@ -384,20 +383,33 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     k_walk<<<grid_for(c, n_paths, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
                                                              as<uint64_t>(B->off), NP, as<double>(B->mtx),
                                                              as<uint32_t>(B->page), as<uint32_t>(B->ph),
-                                                             as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip));
+                                                             as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_path_pieces), NP))) return rc;
+    if ((rc = read_back(c, as<uint32_t>(c->s_path_pieces) + NP, sizeof(uint32_t)))) return rc;
+    const uint64_t n_pieces = c->h_read[0];
+    const uint32_t NPC = static_cast<uint32_t>(n_pieces);
+    if ((rc = ensure(c, c->s_pieces, std::max<uint64_t>(1, n_pieces) * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_clip, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_edge_off, (n_pieces + 1) * sizeof(uint32_t)))) return rc;
+    k_compact_pieces<<<grid_for(c, n_paths, 128), 128, 0, c->stream>>>(
+        as<uint64_t>(B->off), as<uint32_t>(c->s_path_pieces), NP, as<uint32_t>(B->page), as<uint32_t>(B->ph),
+        as<uint2>(c->s_slots), as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip));
     c->launches += 1;
     stage_end(c, 0);
+    RRB_CUDA(c, cudaGetLastError());
     stage(c, 1);
-    k_seg_count<<<grid_for(c, n_pts, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NS,
-                                                                as<double>(B->mtx), flat_sq,
-                                                                as<uint32_t>(c->s_edge_off));
+    k_seg_count<<<grid_for(c, n_pieces, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NPC,
+                                                                   as<double>(B->mtx), flat_sq,
+                                                                   as<uint32_t>(c->s_edge_off));
     c->launches += 1;
     stage_end(c, 1);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 2);
-    if ((rc = scan_u32(c, as<uint32_t>(c->s_edge_off), as<uint32_t>(c->s_edge_off), NS))) return rc;
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_edge_off), as<uint32_t>(c->s_edge_off), NPC))) return rc;
     stage_end(c, 2);
-    if ((rc = read_back(c, as<uint32_t>(c->s_edge_off) + NS, sizeof(uint32_t)))) return rc;
+    if ((rc = read_back(c, as<uint32_t>(c->s_edge_off) + NPC, sizeof(uint32_t)))) return rc;
     const uint64_t n_edges = c->h_read[0];
     // ---- stage 2: edges, path boxes, row/chunk offsets, supertile bins
     if ((rc = ensure(c, c->s_edges, std::max<uint64_t>(1, n_edges) * sizeof(Edge)))) return rc;
@@ -407,15 +419,15 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_groups, ((n_edges + 31) / 32 + 1) * sizeof(int2)))) return rc;
     stage(c, 3);
-    k_seg_write<<<grid_for(c, n_pts, 128), 128, 0, c->stream>>>(
-        as<double>(B->pts), as<uint2>(c->s_pieces), NS, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
+    k_seg_write<<<grid_for(c, n_pieces, 128), 128, 0, c->stream>>>(
+        as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
         static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip));
     c->launches += 1;
     stage_end(c, 3);
     const int chunk_rows = 32;
     stage(c, 4);
     k_path_bbox<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(
-        as<uint64_t>(B->off), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
+        as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
         as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
         chunk_rows, as<BatchCounters>(c->s_ctr));
@@ -446,18 +458,19 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 4, &as<BatchCounters>(c->s_ctr)->raw_entries, 8, cudaMemcpyDeviceToHost,
                                 c->stream));
     RRB_CUDA(c, cudaStreamSynchronize(c->stream));
-    const uint64_t n_rows = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
+    const uint64_t n_groups = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
     uint64_t raw_entries;
     std::memcpy(&raw_entries, c->h_read + 4, 8);
-    // ---- stage 3: rows. A row with m merged entries yields at most m/2 + 1
-    // spans (every span consumes an opening and a closing entry, except the
-    // last one of a row whose winding never returns to zero).
-    uint64_t span_cap = raw_entries / 2 + n_rows + 1024;
-    if (span_cap > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 spans");
-    if (n_rows > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 rows");
-    if ((rc = ensure(c, c->s_row_idx, std::max<uint64_t>(1, n_rows) * sizeof(uint2)))) return rc;
-    if ((rc = ensure(c, c->s_spans, span_cap * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_ovf, std::max<uint64_t>(1, n_rows) * sizeof(uint2)))) return rc;
+    // ---- stage 3: rows -> coverage cells. An AA row with m merged entries
+    // yields at most m/2 + 1 spans, and a pixel row at most 2 cells per span
+    // boundary: cells <= 4 * spans <= 2 * raw entries + 4 * AA rows.
+    const uint64_t aa_rows = 4 * n_groups;
+    uint64_t cell_cap = 2 * raw_entries + 4 * aa_rows + 1024;
+    if (cell_cap > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 cells");
+    if (n_groups > 0x3FFFFFFFull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^30 pixel rows");
+    if ((rc = ensure(c, c->s_row_idx, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_spans, cell_cap * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_ovf, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
     stage(c, 8);
     k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
@@ -471,39 +484,46 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
             as<int2>(c->s_groups), as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
-            static_cast<uint32_t>(span_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_rows)),
-            as<BatchCounters>(c->s_ctr), chunk_rows);
+            static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
+            as<BatchCounters>(c->s_ctr));
         c->launches += 1;
     }
     stage_end(c, 9);
     RRB_CUDA(c, cudaGetLastError());
-    // Slow rows, if any: read the overflow count.
+    // Slow pixel rows, if any: read the overflow count.
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
     BatchCounters hc;
     std::memcpy(&hc, c->h_read, sizeof hc);
-    uint64_t slow_rows = std::min<uint64_t>(hc.ovf_count, n_rows);
-    if (slow_rows) {
-        uint64_t need = std::min<uint64_t>(slow_rows * 256 + n_edges, 0x7FFFFFFFull);
+    const uint64_t slow = std::min<uint64_t>(hc.ovf_count, n_groups);
+    if (slow) {
+        uint64_t need = std::min<uint64_t>(slow * 1024 + 4 * n_edges, 0x7FFFFFFFull);
+        // Every attempt re-runs all slow rows, so it restarts the cell
+        // allocation where the fast path left it.
+        c->h_read[64] = hc.cell_cursor;
+        c->h_read[65] = 0;
         stage(c, 10);
         for (int attempt = 0; attempt < 4; ++attempt) {
             if ((rc = ensure(c, c->s_scratch, need * sizeof(int3)))) return rc;
-            uint32_t zero = 0;
-            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &zero, 4, cudaMemcpyHostToDevice,
-                                        c->stream));
-            k_rows_slow<<<grid_for(c, slow_rows, 128), 128, 0, c->stream>>>(
+            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->cell_cursor, &c->h_read[64], 4,
+                                        cudaMemcpyHostToDevice, c->stream));
+            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &c->h_read[65], 4,
+                                        cudaMemcpyHostToDevice, c->stream));
+            k_groups_slow<<<grid_for(c, slow, 128), 128, 0, c->stream>>>(
                 as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), as<uint32_t>(B->pw),
-                as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_rows)), as<int3>(c->s_scratch),
-                static_cast<uint32_t>(c->s_scratch.cap / sizeof(int3)), as<uint2>(c->s_row_idx),
-                as<uint32_t>(c->s_spans), static_cast<uint32_t>(span_cap), as<BatchCounters>(c->s_ctr));
+                as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)), as<int3>(c->s_scratch),
+                static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
+                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
+                as<BatchCounters>(c->s_ctr));
             c->launches += 1;
             RRB_CUDA(c, cudaGetLastError());
             if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
             std::memcpy(&hc, c->h_read, sizeof hc);
             if (!(hc.err & ERR_SCRATCH_CAP)) break;
             // Not enough scratch: grow to what was asked for and run again.
-            need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + n_edges, 0x7FFFFFFFull);
-            uint32_t e0 = hc.err & ~ERR_SCRATCH_CAP;
-            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->err, &e0, 4, cudaMemcpyHostToDevice, c->stream));
+            need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + 4 * n_edges, 0x7FFFFFFFull);
+            c->h_read[66] = hc.err & ~ERR_SCRATCH_CAP;
+            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->err, &c->h_read[66], 4, cudaMemcpyHostToDevice,
+                                        c->stream));
         }
         stage_end(c, 10);
     }
@@ -519,10 +539,10 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
     std::memcpy(&hc, c->h_read, sizeof hc);
     c->stats.paths = n_paths;
-    c->stats.pieces = n_pts;
+    c->stats.pieces = n_pieces;
     c->stats.segments = n_edges;
-    c->stats.aa_rows = n_rows;
-    c->stats.spans = hc.span_cursor;
+    c->stats.aa_rows = aa_rows;
+    c->stats.spans = hc.cell_cursor;
     c->stats.row_overflows = hc.ovf_count;
     c->stats.tiles = tiles;
     c->stats.tile_pairs = n_pairs;
@@ -615,7 +635,7 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
-                      &c->s_groups};
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);

@@ -45,7 +45,7 @@ constexpr uint32_t ERR_EDGE_CAP = 1, ERR_ROW_CAP = 2, ERR_SPAN_CAP = 4, ERR_OVF_
 // Device counters of a batch.
 struct BatchCounters {
     uint32_t err;
-    uint32_t span_cursor;
+    uint32_t cell_cursor;
     uint32_t ovf_count;
     uint32_t scratch_cursor;
     uint32_t nonterminating;
@@ -67,7 +67,7 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
                        const uint64_t* __restrict__ path_pt_off, uint32_t n_paths,
                        const double* __restrict__ mtx, const uint32_t* __restrict__ path_page,
                        const uint32_t* __restrict__ page_h, uint2* __restrict__ pieces,
-                       uint32_t* __restrict__ slot_clip_hi) {
+                       uint32_t* __restrict__ path_pieces) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -75,8 +75,6 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
         uint32_t off = static_cast<uint32_t>(path_pt_off[p]);
         uint32_t n = static_cast<uint32_t>(path_pt_off[p + 1]) - off;
         uint32_t slot = off;
-        const uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u;
-        for (uint32_t k = 0; k < n; ++k) slot_clip_hi[off + k] = clip_hi;
         uint32_t i = 0;
         while (i < n) {
             if (flags[off + i] & PF_FIRST) {
@@ -105,7 +103,24 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
                 ++i;
             }
         }
-        for (; slot < off + n; ++slot) pieces[slot] = make_uint2(0u, PK_NONE << 30);
+        path_pieces[p] = slot - off;
+    }
+}
+
+// Pack each path's pieces (the first path_pieces[p] slots of its point range)
+// densely at piece_off[p], with the AA-row clip of the path's page.
+__global__ void k_compact_pieces(const uint64_t* __restrict__ path_pt_off, const uint32_t* __restrict__ piece_off,
+                                 uint32_t n_paths, const uint32_t* __restrict__ path_page,
+                                 const uint32_t* __restrict__ page_h, const uint2* __restrict__ slots,
+                                 uint2* __restrict__ pieces, uint32_t* __restrict__ piece_clip) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        const uint32_t src = static_cast<uint32_t>(path_pt_off[p]);
+        const uint32_t dst = piece_off[p], n = piece_off[p + 1] - dst;
+        const uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u;
+        for (uint32_t k = 0; k < n; ++k) {
+            pieces[dst + k] = slots[src + k];
+            piece_clip[dst + k] = clip_hi;
+        }
     }
 }
 
@@ -256,18 +271,18 @@ __global__ void k_scan_down(const uint32_t* __restrict__ in, uint32_t* __restric
 // path reduces its edges to the AA row range and AA column range, then maps
 // them to the pixel rectangle the row map can touch.
 // ---------------------------------------------------------------------------
-__global__ void k_path_bbox(const uint64_t* __restrict__ path_pt_off, const uint32_t* __restrict__ edge_off,
+__global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
                             const Edge* __restrict__ edges, uint32_t n_paths, const uint8_t* __restrict__ rule,
                             const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha,
                             const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
                             const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
-                            uint32_t* __restrict__ path_rows, uint32_t* __restrict__ path_chunks,
+                            uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
                             int chunk_rows, BatchCounters* __restrict__ ctr) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t p = warp_g; p < n_paths; p += nwarps) {
-        uint32_t eb = edge_off[path_pt_off[p]], ee = edge_off[path_pt_off[p + 1]];
+        uint32_t eb = edge_off[piece_off[p]], ee = edge_off[piece_off[p + 1]];
         int32_t y0 = INT32_MAX, y1 = INT32_MIN, xl = INT32_MAX, xh = INT32_MIN;
         unsigned long long raw = 0;
         for (uint32_t j = eb + lane; j < ee; j += 32) {
@@ -298,11 +313,12 @@ __global__ void k_path_bbox(const uint64_t* __restrict__ path_pt_off, const uint
             pi.paint = uint32_t(gray[p]) | (uint32_t(alpha[p]) << 8) | (uint32_t(rule[p] ? 1 : 0) << 16);
             pi.page = pg;
             pi.pad0 = pi.pad1 = 0;
-            uint32_t rows = 0;
+            uint32_t rows = 0, groups = 0;
             if (y0 <= y1) {
                 pi.y0 = y0;
                 pi.y1 = y1;
-                rows = static_cast<uint32_t>(y1 - y0 + 1);
+                rows = static_cast<uint32_t>(y1 - (y0 & ~3) + 1);     // rows of the 4-aligned chunks
+                groups = static_cast<uint32_t>((y1 >> 2) - (y0 >> 2) + 1);
                 // Pixel columns: spans cover AA columns [max(x0,0), min(x1+1, 4W)).
                 int32_t cl = max(xl, 0), ch = min(xh, 4 * W - 1);
                 pi.px0 = cl >> 2;
@@ -331,7 +347,7 @@ __global__ void k_path_bbox(const uint64_t* __restrict__ path_pt_off, const uint
                 pi.py1 = 0;
             }
             info[p] = pi;
-            path_rows[p] = rows;
+            path_groups[p] = groups;
             path_chunks[p] = (rows + chunk_rows - 1) / chunk_rows;
         }
     }
@@ -423,6 +439,21 @@ __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* _
 // ---------------------------------------------------------------------------
 constexpr int ROWS_WARPS = 4;
 
+// 32x32 bit-matrix transpose across a warp: on entry bit j of lane i is
+// A[i][j]; on exit bit j of lane i is A[j][i]. Five butterfly stages, each
+// swapping the off-diagonal s x s blocks with the partner lane i ^ s.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
+    const uint32_t LOW[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int s = 16 >> k;
+        const uint32_t lo = LOW[k];
+        const uint32_t p = __shfl_xor_sync(0xffffffffu, x, s);
+        x = (lane & s) ? ((x & ~lo) | ((p & ~lo) >> s)) : ((x & lo) | ((p & lo) << s));
+    }
+    return x;
+}
+
 __device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? v : v + 1; }
 
 // Winding walk of render_aa_line (scanner/mod.rs:393-467) for one AA row over
@@ -484,6 +515,59 @@ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, G
     return ns;
 }
 
+// Coverage cells of one pixel row from the sorted, disjoint span lists of its
+// four AA sub-rows (draw_aa_line's per-pixel nibble popcount, fill/mod.rs:
+// 344-401, computed from spans): the coverage of pixel x is the number of
+// (sub-row, AA column) pairs covered in columns [4x, 4x+4), 0..16. Boundaries
+// of all four lists are merged in column order; pixels that contain a
+// boundary get their own cell, the pixels between two such pixels share one
+// run cell of coverage 4 x depth. Cells come out sorted by x, disjoint, with
+// coverage > 0; at most one per boundary plus one run per gap, i.e. at most
+// 2 x (number of boundaries). Cell: x0 (bits 0-13) | len-1 (14-27) | cov-1 (28-31).
+template <typename Bound, typename Put>
+__device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bound, Put put) {
+    int bi[4] = {0, 0, 0, 0};
+    int depth = 0, nc = 0;
+    int32_t prev_px = -1;
+    auto next = [&](int& kmin) -> int32_t {
+        int32_t best = INT32_MAX;
+        kmin = -1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (bi[k] < 2 * n[k]) {
+                const int32_t v = bound(k, bi[k] >> 1, (bi[k] & 1) != 0);
+                if (v < best) {
+                    best = v;
+                    kmin = k;
+                }
+            }
+        }
+        return best;
+    };
+    auto emit = [&](int32_t x0, int32_t len, int32_t cov) {
+        put(nc++, static_cast<uint32_t>(x0) | (static_cast<uint32_t>(len - 1) << 14) |
+                      (static_cast<uint32_t>(cov - 1) << 28));
+    };
+    int k;
+    int32_t b = next(k);
+    while (k >= 0) {
+        const int32_t px = b >> 2;
+        if (depth > 0 && px - 1 >= prev_px + 1) emit(prev_px + 1, px - 1 - prev_px, 4 * depth);
+        int32_t col = 4 * px, cov = 0;
+        while (k >= 0 && b < 4 * px + 4) {
+            cov += depth * (b - col);
+            col = b;
+            depth += (bi[k] & 1) ? -1 : 1;
+            ++bi[k];
+            b = next(k);
+        }
+        cov += depth * (4 * px + 4 - col);
+        if (cov > 0) emit(px, 1, cov);
+        prev_px = px;
+    }
+    return nc;
+}
+
 // Row range [min row0, max row1] of each aligned group of 32 edges (empty
 // edges excluded), so a chunk can skip whole groups with one load.
 __global__ void k_edge_groups(const Edge* __restrict__ edges, uint32_t n_edges, int2* __restrict__ groups) {
@@ -503,16 +587,17 @@ __global__ void k_edge_groups(const Edge* __restrict__ edges, uint32_t n_edges, 
 
 template <int KCAP>
 __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
-    const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ row_off,
+    const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
     const Edge* __restrict__ edges, const int2* __restrict__ groups, const uint32_t* __restrict__ page_w,
-    uint32_t n_paths, uint2* __restrict__ row_idx, uint32_t* __restrict__ spans, uint32_t span_cap,
-    uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr, int chunk_rows) {
+    uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells, uint32_t cell_cap,
+    uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr) {
     __shared__ int32_t sx0[ROWS_WARPS][KCAP][32];
     __shared__ int32_t sx1[ROWS_WARPS][KCAP][32];
     __shared__ int32_t scn[ROWS_WARPS][KCAP][32];
     // Edge records of the current batch, field-major so that lanes reading
     // different edges hit different banks.
     __shared__ int32_t sedge[ROWS_WARPS][8][32];
+    __shared__ int32_t sns[ROWS_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
@@ -526,10 +611,12 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
         }
         const uint32_t p = lo;
         const PathInfo P = info[p];
-        const int32_t chunk_lo = P.y0 + static_cast<int32_t>(c - chunk_off[p]) * chunk_rows;
-        const int32_t chunk_hi = min(chunk_lo + chunk_rows - 1, P.y1);
+        // Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the
+        // four sub-rows of one pixel row.
+        const int32_t chunk_lo = (P.y0 & ~3) + static_cast<int32_t>(c - chunk_off[p]) * 32;
+        const int32_t chunk_hi = min(chunk_lo + 31, P.y1);
         const int32_t r = chunk_lo + lane;
-        const bool valid = lane < chunk_rows && r <= chunk_hi;
+        const bool valid = r >= P.y0 && r <= chunk_hi;
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
         int n = 0;
@@ -545,8 +632,7 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
                 e = edges[j];
                 hit = !(e.flags & EF_EMPTY) && e.row0 <= chunk_hi && e.row1 >= chunk_lo;
             }
-            uint32_t m = __ballot_sync(0xffffffffu, hit);
-            if (!m) continue;
+            if (!__any_sync(0xffffffffu, hit)) continue;
             if (hit) {
                 sedge[w][0][lane] = e.row0;
                 sedge[w][1][lane] = e.row1;
@@ -558,14 +644,15 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
                 sedge[w][7][lane] = e.cmax;
             }
             __syncwarp();
-            // Edges of this batch covering this lane's row, in edge order.
-            uint32_t mine = 0;
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                if (sedge[w][0][b] <= r && r <= sedge[w][1][b]) mine |= 1u << b;
+            // Lane j holds the chunk rows edge j covers; transposing the 32x32
+            // bit matrix gives lane r the edges covering row r, in edge order.
+            uint32_t rows_of_edge = 0;
+            if (hit) {
+                const int32_t a = max(e.row0, chunk_lo) - chunk_lo, b = min(e.row1, chunk_hi) - chunk_lo;
+                rows_of_edge = (0xffffffffu >> (31 - b)) & (0xffffffffu << a);
             }
-            if (!valid) mine = 0;
+            const uint32_t mine_all = warp_transpose32(rows_of_edge, lane);
+            uint32_t mine = valid ? mine_all : 0u;
             while (mine) {
                 const int b = __ffs(mine) - 1;
                 mine &= mine - 1;
@@ -642,32 +729,47 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
                 },
                 nonterm);
         }
-        // Allocate span storage for the whole warp with one atomic.
-        uint32_t incl = ns;
+        // ---- one pixel row per 4 lanes: merge the sub-rows' spans into cells
+        sns[w][lane] = (valid && !overflow) ? ns : 0;
+        const uint32_t ovf_lanes = __ballot_sync(0xffffffffu, overflow);
+        __syncwarp();
+        const bool leader = (lane & 3) == 0 && r <= P.y1;  // group has a row in [y0, y1]
+        const bool g_ovf = ((ovf_lanes >> (lane & ~3)) & 0xFu) != 0;
+        int n4[4] = {0, 0, 0, 0};
+        uint32_t need = 0;
+        if (leader && !g_ovf) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) n4[k] = sns[w][lane + k];
+            need = 4u * static_cast<uint32_t>(n4[0] + n4[1] + n4[2] + n4[3]);  // 2 cells per span boundary
+        }
+        uint32_t incl = need;
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
         uint32_t base = 0;
-        if (lane == 31 && total) base = atomicAdd(&ctr->span_cursor, total);
+        if (lane == 31 && total) base = atomicAdd(&ctr->cell_cursor, total);
         base = __shfl_sync(0xffffffffu, base, 31);
-        const bool fits = static_cast<uint64_t>(base) + total <= span_cap;
+        const bool fits = static_cast<uint64_t>(base) + total <= cell_cap;
         if (lane == 0 && total && !fits) atomicOr(&ctr->err, ERR_SPAN_CAP);
-        if (valid) {
-            uint32_t ri = row_off[p] + static_cast<uint32_t>(r - P.y0);
-            if (overflow) {
-                uint32_t k = atomicAdd(&ctr->ovf_count, 1u);
-                if (k < ovf_cap) ovf[k] = make_uint2(p, static_cast<uint32_t>(r));
+        if (leader) {
+            const int32_t g = r >> 2;
+            const uint32_t gi = group_off[p] + static_cast<uint32_t>(g - (P.y0 >> 2));
+            if (g_ovf) {
+                const uint32_t k = atomicAdd(&ctr->ovf_count, 1u);
+                if (k < ovf_cap) ovf[k] = make_uint2(p, static_cast<uint32_t>(g));
                 else atomicOr(&ctr->err, ERR_OVF_CAP);
-                row_idx[ri] = make_uint2(0u, 0u);
+                group_idx[gi] = make_uint2(0u, 0u);
             } else if (fits) {
-                uint32_t o0 = base + incl - ns;
-                for (int k = 0; k < ns; ++k)
-                    spans[o0 + k] = static_cast<uint32_t>(sx0[w][k][lane]) | (static_cast<uint32_t>(sx1[w][k][lane]) << 16);
-                row_idx[ri] = make_uint2(o0, static_cast<uint32_t>(ns));
+                const uint32_t o0 = base + incl - need;
+                const int nc = sweep_cells(
+                    n4,
+                    [&](int k, int i, bool end) { return end ? sx1[w][i][lane + k] : sx0[w][i][lane + k]; },
+                    [&](int q, uint32_t cell) { cells[o0 + q] = cell; });
+                group_idx[gi] = make_uint2(o0, static_cast<uint32_t>(nc));
             } else {
-                row_idx[ri] = make_uint2(0u, 0u);
+                group_idx[gi] = make_uint2(0u, 0u);
             }
         }
         __syncwarp();
@@ -675,74 +777,87 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
 }
 
-// Rows whose merged list exceeded KCAP: one thread per row, the list in a
-// global scratch slice sized by the path's edge count.
-__global__ void k_rows_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ row_off,
-                            const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w,
-                            const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
-                            uint32_t scratch_cap, uint2* __restrict__ row_idx, uint32_t* __restrict__ spans,
-                            uint32_t span_cap, BatchCounters* __restrict__ ctr) {
-    uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);
+// Pixel rows with a sub-row whose merged list exceeded KCAP: one thread per
+// pixel row, the four sub-row lists in a global scratch slice of 4 x the
+// path's edge count.
+__global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off,
+                              const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w,
+                              const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
+                              uint32_t scratch_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
+                              uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
+    const uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);
     uint32_t nonterm = 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_ovf; k += gridDim.x * blockDim.x) {
-        uint32_t p = ovf[k].x;
-        int32_t r = static_cast<int32_t>(ovf[k].y);
+        const uint32_t p = ovf[k].x;
+        const int32_t g = static_cast<int32_t>(ovf[k].y);
         const PathInfo P = info[p];
-        uint32_t ne = P.e_end - P.e_begin;
-        uint32_t sb = atomicAdd(&ctr->scratch_cursor, ne);
-        if (static_cast<uint64_t>(sb) + ne > scratch_cap) {
+        const uint32_t ne = P.e_end - P.e_begin;
+        const uint32_t sb = atomicAdd(&ctr->scratch_cursor, 4u * ne);
+        if (static_cast<uint64_t>(sb) + 4ull * ne > scratch_cap) {
             atomicOr(&ctr->err, ERR_SCRATCH_CAP);
             continue;
         }
-        int3* L = scratch + sb;
-        int n = 0;
-        for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
-            Edge E = edges[j];
-            if ((E.flags & EF_EMPTY) || r < E.row0 || r > E.row1) continue;
-            int32_t elo, ehi, ec;
-            edge_entry(E, r, elo, ehi, ec);
-            if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
-                L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
-                L[n - 1].x = min(L[n - 1].x, elo);
-                L[n - 1].y = max(L[n - 1].y, ehi);
-            } else {
-                L[n++] = make_int3(elo, ehi, ec);
-            }
-        }
-        // Stable sort by x0 (rows > 20 entries: see the tie note in the oracle).
-        for (int a = 1; a < n; ++a) {
-            int3 t = L[a];
-            int b = a;
-            while (b > 0 && t.x < L[b - 1].x) {
-                L[b] = L[b - 1];
-                --b;
-            }
-            L[b] = t;
-        }
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
-        int ns = walk_row(
-            n, mask, aa_width,
-            [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
-                x0 = L[i].x;
-                x1 = L[i].y;
-                cc = L[i].z;
-            },
-            [&](int q, int32_t s, int32_t e) {
-                L[q].x = s;
-                L[q].y = e;
-            },
-            nonterm);
-        uint32_t ri = row_off[p] + static_cast<uint32_t>(r - P.y0);
-        uint32_t o0 = ns ? atomicAdd(&ctr->span_cursor, static_cast<uint32_t>(ns)) : 0u;
-        if (static_cast<uint64_t>(o0) + ns > span_cap) {
+        int n4[4] = {0, 0, 0, 0};
+        for (int sub = 0; sub < 4; ++sub) {
+            const int32_t r = 4 * g + sub;
+            if (r < P.y0 || r > P.y1) continue;
+            int3* L = scratch + sb + static_cast<uint32_t>(sub) * ne;
+            int n = 0;
+            for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
+                const Edge E = edges[j];
+                if ((E.flags & EF_EMPTY) || r < E.row0 || r > E.row1) continue;
+                int32_t elo, ehi, ec;
+                edge_entry(E, r, elo, ehi, ec);
+                if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
+                    L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
+                    L[n - 1].x = min(L[n - 1].x, elo);
+                    L[n - 1].y = max(L[n - 1].y, ehi);
+                } else {
+                    L[n++] = make_int3(elo, ehi, ec);
+                }
+            }
+            // Stable sort by x0 (a row of more than 20 entries: see the tie note in the oracle).
+            for (int a = 1; a < n; ++a) {
+                const int3 t = L[a];
+                int b = a;
+                while (b > 0 && t.x < L[b - 1].x) {
+                    L[b] = L[b - 1];
+                    --b;
+                }
+                L[b] = t;
+            }
+            n4[sub] = walk_row(
+                n, mask, aa_width,
+                [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
+                    x0 = L[i].x;
+                    x1 = L[i].y;
+                    cc = L[i].z;
+                },
+                [&](int q, int32_t s0, int32_t e0) {
+                    L[q].x = s0;
+                    L[q].y = e0;
+                },
+                nonterm);
+        }
+        const uint32_t need = 4u * static_cast<uint32_t>(n4[0] + n4[1] + n4[2] + n4[3]);
+        const uint32_t gi = group_off[p] + static_cast<uint32_t>(g - (P.y0 >> 2));
+        const uint32_t o0 = need ? atomicAdd(&ctr->cell_cursor, need) : 0u;
+        if (static_cast<uint64_t>(o0) + need > cell_cap) {
             atomicOr(&ctr->err, ERR_SPAN_CAP);
-            row_idx[ri] = make_uint2(0u, 0u);
+            group_idx[gi] = make_uint2(0u, 0u);
             continue;
         }
-        for (int q = 0; q < ns; ++q)
-            spans[o0 + q] = static_cast<uint32_t>(L[q].x) | (static_cast<uint32_t>(L[q].y) << 16);
-        row_idx[ri] = make_uint2(o0, static_cast<uint32_t>(ns));
+        const int3* base = scratch + sb;
+        const int nc = sweep_cells(
+            n4,
+            [&](int sub, int i, bool end) {
+                const int3 v = base[static_cast<uint32_t>(sub) * ne + i];
+                return end ? v.y : v.x;
+            },
+            [&](int q, uint32_t cell) { cells[o0 + q] = cell; });
+        group_idx[gi] = make_uint2(o0, static_cast<uint32_t>(nc));
     }
     if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
 }
@@ -760,59 +875,95 @@ constexpr int COMP_CHUNK = 256;
 __constant__ uint8_t c_gamma[17] = {0, 4, 11, 21, 32, 45, 59, 74, 90, 108, 126, 145, 166, 187, 209, 231, 255};
 
 struct HitInfo {
-    int32_t y0, y1, py0, py1;
-    uint32_t row_off, paint;
+    int32_t g0, g1, py0, py1;  // pixel-row groups [g0, g1] (AA rows >> 2), pixel rows touched
+    uint32_t goff, paint;      // first group index entry, paint word
 };
 
+template <int TW>
+struct CompLayout {
+    static constexpr int LPR = TW < 32 ? TW : 32;  // lanes per pixel row
+    static constexpr int PX = TW / LPR;            // pixels per lane
+    static constexpr int RPW = 32 / LPR;           // rows per warp step
+    static constexpr int NW = COMP_THREADS / 32;
+};
+
+// One path over the rows of this thread's tile slots: fetch the pixel row's
+// coverage cells (group g = y, or 4y+3 under the as-shipped row map), find
+// each pixel's cell (start marks in shared memory + a prefix max across the
+// row's lanes), then AA_GAMMA and the div255 source-over of
+// render_span_aa_inner's no-alpha arm (pipe/aa.rs:192-208).
 template <int TW, int TH>
-__device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap, int tile_x0, int tile_y0, int W,
-                                                    int H, const uint2* __restrict__ row_idx,
-                                                    const uint32_t* __restrict__ spans, const uint8_t* gamma,
+__device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap, int X0, int Y0, int H,
+                                                    const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
+                                                    const uint8_t* gamma, int32_t (*mark)[TW],
                                                     uint32_t (&pix)[TH * TW / COMP_THREADS]) {
-    constexpr int LPR = TW < 32 ? TW : 32;            // lanes per pixel row
-    constexpr int PX = TW / LPR;                      // pixels per lane
-    constexpr int RPW = 32 / LPR;                     // rows per warp step
-    constexpr int NW = COMP_THREADS / 32;
-    constexpr int ITERS = TH / (NW * RPW);
+    using L = CompLayout<TW>;
+    constexpr int ITERS = TH / (L::NW * L::RPW);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int col = (lane % LPR) * PX;
-    const int32_t g = static_cast<int32_t>(h.paint & 0xff);
-    const uint32_t alpha = (h.paint >> 8) & 0xff;
-    const int32_t c_tile0 = 4 * tile_x0, c_tile1 = 4 * (tile_x0 + TW);
+    const int sub = lane % L::LPR;            // lane within its pixel row
+    const int slot = lane / L::LPR;           // pixel row of this warp step
+    const int col = sub * L::PX;
+    const uint32_t g = h.paint & 0xff, alpha = (h.paint >> 8) & 0xff;
 #pragma unroll
     for (int it = 0; it < ITERS; ++it) {
-        const int ry = (w * RPW + lane / LPR) + it * NW * RPW;
-        const int y = tile_y0 + ry;
-        if (y < h.py0 || y > h.py1 || y >= H) continue;
-        const int32_t base = rowmap ? 16 * y + 12 : 4 * y;
-        int32_t cov[PX];
+        const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
+        const int32_t grp = rowmap ? 4 * y + 3 : y;
+        const bool rowok = y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
+        uint2 ix = make_uint2(0u, 0u);
+        if (rowok) ix = gidx[h.goff + static_cast<uint32_t>(grp - h.g0)];
+        // Cells of this row overlapping the tile are processed LPR at a time.
+        uint32_t nb = (ix.y + L::LPR - 1) / L::LPR;
+        for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
+        int32_t cov[L::PX];
 #pragma unroll
-        for (int q = 0; q < PX; ++q) cov[q] = 0;
+        for (int q = 0; q < L::PX; ++q) cov[q] = 0;
+        for (uint32_t bt = 0; bt < nb; ++bt) {
 #pragma unroll
-        for (int sub = 0; sub < 4; ++sub) {
-            const int32_t r = base + sub;
-            if (r < h.y0 || r > h.y1) continue;
-            const uint2 ix = row_idx[h.row_off + static_cast<uint32_t>(r - h.y0)];
-            for (uint32_t j = 0; j < ix.y; ++j) {
-                const uint32_t sp = spans[ix.x + j];
-                const int32_t s = static_cast<int32_t>(sp & 0xffffu), e = static_cast<int32_t>(sp >> 16);
-                if (e <= c_tile0) continue;
-                if (s >= c_tile1) break;
+            for (int q = 0; q < L::PX; ++q) mark[w * L::RPW + slot][col + q] = -1;
+            __syncwarp();
+            const uint32_t j = bt * L::LPR + sub;
+            uint32_t cell = 0;
+            if (j < ix.y) {
+                cell = cells[ix.x + j];
+                const int32_t x0 = static_cast<int32_t>(cell & 0x3fffu);
+                const int32_t x1 = x0 + static_cast<int32_t>((cell >> 14) & 0x3fffu) + 1;
+                const int32_t sx = max(x0, X0);
+                if (sx < min(x1, X0 + TW)) mark[w * L::RPW + slot][sx - X0] = sub;
+            }
+            __syncwarp();
+            int32_t v[L::PX];
+            int32_t run = -1;
 #pragma unroll
-                for (int q = 0; q < PX; ++q) {
-                    const int32_t pc = 4 * (tile_x0 + col + q);
-                    cov[q] += max(0, min(e, pc + 4) - max(s, pc));
-                }
+            for (int q = 0; q < L::PX; ++q) {
+                run = max(run, mark[w * L::RPW + slot][col + q]);
+                v[q] = run;
+            }
+            // Exclusive prefix max of `run` over the lanes before this one in the row.
+            int32_t incl = run;
+#pragma unroll
+            for (int o = 1; o < L::LPR; o <<= 1) {
+                const int32_t t = __shfl_up_sync(0xffffffffu, incl, o, L::LPR);
+                if (sub >= o) incl = max(incl, t);
+            }
+            int32_t before = __shfl_up_sync(0xffffffffu, incl, 1, L::LPR);
+            if (sub == 0) before = -1;
+#pragma unroll
+            for (int q = 0; q < L::PX; ++q) {
+                const int32_t idx = max(before, v[q]);
+                const uint32_t c = __shfl_sync(0xffffffffu, cell, idx >= 0 ? idx : sub, L::LPR);
+                const int32_t x0 = static_cast<int32_t>(c & 0x3fffu);
+                const int32_t x1 = x0 + static_cast<int32_t>((c >> 14) & 0x3fffu) + 1;
+                const int32_t x = X0 + col + q;
+                if (idx >= 0 && x < x1) cov[q] = static_cast<int32_t>(c >> 28) + 1;
             }
         }
 #pragma unroll
-        for (int q = 0; q < PX; ++q) {
+        for (int q = 0; q < L::PX; ++q) {
             if (cov[q] == 0) continue;
             const uint32_t shape = gamma[min(cov[q], 16)];
             const uint32_t a_src = div255(alpha * shape);
-            const int k = it * PX + q;
-            const uint32_t d = pix[k];
-            pix[k] = div255((255u - a_src) * d + a_src * static_cast<uint32_t>(g));
+            const int k = it * L::PX + q;
+            pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
         }
     }
 }
@@ -821,22 +972,20 @@ template <int TW, int TH>
 __global__ void __launch_bounds__(COMP_THREADS) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
-    const uint32_t* __restrict__ row_off, const uint2* __restrict__ row_idx, const uint32_t* __restrict__ spans,
+    const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
     uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr) {
-    constexpr int LPR = TW < 32 ? TW : 32;
-    constexpr int PX = TW / LPR;
-    constexpr int RPW = 32 / LPR;
-    constexpr int NW = COMP_THREADS / 32;
-    constexpr int ITERS = TH / (NW * RPW);
+    using L = CompLayout<TW>;
+    constexpr int ITERS = TH / (L::NW * L::RPW);
     constexpr int NPIX = TH * TW / COMP_THREADS;
-    static_assert(ITERS * PX == NPIX, "tile shape must cover the CTA exactly");
+    static_assert(ITERS * L::PX == NPIX, "tile shape must cover the CTA exactly");
     __shared__ HitInfo hits[COMP_CHUNK];
-    __shared__ uint32_t wcnt[NW];
+    __shared__ uint32_t wcnt[L::NW];
     __shared__ uint8_t gamma[17];
+    __shared__ int32_t mark[L::NW * L::RPW][TW];
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int col = (lane % LPR) * PX;
+    const int col = (lane % L::LPR) * L::PX;
     for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const uint32_t pg = find_page_by(pages, n_pages, t, false);
         const PageGeom G = pages[pg];
@@ -848,11 +997,11 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
         uint32_t pix[NPIX];
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int y = Y0 + (w * RPW + lane / LPR) + it * NW * RPW;
+            const int y = Y0 + (w * L::RPW + lane / L::LPR) + it * L::NW * L::RPW;
 #pragma unroll
-            for (int q = 0; q < PX; ++q) {
+            for (int q = 0; q < L::PX; ++q) {
                 const int x = X0 + col + q;
-                pix[it * PX + q] = (y < H && x < W) ? page[static_cast<size_t>(y) * W + x] : 0u;
+                pix[it * L::PX + q] = (y < H && x < W) ? page[static_cast<size_t>(y) * W + x] : 0u;
             }
         }
         const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
@@ -871,7 +1020,7 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
             __syncthreads();
             uint32_t before = 0, total = 0;
 #pragma unroll
-            for (int k = 0; k < NW; ++k) {
+            for (int k = 0; k < L::NW; ++k) {
                 const uint32_t v = wcnt[k];
                 before += k < w ? v : 0u;
                 total += v;
@@ -879,28 +1028,28 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
             if (hit) {
                 const uint32_t pos = before + __popc(m & lanemask_lt());
                 HitInfo hi;
-                hi.y0 = P.y0;
-                hi.y1 = P.y1;
+                hi.g0 = P.y0 >> 2;
+                hi.g1 = P.y1 >> 2;
                 hi.py0 = P.py0;
                 hi.py1 = P.py1;
-                hi.row_off = row_off[super_list[q]];
+                hi.goff = group_off[super_list[q]];
                 hi.paint = P.paint;
                 hits[pos] = hi;
             }
             __syncthreads();
             for (uint32_t k = 0; k < total; ++k) {
-                HitInfo h = hits[k];
-                composite_path_rows<TW, TH>(h, rowmap, X0, Y0, W, H, row_idx, spans, gamma, pix);
+                const HitInfo h = hits[k];
+                composite_path_rows<TW, TH>(h, rowmap, X0, Y0, H, gidx, cells, gamma, mark, pix);
             }
             __syncthreads();
         }
 #pragma unroll
         for (int it = 0; it < ITERS; ++it) {
-            const int y = Y0 + (w * RPW + lane / LPR) + it * NW * RPW;
+            const int y = Y0 + (w * L::RPW + lane / L::LPR) + it * L::NW * L::RPW;
 #pragma unroll
-            for (int q = 0; q < PX; ++q) {
+            for (int q = 0; q < L::PX; ++q) {
                 const int x = X0 + col + q;
-                if (y < H && x < W) page[static_cast<size_t>(y) * W + x] = static_cast<uint8_t>(pix[it * PX + q]);
+                if (y < H && x < W) page[static_cast<size_t>(y) * W + x] = static_cast<uint8_t>(pix[it * L::PX + q]);
             }
         }
     }
