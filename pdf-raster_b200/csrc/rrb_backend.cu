@@ -541,7 +541,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     c->stats.paths = n_paths;
     c->stats.pieces = n_pieces;
     c->stats.segments = n_edges;
-    c->stats.aa_rows = aa_rows;
+    c->stats.aa_rows = hc.aa_rows;
     c->stats.spans = hc.cell_cursor;
     c->stats.row_overflows = hc.ovf_count;
     c->stats.tiles = tiles;

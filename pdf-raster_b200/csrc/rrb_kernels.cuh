@@ -51,6 +51,7 @@ struct BatchCounters {
     uint32_t nonterminating;
     uint32_t pad[3];
     unsigned long long raw_entries;  // sum over edges of the rows they cover
+    unsigned long long aa_rows;      // sum over paths of y1 - y0 + 1
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -305,6 +306,7 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
         }
         if (lane == 0) {
             if (raw) atomicAdd(&ctr->raw_entries, raw);
+            if (y0 <= y1) atomicAdd(&ctr->aa_rows, static_cast<unsigned long long>(y1 - y0 + 1));
             uint32_t pg = path_page[p];
             int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
             PathInfo pi;
