@@ -62,7 +62,7 @@ struct rrb_ctx {
     // Batch scratch.
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
-    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces;
+    Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
@@ -417,7 +417,13 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_rows, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_chunks, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_groups, ((n_edges + 31) / 32 + 1) * sizeof(int2)))) return rc;
+    const uint64_t n_egroups = (n_edges + 31) / 32 + 1;
+    if ((rc = ensure(c, c->s_groups, n_egroups * 2 * sizeof(int32_t)))) return rc;
+    int32_t* gmin = as<int32_t>(c->s_groups);
+    int32_t* gmax = gmin + n_egroups;
+    // 0x7f7f7f7f / 0x80808080: beyond any AA row, so they act as +inf / -inf.
+    RRB_CUDA(c, cudaMemsetAsync(gmin, 0x7f, n_egroups * sizeof(int32_t), c->stream));
+    RRB_CUDA(c, cudaMemsetAsync(gmax, 0x80, n_egroups * sizeof(int32_t), c->stream));
     stage(c, 3);
     k_seg_write<<<grid_for(c, n_pieces, 128), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
@@ -430,10 +436,8 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
         as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
-        chunk_rows, as<BatchCounters>(c->s_ctr));
-    k_edge_groups<<<grid_for(c, (n_edges + 31) / 32, 128), 128, 0, c->stream>>>(
-        as<Edge>(c->s_edges), static_cast<uint32_t>(n_edges), as<int2>(c->s_groups));
-    c->launches += 2;
+        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax);
+    c->launches += 1;
     stage_end(c, 4);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 5);
@@ -483,47 +487,61 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         int g = grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16);
         k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
-            as<int2>(c->s_groups), as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+            gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
             static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
             as<BatchCounters>(c->s_ctr));
         c->launches += 1;
     }
     stage_end(c, 9);
     RRB_CUDA(c, cudaGetLastError());
-    // Slow pixel rows, if any: read the overflow count.
+    // Overflowing pixel rows, if any: the warp-per-row middle path, then the
+    // sequential path for rows longer than its shared lists.
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
     BatchCounters hc;
     std::memcpy(&hc, c->h_read, sizeof hc);
-    const uint64_t slow = std::min<uint64_t>(hc.ovf_count, n_groups);
-    if (slow) {
-        uint64_t need = std::min<uint64_t>(slow * 1024 + 4 * n_edges, 0x7FFFFFFFull);
-        // Every attempt re-runs all slow rows, so it restarts the cell
-        // allocation where the fast path left it.
-        c->h_read[64] = hc.cell_cursor;
-        c->h_read[65] = 0;
+    const uint32_t ovf_cap = static_cast<uint32_t>(std::max<uint64_t>(1, n_groups));
+    const uint64_t mid = std::min<uint64_t>(hc.ovf_count, n_groups);
+    if (mid) {
+        if ((rc = ensure(c, c->s_ovf2, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
         stage(c, 10);
-        for (int attempt = 0; attempt < 4; ++attempt) {
-            if ((rc = ensure(c, c->s_scratch, need * sizeof(int3)))) return rc;
-            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->cell_cursor, &c->h_read[64], 4,
-                                        cudaMemcpyHostToDevice, c->stream));
-            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &c->h_read[65], 4,
-                                        cudaMemcpyHostToDevice, c->stream));
-            k_groups_slow<<<grid_for(c, slow, 128), 128, 0, c->stream>>>(
-                as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), as<uint32_t>(B->pw),
-                as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)), as<int3>(c->s_scratch),
-                static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
-                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
-                as<BatchCounters>(c->s_ctr));
-            c->launches += 1;
-            RRB_CUDA(c, cudaGetLastError());
-            if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
-            std::memcpy(&hc, c->h_read, sizeof hc);
-            if (!(hc.err & ERR_SCRATCH_CAP)) break;
-            // Not enough scratch: grow to what was asked for and run again.
-            need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + 4 * n_edges, 0x7FFFFFFFull);
-            c->h_read[66] = hc.err & ~ERR_SCRATCH_CAP;
-            RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->err, &c->h_read[66], 4, cudaMemcpyHostToDevice,
-                                        c->stream));
+        k_groups_mid<<<grid_for(c, mid * 32, MID_WARPS * 32, 16), MID_WARPS * 32, 0, c->stream>>>(
+            as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), gmin, gmax,
+            as<uint32_t>(B->pw), as<uint2>(c->s_ovf), ovf_cap, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+            static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf2), as<BatchCounters>(c->s_ctr));
+        c->launches += 1;
+        RRB_CUDA(c, cudaGetLastError());
+        if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+        std::memcpy(&hc, c->h_read, sizeof hc);
+        const uint64_t slow = std::min<uint64_t>(hc.ovf2_count, n_groups);
+        if (slow) {
+            uint64_t need = std::min<uint64_t>(slow * 4096 + 4 * n_edges, 0x7FFFFFFFull);
+            // Every attempt re-runs all slow rows, so it restarts the cell
+            // allocation where the faster paths left it.
+            c->h_read[64] = hc.cell_cursor;
+            c->h_read[65] = 0;
+            for (int attempt = 0; attempt < 4; ++attempt) {
+                if ((rc = ensure(c, c->s_scratch, need * sizeof(int3)))) return rc;
+                RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->cell_cursor, &c->h_read[64], 4,
+                                            cudaMemcpyHostToDevice, c->stream));
+                RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &c->h_read[65], 4,
+                                            cudaMemcpyHostToDevice, c->stream));
+                k_groups_slow<<<grid_for(c, slow, 128), 128, 0, c->stream>>>(
+                    as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), as<uint32_t>(B->pw),
+                    as<uint2>(c->s_ovf2), ovf_cap, as<int3>(c->s_scratch),
+                    static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
+                    as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
+                    as<BatchCounters>(c->s_ctr));
+                c->launches += 1;
+                RRB_CUDA(c, cudaGetLastError());
+                if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+                std::memcpy(&hc, c->h_read, sizeof hc);
+                if (!(hc.err & ERR_SCRATCH_CAP)) break;
+                // Not enough scratch: grow to what was asked for and run again.
+                need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + 4 * n_edges, 0x7FFFFFFFull);
+                c->h_read[66] = hc.err & ~ERR_SCRATCH_CAP;
+                RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->err, &c->h_read[66], 4,
+                                            cudaMemcpyHostToDevice, c->stream));
+            }
         }
         stage_end(c, 10);
     }
@@ -544,6 +562,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     c->stats.aa_rows = hc.aa_rows;
     c->stats.spans = hc.cell_cursor;
     c->stats.row_overflows = hc.ovf_count;
+    c->stats.pieces = n_pieces;
     c->stats.tiles = tiles;
     c->stats.tile_pairs = n_pairs;
     c->stats.nonterminating_rows = hc.nonterminating;
@@ -635,7 +654,7 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
-                      &c->s_groups, &c->s_slots, &c->s_path_pieces};
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);

@@ -28,15 +28,17 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
-// f64::midpoint (Rust std): (a+b)/2 when both |a|,|b| <= f64::MAX/2.
+// f64::midpoint (Rust std): (a+b)/2 when both |a|,|b| <= f64::MAX/2. x/2
+// and x*0.5 are the same correctly rounded value of the same real number, so
+// the halving is a multiplication.
 __device__ __forceinline__ double midpoint(double a, double b) {
     const double HI = 8.98846567431157854e+307;   // f64::MAX / 2
     const double LO = 4.45014771701440277e-308;   // f64::MIN_POSITIVE * 2
     double aa = fabs(a), ab = fabs(b);
-    if (aa <= HI && ab <= HI) return ddiv(dadd(a, b), 2.0);
-    if (aa < LO) return dadd(a, ddiv(b, 2.0));
-    if (ab < LO) return dadd(ddiv(a, 2.0), b);
-    return dadd(ddiv(a, 2.0), ddiv(b, 2.0));
+    if (aa <= HI && ab <= HI) return dmul(dadd(a, b), 0.5);
+    if (aa < LO) return dadd(a, dmul(b, 0.5));
+    if (ab < LO) return dadd(dmul(a, 0.5), b);
+    return dadd(dmul(a, 0.5), dmul(b, 0.5));
 }
 
 // saturate_f64_to_i32 / splash_floor (crates/color/src/convert.rs:221-265).

@@ -49,7 +49,8 @@ struct BatchCounters {
     uint32_t ovf_count;
     uint32_t scratch_cursor;
     uint32_t nonterminating;
-    uint32_t pad[3];
+    uint32_t ovf2_count;
+    uint32_t pad[2];
     unsigned long long raw_entries;  // sum over edges of the rows they cover
     unsigned long long aa_rows;      // sum over paths of y1 - y0 + 1
 };
@@ -278,7 +279,8 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                             const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
                             const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
                             uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
-                            int chunk_rows, BatchCounters* __restrict__ ctr) {
+                            int chunk_rows, BatchCounters* __restrict__ ctr, int32_t* __restrict__ gmin,
+                            int32_t* __restrict__ gmax) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -286,16 +288,33 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
         uint32_t eb = edge_off[piece_off[p]], ee = edge_off[piece_off[p + 1]];
         int32_t y0 = INT32_MAX, y1 = INT32_MIN, xl = INT32_MAX, xh = INT32_MIN;
         unsigned long long raw = 0;
-        for (uint32_t j = eb + lane; j < ee; j += 32) {
-            Edge e = edges[j];
-            if (e.flags & EF_EMPTY) continue;
-            int32_t lo, hi;
-            edge_xrange(e, lo, hi);
-            raw += static_cast<unsigned long long>(e.row1 - e.row0 + 1);
-            y0 = min(y0, e.row0);
-            y1 = max(y1, e.row1);
-            xl = min(xl, lo);
-            xh = max(xh, hi);
+        // Aligned groups of 32 edges: one group per iteration, its row range
+        // merged into gmin/gmax (atomically: a group can straddle two paths).
+        for (uint32_t base = eb & ~31u; base < ee; base += 32) {
+            const uint32_t j = base + lane;
+            int32_t g0 = INT32_MAX, g1 = INT32_MIN;
+            if (j >= eb && j < ee) {
+                const Edge e = edges[j];
+                if (!(e.flags & EF_EMPTY)) {
+                    int32_t lo, hi;
+                    edge_xrange(e, lo, hi);
+                    raw += static_cast<unsigned long long>(e.row1 - e.row0 + 1);
+                    y0 = min(y0, e.row0);
+                    y1 = max(y1, e.row1);
+                    xl = min(xl, lo);
+                    xh = max(xh, hi);
+                    g0 = e.row0;
+                    g1 = e.row1;
+                }
+            }
+            for (int o = 16; o; o >>= 1) {
+                g0 = min(g0, __shfl_xor_sync(0xffffffffu, g0, o));
+                g1 = max(g1, __shfl_xor_sync(0xffffffffu, g1, o));
+            }
+            if (lane == 0 && g0 <= g1) {
+                atomicMin(&gmin[base >> 5], g0);
+                atomicMax(&gmax[base >> 5], g1);
+            }
         }
         for (int o = 16; o; o >>= 1) {
             y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
@@ -570,172 +589,176 @@ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bound, Put p
     return nc;
 }
 
-// Row range [min row0, max row1] of each aligned group of 32 edges (empty
-// edges excluded), so a chunk can skip whole groups with one load.
-__global__ void k_edge_groups(const Edge* __restrict__ edges, uint32_t n_edges, int2* __restrict__ groups) {
-    const uint32_t n_groups = (n_edges + 31) / 32;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
-        int32_t lo = INT32_MAX, hi = INT32_MIN;
-        const uint32_t e1 = min(n_edges, g * 32 + 32);
-        for (uint32_t j = g * 32; j < e1; ++j) {
-            const Edge e = edges[j];
-            if (e.flags & EF_EMPTY) continue;
-            lo = min(lo, e.row0);
-            hi = max(hi, e.row1);
+// Merged Intersect lists of up to 32 consecutive AA rows of one path, one
+// row per lane, in shared memory: entry k of lane l at [k * LS + l].
+//
+// The path's edges are visited in order, 32 at a time: a ballot finds those
+// overlapping [lo, hi], a 32x32 bit transpose gives each lane the edges that
+// cover its row, and each lane folds its entries in edge order, so every row
+// sees its entries in segment order and the write_intersect merge (merge only
+// with the last entry written to the row, scanner/mod.rs:600-642) is exact.
+// Groups of 32 edges whose row range misses [lo, hi] are skipped from the
+// per-group bounds gmin/gmax. Returns the entry count; entries past K are
+// counted but not stored (the caller treats n > K as overflow).
+template <int K, int LS>
+__device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t hi, int32_t r, bool valid,
+                                          const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
+                                          const int32_t* __restrict__ gmax, int32_t (*sedge)[32], int32_t* x0s,
+                                          int32_t* x1s, int32_t* cns, int lane) {
+    int n = 0;
+    bool has_last = false;
+    int32_t lx0 = 0, lx1 = 0, lc = 0;
+    for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
+        const uint32_t gi = eb >> 5;
+        if (gmin[gi] > hi || gmax[gi] < lo) continue;  // no edge of this group touches the rows
+        const uint32_t j = eb + lane;
+        Edge e;
+        bool hit = false;
+        if (j >= P.e_begin && j < P.e_end) {
+            e = edges[j];
+            hit = !(e.flags & EF_EMPTY) && e.row0 <= hi && e.row1 >= lo;
         }
-        groups[g] = make_int2(lo, hi);
+        if (!__any_sync(0xffffffffu, hit)) continue;
+        if (hit) {
+            sedge[0][lane] = e.row0;
+            sedge[1][lane] = e.row1;
+            sedge[2][lane] = e.flags;
+            sedge[3][lane] = e.a;
+            sedge[4][lane] = e.b;
+            sedge[5][lane] = e.dfp;
+            sedge[6][lane] = e.cmin;
+            sedge[7][lane] = e.cmax;
+        }
+        __syncwarp();
+        uint32_t rows_of_edge = 0;
+        if (hit) {
+            const int32_t ra = max(e.row0, lo) - lo, rb = min(e.row1, hi) - lo;
+            rows_of_edge = (0xffffffffu >> (31 - rb)) & (0xffffffffu << ra);
+        }
+        uint32_t mine = warp_transpose32(rows_of_edge, lane);
+        if (!valid) mine = 0;
+        while (mine) {
+            const int bb = __ffs(mine) - 1;
+            mine &= mine - 1;
+            Edge E;
+            E.row0 = sedge[0][bb];
+            E.row1 = sedge[1][bb];
+            E.flags = sedge[2][bb];
+            E.a = sedge[3][bb];
+            E.b = sedge[4][bb];
+            E.dfp = sedge[5][bb];
+            E.cmin = sedge[6][bb];
+            E.cmax = sedge[7][bb];
+            int32_t elo, ehi, ec;
+            edge_entry(E, r, elo, ehi, ec);
+            if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
+                lc = static_cast<int32_t>(static_cast<uint32_t>(lc) + static_cast<uint32_t>(ec));
+                lx0 = min(lx0, elo);
+                lx1 = max(lx1, ehi);
+            } else {
+                if (has_last) {
+                    if (n < K) {
+                        x0s[n * LS + lane] = lx0;
+                        x1s[n * LS + lane] = lx1;
+                        cns[n * LS + lane] = lc;
+                    }
+                    ++n;
+                }
+                lx0 = elo;
+                lx1 = ehi;
+                lc = ec;
+                has_last = true;
+            }
+        }
+        __syncwarp();
     }
+    if (has_last) {
+        if (n < K) {
+            x0s[n * LS + lane] = lx0;
+            x1s[n * LS + lane] = lx1;
+            cns[n * LS + lane] = lc;
+        }
+        ++n;
+    }
+    return n;
 }
 
+// sort_unstable_by_key(x0) on a lane's list (stable insertion sort, as Rust
+// std sorts slices of up to 20 elements) followed by the render_aa_line
+// winding walk; the row's union of spans replaces the list in place.
+template <int LS>
+__device__ __forceinline__ int sort_and_walk(int n, int32_t mask, int32_t aa_width, int32_t* x0s, int32_t* x1s,
+                                             int32_t* cns, int lane, uint32_t& nonterm) {
+    for (int a = 1; a < n; ++a) {
+        const int32_t t0 = x0s[a * LS + lane], t1 = x1s[a * LS + lane], tc = cns[a * LS + lane];
+        int b = a;
+        while (b > 0 && t0 < x0s[(b - 1) * LS + lane]) {
+            x0s[b * LS + lane] = x0s[(b - 1) * LS + lane];
+            x1s[b * LS + lane] = x1s[(b - 1) * LS + lane];
+            cns[b * LS + lane] = cns[(b - 1) * LS + lane];
+            --b;
+        }
+        x0s[b * LS + lane] = t0;
+        x1s[b * LS + lane] = t1;
+        cns[b * LS + lane] = tc;
+    }
+    return walk_row(
+        n, mask, aa_width,
+        [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
+            x0 = x0s[i * LS + lane];
+            x1 = x1s[i * LS + lane];
+            cc = cns[i * LS + lane];
+        },
+        [&](int k, int32_t s0, int32_t e0) {
+            x0s[k * LS + lane] = s0;
+            x1s[k * LS + lane] = e0;
+        },
+        nonterm);
+}
+
+// Row stage: one warp per chunk of 32 AA rows of one path, lane = row.
+// Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the four
+// sub-rows of one pixel row; their spans are merged into coverage cells by
+// lane 4k. Pixel rows with a list over KCAP go to k_groups_mid.
 template <int KCAP>
 __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
-    const Edge* __restrict__ edges, const int2* __restrict__ groups, const uint32_t* __restrict__ page_w,
-    uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells, uint32_t cell_cap,
-    uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr) {
-    __shared__ int32_t sx0[ROWS_WARPS][KCAP][32];
-    __shared__ int32_t sx1[ROWS_WARPS][KCAP][32];
-    __shared__ int32_t scn[ROWS_WARPS][KCAP][32];
-    // Edge records of the current batch, field-major so that lanes reading
-    // different edges hit different banks.
+    const Edge* __restrict__ edges, const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax,
+    const uint32_t* __restrict__ page_w, uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
+    uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr) {
+    __shared__ int32_t sx0[ROWS_WARPS][KCAP * 32];
+    __shared__ int32_t sx1[ROWS_WARPS][KCAP * 32];
+    __shared__ int32_t scn[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t sedge[ROWS_WARPS][8][32];
     __shared__ int32_t sns[ROWS_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
     for (uint32_t c = blockIdx.x * ROWS_WARPS + w; c < total_chunks; c += gridDim.x * ROWS_WARPS) {
-        // Path owning chunk c: last p with chunk_off[p] <= c.
-        uint32_t lo = 0, hi = n_paths;
+        uint32_t lo = 0, hi = n_paths;  // path owning chunk c: last p with chunk_off[p] <= c
         while (hi - lo > 1) {
-            uint32_t mid = (lo + hi) >> 1;
+            const uint32_t mid = (lo + hi) >> 1;
             if (chunk_off[mid] <= c) lo = mid;
             else hi = mid;
         }
         const uint32_t p = lo;
         const PathInfo P = info[p];
-        // Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the
-        // four sub-rows of one pixel row.
         const int32_t chunk_lo = (P.y0 & ~3) + static_cast<int32_t>(c - chunk_off[p]) * 32;
         const int32_t chunk_hi = min(chunk_lo + 31, P.y1);
         const int32_t r = chunk_lo + lane;
         const bool valid = r >= P.y0 && r <= chunk_hi;
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
-        int n = 0;
-        bool has_last = false;
-        int32_t lx0 = 0, lx1 = 0, lc = 0;
-        for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
-            const int2 grp = groups[eb >> 5];
-            if (grp.x > chunk_hi || grp.y < chunk_lo) continue;  // no edge of this group touches the chunk
-            const uint32_t j = eb + lane;
-            Edge e;
-            bool hit = false;
-            if (j >= P.e_begin && j < P.e_end) {
-                e = edges[j];
-                hit = !(e.flags & EF_EMPTY) && e.row0 <= chunk_hi && e.row1 >= chunk_lo;
-            }
-            if (!__any_sync(0xffffffffu, hit)) continue;
-            if (hit) {
-                sedge[w][0][lane] = e.row0;
-                sedge[w][1][lane] = e.row1;
-                sedge[w][2][lane] = e.flags;
-                sedge[w][3][lane] = e.a;
-                sedge[w][4][lane] = e.b;
-                sedge[w][5][lane] = e.dfp;
-                sedge[w][6][lane] = e.cmin;
-                sedge[w][7][lane] = e.cmax;
-            }
-            __syncwarp();
-            // Lane j holds the chunk rows edge j covers; transposing the 32x32
-            // bit matrix gives lane r the edges covering row r, in edge order.
-            uint32_t rows_of_edge = 0;
-            if (hit) {
-                const int32_t a = max(e.row0, chunk_lo) - chunk_lo, b = min(e.row1, chunk_hi) - chunk_lo;
-                rows_of_edge = (0xffffffffu >> (31 - b)) & (0xffffffffu << a);
-            }
-            const uint32_t mine_all = warp_transpose32(rows_of_edge, lane);
-            uint32_t mine = valid ? mine_all : 0u;
-            while (mine) {
-                const int b = __ffs(mine) - 1;
-                mine &= mine - 1;
-                Edge E;
-                E.row0 = sedge[w][0][b];
-                E.row1 = sedge[w][1][b];
-                E.flags = sedge[w][2][b];
-                E.a = sedge[w][3][b];
-                E.b = sedge[w][4][b];
-                E.dfp = sedge[w][5][b];
-                E.cmin = sedge[w][6][b];
-                E.cmax = sedge[w][7][b];
-                {
-                    int32_t elo, ehi, ec;
-                    edge_entry(E, r, elo, ehi, ec);
-                    if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
-                        lc = static_cast<int32_t>(static_cast<uint32_t>(lc) + static_cast<uint32_t>(ec));
-                        lx0 = min(lx0, elo);
-                        lx1 = max(lx1, ehi);
-                    } else {
-                        if (has_last) {
-                            if (n < KCAP) {
-                                sx0[w][n][lane] = lx0;
-                                sx1[w][n][lane] = lx1;
-                                scn[w][n][lane] = lc;
-                            }
-                            ++n;
-                        }
-                        lx0 = elo;
-                        lx1 = ehi;
-                        lc = ec;
-                        has_last = true;
-                    }
-                }
-            }
-            __syncwarp();
-        }
-        if (has_last) {
-            if (n < KCAP) {
-                sx0[w][n][lane] = lx0;
-                sx1[w][n][lane] = lx1;
-                scn[w][n][lane] = lc;
-            }
-            ++n;
-        }
+        const int n = gather_row<KCAP, 32>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
+                                           sx1[w], scn[w], lane);
         const bool overflow = valid && n > KCAP;
         int ns = 0;
-        if (valid && !overflow) {
-            // sort_unstable_by_key(x0) on <= KCAP (<= 20 in practice) entries:
-            // stable insertion sort, as Rust std sorts short slices.
-            for (int a = 1; a < n; ++a) {
-                int32_t t0 = sx0[w][a][lane], t1 = sx1[w][a][lane], tc = scn[w][a][lane];
-                int b = a;
-                while (b > 0 && t0 < sx0[w][b - 1][lane]) {
-                    sx0[w][b][lane] = sx0[w][b - 1][lane];
-                    sx1[w][b][lane] = sx1[w][b - 1][lane];
-                    scn[w][b][lane] = scn[w][b - 1][lane];
-                    --b;
-                }
-                sx0[w][b][lane] = t0;
-                sx1[w][b][lane] = t1;
-                scn[w][b][lane] = tc;
-            }
-            ns = walk_row(
-                n, mask, aa_width,
-                [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
-                    x0 = sx0[w][i][lane];
-                    x1 = sx1[w][i][lane];
-                    cc = scn[w][i][lane];
-                },
-                [&](int k, int32_t s, int32_t e) {
-                    sx0[w][k][lane] = s;
-                    sx1[w][k][lane] = e;
-                },
-                nonterm);
-        }
+        if (valid && !overflow) ns = sort_and_walk<32>(n, mask, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
         // ---- one pixel row per 4 lanes: merge the sub-rows' spans into cells
         sns[w][lane] = (valid && !overflow) ? ns : 0;
         const uint32_t ovf_lanes = __ballot_sync(0xffffffffu, overflow);
         __syncwarp();
-        const bool leader = (lane & 3) == 0 && r <= P.y1;  // group has a row in [y0, y1]
+        const bool leader = (lane & 3) == 0 && r <= P.y1;  // this pixel row has an AA row in [y0, y1]
         const bool g_ovf = ((ovf_lanes >> (lane & ~3)) & 0xFu) != 0;
         int n4[4] = {0, 0, 0, 0};
         uint32_t need = 0;
@@ -746,7 +769,7 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
         }
         uint32_t incl = need;
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
@@ -767,7 +790,9 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
                 const uint32_t o0 = base + incl - need;
                 const int nc = sweep_cells(
                     n4,
-                    [&](int k, int i, bool end) { return end ? sx1[w][i][lane + k] : sx0[w][i][lane + k]; },
+                    [&](int k, int i, bool end) {
+                        return end ? sx1[w][i * 32 + lane + k] : sx0[w][i * 32 + lane + k];
+                    },
                     [&](int q, uint32_t cell) { cells[o0 + q] = cell; });
                 group_idx[gi] = make_uint2(o0, static_cast<uint32_t>(nc));
             } else {
@@ -779,7 +804,72 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
 }
 
-// Pixel rows with a sub-row whose merged list exceeded KCAP: one thread per
+// Pixel rows whose sub-row lists overflowed KCAP: one warp per pixel row
+// (lanes 0-3 = its AA rows) with MID_K entries per row in shared memory.
+// Rows longer than that go to k_groups_slow through ovf2.
+constexpr int MID_K = 128;
+constexpr int MID_WARPS = 4;
+
+__global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
+    const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off, const Edge* __restrict__ edges,
+    const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax, const uint32_t* __restrict__ page_w,
+    const uint2* __restrict__ ovf, uint32_t ovf_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
+    uint32_t cell_cap, uint2* __restrict__ ovf2, BatchCounters* __restrict__ ctr) {
+    __shared__ int32_t sx0[MID_WARPS][MID_K * 4];
+    __shared__ int32_t sx1[MID_WARPS][MID_K * 4];
+    __shared__ int32_t scn[MID_WARPS][MID_K * 4];
+    __shared__ int32_t sedge[MID_WARPS][8][32];
+    __shared__ int32_t sns[MID_WARPS][4];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);
+    uint32_t nonterm = 0;
+    for (uint32_t k = blockIdx.x * MID_WARPS + w; k < n_ovf; k += gridDim.x * MID_WARPS) {
+        const uint32_t p = ovf[k].x;
+        const int32_t g = static_cast<int32_t>(ovf[k].y);
+        const PathInfo P = info[p];
+        const int32_t lo = 4 * g, hi = min(4 * g + 3, P.y1);
+        const int32_t r = lo + lane;
+        const bool valid = lane < 4 && r >= P.y0 && r <= hi;
+        const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
+        const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        const int n = gather_row<MID_K, 4>(P, lo, hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w], sx1[w], scn[w],
+                                           lane);
+        const bool overflow = valid && n > MID_K;
+        int ns = 0;
+        if (valid && !overflow) ns = sort_and_walk<4>(n, mask, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
+        if (lane < 4) sns[w][lane] = (valid && !overflow) ? ns : 0;
+        const bool any_ovf = __any_sync(0xffffffffu, overflow);
+        __syncwarp();
+        if (lane == 0) {
+            const uint32_t gi = group_off[p] + static_cast<uint32_t>(g - (P.y0 >> 2));
+            if (any_ovf) {
+                const uint32_t k2 = atomicAdd(&ctr->ovf2_count, 1u);
+                if (k2 < ovf_cap) ovf2[k2] = make_uint2(p, static_cast<uint32_t>(g));
+                else atomicOr(&ctr->err, ERR_OVF_CAP);
+                group_idx[gi] = make_uint2(0u, 0u);
+            } else {
+                int n4[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) n4[q] = sns[w][q];
+                const uint32_t need = 4u * static_cast<uint32_t>(n4[0] + n4[1] + n4[2] + n4[3]);
+                const uint32_t o0 = need ? atomicAdd(&ctr->cell_cursor, need) : 0u;
+                if (static_cast<uint64_t>(o0) + need > cell_cap) {
+                    atomicOr(&ctr->err, ERR_SPAN_CAP);
+                    group_idx[gi] = make_uint2(0u, 0u);
+                } else {
+                    const int nc = sweep_cells(
+                        n4, [&](int q, int i, bool end) { return end ? sx1[w][i * 4 + q] : sx0[w][i * 4 + q]; },
+                        [&](int q, uint32_t cell) { cells[o0 + q] = cell; });
+                    group_idx[gi] = make_uint2(o0, static_cast<uint32_t>(nc));
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
+}
+
+// Pixel rows with a sub-row whose merged list exceeded MID_K: one thread per
 // pixel row, the four sub-row lists in a global scratch slice of 4 x the
 // path's edge count.
 __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off,
@@ -787,7 +877,7 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
                               const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
                               uint32_t scratch_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
                               uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
-    const uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);
+    const uint32_t n_ovf = min(ctr->ovf2_count, ovf_cap);
     uint32_t nonterm = 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_ovf; k += gridDim.x * blockDim.x) {
         const uint32_t p = ovf[k].x;
@@ -921,7 +1011,7 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap
         for (int q = 0; q < L::PX; ++q) cov[q] = 0;
         for (uint32_t bt = 0; bt < nb; ++bt) {
 #pragma unroll
-            for (int q = 0; q < L::PX; ++q) mark[w * L::RPW + slot][col + q] = -1;
+            for (int q = 0; q < L::PX; ++q) mark[w * L::RPW + slot][q * L::LPR + sub] = -1;
             __syncwarp();
             const uint32_t j = bt * L::LPR + sub;
             uint32_t cell = 0;
@@ -930,14 +1020,18 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap
                 const int32_t x0 = static_cast<int32_t>(cell & 0x3fffu);
                 const int32_t x1 = x0 + static_cast<int32_t>((cell >> 14) & 0x3fffu) + 1;
                 const int32_t sx = max(x0, X0);
-                if (sx < min(x1, X0 + TW)) mark[w * L::RPW + slot][sx - X0] = sub;
+                if (sx < min(x1, X0 + TW)) {
+                    // Pixel p = lane * PX + q of the row lives at [q * LPR + lane] (no bank conflicts).
+                    const int32_t pp = sx - X0;
+                    mark[w * L::RPW + slot][(pp % L::PX) * L::LPR + pp / L::PX] = sub;
+                }
             }
             __syncwarp();
             int32_t v[L::PX];
             int32_t run = -1;
 #pragma unroll
             for (int q = 0; q < L::PX; ++q) {
-                run = max(run, mark[w * L::RPW + slot][col + q]);
+                run = max(run, mark[w * L::RPW + slot][q * L::LPR + sub]);
                 v[q] = run;
             }
             // Exclusive prefix max of `run` over the lanes before this one in the row.
