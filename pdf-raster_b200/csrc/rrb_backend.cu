@@ -380,7 +380,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
     RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
     stage(c, 0);
-    k_walk<<<grid_for(c, n_paths, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
+    k_walk<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
                                                              as<uint64_t>(B->off), NP, as<double>(B->mtx),
                                                              as<uint32_t>(B->page), as<uint32_t>(B->ph),
                                                              as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces));
@@ -393,14 +393,14 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_pieces, std::max<uint64_t>(1, n_pieces) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_clip, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_edge_off, (n_pieces + 1) * sizeof(uint32_t)))) return rc;
-    k_compact_pieces<<<grid_for(c, n_paths, 128), 128, 0, c->stream>>>(
+    k_compact_pieces<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(
         as<uint64_t>(B->off), as<uint32_t>(c->s_path_pieces), NP, as<uint32_t>(B->page), as<uint32_t>(B->ph),
         as<uint2>(c->s_slots), as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip));
     c->launches += 1;
     stage_end(c, 0);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 1);
-    k_seg_count<<<grid_for(c, n_pieces, 128), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NPC,
+    k_seg_count<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NPC,
                                                                    as<double>(B->mtx), flat_sq,
                                                                    as<uint32_t>(c->s_edge_off));
     c->launches += 1;
@@ -425,7 +425,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     RRB_CUDA(c, cudaMemsetAsync(gmin, 0x7f, n_egroups * sizeof(int32_t), c->stream));
     RRB_CUDA(c, cudaMemsetAsync(gmax, 0x80, n_egroups * sizeof(int32_t), c->stream));
     stage(c, 3);
-    k_seg_write<<<grid_for(c, n_pieces, 128), 128, 0, c->stream>>>(
+    k_seg_write<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
         static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip));
     c->launches += 1;

@@ -979,31 +979,58 @@ struct CompLayout {
     static constexpr int NW = COMP_THREADS / 32;
 };
 
-// One path over the rows of this thread's tile slots: fetch the pixel row's
-// coverage cells (group g = y, or 4y+3 under the as-shipped row map), find
-// each pixel's cell (start marks in shared memory + a prefix max across the
-// row's lanes), then AA_GAMMA and the div255 source-over of
-// render_span_aa_inner's no-alpha arm (pipe/aa.rs:192-208).
+// Loads of one hit for this thread's tile rows: the pixel row's entry in the
+// group index (g = y, or 4y+3 under the as-shipped row map) and this lane's
+// first cell. k_composite issues them two and one hits ahead of use.
 template <int TW, int TH>
-__device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap, int X0, int Y0, int H,
-                                                    const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
-                                                    const uint8_t* gamma, int32_t (*mark)[TW],
-                                                    uint32_t (&pix)[TH * TW / COMP_THREADS]) {
+struct HitRows {
+    static constexpr int ITERS = TH / (CompLayout<TW>::NW * CompLayout<TW>::RPW);
+    uint2 ix[ITERS];
+    uint32_t cell0[ITERS];
+};
+
+template <int TW, int TH>
+__device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
+                                               const uint2* __restrict__ gidx, HitRows<TW, TH>& hr) {
     using L = CompLayout<TW>;
-    constexpr int ITERS = TH / (L::NW * L::RPW);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int sub = lane % L::LPR;            // lane within its pixel row
-    const int slot = lane / L::LPR;           // pixel row of this warp step
+    const int slot = lane / L::LPR;
+#pragma unroll
+    for (int it = 0; it < HitRows<TW, TH>::ITERS; ++it) {
+        const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
+        const int32_t grp = rowmap ? 4 * y + 3 : y;
+        const bool rowok = y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
+        hr.ix[it] = rowok ? gidx[h.goff + static_cast<uint32_t>(grp - h.g0)] : make_uint2(0u, 0u);
+    }
+}
+
+template <int TW, int TH>
+__device__ __forceinline__ void load_hit_cells(const uint32_t* __restrict__ cells, HitRows<TW, TH>& hr) {
+    using L = CompLayout<TW>;
+    const int sub = (threadIdx.x & 31) % L::LPR;
+#pragma unroll
+    for (int it = 0; it < HitRows<TW, TH>::ITERS; ++it)
+        hr.cell0[it] = static_cast<uint32_t>(sub) < hr.ix[it].y ? cells[hr.ix[it].x + sub] : 0u;
+}
+
+// One path over the rows of this thread's tile slots: find each pixel's
+// coverage cell (start marks in shared memory + a prefix max across the row's
+// lanes), then AA_GAMMA and the div255 source-over of render_span_aa_inner's
+// no-alpha arm (pipe/aa.rs:192-208).
+template <int TW, int TH>
+__device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitRows<TW, TH>& hr, int X0,
+                                                    const uint32_t* __restrict__ cells, const uint8_t* gamma,
+                                                    int32_t (*mark)[TW], uint32_t (&pix)[TH * TW / COMP_THREADS]) {
+    using L = CompLayout<TW>;
+    constexpr int ITERS = HitRows<TW, TH>::ITERS;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane % L::LPR;
+    const int slot = lane / L::LPR;
     const int col = sub * L::PX;
     const uint32_t g = h.paint & 0xff, alpha = (h.paint >> 8) & 0xff;
 #pragma unroll
     for (int it = 0; it < ITERS; ++it) {
-        const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
-        const int32_t grp = rowmap ? 4 * y + 3 : y;
-        const bool rowok = y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
-        uint2 ix = make_uint2(0u, 0u);
-        if (rowok) ix = gidx[h.goff + static_cast<uint32_t>(grp - h.g0)];
-        // Cells of this row overlapping the tile are processed LPR at a time.
+        const uint2 ix = hr.ix[it];
         uint32_t nb = (ix.y + L::LPR - 1) / L::LPR;
         for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
         int32_t cov[L::PX];
@@ -1016,7 +1043,7 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, int rowmap
             const uint32_t j = bt * L::LPR + sub;
             uint32_t cell = 0;
             if (j < ix.y) {
-                cell = cells[ix.x + j];
+                cell = bt == 0 ? hr.cell0[it] : cells[ix.x + j];
                 const int32_t x0 = static_cast<int32_t>(cell & 0x3fffu);
                 const int32_t x1 = x0 + static_cast<int32_t>((cell >> 14) & 0x3fffu) + 1;
                 const int32_t sx = max(x0, X0);
@@ -1133,9 +1160,20 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
                 hits[pos] = hi;
             }
             __syncthreads();
+            // Software pipeline over the hits: the index entries of hit k+2 and
+            // the first cells of hit k+1 are in flight while hit k is blended.
+            HitRows<TW, TH> cur, nxt, nxt2;
+            if (total > 0) {
+                load_hit_index<TW, TH>(hits[0], rowmap, Y0, H, gidx, cur);
+                load_hit_cells<TW, TH>(cells, cur);
+            }
+            if (total > 1) load_hit_index<TW, TH>(hits[1], rowmap, Y0, H, gidx, nxt);
             for (uint32_t k = 0; k < total; ++k) {
-                const HitInfo h = hits[k];
-                composite_path_rows<TW, TH>(h, rowmap, X0, Y0, H, gidx, cells, gamma, mark, pix);
+                if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, nxt2);
+                if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
+                composite_path_rows<TW, TH>(hits[k], cur, X0, cells, gamma, mark, pix);
+                cur = nxt;
+                nxt = nxt2;
             }
             __syncthreads();
         }
