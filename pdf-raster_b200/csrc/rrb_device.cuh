@@ -225,10 +225,32 @@ __device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo, int32_t&
 // pp3 = (pp1+pp2)/2; emitting pops. Interval lengths halve per push, so at
 // most log2(1024) = 10 halves are pending. Same operations in the same
 // order as the reference, hence the same points.
+// (a+b)/2 for operands known to be within +-f64::MAX/2 (midpoint's first branch).
+__device__ __forceinline__ double midpoint_in_range(double a, double b) { return dmul(dadd(a, b), 0.5); }
+
+template <bool IN_RANGE, typename Emit>
+__device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                  double p2y, double p3x, double p3y, double flat_sq, Emit& emit);
+
+// Every point the subdivision computes is a midpoint of two earlier points,
+// i.e. a convex combination of the four control points, so when all control
+// coordinates lie within +-f64::MAX/2 every midpoint call takes the (a+b)/2
+// branch: the check is made once per curve and the loop runs branch-free.
 template <typename Emit>
 __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x, double p1y, double p2x,
                                              double p2y, double p3x, double p3y, double flat_sq,
                                              Emit emit) {
+    const double HI = 8.98846567431157854e+307;
+    const double m = fmax(fmax(fmax(fabs(p0x), fabs(p0y)), fmax(fabs(p1x), fabs(p1y))),
+                          fmax(fmax(fabs(p2x), fabs(p2y)), fmax(fabs(p3x), fabs(p3y))));
+    if (m <= HI) return flatten_curve_impl<true>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, flat_sq, emit);
+    return flatten_curve_impl<false>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, flat_sq, emit);
+}
+
+template <bool IN_RANGE, typename Emit>
+__device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                  double p2y, double p3x, double p3y, double flat_sq, Emit& emit) {
+    auto mid = [](double a, double b) { return IN_RANGE ? midpoint_in_range(a, b) : midpoint(a, b); };
     double sx[FLATTEN_STACK][6];
     int sidx[FLATTEN_STACK];
     int top = 0;
@@ -247,7 +269,7 @@ __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x,
             xr3 = p3x;
             yr3 = p3y;
         }
-        double mx = midpoint(c0x, xr3), my = midpoint(c0y, yr3);
+        double mx = mid(c0x, xr3), my = mid(c0y, yr3);
         double dx1 = dsub(c1x, mx), dy1 = dsub(c1y, my);
         double dx2 = dsub(c2x, mx), dy2 = dsub(c2y, my);
         double d1 = dfma(dx1, dx1, dmul(dy1, dy1));
@@ -266,12 +288,12 @@ __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x,
                 c2y = sx[top][5];
             }
         } else {
-            double xl1 = midpoint(c0x, c1x), yl1 = midpoint(c0y, c1y);
-            double xh = midpoint(c1x, c2x), yh = midpoint(c1y, c2y);
-            double xl2 = midpoint(xl1, xh), yl2 = midpoint(yl1, yh);
-            double xr2 = midpoint(c2x, xr3), yr2 = midpoint(c2y, yr3);
-            double xr1 = midpoint(xh, xr2), yr1 = midpoint(yh, yr2);
-            double xr0 = midpoint(xl2, xr1), yr0 = midpoint(yl2, yr1);
+            double xl1 = mid(c0x, c1x), yl1 = mid(c0y, c1y);
+            double xh = mid(c1x, c2x), yh = mid(c1y, c2y);
+            double xl2 = mid(xl1, xh), yl2 = mid(yl1, yh);
+            double xr2 = mid(c2x, xr3), yr2 = mid(c2y, yr3);
+            double xr1 = mid(xh, xr2), yr1 = mid(yh, yr2);
+            double xr0 = mid(xl2, xr1), yr0 = mid(yl2, yr1);
             int pp3 = (pp1 + pp2) >> 1;
             // pp2 - pp1 >= 2 here, so fewer than FLATTEN_STACK halves are pending.
             sx[top][0] = xr0;

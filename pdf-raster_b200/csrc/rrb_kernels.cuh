@@ -290,11 +290,22 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
         unsigned long long raw = 0;
         // Aligned groups of 32 edges: one group per iteration, its row range
         // merged into gmin/gmax (atomically: a group can straddle two paths).
-        for (uint32_t base = eb & ~31u; base < ee; base += 32) {
-            const uint32_t j = base + lane;
+        for (uint32_t base4 = eb & ~31u; base4 < ee; base4 += 128) {
+          // Four groups' loads in flight before any is reduced.
+          Edge e4[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+              const uint32_t j = base4 + 32 * u + lane;
+              if (j >= eb && j < ee) e4[u] = edges[j];
+              else e4[u].flags = EF_EMPTY;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const uint32_t base = base4 + 32 * u;
+            if (base >= ee) break;
             int32_t g0 = INT32_MAX, g1 = INT32_MIN;
-            if (j >= eb && j < ee) {
-                const Edge e = edges[j];
+            {
+                const Edge e = e4[u];
                 if (!(e.flags & EF_EMPTY)) {
                     int32_t lo, hi;
                     edge_xrange(e, lo, hi);
@@ -315,6 +326,7 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                 atomicMin(&gmin[base >> 5], g0);
                 atomicMax(&gmax[base >> 5], g1);
             }
+          }
         }
         for (int o = 16; o; o >>= 1) {
             y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
