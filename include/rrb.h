@@ -198,7 +198,8 @@ int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, ch
 typedef struct {
     uint32_t tile_w, tile_h;
     uint32_t rows_per_chunk;    /* AA rows per row-kernel work item: 32 */
-    uint32_t reserved[5];
+    uint32_t wave_points;       /* path points per wave of pages (0 = default, 40 Mi) */
+    uint32_t reserved[4];
 } rrb_tuning;
 int rrb_set_tuning(rrb_ctx* ctx, const rrb_tuning* t);
 int rrb_get_tuning(rrb_ctx* ctx, rrb_tuning* t);

@@ -63,9 +63,11 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
+    Scratch s_run_off, s_runs;
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
+    struct rrb_batch* wave_batch = nullptr; // view of a group of pages of a larger batch
     struct StageTimer* timer = nullptr;
     float stage_ms[16] = {};
     uint32_t stage_launches[16] = {};
@@ -175,12 +177,12 @@ bool valid_tile(uint32_t w, uint32_t h) {
 
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
                      uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
-                     const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, uint8_t* arena,
-                     int rowmap, const BatchCounters* ctr) {
+                     const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, const int4* runs,
+                     uint8_t* arena, int rowmap, const BatchCounters* ctr) {
 #define RRB_COMP(TW, TH)                                                                                 \
     k_composite<TW, TH><<<grid, COMP_THREADS, 0, c->stream>>>(info, geom, n_pages, n_tiles, SUPER, SUPER, \
                                                               super_off, super_list, row_off, row_idx,    \
-                                                              spans, arena, rowmap, ctr)
+                                                              spans, runs, arena, rowmap, ctr)
     if (tw == 64 && th == 16) RRB_COMP(64, 16);
     else if (tw == 32 && th == 32) RRB_COMP(32, 32);
     else RRB_COMP(16, 16);
@@ -272,6 +274,8 @@ void set_tiles(std::vector<PageGeom>& geom, uint32_t tw, uint32_t th, uint64_t& 
 struct rrb_batch {
     Scratch pts, flags, off, rule, gray, alpha, page, geom, pw, ph, mtx;
     std::vector<PageGeom> geom_h;
+    std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
+    bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
     uint64_t supers = 0, arena_need = 0;
     uint64_t n_paths = 0, n_pts = 0;
     uint32_t n_pages = 0;
@@ -319,6 +323,11 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
                       &B->mtx};
     for (Scratch* s : all) {
+        if (B->view && s != &B->off && s != &B->page && s != &B->geom) {
+            s->p = nullptr;
+            s->cap = 0;
+            continue;
+        }
         dev_free(c, s->p, s->cap);
         s->p = nullptr;
         s->cap = 0;
@@ -338,6 +347,9 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
     B->arena_need = 0;
     for (const PageGeom& G : B->geom_h)
         B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(G.w) * G.h);
+    B->page_pt.assign(B->n_pages + 1, 0);
+    for (uint32_t pg = 0; pg < B->n_pages; ++pg) B->page_pt[pg] = h->path_pt_off[B->geom_h[pg].path_begin];
+    B->page_pt[B->n_pages] = h->n_paths ? h->path_pt_off[h->n_paths] : 0;
     if (B->n_paths == 0) return RRB_OK;
     int rc;
     if ((rc = upload(c, B->pts, h->pts, 2 * h->n_pts))) return rc;
@@ -355,7 +367,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
 }
 
 // The pipeline over a device-resident batch into the device page arena.
-int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
+int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     c->launches = 0;
     std::memset(&c->stats, 0, sizeof c->stats);
     if (B->n_paths == 0) return RRB_OK;
@@ -454,6 +466,14 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 7);
     if ((rc = scan_u32(c, as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_cnt), NSUP))) return rc;
+    // Rectilinear paths: runs per path, then their offsets.
+    if ((rc = ensure(c, c->s_run_off, (n_paths + 1) * sizeof(uint32_t)))) return rc;
+    k_recti<false><<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
+        as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, as<uint32_t>(c->s_run_off),
+        nullptr, nullptr, nullptr, 0, as<BatchCounters>(c->s_ctr));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NP))) return rc;
     stage_end(c, 7);
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 0, as<uint32_t>(c->s_rows) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 1, as<uint32_t>(c->s_chunks) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -461,8 +481,11 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
                                 c->stream));
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 4, &as<BatchCounters>(c->s_ctr)->raw_entries, 8, cudaMemcpyDeviceToHost,
                                 c->stream));
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 6, as<uint32_t>(c->s_run_off) + NP, 4, cudaMemcpyDeviceToHost,
+                                c->stream));
     RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     const uint64_t n_groups = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
+    const uint64_t n_runs = c->h_read[6];
     uint64_t raw_entries;
     std::memcpy(&raw_entries, c->h_read + 4, 8);
     // ---- stage 3: rows -> coverage cells. An AA row with m merged entries
@@ -476,6 +499,7 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = ensure(c, c->s_spans, cell_cap * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_ovf, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_runs, std::max<uint64_t>(1, n_runs) * sizeof(int4)))) return rc;
     stage(c, 8);
     k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
         as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, nullptr,
@@ -489,6 +513,13 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
             gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
             static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
+            as<BatchCounters>(c->s_ctr));
+        c->launches += 1;
+    }
+    if (n_runs) {
+        k_recti<true><<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
+            as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, nullptr,
+            as<uint32_t>(c->s_run_off), as<int4>(c->s_runs), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
             as<BatchCounters>(c->s_ctr));
         c->launches += 1;
     }
@@ -550,8 +581,8 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 8),
                                as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
-                               as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), arena, rowmap,
-                               as<BatchCounters>(c->s_ctr))))
+                               as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
+                               rowmap, as<BatchCounters>(c->s_ctr))))
         return rc;
     stage_end(c, 11);
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
@@ -581,6 +612,137 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         std::snprintf(buf, sizeof buf, "batch capacity exceeded (error bits 0x%x); pages left untouched", hc.err);
         return set_err(c, RRB_ERR_POOL_EXHAUSTED, buf);
     }
+    return RRB_OK;
+}
+
+// Binning geometry (supertiles, (supertile x path block) work items) of pages
+// whose path ranges are already set.
+void set_binning(std::vector<PageGeom>& geom, uint64_t& supers_out) {
+    uint64_t supers = 0, work = 0;
+    for (PageGeom& G : geom) {
+        G.nsx = (G.w + SUPER - 1) / SUPER;
+        G.super_base = static_cast<uint32_t>(supers);
+        supers += static_cast<uint64_t>(G.nsx) * ((G.h + SUPER - 1) / SUPER);
+        G.nblk = std::max<uint32_t>(1, (G.path_end - G.path_begin + BIN_BLOCK - 1) / BIN_BLOCK);
+        G.work_base = static_cast<uint32_t>(work);
+        work += static_cast<uint64_t>(G.nsx) * ((G.h + SUPER - 1) / SUPER) * G.nblk;
+    }
+    supers_out = work;
+}
+
+void release_scratch(rrb_ctx* c) {
+    cudaStreamSynchronize(c->stream);
+    Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
+                      &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
+    for (Scratch* x : all) {
+        dev_free(c, x->p, x->cap);
+        x->p = nullptr;
+        x->cap = 0;
+    }
+}
+
+// Pages [pg0, pg1) of B as a batch of their own: the inputs are views into
+// B's device arrays; only the per-path offsets and page indices are rebased.
+int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W) {
+    W->view = true;  // off / page / geom are owned (and reused across waves), the rest are views
+    const uint32_t pb = B->geom_h[pg0].path_begin, pe = B->geom_h[pg1 - 1].path_end;
+    const uint64_t ptb = B->page_pt[pg0], pte = B->page_pt[pg1];
+    W->n_paths = pe - pb;
+    W->n_pts = pte - ptb;
+    W->n_pages = pg1 - pg0;
+    W->flat_sq = B->flat_sq;
+    W->rowmap = B->rowmap;
+    W->arena_need = B->arena_need;
+    auto view = [](Scratch& dst, const Scratch& src, size_t byte_off) {
+        dst.p = static_cast<char*>(src.p) + byte_off;
+        dst.cap = 0;
+    };
+    view(W->pts, B->pts, 2 * ptb * sizeof(double));
+    view(W->flags, B->flags, ptb);
+    view(W->rule, B->rule, pb);
+    view(W->gray, B->gray, pb);
+    view(W->alpha, B->alpha, pb);
+    view(W->pw, B->pw, pg0 * sizeof(uint32_t));
+    view(W->ph, B->ph, pg0 * sizeof(uint32_t));
+    view(W->mtx, B->mtx, 0);
+    int rc;
+    if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
+    if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, W->geom, W->n_pages * sizeof(PageGeom)))) return rc;
+    k_rebase_paths<<<grid_for(c, W->n_paths + 1, 256), 256, 0, c->stream>>>(
+        as<uint64_t>(B->off) + pb, as<uint64_t>(W->off), ptb, as<uint32_t>(B->page) + pb, as<uint32_t>(W->page), pg0,
+        static_cast<uint32_t>(W->n_paths));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    W->geom_h.assign(B->geom_h.begin() + pg0, B->geom_h.begin() + pg1);
+    for (PageGeom& G : W->geom_h) {
+        G.path_begin -= pb;
+        G.path_end -= pb;
+    }
+    set_binning(W->geom_h, W->supers);
+    W->page_pt.clear();
+    return RRB_OK;
+}
+
+// Points per wave: a page is never split, consecutive pages are grouped up
+// to this many path points; a wave that runs out of device memory is split
+// in half and retried.
+constexpr uint64_t kWavePoints = 40ull << 20;
+
+int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* arena, size_t arena_len, int rowmap,
+              rrb_batch_stats& acc, int depth) {
+    int rc;
+    if (pg0 == 0 && pg1 == B->n_pages) {
+        rc = run_resident_one(c, B, arena, arena_len, rowmap);
+    } else {
+        rc = make_wave(c, B, pg0, pg1, c->wave_batch);
+        if (!rc) rc = run_resident_one(c, c->wave_batch, arena, arena_len, rowmap);
+    }
+    if (rc == RRB_OK) {
+        const rrb_batch_stats& s = c->stats;
+        acc.paths += s.paths;
+        acc.pieces += s.pieces;
+        acc.segments += s.segments;
+        acc.aa_rows += s.aa_rows;
+        acc.spans += s.spans;
+        acc.row_overflows += s.row_overflows;
+        acc.tiles += s.tiles;
+        acc.tile_pairs += s.tile_pairs;
+        acc.nonterminating_rows += s.nonterminating_rows;
+        acc.kernel_launches += s.kernel_launches;
+        return RRB_OK;
+    }
+    const bool splittable = (rc == RRB_ERR_OUT_OF_MEMORY || rc == RRB_ERR_POOL_EXHAUSTED) && pg1 - pg0 > 1 && depth < 20;
+    if (!splittable) return rc;
+    // The composite had not run, so the pages are untouched: free the scratch and split.
+    cudaGetLastError();
+    release_scratch(c);
+    const uint32_t mid = pg0 + (pg1 - pg0) / 2;
+    if ((rc = run_pages(c, B, pg0, mid, arena, arena_len, rowmap, acc, depth + 1))) return rc;
+    return run_pages(c, B, mid, pg1, arena, arena_len, rowmap, acc, depth + 1);
+}
+
+int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
+    rrb_batch_stats acc{};
+    const uint64_t wave_pts = c->tuning.wave_points ? c->tuning.wave_points : kWavePoints;
+    if (B->n_paths == 0 || B->n_pts <= wave_pts) {
+        int rc = run_pages(c, B, 0, B->n_pages, arena, arena_len, rowmap, acc, 0);
+        c->stats = acc;
+        return rc;
+    }
+    uint32_t pg = 0;
+    while (pg < B->n_pages) {
+        uint32_t end = pg + 1;
+        while (end < B->n_pages && B->page_pt[end + 1] - B->page_pt[pg] <= wave_pts) ++end;
+        int rc = run_pages(c, B, pg, end, arena, arena_len, rowmap, acc, 0);
+        if (rc) {
+            c->stats = acc;
+            return rc;
+        }
+        pg = end;
+    }
+    c->stats = acc;
     return RRB_OK;
 }
 
@@ -639,6 +801,7 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
         return RRB_ERR_DEVICE;
     }
     c->tmp_batch = new rrb_batch();
+    c->wave_batch = new rrb_batch();
     c->tuning.tile_w = 64;
     c->tuning.tile_h = 16;
     c->tuning.rows_per_chunk = 32;
@@ -654,11 +817,15 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
-                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2};
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);
         delete c->tmp_batch;
+    }
+    if (c->wave_batch) {
+        free_batch_bufs(c, c->wave_batch);
+        delete c->wave_batch;
     }
     if (c->timer) {
         for (int k = 0; k < kStages; ++k) {
@@ -830,6 +997,7 @@ int rrb_set_tuning(rrb_ctx* c, const rrb_tuning* t) {
     if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32 or 64x16");
     c->tuning.tile_w = w;
     c->tuning.tile_h = h;
+    if (t->wave_points != 0xFFFFFFFFu) c->tuning.wave_points = t->wave_points;  // all ones: keep
     return RRB_OK;
 }
 

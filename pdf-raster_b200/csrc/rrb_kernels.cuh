@@ -27,16 +27,20 @@ namespace rrb {
 // Piece slots: one per input point. kind in bits 30-31 of .y.
 constexpr uint32_t PK_NONE = 0, PK_LINE = 1, PK_CURVE = 2, PK_CLOSE = 3;
 
-// 48 bytes, 16-byte aligned; the pixel rectangle leads so it loads as one int4.
+// 64 bytes, 16-byte aligned; the pixel rectangle leads so it loads as one int4.
 struct __align__(16) PathInfo {
     int32_t px0, px1;        // pixel columns touched (px0 > px1: none)
     int32_t py0, py1;        // pixel rows touched under the row map
     int32_t y0, y1;          // AA rows [y0, y1] (y0 > y1: no rows)
     uint32_t e_begin, e_end; // edge range
-    uint32_t paint;          // gray | alpha << 8 | rule << 16
+    uint32_t paint;          // gray | alpha << 8 | rule << 16 | PI_RECTI
     uint32_t page;
-    uint32_t pad0, pad1;
+    uint32_t run_off, run_cnt; // rectilinear paths: pixel-row runs of identical coverage
+    int32_t bx0, bx1, by0, by1; // solid box: pixels with coverage 16 (bx0 > bx1: none)
 };
+
+constexpr uint32_t PI_RECTI = 1u << 17;  // all edges horizontal or vertical, at most RECTI_MAX_EDGES
+constexpr uint32_t RECTI_MAX_EDGES = 32;
 
 // Error / status word bits shared by all kernels of a batch.
 constexpr uint32_t ERR_EDGE_CAP = 1, ERR_ROW_CAP = 2, ERR_SPAN_CAP = 4, ERR_OVF_CAP = 8,
@@ -193,6 +197,17 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
     }
 }
 
+// Per-path offsets and page indices of a wave (a run of pages of a larger
+// batch), rebased to the wave's first point and first page.
+__global__ void k_rebase_paths(const uint64_t* __restrict__ off_in, uint64_t* __restrict__ off_out, uint64_t pt_base,
+                               const uint32_t* __restrict__ page_in, uint32_t* __restrict__ page_out, uint32_t pg_base,
+                               uint32_t n_paths) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n_paths; i += gridDim.x * blockDim.x) {
+        off_out[i] = off_in[i] - pt_base;
+        if (i < n_paths) page_out[i] = page_in[i] - pg_base;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Device-wide exclusive scan of u32 (three phases, host-known n).
 // out[i] = sum(in[0..i)), out[n] = total. in and out may alias.
@@ -288,6 +303,7 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
         uint32_t eb = edge_off[piece_off[p]], ee = edge_off[piece_off[p + 1]];
         int32_t y0 = INT32_MAX, y1 = INT32_MIN, xl = INT32_MAX, xh = INT32_MIN;
         unsigned long long raw = 0;
+        bool axis_only = true;
         // Aligned groups of 32 edges: one group per iteration, its row range
         // merged into gmin/gmax (atomically: a group can straddle two paths).
         for (uint32_t base4 = eb & ~31u; base4 < ee; base4 += 128) {
@@ -322,6 +338,8 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                 g0 = min(g0, __shfl_xor_sync(0xffffffffu, g0, o));
                 g1 = max(g1, __shfl_xor_sync(0xffffffffu, g1, o));
             }
+            axis_only &= __all_sync(0xffffffffu, (e4[u].flags & EF_EMPTY) ||
+                                                     (e4[u].flags & EF_KIND_MASK) != EK_SLOPED);
             if (lane == 0 && g0 <= g1) {
                 atomicMin(&gmin[base >> 5], g0);
                 atomicMax(&gmax[base >> 5], g1);
@@ -345,7 +363,13 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
             pi.e_end = ee;
             pi.paint = uint32_t(gray[p]) | (uint32_t(alpha[p]) << 8) | (uint32_t(rule[p] ? 1 : 0) << 16);
             pi.page = pg;
-            pi.pad0 = pi.pad1 = 0;
+            pi.run_off = pi.run_cnt = 0;
+            pi.bx0 = 1;
+            pi.bx1 = 0;
+            pi.by0 = 1;
+            pi.by1 = 0;
+            const bool recti = axis_only && y0 <= y1 && ee - eb <= RECTI_MAX_EDGES;
+            if (recti) pi.paint |= PI_RECTI;
             uint32_t rows = 0, groups = 0;
             if (y0 <= y1) {
                 pi.y0 = y0;
@@ -380,8 +404,9 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                 pi.py1 = 0;
             }
             info[p] = pi;
-            path_groups[p] = groups;
-            path_chunks[p] = (rows + chunk_rows - 1) / chunk_rows;
+            // Rectilinear paths skip the row stage: k_recti builds their row runs.
+            path_groups[p] = recti ? 0u : groups;
+            path_chunks[p] = recti ? 0u : (rows + chunk_rows - 1) / chunk_rows;
         }
     }
 }
@@ -816,6 +841,214 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     if (nonterm) atomicAdd(&ctr->nonterminating, nonterm);
 }
 
+// ---------------------------------------------------------------------------
+// Rectilinear paths (every edge horizontal or vertical, at most 32 edges: all
+// rectangles). Between "event rows" — a vertical edge's first row, the row
+// after it (the first row's count is 0 when it is not below seg_y_min) and
+// the row after its last; a horizontal edge's row and the row after — every
+// AA row has the same merged entries, so one row per band is computed and
+// pixel rows whose four sub-rows lie in one band share one cell list. The
+// path gets a list of runs (group range, cells) instead of a per-row index,
+// and a solid box (pixels of coverage 16) for the composite's full-tile path.
+// ---------------------------------------------------------------------------
+constexpr int RECTI_MAX_EVENTS = 4 * RECTI_MAX_EDGES + 2;
+constexpr int RECTI_MAX_SPANS = RECTI_MAX_EDGES / 2 + 1;
+
+// Spans of AA row r of a rectilinear path (fold, sort, walk over <= 32 edges).
+__device__ __forceinline__ int recti_row_spans(const PathInfo& P, const Edge* __restrict__ edges, int32_t r,
+                                               int32_t aa_width, int32_t* sx0, int32_t* sx1, uint32_t& nonterm) {
+    int32_t x0s[RECTI_MAX_EDGES], x1s[RECTI_MAX_EDGES], cs[RECTI_MAX_EDGES];
+    int n = 0;
+    for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
+        const Edge E = edges[j];
+        if ((E.flags & EF_EMPTY) || r < E.row0 || r > E.row1) continue;
+        int32_t elo, ehi, ec;
+        edge_entry(E, r, elo, ehi, ec);
+        if (n > 0 && sat_inc(x1s[n - 1]) >= elo && x0s[n - 1] <= sat_inc(ehi)) {
+            cs[n - 1] = static_cast<int32_t>(static_cast<uint32_t>(cs[n - 1]) + static_cast<uint32_t>(ec));
+            x0s[n - 1] = min(x0s[n - 1], elo);
+            x1s[n - 1] = max(x1s[n - 1], ehi);
+        } else {
+            x0s[n] = elo;
+            x1s[n] = ehi;
+            cs[n] = ec;
+            ++n;
+        }
+    }
+    for (int a = 1; a < n; ++a) {
+        const int32_t t0 = x0s[a], t1 = x1s[a], tc = cs[a];
+        int b = a;
+        while (b > 0 && t0 < x0s[b - 1]) {
+            x0s[b] = x0s[b - 1];
+            x1s[b] = x1s[b - 1];
+            cs[b] = cs[b - 1];
+            --b;
+        }
+        x0s[b] = t0;
+        x1s[b] = t1;
+        cs[b] = tc;
+    }
+    const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
+    return walk_row(
+        n, mask, aa_width,
+        [&](int i, int32_t& a, int32_t& b, int32_t& c) {
+            a = x0s[i];
+            b = x1s[i];
+            c = cs[i];
+        },
+        [&](int k, int32_t s0, int32_t e0) {
+            sx0[k] = s0;
+            sx1[k] = e0;
+        },
+        nonterm);
+}
+
+template <bool WRITE>
+__global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edge* __restrict__ edges,
+                        const uint32_t* __restrict__ page_w, int rowmap, uint32_t* __restrict__ run_count,
+                        const uint32_t* __restrict__ run_off, int4* __restrict__ runs, uint32_t* __restrict__ cells,
+                        uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
+    uint32_t nonterm = 0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        PathInfo P = info[p];
+        if (!(P.paint & PI_RECTI)) {
+            if (!WRITE) run_count[p] = 0;
+            continue;
+        }
+        // Event rows, sorted and unique, within [y0, y1 + 1].
+        int32_t ev[RECTI_MAX_EVENTS];
+        int nev = 0;
+        auto push = [&](int32_t v) {
+            if (v >= P.y0 && v <= P.y1 + 1) ev[nev++] = v;
+        };
+        push(P.y0);
+        push(P.y1 + 1);
+        for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
+            const Edge E = edges[j];
+            if (E.flags & EF_EMPTY) continue;
+            push(E.row0);
+            push(E.row0 + 1);
+            if ((E.flags & EF_KIND_MASK) == EK_VERT) push(E.row1 + 1);
+        }
+        for (int a = 1; a < nev; ++a) {
+            const int32_t t = ev[a];
+            int b = a;
+            while (b > 0 && t < ev[b - 1]) {
+                ev[b] = ev[b - 1];
+                --b;
+            }
+            ev[b] = t;
+        }
+        int m = 0;
+        for (int a = 0; a < nev; ++a)
+            if (m == 0 || ev[a] != ev[m - 1]) ev[m++] = ev[a];
+        nev = m;  // ev[0] = y0, ev[nev-1] = y1 + 1
+        auto band_of = [&](int32_t r) {  // last k with ev[k] <= r
+            int lo = 0, hi = nev - 1;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (ev[mid] <= r) lo = mid;
+                else hi = mid;
+            }
+            return lo;
+        };
+        const int32_t g0 = P.y0 >> 2, g1 = P.y1 >> 2;
+        const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        uint32_t nrun = 0;
+        uint32_t ro = WRITE ? run_off[p] : 0u;
+        int32_t best_rows = 0, bx0 = 1, bx1 = 0, bg0 = 1, bg1 = 0;
+        for (int32_t g = g0; g <= g1;) {
+            const int32_t r_lo = 4 * g, r_hi = 4 * g + 3;
+            const bool inside = r_lo >= P.y0 && r_hi <= P.y1;
+            int32_t g_end = g;
+            bool uniform = false;
+            int b = 0;
+            if (inside) {
+                b = band_of(r_lo);
+                if (band_of(r_hi) == b) {
+                    uniform = true;
+                    g_end = min((ev[b + 1] - 4) >> 2, (P.y1 - 3) >> 2);
+                }
+            }
+            if (WRITE) {
+                int32_t s0[4][RECTI_MAX_SPANS], s1[4][RECTI_MAX_SPANS];
+                int n4[4] = {0, 0, 0, 0};
+                if (uniform) {
+                    n4[0] = recti_row_spans(P, edges, r_lo, aa_width, s0[0], s1[0], nonterm);
+                    n4[1] = n4[2] = n4[3] = n4[0];
+                } else {
+                    for (int k = 0; k < 4; ++k) {
+                        const int32_t r = r_lo + k;
+                        if (r >= P.y0 && r <= P.y1) n4[k] = recti_row_spans(P, edges, r, aa_width, s0[k], s1[k], nonterm);
+                    }
+                }
+                const uint32_t need = 4u * static_cast<uint32_t>(n4[0] + n4[1] + n4[2] + n4[3]);
+                const uint32_t o0 = need ? atomicAdd(&ctr->cell_cursor, need) : 0u;
+                int nc = 0;
+                if (static_cast<uint64_t>(o0) + need > cell_cap) {
+                    atomicOr(&ctr->err, ERR_SPAN_CAP);
+                } else {
+                    int32_t f0 = 1, f1 = 0;  // widest coverage-16 cell of a uniform run
+                    nc = sweep_cells(
+                        n4,
+                        [&](int k, int i, bool end) {
+                            const int kk = uniform ? 0 : k;
+                            return end ? s1[kk][i] : s0[kk][i];
+                        },
+                        [&](int q, uint32_t cell) {
+                            cells[o0 + q] = cell;
+                            const int32_t len = static_cast<int32_t>((cell >> 14) & 0x3fffu) + 1;
+                            if ((cell >> 28) == 15u && len > f1 - f0 + 1) {
+                                f0 = static_cast<int32_t>(cell & 0x3fffu);
+                                f1 = f0 + len - 1;
+                            }
+                        });
+                    if (uniform && f0 <= f1) {
+                        const int32_t rows = g_end - g + 1;
+                        if (static_cast<int64_t>(rows) * (f1 - f0 + 1) > static_cast<int64_t>(best_rows) * (bx1 - bx0 + 1)) {
+                            best_rows = rows;
+                            bx0 = f0;
+                            bx1 = f1;
+                            bg0 = g;
+                            bg1 = g_end;
+                        }
+                    }
+                }
+                runs[ro + nrun] = make_int4(g, g_end, static_cast<int32_t>(o0), nc);
+            }
+            ++nrun;
+            g = g_end + 1;
+        }
+        if (!WRITE) {
+            run_count[p] = nrun;
+        } else {
+            P.run_off = ro;
+            P.run_cnt = nrun;
+            // Solid box in pixel rows of the row map, inside the rows the path draws.
+            int32_t by0, by1;
+            if (rowmap == 0) {
+                by0 = bg0;
+                by1 = bg1;
+            } else {  // pixel row y shows group 4y + 3
+                by0 = (bg0 - 3 + 3) >> 2;
+                by0 = (4 * by0 + 3 < bg0) ? by0 + 1 : by0;
+                by1 = bg1 >= 3 ? (bg1 - 3) >> 2 : -1;
+            }
+            by0 = max(by0, P.py0);
+            by1 = min(by1, P.py1);
+            if (bx0 <= bx1 && by0 <= by1) {
+                info[p].bx0 = bx0;
+                info[p].bx1 = bx1;
+                info[p].by0 = by0;
+                info[p].by1 = by1;
+            }
+            info[p].run_off = ro;
+            info[p].run_cnt = nrun;
+        }
+    }
+    if (WRITE && nonterm) atomicAdd(&ctr->nonterminating, nonterm);
+}
+
 // Pixel rows whose sub-row lists overflowed KCAP: one warp per pixel row
 // (lanes 0-3 = its AA rows) with MID_K entries per row in shared memory.
 // Rows longer than that go to k_groups_slow through ovf2.
@@ -980,8 +1213,11 @@ __constant__ uint8_t c_gamma[17] = {0, 4, 11, 21, 32, 45, 59, 74, 90, 108, 126, 
 
 struct HitInfo {
     int32_t g0, g1, py0, py1;  // pixel-row groups [g0, g1] (AA rows >> 2), pixel rows touched
-    uint32_t goff, paint;      // first group index entry, paint word
+    uint32_t goff, paint;      // first group index entry (or first run), paint word (| HIT_FULL)
+    uint32_t run_cnt, pad;     // rectilinear paths: number of runs
 };
+
+constexpr uint32_t HIT_FULL = 1u << 18;  // every pixel of this tile has coverage 16 for this path
 
 template <int TW>
 struct CompLayout {
@@ -1003,7 +1239,8 @@ struct HitRows {
 
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
-                                               const uint2* __restrict__ gidx, HitRows<TW, TH>& hr) {
+                                               const uint2* __restrict__ gidx, const int4* __restrict__ runs,
+                                               HitRows<TW, TH>& hr) {
     using L = CompLayout<TW>;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int slot = lane / L::LPR;
@@ -1012,7 +1249,23 @@ __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int
         const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
         const int32_t grp = rowmap ? 4 * y + 3 : y;
         const bool rowok = y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
-        hr.ix[it] = rowok ? gidx[h.goff + static_cast<uint32_t>(grp - h.g0)] : make_uint2(0u, 0u);
+        uint2 ix = make_uint2(0u, 0u);
+        if (rowok) {
+            if (h.paint & PI_RECTI) {
+                // Runs cover [g0, g1] in order: the last run starting at or before grp.
+                uint32_t lo = 0, hi = h.run_cnt;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (runs[h.goff + mid].x <= grp) lo = mid;
+                    else hi = mid;
+                }
+                const int4 rn = runs[h.goff + lo];
+                if (rn.x <= grp && grp <= rn.y) ix = make_uint2(static_cast<uint32_t>(rn.z), static_cast<uint32_t>(rn.w));
+            } else {
+                ix = gidx[h.goff + static_cast<uint32_t>(grp - h.g0)];
+            }
+        }
+        hr.ix[it] = ix;
     }
 }
 
@@ -1104,11 +1357,11 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 }
 
 template <int TW, int TH>
-__global__ void __launch_bounds__(COMP_THREADS) k_composite(
+__global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
     const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
-    uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr) {
+    const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr) {
     using L = CompLayout<TW>;
     constexpr int ITERS = TH / (L::NW * L::RPW);
     constexpr int NPIX = TH * TW / COMP_THREADS;
@@ -1117,6 +1370,8 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
     __shared__ uint32_t wcnt[L::NW];
     __shared__ uint8_t gamma[17];
     __shared__ int32_t mark[L::NW * L::RPW][TW];
+    __shared__ uint8_t lut[256];
+    __shared__ uint32_t red[L::NW];
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1142,11 +1397,37 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
         const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
         const uint32_t q0 = G.work_base + (sy * G.nsx + sx) * G.nblk;
         const uint32_t l0 = super_off[q0], l1 = super_off[q0 + G.nblk];
-        for (uint32_t c0 = l0; c0 < l1; c0 += COMP_CHUNK) {
+        // The tile clipped to the page: a path whose solid box holds it covers
+        // every pixel that matters with coverage 16.
+        const int TX1 = min(X0 + TW, W) - 1, TY1 = min(Y0 + TH, H) - 1;
+        auto full_over = [&](const PathInfo& P) {
+            return P.bx0 <= X0 && P.bx1 >= TX1 && P.by0 <= Y0 && P.by1 >= TY1;
+        };
+        // Pre-pass: the last opaque layer covering the whole tile sets every
+        // pixel to its gray (div255(255 * g) = g), so compositing starts there.
+        uint32_t start = l0;
+        {
+            uint32_t best = 0;
+            for (uint32_t c0 = l0; c0 < l1; c0 += COMP_CHUNK) {
+                const uint32_t q = c0 + threadIdx.x;
+                if (q < l1) {
+                    const PathInfo P = info[super_list[q]];
+                    if (((P.paint >> 8) & 0xff) == 255u && full_over(P)) best = q + 1;
+                }
+            }
+            for (int o = 16; o; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+            if (lane == 0) red[w] = best;
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < L::NW; ++k) best = max(best, red[k]);
+            __syncthreads();
+            if (best) start = best - 1;
+        }
+        for (uint32_t c0 = l0 + ((start - l0) / COMP_CHUNK) * COMP_CHUNK; c0 < l1; c0 += COMP_CHUNK) {
             const uint32_t q = c0 + threadIdx.x;
             bool hit = false;
             PathInfo P;
-            if (q < l1) {
+            if (q < l1 && q >= start) {
                 P = info[super_list[q]];
                 hit = P.px0 <= X0 + TW - 1 && P.px1 >= X0 && P.py0 <= Y0 + TH - 1 && P.py1 >= Y0 && P.px0 <= P.px1;
             }
@@ -1167,25 +1448,57 @@ __global__ void __launch_bounds__(COMP_THREADS) k_composite(
                 hi.g1 = P.y1 >> 2;
                 hi.py0 = P.py0;
                 hi.py1 = P.py1;
-                hi.goff = group_off[super_list[q]];
-                hi.paint = P.paint;
+                hi.goff = (P.paint & PI_RECTI) ? P.run_off : group_off[super_list[q]];
+                hi.run_cnt = P.run_cnt;
+                hi.pad = 0;
+                hi.paint = P.paint | (full_over(P) ? HIT_FULL : 0u);
                 hits[pos] = hi;
             }
             __syncthreads();
             // Software pipeline over the hits: the index entries of hit k+2 and
             // the first cells of hit k+1 are in flight while hit k is blended.
+            // A run of layers covering the whole tile is applied as one 256-entry
+            // map (one blend per thread per layer) instead of per pixel.
             HitRows<TW, TH> cur, nxt, nxt2;
-            if (total > 0) {
-                load_hit_index<TW, TH>(hits[0], rowmap, Y0, H, gidx, cur);
-                load_hit_cells<TW, TH>(cells, cur);
-            }
-            if (total > 1) load_hit_index<TW, TH>(hits[1], rowmap, Y0, H, gidx, nxt);
-            for (uint32_t k = 0; k < total; ++k) {
-                if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, nxt2);
+            auto prime = [&](uint32_t k) {
+                if (k < total) {
+                    load_hit_index<TW, TH>(hits[k], rowmap, Y0, H, gidx, runs, cur);
+                    load_hit_cells<TW, TH>(cells, cur);
+                }
+                if (k + 1 < total) load_hit_index<TW, TH>(hits[k + 1], rowmap, Y0, H, gidx, runs, nxt);
+            };
+            prime(0);
+            uint32_t k = 0;
+            while (k < total) {
+                if (hits[k].paint & HIT_FULL) {
+                    uint32_t m = k + 1;
+                    while (m < total && (hits[m].paint & HIT_FULL)) ++m;
+                    if (m - k >= 2) {
+                        __syncthreads();  // the previous map's readers are done
+                        uint32_t v = threadIdx.x;
+                        for (uint32_t i = k; i < m; ++i) {
+                            const uint32_t a = (hits[i].paint >> 8) & 0xff, gg = hits[i].paint & 0xff;
+                            v = div255((255u - a) * v + a * gg);  // a_src = div255(a * AA_GAMMA[16]) = a
+                        }
+                        lut[threadIdx.x] = static_cast<uint8_t>(v);
+                        __syncthreads();
+#pragma unroll
+                        for (int j = 0; j < NPIX; ++j) pix[j] = lut[pix[j]];
+                    } else {
+                        const uint32_t a = (hits[k].paint >> 8) & 0xff, gg = hits[k].paint & 0xff;
+#pragma unroll
+                        for (int j = 0; j < NPIX; ++j) pix[j] = div255((255u - a) * pix[j] + a * gg);
+                    }
+                    k = m;
+                    prime(k);
+                    continue;
+                }
+                if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
                 if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
                 composite_path_rows<TW, TH>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
                 nxt = nxt2;
+                ++k;
             }
             __syncthreads();
         }

@@ -363,8 +363,9 @@ class B200Backend:
         return {buf[i].name.decode(): (float(buf[i].ms), int(buf[i].launches)) for i in range(min(n.value, 32))}
 
     # ---- tuning / stats
-    def set_tuning(self, tile_w: int = 0, tile_h: int = 0):
-        t = Tuning(tile_w=tile_w, tile_h=tile_h)
+    def set_tuning(self, tile_w: int = 0, tile_h: int = 0, wave_points: int | None = None):
+        """Tile shape (16x16 / 32x32 / 64x16) and, if given, path points per page wave (0 = default)."""
+        t = Tuning(tile_w=tile_w, tile_h=tile_h, wave_points=0xFFFFFFFF if wave_points is None else wave_points)
         self._chk(lib().rrb_set_tuning(self._h, C.byref(t)))
 
     def get_tuning(self) -> Tuning:

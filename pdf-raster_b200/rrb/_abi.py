@@ -77,7 +77,7 @@ class PathBatchParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("rows_per_chunk", C.c_uint32),
-                ("reserved", C.c_uint32 * 5)]
+                ("wave_points", C.c_uint32), ("reserved", C.c_uint32 * 4)]
 
 
 class BatchStats(C.Structure):

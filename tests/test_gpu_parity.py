@@ -248,3 +248,82 @@ def test_memory_budget_is_enforced(rrb_lib):
         assert e.value.kind == "OutOfMemory"
         assert b.detect_vram_budget().used_bytes >= 1 << 19
         b.free_device(x)
+
+
+# ---- overdraw: rectilinear runs, full-tile layers, opaque occlusion, waves ----------
+
+def _stacked_rects(rrb, W, H, n, seed):
+    """Rectangles covering most of the page (some opaque, most translucent) with
+    polygons in between: full-tile layer runs, occluding opaque layers, and
+    rectangle edges inside tiles."""
+    rng = np.random.default_rng(seed)
+    pts, flags, off, rule, gray, alpha = [], [], [0], [], [], []
+    for i in range(n):
+        b = rrb.PathBuilder()
+        if i % 5 == 3:
+            cx, cy, r = rng.uniform(0, W), rng.uniform(0, H), rng.uniform(5, 40)
+            b.move_to(cx + r, cy)
+            for k in range(1, 9):
+                t = 2 * np.pi * k / 9
+                b.curve_to(cx + r * np.cos(t - 0.3), cy + r * np.sin(t - 0.3), cx + r * np.cos(t - 0.1),
+                           cy + r * np.sin(t - 0.1), cx + r * np.cos(t), cy + r * np.sin(t))
+            b.close()
+        else:
+            x0, y0 = rng.uniform(-10, W * 0.3), rng.uniform(-10, H * 0.3)
+            x1, y1 = rng.uniform(W * 0.6, W + 10), rng.uniform(H * 0.6, H + 10)
+            if i % 7 == 1:  # counter-clockwise and integral
+                x0, y0, x1, y1 = float(int(x0)), float(int(y0)), float(int(x1)), float(int(y1))
+                b.move_to(x0, y0)
+                b.line_to(x0, y1)
+                b.line_to(x1, y1)
+                b.line_to(x1, y0)
+            else:
+                b.move_to(x0, y0)
+                b.line_to(x1, y0)
+                b.line_to(x1, y1)
+                b.line_to(x0, y1)
+            b.close()
+        p, f = b.build()
+        pts.append(p)
+        flags.append(f)
+        off.append(off[-1] + len(f))
+        rule.append(i % 2)
+        gray.append(int(rng.integers(0, 256)))
+        alpha.append(255 if i % 11 == 5 else int(rng.integers(32, 255)))
+    return (np.concatenate(pts), np.concatenate(flags), np.array(off, np.uint64), np.array(rule, np.uint8),
+            np.array(gray, np.uint8), np.array(alpha, np.uint8))
+
+
+@pytest.mark.parametrize("rowmap", ROWMAPS)
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16)])
+def test_stacked_rectangles(backend, oracle, rrb_lib, rowmap, tile):
+    W, H = 211, 157
+    pts, flags, off, rule, gray, alpha = _stacked_rects(rrb_lib, W, H, 60, seed=7)
+    n = len(rule)
+    init = np.random.default_rng(1).integers(0, 256, W * H, dtype=np.uint8)
+    exp = init.copy()
+    oracle.render_arrays(exp, [0], [W], [H], pts, flags, off, rule, gray, alpha, np.zeros(n, np.uint32), rowmap=rowmap)
+    buf = backend.alloc_device(W * H)
+    keep = []
+    backend.set_tuning(*tile)
+    try:
+        p = rrb_lib.batch_params(pts, flags, off, rule, gray, alpha, np.zeros(n, np.uint32), [W], [H], [0], buf,
+                                 rowmap=rowmap, keep=keep)
+        got = init.copy()
+        backend.render_pages_host(p, got)
+    finally:
+        backend.set_tuning(64, 16)
+        backend.free_device(buf)
+    assert np.array_equal(got, exp), _diff(got, exp)
+
+
+def test_waves_match_oracle(backend, oracle, rrb_lib):
+    """Pages processed in several memory waves give the same pages."""
+    s = rrb_lib.Scene(kind=2, seed=13, n_pages=7, page_scale=0.12, paths_scale=0.03)
+    exp, _ = _oracle_arena(oracle, s, 0)
+    backend.set_tuning(wave_points=max(1000, s.n_pts // 5))
+    try:
+        got = _gpu_arena(backend, s, 0)
+    finally:
+        backend.set_tuning(wave_points=0)
+    assert np.array_equal(got, exp), _diff(got, exp)
