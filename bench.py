@@ -44,6 +44,10 @@ WORKLOADS = {
     "glyphs": (dict(kind=1, seed=0),
                "glyph-dense text page: 150,000 quadratic glyph paths (2 contours avg, 12-60 quads each, "
                "8-12 pt em @300 dpi, 60 baselines) on one 2550x3300 u8 page (Letter @300 dpi), NZ, gray 0, alpha 255"),
+    "mixed": (dict(kind=2, seed=0),
+              "mixed pages in one batch: 64 u8 pages of {A4, Letter, A3} x {150, 300, 600} dpi, log-normal path "
+              "count (median 5,000, sigma 1.2, cap 50,000) of 30% glyphs / 40% polygons / 30% axis-aligned "
+              "rectangles covering 5-80% of the page, alpha 32-255"),
     "polygons": (dict(kind=0, seed=0),
                  "polygon page: 2,000 closed paths (1-3 contours x 4-32 line/cubic segments, jittered circles, "
                  "log-normal radius) on one 2550x3300 u8 page, NZ 70% / EO 30%, opaque"),

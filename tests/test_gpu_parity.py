@@ -327,3 +327,47 @@ def test_waves_match_oracle(backend, oracle, rrb_lib):
     finally:
         backend.set_tuning(wave_points=0)
     assert np.array_equal(got, exp), _diff(got, exp)
+
+
+def _page_subscene(s, pages):
+    """Arrays of the paths of `pages` of scene `s`, with their own page arena."""
+    sel = np.isin(s.path_page, pages)
+    idx = np.nonzero(sel)[0]
+    pts, flags, off = [], [], [0]
+    for p in idx:
+        a, b = int(s.path_pt_off[p]), int(s.path_pt_off[p + 1])
+        pts.append(s.pts[a:b])
+        flags.append(s.flags[a:b])
+        off.append(off[-1] + b - a)
+    remap = {pg: i for i, pg in enumerate(pages)}
+    w = np.array([s.page_width[pg] for pg in pages], np.uint32)
+    h = np.array([s.page_height[pg] for pg in pages], np.uint32)
+    po = np.concatenate([[0], np.cumsum(w.astype(np.uint64) * h)[:-1]]).astype(np.uint64)
+    return dict(pts=np.concatenate(pts), flags=np.concatenate(flags), path_pt_off=np.array(off, np.uint64),
+                fill_rule=s.fill_rule[idx], gray=s.gray[idx], alpha=s.alpha[idx],
+                path_page=np.array([remap[int(x)] for x in s.path_page[idx]], np.uint32),
+                page_width=w, page_height=h, page_offset=po, arena=int(np.sum(w.astype(np.uint64) * h)))
+
+
+def test_full_mixed_pages(backend, oracle, rrb_lib):
+    """64 mixed pages (1.17 Gpx, 662k paths) in one batch: the two smallest pages
+    against the oracle byte for byte, and the whole arena identical when the
+    batch is split into waves."""
+    s = rrb_lib.Scene(kind=2, seed=0)
+    got = _gpu_arena(backend, s, 0)
+    sizes = s.page_width.astype(np.int64) * s.page_height
+    small = [int(i) for i in np.argsort(sizes, kind="stable")[:2]]
+    sub = _page_subscene(s, small)
+    exp = np.full(sub["arena"], 255, np.uint8)
+    oracle.render_arrays(exp, sub["page_offset"], sub["page_width"], sub["page_height"], sub["pts"], sub["flags"],
+                         sub["path_pt_off"], sub["fill_rule"], sub["gray"], sub["alpha"], sub["path_page"], threads=2)
+    for i, pg in enumerate(small):
+        o, n = int(s.page_offset[pg]), int(sizes[pg])
+        oo = int(sub["page_offset"][i])
+        assert np.array_equal(got[o:o + n], exp[oo:oo + n]), f"page {pg}: {_diff(got[o:o + n], exp[oo:oo + n])}"
+    backend.set_tuning(wave_points=s.n_pts // 6)
+    try:
+        waved = _gpu_arena(backend, s, 0)
+    finally:
+        backend.set_tuning(wave_points=0)
+    assert np.array_equal(waved, got), _diff(waved, got)
