@@ -346,6 +346,65 @@ def run_rrb(args, rank, local, world):
         dist.destroy_process_group()
 
 
+def page_requests(rrb, scene):
+    """One request per page of `scene`: (params, keep-alive arrays, page bytes)."""
+    out = []
+    for pg in range(scene.n_pages):
+        idx = np.nonzero(scene.path_page == pg)[0]
+        a, b = int(scene.path_pt_off[idx[0]]), int(scene.path_pt_off[idx[-1] + 1])
+        keep = []
+        w, h = int(scene.page_width[pg]), int(scene.page_height[pg])
+        p = rrb.batch_params(scene.pts[a:b], scene.flags[a:b], scene.path_pt_off[idx[0]:idx[-1] + 2] - a,
+                             scene.fill_rule[idx], scene.gray[idx], scene.alpha[idx], np.zeros(len(idx), np.uint32),
+                             [w], [h], [0], None, keep=keep)
+        out.append((p, keep, w * h))
+    return out
+
+
+def run_serving(args, rank, world):
+    """Poisson page-render requests against the continuous-batching server."""
+    if rank != 0:
+        return
+    import rrb
+    scene = rrb.Scene(kind=2, seed=0)
+    reqs = page_requests(rrb, scene)
+    rates = [float(r) for r in args.rates.split(",")]
+    rng = np.random.default_rng(0)
+    results = []
+    with rrb.Server(workers=args.workers, mem_budget=args.mem_budget_gb << 30, max_batch_pages=64) as srv:
+        # warm-up: every distinct page once
+        warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n in reqs[:8]]
+        for t in warm:
+            srv.wait(t)
+        for rate in rates:
+            n = args.requests
+            gaps = rng.exponential(1.0 / rate, n)
+            outs = [np.empty(reqs[i % len(reqs)][2], np.uint8) for i in range(n)]
+            tickets = []
+            t0 = time.perf_counter()
+            due = t0
+            for i in range(n):
+                due += gaps[i]
+                dt = due - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                p, k, _ = reqs[i % len(reqs)]
+                tickets.append(srv.submit(p, outs[i], keep=k))
+            lat = [srv.wait(t)["latency_ns"] / 1e6 for t in tickets]
+            wall = time.perf_counter() - t0
+            px = sum(reqs[i % len(reqs)][2] for i in range(n))
+            results.append({"rate_pages_s": rate, "requests": n, "completed_pages_s": n / wall,
+                            "mpixel_s": px / wall / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                            "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99))})
+        st = srv.stats()
+    line = {"metric": "p99 page latency under Poisson load (continuous batching)", "unit": "ms",
+            "value": results[-1]["p99_ms"], "higher_is_better": False, "n_gpus": 1,
+            "config": {"workload": "requests = single pages of the mixed 64-page scene (seed 0), cycled",
+                       "workers": args.workers, "mem_budget_gb": args.mem_budget_gb},
+            "serving": results, "server_stats": st}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,9 +418,16 @@ def main():
     ap.add_argument("--ref-threads", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
+    ap.add_argument("--serving", action="store_true", help="Poisson request load against the server")
+    ap.add_argument("--rates", default="50,200,1000,2000")
+    ap.add_argument("--requests", type=int, default=128)
+    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--mem-budget-gb", type=int, default=60)
     args = ap.parse_args()
     rank, local, world = dist_env()
-    if args.impl == "reference":
+    if args.serving:
+        run_serving(args, rank, world)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_rrb(args, rank, local, world)

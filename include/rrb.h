@@ -219,6 +219,59 @@ int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
 int rrb_render_pages_host(rrb_ctx* ctx, const rrb_path_batch_params* p, uint8_t* host_pages,
                           size_t host_pages_len);
 
+/* ---- serving: continuous batching of page renders --------------------------
+ * Worker threads, each with its own context and stream, form batches from the
+ * request queue in arrival order at every batch boundary, admitting requests
+ * while the estimated device bytes of all in-flight batches stay within
+ * mem_budget_bytes (a single request larger than the budget still runs when
+ * nothing else is in flight). Requests arriving while batches run join the
+ * next batch that has room. A request's arrays must stay valid until
+ * rrb_server_wait returns for it; its pages start at init_value and come
+ * back into host_pages (layout of its page_offset). */
+typedef struct rrb_server rrb_server;
+typedef struct {
+    int device;
+    uint32_t workers;          /* contexts (streams) rendering concurrently; 0 = 2 */
+    uint64_t mem_budget_bytes; /* admission cap on in-flight device bytes; 0 = none */
+    uint32_t max_batch_pages;  /* pages per batch; 0 = 64 */
+    uint32_t tile_w, tile_h;   /* 0 = default tile */
+    uint32_t reserved[3];
+} rrb_server_config;
+typedef struct {
+    int status;
+    uint64_t latency_ns; /* submit -> pages on the host */
+    uint64_t queue_ns;   /* submit -> its batch started */
+} rrb_request_result;
+typedef struct {
+    uint64_t completed, batches, batched_requests, queued, in_use_bytes, peak_in_use_bytes;
+} rrb_server_stats_t;
+int rrb_server_create(const rrb_server_config* cfg, rrb_server** out);
+int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* host_pages, size_t host_pages_len,
+                      uint8_t init_value, uint64_t* ticket);
+int rrb_server_wait(rrb_server* s, uint64_t ticket, uint64_t timeout_ns, rrb_request_result* res);
+int rrb_server_stats(rrb_server* s, rrb_server_stats_t* out);
+int rrb_server_destroy(rrb_server* s);
+
+/* ---- learned cost model -----------------------------------------------------
+ * FP32 MLP RRB_MLP_IN -> 64 -> 64 -> 1 (ReLU) predicting log render time of a
+ * page for a tile shape from page features, trained on the device by its own
+ * forward / backward / Adam kernels (MSE loss). Parameters, in order:
+ * W1[64][24], b1[64], W2[64][64], b2[64], W3[64], b3. It never touches pixels. */
+#define RRB_MLP_IN 24
+#define RRB_MLP_HIDDEN 64
+#define RRB_MLP_PARAMS (64 * 24 + 64 + 64 * 64 + 64 + 64 + 1)
+typedef struct rrb_mlp rrb_mlp;
+int rrb_mlp_create(int device, uint64_t seed, rrb_mlp** out);  /* He-normal initialisation */
+int rrb_mlp_destroy(rrb_mlp* m);
+int rrb_mlp_set_params(rrb_mlp* m, const float* params);       /* also resets Adam state */
+int rrb_mlp_get_params(rrb_mlp* m, float* params);
+/* One forward/backward over n samples without updating: mean loss and its gradient. */
+int rrb_mlp_loss_grad(rrb_mlp* m, const float* X, const float* y, uint32_t n, float* grad_out, float* loss_out);
+/* Adam over shuffled minibatches of `batch` (0 = full batch); host arrays X[n][24], y[n]. */
+int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32_t epochs, uint32_t batch,
+                  float lr, uint64_t seed, float* final_loss);
+int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out);
+
 /* ---- path construction on the host (A1, A2) --------------------------------
  * PathBuilder::{move_to, line_to, curve_to, close} (crates/raster/src/path/
  * mod.rs:310-448) and conic_to_cubic (crates/font/src/outline.rs:106-112). */

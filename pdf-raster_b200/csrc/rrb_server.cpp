@@ -1,0 +1,294 @@
+// rrb_server.cpp — continuous-batching page-render server over the C ABI.
+//
+// Requests are page renders (a path batch over its own pages). Worker threads,
+// each with its own backend context (own stream and scratch), take the queue
+// in arrival order and form batches at every batch boundary: as many queued
+// requests as fit the device-memory budget (estimated resident bytes of all
+// in-flight batches) and the per-batch page cap. A request that arrives while
+// batches are on the device joins the next batch that has room, so work from
+// different requests overlaps on the device across workers. Each request's
+// pages come back to its own host buffer; latency is submit -> pages on host.
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/rrb.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    rrb_path_batch_params p{};  // host arrays, valid until the request completes
+    uint8_t* out = nullptr;     // host pages (arena layout of p.page_offset)
+    size_t out_len = 0;
+    uint8_t init = 255;
+    uint64_t est_bytes = 0;
+    int status = RRB_OK;
+    bool done = false;
+    Clock::time_point t_submit, t_start, t_done;
+};
+
+}  // namespace
+
+struct rrb_server {
+    rrb_server_config cfg{};
+    std::vector<rrb_ctx*> ctx;
+    std::vector<std::thread> threads;
+    std::mutex m;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request*> queue;
+    std::unordered_map<uint64_t, Request*> live;
+    uint64_t next_id = 1;
+    uint64_t in_use = 0, peak_in_use = 0;
+    uint64_t batches = 0, batched_requests = 0, completed = 0;
+    bool stop = false;
+};
+
+namespace {
+
+// Device bytes a request needs while it is on the device: its pages, its
+// inputs, and the intermediate edge / row data (about 3.5 edges of 32 B per
+// input point on curve-heavy content, and a few bytes per pixel row).
+uint64_t estimate_bytes(const rrb_path_batch_params& p) {
+    uint64_t pages = 0;
+    for (uint32_t i = 0; i < p.n_pages; ++i) pages += static_cast<uint64_t>(p.page_width[i]) * p.page_height[i];
+    return 3 * pages + p.n_pts * (17 + 112) + p.n_paths * 256 + (1u << 20);
+}
+
+struct Staging {
+    std::vector<double> pts;
+    std::vector<uint8_t> flags, rule, gray, alpha;
+    std::vector<uint64_t> off, page_off;
+    std::vector<uint32_t> path_page, pw, ph;
+};
+
+void worker(rrb_server* s, int wi) {
+    rrb_ctx* c = s->ctx[wi];
+    Staging st;
+    rrb_buf* arena = nullptr;
+    size_t arena_cap = 0;
+    for (;;) {
+        std::vector<Request*> batch;
+        uint64_t bytes = 0;
+        {
+            std::unique_lock<std::mutex> lk(s->m);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+            if (s->stop && s->queue.empty()) break;
+            uint32_t pages = 0;
+            while (!s->queue.empty()) {
+                Request* r = s->queue.front();
+                const bool fits = s->in_use + bytes + r->est_bytes <= s->cfg.mem_budget_bytes || s->cfg.mem_budget_bytes == 0;
+                if (!batch.empty() && (!fits || pages + r->p.n_pages > s->cfg.max_batch_pages)) break;
+                if (batch.empty() && !fits && s->in_use > 0) break;  // wait for memory to free up
+                s->queue.pop_front();
+                batch.push_back(r);
+                bytes += r->est_bytes;
+                pages += r->p.n_pages;
+            }
+            if (batch.empty()) {
+                // Nothing admissible: let another batch finish first.
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(1));
+                continue;
+            }
+            s->in_use += bytes;
+            s->peak_in_use = std::max(s->peak_in_use, s->in_use);
+            s->batches += 1;
+            s->batched_requests += batch.size();
+        }
+        const auto t_start = Clock::now();
+        // Concatenate the requests into one batch over one device arena.
+        st.pts.clear(); st.flags.clear(); st.rule.clear(); st.gray.clear(); st.alpha.clear();
+        st.off.assign(1, 0); st.page_off.clear(); st.path_page.clear(); st.pw.clear(); st.ph.clear();
+        std::vector<uint64_t> req_arena_off;
+        uint64_t arena_len = 0;
+        uint32_t page_base = 0;
+        for (Request* r : batch) {
+            const rrb_path_batch_params& p = r->p;
+            req_arena_off.push_back(arena_len);
+            const uint64_t pt_base = st.flags.size();
+            st.pts.insert(st.pts.end(), p.pts, p.pts + 2 * p.n_pts);
+            st.flags.insert(st.flags.end(), p.flags, p.flags + p.n_pts);
+            for (uint64_t i = 0; i < p.n_paths; ++i) {
+                st.off.push_back(pt_base + p.path_pt_off[i + 1]);
+                st.path_page.push_back(page_base + p.path_page[i]);
+            }
+            st.rule.insert(st.rule.end(), p.fill_rule, p.fill_rule + p.n_paths);
+            st.gray.insert(st.gray.end(), p.gray, p.gray + p.n_paths);
+            st.alpha.insert(st.alpha.end(), p.alpha, p.alpha + p.n_paths);
+            for (uint32_t i = 0; i < p.n_pages; ++i) {
+                st.pw.push_back(p.page_width[i]);
+                st.ph.push_back(p.page_height[i]);
+                st.page_off.push_back(arena_len + p.page_offset[i]);
+            }
+            arena_len += (r->out_len + 255) & ~size_t(255);
+            page_base += p.n_pages;
+        }
+        int rc = RRB_OK;
+        if (arena_len > arena_cap) {
+            if (arena) rrb_free_device(c, arena);
+            arena = nullptr;
+            arena_cap = 0;
+            rc = rrb_alloc_device(c, arena_len + arena_len / 4, &arena);
+            if (!rc) arena_cap = arena_len + arena_len / 4;
+        }
+        rrb_path_batch_params b = batch.front()->p;
+        b.pts = st.pts.data();
+        b.flags = st.flags.data();
+        b.n_pts = st.flags.size();
+        b.path_pt_off = st.off.data();
+        b.fill_rule = st.rule.data();
+        b.gray = st.gray.data();
+        b.alpha = st.alpha.data();
+        b.path_page = st.path_page.data();
+        b.n_paths = st.rule.size();
+        b.page_width = st.pw.data();
+        b.page_height = st.ph.data();
+        b.page_offset = st.page_off.data();
+        b.n_pages = static_cast<uint32_t>(st.pw.size());
+        b.pages = arena;
+        rrb_fence f = 0;
+        if (!rc) rc = rrb_begin_page(c);
+        if (!rc) {
+            for (size_t k = 0; k < batch.size() && !rc; ++k)
+                rc = rrb_record_fill_buffer(c, arena, req_arena_off[k], batch[k]->out_len, batch[k]->init);
+            if (!rc) rc = rrb_record_path_batch(c, &b);
+            int rc2 = rrb_submit_page(c, &f);
+            if (!rc) rc = rc2;
+        }
+        if (!rc) rc = rrb_wait_page(c, f, 0);
+        for (size_t k = 0; k < batch.size() && !rc; ++k) {
+            rrb_fence df = 0;
+            rc = rrb_download_async(c, arena, req_arena_off[k], batch[k]->out, batch[k]->out_len, &df);
+            if (!rc) rc = rrb_wait_download(c, df);
+        }
+        const auto t_done = Clock::now();
+        {
+            std::lock_guard<std::mutex> lk(s->m);
+            s->in_use -= bytes;
+            for (Request* r : batch) {
+                r->status = rc;
+                r->t_start = t_start;
+                r->t_done = t_done;
+                r->done = true;
+                s->completed += 1;
+            }
+        }
+        s->cv_done.notify_all();
+        s->cv_work.notify_all();
+    }
+    if (arena) rrb_free_device(c, arena);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rrb_server_create(const rrb_server_config* cfg, rrb_server** out) {
+    if (!cfg || !out) return RRB_ERR_INVARIANT;
+    rrb_server* s = new rrb_server();
+    s->cfg = *cfg;
+    if (!s->cfg.workers) s->cfg.workers = 2;
+    if (!s->cfg.max_batch_pages) s->cfg.max_batch_pages = 64;
+    for (uint32_t i = 0; i < s->cfg.workers; ++i) {
+        rrb_ctx* c = nullptr;
+        int rc = rrb_init(cfg->device, 0, &c);
+        if (rc) {
+            for (rrb_ctx* x : s->ctx) rrb_destroy(x);
+            delete s;
+            return rc;
+        }
+        rrb_tuning t{};
+        t.tile_w = cfg->tile_w;
+        t.tile_h = cfg->tile_h;
+        t.wave_points = 0xFFFFFFFFu;
+        if (t.tile_w && t.tile_h) rrb_set_tuning(c, &t);
+        s->ctx.push_back(c);
+    }
+    for (uint32_t i = 0; i < s->cfg.workers; ++i) s->threads.emplace_back(worker, s, static_cast<int>(i));
+    *out = s;
+    return RRB_OK;
+}
+
+int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* host_pages, size_t host_pages_len,
+                      uint8_t init_value, uint64_t* ticket) {
+    if (!s || !p || !host_pages || !ticket) return RRB_ERR_INVARIANT;
+    char msg[8];
+    int rc = rrb_validate_path_batch(p, host_pages_len, msg, sizeof msg);
+    if (rc) return rc;
+    Request* r = new Request();
+    r->p = *p;
+    r->out = host_pages;
+    r->out_len = host_pages_len;
+    r->init = init_value;
+    r->est_bytes = estimate_bytes(*p);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        r->id = s->next_id++;
+        s->live[r->id] = r;
+        s->queue.push_back(r);
+    }
+    *ticket = r->id;
+    s->cv_work.notify_one();
+    return RRB_OK;
+}
+
+int rrb_server_wait(rrb_server* s, uint64_t ticket, uint64_t timeout_ns, rrb_request_result* res) {
+    if (!s) return RRB_ERR_INVARIANT;
+    std::unique_lock<std::mutex> lk(s->m);
+    auto it = s->live.find(ticket);
+    if (it == s->live.end()) return RRB_ERR_INVARIANT;
+    Request* r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_ns) {
+        if (!s->cv_done.wait_for(lk, std::chrono::nanoseconds(timeout_ns), ready)) return RRB_ERR_TIMEOUT;
+    } else {
+        s->cv_done.wait(lk, ready);
+    }
+    if (res) {
+        res->status = r->status;
+        res->latency_ns = static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(r->t_done - r->t_submit).count());
+        res->queue_ns = static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(r->t_start - r->t_submit).count());
+    }
+    const int st = r->status;
+    s->live.erase(it);
+    delete r;
+    return st;
+}
+
+int rrb_server_stats(rrb_server* s, rrb_server_stats_t* out) {
+    if (!s || !out) return RRB_ERR_INVARIANT;
+    std::lock_guard<std::mutex> lk(s->m);
+    out->completed = s->completed;
+    out->batches = s->batches;
+    out->batched_requests = s->batched_requests;
+    out->queued = s->queue.size();
+    out->in_use_bytes = s->in_use;
+    out->peak_in_use_bytes = s->peak_in_use;
+    return RRB_OK;
+}
+
+int rrb_server_destroy(rrb_server* s) {
+    if (!s) return RRB_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (std::thread& t : s->threads) t.join();
+    for (rrb_ctx* c : s->ctx) rrb_destroy(c);
+    for (auto& kv : s->live) delete kv.second;
+    delete s;
+    return RRB_OK;
+}
+
+}  // extern "C"

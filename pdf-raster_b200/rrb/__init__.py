@@ -18,10 +18,10 @@ import numpy as np
 
 from . import _abi
 from ._abi import (RRB_FILL_EVEN_ODD, RRB_FILL_NONZERO, RRB_ROWMAP_AS_SHIPPED,  # noqa: F401
-                   RRB_ROWMAP_DOCUMENTED, BatchStats, PathBatchParams, PathFillParams, SceneParams, StageTime,
-                   Tuning, VramBudget)
+                   RRB_ROWMAP_DOCUMENTED, BatchStats, PathBatchParams, PathFillParams, RequestResult, SceneParams,
+                   ServerConfig, ServerStats, StageTime, Tuning, VramBudget)
 
-__all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "lib",
+__all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "Server", "lib",
            "conic_to_cubic", "RRB_FILL_NONZERO", "RRB_FILL_EVEN_ODD", "RRB_ROWMAP_DOCUMENTED",
            "RRB_ROWMAP_AS_SHIPPED"]
 
@@ -408,3 +408,125 @@ class ResidentBatch:
         h, self.handle = self.handle, None
         if h and self.backend.handle:
             self.backend._chk(lib().rrb_batch_free(self.backend.handle, h))
+
+
+class Server:
+    """Continuous-batching page-render server (rrb_server_*)."""
+
+    def __init__(self, device: int = 0, workers: int = 2, mem_budget: int = 0, max_batch_pages: int = 64,
+                 tile: tuple[int, int] = (0, 0)):
+        cfg = ServerConfig(device=device, workers=workers, mem_budget_bytes=mem_budget,
+                           max_batch_pages=max_batch_pages, tile_w=tile[0], tile_h=tile[1])
+        h = C.c_void_p()
+        rc = lib().rrb_server_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise BackendError(rc, "rrb_server_create failed")
+        self._h = h.value
+        self._keep = {}
+
+    def submit(self, params: PathBatchParams, host_pages: np.ndarray, init: int = 255, keep=None) -> int:
+        """Queue a render; `params`' arrays and `host_pages` must live until wait()."""
+        t = C.c_uint64()
+        rc = lib().rrb_server_submit(self._h, C.byref(params), host_pages.ctypes.data, host_pages.nbytes, init,
+                                     C.byref(t))
+        if rc:
+            raise BackendError(rc, "rrb_server_submit rejected the request")
+        self._keep[t.value] = (params, host_pages, keep)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ns: int = 0) -> dict:
+        r = RequestResult()
+        rc = lib().rrb_server_wait(self._h, ticket, timeout_ns, C.byref(r))
+        self._keep.pop(ticket, None)
+        if rc:
+            raise BackendError(rc, f"request {ticket} failed")
+        return {"latency_ns": int(r.latency_ns), "queue_ns": int(r.queue_ns)}
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        lib().rrb_server_stats(self._h, C.byref(s))
+        return {n: int(getattr(s, n)) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().rrb_server_destroy(h)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+
+class MLP:
+    """The cost model's network on the device (rrb_mlp_*): 24 -> 64 -> 64 -> 1."""
+
+    N_PARAMS = _abi.RRB_MLP_PARAMS
+    N_IN = _abi.RRB_MLP_IN
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        h = C.c_void_p()
+        rc = lib().rrb_mlp_create(device, seed, C.byref(h))
+        if rc:
+            raise BackendError(rc, "rrb_mlp_create failed")
+        self._h = h.value
+
+    def close(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            lib().rrb_mlp_destroy(h)
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def _f32(a, shape=None):
+        a = np.ascontiguousarray(a, np.float32)
+        if shape is not None:
+            a = a.reshape(shape)
+        return a
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.N_PARAMS, np.float32)
+        rc = lib().rrb_mlp_get_params(self._h, _ptr(out, C.c_float))
+        if rc:
+            raise BackendError(rc, "get_params")
+        return out
+
+    def set_params(self, w):
+        w = self._f32(w)
+        assert w.size == self.N_PARAMS
+        rc = lib().rrb_mlp_set_params(self._h, _ptr(w, C.c_float))
+        if rc:
+            raise BackendError(rc, "set_params")
+
+    def loss_grad(self, X, y):
+        X, y = self._f32(X, (-1, self.N_IN)), self._f32(y)
+        g = np.empty(self.N_PARAMS, np.float32)
+        loss = C.c_float()
+        rc = lib().rrb_mlp_loss_grad(self._h, _ptr(X, C.c_float), _ptr(y, C.c_float), len(y), _ptr(g, C.c_float),
+                                     C.byref(loss))
+        if rc:
+            raise BackendError(rc, "loss_grad")
+        return float(loss.value), g
+
+    def train(self, X, y, epochs=30, batch=4096, lr=1e-3, seed=0) -> float:
+        X, y = self._f32(X, (-1, self.N_IN)), self._f32(y)
+        loss = C.c_float()
+        rc = lib().rrb_mlp_train(self._h, _ptr(X, C.c_float), _ptr(y, C.c_float), len(y), epochs, batch, lr, seed,
+                                 C.byref(loss))
+        if rc:
+            raise BackendError(rc, "train")
+        return float(loss.value)
+
+    def predict(self, X) -> np.ndarray:
+        X = self._f32(X, (-1, self.N_IN))
+        out = np.empty(len(X), np.float32)
+        rc = lib().rrb_mlp_predict(self._h, _ptr(X, C.c_float), len(X), _ptr(out, C.c_float))
+        if rc:
+            raise BackendError(rc, "predict")
+        return out

@@ -28,6 +28,9 @@ RRB_FILL_NONZERO = 0
 RRB_FILL_EVEN_ODD = 1
 RRB_ROWMAP_DOCUMENTED = 0
 RRB_ROWMAP_AS_SHIPPED = 1
+RRB_MLP_IN = 24
+RRB_MLP_HIDDEN = 64
+RRB_MLP_PARAMS = 64 * 24 + 64 + 64 * 64 + 64 + 64 + 1
 
 
 class VramBudget(C.Structure):
@@ -90,6 +93,21 @@ class StageTime(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("ms", C.c_float), ("launches", C.c_uint32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("workers", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
+                ("max_batch_pages", C.c_uint32), ("tile_w", C.c_uint32), ("tile_h", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("latency_ns", C.c_uint64), ("queue_ns", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("completed", "batches", "batched_requests", "queued", "in_use_bytes",
+                                          "peak_in_use_bytes")]
+
+
 class SceneParams(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32),
@@ -145,6 +163,21 @@ SIGNATURES = {
     "rrb_last_stage_times": (C.c_int, [VP, C.POINTER(StageTime), C.c_int, C.POINTER(C.c_int)]),
     "rrb_validate_path_batch": (C.c_int, [C.POINTER(PathBatchParams), C.c_size_t, C.c_char_p, C.c_size_t]),
     "rrb_render_pages_host": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t]),
+    "rrb_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(VP)]),
+    "rrb_server_submit": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t, C.c_uint8,
+                                    C.POINTER(C.c_uint64)]),
+    "rrb_server_wait": (C.c_int, [VP, C.c_uint64, C.c_uint64, C.POINTER(RequestResult)]),
+    "rrb_server_stats": (C.c_int, [VP, C.POINTER(ServerStats)]),
+    "rrb_server_destroy": (C.c_int, [VP]),
+    "rrb_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(VP)]),
+    "rrb_mlp_destroy": (C.c_int, [VP]),
+    "rrb_mlp_set_params": (C.c_int, [VP, C.POINTER(C.c_float)]),
+    "rrb_mlp_get_params": (C.c_int, [VP, C.POINTER(C.c_float)]),
+    "rrb_mlp_loss_grad": (C.c_int, [VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32,
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "rrb_mlp_train": (C.c_int, [VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "rrb_mlp_predict": (C.c_int, [VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float)]),
     "rrb_path_new": (VP, []),
     "rrb_path_free": (None, [VP]),
     "rrb_path_clear": (None, [VP]),

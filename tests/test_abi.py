@@ -49,6 +49,11 @@ STRUCTS = {
     "rrb_batch_stats": ("BatchStats", ["paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles",
                                        "tile_pairs", "nonterminating_rows", "kernel_launches"]),
     "rrb_stage_time": ("StageTime", ["name", "ms", "launches"]),
+    "rrb_server_config": ("ServerConfig", ["device", "workers", "mem_budget_bytes", "max_batch_pages", "tile_w",
+                                           "tile_h", "reserved"]),
+    "rrb_request_result": ("RequestResult", ["status", "latency_ns", "queue_ns"]),
+    "rrb_server_stats_t": ("ServerStats", ["completed", "batches", "batched_requests", "queued", "in_use_bytes",
+                                           "peak_in_use_bytes"]),
     "rrb_scene_params": ("SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h", "page_scale",
                                          "paths_scale", "path_cap", "reserved"]),
 }

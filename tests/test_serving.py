@@ -1,0 +1,57 @@
+"""Continuous-batching server: every request's pages are the same rendered
+alone, in a mixed batch, and by the oracle; admission respects the budget."""
+
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(rrb, n, seed0=100):
+    out = []
+    for i in range(n):
+        s = rrb.Scene(kind=2, seed=seed0 + i, n_pages=1 + (i % 2), page_scale=0.1, paths_scale=0.02)
+        out.append(s)
+    return out
+
+
+def _run(server, scenes, stagger_s=0.0):
+    pages, tickets, res = [], [], []
+    for s in scenes:
+        s.view.pages = None
+        a = s.blank_arena(0)  # overwritten: the server fills pages with `init`
+        pages.append(a)
+        tickets.append(server.submit(s.view, a, init=255, keep=s))
+        if stagger_s:
+            time.sleep(stagger_s)
+    for t in tickets:
+        res.append(server.wait(t))
+    return pages, res
+
+
+def test_same_alone_and_in_the_mix(rrb_lib, oracle):
+    scenes = _requests(rrb_lib, 10)
+    with rrb_lib.Server(workers=2, max_batch_pages=8) as srv:
+        mixed, _ = _run(srv, scenes, stagger_s=0.002)
+        st = srv.stats()
+    assert st["completed"] == 10 and st["batches"] < 10  # requests shared batches
+    with rrb_lib.Server(workers=1, max_batch_pages=1) as srv:
+        alone, _ = _run(srv, scenes)
+    for i, s in enumerate(scenes):
+        assert np.array_equal(mixed[i], alone[i]), i
+        if i < 4:
+            exp = s.blank_arena()
+            oracle.render_scene(s, exp)
+            assert np.array_equal(mixed[i], exp), i
+
+
+def test_admission_under_a_small_budget(rrb_lib):
+    scenes = _requests(rrb_lib, 6, seed0=300)
+    budget = 64 << 20
+    with rrb_lib.Server(workers=2, mem_budget=budget, max_batch_pages=16) as srv:
+        pages, res = _run(srv, scenes)
+        st = srv.stats()
+    assert st["completed"] == 6 and st["in_use_bytes"] == 0
+    assert all(r["latency_ns"] > 0 for r in res)
