@@ -33,10 +33,14 @@ def _run(server, scenes, stagger_s=0.0):
 
 def test_same_alone_and_in_the_mix(rrb_lib, oracle):
     scenes = _requests(rrb_lib, 10)
-    with rrb_lib.Server(workers=2, max_batch_pages=8) as srv:
-        mixed, _ = _run(srv, scenes, stagger_s=0.002)
+    # A large first request keeps the single worker busy while the small ones
+    # queue up behind it, so they are batched together whatever the timing.
+    blocker = rrb_lib.Scene(kind=2, seed=7, n_pages=4)
+    with rrb_lib.Server(workers=1, max_batch_pages=8) as srv:
+        mixed, _ = _run(srv, [blocker] + scenes)
         st = srv.stats()
-    assert st["completed"] == 10 and st["batches"] < 10  # requests shared batches
+    mixed = mixed[1:]
+    assert st["completed"] == 11 and st["batches"] < 11  # requests shared batches
     with rrb_lib.Server(workers=1, max_batch_pages=1) as srv:
         alone, _ = _run(srv, scenes)
     for i, s in enumerate(scenes):
