@@ -135,6 +135,42 @@ typedef struct {
 } rrb_path_fill_params;
 int rrb_record_path_fill(rrb_ctx* ctx, const rrb_path_fill_params* p);
 
+/* rrb_record_path_fill_static: the same fill, with the same parameters and
+ * the same pixels as rrb_record_path_fill, that allocates no device memory.
+ * It has no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they draw: cudaMalloc
+ * and cudaFree synchronise the whole device, which stalls every other stream
+ * of a busy serving GPU, and a process whose device memory was handed out up
+ * front (an external pool, an admission budget already granted) must not hit
+ * an out-of-memory error in the middle of a page. Every intermediate lives
+ * in one array of RRB_STATIC_SCRATCH_BYTES that the library reserves in
+ * device memory when its module loads; the array is not counted in the
+ * context's memory budget and the context's own buffers are not touched.
+ *
+ * Limits (beyond them: RRB_ERR_POOL_EXHAUSTED with the limit in
+ * rrb_last_error_message, and the page untouched): at most
+ * RRB_STATIC_MAX_POINTS points, flattening to at most RRB_STATIC_MAX_EDGES
+ * edges, at most RRB_STATIC_MAX_ROW_CROSSINGS merged crossings on any AA
+ * row, and at most RRB_STATIC_MAX_CELLS coverage cells. Larger paths go
+ * through rrb_record_path_fill.
+ *
+ * The first call on a device does the set-up: it looks up the array's
+ * device address (which loads the module holding it). Make that first call
+ * before any stream capture begins. All calls in a process share the one
+ * array per device; calls that overlapped on the device would race on it,
+ * so each call holds a process-wide lock until its own device work has
+ * finished and concurrent callers run one after another. Like
+ * rrb_record_path_fill it must come between rrb_begin_page and
+ * rrb_submit_page, runs on the context's stream and has finished when it
+ * returns. It does not update rrb_last_batch_stats. */
+#define RRB_STATIC_SCRATCH_BYTES (32u << 20)
+#define RRB_STATIC_MAX_POINTS (1u << 16)
+#define RRB_STATIC_MAX_EDGES (1u << 18)
+#define RRB_STATIC_MAX_ROW_CROSSINGS 128
+#define RRB_STATIC_MAX_CELLS 2801024u
+int rrb_record_path_fill_static(rrb_ctx* ctx, const rrb_path_fill_params* p);
+
 /* Many paths over many pages in one submission (the batched form). All
  * arrays are HOST memory; the backend uploads them and renders every path,
  * in index order per page, into device pages. Paths on different pages are

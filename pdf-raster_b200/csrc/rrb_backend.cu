@@ -755,6 +755,13 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
 
 }  // namespace
 
+// Library-internal hooks for the other translation units (C++ linkage, not
+// part of the C ABI): the context's device, whether a page is open, and its
+// last error message.
+int rrb_ctx_device(const rrb_ctx* c) { return c->device; }
+bool rrb_ctx_page_open(const rrb_ctx* c) { return c->in_page; }
+int rrb_ctx_fail(rrb_ctx* c, int code, const char* msg) { return set_err(c, code, msg); }
+
 extern "C" {
 
 const char* rrb_version(void) { return "rrb 0.1 sm_100a"; }

@@ -327,6 +327,33 @@ class B200Backend:
         p.width, p.height = width, height
         self._chk(lib().rrb_record_path_fill(self._h, C.byref(p)))
 
+    def record_path_fill_static(self, pts, flags, page: DeviceBuffer, width: int, height: int, *, fill_rule=0,
+                                gray=0, alpha=255, rowmap=RRB_ROWMAP_DOCUMENTED, matrix=IDENTITY, flatness=0.1,
+                                page_offset=0):
+        """record_path_fill without device allocation (rrb_record_path_fill_static)."""
+        self._chk(lib().rrb_record_path_fill_static(
+            self._h, C.byref(self._fill_params(pts, flags, page, width, height, fill_rule, gray, alpha, rowmap,
+                                               matrix, flatness, page_offset))))
+
+    @staticmethod
+    def _fill_params(pts, flags, page, width, height, fill_rule, gray, alpha, rowmap, matrix, flatness,
+                     page_offset) -> PathFillParams:
+        pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+        flags = np.ascontiguousarray(flags, np.uint8)
+        p = PathFillParams()
+        p._keep = (pts, flags)
+        p.pts = _ptr(pts, C.c_double)
+        p.flags = _ptr(flags, C.c_uint8)
+        p.n_pts = flags.size
+        for i in range(6):
+            p.matrix[i] = matrix[i]
+        p.flatness = flatness
+        p.fill_rule, p.gray, p.alpha, p.rowmap = fill_rule, gray, alpha, rowmap
+        p.page = page.handle
+        p.page_offset = page_offset
+        p.width, p.height = width, height
+        return p
+
     def record_path_batch(self, params: PathBatchParams):
         self._chk(lib().rrb_record_path_batch(self._h, C.byref(params)))
 

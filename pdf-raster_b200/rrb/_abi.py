@@ -28,6 +28,11 @@ RRB_FILL_NONZERO = 0
 RRB_FILL_EVEN_ODD = 1
 RRB_ROWMAP_DOCUMENTED = 0
 RRB_ROWMAP_AS_SHIPPED = 1
+RRB_STATIC_SCRATCH_BYTES = 32 << 20
+RRB_STATIC_MAX_POINTS = 1 << 16
+RRB_STATIC_MAX_EDGES = 1 << 18
+RRB_STATIC_MAX_ROW_CROSSINGS = 128
+RRB_STATIC_MAX_CELLS = 2801024
 RRB_MLP_IN = 24
 RRB_MLP_HIDDEN = 64
 RRB_MLP_PARAMS = 64 * 24 + 64 + 64 * 64 + 64 + 64 + 1
@@ -150,6 +155,7 @@ SIGNATURES = {
     "rrb_submit_page": (C.c_int, [VP, C.POINTER(C.c_uint64)]),
     "rrb_wait_page": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
     "rrb_record_path_fill": (C.c_int, [VP, C.POINTER(PathFillParams)]),
+    "rrb_record_path_fill_static": (C.c_int, [VP, C.POINTER(PathFillParams)]),
     "rrb_record_path_batch": (C.c_int, [VP, C.POINTER(PathBatchParams)]),
     "rrb_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "rrb_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
