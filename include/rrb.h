@@ -171,6 +171,52 @@ int rrb_record_path_fill(rrb_ctx* ctx, const rrb_path_fill_params* p);
 #define RRB_STATIC_MAX_CELLS 2801024u
 int rrb_record_path_fill_static(rrb_ctx* ctx, const rrb_path_fill_params* p);
 
+/* ---- the reference's coverage operators (record_aa_fill / record_tile_fill) ----
+ * Same parameter layouts as AaFillParams / TileFillParams
+ * (crates/gpu/src/backend/params.rs:90-103,170-185) and the same contract:
+ * device buffers in, a u8 coverage buffer of width x height written (every
+ * byte), no compositing, queued on the context's stream inside
+ * begin_page/submit_page. fill_rule: 0 nonzero, anything else even-odd. */
+typedef struct {
+    const rrb_buf* segs;      /* device f32 [n_segs][4] = {x0, y0, x1, y1}, coverage-local pixels, 16-B aligned */
+    uint32_t n_segs;
+    const rrb_buf* coverage;  /* device u8 [height][width] */
+    uint32_t width, height;
+    uint8_t fill_rule;
+} rrb_aa_fill_params;
+/* 64 Halton(2,3) samples per pixel, coverage = (hits * 255 + 32) >> 6;
+ * bit-identical to aa_fill_cpu (crates/gpu/src/fill.rs:346-421). */
+int rrb_record_aa_fill(rrb_ctx* ctx, const rrb_aa_fill_params* p);
+/* The 64 sample offsets (x, y in [0,1)) the operator uses. */
+void rrb_aa_fill_jitter(float* x64, float* y64);
+
+/* TileRecord (crates/gpu/src/fill.rs:12-39; tile_fill.cu), 32 bytes. */
+typedef struct {
+    uint32_t key;       /* (tile_y << 16) | tile_x */
+    float x_enter;      /* tile-local x at y0_tile */
+    float dxdy;
+    float y0_tile, y1_tile;
+    float sign;         /* +1 / -1 */
+    uint32_t pad, pad2;
+} rrb_tile_record;
+typedef struct {
+    const rrb_buf* records;      /* device rrb_tile_record[], sorted by key */
+    const rrb_buf* tile_starts;  /* device u32 [grid_w * grid_h], grid_w = ceil(width / 16) */
+    const rrb_buf* tile_counts;  /* device u32 [grid_w * grid_h] */
+    const rrb_buf* coverage;     /* device u8 [height][width] */
+    uint32_t width, height;
+    uint8_t fill_rule;
+} rrb_tile_fill_params;
+/* Analytic signed-area coverage per 16x16 tile (tile_fill.cu:60-177), every
+ * operation in IEEE f32 as written. A tile whose record range runs past the
+ * records buffer is filled as empty. */
+int rrb_record_tile_fill(rrb_ctx* ctx, const rrb_tile_fill_params* p);
+/* tile_fill from segments: the tile records are built on the device
+ * (build_tile_records, crates/gpu/src/fill.rs:82-264, with a stable key
+ * sort) and kept in the context's scratch. Synchronises once, to size the
+ * records; *n_records (optional) receives their count. */
+int rrb_record_tile_fill_segs(rrb_ctx* ctx, const rrb_aa_fill_params* p, uint64_t* n_records);
+
 /* Many paths over many pages in one submission (the batched form). All
  * arrays are HOST memory; the backend uploads them and renders every path,
  * in index order per page, into device pages. Paths on different pages are

@@ -47,9 +47,8 @@ _LIB = None
 
 def build(arch: str | None = None) -> Path:
     """Compile the oracle if needed. `arch` overrides -march (default x86-64-v3, portable to any AVX2 host)."""
-    src = HERE / "rr_oracle.cpp"
-    if LIB_PATH.exists() and LIB_PATH.stat().st_mtime >= max(src.stat().st_mtime,
-                                                              (HERE / "rr_oracle.h").stat().st_mtime):
+    srcs = [HERE / n for n in ("rr_oracle.cpp", "rr_oracle.h", "fill_oracle.cpp", "fill_oracle.h", "Makefile")]
+    if LIB_PATH.exists() and LIB_PATH.stat().st_mtime >= max(p.stat().st_mtime for p in srcs):
         return LIB_PATH
     env = dict(os.environ)
     cmd = ["make", "-C", str(HERE), f"ARCHFLAGS=-march={arch or 'x86-64-v3'}"]
@@ -97,6 +96,14 @@ def lib() -> C.CDLL:
                                        C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
                                        C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D), D, C.c_int, C.c_int,
                                        C.POINTER(Stats)]),
+            "or_aa_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+            "or_aa_fill_cpu": (None, [C.POINTER(C.c_float), C.c_uint32, C.c_float, C.c_float, C.c_uint32,
+                                      C.c_uint32, C.c_int, C.POINTER(U8)]),
+            "or_build_tile_records": (I64, [C.POINTER(C.c_float), C.c_uint32, C.c_float, C.c_float, C.c_uint32,
+                                            C.c_uint32, VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                            C.POINTER(C.c_uint32)]),
+            "or_tile_fill": (None, [VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.c_int, C.POINTER(U8)]),
         }
         for n, (r, a) in sig.items():
             f = getattr(L, n)
@@ -305,3 +312,54 @@ def render_scene(scene, arena: np.ndarray, rowmap=ROWMAP_DOCUMENTED, threads=1) 
     return render_arrays(arena, scene.page_offset, scene.page_width, scene.page_height, scene.pts, scene.flags,
                          scene.path_pt_off, scene.fill_rule, scene.gray, scene.alpha, scene.path_page,
                          rowmap=rowmap, threads=threads)
+
+
+# ---- F1: the reference's GPU fill operators (fill.rs, tile_fill.cu) -------------
+TILE_RECORD = np.dtype([("key", "<u4"), ("x_enter", "<f4"), ("dxdy", "<f4"), ("y0_tile", "<f4"),
+                        ("y1_tile", "<f4"), ("sign", "<f4"), ("pad", "<u4"), ("pad2", "<u4")])
+
+
+def aa_jitter():
+    """The oracle's 64 sample offsets (x, y) as f32 arrays."""
+    x, y = np.zeros(64, np.float32), np.zeros(64, np.float32)
+    lib().or_aa_jitter(_p(x, C.c_float), _p(y, C.c_float))
+    return x, y
+
+
+def aa_fill_cpu(segs, x_min, y_min, width, height, eo=False):
+    """aa_fill_cpu (fill.rs:346-398): u8 coverage [height, width] from f32 segs [n, 4]."""
+    segs = np.ascontiguousarray(segs, np.float32).reshape(-1)
+    out = np.zeros(width * height, np.uint8)
+    lib().or_aa_fill_cpu(_p(segs, C.c_float), segs.size // 4, x_min, y_min, width, height, int(eo),
+                         _p(out, C.c_uint8))
+    return out.reshape(height, width)
+
+
+def build_tile_records(segs, x_min, y_min, width, height):
+    """build_tile_records (fill.rs:82-264) with a stable key sort: (records, starts, counts, grid_w)."""
+    segs = np.ascontiguousarray(segs, np.float32).reshape(-1)
+    gw = C.c_uint32()
+    n = lib().or_build_tile_records(_p(segs, C.c_float), segs.size // 4, x_min, y_min, width, height, None, None,
+                                    None, C.byref(gw))
+    if n < 0:
+        raise ValueError("raster too large for 16-bit tile keys")
+    grid_w, grid_h = gw.value, (height + 15) // 16
+    recs = np.zeros(max(n, 1), TILE_RECORD)
+    starts = np.zeros(grid_w * grid_h, np.uint32)
+    counts = np.zeros(grid_w * grid_h, np.uint32)
+    lib().or_build_tile_records(_p(segs, C.c_float), segs.size // 4, x_min, y_min, width, height,
+                                recs.ctypes.data, _p(starts, C.c_uint32), _p(counts, C.c_uint32), C.byref(gw))
+    return recs[:n], starts, counts, grid_w
+
+
+def tile_fill(records, starts, counts, grid_w, width, height, eo=False):
+    """tile_fill (tile_fill.cu:132-177), IEEE f32 as written: u8 coverage [height, width]."""
+    records = np.ascontiguousarray(records, TILE_RECORD)
+    if records.size == 0:
+        records = np.zeros(1, TILE_RECORD)
+    starts = np.ascontiguousarray(starts, np.uint32)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    out = np.zeros(width * height, np.uint8)
+    lib().or_tile_fill(records.ctypes.data, _p(starts, C.c_uint32), _p(counts, C.c_uint32), grid_w, width, height,
+                       int(eo), _p(out, C.c_uint8))
+    return out.reshape(height, width)

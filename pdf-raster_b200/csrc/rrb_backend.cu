@@ -64,6 +64,7 @@ struct rrb_ctx {
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
     Scratch s_run_off, s_runs;
+    Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
@@ -761,6 +762,16 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
 int rrb_ctx_device(const rrb_ctx* c) { return c->device; }
 bool rrb_ctx_page_open(const rrb_ctx* c) { return c->in_page; }
 int rrb_ctx_fail(rrb_ctx* c, int code, const char* msg) { return set_err(c, code, msg); }
+int rrb_ctx_sm_count(const rrb_ctx* c) { return c->sm_count; }
+// Scratch slot k (0..7) of the fill operators, grown to at least `bytes`
+// within the context's memory budget; contents are not kept across growth.
+int rrb_ctx_fill_scratch(rrb_ctx* c, int k, size_t bytes, void** out) {
+    if (k < 0 || k >= 8) return set_err(c, RRB_ERR_INVARIANT, "fill scratch slot out of range");
+    int rc = ensure(c, c->s_fill[k], bytes);
+    if (rc) return rc;
+    *out = c->s_fill[k].p;
+    return RRB_OK;
+}
 
 extern "C" {
 
@@ -826,6 +837,7 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
+    for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);
         delete c->tmp_batch;

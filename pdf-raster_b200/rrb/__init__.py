@@ -354,6 +354,29 @@ class B200Backend:
         p.width, p.height = width, height
         return p
 
+    # ---- the reference's coverage operators (record_aa_fill / record_tile_fill)
+    def record_aa_fill(self, segs: DeviceBuffer, n_segs: int, coverage: DeviceBuffer, width: int, height: int,
+                       fill_rule: int = 0):
+        p = _abi.AaFillParams(segs=segs.handle, n_segs=n_segs, coverage=coverage.handle, width=width,
+                              height=height, fill_rule=fill_rule)
+        self._chk(lib().rrb_record_aa_fill(self._h, C.byref(p)))
+
+    def record_tile_fill(self, records: DeviceBuffer, tile_starts: DeviceBuffer, tile_counts: DeviceBuffer,
+                         coverage: DeviceBuffer, width: int, height: int, fill_rule: int = 0):
+        p = _abi.TileFillParams(records=records.handle, tile_starts=tile_starts.handle,
+                                tile_counts=tile_counts.handle, coverage=coverage.handle, width=width,
+                                height=height, fill_rule=fill_rule)
+        self._chk(lib().rrb_record_tile_fill(self._h, C.byref(p)))
+
+    def record_tile_fill_segs(self, segs: DeviceBuffer, n_segs: int, coverage: DeviceBuffer, width: int,
+                              height: int, fill_rule: int = 0) -> int:
+        """tile_fill with the records built on the device; returns the record count."""
+        p = _abi.AaFillParams(segs=segs.handle, n_segs=n_segs, coverage=coverage.handle, width=width,
+                              height=height, fill_rule=fill_rule)
+        n = C.c_uint64()
+        self._chk(lib().rrb_record_tile_fill_segs(self._h, C.byref(p), C.byref(n)))
+        return int(n.value)
+
     def record_path_batch(self, params: PathBatchParams):
         self._chk(lib().rrb_record_path_batch(self._h, C.byref(params)))
 
@@ -487,6 +510,13 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def aa_fill_jitter() -> tuple[np.ndarray, np.ndarray]:
+    """The 64 (x, y) sample offsets of rrb_record_aa_fill."""
+    x, y = np.zeros(64, np.float32), np.zeros(64, np.float32)
+    lib().rrb_aa_fill_jitter(_ptr(x, C.c_float), _ptr(y, C.c_float))
+    return x, y
 
 
 class MLP:

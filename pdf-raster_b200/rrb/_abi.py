@@ -61,6 +61,21 @@ class PathFillParams(C.Structure):
     ]
 
 
+class AaFillParams(C.Structure):
+    _fields_ = [("segs", C.c_void_p), ("n_segs", C.c_uint32), ("coverage", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("fill_rule", C.c_uint8)]
+
+
+class TileRecord(C.Structure):
+    _fields_ = [("key", C.c_uint32), ("x_enter", C.c_float), ("dxdy", C.c_float), ("y0_tile", C.c_float),
+                ("y1_tile", C.c_float), ("sign", C.c_float), ("pad", C.c_uint32), ("pad2", C.c_uint32)]
+
+
+class TileFillParams(C.Structure):
+    _fields_ = [("records", C.c_void_p), ("tile_starts", C.c_void_p), ("tile_counts", C.c_void_p), ("coverage", C.c_void_p),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("fill_rule", C.c_uint8)]
+
+
 class PathBatchParams(C.Structure):
     _fields_ = [
         ("pts", C.POINTER(C.c_double)),
@@ -156,6 +171,10 @@ SIGNATURES = {
     "rrb_wait_page": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
     "rrb_record_path_fill": (C.c_int, [VP, C.POINTER(PathFillParams)]),
     "rrb_record_path_fill_static": (C.c_int, [VP, C.POINTER(PathFillParams)]),
+    "rrb_record_aa_fill": (C.c_int, [VP, C.POINTER(AaFillParams)]),
+    "rrb_aa_fill_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "rrb_record_tile_fill": (C.c_int, [VP, C.POINTER(TileFillParams)]),
+    "rrb_record_tile_fill_segs": (C.c_int, [VP, C.POINTER(AaFillParams), C.POINTER(C.c_uint64)]),
     "rrb_record_path_batch": (C.c_int, [VP, C.POINTER(PathBatchParams)]),
     "rrb_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "rrb_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),

@@ -54,6 +54,10 @@ STRUCTS = {
     "rrb_request_result": ("RequestResult", ["status", "latency_ns", "queue_ns"]),
     "rrb_server_stats_t": ("ServerStats", ["completed", "batches", "batched_requests", "queued", "in_use_bytes",
                                            "peak_in_use_bytes"]),
+    "rrb_aa_fill_params": ("AaFillParams", ["segs", "n_segs", "coverage", "width", "height", "fill_rule"]),
+    "rrb_tile_record": ("TileRecord", ["key", "x_enter", "dxdy", "y0_tile", "y1_tile", "sign", "pad", "pad2"]),
+    "rrb_tile_fill_params": ("TileFillParams", ["records", "tile_starts", "tile_counts", "coverage", "width",
+                                                "height", "fill_rule"]),
     "rrb_scene_params": ("SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h", "page_scale",
                                          "paths_scale", "path_cap", "reserved"]),
 }
