@@ -354,6 +354,21 @@ int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32
                   float lr, uint64_t seed, float* final_loss);
 int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out);
 
+/* ---- cost-model features ------------------------------------------------------
+ * RRB_MLP_IN floats describing page `page` of a batch for composite tile
+ * shape tile_w x tile_h (16x16, 32x32 or 64x16), computed on the host from
+ * the batch's arrays in one pass (no device work):
+ *   0 log1p(pixels)            1 log1p(paths)          2 log1p(points)
+ *   3 line / (line + curve)    4 log1p(curves)         5 log1p(est. flattened edges)
+ *   6 log1p(mean segment len)  7 log1p(sum path-box area / page area)
+ *   8 log1p(mean path-box area) 9 even-odd fraction    10 alpha < 255 fraction
+ *  11 rectilinear fraction     12 fraction of tiles under some path box
+ *  13-20 fraction of tiles whose path-box count is 0, 1-3, 4-15, 16-63, 64-255, 256-1023,
+ *        1024-4095, >= 4096
+ *  21-23 tile shape one-hot (16x16, 32x32, 64x16) */
+int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, uint32_t tile_w, uint32_t tile_h,
+                      float* out);
+
 /* ---- path construction on the host (A1, A2) --------------------------------
  * PathBuilder::{move_to, line_to, curve_to, close} (crates/raster/src/path/
  * mod.rs:310-448) and conic_to_cubic (crates/font/src/outline.rs:106-112). */

@@ -91,39 +91,46 @@ int cuda_err(rrb_ctx* c, cudaError_t e, const char* what) {
         if (e__ != cudaSuccess) return cuda_err(ctx, e__, #call); \
     } while (0)
 
-int dev_alloc(rrb_ctx* c, size_t bytes, void** out) {
+// Device memory within the context's budget. Scratch (`ordered`) comes from
+// the device's stream-ordered pool on the context's stream: allocating and
+// freeing it neither synchronises the device nor waits for other streams,
+// so contexts on other host threads (server workers) keep running while one
+// of them grows its scratch. Buffers handed to the caller use cudaMalloc.
+int dev_alloc(rrb_ctx* c, size_t bytes, void** out, bool ordered = false) {
     if (c->budget && c->used + bytes > c->budget)
         return set_err(c, RRB_ERR_OUT_OF_MEMORY,
                        "device allocation of " + std::to_string(bytes) + " bytes exceeds the budget");
-    cudaError_t e = cudaMalloc(out, bytes);
+    cudaError_t e = ordered ? cudaMallocAsync(out, bytes, c->stream) : cudaMalloc(out, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return set_err(c, RRB_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        return set_err(c, RRB_ERR_OUT_OF_MEMORY, std::string(ordered ? "cudaMallocAsync: " : "cudaMalloc: ") +
+                                                     cudaGetErrorString(e));
     }
     c->used += bytes;
     return RRB_OK;
 }
 
-void dev_free(rrb_ctx* c, void* p, size_t bytes) {
+void dev_free(rrb_ctx* c, void* p, size_t bytes, bool ordered = false) {
     if (!p) return;
-    cudaFree(p);
+    if (ordered) cudaFreeAsync(p, c->stream);
+    else cudaFree(p);
     c->used -= std::min<uint64_t>(c->used, bytes);
 }
 
-// Grow a scratch buffer to at least `bytes` (x1.25 headroom); contents are not kept.
+// Grow a scratch buffer to at least `bytes` (x1.25 headroom); contents are not
+// kept. The old buffer is released in stream order, after the work queued on
+// the context's stream that still reads it.
 int ensure(rrb_ctx* c, Scratch& s, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (s.cap >= bytes) return RRB_OK;
     if (s.p) {
-        cudaError_t e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamSynchronize");
-        dev_free(c, s.p, s.cap);
+        dev_free(c, s.p, s.cap, true);
         s.p = nullptr;
         s.cap = 0;
     }
     size_t want = bytes + bytes / 4;
     want = (want + 255) & ~size_t(255);
-    int rc = dev_alloc(c, want, &s.p);
+    int rc = dev_alloc(c, want, &s.p, true);
     if (rc) return rc;
     s.cap = want;
     return RRB_OK;
@@ -329,7 +336,7 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
             s->cap = 0;
             continue;
         }
-        dev_free(c, s->p, s->cap);
+        dev_free(c, s->p, s->cap, true);
         s->p = nullptr;
         s->cap = 0;
     }
@@ -637,10 +644,14 @@ void release_scratch(rrb_ctx* c) {
                       &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
     for (Scratch* x : all) {
-        dev_free(c, x->p, x->cap);
+        dev_free(c, x->p, x->cap, true);
         x->p = nullptr;
         x->cap = 0;
     }
+    // Hand the freed scratch back to the device, not just to the pool.
+    cudaStreamSynchronize(c->stream);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
 }
 
 // Pages [pg0, pg1) of B as a batch of their own: the inputs are views into
@@ -812,6 +823,14 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
         delete c;
         return RRB_ERR_DEVICE;
     }
+    // Scratch comes from the device's default stream-ordered pool; keep what
+    // is freed there cached for the next batch instead of returning it to the
+    // device at every synchronisation.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     e = cudaMallocHost(reinterpret_cast<void**>(&c->h_read), 4096);
     if (e != cudaSuccess) {
         cudaStreamDestroy(c->stream);
@@ -836,8 +855,8 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
-    for (Scratch* s : all) dev_free(c, s->p, s->cap);
-    for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap);
+    for (Scratch* s : all) dev_free(c, s->p, s->cap, true);
+    for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap, true);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);
         delete c->tmp_batch;

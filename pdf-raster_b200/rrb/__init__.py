@@ -512,6 +512,18 @@ class Server:
         self.close()
 
 
+TILE_SHAPES = ((16, 16), (32, 32), (64, 16))
+
+
+def page_features(params: PathBatchParams, page: int, tile: tuple[int, int]) -> np.ndarray:
+    """The cost model's 24 features of one page for one tile shape (rrb_page_features)."""
+    out = np.zeros(_abi.RRB_MLP_IN, np.float32)
+    rc = lib().rrb_page_features(C.byref(params), page, tile[0], tile[1], _ptr(out, C.c_float))
+    if rc:
+        raise BackendError(rc, "rrb_page_features")
+    return out
+
+
 def aa_fill_jitter() -> tuple[np.ndarray, np.ndarray]:
     """The 64 (x, y) sample offsets of rrb_record_aa_fill."""
     x, y = np.zeros(64, np.float32), np.zeros(64, np.float32)

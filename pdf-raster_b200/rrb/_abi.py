@@ -194,6 +194,8 @@ SIGNATURES = {
     "rrb_server_wait": (C.c_int, [VP, C.c_uint64, C.c_uint64, C.POINTER(RequestResult)]),
     "rrb_server_stats": (C.c_int, [VP, C.POINTER(ServerStats)]),
     "rrb_server_destroy": (C.c_int, [VP]),
+    "rrb_page_features": (C.c_int, [C.POINTER(PathBatchParams), C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.POINTER(C.c_float)]),
     "rrb_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(VP)]),
     "rrb_mlp_destroy": (C.c_int, [VP]),
     "rrb_mlp_set_params": (C.c_int, [VP, C.POINTER(C.c_float)]),
