@@ -361,47 +361,65 @@ def page_requests(rrb, scene):
     return out
 
 
+def serve_rates(srv, reqs, rates, n_req, seed=0):
+    """Poisson arrivals at each rate; latency percentiles of the completed requests."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for rate in rates:
+        gaps = rng.exponential(1.0 / rate, n_req)
+        outs = [np.empty(reqs[i % len(reqs)][2], np.uint8) for i in range(n_req)]
+        tickets = []
+        t0 = time.perf_counter()
+        due = t0
+        for i in range(n_req):
+            due += gaps[i]
+            dt = due - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            p, k, _ = reqs[i % len(reqs)]
+            tickets.append(srv.submit(p, outs[i], keep=k))
+        res = [srv.wait(t) for t in tickets]
+        lat = [r["latency_ns"] / 1e6 for r in res]
+        wall = time.perf_counter() - t0
+        px = sum(reqs[i % len(reqs)][2] for i in range(n_req))
+        out.append({"rate_pages_s": rate, "requests": n_req, "completed_pages_s": n_req / wall,
+                    "mpixel_s": px / wall / 1e6, "p50_ms": float(np.percentile(lat, 50)),
+                    "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99)),
+                    "mean_ms": float(np.mean(lat))})
+    return out
+
+
 def run_serving(args, rank, world):
-    """Poisson page-render requests against the continuous-batching server."""
+    """Poisson page-render requests against the continuous-batching server,
+    first in arrival order with the default tile, then with the cost model
+    (shortest predicted first, tile shape per batch from the model)."""
     if rank != 0:
         return
     import rrb
+    from rrb.autotune import CostModel
     scene = rrb.Scene(kind=2, seed=0)
     reqs = page_requests(rrb, scene)
     rates = [float(r) for r in args.rates.split(",")]
-    rng = np.random.default_rng(0)
-    results = []
-    with rrb.Server(workers=args.workers, mem_budget=args.mem_budget_gb << 30, max_batch_pages=64) as srv:
-        # warm-up: every distinct page once
-        warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n in reqs[:8]]
-        for t in warm:
-            srv.wait(t)
-        for rate in rates:
-            n = args.requests
-            gaps = rng.exponential(1.0 / rate, n)
-            outs = [np.empty(reqs[i % len(reqs)][2], np.uint8) for i in range(n)]
-            tickets = []
-            t0 = time.perf_counter()
-            due = t0
-            for i in range(n):
-                due += gaps[i]
-                dt = due - time.perf_counter()
-                if dt > 0:
-                    time.sleep(dt)
-                p, k, _ = reqs[i % len(reqs)]
-                tickets.append(srv.submit(p, outs[i], keep=k))
-            lat = [srv.wait(t)["latency_ns"] / 1e6 for t in tickets]
-            wall = time.perf_counter() - t0
-            px = sum(reqs[i % len(reqs)][2] for i in range(n))
-            results.append({"rate_pages_s": rate, "requests": n, "completed_pages_s": n / wall,
-                            "mpixel_s": px / wall / 1e6, "p50_ms": float(np.percentile(lat, 50)),
-                            "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99))})
-        st = srv.stats()
+    model_path = Path(args.cost_model)
+    policies = ["arrival_order"] + (["cost_model"] if model_path.exists() else [])
+    report = {}
+    for policy in policies:
+        with rrb.Server(workers=args.workers, mem_budget=args.mem_budget_gb << 30, max_batch_pages=64) as srv:
+            if policy == "cost_model":
+                srv.set_cost_model(CostModel.load(model_path))
+            # warm-up: every distinct page, queued at once, twice (scratch reaches its working size)
+            for _ in range(2):
+                warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n in reqs]
+                for t in warm:
+                    srv.wait(t)
+            report[policy] = {"rates": serve_rates(srv, reqs, rates, args.requests), "server_stats": srv.stats()}
+    best = report.get("cost_model", report["arrival_order"])
     line = {"metric": "p99 page latency under Poisson load (continuous batching)", "unit": "ms",
-            "value": results[-1]["p99_ms"], "higher_is_better": False, "n_gpus": 1,
+            "value": best["rates"][-1]["p99_ms"], "higher_is_better": False, "n_gpus": 1,
             "config": {"workload": "requests = single pages of the mixed 64-page scene (seed 0), cycled",
-                       "workers": args.workers, "mem_budget_gb": args.mem_budget_gb},
-            "serving": results, "server_stats": st}
+                       "workers": args.workers, "mem_budget_gb": args.mem_budget_gb,
+                       "cost_model": str(model_path) if model_path.exists() else None},
+            "serving": report}
     print(json.dumps(line), flush=True)
 
 
@@ -423,6 +441,7 @@ def main():
     ap.add_argument("--requests", type=int, default=128)
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--mem-budget-gb", type=int, default=60)
+    ap.add_argument("--cost-model", default=str(ROOT / "pdf-raster_b200" / "rrb" / "cost_model.npz"))
     args = ap.parse_args()
     rank, local, world = dist_env()
     if args.serving:

@@ -326,6 +326,7 @@ typedef struct {
 } rrb_request_result;
 typedef struct {
     uint64_t completed, batches, batched_requests, queued, in_use_bytes, peak_in_use_bytes;
+    uint64_t tile_batches[3]; /* batches rendered with 16x16, 32x32, 64x16 tiles */
 } rrb_server_stats_t;
 int rrb_server_create(const rrb_server_config* cfg, rrb_server** out);
 int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* host_pages, size_t host_pages_len,
@@ -333,6 +334,29 @@ int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* ho
 int rrb_server_wait(rrb_server* s, uint64_t ticket, uint64_t timeout_ns, rrb_request_result* res);
 int rrb_server_stats(rrb_server* s, rrb_server_stats_t* out);
 int rrb_server_destroy(rrb_server* s);
+
+/* The scheduler's cost model (trained by rrb.autotune): the MLP of the
+ * rrb_mlp_* section predicts log device ms of each queued page for each tile
+ * shape from rrb_page_features, normalised by x_mean / x_std, and
+ * ms = exp(y * y_std + y_mean). With RRB_SCHED_SHORTEST_FIRST, batches admit
+ * queued requests by predicted time, shortest first (arrival order
+ * otherwise); with RRB_SCHED_TILE_BY_MODEL each batch renders with the tile
+ * shape of least predicted total time — from the autotuner table (16
+ * entries, index page-size bin * 4 + edge-density bin, value 0..2 in the
+ * order 16x16, 32x32, 64x16) when params is NULL, and 64x16 when both are
+ * NULL. Features and predictions are computed in rrb_server_submit. Set the
+ * model before submitting requests. */
+#define RRB_SCHED_SHORTEST_FIRST 1u
+#define RRB_SCHED_TILE_BY_MODEL 2u
+typedef struct {
+    const float* params;   /* RRB_MLP_PARAMS floats, or NULL */
+    const float* x_mean;   /* RRB_MLP_IN floats (with params) */
+    const float* x_std;
+    float y_mean, y_std;
+    const int32_t* table;  /* [16], or NULL */
+    uint32_t policy;       /* RRB_SCHED_* bits */
+} rrb_server_cost_model;
+int rrb_server_set_cost_model(rrb_server* s, const rrb_server_cost_model* m);
 
 /* ---- learned cost model -----------------------------------------------------
  * FP32 MLP RRB_MLP_IN -> 64 -> 64 -> 1 (ReLU) predicting log render time of a

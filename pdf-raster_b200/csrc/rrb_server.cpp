@@ -8,9 +8,15 @@
 // batches are on the device joins the next batch that has room, so work from
 // different requests overlaps on the device across workers. Each request's
 // pages come back to its own host buffer; latency is submit -> pages on host.
+//
+// With a cost model (rrb_server_set_cost_model) every request gets, at
+// submit, the predicted device time of its pages for each tile shape; batches
+// then admit queued requests shortest-predicted first and/or render with the
+// tile shape of least predicted total time (autotuner table as fallback).
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -34,8 +40,13 @@ struct Request {
     uint64_t est_bytes = 0;
     int status = RRB_OK;
     bool done = false;
+    float pred[3] = {0, 0, 0};  // predicted device ms per tile shape (cost model)
+    float pred_best = 0;
+    int table_shape = -1;       // autotuner table's shape for its largest page
     Clock::time_point t_submit, t_start, t_done;
 };
+
+constexpr uint32_t kTiles[3][2] = {{16, 16}, {32, 32}, {64, 16}};
 
 }  // namespace
 
@@ -50,7 +61,15 @@ struct rrb_server {
     uint64_t next_id = 1;
     uint64_t in_use = 0, peak_in_use = 0;
     uint64_t batches = 0, batched_requests = 0, completed = 0;
+    uint64_t tile_batches[3] = {0, 0, 0};
     bool stop = false;
+    // Cost model (set before traffic; read by submitters and workers).
+    std::mutex mlp_mu;
+    rrb_mlp* mlp = nullptr;
+    bool have_params = false, have_table = false;
+    uint32_t policy = 0;
+    float x_mean[RRB_MLP_IN], x_std[RRB_MLP_IN], y_mean = 0, y_std = 1;
+    int32_t table[16];
 };
 
 namespace {
@@ -84,6 +103,11 @@ void worker(rrb_server* s, int wi) {
             s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
             if (s->stop && s->queue.empty()) break;
             uint32_t pages = 0;
+            if (s->policy & RRB_SCHED_SHORTEST_FIRST) {
+                // Shortest predicted first (stable: arrival order among equals).
+                std::stable_sort(s->queue.begin(), s->queue.end(),
+                                 [](const Request* a, const Request* b) { return a->pred_best < b->pred_best; });
+            }
             while (!s->queue.empty()) {
                 Request* r = s->queue.front();
                 const bool fits = s->in_use + bytes + r->est_bytes <= s->cfg.mem_budget_bytes || s->cfg.mem_budget_bytes == 0;
@@ -103,6 +127,32 @@ void worker(rrb_server* s, int wi) {
             s->peak_in_use = std::max(s->peak_in_use, s->in_use);
             s->batches += 1;
             s->batched_requests += batch.size();
+        }
+        // Tile shape of this batch.
+        int shape = -1;
+        if (s->policy & RRB_SCHED_TILE_BY_MODEL) {
+            if (s->have_params) {
+                float tot[3] = {0, 0, 0};
+                for (Request* r : batch)
+                    for (int k = 0; k < 3; ++k) tot[k] += r->pred[k];
+                shape = static_cast<int>(std::min_element(tot, tot + 3) - tot);
+            } else if (s->have_table) {
+                shape = batch.front()->table_shape;
+            }
+        }
+        if (shape < 0 && s->cfg.tile_w && s->cfg.tile_h) {
+            for (int k = 0; k < 3; ++k)
+                if (kTiles[k][0] == s->cfg.tile_w && kTiles[k][1] == s->cfg.tile_h) shape = k;
+        }
+        if (shape < 0) shape = 2;
+        {
+            rrb_tuning t{};
+            t.tile_w = kTiles[shape][0];
+            t.tile_h = kTiles[shape][1];
+            t.wave_points = 0xFFFFFFFFu;
+            rrb_set_tuning(c, &t);
+            std::lock_guard<std::mutex> lk(s->m);
+            s->tile_batches[shape] += 1;
         }
         const auto t_start = Clock::now();
         // Concatenate the requests into one batch over one device arena.
@@ -188,9 +238,74 @@ void worker(rrb_server* s, int wi) {
     if (arena) rrb_free_device(c, arena);
 }
 
+// Cost-model predictions of one request (per tile shape, summed over its
+// pages) and the table's shape for its largest page.
+int predict_request(rrb_server* s, Request* r) {
+    const uint32_t n = r->p.n_pages;
+    std::vector<float> X(static_cast<size_t>(n) * 3 * RRB_MLP_IN);
+    uint64_t biggest = 0;
+    for (uint32_t pg = 0; pg < n; ++pg) {
+        for (int k = 0; k < 3; ++k) {
+            float* x = &X[(static_cast<size_t>(pg) * 3 + k) * RRB_MLP_IN];
+            int rc = rrb_page_features(&r->p, pg, kTiles[k][0], kTiles[k][1], x);
+            if (rc) return rc;
+        }
+        const uint64_t px = static_cast<uint64_t>(r->p.page_width[pg]) * r->p.page_height[pg];
+        if (s->have_table && px >= biggest) {
+            biggest = px;
+            const float* x = &X[static_cast<size_t>(pg) * 3 * RRB_MLP_IN];
+            const int b0 = std::min(3, std::max(0, static_cast<int>((x[0] - 13.0f) / 1.0f)));
+            const int b1 = std::min(3, std::max(0, static_cast<int>((x[5] - x[0] + 6.0f) / 1.5f)));
+            r->table_shape = s->table[b0 * 4 + b1];
+        }
+    }
+    if (!s->have_params) return RRB_OK;
+    for (size_t i = 0; i < X.size(); ++i) {
+        const size_t j = i % RRB_MLP_IN;
+        X[i] = (X[i] - s->x_mean[j]) / s->x_std[j];
+    }
+    std::vector<float> y(static_cast<size_t>(n) * 3);
+    {
+        std::lock_guard<std::mutex> lk(s->mlp_mu);
+        int rc = rrb_mlp_predict(s->mlp, X.data(), n * 3, y.data());
+        if (rc) return rc;
+    }
+    for (int k = 0; k < 3; ++k) r->pred[k] = 0;
+    for (uint32_t pg = 0; pg < n; ++pg)
+        for (int k = 0; k < 3; ++k) r->pred[k] += std::exp(y[pg * 3 + k] * s->y_std + s->y_mean);
+    r->pred_best = *std::min_element(r->pred, r->pred + 3);
+    return RRB_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int rrb_server_set_cost_model(rrb_server* s, const rrb_server_cost_model* m) {
+    if (!s || !m) return RRB_ERR_INVARIANT;
+    if (m->params && (!m->x_mean || !m->x_std)) return RRB_ERR_INVARIANT;
+    if (m->table)
+        for (int k = 0; k < 16; ++k)
+            if (m->table[k] < 0 || m->table[k] > 2) return RRB_ERR_INVARIANT;
+    std::lock_guard<std::mutex> lk(s->mlp_mu);
+    if (m->params) {
+        if (!s->mlp) {
+            int rc = rrb_mlp_create(s->cfg.device, 0, &s->mlp);
+            if (rc) return rc;
+        }
+        int rc = rrb_mlp_set_params(s->mlp, m->params);
+        if (rc) return rc;
+        std::memcpy(s->x_mean, m->x_mean, sizeof s->x_mean);
+        std::memcpy(s->x_std, m->x_std, sizeof s->x_std);
+        s->y_mean = m->y_mean;
+        s->y_std = m->y_std;
+    }
+    s->have_params = m->params != nullptr;
+    s->have_table = m->table != nullptr;
+    if (m->table) std::memcpy(s->table, m->table, sizeof s->table);
+    s->policy = m->policy;
+    return RRB_OK;
+}
 
 int rrb_server_create(const rrb_server_config* cfg, rrb_server** out) {
     if (!cfg || !out) return RRB_ERR_INVARIANT;
@@ -224,13 +339,21 @@ int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* ho
     char msg[8];
     int rc = rrb_validate_path_batch(p, host_pages_len, msg, sizeof msg);
     if (rc) return rc;
+    const auto t0 = Clock::now();
     Request* r = new Request();
     r->p = *p;
+    if (s->have_params || s->have_table) {
+        rc = predict_request(s, r);
+        if (rc) {
+            delete r;
+            return rc;
+        }
+    }
     r->out = host_pages;
     r->out_len = host_pages_len;
     r->init = init_value;
     r->est_bytes = estimate_bytes(*p);
-    r->t_submit = Clock::now();
+    r->t_submit = t0;
     {
         std::lock_guard<std::mutex> lk(s->m);
         r->id = s->next_id++;
@@ -274,6 +397,7 @@ int rrb_server_stats(rrb_server* s, rrb_server_stats_t* out) {
     out->queued = s->queue.size();
     out->in_use_bytes = s->in_use;
     out->peak_in_use_bytes = s->peak_in_use;
+    for (int k = 0; k < 3; ++k) out->tile_batches[k] = s->tile_batches[k];
     return RRB_OK;
 }
 
@@ -286,6 +410,7 @@ int rrb_server_destroy(rrb_server* s) {
     s->cv_work.notify_all();
     for (std::thread& t : s->threads) t.join();
     for (rrb_ctx* c : s->ctx) rrb_destroy(c);
+    if (s->mlp) rrb_mlp_destroy(s->mlp);
     for (auto& kv : s->live) delete kv.second;
     delete s;
     return RRB_OK;

@@ -495,7 +495,33 @@ class Server:
     def stats(self) -> dict:
         s = ServerStats()
         lib().rrb_server_stats(self._h, C.byref(s))
-        return {n: int(getattr(s, n)) for n, _ in ServerStats._fields_}
+        out = {n: int(getattr(s, n)) for n, _ in ServerStats._fields_ if n != "tile_batches"}
+        out["tile_batches"] = [int(v) for v in s.tile_batches]
+        return out
+
+    def set_cost_model(self, model=None, table=None, shortest_first=True, tile_by_model=True):
+        """Scheduler policy from a trained rrb.autotune.CostModel (or only its table)."""
+        keep = []
+
+        def f32(a):
+            a = np.ascontiguousarray(a, np.float32)
+            keep.append(a)
+            return _ptr(a, C.c_float)
+
+        m = _abi.ServerCostModel()
+        if model is not None:
+            m.params, m.x_mean, m.x_std = f32(model.params), f32(model.x_mean), f32(model.x_std)
+            m.y_mean, m.y_std = model.y_mean, model.y_std
+            table = model.table if table is None else table
+        if table is not None:
+            t = np.ascontiguousarray(table, np.int32)
+            keep.append(t)
+            m.table = _ptr(t, C.c_int32)
+        m.policy = (_abi.RRB_SCHED_SHORTEST_FIRST if shortest_first else 0) | \
+                   (_abi.RRB_SCHED_TILE_BY_MODEL if tile_by_model else 0)
+        rc = lib().rrb_server_set_cost_model(self._h, C.byref(m))
+        if rc:
+            raise BackendError(rc, "rrb_server_set_cost_model failed")
 
     def close(self):
         h, self._h = getattr(self, "_h", None), None

@@ -34,6 +34,8 @@ RRB_STATIC_MAX_EDGES = 1 << 18
 RRB_STATIC_MAX_ROW_CROSSINGS = 128
 RRB_STATIC_MAX_CELLS = 2801024
 RRB_MLP_IN = 24
+RRB_SCHED_SHORTEST_FIRST = 1
+RRB_SCHED_TILE_BY_MODEL = 2
 RRB_MLP_HIDDEN = 64
 RRB_MLP_PARAMS = 64 * 24 + 64 + 64 * 64 + 64 + 64 + 1
 
@@ -125,7 +127,12 @@ class RequestResult(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("completed", "batches", "batched_requests", "queued", "in_use_bytes",
-                                          "peak_in_use_bytes")]
+                                          "peak_in_use_bytes")] + [("tile_batches", C.c_uint64 * 3)]
+
+
+class ServerCostModel(C.Structure):
+    _fields_ = [("params", C.POINTER(C.c_float)), ("x_mean", C.POINTER(C.c_float)), ("x_std", C.POINTER(C.c_float)),
+                ("y_mean", C.c_float), ("y_std", C.c_float), ("table", C.POINTER(C.c_int32)), ("policy", C.c_uint32)]
 
 
 class SceneParams(C.Structure):
@@ -193,6 +200,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_uint64)]),
     "rrb_server_wait": (C.c_int, [VP, C.c_uint64, C.c_uint64, C.POINTER(RequestResult)]),
     "rrb_server_stats": (C.c_int, [VP, C.POINTER(ServerStats)]),
+    "rrb_server_set_cost_model": (C.c_int, [VP, C.POINTER(ServerCostModel)]),
     "rrb_server_destroy": (C.c_int, [VP]),
     "rrb_page_features": (C.c_int, [C.POINTER(PathBatchParams), C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.POINTER(C.c_float)]),

@@ -59,3 +59,32 @@ def test_admission_under_a_small_budget(rrb_lib):
         st = srv.stats()
     assert st["completed"] == 6 and st["in_use_bytes"] == 0
     assert all(r["latency_ns"] > 0 for r in res)
+
+
+def test_cost_model_policies_keep_the_pixels(rrb_lib, oracle):
+    """Shortest-first admission and per-batch tile shapes reorder and retile
+    the work but never change a request's pages."""
+    from rrb.autotune import CostModel
+
+    scenes = _requests(rrb_lib, 6, seed0=500)
+    m = rrb_lib.MLP(0, seed=1)
+    params = m.params()
+    m.close()
+    model = CostModel(params, np.zeros(24, np.float32), np.ones(24, np.float32), 0.0, 1.0,
+                      np.tile(np.array([0, 1, 2, 0], np.int32), 4))
+    with rrb_lib.Server(workers=2, max_batch_pages=4) as srv:
+        srv.set_cost_model(model)
+        by_model, _ = _run(srv, scenes)
+        st = srv.stats()
+    assert st["completed"] == 6 and sum(st["tile_batches"]) == st["batches"]
+    with rrb_lib.Server(workers=1, max_batch_pages=4) as srv:
+        srv.set_cost_model(table=np.full(16, 1, np.int32), shortest_first=False)
+        by_table, _ = _run(srv, scenes)
+        st = srv.stats()
+    assert st["tile_batches"] == [0, st["batches"], 0]  # every batch took the table's 32x32
+    for i, s in enumerate(scenes):
+        assert np.array_equal(by_model[i], by_table[i]), i
+        if i < 3:
+            exp = s.blank_arena()
+            oracle.render_scene(s, exp)
+            assert np.array_equal(by_model[i], exp), i
