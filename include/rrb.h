@@ -242,6 +242,19 @@ typedef struct {
 } rrb_path_batch_params;
 int rrb_record_path_batch(rrb_ctx* ctx, const rrb_path_batch_params* p);
 
+/* The product renderer's RGB page form (the A12 variant: the page is Rgb8 and
+ * each path composites with composite_aa_rgb8_opaque, crates/raster/src/simd/
+ * composite.rs:56+, a_src = (alpha * shape + 255) >> 8 and per channel
+ * ((255 - a_src) * dst + a_src * src + 255) >> 8). Pages are 3 bytes per
+ * pixel (row stride 3 * width, page_offset in bytes); path p is painted with
+ * path_rgb[3p..3p+2] (host); the gray array is not read. Coverage, order and
+ * every other rule are those of rrb_record_path_batch. */
+int rrb_record_path_batch_rgb(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb);
+/* rgb_to_gray (crates/pdf_raster/src/render.rs:1306-1324) on the device:
+ * gray[i] = (2126 r + 7152 g + 722 b + 5000) / 10000 for n_px pixels. */
+int rrb_record_rgb_to_gray(rrb_ctx* ctx, const rrb_buf* rgb, size_t rgb_offset, const rrb_buf* gray,
+                           size_t gray_offset, uint64_t n_px);
+
 /* Device-resident batches: the inputs of a path batch are validated and
  * uploaded once, then rendered any number of times into device pages with no
  * further host-to-device traffic (the serving loop keeps them resident).

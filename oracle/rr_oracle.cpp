@@ -751,9 +751,15 @@ void or_rgb_to_gray(const uint8_t* rgb, uint8_t* gray, int64_t n) {
 // fill_impl (crates/raster/src/fill/mod.rs:110-244), vector_antialias = true,
 // page clip Clip::new(0, 0, W, H, true) (clip.rs:73-88, recompute_int_bounds
 // :266-271), Gray8 page without alpha plane, identity transfer, solid source.
-void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pts,
-                  const uint8_t* flags, int64_t n_pts, const double m[6], double flatness, int eo,
-                  uint8_t gray, uint8_t alpha, int rowmap, or_stats* st) {
+}  // extern "C"
+
+namespace {
+
+// fill_impl for one path; `span(y, x0, shape, n)` composites a gamma-mapped
+// shape span onto pixel row y (the page's pixel format lives in `span`).
+template <typename Span>
+void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint8_t* flags, int64_t n_pts,
+                    const double m[6], double flatness, int eo, int rowmap, or_stats* st, Span span) {
     if (n_pts == 0) return;
     if (st) st->paths++;
     // XPath::new with close_subpaths = true, then aa_scale.
@@ -801,7 +807,7 @@ void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pt
             }
         }
         if (!any) return;
-        or_render_span_aa_gray(page + static_cast<int64_t>(y) * width + x0, shape.data(), cnt, alpha, gray);
+        span(y, x0, shape.data(), cnt);
     };
     auto clip_aa_line = [&](int32_t* x0, int32_t* x1) {
         // Clip::clip_aa_line (clip.rs:246-254) with no path-clip scanners.
@@ -834,12 +840,67 @@ void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pt
     delete sc;
 }
 
+// Pages of a scene on up to n_threads workers; rgb == nullptr: Gray8 pages
+// and gray[] sources, else Rgb8 pages (3 bytes per pixel) and rgb[3 * p].
+void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w,
+                       const uint32_t* page_h, uint32_t n_pages, const double* pts,
+                       const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
+                       const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
+                       uint64_t n_paths, const double m[6], double flatness, int rowmap,
+                       int n_threads, or_stats* st);
+
+}  // namespace
+
+extern "C" {
+
+void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pts,
+                  const uint8_t* flags, int64_t n_pts, const double m[6], double flatness, int eo,
+                  uint8_t gray, uint8_t alpha, int rowmap, or_stats* st) {
+    fill_path_impl(width, height, pts, flags, n_pts, m, flatness, eo, rowmap, st,
+                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                       or_render_span_aa_gray(page + static_cast<int64_t>(y) * width + x0, shape, n, alpha, gray);
+                   });
+}
+
+void or_fill_path_rgb(uint8_t* page_rgb, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                      int64_t n_pts, const double m[6], double flatness, int eo, const uint8_t rgb[3], uint8_t alpha,
+                      int rowmap, or_stats* st) {
+    fill_path_impl(width, height, pts, flags, n_pts, m, flatness, eo, rowmap, st,
+                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                       or_composite_aa_rgb8_opaque(page_rgb + 3 * (static_cast<int64_t>(y) * width + x0), rgb, alpha,
+                                                   shape, n);
+                   });
+}
+
 void or_render_scene(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w,
                      const uint32_t* page_h, uint32_t n_pages, const double* pts,
                      const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
                      const uint8_t* gray, const uint8_t* alpha, const uint32_t* path_page,
                      uint64_t n_paths, const double m[6], double flatness, int rowmap,
                      int n_threads, or_stats* st) {
+    render_scene_impl(arena, page_off, page_w, page_h, n_pages, pts, flags, path_pt_off, rule, gray, nullptr, alpha,
+                      path_page, n_paths, m, flatness, rowmap, n_threads, st);
+}
+
+void or_render_scene_rgb(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                         uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                         const uint8_t* rule, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
+                         uint64_t n_paths, const double m[6], double flatness, int rowmap, int n_threads,
+                         or_stats* st) {
+    render_scene_impl(arena, page_off, page_w, page_h, n_pages, pts, flags, path_pt_off, rule, nullptr, rgb, alpha,
+                      path_page, n_paths, m, flatness, rowmap, n_threads, st);
+}
+
+}  // extern "C"
+
+namespace {
+
+void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w,
+                       const uint32_t* page_h, uint32_t n_pages, const double* pts,
+                       const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
+                       const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
+                       uint64_t n_paths, const double m[6], double flatness, int rowmap,
+                       int n_threads, or_stats* st) {
     // Paths of each page, in scene order.
     std::vector<std::vector<uint64_t>> per_page(n_pages);
     for (uint64_t p = 0; p < n_paths; ++p)
@@ -855,9 +916,14 @@ void or_render_scene(uint8_t* arena, const uint64_t* page_off, const uint32_t* p
             uint8_t* page = arena + page_off[pg];
             for (uint64_t p : per_page[pg]) {
                 uint64_t a = path_pt_off[p], b = path_pt_off[p + 1];
-                or_fill_path(page, static_cast<int32_t>(page_w[pg]), static_cast<int32_t>(page_h[pg]),
-                             pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
-                             gray[p], alpha[p], rowmap, &ls);
+                if (rgb)
+                    or_fill_path_rgb(page, static_cast<int32_t>(page_w[pg]), static_cast<int32_t>(page_h[pg]),
+                                     pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
+                                     rgb + 3 * p, alpha[p], rowmap, &ls);
+                else
+                    or_fill_path(page, static_cast<int32_t>(page_w[pg]), static_cast<int32_t>(page_h[pg]),
+                                 pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
+                                 gray[p], alpha[p], rowmap, &ls);
             }
         }
     };
@@ -881,4 +947,4 @@ void or_render_scene(uint8_t* arena, const uint64_t* page_off, const uint32_t* p
     }
 }
 
-}  // extern "C"
+}  // namespace

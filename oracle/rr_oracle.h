@@ -136,6 +136,12 @@ void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pt
                   const uint8_t* flags, int64_t n_pts, const double m[6], double flatness, int eo,
                   uint8_t gray, uint8_t alpha, int rowmap, or_stats* st);
 
+/* The same fill onto an Rgb8 page (3 bytes per pixel, row stride 3 * width)
+ * with a solid RGB source, through composite_aa_rgb8_opaque (A12). */
+void or_fill_path_rgb(uint8_t* page_rgb, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                      int64_t n_pts, const double m[6], double flatness, int eo, const uint8_t rgb[3], uint8_t alpha,
+                      int rowmap, or_stats* st);
+
 /* Render a whole scene: paths [0, n_paths) in order onto their pages.
  * path_pt_off[n_paths+1] indexes pts/flags; pages live in one arena at
  * page_off[p] with page_w[p] x page_h[p]. Pages are independent and are
@@ -146,6 +152,13 @@ void or_render_scene(uint8_t* arena, const uint64_t* page_off, const uint32_t* p
                      const uint8_t* gray, const uint8_t* alpha, const uint32_t* path_page,
                      uint64_t n_paths, const double m[6], double flatness, int rowmap,
                      int n_threads, or_stats* st);
+/* The scene on Rgb8 pages (page_off in bytes, 3 bytes per pixel), path p
+ * painted with rgb[3p..3p+2]. */
+void or_render_scene_rgb(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                         uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                         const uint8_t* rule, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
+                         uint64_t n_paths, const double m[6], double flatness, int rowmap, int n_threads,
+                         or_stats* st);
 
 #ifdef __cplusplus
 }

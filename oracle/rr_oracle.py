@@ -96,6 +96,11 @@ def lib() -> C.CDLL:
                                        C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
                                        C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D), D, C.c_int, C.c_int,
                                        C.POINTER(Stats)]),
+            "or_render_scene_rgb": (None, [C.POINTER(U8), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                           C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(D), C.POINTER(U8),
+                                           C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
+                                           C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D), D, C.c_int, C.c_int,
+                                           C.POINTER(Stats)]),
             "or_aa_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
             "or_aa_fill_cpu": (None, [C.POINTER(C.c_float), C.c_uint32, C.c_float, C.c_float, C.c_uint32,
                                       C.c_uint32, C.c_int, C.POINTER(U8)]),
@@ -304,6 +309,24 @@ def render_arrays(arena, page_offset, page_width, page_height, pts, flags, path_
                           a[1].size, _p(a[3], C.c_double), _p(a[4], C.c_uint8), _p(a[5], C.c_uint64),
                           _p(a[6], C.c_uint8), _p(a[7], C.c_uint8), _p(a[8], C.c_uint8), _p(a[9], C.c_uint32),
                           a[6].size, _mat(matrix), flatness, rowmap, threads, C.byref(st))
+    return st.as_dict()
+
+
+def render_scene_rgb(scene, arena: np.ndarray, rgb: np.ndarray, rowmap=ROWMAP_DOCUMENTED, threads=1,
+                     page_offset=None) -> dict:
+    """The scene on Rgb8 pages (A12): `arena` holds 3 bytes per pixel at
+    `page_offset` (default: 3 x the scene's), path p painted with rgb[p]."""
+    po = np.ascontiguousarray(3 * scene.page_offset.astype(np.uint64) if page_offset is None else page_offset,
+                              np.uint64)
+    a = [np.ascontiguousarray(x, t) for x, t in (
+        (scene.page_width, np.uint32), (scene.page_height, np.uint32), (np.reshape(scene.pts, -1), np.float64),
+        (scene.flags, np.uint8), (scene.path_pt_off, np.uint64), (scene.fill_rule, np.uint8),
+        (np.reshape(rgb, -1), np.uint8), (scene.alpha, np.uint8), (scene.path_page, np.uint32))]
+    st = Stats()
+    lib().or_render_scene_rgb(_p(arena, C.c_uint8), _p(po, C.c_uint64), _p(a[0], C.c_uint32), _p(a[1], C.c_uint32),
+                              a[0].size, _p(a[2], C.c_double), _p(a[3], C.c_uint8), _p(a[4], C.c_uint64),
+                              _p(a[5], C.c_uint8), _p(a[6], C.c_uint8), _p(a[7], C.c_uint8), _p(a[8], C.c_uint32),
+                              a[5].size, _mat(IDENTITY), 0.1, rowmap, threads, C.byref(st))
     return st.as_dict()
 
 

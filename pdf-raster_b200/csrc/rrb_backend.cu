@@ -186,14 +186,20 @@ bool valid_tile(uint32_t w, uint32_t h) {
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
                      uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
                      const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, const int4* runs,
-                     uint8_t* arena, int rowmap, const BatchCounters* ctr) {
-#define RRB_COMP(TW, TH)                                                                                 \
-    k_composite<TW, TH><<<grid, COMP_THREADS, 0, c->stream>>>(info, geom, n_pages, n_tiles, SUPER, SUPER, \
-                                                              super_off, super_list, row_off, row_idx,    \
-                                                              spans, runs, arena, rowmap, ctr)
-    if (tw == 64 && th == 16) RRB_COMP(64, 16);
-    else if (tw == 32 && th == 32) RRB_COMP(32, 32);
-    else RRB_COMP(16, 16);
+                     uint8_t* arena, int rowmap, const BatchCounters* ctr, const uint32_t* path_rgb) {
+#define RRB_COMP(TW, TH, RGB)                                                                                  \
+    k_composite<TW, TH, RGB><<<grid, COMP_THREADS, 0, c->stream>>>(info, geom, n_pages, n_tiles, SUPER, SUPER, \
+                                                                   super_off, super_list, row_off, row_idx,    \
+                                                                   spans, runs, arena, rowmap, ctr, path_rgb)
+    if (path_rgb) {
+        if (tw == 64 && th == 16) RRB_COMP(64, 16, true);
+        else if (tw == 32 && th == 32) RRB_COMP(32, 32, true);
+        else RRB_COMP(16, 16, true);
+    } else {
+        if (tw == 64 && th == 16) RRB_COMP(64, 16, false);
+        else if (tw == 32 && th == 32) RRB_COMP(32, 32, false);
+        else RRB_COMP(16, 16, false);
+    }
 #undef RRB_COMP
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
@@ -204,7 +210,7 @@ int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info,
 // crates/gpu/src/backend/params.rs:57,334), plus the page geometry the
 // kernels need. No device access.
 int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw, uint32_t th,
-                   std::vector<PageGeom>& geom, uint64_t& tiles, uint64_t& supers, std::string& msg) {
+                   std::vector<PageGeom>& geom, uint64_t& tiles, uint64_t& supers, std::string& msg, uint32_t bpp = 1) {
     const uint64_t n_paths = h->n_paths, n_pts = h->n_pts;
     const uint32_t n_pages = h->n_pages;
     tiles = supers = 0;
@@ -228,7 +234,7 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
         uint32_t w = h->page_width[pg], ht = h->page_height[pg];
         if (w == 0 || ht == 0 || w > 16383 || ht > (1u << 28))
             return msg = "page width must be 1..16383 and height 1..2^28", RRB_ERR_INVARIANT;
-        if (h->page_offset[pg] + static_cast<uint64_t>(w) * ht > arena_len)
+        if (h->page_offset[pg] + static_cast<uint64_t>(bpp) * w * ht > arena_len)
             return msg = "page extends past the page buffer", RRB_ERR_INVARIANT;
         PageGeom& G = geom[pg];
         G.w = w;
@@ -281,6 +287,8 @@ void set_tiles(std::vector<PageGeom>& geom, uint32_t tw, uint32_t th, uint64_t& 
 // number of times (the serving loop keeps these resident).
 struct rrb_batch {
     Scratch pts, flags, off, rule, gray, alpha, page, geom, pw, ph, mtx;
+    Scratch rgb;                    // Rgb8 pages: per-path colour r | g << 8 | b << 16
+    uint32_t bpp = 1;               // page bytes per pixel: 1 Gray8, 3 Rgb8
     std::vector<PageGeom> geom_h;
     std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
     bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
@@ -329,7 +337,7 @@ void stage_end(rrb_ctx* c, int k) {
 
 void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
-                      &B->mtx};
+                      &B->mtx, &B->rgb};
     for (Scratch* s : all) {
         if (B->view && s != &B->off && s != &B->page && s != &B->geom) {
             s->p = nullptr;
@@ -342,10 +350,12 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     }
 }
 
-int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
+// Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages.
+int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr) {
     std::string msg;
     uint64_t tiles = 0;
-    int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg);
+    B->bpp = rgb ? 3 : 1;
+    int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg, B->bpp);
     if (v) return set_err(c, v, msg);
     B->n_paths = h->n_paths;
     B->n_pts = h->n_pts;
@@ -354,7 +364,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
     B->rowmap = h->rowmap;
     B->arena_need = 0;
     for (const PageGeom& G : B->geom_h)
-        B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(G.w) * G.h);
+        B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(B->bpp) * G.w * G.h);
     B->page_pt.assign(B->n_pages + 1, 0);
     for (uint32_t pg = 0; pg < B->n_pages; ++pg) B->page_pt[pg] = h->path_pt_off[B->geom_h[pg].path_begin];
     B->page_pt[B->n_pages] = h->n_paths ? h->path_pt_off[h->n_paths] : 0;
@@ -371,6 +381,14 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B) {
     if ((rc = upload(c, B->ph, h->page_height, h->n_pages))) return rc;
     if ((rc = ensure(c, B->geom, h->n_pages * sizeof(PageGeom)))) return rc;
     if ((rc = upload(c, B->mtx, h->matrix, 6))) return rc;
+    if (rgb) {
+        std::vector<uint32_t> packed(h->n_paths);
+        for (uint64_t p = 0; p < h->n_paths; ++p)
+            packed[p] = rgb[3 * p] | (uint32_t(rgb[3 * p + 1]) << 8) | (uint32_t(rgb[3 * p + 2]) << 16);
+        if ((rc = upload(c, B->rgb, packed.data(), packed.size()))) return rc;
+        // The staging vector is released on return: let the copy finish first.
+        RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     return RRB_OK;
 }
 
@@ -590,7 +608,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
                                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
-                               rowmap, as<BatchCounters>(c->s_ctr))))
+                               rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr)))
         return rc;
     stage_end(c, 11);
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
@@ -678,6 +696,8 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     view(W->pw, B->pw, pg0 * sizeof(uint32_t));
     view(W->ph, B->ph, pg0 * sizeof(uint32_t));
     view(W->mtx, B->mtx, 0);
+    W->bpp = B->bpp;
+    if (B->bpp == 3) view(W->rgb, B->rgb, pb * sizeof(uint32_t));
     int rc;
     if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
     if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
@@ -758,9 +778,10 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     return RRB_OK;
 }
 
-int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len) {
+int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
+              const uint8_t* rgb = nullptr) {
     rrb_batch* B = c->tmp_batch;
-    int rc = batch_upload(c, h, B);
+    int rc = batch_upload(c, h, B, rgb);
     if (rc) return rc;
     return run_resident(c, B, arena, arena_len, h->rowmap);
 }
@@ -1167,6 +1188,37 @@ int rrb_last_stage_times(rrb_ctx* c, rrb_stage_time* out, int cap, int* n) {
         ++m;
     }
     *n = m;
+    return RRB_OK;
+}
+
+int rrb_record_path_batch_rgb(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb) {
+    if (!c || !p) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
+    if (p->n_paths && !path_rgb) return set_err(c, RRB_ERR_INVARIANT, "path_rgb is null");
+    cudaSetDevice(c->device);
+    {
+        std::vector<PageGeom> geom;
+        uint64_t tiles = 0, supers = 0;
+        std::string m;
+        int v = validate_batch(p, p->pages->len, 64, 16, geom, tiles, supers, m, 3);
+        if (v) return set_err(c, v, m);
+    }
+    static const uint8_t kNone[3] = {0, 0, 0};
+    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, p->n_paths ? path_rgb : kNone);
+}
+
+int rrb_record_rgb_to_gray(rrb_ctx* c, const rrb_buf* rgb, size_t rgb_offset, const rrb_buf* gray,
+                           size_t gray_offset, uint64_t n_px) {
+    if (!c || !rgb || !gray) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    if (rgb_offset + 3 * n_px > rgb->len || gray_offset + n_px > gray->len)
+        return set_err(c, RRB_ERR_INVARIANT, "rgb_to_gray range past a buffer");
+    if (!n_px) return RRB_OK;
+    cudaSetDevice(c->device);
+    k_rgb_to_gray<<<grid_for(c, n_px, 256), 256, 0, c->stream>>>(static_cast<const uint8_t*>(rgb->p) + rgb_offset,
+                                                                static_cast<uint8_t*>(gray->p) + gray_offset, n_px);
+    RRB_CUDA(c, cudaGetLastError());
     return RRB_OK;
 }
 

@@ -1214,7 +1214,7 @@ __constant__ uint8_t c_gamma[17] = {0, 4, 11, 21, 32, 45, 59, 74, 90, 108, 126, 
 struct HitInfo {
     int32_t g0, g1, py0, py1;  // pixel-row groups [g0, g1] (AA rows >> 2), pixel rows touched
     uint32_t goff, paint;      // first group index entry (or first run), paint word (| HIT_FULL)
-    uint32_t run_cnt, pad;     // rectilinear paths: number of runs
+    uint32_t run_cnt, rgb;     // rectilinear paths: number of runs; Rgb8 pages: the path's colour
 };
 
 constexpr uint32_t HIT_FULL = 1u << 18;  // every pixel of this tile has coverage 16 for this path
@@ -1282,7 +1282,22 @@ __device__ __forceinline__ void load_hit_cells(const uint32_t* __restrict__ cell
 // coverage cell (start marks in shared memory + a prefix max across the row's
 // lanes), then AA_GAMMA and the div255 source-over of render_span_aa_inner's
 // no-alpha arm (pipe/aa.rs:192-208).
-template <int TW, int TH>
+// Rgb8 pages (A12, composite_aa_rgb8_opaque, simd/composite.rs:56+): pixels
+// and colours packed r | g << 8 | b << 16; per channel
+// c = ((255 - a) * dst + a * src + 255) >> 8.
+__device__ __forceinline__ uint32_t rgb_over(uint32_t d, uint32_t a, uint32_t s) {
+    const uint32_t inv = 255u - a;
+    uint32_t out = 0;
+#pragma unroll
+    for (int c = 0; c < 24; c += 8)
+        out |= (((inv * ((d >> c) & 0xffu) + a * ((s >> c) & 0xffu) + 255u) >> 8) & 0xffu) << c;
+    return out;
+}
+
+// a_src of the Rgb8 path: (a_input * shape + 255) >> 8.
+__device__ __forceinline__ uint32_t rgb_a_src(uint32_t alpha, uint32_t shape) { return (alpha * shape + 255u) >> 8; }
+
+template <int TW, int TH, bool RGB>
 __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitRows<TW, TH>& hr, int X0,
                                                     const uint32_t* __restrict__ cells, const uint8_t* gamma,
                                                     int32_t (*mark)[TW], uint32_t (&pix)[TH * TW / COMP_THREADS]) {
@@ -1349,19 +1364,26 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
         for (int q = 0; q < L::PX; ++q) {
             if (cov[q] == 0) continue;
             const uint32_t shape = gamma[min(cov[q], 16)];
-            const uint32_t a_src = div255(alpha * shape);
             const int k = it * L::PX + q;
-            pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
+            if (RGB) {
+                pix[k] = rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
+            } else {
+                const uint32_t a_src = div255(alpha * shape);
+                pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
+            }
         }
     }
 }
 
-template <int TW, int TH>
+// RGB: the pages are Rgb8 (3 bytes per pixel) and path_rgb[p] is path p's
+// colour; otherwise Gray8 pages painted with each path's gray.
+template <int TW, int TH, bool RGB>
 __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
     const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
-    const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr) {
+    const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr,
+    const uint32_t* __restrict__ path_rgb) {
     using L = CompLayout<TW>;
     constexpr int ITERS = TH / (L::NW * L::RPW);
     constexpr int NPIX = TH * TW / COMP_THREADS;
@@ -1370,7 +1392,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     __shared__ uint32_t wcnt[L::NW];
     __shared__ uint8_t gamma[17];
     __shared__ int32_t mark[L::NW * L::RPW][TW];
-    __shared__ uint8_t lut[256];
+    __shared__ uint8_t lut[RGB ? 768 : 256];
     __shared__ uint32_t red[L::NW];
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
@@ -1391,7 +1413,16 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
 #pragma unroll
             for (int q = 0; q < L::PX; ++q) {
                 const int x = X0 + col + q;
-                pix[it * L::PX + q] = (y < H && x < W) ? page[static_cast<size_t>(y) * W + x] : 0u;
+                uint32_t v = 0;
+                if (y < H && x < W) {
+                    if (RGB) {
+                        const uint8_t* p = page + 3 * (static_cast<size_t>(y) * W + x);
+                        v = p[0] | (uint32_t(p[1]) << 8) | (uint32_t(p[2]) << 16);
+                    } else {
+                        v = page[static_cast<size_t>(y) * W + x];
+                    }
+                }
+                pix[it * L::PX + q] = v;
             }
         }
         const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
@@ -1404,7 +1435,8 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
             return P.bx0 <= X0 && P.bx1 >= TX1 && P.by0 <= Y0 && P.by1 >= TY1;
         };
         // Pre-pass: the last opaque layer covering the whole tile sets every
-        // pixel to its gray (div255(255 * g) = g), so compositing starts there.
+        // pixel to its colour (div255(255 * g) = g; on Rgb8 pages
+        // (255 * s + 255) >> 8 = s), so compositing starts there.
         uint32_t start = l0;
         {
             uint32_t best = 0;
@@ -1450,7 +1482,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 hi.py1 = P.py1;
                 hi.goff = (P.paint & PI_RECTI) ? P.run_off : group_off[super_list[q]];
                 hi.run_cnt = P.run_cnt;
-                hi.pad = 0;
+                hi.rgb = RGB ? path_rgb[super_list[q]] : 0u;
                 hi.paint = P.paint | (full_over(P) ? HIT_FULL : 0u);
                 hits[pos] = hi;
             }
@@ -1473,7 +1505,27 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 if (hits[k].paint & HIT_FULL) {
                     uint32_t m = k + 1;
                     while (m < total && (hits[m].paint & HIT_FULL)) ++m;
-                    if (m - k >= 2) {
+                    if (RGB) {
+                        // One map per channel (each channel composes on its own).
+                        if (m - k >= 2) {
+                            __syncthreads();  // the previous maps' readers are done
+                            uint32_t v = threadIdx.x | (threadIdx.x << 8) | (threadIdx.x << 16);
+                            for (uint32_t i = k; i < m; ++i)
+                                v = rgb_over(v, rgb_a_src((hits[i].paint >> 8) & 0xff, 255u), hits[i].rgb);
+                            lut[threadIdx.x] = static_cast<uint8_t>(v);
+                            lut[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
+                            lut[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
+                            __syncthreads();
+#pragma unroll
+                            for (int j = 0; j < NPIX; ++j)
+                                pix[j] = lut[pix[j] & 0xffu] | (uint32_t(lut[256 + ((pix[j] >> 8) & 0xffu)]) << 8) |
+                                         (uint32_t(lut[512 + (pix[j] >> 16)]) << 16);
+                        } else {
+                            const uint32_t a = rgb_a_src((hits[k].paint >> 8) & 0xff, 255u), s = hits[k].rgb;
+#pragma unroll
+                            for (int j = 0; j < NPIX; ++j) pix[j] = rgb_over(pix[j], a, s);
+                        }
+                    } else if (m - k >= 2) {
                         __syncthreads();  // the previous map's readers are done
                         uint32_t v = threadIdx.x;
                         for (uint32_t i = k; i < m; ++i) {
@@ -1495,7 +1547,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 }
                 if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
                 if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
-                composite_path_rows<TW, TH>(hits[k], cur, X0, cells, gamma, mark, pix);
+                composite_path_rows<TW, TH, RGB>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
                 nxt = nxt2;
                 ++k;
@@ -1508,9 +1560,29 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
 #pragma unroll
             for (int q = 0; q < L::PX; ++q) {
                 const int x = X0 + col + q;
-                if (y < H && x < W) page[static_cast<size_t>(y) * W + x] = static_cast<uint8_t>(pix[it * L::PX + q]);
+                if (y < H && x < W) {
+                    const uint32_t v = pix[it * L::PX + q];
+                    if (RGB) {
+                        uint8_t* p = page + 3 * (static_cast<size_t>(y) * W + x);
+                        p[0] = static_cast<uint8_t>(v);
+                        p[1] = static_cast<uint8_t>(v >> 8);
+                        p[2] = static_cast<uint8_t>(v >> 16);
+                    } else {
+                        page[static_cast<size_t>(y) * W + x] = static_cast<uint8_t>(v);
+                    }
+                }
             }
         }
+    }
+}
+
+// rgb_to_gray (crates/pdf_raster/src/render.rs:1306-1324): BT.709 luma,
+// (2126 r + 7152 g + 722 b + 5000) / 10000, exact in integers.
+__global__ void k_rgb_to_gray(const uint8_t* __restrict__ rgb, uint8_t* __restrict__ gray, uint64_t n) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
+        gray[i] = static_cast<uint8_t>((2126u * r + 7152u * g + 722u * b + 5000u) / 10000u);
     }
 }
 

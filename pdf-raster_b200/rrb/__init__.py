@@ -377,6 +377,15 @@ class B200Backend:
         self._chk(lib().rrb_record_tile_fill_segs(self._h, C.byref(p), C.byref(n)))
         return int(n.value)
 
+    def record_path_batch_rgb(self, params: PathBatchParams, path_rgb: np.ndarray):
+        """Rgb8 pages (3 bytes per pixel): path p painted with path_rgb[p] = (r, g, b)."""
+        rgb = np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
+        self._chk(lib().rrb_record_path_batch_rgb(self._h, C.byref(params), _ptr(rgb, C.c_uint8)))
+
+    def record_rgb_to_gray(self, rgb: DeviceBuffer, gray: DeviceBuffer, n_px: int, rgb_offset: int = 0,
+                           gray_offset: int = 0):
+        self._chk(lib().rrb_record_rgb_to_gray(self._h, rgb.handle, rgb_offset, gray.handle, gray_offset, n_px))
+
     def record_path_batch(self, params: PathBatchParams):
         self._chk(lib().rrb_record_path_batch(self._h, C.byref(params)))
 
