@@ -391,6 +391,13 @@ int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32
                   float lr, uint64_t seed, float* final_loss);
 int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out);
 
+/* ---- page output (crates/encode pgm.rs / ppm.rs) -----------------------------
+ * Netpbm bytes of a page already on the host: channels 1 writes P5 (Gray8),
+ * 3 writes P6 (Rgb8); header "P5\n{w} {h}\n255\n" then the pixel rows.
+ * *out_len receives the byte count; out == NULL only queries it. */
+int rrb_encode_netpbm(const uint8_t* pixels, uint32_t width, uint32_t height, uint32_t channels, uint8_t* out,
+                      size_t out_cap, size_t* out_len);
+
 /* ---- cost-model features ------------------------------------------------------
  * RRB_MLP_IN floats describing page `page` of a batch for composite tile
  * shape tile_w x tile_h (16x16, 32x32 or 64x16), computed on the host from

@@ -547,6 +547,22 @@ class Server:
         self.close()
 
 
+def encode_netpbm(page: np.ndarray) -> bytes:
+    """P5 (a [h, w] Gray8 page) or P6 (a [h, w, 3] Rgb8 page) bytes (rrb_encode_netpbm)."""
+    page = np.ascontiguousarray(page, np.uint8)
+    h, w = page.shape[:2]
+    ch = 1 if page.ndim == 2 else page.shape[2]
+    n = C.c_size_t()
+    rc = lib().rrb_encode_netpbm(page.ctypes.data, w, h, ch, None, 0, C.byref(n))
+    if rc:
+        raise BackendError(rc, "rrb_encode_netpbm")
+    out = np.empty(n.value, np.uint8)
+    rc = lib().rrb_encode_netpbm(page.ctypes.data, w, h, ch, out.ctypes.data, out.size, C.byref(n))
+    if rc:
+        raise BackendError(rc, "rrb_encode_netpbm")
+    return out.tobytes()
+
+
 TILE_SHAPES = ((16, 16), (32, 32), (64, 16))
 
 

@@ -204,6 +204,8 @@ SIGNATURES = {
     "rrb_server_stats": (C.c_int, [VP, C.POINTER(ServerStats)]),
     "rrb_server_set_cost_model": (C.c_int, [VP, C.POINTER(ServerCostModel)]),
     "rrb_server_destroy": (C.c_int, [VP]),
+    "rrb_encode_netpbm": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t,
+                                    C.POINTER(C.c_size_t)]),
     "rrb_page_features": (C.c_int, [C.POINTER(PathBatchParams), C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.POINTER(C.c_float)]),
     "rrb_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(VP)]),

@@ -21,7 +21,7 @@ CSRC = ROOT / "csrc"
 INCLUDE = ROOT.parent / "include"
 LIB = PKG_DIR / "librrb.so"
 
-SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp"]
+SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "rrb_encode.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp"]
 DEPS = SOURCES + [CSRC / "rrb_kernels.cuh", CSRC / "rrb_device.cuh", INCLUDE / "rrb.h"]
 
 NVCC_FLAGS = [

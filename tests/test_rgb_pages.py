@@ -139,3 +139,14 @@ def test_rgb_full_tile_layers_and_luma(backend, oracle, rrb_lib):
         backend.set_tuning(64, 16)
         backend.free_device(pages)
         backend.free_device(gray)
+
+
+def test_netpbm_output_matches_the_reference_format(rrb_lib):
+    # pgm.rs / ppm.rs tests: "P5\n3 2\n255\n" + 6 bytes; P6 with 3 bytes per pixel.
+    g = np.full((2, 3), 128, np.uint8)
+    out = rrb_lib.encode_netpbm(g)
+    assert out == b"P5\n3 2\n255\n" + bytes([128] * 6)
+    rgb = np.arange(2 * 3 * 3, dtype=np.uint8).reshape(2, 3, 3)
+    out = rrb_lib.encode_netpbm(rgb)
+    assert out == b"P6\n3 2\n255\n" + rgb.tobytes()
+    assert rrb_lib.encode_netpbm(np.zeros((0, 5), np.uint8)) == b"P5\n5 0\n255\n"
