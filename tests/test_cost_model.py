@@ -68,3 +68,46 @@ def test_device_training_reduces_loss(rrb_lib):
     Xt, yt = _data(2000, seed=99)
     assert float(np.mean((m.predict(Xt) - yt) ** 2)) < 0.3 * float(np.var(yt))
     m.close()
+
+
+# ---- features, autotuner table and the trained model --------------------------------
+
+def test_page_features_are_consistent(rrb_lib):
+    s = rrb_lib.Scene(2, 3, n_pages=2, page_scale=0.1, paths_scale=0.01)
+    for pg in range(2):
+        rows = [rrb_lib.page_features(s.view, pg, t) for t in rrb_lib.TILE_SHAPES]
+        for k, f in enumerate(rows):
+            assert f[21:24].tolist() == [float(j == k) for j in range(3)]
+            assert abs(f[13:21].sum() - 1.0) < 1e-5 and abs(f[12] - (1.0 - f[13])) < 1e-5
+            n = int(np.sum(s.path_page == pg))
+            assert abs(f[1] - np.log1p(n)) < 1e-4
+            w, h = int(s.page_width[pg]), int(s.page_height[pg])
+            assert abs(f[0] - np.log1p(w * h)) < 1e-3
+        # Only the tile-dependent features differ between shapes.
+        assert np.array_equal(rows[0][:12], rows[1][:12]) and np.array_equal(rows[0][:12], rows[2][:12])
+
+
+def test_autotuner_table_picks_the_fastest_shape_per_bin():
+    from rrb.autotune import bins, build_table
+
+    rng = np.random.default_rng(0)
+    X = np.zeros((300, 3, 24), np.float32)
+    X[:, :, 0] = rng.uniform(12, 18, 300)[:, None]
+    X[:, :, 5] = X[:, :, 0] + rng.uniform(-8, 0, 300)[:, None]
+    T = rng.uniform(1, 2, (300, 3))
+    T[:, 1] *= 0.5  # 32x32 fastest everywhere
+    table = build_table(X, T)
+    keys = np.unique(bins(X[:, 0]))
+    assert all(table[k] == 1 for k in keys)
+    assert all(table[k] == 2 for k in set(range(16)) - set(keys.tolist()))  # empty bins: 64x16
+
+
+def test_cost_model_round_trips(tmp_path):
+    from rrb.autotune import CostModel
+
+    m = CostModel(np.arange(5825, dtype=np.float32), np.ones(24, np.float32), np.full(24, 2, np.float32), 0.5, 1.5,
+                  np.arange(16, dtype=np.int32) % 3)
+    m.save(tmp_path / "m.npz")
+    r = CostModel.load(tmp_path / "m.npz")
+    assert np.array_equal(r.params, m.params) and r.y_mean == 0.5 and r.y_std == 1.5
+    assert np.array_equal(r.table, m.table)
