@@ -357,6 +357,98 @@ def run_rrb(args, rank, local, world):
         dist.destroy_process_group()
 
 
+def run_fill_ops(args, rank, world):
+    """The reference's coverage operators (record_aa_fill / record_tile_fill)
+    on the reference's own benchmark shapes (threshold_bench: a w x h square
+    for 2^8 .. 2^22 pixels) and on glyph outlines (a 1024 x 1024 coverage
+    window holding the flattened outlines of 48 glyphs). GPU time is the
+    kernel with segments resident (CUDA events on the backend stream); e2e
+    adds the segment upload and the coverage download; the CPU baseline is
+    aa_fill_cpu (the oracle), 1 thread, on a bounded sample of rows."""
+    if rank != 0:
+        return
+    import torch
+    import rr_oracle
+    import rrb
+    rr_oracle.build()
+    be = rrb.B200Backend(0)
+    stream = torch.cuda.ExternalStream(be.stream, device=torch.device("cuda", 0))
+
+    def outline_segs(n_glyphs, size):
+        sc = rrb.Scene(1, 7, n_paths=n_glyphs, page_w=size, page_h=size)
+        out = []
+        for i in range(sc.n_paths):
+            a, b = int(sc.path_pt_off[i]), int(sc.path_pt_off[i + 1])
+            for g in rr_oracle.xpath_new(sc.pts[a:b], sc.flags[a:b]):
+                out.append((g.x1, g.y1, g.x0, g.y0) if g.flags & 0x04 else (g.x0, g.y0, g.x1, g.y1))
+        return np.asarray(out, np.float32).reshape(-1, 4)
+
+    def square(w, h):
+        return np.array([[0, 0, w, 0], [w, 0, w, h], [w, h, 0, h], [0, h, 0, 0]], np.float32)
+
+    def measure(segs, w, h, op, reps):
+        sb = be.alloc_device(max(16, segs.nbytes))
+        cb = be.alloc_device(w * h)
+        be.upload_async(sb, segs.view(np.uint8).reshape(-1))
+
+        def run():
+            be.begin_page()
+            if op == "aa_fill":
+                be.record_aa_fill(sb, len(segs), cb, w, h, 0)
+            else:
+                be.record_tile_fill_segs(sb, len(segs), cb, w, h, 0)
+            be.wait_page(be.submit_page())
+
+        run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        host = np.empty(w * h, np.uint8)
+        t = time.perf_counter()
+        for _ in range(reps):
+            be.upload_async(sb, segs.view(np.uint8).reshape(-1))
+            run()
+            be.wait_download(be.download_async(cb, host))
+        e2e_ms = (time.perf_counter() - t) * 1e3 / reps
+        exp_rows = min(h, max(1, 2_000_000 // max(1, w * len(segs))))  # bounded CPU sample
+        t = time.perf_counter()
+        exp = rr_oracle.aa_fill_cpu(segs, 0.0, 0.0, w, exp_rows, False)
+        cpu_s = time.perf_counter() - t
+        same = bool(np.array_equal(exp.ravel(), host[: w * exp_rows])) if op == "aa_fill" else None
+        be.free_device(sb)
+        be.free_device(cb)
+        return {"pixels": w * h, "segments": len(segs), "gpu_ms": ms, "gpu_mpixel_s": w * h / ms / 1e3,
+                "e2e_ms": e2e_ms, "cpu_mpixel_s": w * exp_rows / cpu_s / 1e6, "cpu_sample_rows": exp_rows,
+                "bit_exact_sample": same}
+
+    out = {"aa_fill": {}, "tile_fill_segs": {}}
+    for e in range(8, 23, 2):
+        n = 1 << e
+        w = int(np.ceil(np.sqrt(n)))
+        h = (n + w - 1) // w
+        for op in out:
+            out[op][f"square_{n}px"] = measure(square(w, h), w, h, op, args.steps)
+    segs = outline_segs(48, 1024)
+    for op in out:
+        out[op]["glyph_outlines_1024"] = measure(segs, 1024, 1024, op, args.steps)
+    head = out["aa_fill"]["glyph_outlines_1024"]
+    line = {"metric": "aa_fill coverage Mpixel/s (reference operator, 64 samples/pixel)", "unit": "Mpixel/s",
+            "value": head["gpu_mpixel_s"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "48 glyph outlines flattened at 0.1 in a 1024x1024 coverage window; "
+                                   "plus the reference threshold_bench squares 2^8..2^22 px"},
+            "cpu_baseline": {"value": head["cpu_mpixel_s"], "unit": "Mpixel/s", "cores": 1, "kind": "port",
+                             "sample": f"aa_fill_cpu on the first {head['cpu_sample_rows']} rows"},
+            "ops": out}
+    print(json.dumps(line), flush=True)
+    be.close()
+
+
 def page_requests(rrb, scene):
     """One request per page of `scene`: (params, keep-alive arrays, page bytes)."""
     out = []
@@ -440,7 +532,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["rrb", "reference"], default="rrb")
-    ap.add_argument("--workload", choices=list(WORKLOADS), default="glyphs")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fill_ops"], default="glyphs")
     ap.add_argument("--rowmap", type=int, default=0)
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -457,6 +549,8 @@ def main():
     rank, local, world = dist_env()
     if args.serving:
         run_serving(args, rank, world)
+    elif args.workload == "fill_ops":
+        run_fill_ops(args, rank, world)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
