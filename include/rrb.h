@@ -340,6 +340,9 @@ typedef struct {
 typedef struct {
     uint64_t completed, batches, batched_requests, queued, in_use_bytes, peak_in_use_bytes;
     uint64_t tile_batches[3]; /* batches rendered with 16x16, 32x32, 64x16 tiles */
+    uint64_t prep_ns;         /* workers' time concatenating requests into batches */
+    uint64_t render_ns;       /* ... uploading and rendering batches (until the pages are done) */
+    uint64_t download_ns;     /* ... copying pages back to the requests' buffers */
 } rrb_server_stats_t;
 int rrb_server_create(const rrb_server_config* cfg, rrb_server** out);
 int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* host_pages, size_t host_pages_len,
@@ -357,8 +360,9 @@ int rrb_server_destroy(rrb_server* s);
  * shape of least predicted total time — from the autotuner table (16
  * entries, index page-size bin * 4 + edge-density bin, value 0..2 in the
  * order 16x16, 32x32, 64x16) when params is NULL, and 64x16 when both are
- * NULL. Features and predictions are computed in rrb_server_submit. Set the
- * model before submitting requests. */
+ * NULL. Features and predictions (rrb_mlp_predict_host: no device work in
+ * the submit path) are computed in rrb_server_submit. Set the model before
+ * submitting requests. */
 #define RRB_SCHED_SHORTEST_FIRST 1u
 #define RRB_SCHED_TILE_BY_MODEL 2u
 typedef struct {
@@ -390,6 +394,9 @@ int rrb_mlp_loss_grad(rrb_mlp* m, const float* X, const float* y, uint32_t n, fl
 int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32_t epochs, uint32_t batch,
                   float lr, uint64_t seed, float* final_loss);
 int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out);
+/* The forward pass on the host from a parameter vector: the same operations in
+ * the same order as the device kernel, so the same bits as rrb_mlp_predict. */
+int rrb_mlp_predict_host(const float* params, const float* X, uint32_t n, float* out);
 
 /* ---- page output (crates/encode pgm.rs / ppm.rs) -----------------------------
  * Netpbm bytes of a page already on the host: channels 1 writes P5 (Gray8),

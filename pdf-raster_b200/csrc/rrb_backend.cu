@@ -63,7 +63,7 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
-    Scratch s_run_off, s_runs;
+    Scratch s_run_off, s_runs, s_chunk_path;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
@@ -91,46 +91,39 @@ int cuda_err(rrb_ctx* c, cudaError_t e, const char* what) {
         if (e__ != cudaSuccess) return cuda_err(ctx, e__, #call); \
     } while (0)
 
-// Device memory within the context's budget. Scratch (`ordered`) comes from
-// the device's stream-ordered pool on the context's stream: allocating and
-// freeing it neither synchronises the device nor waits for other streams,
-// so contexts on other host threads (server workers) keep running while one
-// of them grows its scratch. Buffers handed to the caller use cudaMalloc.
-int dev_alloc(rrb_ctx* c, size_t bytes, void** out, bool ordered = false) {
+int dev_alloc(rrb_ctx* c, size_t bytes, void** out) {
     if (c->budget && c->used + bytes > c->budget)
         return set_err(c, RRB_ERR_OUT_OF_MEMORY,
                        "device allocation of " + std::to_string(bytes) + " bytes exceeds the budget");
-    cudaError_t e = ordered ? cudaMallocAsync(out, bytes, c->stream) : cudaMalloc(out, bytes);
+    cudaError_t e = cudaMalloc(out, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return set_err(c, RRB_ERR_OUT_OF_MEMORY, std::string(ordered ? "cudaMallocAsync: " : "cudaMalloc: ") +
-                                                     cudaGetErrorString(e));
+        return set_err(c, RRB_ERR_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     }
     c->used += bytes;
     return RRB_OK;
 }
 
-void dev_free(rrb_ctx* c, void* p, size_t bytes, bool ordered = false) {
+void dev_free(rrb_ctx* c, void* p, size_t bytes) {
     if (!p) return;
-    if (ordered) cudaFreeAsync(p, c->stream);
-    else cudaFree(p);
+    cudaFree(p);
     c->used -= std::min<uint64_t>(c->used, bytes);
 }
 
-// Grow a scratch buffer to at least `bytes` (x1.25 headroom); contents are not
-// kept. The old buffer is released in stream order, after the work queued on
-// the context's stream that still reads it.
+// Grow a scratch buffer to at least `bytes` (x1.25 headroom); contents are not kept.
 int ensure(rrb_ctx* c, Scratch& s, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (s.cap >= bytes) return RRB_OK;
     if (s.p) {
-        dev_free(c, s.p, s.cap, true);
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return cuda_err(c, e, "cudaStreamSynchronize");
+        dev_free(c, s.p, s.cap);
         s.p = nullptr;
         s.cap = 0;
     }
     size_t want = bytes + bytes / 4;
     want = (want + 255) & ~size_t(255);
-    int rc = dev_alloc(c, want, &s.p, true);
+    int rc = dev_alloc(c, want, &s.p);
     if (rc) return rc;
     s.cap = want;
     return RRB_OK;
@@ -344,7 +337,7 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
             s->cap = 0;
             continue;
         }
-        dev_free(c, s->p, s->cap, true);
+        dev_free(c, s->p, s->cap);
         s->p = nullptr;
         s->cap = 0;
     }
@@ -534,12 +527,16 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage_end(c, 8);
     stage(c, 9);
     if (n_chunks) {
+        if ((rc = ensure(c, c->s_chunk_path, n_chunks * sizeof(uint32_t)))) return rc;
+        k_chunk_paths<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(as<uint32_t>(c->s_chunks), NP,
+                                                                            as<uint32_t>(c->s_chunk_path));
+        c->launches += 1;
         int g = grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16);
         k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
             gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
             static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
-            as<BatchCounters>(c->s_ctr));
+            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path));
         c->launches += 1;
     }
     if (n_runs) {
@@ -660,16 +657,13 @@ void release_scratch(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
                       &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
-                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
+                      &c->s_chunk_path};
     for (Scratch* x : all) {
-        dev_free(c, x->p, x->cap, true);
+        dev_free(c, x->p, x->cap);
         x->p = nullptr;
         x->cap = 0;
     }
-    // Hand the freed scratch back to the device, not just to the pool.
-    cudaStreamSynchronize(c->stream);
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
 }
 
 // Pages [pg0, pg1) of B as a batch of their own: the inputs are views into
@@ -844,14 +838,6 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
         delete c;
         return RRB_ERR_DEVICE;
     }
-    // Scratch comes from the device's default stream-ordered pool; keep what
-    // is freed there cached for the next batch instead of returning it to the
-    // device at every synchronisation.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
     e = cudaMallocHost(reinterpret_cast<void**>(&c->h_read), 4096);
     if (e != cudaSuccess) {
         cudaStreamDestroy(c->stream);
@@ -875,9 +861,10 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
-                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs};
-    for (Scratch* s : all) dev_free(c, s->p, s->cap, true);
-    for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap, true);
+                      &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
+                      &c->s_chunk_path};
+    for (Scratch* s : all) dev_free(c, s->p, s->cap);
+    for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);
         delete c->tmp_batch;

@@ -753,6 +753,15 @@ __device__ __forceinline__ int sort_and_walk(int n, int32_t mask, int32_t aa_wid
         nonterm);
 }
 
+// Owner path of every row chunk (one warp per path writes its chunk range).
+__global__ void k_chunk_paths(const uint32_t* __restrict__ chunk_off, uint32_t n_paths,
+                              uint32_t* __restrict__ chunk_path) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = warp_g; p < n_paths; p += nwarps)
+        for (uint32_t c = chunk_off[p] + lane; c < chunk_off[p + 1]; c += 32) chunk_path[c] = p;
+}
+
 // Row stage: one warp per chunk of 32 AA rows of one path, lane = row.
 // Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the four
 // sub-rows of one pixel row; their spans are merged into coverage cells by
@@ -762,7 +771,8 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
     const Edge* __restrict__ edges, const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax,
     const uint32_t* __restrict__ page_w, uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
-    uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr) {
+    uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr,
+    const uint32_t* __restrict__ chunk_path) {
     __shared__ int32_t sx0[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t sx1[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t scn[ROWS_WARPS][KCAP * 32];
@@ -772,13 +782,7 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
     for (uint32_t c = blockIdx.x * ROWS_WARPS + w; c < total_chunks; c += gridDim.x * ROWS_WARPS) {
-        uint32_t lo = 0, hi = n_paths;  // path owning chunk c: last p with chunk_off[p] <= c
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (chunk_off[mid] <= c) lo = mid;
-            else hi = mid;
-        }
-        const uint32_t p = lo;
+        const uint32_t p = chunk_path[c];  // path owning chunk c
         const PathInfo P = info[p];
         const int32_t chunk_lo = (P.y0 & ~3) + static_cast<int32_t>(c - chunk_off[p]) * 32;
         const int32_t chunk_hi = min(chunk_lo + 31, P.y1);

@@ -295,4 +295,38 @@ int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out) {
     return RRB_OK;
 }
 
+// The same forward pass on the host, operation for operation (fmaf chains in
+// the kernel's order, the output summed as the kernel's two-warp butterfly),
+// so its predictions equal rrb_mlp_predict's bit for bit. For callers that
+// must not wait on the device (a scheduler deciding while kernels run).
+int rrb_mlp_predict_host(const float* params, const float* X, uint32_t n, float* out) {
+    if (!params || (!X && n) || (!out && n)) return RRB_ERR_INVARIANT;
+    float h1[H], h2[H], o[H];
+    for (uint32_t s = 0; s < n; ++s) {
+        const float* x = X + static_cast<size_t>(s) * IN;
+        for (int j = 0; j < H; ++j) {
+            float a = params[OFF_B1 + j];
+            for (int k = 0; k < IN; ++k) a = std::fmaf(params[OFF_W1 + j * IN + k], x[k], a);
+            h1[j] = std::fmax(a, 0.f);
+        }
+        for (int j = 0; j < H; ++j) {
+            float a = params[OFF_B2 + j];
+            for (int k = 0; k < H; ++k) a = std::fmaf(params[OFF_W2 + j * H + k], h1[k], a);
+            h2[j] = std::fmax(a, 0.f);
+            o[j] = params[OFF_W3 + j] * h2[j];
+        }
+        // __shfl_xor_sync butterfly within each warp of 32 lanes.
+        for (int w = 0; w < H / 32; ++w) {
+            float* v = o + 32 * w;
+            for (int d = 16; d; d >>= 1) {
+                float t[32];
+                for (int l = 0; l < 32; ++l) t[l] = v[l] + v[l ^ d];
+                for (int l = 0; l < 32; ++l) v[l] = t[l];
+            }
+        }
+        out[s] = (o[0] + o[32]) + params[OFF_B3];
+    }
+    return RRB_OK;
+}
+
 }  // extern "C"

@@ -62,10 +62,10 @@ struct rrb_server {
     uint64_t in_use = 0, peak_in_use = 0;
     uint64_t batches = 0, batched_requests = 0, completed = 0;
     uint64_t tile_batches[3] = {0, 0, 0};
+    uint64_t prep_ns = 0, render_ns = 0, download_ns = 0;
     bool stop = false;
     // Cost model (set before traffic; read by submitters and workers).
-    std::mutex mlp_mu;
-    rrb_mlp* mlp = nullptr;
+    std::vector<float> params;  // MLP parameters (evaluated on the host)
     bool have_params = false, have_table = false;
     uint32_t policy = 0;
     float x_mean[RRB_MLP_IN], x_std[RRB_MLP_IN], y_mean = 0, y_std = 1;
@@ -155,6 +155,9 @@ void worker(rrb_server* s, int wi) {
             s->tile_batches[shape] += 1;
         }
         const auto t_start = Clock::now();
+        auto ns_since = [](Clock::time_point a) {
+            return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - a).count());
+        };
         // Concatenate the requests into one batch over one device arena.
         st.pts.clear(); st.flags.clear(); st.rule.clear(); st.gray.clear(); st.alpha.clear();
         st.off.assign(1, 0); st.page_off.clear(); st.path_page.clear(); st.pw.clear(); st.ph.clear();
@@ -205,6 +208,8 @@ void worker(rrb_server* s, int wi) {
         b.page_offset = st.page_off.data();
         b.n_pages = static_cast<uint32_t>(st.pw.size());
         b.pages = arena;
+        const uint64_t prep = ns_since(t_start);
+        const auto t_render = Clock::now();
         rrb_fence f = 0;
         if (!rc) rc = rrb_begin_page(c);
         if (!rc) {
@@ -215,14 +220,20 @@ void worker(rrb_server* s, int wi) {
             if (!rc) rc = rc2;
         }
         if (!rc) rc = rrb_wait_page(c, f, 0);
+        const uint64_t render = ns_since(t_render);
+        const auto t_down = Clock::now();
         for (size_t k = 0; k < batch.size() && !rc; ++k) {
             rrb_fence df = 0;
             rc = rrb_download_async(c, arena, req_arena_off[k], batch[k]->out, batch[k]->out_len, &df);
             if (!rc) rc = rrb_wait_download(c, df);
         }
         const auto t_done = Clock::now();
+        const uint64_t down = ns_since(t_down);
         {
             std::lock_guard<std::mutex> lk(s->m);
+            s->prep_ns += prep;
+            s->render_ns += render;
+            s->download_ns += down;
             s->in_use -= bytes;
             for (Request* r : batch) {
                 r->status = rc;
@@ -265,11 +276,8 @@ int predict_request(rrb_server* s, Request* r) {
         X[i] = (X[i] - s->x_mean[j]) / s->x_std[j];
     }
     std::vector<float> y(static_cast<size_t>(n) * 3);
-    {
-        std::lock_guard<std::mutex> lk(s->mlp_mu);
-        int rc = rrb_mlp_predict(s->mlp, X.data(), n * 3, y.data());
-        if (rc) return rc;
-    }
+    int rc = rrb_mlp_predict_host(s->params.data(), X.data(), n * 3, y.data());
+    if (rc) return rc;
     for (int k = 0; k < 3; ++k) r->pred[k] = 0;
     for (uint32_t pg = 0; pg < n; ++pg)
         for (int k = 0; k < 3; ++k) r->pred[k] += std::exp(y[pg * 3 + k] * s->y_std + s->y_mean);
@@ -287,14 +295,9 @@ int rrb_server_set_cost_model(rrb_server* s, const rrb_server_cost_model* m) {
     if (m->table)
         for (int k = 0; k < 16; ++k)
             if (m->table[k] < 0 || m->table[k] > 2) return RRB_ERR_INVARIANT;
-    std::lock_guard<std::mutex> lk(s->mlp_mu);
+    std::lock_guard<std::mutex> lk(s->m);
     if (m->params) {
-        if (!s->mlp) {
-            int rc = rrb_mlp_create(s->cfg.device, 0, &s->mlp);
-            if (rc) return rc;
-        }
-        int rc = rrb_mlp_set_params(s->mlp, m->params);
-        if (rc) return rc;
+        s->params.assign(m->params, m->params + RRB_MLP_PARAMS);
         std::memcpy(s->x_mean, m->x_mean, sizeof s->x_mean);
         std::memcpy(s->x_std, m->x_std, sizeof s->x_std);
         s->y_mean = m->y_mean;
@@ -398,6 +401,9 @@ int rrb_server_stats(rrb_server* s, rrb_server_stats_t* out) {
     out->in_use_bytes = s->in_use;
     out->peak_in_use_bytes = s->peak_in_use;
     for (int k = 0; k < 3; ++k) out->tile_batches[k] = s->tile_batches[k];
+    out->prep_ns = s->prep_ns;
+    out->render_ns = s->render_ns;
+    out->download_ns = s->download_ns;
     return RRB_OK;
 }
 
@@ -410,7 +416,6 @@ int rrb_server_destroy(rrb_server* s) {
     s->cv_work.notify_all();
     for (std::thread& t : s->threads) t.join();
     for (rrb_ctx* c : s->ctx) rrb_destroy(c);
-    if (s->mlp) rrb_mlp_destroy(s->mlp);
     for (auto& kv : s->live) delete kv.second;
     delete s;
     return RRB_OK;

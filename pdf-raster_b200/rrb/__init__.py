@@ -643,6 +643,17 @@ class MLP:
             raise BackendError(rc, "train")
         return float(loss.value)
 
+    @staticmethod
+    def predict_host(params, X) -> np.ndarray:
+        """rrb_mlp_predict_host: the same forward pass on the host (same bits)."""
+        params = np.ascontiguousarray(params, np.float32)
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, MLP.N_IN)
+        out = np.empty(len(X), np.float32)
+        rc = lib().rrb_mlp_predict_host(_ptr(params, C.c_float), _ptr(X, C.c_float), len(X), _ptr(out, C.c_float))
+        if rc:
+            raise BackendError(rc, "predict_host")
+        return out
+
     def predict(self, X) -> np.ndarray:
         X = self._f32(X, (-1, self.N_IN))
         out = np.empty(len(X), np.float32)

@@ -127,7 +127,8 @@ class RequestResult(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("completed", "batches", "batched_requests", "queued", "in_use_bytes",
-                                          "peak_in_use_bytes")] + [("tile_batches", C.c_uint64 * 3)]
+                                          "peak_in_use_bytes")] + [("tile_batches", C.c_uint64 * 3)] + [
+        (n, C.c_uint64) for n in ("prep_ns", "render_ns", "download_ns")]
 
 
 class ServerCostModel(C.Structure):
@@ -216,6 +217,8 @@ SIGNATURES = {
                                     C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "rrb_mlp_train": (C.c_int, [VP, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32, C.c_uint32, C.c_uint32,
                                 C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "rrb_mlp_predict_host": (C.c_int, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint32,
+                                       C.POINTER(C.c_float)]),
     "rrb_mlp_predict": (C.c_int, [VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_float)]),
     "rrb_path_new": (VP, []),
     "rrb_path_free": (None, [VP]),

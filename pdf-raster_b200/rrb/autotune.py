@@ -243,7 +243,7 @@ def main(argv=None):
     parts = [np.load(p) for p in a.data]
     X = np.concatenate([p["X"] for p in parts])
     T = np.concatenate([p["ms"] for p in parts])
-    h = min(a.holdout, len(T) // 5)
+    h = min(a.holdout, len(T) // 2)
     model = train(X[:-h], T[:-h], epochs=a.epochs)
     model.save(a.out)
     if a.holdout_out:

@@ -53,7 +53,7 @@ STRUCTS = {
                                            "tile_h", "reserved"]),
     "rrb_request_result": ("RequestResult", ["status", "latency_ns", "queue_ns"]),
     "rrb_server_stats_t": ("ServerStats", ["completed", "batches", "batched_requests", "queued", "in_use_bytes",
-                                           "peak_in_use_bytes", "tile_batches"]),
+                                           "peak_in_use_bytes", "tile_batches", "prep_ns", "render_ns", "download_ns"]),
     "rrb_server_cost_model": ("ServerCostModel", ["params", "x_mean", "x_std", "y_mean", "y_std", "table", "policy"]),
     "rrb_aa_fill_params": ("AaFillParams", ["segs", "n_segs", "coverage", "width", "height", "fill_rule"]),
     "rrb_tile_record": ("TileRecord", ["key", "x_enter", "dxdy", "y0_tile", "y1_tile", "sign", "pad", "pad2"]),

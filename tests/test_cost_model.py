@@ -111,3 +111,21 @@ def test_cost_model_round_trips(tmp_path):
     r = CostModel.load(tmp_path / "m.npz")
     assert np.array_equal(r.params, m.params) and r.y_mean == 0.5 and r.y_std == 1.5
     assert np.array_equal(r.table, m.table)
+
+
+def test_host_forward_matches_oracle(rrb_lib):
+    w = _params(13)
+    X, _ = _data(300, seed=4)
+    got = rrb_lib.MLP.predict_host(w, X)
+    np.testing.assert_allclose(got, mlp_oracle.forward(w, X)[0], rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_host_forward_equals_device_forward(rrb_lib):
+    w = _params(17)
+    X, _ = _data(777, seed=8)
+    m = rrb_lib.MLP(0)
+    m.set_params(w)
+    dev = m.predict(X)
+    m.close()
+    assert np.array_equal(dev.view(np.uint32), rrb_lib.MLP.predict_host(w, X).view(np.uint32))
