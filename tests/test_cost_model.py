@@ -129,3 +129,27 @@ def test_host_forward_equals_device_forward(rrb_lib):
     dev = m.predict(X)
     m.close()
     assert np.array_equal(dev.view(np.uint32), rrb_lib.MLP.predict_host(w, X).view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_trained_model_beats_the_default_tile_on_held_out_pages(rrb_lib):
+    """The committed model (trained on 50,100 (page, tile) pairs) against the
+    5,000 held-out pages of the sweep: its per-page tile choice costs less
+    measured device time than the fixed 64x16 default, about as little as the
+    autotuner table, and its time predictions stay within 20% on average."""
+    from pathlib import Path
+
+    from rrb.autotune import CostModel, evaluate
+
+    root = Path(__file__).resolve().parents[1]
+    model = CostModel.load(root / "pdf-raster_b200" / "rrb" / "cost_model.npz")
+    d = np.load(root / "tests" / "golden" / "cost_model_holdout.npz")
+    rep = evaluate(model, d["X"], d["ms"])
+    assert rep["pages"] == 5000
+    assert rep["model_vs_default"] > 1.05
+    assert rep["model_vs_table"] > 0.98
+    assert rep["mape"] < 0.2
+    # The device and host forward passes give the same choices.
+    X = d["X"][:200]
+    host = rrb_lib.MLP.predict_host(model.params, model.norm(X.reshape(-1, 24))).reshape(-1, 3)
+    assert np.array_equal(np.argmin(host, 1), model.choose(X))
