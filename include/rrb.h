@@ -330,7 +330,8 @@ typedef struct {
     uint64_t mem_budget_bytes; /* admission cap on in-flight device bytes; 0 = none */
     uint32_t max_batch_pages;  /* pages per batch; 0 = 64 */
     uint32_t tile_w, tile_h;   /* 0 = default tile */
-    uint32_t reserved[3];
+    uint32_t predict_threads;  /* host threads computing cost-model predictions; 0 = 4 */
+    uint32_t reserved[2];
 } rrb_server_config;
 typedef struct {
     int status;
@@ -360,9 +361,10 @@ int rrb_server_destroy(rrb_server* s);
  * shape of least predicted total time — from the autotuner table (16
  * entries, index page-size bin * 4 + edge-density bin, value 0..2 in the
  * order 16x16, 32x32, 64x16) when params is NULL, and 64x16 when both are
- * NULL. Features and predictions (rrb_mlp_predict_host: no device work in
- * the submit path) are computed in rrb_server_submit. Set the model before
- * submitting requests. */
+ * NULL. Features and predictions (rrb_page_features_all, rrb_mlp_predict_host:
+ * host work only) are computed by predict_threads host threads between submit
+ * and the queue, so submitting stays cheap. Set the model before submitting
+ * requests. */
 #define RRB_SCHED_SHORTEST_FIRST 1u
 #define RRB_SCHED_TILE_BY_MODEL 2u
 typedef struct {
@@ -419,6 +421,9 @@ int rrb_encode_netpbm(const uint8_t* pixels, uint32_t width, uint32_t height, ui
  *  21-23 tile shape one-hot (16x16, 32x32, 64x16) */
 int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, uint32_t tile_w, uint32_t tile_h,
                       float* out);
+/* The features of all three tile shapes in one pass: out[3][RRB_MLP_IN], rows
+ * 16x16, 32x32, 64x16. */
+int rrb_page_features_all(const rrb_path_batch_params* p, uint32_t page, float* out);
 
 /* ---- path construction on the host (A1, A2) --------------------------------
  * PathBuilder::{move_to, line_to, curve_to, close} (crates/raster/src/path/

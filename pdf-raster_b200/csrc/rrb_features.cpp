@@ -34,23 +34,24 @@ int tile_index(uint32_t w, uint32_t h) {
     return -1;
 }
 
-}  // namespace
-
-extern "C" int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, uint32_t tile_w, uint32_t tile_h,
-                                 float* out) {
+// All three tile shapes of one page in one pass over its points: the
+// shape-independent features once, then one difference-array histogram per
+// tile shape. out: [3][RRB_MLP_IN], rows in the order 16x16, 32x32, 64x16.
+int features_all(const rrb_path_batch_params* p, uint32_t page, float* out) {
     if (!p || !out || page >= p->n_pages || !p->page_width || !p->page_height) return RRB_ERR_INVARIANT;
-    const int ti = tile_index(tile_w, tile_h);
-    if (ti < 0) return RRB_ERR_INVARIANT;
     if (p->n_paths && (!p->path_page || !p->path_pt_off || !p->pts || !p->flags || !p->fill_rule || !p->alpha))
         return RRB_ERR_INVARIANT;
     const double W = p->page_width[page], H = p->page_height[page];
     const double* m = p->matrix;
-    // Paths of this page: path_page is non-decreasing.
+    const bool ident = m[0] == 1.0 && m[1] == 0.0 && m[2] == 0.0 && m[3] == 1.0 && m[4] == 0.0 && m[5] == 0.0;
     const uint32_t* pp = p->path_page;
     const uint64_t b = p->n_paths ? static_cast<uint64_t>(std::lower_bound(pp, pp + p->n_paths, page) - pp) : 0;
     const uint64_t e = p->n_paths ? static_cast<uint64_t>(std::upper_bound(pp, pp + p->n_paths, page) - pp) : 0;
-    const uint32_t gw = static_cast<uint32_t>((W + tile_w - 1) / tile_w), gh = static_cast<uint32_t>((H + tile_h - 1) / tile_h);
-    std::vector<int32_t> diff(static_cast<size_t>(gw + 1) * (gh + 1), 0);
+    struct Box {
+        double x0, y0, x1, y1;
+    };
+    std::vector<Box> boxes;
+    boxes.reserve(e - b);
     double n_pts = 0, n_lines = 0, n_curves = 0, edges = 0, length = 0, area_sum = 0;
     double eo = 0, translucent = 0, recti = 0;
     for (uint64_t k = b; k < e; ++k) {
@@ -63,7 +64,8 @@ extern "C" int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, 
         double px = 0, py = 0;
         for (uint64_t i = a0; i < a1; ++i) {
             const double sx = p->pts[2 * i], sy = p->pts[2 * i + 1];
-            const double x = m[0] * sx + m[2] * sy + m[4], y = m[1] * sx + m[3] * sy + m[5];
+            const double x = ident ? sx : m[0] * sx + m[2] * sy + m[4];
+            const double y = ident ? sy : m[1] * sx + m[3] * sy + m[5];
             x0 = std::min(x0, x);
             y0 = std::min(y0, y);
             x1 = std::max(x1, x);
@@ -81,13 +83,15 @@ extern "C" int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, 
                         }
                         n_curves += 1;
                         edges += cubic_pieces(q, p->flatness);
-                        length += std::hypot(q[6] - q[0], q[7] - q[1]);
+                        const double dx = q[6] - q[0], dy = q[7] - q[1];
+                        length += std::sqrt(dx * dx + dy * dy);
                         axis = false;
                     }
                 } else if (!(i > a0 + 1 && (p->flags[i - 1] & RRB_PATH_CURVE))) {
                     n_lines += 1;
                     edges += 1;
-                    length += std::hypot(x - px, y - py);
+                    const double dx = x - px, dy = y - py;
+                    length += std::sqrt(dx * dx + dy * dy);
                     axis = axis && (x == px || y == py);
                 }
             }
@@ -100,48 +104,77 @@ extern "C" int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, 
         const double cx1 = std::min(W, x1), cy1 = std::min(H, y1);
         if (cx0 >= cx1 || cy0 >= cy1) continue;
         area_sum += (cx1 - cx0) * (cy1 - cy0);
-        const uint32_t tx0 = static_cast<uint32_t>(cx0 / tile_w), ty0 = static_cast<uint32_t>(cy0 / tile_h);
-        const uint32_t tx1 = std::min(gw - 1, static_cast<uint32_t>(cx1 / tile_w));
-        const uint32_t ty1 = std::min(gh - 1, static_cast<uint32_t>(cy1 / tile_h));
-        const size_t s = gw + 1;
-        diff[ty0 * s + tx0] += 1;
-        diff[ty0 * s + tx1 + 1] -= 1;
-        diff[(ty1 + 1) * s + tx0] -= 1;
-        diff[(ty1 + 1) * s + tx1 + 1] += 1;
+        boxes.push_back({cx0, cy0, cx1, cy1});
     }
-    // Paths per tile (2-D prefix sum of the rectangle marks) -> 8-bin histogram
-    // in powers of 4.
-    double hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    std::vector<int32_t> row(gw + 1, 0);
-    for (uint32_t y = 0; y < gh; ++y) {
-        int32_t run = 0;
-        for (uint32_t x = 0; x < gw; ++x) {
-            row[x] += diff[static_cast<size_t>(y) * (gw + 1) + x];
-            run += row[x];
-            int bin = 0;
-            for (int32_t v = run; v > 0 && bin < 7; v >>= 2) ++bin;  // 0, 1-3, 4-15, 16-63, ..., >= 4096
-            hist[bin] += 1;
+    const double n_paths = static_cast<double>(e - b), segs = n_lines + n_curves;
+    float base[13];
+    base[0] = static_cast<float>(std::log1p(W * H));
+    base[1] = static_cast<float>(std::log1p(n_paths));
+    base[2] = static_cast<float>(std::log1p(n_pts));
+    base[3] = static_cast<float>(segs > 0 ? n_lines / segs : 0);
+    base[4] = static_cast<float>(std::log1p(n_curves));
+    base[5] = static_cast<float>(std::log1p(edges));
+    base[6] = static_cast<float>(std::log1p(segs > 0 ? length / segs : 0));
+    base[7] = static_cast<float>(std::log1p(area_sum / (W * H)));
+    base[8] = static_cast<float>(std::log1p(n_paths > 0 ? area_sum / n_paths : 0));
+    base[9] = static_cast<float>(n_paths > 0 ? eo / n_paths : 0);
+    base[10] = static_cast<float>(n_paths > 0 ? translucent / n_paths : 0);
+    base[11] = static_cast<float>(n_paths > 0 ? recti / n_paths : 0);
+    static const uint32_t kShape[3][2] = {{16, 16}, {32, 32}, {64, 16}};
+    std::vector<int32_t> diff;
+    for (int t = 0; t < 3; ++t) {
+        const uint32_t tw = kShape[t][0], th = kShape[t][1];
+        const uint32_t gw = static_cast<uint32_t>((W + tw - 1) / tw), gh = static_cast<uint32_t>((H + th - 1) / th);
+        diff.assign(static_cast<size_t>(gw + 1) * (gh + 1), 0);
+        const size_t st = gw + 1;
+        for (const Box& bx : boxes) {
+            const uint32_t tx0 = static_cast<uint32_t>(bx.x0 / tw), ty0 = static_cast<uint32_t>(bx.y0 / th);
+            const uint32_t tx1 = std::min(gw - 1, static_cast<uint32_t>(bx.x1 / tw));
+            const uint32_t ty1 = std::min(gh - 1, static_cast<uint32_t>(bx.y1 / th));
+            diff[ty0 * st + tx0] += 1;
+            diff[ty0 * st + tx1 + 1] -= 1;
+            diff[(ty1 + 1) * st + tx0] -= 1;
+            diff[(ty1 + 1) * st + tx1 + 1] += 1;
         }
+        // Paths per tile (2-D prefix sum of the rectangle marks) -> 8-bin
+        // histogram in powers of 4.
+        double hist[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        std::vector<int32_t> col(gw + 1, 0);
+        for (uint32_t y = 0; y < gh; ++y) {
+            int32_t run = 0;
+            for (uint32_t x = 0; x < gw; ++x) {
+                col[x] += diff[static_cast<size_t>(y) * st + x];
+                run += col[x];
+                int bin = 0;
+                for (int32_t v = run; v > 0 && bin < 7; v >>= 2) ++bin;  // 0, 1-3, 4-15, ..., >= 4096
+                hist[bin] += 1;
+            }
+        }
+        const double tiles = static_cast<double>(gw) * gh;
+        float* o = out + t * RRB_MLP_IN;
+        for (int k = 0; k < 12; ++k) o[k] = base[k];
+        o[12] = static_cast<float>(tiles > 0 ? 1.0 - hist[0] / tiles : 0);
+        for (int k = 0; k < 8; ++k) o[13 + k] = static_cast<float>(tiles > 0 ? hist[k] / tiles : 0);
+        o[21] = t == 0 ? 1.f : 0.f;
+        o[22] = t == 1 ? 1.f : 0.f;
+        o[23] = t == 2 ? 1.f : 0.f;
     }
-    const double tiles = static_cast<double>(gw) * gh, n_paths = static_cast<double>(e - b);
-    const double segs = n_lines + n_curves;
-    float* o = out;
-    o[0] = static_cast<float>(std::log1p(W * H));
-    o[1] = static_cast<float>(std::log1p(n_paths));
-    o[2] = static_cast<float>(std::log1p(n_pts));
-    o[3] = static_cast<float>(segs > 0 ? n_lines / segs : 0);
-    o[4] = static_cast<float>(std::log1p(n_curves));
-    o[5] = static_cast<float>(std::log1p(edges));
-    o[6] = static_cast<float>(std::log1p(segs > 0 ? length / segs : 0));
-    o[7] = static_cast<float>(std::log1p(area_sum / (W * H)));
-    o[8] = static_cast<float>(std::log1p(n_paths > 0 ? area_sum / n_paths : 0));
-    o[9] = static_cast<float>(n_paths > 0 ? eo / n_paths : 0);
-    o[10] = static_cast<float>(n_paths > 0 ? translucent / n_paths : 0);
-    o[11] = static_cast<float>(n_paths > 0 ? recti / n_paths : 0);
-    o[12] = static_cast<float>(tiles > 0 ? 1.0 - hist[0] / tiles : 0);
-    for (int k = 0; k < 8; ++k) o[13 + k] = static_cast<float>(tiles > 0 ? hist[k] / tiles : 0);
-    o[21] = ti == 0 ? 1.f : 0.f;
-    o[22] = ti == 1 ? 1.f : 0.f;
-    o[23] = ti == 2 ? 1.f : 0.f;
+    return RRB_OK;
+}
+
+}  // namespace
+
+extern "C" int rrb_page_features_all(const rrb_path_batch_params* p, uint32_t page, float* out) {
+    return features_all(p, page, out);
+}
+
+extern "C" int rrb_page_features(const rrb_path_batch_params* p, uint32_t page, uint32_t tile_w, uint32_t tile_h,
+                                 float* out) {
+    const int ti = tile_index(tile_w, tile_h);
+    if (ti < 0 || !out) return RRB_ERR_INVARIANT;
+    float all[3 * RRB_MLP_IN];
+    const int rc = features_all(p, page, all);
+    if (rc) return rc;
+    std::memcpy(out, all + ti * RRB_MLP_IN, RRB_MLP_IN * sizeof(float));
     return RRB_OK;
 }

@@ -55,8 +55,10 @@ struct rrb_server {
     std::vector<rrb_ctx*> ctx;
     std::vector<std::thread> threads;
     std::mutex m;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_pred;
     std::deque<Request*> queue;
+    std::deque<Request*> pending;  // waiting for their cost-model prediction
+    std::vector<std::thread> predictors;
     std::unordered_map<uint64_t, Request*> live;
     uint64_t next_id = 1;
     uint64_t in_use = 0, peak_in_use = 0;
@@ -256,9 +258,8 @@ int predict_request(rrb_server* s, Request* r) {
     std::vector<float> X(static_cast<size_t>(n) * 3 * RRB_MLP_IN);
     uint64_t biggest = 0;
     for (uint32_t pg = 0; pg < n; ++pg) {
-        for (int k = 0; k < 3; ++k) {
-            float* x = &X[(static_cast<size_t>(pg) * 3 + k) * RRB_MLP_IN];
-            int rc = rrb_page_features(&r->p, pg, kTiles[k][0], kTiles[k][1], x);
+        {
+            int rc = rrb_page_features_all(&r->p, pg, &X[static_cast<size_t>(pg) * 3 * RRB_MLP_IN]);
             if (rc) return rc;
         }
         const uint64_t px = static_cast<uint64_t>(r->p.page_width[pg]) * r->p.page_height[pg];
@@ -285,6 +286,35 @@ int predict_request(rrb_server* s, Request* r) {
     return RRB_OK;
 }
 
+// Predictor thread: computes the predictions of submitted requests and moves
+// them to the render queue.
+void predictor(rrb_server* s) {
+    for (;;) {
+        Request* r;
+        {
+            std::unique_lock<std::mutex> lk(s->m);
+            s->cv_pred.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+            if (s->pending.empty()) break;  // stopping
+            r = s->pending.front();
+            s->pending.pop_front();
+        }
+        const int rc = predict_request(s, r);
+        {
+            std::lock_guard<std::mutex> lk(s->m);
+            if (rc) {
+                r->status = rc;
+                r->t_start = r->t_done = Clock::now();
+                r->done = true;
+                s->completed += 1;
+            } else {
+                s->queue.push_back(r);
+            }
+        }
+        if (rc) s->cv_done.notify_all();
+        else s->cv_work.notify_one();
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -307,6 +337,10 @@ int rrb_server_set_cost_model(rrb_server* s, const rrb_server_cost_model* m) {
     s->have_table = m->table != nullptr;
     if (m->table) std::memcpy(s->table, m->table, sizeof s->table);
     s->policy = m->policy;
+    if ((s->have_params || s->have_table) && s->predictors.empty()) {
+        const uint32_t n = s->cfg.predict_threads ? s->cfg.predict_threads : 4;
+        for (uint32_t i = 0; i < n; ++i) s->predictors.emplace_back(predictor, s);
+    }
     return RRB_OK;
 }
 
@@ -345,26 +379,23 @@ int rrb_server_submit(rrb_server* s, const rrb_path_batch_params* p, uint8_t* ho
     const auto t0 = Clock::now();
     Request* r = new Request();
     r->p = *p;
-    if (s->have_params || s->have_table) {
-        rc = predict_request(s, r);
-        if (rc) {
-            delete r;
-            return rc;
-        }
-    }
     r->out = host_pages;
     r->out_len = host_pages_len;
     r->init = init_value;
     r->est_bytes = estimate_bytes(*p);
     r->t_submit = t0;
+    bool predicted = false;
     {
         std::lock_guard<std::mutex> lk(s->m);
         r->id = s->next_id++;
         s->live[r->id] = r;
-        s->queue.push_back(r);
+        predicted = !s->predictors.empty();
+        if (predicted) s->pending.push_back(r);
+        else s->queue.push_back(r);
     }
     *ticket = r->id;
-    s->cv_work.notify_one();
+    if (predicted) s->cv_pred.notify_one();
+    else s->cv_work.notify_one();
     return RRB_OK;
 }
 
@@ -413,6 +444,8 @@ int rrb_server_destroy(rrb_server* s) {
         std::lock_guard<std::mutex> lk(s->m);
         s->stop = true;
     }
+    s->cv_pred.notify_all();
+    for (std::thread& t : s->predictors) t.join();
     s->cv_work.notify_all();
     for (std::thread& t : s->threads) t.join();
     for (rrb_ctx* c : s->ctx) rrb_destroy(c);

@@ -473,9 +473,10 @@ class Server:
     """Continuous-batching page-render server (rrb_server_*)."""
 
     def __init__(self, device: int = 0, workers: int = 2, mem_budget: int = 0, max_batch_pages: int = 64,
-                 tile: tuple[int, int] = (0, 0)):
+                 tile: tuple[int, int] = (0, 0), predict_threads: int = 0):
         cfg = ServerConfig(device=device, workers=workers, mem_budget_bytes=mem_budget,
-                           max_batch_pages=max_batch_pages, tile_w=tile[0], tile_h=tile[1])
+                           max_batch_pages=max_batch_pages, tile_w=tile[0], tile_h=tile[1],
+                           predict_threads=predict_threads)
         h = C.c_void_p()
         rc = lib().rrb_server_create(C.byref(cfg), C.byref(h))
         if rc:
@@ -572,6 +573,15 @@ def page_features(params: PathBatchParams, page: int, tile: tuple[int, int]) -> 
     rc = lib().rrb_page_features(C.byref(params), page, tile[0], tile[1], _ptr(out, C.c_float))
     if rc:
         raise BackendError(rc, "rrb_page_features")
+    return out
+
+
+def page_features_all(params: PathBatchParams, page: int) -> np.ndarray:
+    """[3, 24] features of one page for the tile shapes of TILE_SHAPES (rrb_page_features_all)."""
+    out = np.zeros((3, _abi.RRB_MLP_IN), np.float32)
+    rc = lib().rrb_page_features_all(C.byref(params), page, _ptr(out, C.c_float))
+    if rc:
+        raise BackendError(rc, "rrb_page_features_all")
     return out
 
 

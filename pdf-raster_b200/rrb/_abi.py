@@ -118,7 +118,8 @@ class StageTime(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("workers", C.c_uint32), ("mem_budget_bytes", C.c_uint64),
                 ("max_batch_pages", C.c_uint32), ("tile_w", C.c_uint32), ("tile_h", C.c_uint32),
-                ("reserved", C.c_uint32 * 3)]
+                ("predict_threads", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class RequestResult(C.Structure):
@@ -207,6 +208,7 @@ SIGNATURES = {
     "rrb_server_destroy": (C.c_int, [VP]),
     "rrb_encode_netpbm": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
+    "rrb_page_features_all": (C.c_int, [C.POINTER(PathBatchParams), C.c_uint32, C.POINTER(C.c_float)]),
     "rrb_page_features": (C.c_int, [C.POINTER(PathBatchParams), C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.POINTER(C.c_float)]),
     "rrb_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(VP)]),

@@ -31,7 +31,7 @@ from pathlib import Path
 
 import numpy as np
 
-from . import B200Backend, MLP, Scene, TILE_SHAPES, page_features
+from . import B200Backend, MLP, Scene, TILE_SHAPES, page_features_all
 
 DEFAULT_SHAPE = 2  # 64x16
 N_SHAPES = len(TILE_SHAPES)
@@ -49,7 +49,7 @@ def page_scene(seed: int) -> Scene:
 
 def features(scene: Scene, page: int = 0) -> np.ndarray:
     """[N_SHAPES, 24] features of one page, one row per tile shape."""
-    return np.stack([page_features(scene.view, page, t) for t in TILE_SHAPES])
+    return page_features_all(scene.view, page)
 
 
 def time_page(backend: B200Backend, scene: Scene, pages, reps: int = 2) -> np.ndarray:

@@ -50,7 +50,7 @@ STRUCTS = {
                                        "tile_pairs", "nonterminating_rows", "kernel_launches"]),
     "rrb_stage_time": ("StageTime", ["name", "ms", "launches"]),
     "rrb_server_config": ("ServerConfig", ["device", "workers", "mem_budget_bytes", "max_batch_pages", "tile_w",
-                                           "tile_h", "reserved"]),
+                                           "tile_h", "predict_threads", "reserved"]),
     "rrb_request_result": ("RequestResult", ["status", "latency_ns", "queue_ns"]),
     "rrb_server_stats_t": ("ServerStats", ["completed", "batches", "batched_requests", "queued", "in_use_bytes",
                                            "peak_in_use_bytes", "tile_batches", "prep_ns", "render_ns", "download_ns"]),
