@@ -250,6 +250,15 @@ int rrb_record_path_batch(rrb_ctx* ctx, const rrb_path_batch_params* p);
  * path_rgb[3p..3p+2] (host); the gray array is not read. Coverage, order and
  * every other rule are those of rrb_record_path_batch. */
 int rrb_record_path_batch_rgb(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb);
+/* The general batch: path_rgb != NULL selects Rgb8 pages as above; with
+ * clip_rects != NULL path p is clipped to the device-space rectangle
+ * clip_rects[4p..4p+3] = (x0, y0, x1, y1) (host doubles, any corner order):
+ * the path's clip is its page intersected with the rectangle, with the integer
+ * bounds floor(x_min) .. ceil(x_max) - 1 of Clip::clip_to_rect
+ * (crates/raster/src/clip.rs:116-125,266-271) — the reference's treatment of a
+ * rectangular W/W* clip path (detect_rect, clip.rs:130-140). */
+int rrb_record_path_batch_ex(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb,
+                             const double* clip_rects);
 /* rgb_to_gray (crates/pdf_raster/src/render.rs:1306-1324) on the device:
  * gray[i] = (2126 r + 7152 g + 722 b + 5000) / 10000 for n_px pixels. */
 int rrb_record_rgb_to_gray(rrb_ctx* ctx, const rrb_buf* rgb, size_t rgb_offset, const rrb_buf* gray,

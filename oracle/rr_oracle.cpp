@@ -757,9 +757,32 @@ namespace {
 
 // fill_impl for one path; `span(y, x0, shape, n)` composites a gamma-mapped
 // shape span onto pixel row y (the page's pixel format lives in `span`).
+// The clip of a fill: Clip::new(0, 0, W, H) and, with `rect`, clip_to_rect
+// (clip.rs:73-88,116-125,266-271): float bounds and their integer bounds.
+struct ClipRect {
+    double x_min, y_min, x_max, y_max;
+    int32_t x_min_i, y_min_i, x_max_i, y_max_i;
+};
+
+ClipRect make_clip(int32_t width, int32_t height, const double* rect) {
+    ClipRect c{0.0, 0.0, static_cast<double>(width), static_cast<double>(height), 0, 0, 0, 0};
+    if (rect) {
+        c.x_min = std::max(c.x_min, std::min(rect[0], rect[2]));
+        c.x_max = std::min(c.x_max, std::max(rect[0], rect[2]));
+        c.y_min = std::max(c.y_min, std::min(rect[1], rect[3]));
+        c.y_max = std::min(c.y_max, std::max(rect[1], rect[3]));
+    }
+    c.x_min_i = splash_floor(c.x_min);
+    c.y_min_i = splash_floor(c.y_min);
+    c.x_max_i = splash_ceil(c.x_max) - 1;
+    c.y_max_i = splash_ceil(c.y_max) - 1;
+    return c;
+}
+
 template <typename Span>
 void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint8_t* flags, int64_t n_pts,
-                    const double m[6], double flatness, int eo, int rowmap, or_stats* st, Span span) {
+                    const double m[6], double flatness, int eo, int rowmap, or_stats* st, Span span,
+                    const double* clip_rect = nullptr) {
     if (n_pts == 0) return;
     if (st) st->paths++;
     // XPath::new with close_subpaths = true, then aa_scale.
@@ -768,10 +791,11 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
     or_xpath_new(pts, flags, n_pts, m, flatness, 1, segs.data(), need);
     or_xpath_aa_scale(segs.data(), need);
     if (st) st->segments += static_cast<uint64_t>(need);
-    // Page clip integer bounds.
-    int32_t clip_x_min_i = splash_floor(0.0), clip_y_min_i = splash_floor(0.0);
-    int32_t clip_x_max_i = splash_ceil(static_cast<double>(width)) - 1;
-    int32_t clip_y_max_i = splash_ceil(static_cast<double>(height)) - 1;
+    // Clip integer bounds (the page, or the page and a clip rectangle).
+    const ClipRect cr = make_clip(width, height, clip_rect);
+    int32_t clip_x_min_i = cr.x_min_i, clip_y_min_i = cr.y_min_i;
+    int32_t clip_x_max_i = cr.x_max_i;
+    int32_t clip_y_max_i = cr.y_max_i;
     int32_t y_lo = clip_y_min_i * AA_SIZE;
     int32_t y_hi = (clip_y_max_i + 1) * AA_SIZE - 1;
     or_scanner* sc = or_scanner_new(segs.data(), need, eo, y_lo, y_hi, st);
@@ -782,7 +806,7 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
     // Clip::test_rect (clip.rs:196-215) against the page rectangle.
     int32_t left = sc->x_min / AA_SIZE, top = sc->y_min / AA_SIZE;
     int32_t right = sc->x_max / AA_SIZE, bottom = sc->y_max / AA_SIZE;
-    double cx_min = 0.0, cx_max = width, cy_min = 0.0, cy_max = height;
+    double cx_min = cr.x_min, cx_max = cr.x_max, cy_min = cr.y_min, cy_max = cr.y_max;
     bool all_outside = static_cast<double>(right + 1) <= cx_min || static_cast<double>(left) >= cx_max ||
                        static_cast<double>(bottom + 1) <= cy_min || static_cast<double>(top) >= cy_max;
     if (all_outside) {
@@ -847,7 +871,7 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
                        const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
                        const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
                        uint64_t n_paths, const double m[6], double flatness, int rowmap,
-                       int n_threads, or_stats* st);
+                       int n_threads, or_stats* st, const double* clip = nullptr);
 
 }  // namespace
 
@@ -882,6 +906,15 @@ void or_render_scene(uint8_t* arena, const uint64_t* page_off, const uint32_t* p
                       path_page, n_paths, m, flatness, rowmap, n_threads, st);
 }
 
+void or_render_scene_ex(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                        uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                        const uint8_t* rule, const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha,
+                        const uint32_t* path_page, uint64_t n_paths, const double* clip, const double m[6],
+                        double flatness, int rowmap, int n_threads, or_stats* st) {
+    render_scene_impl(arena, page_off, page_w, page_h, n_pages, pts, flags, path_pt_off, rule, gray, rgb, alpha,
+                      path_page, n_paths, m, flatness, rowmap, n_threads, st, clip);
+}
+
 void or_render_scene_rgb(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
                          uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
                          const uint8_t* rule, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
@@ -900,7 +933,7 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
                        const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
                        const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
                        uint64_t n_paths, const double m[6], double flatness, int rowmap,
-                       int n_threads, or_stats* st) {
+                       int n_threads, or_stats* st, const double* clip) {
     // Paths of each page, in scene order.
     std::vector<std::vector<uint64_t>> per_page(n_pages);
     for (uint64_t p = 0; p < n_paths; ++p)
@@ -916,14 +949,27 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
             uint8_t* page = arena + page_off[pg];
             for (uint64_t p : per_page[pg]) {
                 uint64_t a = path_pt_off[p], b = path_pt_off[p + 1];
-                if (rgb)
-                    or_fill_path_rgb(page, static_cast<int32_t>(page_w[pg]), static_cast<int32_t>(page_h[pg]),
-                                     pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
-                                     rgb + 3 * p, alpha[p], rowmap, &ls);
-                else
-                    or_fill_path(page, static_cast<int32_t>(page_w[pg]), static_cast<int32_t>(page_h[pg]),
-                                 pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
-                                 gray[p], alpha[p], rowmap, &ls);
+                const int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
+                const double* cp = clip ? clip + 4 * p : nullptr;
+                if (rgb) {
+                    const uint8_t* src = rgb + 3 * p;
+                    const uint8_t a_in = alpha[p];
+                    fill_path_impl(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness,
+                                   rule[p] != 0, rowmap, &ls,
+                                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                                       or_composite_aa_rgb8_opaque(page + 3 * (static_cast<int64_t>(y) * W + x0), src,
+                                                                   a_in, shape, n);
+                                   },
+                                   cp);
+                } else {
+                    const uint8_t g = gray[p], a_in = alpha[p];
+                    fill_path_impl(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness,
+                                   rule[p] != 0, rowmap, &ls,
+                                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                                       or_render_span_aa_gray(page + static_cast<int64_t>(y) * W + x0, shape, n, a_in, g);
+                                   },
+                                   cp);
+                }
             }
         }
     };

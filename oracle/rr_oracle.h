@@ -160,6 +160,16 @@ void or_render_scene_rgb(uint8_t* arena, const uint64_t* page_off, const uint32_
                          uint64_t n_paths, const double m[6], double flatness, int rowmap, int n_threads,
                          or_stats* st);
 
+/* The general form: gray pages (rgb == NULL) or Rgb8 pages (rgb[3p..]); with
+ * clip != NULL path p is clipped to the device-space rectangle
+ * clip[4p..4p+3] = (x0, y0, x1, y1) as Clip::clip_to_rect does on the page clip
+ * (clip.rs:116-125: the clip becomes page ∩ rect, integer bounds floor/ceil). */
+void or_render_scene_ex(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                        uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                        const uint8_t* rule, const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha,
+                        const uint32_t* path_page, uint64_t n_paths, const double* clip, const double m[6],
+                        double flatness, int rowmap, int n_threads, or_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

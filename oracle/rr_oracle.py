@@ -101,6 +101,11 @@ def lib() -> C.CDLL:
                                            C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
                                            C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D), D, C.c_int, C.c_int,
                                            C.POINTER(Stats)]),
+            "or_render_scene_ex": (None, [C.POINTER(U8), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                          C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(D), C.POINTER(U8),
+                                          C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
+                                          C.POINTER(U8), C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D),
+                                          C.POINTER(D), D, C.c_int, C.c_int, C.POINTER(Stats)]),
             "or_aa_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
             "or_aa_fill_cpu": (None, [C.POINTER(C.c_float), C.c_uint32, C.c_float, C.c_float, C.c_uint32,
                                       C.c_uint32, C.c_int, C.POINTER(U8)]),
@@ -327,6 +332,37 @@ def render_scene_rgb(scene, arena: np.ndarray, rgb: np.ndarray, rowmap=ROWMAP_DO
                               a[0].size, _p(a[2], C.c_double), _p(a[3], C.c_uint8), _p(a[4], C.c_uint64),
                               _p(a[5], C.c_uint8), _p(a[6], C.c_uint8), _p(a[7], C.c_uint8), _p(a[8], C.c_uint32),
                               a[5].size, _mat(IDENTITY), 0.1, rowmap, threads, C.byref(st))
+    return st.as_dict()
+
+
+def render_scene_ex(scene, arena: np.ndarray, rgb=None, clip=None, rowmap=ROWMAP_DOCUMENTED, threads=1,
+                    page_offset=None) -> dict:
+    """Gray pages (rgb None) or Rgb8 pages (rgb [n_paths, 3]); clip [n_paths, 4]
+    device-space rectangles (x0, y0, x1, y1) or None. page_offset defaults to
+    the scene's (x3 for Rgb8)."""
+    bpp = 1 if rgb is None else 3
+    po = np.ascontiguousarray(bpp * scene.page_offset.astype(np.uint64) if page_offset is None else page_offset,
+                              np.uint64)
+    a = [np.ascontiguousarray(x, t) for x, t in (
+        (scene.page_width, np.uint32), (scene.page_height, np.uint32), (np.reshape(scene.pts, -1), np.float64),
+        (scene.flags, np.uint8), (scene.path_pt_off, np.uint64), (scene.fill_rule, np.uint8),
+        (scene.alpha, np.uint8), (scene.path_page, np.uint32))]
+    gray = np.ascontiguousarray(getattr(scene, "gray", np.zeros(a[5].size, np.uint8)), np.uint8)
+    rgbp = None if rgb is None else _p(np.ascontiguousarray(np.reshape(rgb, -1), np.uint8), C.c_uint8)
+    keep = []
+    clipp = None
+    if clip is not None:
+        c = np.ascontiguousarray(np.reshape(clip, -1), np.float64)
+        keep.append(c)
+        clipp = _p(c, C.c_double)
+    if rgb is not None:
+        keep.append(rgbp)
+    st = Stats()
+    lib().or_render_scene_ex(_p(arena, C.c_uint8), _p(po, C.c_uint64), _p(a[0], C.c_uint32), _p(a[1], C.c_uint32),
+                             a[0].size, _p(a[2], C.c_double), _p(a[3], C.c_uint8), _p(a[4], C.c_uint64),
+                             _p(a[5], C.c_uint8), _p(gray, C.c_uint8), rgbp, _p(a[6], C.c_uint8),
+                             _p(a[7], C.c_uint32), a[5].size, clipp, _mat(IDENTITY), 0.1, rowmap, threads,
+                             C.byref(st))
     return st.as_dict()
 
 

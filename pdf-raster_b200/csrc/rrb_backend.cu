@@ -63,7 +63,7 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
-    Scratch s_run_off, s_runs, s_chunk_path;
+    Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
@@ -282,6 +282,8 @@ struct rrb_batch {
     Scratch pts, flags, off, rule, gray, alpha, page, geom, pw, ph, mtx;
     Scratch rgb;                    // Rgb8 pages: per-path colour r | g << 8 | b << 16
     uint32_t bpp = 1;               // page bytes per pixel: 1 Gray8, 3 Rgb8
+    Scratch clip;                   // per-path clip in AA units (int4), when has_clip
+    bool has_clip = false;
     std::vector<PageGeom> geom_h;
     std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
     bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
@@ -330,7 +332,7 @@ void stage_end(rrb_ctx* c, int k) {
 
 void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
-                      &B->mtx, &B->rgb};
+                      &B->mtx, &B->rgb, &B->clip};
     for (Scratch* s : all) {
         if (B->view && s != &B->off && s != &B->page && s != &B->geom) {
             s->p = nullptr;
@@ -343,8 +345,10 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     }
 }
 
-// Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages.
-int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr) {
+// Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages;
+// clip (host, 4 doubles per path) clips each path to a device-space rectangle.
+int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr,
+                 const double* clip = nullptr) {
     std::string msg;
     uint64_t tiles = 0;
     B->bpp = rgb ? 3 : 1;
@@ -374,6 +378,29 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     if ((rc = upload(c, B->ph, h->page_height, h->n_pages))) return rc;
     if ((rc = ensure(c, B->geom, h->n_pages * sizeof(PageGeom)))) return rc;
     if ((rc = upload(c, B->mtx, h->matrix, 6))) return rc;
+    B->has_clip = clip != nullptr;
+    if (clip) {
+        // Clip::new(0, 0, W, H) then clip_to_rect (clip.rs:73-88,116-125,266-271),
+        // in AA units: columns [4 x_min_i, 4 (x_max_i + 1)), rows [4 y_min_i, 4 (y_max_i + 1) - 1].
+        std::vector<int4> ci(h->n_paths);
+        for (uint64_t p = 0; p < h->n_paths; ++p) {
+            const double* r = clip + 4 * p;
+            for (int k = 0; k < 4; ++k)
+                if (!std::isfinite(r[k])) return set_err(c, RRB_ERR_INVARIANT, "clip rectangles must be finite");
+            const uint32_t pg = h->path_page[p];
+            const double W = h->page_width[pg], H = h->page_height[pg];
+            const double x_min = std::max(0.0, std::min(r[0], r[2])), x_max = std::min(W, std::max(r[0], r[2]));
+            const double y_min = std::max(0.0, std::min(r[1], r[3])), y_max = std::min(H, std::max(r[1], r[3]));
+            auto fl = [](double v) { return static_cast<int32_t>(std::max(-1e9, std::min(1e9, std::floor(v)))); };
+            auto ce = [](double v) { return static_cast<int32_t>(std::max(-1e9, std::min(1e9, std::ceil(v)))); };
+            const int32_t x_min_i = fl(x_min), y_min_i = fl(y_min), x_max_i = ce(x_max) - 1, y_max_i = ce(y_max) - 1;
+            ci[p] = make_int4(4 * x_min_i, 4 * (x_max_i + 1), 4 * y_min_i, 4 * (y_max_i + 1) - 1);
+            if (ci[p].x > ci[p].y) ci[p].y = ci[p].x;      // empty column range
+            if (ci[p].z > ci[p].w + 1) ci[p].w = ci[p].z - 1;  // empty row range
+        }
+        if ((rc = upload(c, B->clip, ci.data(), ci.size()))) return rc;
+        RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     if (rgb) {
         std::vector<uint32_t> packed(h->n_paths);
         for (uint64_t p = 0; p < h->n_paths; ++p)
@@ -401,6 +428,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     const uint32_t n_pages = B->n_pages;
     const uint32_t NP = static_cast<uint32_t>(n_paths);
     const double flat_sq = B->flat_sq;
+    const int4* pclip = B->has_clip ? as<int4>(B->clip) : nullptr;
     int rc;
     RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
                                 c->stream));
@@ -423,10 +451,12 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     const uint32_t NPC = static_cast<uint32_t>(n_pieces);
     if ((rc = ensure(c, c->s_pieces, std::max<uint64_t>(1, n_pieces) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_clip, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
+    if (pclip && (rc = ensure(c, c->s_clip_lo, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
+    uint32_t* clip_lo = pclip ? as<uint32_t>(c->s_clip_lo) : nullptr;
     if ((rc = ensure(c, c->s_edge_off, (n_pieces + 1) * sizeof(uint32_t)))) return rc;
     k_compact_pieces<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(
         as<uint64_t>(B->off), as<uint32_t>(c->s_path_pieces), NP, as<uint32_t>(B->page), as<uint32_t>(B->ph),
-        as<uint2>(c->s_slots), as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip));
+        as<uint2>(c->s_slots), as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip), pclip, clip_lo);
     c->launches += 1;
     stage_end(c, 0);
     RRB_CUDA(c, cudaGetLastError());
@@ -458,7 +488,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage(c, 3);
     k_seg_write<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
-        static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip));
+        static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo);
     c->launches += 1;
     stage_end(c, 3);
     const int chunk_rows = 32;
@@ -467,7 +497,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
         as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
-        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax);
+        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax, pclip);
     c->launches += 1;
     stage_end(c, 4);
     RRB_CUDA(c, cudaGetLastError());
@@ -489,7 +519,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if ((rc = ensure(c, c->s_run_off, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     k_recti<false><<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
         as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, as<uint32_t>(c->s_run_off),
-        nullptr, nullptr, nullptr, 0, as<BatchCounters>(c->s_ctr));
+        nullptr, nullptr, nullptr, 0, as<BatchCounters>(c->s_ctr), pclip);
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
     if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NP))) return rc;
@@ -536,14 +566,14 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
             gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
             static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
-            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path));
+            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
         c->launches += 1;
     }
     if (n_runs) {
         k_recti<true><<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
             as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, nullptr,
             as<uint32_t>(c->s_run_off), as<int4>(c->s_runs), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
-            as<BatchCounters>(c->s_ctr));
+            as<BatchCounters>(c->s_ctr), pclip);
         c->launches += 1;
     }
     stage_end(c, 9);
@@ -561,7 +591,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         k_groups_mid<<<grid_for(c, mid * 32, MID_WARPS * 32, 16), MID_WARPS * 32, 0, c->stream>>>(
             as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), gmin, gmax,
             as<uint32_t>(B->pw), as<uint2>(c->s_ovf), ovf_cap, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
-            static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf2), as<BatchCounters>(c->s_ctr));
+            static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf2), as<BatchCounters>(c->s_ctr), pclip);
         c->launches += 1;
         RRB_CUDA(c, cudaGetLastError());
         if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
@@ -584,7 +614,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                     as<uint2>(c->s_ovf2), ovf_cap, as<int3>(c->s_scratch),
                     static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
                     as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
-                    as<BatchCounters>(c->s_ctr));
+                    as<BatchCounters>(c->s_ctr), pclip);
                 c->launches += 1;
                 RRB_CUDA(c, cudaGetLastError());
                 if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
@@ -658,7 +688,7 @@ void release_scratch(rrb_ctx* c) {
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
                       &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
-                      &c->s_chunk_path};
+                      &c->s_chunk_path, &c->s_clip_lo};
     for (Scratch* x : all) {
         dev_free(c, x->p, x->cap);
         x->p = nullptr;
@@ -692,6 +722,8 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     view(W->mtx, B->mtx, 0);
     W->bpp = B->bpp;
     if (B->bpp == 3) view(W->rgb, B->rgb, pb * sizeof(uint32_t));
+    W->has_clip = B->has_clip;
+    if (B->has_clip) view(W->clip, B->clip, pb * sizeof(int4));
     int rc;
     if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
     if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
@@ -773,9 +805,9 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
 }
 
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
-              const uint8_t* rgb = nullptr) {
+              const uint8_t* rgb = nullptr, const double* clip = nullptr) {
     rrb_batch* B = c->tmp_batch;
-    int rc = batch_upload(c, h, B, rgb);
+    int rc = batch_upload(c, h, B, rgb, clip);
     if (rc) return rc;
     return run_resident(c, B, arena, arena_len, h->rowmap);
 }
@@ -862,7 +894,7 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
-                      &c->s_chunk_path};
+                      &c->s_chunk_path, &c->s_clip_lo};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap);
     if (c->tmp_batch) {
@@ -1178,21 +1210,28 @@ int rrb_last_stage_times(rrb_ctx* c, rrb_stage_time* out, int cap, int* n) {
     return RRB_OK;
 }
 
-int rrb_record_path_batch_rgb(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb) {
+int rrb_record_path_batch_ex(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb,
+                             const double* clip_rects) {
     if (!c || !p) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
-    if (p->n_paths && !path_rgb) return set_err(c, RRB_ERR_INVARIANT, "path_rgb is null");
     cudaSetDevice(c->device);
     {
         std::vector<PageGeom> geom;
         uint64_t tiles = 0, supers = 0;
         std::string m;
-        int v = validate_batch(p, p->pages->len, 64, 16, geom, tiles, supers, m, 3);
+        int v = validate_batch(p, p->pages->len, 64, 16, geom, tiles, supers, m, path_rgb ? 3 : 1);
         if (v) return set_err(c, v, m);
     }
     static const uint8_t kNone[3] = {0, 0, 0};
-    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, p->n_paths ? path_rgb : kNone);
+    const uint8_t* rgb = path_rgb ? (p->n_paths ? path_rgb : kNone) : nullptr;
+    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, rgb, p->n_paths ? clip_rects : nullptr);
+}
+
+int rrb_record_path_batch_rgb(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb) {
+    if (c && p && p->n_paths && !path_rgb) return set_err(c, RRB_ERR_INVARIANT, "path_rgb is null");
+    static const uint8_t kNone[3] = {0, 0, 0};
+    return rrb_record_path_batch_ex(c, p, path_rgb ? path_rgb : kNone, nullptr);
 }
 
 int rrb_record_rgb_to_gray(rrb_ctx* c, const rrb_buf* rgb, size_t rgb_offset, const rrb_buf* gray,

@@ -59,6 +59,13 @@ struct BatchCounters {
     unsigned long long aa_rows;      // sum over paths of y1 - y0 + 1
 };
 
+// Clip of path p in AA units: columns [x, y) and rows [z, w] — the page, or
+// the page and a clip rectangle (Clip::clip_to_rect) when path_clip is given.
+__device__ __forceinline__ int4 path_clip_of(const int4* __restrict__ path_clip, uint32_t p, int32_t aa_width,
+                                             int32_t aa_height) {
+    return path_clip ? path_clip[p] : make_int4(0, aa_width, 0, aa_height - 1);
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -114,18 +121,26 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
 }
 
 // Pack each path's pieces (the first path_pieces[p] slots of its point range)
-// densely at piece_off[p], with the AA-row clip of the path's page.
+// densely at piece_off[p], with the AA-row clip of the path (its page, or the
+// page and its clip rectangle; the lower bound is only stored with a clip).
 __global__ void k_compact_pieces(const uint64_t* __restrict__ path_pt_off, const uint32_t* __restrict__ piece_off,
                                  uint32_t n_paths, const uint32_t* __restrict__ path_page,
                                  const uint32_t* __restrict__ page_h, const uint2* __restrict__ slots,
-                                 uint2* __restrict__ pieces, uint32_t* __restrict__ piece_clip) {
+                                 uint2* __restrict__ pieces, uint32_t* __restrict__ piece_clip,
+                                 const int4* __restrict__ path_clip, uint32_t* __restrict__ piece_clip_lo) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
         const uint32_t src = static_cast<uint32_t>(path_pt_off[p]);
         const uint32_t dst = piece_off[p], n = piece_off[p + 1] - dst;
-        const uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u;
+        uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u, clip_lo = 0;
+        if (path_clip) {
+            const int4 cl = path_clip[p];
+            clip_lo = static_cast<uint32_t>(cl.z);
+            clip_hi = static_cast<uint32_t>(cl.w);
+        }
         for (uint32_t k = 0; k < n; ++k) {
             pieces[dst + k] = slots[src + k];
             piece_clip[dst + k] = clip_hi;
+            if (piece_clip_lo) piece_clip_lo[dst + k] = clip_lo;
         }
     }
 }
@@ -163,7 +178,7 @@ __global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restr
 __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
                             uint32_t edge_cap, Edge* __restrict__ edges,
-                            const uint32_t* __restrict__ slot_clip_hi) {
+                            const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -173,13 +188,14 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
         if (kind == PK_NONE) continue;
         uint32_t base = edge_off[s];
         int32_t chi = static_cast<int32_t>(slot_clip_hi[s]);
+        const int32_t clo = slot_clip_lo ? static_cast<int32_t>(slot_clip_lo[s]) : 0;
         uint32_t j = pc.y & 0x3fffffffu;
         double x0, y0;
         load_tpt(pts, m, pc.x, x0, y0);
         if (kind == PK_LINE || kind == PK_CLOSE) {
             double x1, y1;
             load_tpt(pts, m, j, x1, y1);
-            if (base < edge_cap) edges[base] = make_edge(x0, y0, x1, y1, 0, chi);
+            if (base < edge_cap) edges[base] = make_edge(x0, y0, x1, y1, clo, chi);
         } else {
             double x1, y1, x2, y2, x3, y3;
             load_tpt(pts, m, j, x1, y1);
@@ -188,7 +204,7 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
             double cx = x0, cy = y0;
             uint32_t k = base;
             flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [&](double fx, double fy) {
-                if (k < edge_cap) edges[k] = make_edge(cx, cy, fx, fy, 0, chi);
+                if (k < edge_cap) edges[k] = make_edge(cx, cy, fx, fy, clo, chi);
                 ++k;
                 cx = fx;
                 cy = fy;
@@ -295,7 +311,7 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                             const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
                             uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
                             int chunk_rows, BatchCounters* __restrict__ ctr, int32_t* __restrict__ gmin,
-                            int32_t* __restrict__ gmax) {
+                            int32_t* __restrict__ gmax, const int4* __restrict__ path_clip) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -376,11 +392,12 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                 pi.y1 = y1;
                 rows = static_cast<uint32_t>(y1 - (y0 & ~3) + 1);     // rows of the 4-aligned chunks
                 groups = static_cast<uint32_t>((y1 >> 2) - (y0 >> 2) + 1);
-                // Pixel columns: spans cover AA columns [max(x0,0), min(x1+1, 4W)).
-                int32_t cl = max(xl, 0), ch = min(xh, 4 * W - 1);
+                // Pixel columns: spans cover AA columns [max(x0, lo), min(x1+1, hi)).
+                const int4 clp = path_clip_of(path_clip, p, 4 * W, 4 * H);
+                int32_t cl = max(xl, clp.x), ch = min(xh, clp.y - 1);
                 pi.px0 = cl >> 2;
                 pi.px1 = ch >> 2;
-                if (xh < 0 || xl >= 4 * W) {
+                if (xh < clp.x || xl >= clp.y || clp.x >= clp.y) {
                     pi.px0 = 1;
                     pi.px1 = 0;
                 }
@@ -515,10 +532,13 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
 __device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? v : v + 1; }
 
 // Winding walk of render_aa_line (scanner/mod.rs:393-467) for one AA row over
-// its sorted entries, emitting the union of the covered spans clamped to
-// [0, aa_width) in place over the entry arrays. Returns the span count.
+// its sorted entries, emitting the union of the covered spans clamped to the
+// clip's AA columns [lo, hi) (the page: [0, aa_width); an unclosed span ends
+// at aa_width as in the reference) in place over the entry arrays. Returns the
+// span count.
 template <typename Get, typename Put>
-__device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, Get get, Put put, uint32_t& nonterm) {
+__device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, int32_t lo, int32_t hi, Get get, Put put,
+                                        uint32_t& nonterm) {
     int32_t count = 0, xx = 0;
     int i = 0, ns = 0;
     bool have = false;
@@ -551,8 +571,8 @@ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, G
                 break;
             }
         }
-        int32_t bx0 = max(xx, 0);
-        int32_t bx1 = max(min(span_x1, aa_width), 0);
+        int32_t bx0 = max(xx, lo);
+        int32_t bx1 = max(min(span_x1, hi), lo);
         if (bx0 < bx1) {
             if (have && bx0 <= ce) {
                 ce = max(ce, bx1);
@@ -724,7 +744,8 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
 // std sorts slices of up to 20 elements) followed by the render_aa_line
 // winding walk; the row's union of spans replaces the list in place.
 template <int LS>
-__device__ __forceinline__ int sort_and_walk(int n, int32_t mask, int32_t aa_width, int32_t* x0s, int32_t* x1s,
+__device__ __forceinline__ int sort_and_walk(int n, int32_t mask, int32_t aa_width, int32_t lo, int32_t hi,
+                                             int32_t* x0s, int32_t* x1s,
                                              int32_t* cns, int lane, uint32_t& nonterm) {
     for (int a = 1; a < n; ++a) {
         const int32_t t0 = x0s[a * LS + lane], t1 = x1s[a * LS + lane], tc = cns[a * LS + lane];
@@ -740,7 +761,7 @@ __device__ __forceinline__ int sort_and_walk(int n, int32_t mask, int32_t aa_wid
         cns[b * LS + lane] = tc;
     }
     return walk_row(
-        n, mask, aa_width,
+        n, mask, aa_width, lo, hi,
         [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
             x0 = x0s[i * LS + lane];
             x1 = x1s[i * LS + lane];
@@ -772,7 +793,7 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     const Edge* __restrict__ edges, const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax,
     const uint32_t* __restrict__ page_w, uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
     uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr,
-    const uint32_t* __restrict__ chunk_path) {
+    const uint32_t* __restrict__ chunk_path, const int4* __restrict__ path_clip) {
     __shared__ int32_t sx0[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t sx1[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t scn[ROWS_WARPS][KCAP * 32];
@@ -794,7 +815,9 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
                                            sx1[w], scn[w], lane);
         const bool overflow = valid && n > KCAP;
         int ns = 0;
-        if (valid && !overflow) ns = sort_and_walk<32>(n, mask, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
+        const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
+        if (valid && !overflow)
+            ns = sort_and_walk<32>(n, mask, aa_width, cx.x, cx.y, sx0[w], sx1[w], scn[w], lane, nonterm);
         // ---- one pixel row per 4 lanes: merge the sub-rows' spans into cells
         sns[w][lane] = (valid && !overflow) ? ns : 0;
         const uint32_t ovf_lanes = __ballot_sync(0xffffffffu, overflow);
@@ -860,7 +883,8 @@ constexpr int RECTI_MAX_SPANS = RECTI_MAX_EDGES / 2 + 1;
 
 // Spans of AA row r of a rectilinear path (fold, sort, walk over <= 32 edges).
 __device__ __forceinline__ int recti_row_spans(const PathInfo& P, const Edge* __restrict__ edges, int32_t r,
-                                               int32_t aa_width, int32_t* sx0, int32_t* sx1, uint32_t& nonterm) {
+                                               int32_t aa_width, int32_t lo, int32_t hi, int32_t* sx0, int32_t* sx1,
+                                               uint32_t& nonterm) {
     int32_t x0s[RECTI_MAX_EDGES], x1s[RECTI_MAX_EDGES], cs[RECTI_MAX_EDGES];
     int n = 0;
     for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
@@ -894,7 +918,7 @@ __device__ __forceinline__ int recti_row_spans(const PathInfo& P, const Edge* __
     }
     const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
     return walk_row(
-        n, mask, aa_width,
+        n, mask, aa_width, lo, hi,
         [&](int i, int32_t& a, int32_t& b, int32_t& c) {
             a = x0s[i];
             b = x1s[i];
@@ -911,7 +935,7 @@ template <bool WRITE>
 __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edge* __restrict__ edges,
                         const uint32_t* __restrict__ page_w, int rowmap, uint32_t* __restrict__ run_count,
                         const uint32_t* __restrict__ run_off, int4* __restrict__ runs, uint32_t* __restrict__ cells,
-                        uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
+                        uint32_t cell_cap, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
     uint32_t nonterm = 0;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
         PathInfo P = info[p];
@@ -958,6 +982,7 @@ __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edg
         };
         const int32_t g0 = P.y0 >> 2, g1 = P.y1 >> 2;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
         uint32_t nrun = 0;
         uint32_t ro = WRITE ? run_off[p] : 0u;
         int32_t best_rows = 0, bx0 = 1, bx1 = 0, bg0 = 1, bg1 = 0;
@@ -978,12 +1003,12 @@ __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edg
                 int32_t s0[4][RECTI_MAX_SPANS], s1[4][RECTI_MAX_SPANS];
                 int n4[4] = {0, 0, 0, 0};
                 if (uniform) {
-                    n4[0] = recti_row_spans(P, edges, r_lo, aa_width, s0[0], s1[0], nonterm);
+                    n4[0] = recti_row_spans(P, edges, r_lo, aa_width, cx.x, cx.y, s0[0], s1[0], nonterm);
                     n4[1] = n4[2] = n4[3] = n4[0];
                 } else {
                     for (int k = 0; k < 4; ++k) {
                         const int32_t r = r_lo + k;
-                        if (r >= P.y0 && r <= P.y1) n4[k] = recti_row_spans(P, edges, r, aa_width, s0[k], s1[k], nonterm);
+                        if (r >= P.y0 && r <= P.y1) n4[k] = recti_row_spans(P, edges, r, aa_width, cx.x, cx.y, s0[k], s1[k], nonterm);
                     }
                 }
                 const uint32_t need = 4u * static_cast<uint32_t>(n4[0] + n4[1] + n4[2] + n4[3]);
@@ -1063,7 +1088,7 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off, const Edge* __restrict__ edges,
     const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax, const uint32_t* __restrict__ page_w,
     const uint2* __restrict__ ovf, uint32_t ovf_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
-    uint32_t cell_cap, uint2* __restrict__ ovf2, BatchCounters* __restrict__ ctr) {
+    uint32_t cell_cap, uint2* __restrict__ ovf2, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
     __shared__ int32_t sx0[MID_WARPS][MID_K * 4];
     __shared__ int32_t sx1[MID_WARPS][MID_K * 4];
     __shared__ int32_t scn[MID_WARPS][MID_K * 4];
@@ -1085,7 +1110,9 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
                                            lane);
         const bool overflow = valid && n > MID_K;
         int ns = 0;
-        if (valid && !overflow) ns = sort_and_walk<4>(n, mask, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
+        const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
+        if (valid && !overflow)
+            ns = sort_and_walk<4>(n, mask, aa_width, cx.x, cx.y, sx0[w], sx1[w], scn[w], lane, nonterm);
         if (lane < 4) sns[w][lane] = (valid && !overflow) ? ns : 0;
         const bool any_ovf = __any_sync(0xffffffffu, overflow);
         __syncwarp();
@@ -1125,7 +1152,7 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
                               const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w,
                               const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
                               uint32_t scratch_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
-                              uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
+                              uint32_t cell_cap, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
     const uint32_t n_ovf = min(ctr->ovf2_count, ovf_cap);
     uint32_t nonterm = 0;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_ovf; k += gridDim.x * blockDim.x) {
@@ -1140,6 +1167,7 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
         }
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
+        const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
         int n4[4] = {0, 0, 0, 0};
         for (int sub = 0; sub < 4; ++sub) {
             const int32_t r = 4 * g + sub;
@@ -1170,7 +1198,7 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
                 L[b] = t;
             }
             n4[sub] = walk_row(
-                n, mask, aa_width,
+                n, mask, aa_width, cx.x, cx.y,
                 [&](int i, int32_t& x0, int32_t& x1, int32_t& cc) {
                     x0 = L[i].x;
                     x1 = L[i].y;

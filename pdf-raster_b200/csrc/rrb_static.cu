@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_static_rows(const PathInfo* 
                                            lane);
         const bool overflow = valid && n > kRowK;
         int ns = 0;
-        if (valid && !overflow) ns = sort_and_walk<4>(n, mask, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
+        if (valid && !overflow) ns = sort_and_walk<4>(n, mask, aa_width, 0, aa_width, sx0[w], sx1[w], scn[w], lane, nonterm);
         if (lane < 4) sns[w][lane] = (valid && !overflow) ? ns : 0;
         const bool any_ovf = __any_sync(0xffffffffu, overflow);
         __syncwarp();
@@ -273,7 +273,8 @@ int fill_static(rrb_ctx* c, const rrb_path_fill_params* p, unsigned char* base, 
     uint32_t n_pieces = 0;
     if ((rc = read_u32(c, s, hdr->path_pieces + 1, n_pieces))) return rc;
     if (n_pieces == 0) return RRB_OK;
-    k_compact_pieces<<<1, 32, 0, s>>>(hdr->off, hdr->path_pieces, 1, &hdr->page, &hdr->ph, slots, pieces, clip);
+    k_compact_pieces<<<1, 32, 0, s>>>(hdr->off, hdr->path_pieces, 1, &hdr->page, &hdr->ph, slots, pieces, clip,
+                                      nullptr, nullptr);
     k_seg_count<<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off);
     if ((rc = scan_static(c, s, edge_off, n_pieces, hdr->block))) return rc;
     uint32_t n_edges = 0;
@@ -292,10 +293,10 @@ int fill_static(rrb_ctx* c, const rrb_path_fill_params* p, unsigned char* base, 
     RRB_STATIC_CUDA(c, cudaMemsetAsync(gmin, 0x7f, groups * sizeof(int32_t), s));  // +inf rows
     RRB_STATIC_CUDA(c, cudaMemsetAsync(gmax, 0x80, groups * sizeof(int32_t), s));  // -inf rows
     k_seg_write<<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off, n_edges,
-                                                         edges, clip);
+                                                         edges, clip, nullptr);
     k_path_bbox<<<1, 32, 0, s>>>(hdr->path_pieces, edge_off, edges, 1, &hdr->rule, &hdr->gray, &hdr->alpha,
                                  &hdr->page, &hdr->pw, &hdr->ph, p->rowmap, &hdr->info, hdr->rows, hdr->chunks, 32,
-                                 &hdr->ctr, gmin, gmax);
+                                 &hdr->ctr, gmin, gmax, nullptr);
     RRB_STATIC_CUDA(c, cudaGetLastError());
 
     // Rows -> cells, then the blend (skipped on the device if a limit was hit).

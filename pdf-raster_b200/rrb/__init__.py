@@ -382,6 +382,15 @@ class B200Backend:
         rgb = np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
         self._chk(lib().rrb_record_path_batch_rgb(self._h, C.byref(params), _ptr(rgb, C.c_uint8)))
 
+    def record_path_batch_ex(self, params: PathBatchParams, path_rgb: np.ndarray | None = None,
+                             clip_rects: np.ndarray | None = None):
+        """Gray or (path_rgb) Rgb8 pages; clip_rects [n_paths, 4] device-space (x0, y0, x1, y1) or None."""
+        rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
+        clip = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
+        self._chk(lib().rrb_record_path_batch_ex(self._h, C.byref(params),
+                                                 None if rgb is None else _ptr(rgb, C.c_uint8),
+                                                 None if clip is None else _ptr(clip, C.c_double)))
+
     def record_rgb_to_gray(self, rgb: DeviceBuffer, gray: DeviceBuffer, n_px: int, rgb_offset: int = 0,
                            gray_offset: int = 0):
         self._chk(lib().rrb_record_rgb_to_gray(self._h, rgb.handle, rgb_offset, gray.handle, gray_offset, n_px))

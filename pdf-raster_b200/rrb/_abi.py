@@ -180,6 +180,8 @@ SIGNATURES = {
     "rrb_wait_page": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
     "rrb_record_path_fill": (C.c_int, [VP, C.POINTER(PathFillParams)]),
     "rrb_record_path_fill_static": (C.c_int, [VP, C.POINTER(PathFillParams)]),
+    "rrb_record_path_batch_ex": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8),
+                                           C.POINTER(C.c_double)]),
     "rrb_record_path_batch_rgb": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8)]),
     "rrb_record_rgb_to_gray": (C.c_int, [VP, VP, C.c_size_t, VP, C.c_size_t, C.c_uint64]),
     "rrb_record_aa_fill": (C.c_int, [VP, C.POINTER(AaFillParams)]),
