@@ -756,7 +756,6 @@ __device__ __forceinline__ int gather_row_pairs(const PathInfo& P, int32_t lo, i
                                                 int32_t* x1s, int32_t* cns, uint32_t* s_pref, uint32_t* s_mask,
                                                 int32_t* s_ra, uint32_t* s_cnt, int lane) {
     s_cnt[lane] = 0;
-    bool ovf = false;
     __syncwarp();
     for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
         const uint32_t gi = eb >> 5;
@@ -826,35 +825,31 @@ __device__ __forceinline__ int gather_row_pairs(const PathInfo& P, int32_t lo, i
             }
         }
         __syncwarp();
-        // Fold this group's entries of the row (slots [m0, m0 + k)) into its
-        // merged list with the write_intersect merge, in place.
-        const int m0 = static_cast<int>(s_cnt[lane]), k = __popc(mine);
-        int n = m0;
-        if (m0 + k > K) {
-            ovf = true;
-        } else {
-            for (int i = m0; i < m0 + k; ++i) {
-                const int32_t elo = x0s[i * LS + lane], ehi = x1s[i * LS + lane], ec = cns[i * LS + lane];
-                if (n > 0) {
-                    const int32_t lx0 = x0s[(n - 1) * LS + lane], lx1 = x1s[(n - 1) * LS + lane];
-                    if (sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
-                        cns[(n - 1) * LS + lane] = static_cast<int32_t>(
-                            static_cast<uint32_t>(cns[(n - 1) * LS + lane]) + static_cast<uint32_t>(ec));
-                        x0s[(n - 1) * LS + lane] = min(lx0, elo);
-                        x1s[(n - 1) * LS + lane] = max(lx1, ehi);
-                        continue;
-                    }
-                }
-                x0s[n * LS + lane] = elo;
-                x1s[n * LS + lane] = ehi;
-                cns[n * LS + lane] = ec;
-                ++n;
-            }
-        }
-        s_cnt[lane] = static_cast<uint32_t>(ovf ? K + 1 : n);
+        s_cnt[lane] += __popc(mine);
         __syncwarp();
     }
-    return static_cast<int>(s_cnt[lane]);
+    const int raw = static_cast<int>(s_cnt[lane]);
+    if (raw > K) return raw;
+    // The write_intersect merge over the row's raw entries, in place.
+    int n = 0;
+    for (int i = 0; i < raw; ++i) {
+        const int32_t elo = x0s[i * LS + lane], ehi = x1s[i * LS + lane], ec = cns[i * LS + lane];
+        if (n > 0) {
+            const int32_t lx0 = x0s[(n - 1) * LS + lane], lx1 = x1s[(n - 1) * LS + lane];
+            if (sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
+                cns[(n - 1) * LS + lane] =
+                    static_cast<int32_t>(static_cast<uint32_t>(cns[(n - 1) * LS + lane]) + static_cast<uint32_t>(ec));
+                x0s[(n - 1) * LS + lane] = min(lx0, elo);
+                x1s[(n - 1) * LS + lane] = max(lx1, ehi);
+                continue;
+            }
+        }
+        x0s[n * LS + lane] = elo;
+        x1s[n * LS + lane] = ehi;
+        cns[n * LS + lane] = ec;
+        ++n;
+    }
+    return n;
 }
 
 // sort_unstable_by_key(x0) on a lane's list (stable insertion sort, as Rust
