@@ -740,118 +740,6 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
     return n;
 }
 
-// gather_row with the entry computation spread over the whole warp: for each
-// group of 32 edges the (edge, row) pairs of the chunk are enumerated by a
-// warp prefix sum of the edges' row counts and computed lane-parallel; pair
-// (e, r) lands at slot (entries of row r from earlier groups) + (edges before
-// e in this group that cover r), so every row's raw list is in segment order.
-// Then each lane folds its row's raw list with the write_intersect merge
-// (merge only with the last entry, scanner/mod.rs:600-642) in place. Same
-// lists as gather_row; a row with more than K raw entries returns a count
-// above K (the caller treats it as overflow).
-template <int K, int LS>
-__device__ __forceinline__ int gather_row_pairs(const PathInfo& P, int32_t lo, int32_t hi, int32_t r, bool valid,
-                                                const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
-                                                const int32_t* __restrict__ gmax, int32_t (*sedge)[32], int32_t* x0s,
-                                                int32_t* x1s, int32_t* cns, uint32_t* s_pref, uint32_t* s_mask,
-                                                int32_t* s_ra, uint32_t* s_cnt, int lane) {
-    s_cnt[lane] = 0;
-    __syncwarp();
-    for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
-        const uint32_t gi = eb >> 5;
-        if (gmin[gi] > hi || gmax[gi] < lo) continue;  // no edge of this group touches the rows
-        const uint32_t j = eb + lane;
-        Edge e;
-        bool hit = false;
-        if (j >= P.e_begin && j < P.e_end) {
-            e = edges[j];
-            hit = !(e.flags & EF_EMPTY) && e.row0 <= hi && e.row1 >= lo;
-        }
-        if (!__any_sync(0xffffffffu, hit)) continue;
-        uint32_t rows_of_edge = 0, cnt = 0;
-        int32_t ra = 0;
-        if (hit) {
-            sedge[0][lane] = e.row0;
-            sedge[1][lane] = e.row1;
-            sedge[2][lane] = e.flags;
-            sedge[3][lane] = e.a;
-            sedge[4][lane] = e.b;
-            sedge[5][lane] = e.dfp;
-            sedge[6][lane] = e.cmin;
-            sedge[7][lane] = e.cmax;
-            ra = max(e.row0, lo) - lo;
-            const int32_t rb = min(e.row1, hi) - lo;
-            rows_of_edge = (0xffffffffu >> (31 - rb)) & (0xffffffffu << ra);
-            cnt = static_cast<uint32_t>(rb - ra + 1);
-        }
-        uint32_t mine = warp_transpose32(rows_of_edge, lane);
-        if (!valid) mine = 0;
-        uint32_t inc = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-        s_pref[lane] = inc;
-        s_mask[lane] = mine;
-        s_ra[lane] = ra;
-        __syncwarp();
-        for (uint32_t t = lane; t < total; t += 32) {
-            int ei = 0;  // the edge of pair t: the first lane whose inclusive prefix exceeds t
-#pragma unroll
-            for (int step = 16; step; step >>= 1)
-                if (s_pref[ei + step - 1] <= t) ei += step;
-            const uint32_t excl = ei ? s_pref[ei - 1] : 0u;
-            const int row = s_ra[ei] + static_cast<int>(t - excl);
-            const uint32_t rmask = s_mask[row];
-            if (!(rmask >> ei & 1u)) continue;  // an invalid row (no entries kept)
-            const uint32_t slot = s_cnt[row] + __popc(rmask & ((1u << ei) - 1u));
-            if (slot < K) {
-                Edge E;
-                E.row0 = sedge[0][ei];
-                E.row1 = sedge[1][ei];
-                E.flags = sedge[2][ei];
-                E.a = sedge[3][ei];
-                E.b = sedge[4][ei];
-                E.dfp = sedge[5][ei];
-                E.cmin = sedge[6][ei];
-                E.cmax = sedge[7][ei];
-                int32_t elo, ehi, ec;
-                edge_entry(E, lo + row, elo, ehi, ec);
-                x0s[slot * LS + row] = elo;
-                x1s[slot * LS + row] = ehi;
-                cns[slot * LS + row] = ec;
-            }
-        }
-        __syncwarp();
-        s_cnt[lane] += __popc(mine);
-        __syncwarp();
-    }
-    const int raw = static_cast<int>(s_cnt[lane]);
-    if (raw > K) return raw;
-    // The write_intersect merge over the row's raw entries, in place.
-    int n = 0;
-    for (int i = 0; i < raw; ++i) {
-        const int32_t elo = x0s[i * LS + lane], ehi = x1s[i * LS + lane], ec = cns[i * LS + lane];
-        if (n > 0) {
-            const int32_t lx0 = x0s[(n - 1) * LS + lane], lx1 = x1s[(n - 1) * LS + lane];
-            if (sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
-                cns[(n - 1) * LS + lane] =
-                    static_cast<int32_t>(static_cast<uint32_t>(cns[(n - 1) * LS + lane]) + static_cast<uint32_t>(ec));
-                x0s[(n - 1) * LS + lane] = min(lx0, elo);
-                x1s[(n - 1) * LS + lane] = max(lx1, ehi);
-                continue;
-            }
-        }
-        x0s[n * LS + lane] = elo;
-        x1s[n * LS + lane] = ehi;
-        cns[n * LS + lane] = ec;
-        ++n;
-    }
-    return n;
-}
-
 // sort_unstable_by_key(x0) on a lane's list (stable insertion sort, as Rust
 // std sorts slices of up to 20 elements) followed by the render_aa_line
 // winding walk; the row's union of spans replaces the list in place.
@@ -911,8 +799,6 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
     __shared__ int32_t scn[ROWS_WARPS][KCAP * 32];
     __shared__ int32_t sedge[ROWS_WARPS][8][32];
     __shared__ int32_t sns[ROWS_WARPS][32];
-    __shared__ uint32_t s_pref[ROWS_WARPS][32], s_mask[ROWS_WARPS][32], s_cnt[ROWS_WARPS][32];
-    __shared__ int32_t s_ra[ROWS_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
@@ -925,9 +811,8 @@ __global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
         const bool valid = r >= P.y0 && r <= chunk_hi;
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
-        const int n = gather_row_pairs<KCAP, 32>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w],
-                                                 sx0[w], sx1[w], scn[w], s_pref[w], s_mask[w], s_ra[w], s_cnt[w],
-                                                 lane);
+        const int n = gather_row<KCAP, 32>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
+                                           sx1[w], scn[w], lane);
         const bool overflow = valid && n > KCAP;
         int ns = 0;
         const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
