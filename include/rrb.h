@@ -315,6 +315,8 @@ typedef struct {
     uint64_t tiles, tile_pairs;             /* tiles with work, (tile, path) pairs */
     uint64_t nonterminating_rows;           /* rows whose winding never returns to 0 */
     uint64_t kernel_launches;               /* kernels launched by the last record call */
+    uint64_t scratch_grows;                 /* scratch buffers the call had to (re)allocate */
+    uint64_t waves;                         /* page groups the batch was rendered in */
 } rrb_batch_stats;
 int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
 

@@ -67,6 +67,7 @@ struct rrb_ctx {
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
+    uint64_t scratch_grows = 0;  // ensure() reallocations since the last record call began
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
     struct rrb_batch* wave_batch = nullptr; // view of a group of pages of a larger batch
     struct StageTimer* timer = nullptr;
@@ -126,6 +127,7 @@ int ensure(rrb_ctx* c, Scratch& s, size_t bytes) {
     int rc = dev_alloc(c, want, &s.p);
     if (rc) return rc;
     s.cap = want;
+    c->scratch_grows += 1;
     return RRB_OK;
 }
 
@@ -769,6 +771,7 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
         acc.tile_pairs += s.tile_pairs;
         acc.nonterminating_rows += s.nonterminating_rows;
         acc.kernel_launches += s.kernel_launches;
+        acc.waves += 1;
         return RRB_OK;
     }
     const bool splittable = (rc == RRB_ERR_OUT_OF_MEMORY || rc == RRB_ERR_POOL_EXHAUSTED) && pg1 - pg0 > 1 && depth < 20;
@@ -783,6 +786,12 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
 
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     rrb_batch_stats acc{};
+    const uint64_t grows0 = c->scratch_grows;
+    struct Done {
+        rrb_ctx* c;
+        uint64_t g0;
+        ~Done() { c->stats.scratch_grows = c->scratch_grows - g0; }
+    } done{c, grows0};
     const uint64_t wave_pts = c->tuning.wave_points ? c->tuning.wave_points : kWavePoints;
     if (B->n_paths == 0 || B->n_pts <= wave_pts) {
         int rc = run_pages(c, B, 0, B->n_pages, arena, arena_len, rowmap, acc, 0);
