@@ -120,6 +120,57 @@ def oracle_page(scene, threads=1):
     return a, time.perf_counter() - t, st
 
 
+class PathRange:
+    """Paths [a, b) of a one-page scene, as a scene of their own (the oracle
+    composites them onto the page exactly as it would inside the whole page)."""
+
+    def __init__(self, page, a, b):
+        p0, p1 = int(page.path_pt_off[a]), int(page.path_pt_off[b])
+        self.pts, self.flags = page.pts[p0:p1], page.flags[p0:p1]
+        self.path_pt_off = (page.path_pt_off[a:b + 1] - p0).astype(np.uint64)
+        self.fill_rule, self.gray, self.alpha = page.fill_rule[a:b], page.gray[a:b], page.alpha[a:b]
+        self.path_page = np.zeros(b - a, np.uint32)
+        self.page_width, self.page_height = page.page_width, page.page_height
+        self.page_offset = np.zeros(1, np.uint64)
+
+
+def oracle_prefix(page, arena, budget_s):
+    """The oracle, one thread, over the leading paths of a one-page scene
+    until budget_s seconds: (paths done, seconds, unpinned tie rows)."""
+    import rr_oracle
+    rr_oracle.build()
+    done, spent, ties, chunk = 0, 0.0, 0, 16
+    while done < page.n_paths and spent < budget_s:
+        e = min(page.n_paths, done + chunk)
+        t = time.perf_counter()
+        st = rr_oracle.render_scene(PathRange(page, done, e), arena)
+        dt = time.perf_counter() - t
+        spent += dt
+        ties += st["unpinned_tie_rows"]
+        done = e
+        if dt < 0.25:
+            chunk *= 2
+    return done, spent, ties
+
+
+def oracle_pages(scene, budget_s=20.0, page_budget_s=5.0):
+    """A bounded CPU sample of a multi-page batch: pages in batch order, each
+    rendered by the oracle on one thread for at most page_budget_s (its
+    leading paths), until budget_s in all. Returns
+    [(page, sub-scene, arena, paths done, seconds, tie rows)]."""
+    from rrb.shard import SceneShard
+    out, spent = [], 0.0
+    for pg in range(scene.n_pages):
+        sub = SceneShard(scene, pages=(pg, pg + 1))
+        a = sub.blank_arena()
+        done, secs, ties = oracle_prefix(sub, a, page_budget_s)
+        out.append((pg, sub, a, done, secs, ties))
+        spent += secs
+        if spent >= budget_s:
+            break
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference CPU path (its restatement) on the host cores."""
     if rank != 0:
@@ -129,14 +180,28 @@ def run_reference(args, rank, world):
     rr_oracle.build()
     kw, desc = WORKLOADS[args.workload]
     scene = rrb.Scene(**kw)
+    sample_desc, work = "the page", scene
+    px_per_copy = scene.pixels
+    if scene.n_pages > 1:
+        # A bounded sample of the batch: the leading paths of its first page
+        # that one thread renders in about 3 s, credited with that share of
+        # the page's pixels (pixels x paths done / paths on the page).
+        from rrb.shard import SceneShard
+        page0 = SceneShard(scene, pages=(0, 1))
+        k, _, _ = oracle_prefix(page0, page0.blank_arena(), 3.0)
+        work = PathRange(page0, 0, k)
+        px_per_copy = page0.pixels * k / max(1, page0.n_paths)
+        sample_desc = (f"the first {k} of {page0.n_paths} paths of the batch's first page, credited with "
+                       f"{k}/{page0.n_paths} of its pixels")
     cores = os.cpu_count() or 1
     threads = max(1, min(cores, args.ref_threads))
-    arenas = [scene.blank_arena() for _ in range(threads)]
+    arenas = [scene.blank_arena() if work is scene else np.full(int(work.page_width[0]) * int(work.page_height[0]),
+                                                                  255, np.uint8) for _ in range(threads)]
 
     def step():
         for a in arenas:
             a.fill(255)
-        ts = [threading.Thread(target=rr_oracle.render_scene, args=(scene, a), kwargs=dict(threads=1))
+        ts = [threading.Thread(target=rr_oracle.render_scene, args=(work, a), kwargs=dict(threads=1))
               for a in arenas]
         t = time.perf_counter()
         for x in ts:
@@ -149,8 +214,9 @@ def run_reference(args, rank, world):
         step()
     times = [step() for _ in range(args.steps)]
     total = sum(times)
-    mpx = scene.pixels * threads * args.steps / total / 1e6
-    sample = f"{threads} copies of the page per step, one per host thread (page-parallel, as the reference's per-page workers)"
+    mpx = px_per_copy * threads * args.steps / total / 1e6
+    sample = (f"{threads} copies of {sample_desc} per step, one per host thread (page-parallel, as the "
+              "reference's per-page workers)")
     line = {"impl": "reference", "metric": METRIC, "value": mpx, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
@@ -322,12 +388,30 @@ def run_rrb(args, rank, local, world):
     backend.wait_download(backend.download_async(pages, gpu_page))
     cpu = None
     bit_exact = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and scene.n_pages == 1:
         ref, secs, ost = oracle_page(scene, threads=1)
         bit_exact = bool(np.array_equal(ref, np.asarray(host_page)) and np.array_equal(ref, gpu_page))
         cpu = {"value": px / secs / 1e6, "unit": "Mpixel/s", "cores": 1, "kind": "port",
                "sample": "the whole page (all paths), 1 host thread, C++ restatement of the reference CPU path",
                "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"]}
+    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = oracle_pages(scene, budget_s=20.0, page_budget_s=5.0)
+        bit_exact, spx, est, secs, ties, whole = True, 0, 0.0, 0.0, 0, 0
+        hp = np.asarray(host_page)
+        for pg, sub, ref, done, s_, t_ in sample:
+            spx += sub.pixels
+            secs += s_
+            est += s_ * sub.n_paths / max(1, done)  # the page's time at the sample's paths-per-second
+            ties += t_
+            if done == sub.n_paths:
+                whole += 1
+                lo, hi = sub.arena_base, sub.arena_base + sub.arena_bytes
+                bit_exact &= bool(np.array_equal(ref, hp[lo:hi]) and np.array_equal(ref, gpu_page[lo:hi]))
+        cpu = {"value": spx / est / 1e6 if est > 0 else None, "unit": "Mpixel/s", "cores": 1, "kind": "port",
+               "sample": f"the first {len(sample)} of {scene.n_pages} pages, each for at most 5 s of its leading "
+                         "paths (page time extrapolated by its path count), 1 host thread, C++ restatement of "
+                         f"the reference CPU path; bit_exact covers the {whole} pages rendered whole",
+               "seconds": secs, "unpinned_tie_rows": ties}
     batch.free()
     if rank == 0:
         p50, p99 = (float(np.percentile(step_ms, q)) for q in (50, 99))

@@ -286,6 +286,11 @@ struct rrb_batch {
     uint32_t bpp = 1;               // page bytes per pixel: 1 Gray8, 3 Rgb8
     Scratch clip;                   // per-path clip in AA units (int4), when has_clip
     bool has_clip = false;
+    // Page groups [plan[i], plan[i+1]) that rendered without running out of
+    // scratch or cell capacity last time (with plan_wave_points); reused so a
+    // resident batch does not fail and split on every render.
+    std::vector<uint32_t> plan;
+    uint64_t plan_wave_points = 0;
     std::vector<PageGeom> geom_h;
     std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
     bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
@@ -364,6 +369,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     B->arena_need = 0;
     for (const PageGeom& G : B->geom_h)
         B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(B->bpp) * G.w * G.h);
+    B->plan.clear();
     B->page_pt.assign(B->n_pages + 1, 0);
     for (uint32_t pg = 0; pg < B->n_pages; ++pg) B->page_pt[pg] = h->path_pt_off[B->geom_h[pg].path_begin];
     B->page_pt[B->n_pages] = h->n_paths ? h->path_pt_off[h->n_paths] : 0;
@@ -751,7 +757,7 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
 constexpr uint64_t kWavePoints = 40ull << 20;
 
 int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* arena, size_t arena_len, int rowmap,
-              rrb_batch_stats& acc, int depth) {
+              rrb_batch_stats& acc, int depth, std::vector<uint32_t>& done_plan) {
     int rc;
     if (pg0 == 0 && pg1 == B->n_pages) {
         rc = run_resident_one(c, B, arena, arena_len, rowmap);
@@ -772,16 +778,19 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
         acc.nonterminating_rows += s.nonterminating_rows;
         acc.kernel_launches += s.kernel_launches;
         acc.waves += 1;
+        done_plan.push_back(pg1);
         return RRB_OK;
     }
     const bool splittable = (rc == RRB_ERR_OUT_OF_MEMORY || rc == RRB_ERR_POOL_EXHAUSTED) && pg1 - pg0 > 1 && depth < 20;
     if (!splittable) return rc;
-    // The composite had not run, so the pages are untouched: free the scratch and split.
+    // The composite had not run, so the pages are untouched: split. Out of
+    // memory also gives the scratch back first; a cell-capacity overflow
+    // (more than 2^32 coverage cells) keeps it.
     cudaGetLastError();
-    release_scratch(c);
+    if (rc == RRB_ERR_OUT_OF_MEMORY) release_scratch(c);
     const uint32_t mid = pg0 + (pg1 - pg0) / 2;
-    if ((rc = run_pages(c, B, pg0, mid, arena, arena_len, rowmap, acc, depth + 1))) return rc;
-    return run_pages(c, B, mid, pg1, arena, arena_len, rowmap, acc, depth + 1);
+    if ((rc = run_pages(c, B, pg0, mid, arena, arena_len, rowmap, acc, depth + 1, done_plan))) return rc;
+    return run_pages(c, B, mid, pg1, arena, arena_len, rowmap, acc, depth + 1, done_plan);
 }
 
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
@@ -793,22 +802,34 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         ~Done() { c->stats.scratch_grows = c->scratch_grows - g0; }
     } done{c, grows0};
     const uint64_t wave_pts = c->tuning.wave_points ? c->tuning.wave_points : kWavePoints;
-    if (B->n_paths == 0 || B->n_pts <= wave_pts) {
-        int rc = run_pages(c, B, 0, B->n_pages, arena, arena_len, rowmap, acc, 0);
-        c->stats = acc;
-        return rc;
+    // Wave plan: the groups that worked last time, else consecutive pages up
+    // to wave_pts points each (any group that fails is split in two).
+    std::vector<uint32_t> plan;
+    if (!B->plan.empty() && B->plan_wave_points == wave_pts && B->plan.back() == B->n_pages) {
+        plan = B->plan;
+    } else if (B->n_paths == 0 || B->n_pts <= wave_pts) {
+        plan = {0, B->n_pages};
+    } else {
+        plan.push_back(0);
+        uint32_t pg = 0;
+        while (pg < B->n_pages) {
+            uint32_t end = pg + 1;
+            while (end < B->n_pages && B->page_pt[end + 1] - B->page_pt[pg] <= wave_pts) ++end;
+            plan.push_back(end);
+            pg = end;
+        }
     }
-    uint32_t pg = 0;
-    while (pg < B->n_pages) {
-        uint32_t end = pg + 1;
-        while (end < B->n_pages && B->page_pt[end + 1] - B->page_pt[pg] <= wave_pts) ++end;
-        int rc = run_pages(c, B, pg, end, arena, arena_len, rowmap, acc, 0);
+    std::vector<uint32_t> done_plan{plan.front()};
+    for (size_t i = 0; i + 1 < plan.size(); ++i) {
+        int rc = run_pages(c, B, plan[i], plan[i + 1], arena, arena_len, rowmap, acc, 0, done_plan);
         if (rc) {
             c->stats = acc;
+            B->plan.clear();
             return rc;
         }
-        pg = end;
     }
+    B->plan = done_plan;
+    B->plan_wave_points = wave_pts;
     c->stats = acc;
     return RRB_OK;
 }

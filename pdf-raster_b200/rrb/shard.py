@@ -24,7 +24,13 @@ def page_shard(n_pages: int, rank: int, world: int) -> tuple[int, int]:
 def shard_arrays(scene, rank: int, world: int) -> dict:
     """The arrays of `scene` (rrb.Scene) restricted to this rank's pages,
     re-based to start at point 0, path 0, page 0 and arena byte 0."""
-    p0, p1 = page_shard(scene.n_pages, rank, world)
+    return range_arrays(scene, *page_shard(scene.n_pages, rank, world))
+
+
+def range_arrays(scene, p0: int, p1: int) -> dict:
+    """The arrays of `scene` restricted to pages [p0, p1), re-based as in shard_arrays."""
+    if not 0 <= p0 <= p1 <= scene.n_pages:
+        raise ValueError("page range out of bounds")
     sel = np.nonzero((scene.path_page >= p0) & (scene.path_page < p1))[0]
     if sel.size:
         a, b = int(scene.path_pt_off[sel[0]]), int(scene.path_pt_off[sel[-1] + 1])
@@ -58,13 +64,16 @@ def max_over_ranks(value: float, dist=None) -> float:
 
 
 class SceneShard:
-    """This rank's pages of an rrb.Scene, with the Scene attributes a renderer
-    uses (arrays, counts, `view` batch parameters, blank_arena)."""
+    """This rank's pages of an rrb.Scene (or the pages `pages` = [p0, p1)), with
+    the Scene attributes a renderer uses (arrays, counts, `view` batch
+    parameters, blank_arena); arena_base is the first page's byte offset in the
+    whole scene's arena."""
 
-    def __init__(self, scene, rank: int, world: int):
+    def __init__(self, scene, rank: int = 0, world: int = 1, pages: tuple[int, int] | None = None):
         from . import batch_params
 
-        sh = shard_arrays(scene, rank, world)
+        sh = range_arrays(scene, *pages) if pages is not None else shard_arrays(scene, rank, world)
+        self.arena_base = int(sh["arena_base"])
         self.pages_range = sh["pages"]
         for k in ("pts", "flags", "path_pt_off", "fill_rule", "gray", "alpha", "path_page", "page_width",
                   "page_height", "page_offset"):
