@@ -103,6 +103,16 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+# DRAM bytes per flattened segment of the row and flatten kernels on the glyph
+# page: dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of each
+# kernel on the glyph page reduced to 30,000 paths (10,979,156 segments, edge
+# records larger than L2), scaled to a full launch by its segment count.
+GLYPH_DRAM_BYTES_PER_SEGMENT = {
+    "rows": (387_620_864 + 43_667_712) / 10_979_156,
+    "seg_write": (169_890_304 + 404_720_384) / 10_979_156,
+}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -326,11 +336,18 @@ def run_rrb(args, rank, local, world):
     alg_b = alg.get(dom)
     roofline = None
     if alg_b:
-        dur = stage_ms[dom] / max(1, stage_acc[dom][1] / args.steps) / 1e3
-        ach = alg_b / dur / 1e9
+        # The stage runs its dominant kernel once per wave (k_rows beside the
+        # short k_chunk_paths / k_recti launches): per launch = per step / waves.
+        waves = max(1, int(stats.get("waves", 1)))
+        dur = stage_ms[dom] / waves / 1e3
+        ach = alg_b / waves / dur / 1e9
+        per_seg = GLYPH_DRAM_BYTES_PER_SEGMENT.get(dom) if args.workload == "glyphs" else None
+        traffic = per_seg * stats["segments"] / waves if per_seg else None
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "traffic": None, "peak_source": peak_kind,
-                    "algorithmic_bytes_per_launch": alg_b}
+                    "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
+                    "algorithmic_bytes_per_launch": alg_b / waves, "launch_ms": dur * 1e3,
+                    "traffic_source": ("ncu capture of the glyph page at 30,000 paths, scaled by segments"
+                                       if traffic else None)}
 
     # ---- plain per-path form on a sample of paths (one record_path_fill per path)
     plain = None
@@ -395,7 +412,7 @@ def run_rrb(args, rank, local, world):
                "sample": "the whole page (all paths), 1 host thread, C++ restatement of the reference CPU path",
                "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"]}
     elif rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = oracle_pages(scene, budget_s=20.0, page_budget_s=5.0)
+        sample = oracle_pages(scene, budget_s=15.0, page_budget_s=5.0)
         bit_exact, spx, est, secs, ties, whole = True, 0, 0.0, 0.0, 0, 0
         hp = np.asarray(host_page)
         for pg, sub, ref, done, s_, t_ in sample:
@@ -407,10 +424,26 @@ def run_rrb(args, rank, local, world):
                 whole += 1
                 lo, hi = sub.arena_base, sub.arena_base + sub.arena_bytes
                 bit_exact &= bool(np.array_equal(ref, hp[lo:hi]) and np.array_equal(ref, gpu_page[lo:hi]))
+        # Parity on whole pages as well: the pages with the fewest points,
+        # while they take the oracle about 10 s in all.
+        from rrb.shard import SceneShard
+        pts_per_page = np.diff(np.append(scene.path_pt_off[np.searchsorted(scene.path_page, np.arange(scene.n_pages))],
+                                         scene.path_pt_off[-1]).astype(np.int64))
+        checked = 0.0
+        for pg in np.argsort(pts_per_page, kind="stable"):
+            if checked >= 10.0:
+                break
+            sub = SceneShard(scene, pages=(int(pg), int(pg) + 1))
+            ref, secs_pg, _ = oracle_page(sub)
+            checked += secs_pg
+            lo, hi = sub.arena_base, sub.arena_base + sub.arena_bytes
+            bit_exact &= bool(np.array_equal(ref, hp[lo:hi]) and np.array_equal(ref, gpu_page[lo:hi]))
+            whole += 1
         cpu = {"value": spx / est / 1e6 if est > 0 else None, "unit": "Mpixel/s", "cores": 1, "kind": "port",
                "sample": f"the first {len(sample)} of {scene.n_pages} pages, each for at most 5 s of its leading "
                          "paths (page time extrapolated by its path count), 1 host thread, C++ restatement of "
-                         f"the reference CPU path; bit_exact covers the {whole} pages rendered whole",
+                         f"the reference CPU path; bit_exact covers {whole} whole pages (those sampled whole and the "
+                         "pages with the fewest points)",
                "seconds": secs, "unpinned_tie_rows": ties}
     batch.free()
     if rank == 0:

@@ -73,6 +73,9 @@ struct rrb_ctx {
     struct StageTimer* timer = nullptr;
     float stage_ms[16] = {};
     uint32_t stage_launches[16] = {};
+    // Per-stage sums over the waves of one resident render.
+    float stage_sum_ms[16] = {};
+    uint32_t stage_sum_launches[16] = {};
 };
 
 namespace {
@@ -424,6 +427,9 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
 int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     c->launches = 0;
     std::memset(&c->stats, 0, sizeof c->stats);
+    std::memset(c->stage_ms, 0, sizeof c->stage_ms);
+    std::memset(c->stage_launches, 0, sizeof c->stage_launches);
+    if (c->timer) std::memset(c->timer->used, 0, sizeof c->timer->used);
     if (B->n_paths == 0) return RRB_OK;
     if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
     if (rowmap < 0 || rowmap > 1) return set_err(c, RRB_ERR_INVARIANT, "rowmap must be 0 or 1");
@@ -778,6 +784,10 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
         acc.nonterminating_rows += s.nonterminating_rows;
         acc.kernel_launches += s.kernel_launches;
         acc.waves += 1;
+        for (int k = 0; k < 16; ++k) {
+            c->stage_sum_ms[k] += c->stage_ms[k];
+            c->stage_sum_launches[k] += c->stage_launches[k];
+        }
         done_plan.push_back(pg1);
         return RRB_OK;
     }
@@ -819,6 +829,8 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
             pg = end;
         }
     }
+    std::memset(c->stage_sum_ms, 0, sizeof c->stage_sum_ms);
+    std::memset(c->stage_sum_launches, 0, sizeof c->stage_sum_launches);
     std::vector<uint32_t> done_plan{plan.front()};
     for (size_t i = 0; i + 1 < plan.size(); ++i) {
         int rc = run_pages(c, B, plan[i], plan[i + 1], arena, arena_len, rowmap, acc, 0, done_plan);
@@ -831,6 +843,9 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     B->plan = done_plan;
     B->plan_wave_points = wave_pts;
     c->stats = acc;
+    // Stage times of the whole render: the sums over its waves.
+    std::memcpy(c->stage_ms, c->stage_sum_ms, sizeof c->stage_ms);
+    std::memcpy(c->stage_launches, c->stage_sum_launches, sizeof c->stage_launches);
     return RRB_OK;
 }
 
