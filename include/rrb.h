@@ -259,6 +259,49 @@ int rrb_record_path_batch_rgb(rrb_ctx* ctx, const rrb_path_batch_params* p, cons
  * rectangular W/W* clip path (detect_rect, clip.rs:130-140). */
 int rrb_record_path_batch_ex(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb,
                              const double* clip_rects);
+/* ---- strokes (crates/raster/src/stroke/mod.rs:58-283, stroke/path.rs) ----
+ * StrokeParams (stroke/mod.rs:29-48) of one path. The flatness is the batch's
+ * (the reference's renderer passes max(gs.flatness, 0.1) for both), and
+ * stroke adjustment is off as the reference's renderer always has it
+ * (crates/pdf_interp/src/renderer/page/mod.rs:1217-1227). */
+#define RRB_CAP_BUTT 0
+#define RRB_CAP_ROUND 1
+#define RRB_CAP_PROJECTING 2
+#define RRB_JOIN_MITER 0
+#define RRB_JOIN_ROUND 1
+#define RRB_JOIN_BEVEL 2
+typedef struct {
+    double line_width;    /* user space; 0 draws a hairline (stroke_narrow), > 0 an outline (stroke_wide) */
+    double miter_limit;
+    double dash_phase;
+    const double* dash;   /* host, n_dash entries >= 0; n_dash 0: solid */
+    uint32_t n_dash;
+    uint8_t line_cap;     /* RRB_CAP_* */
+    uint8_t line_join;    /* RRB_JOIN_* */
+    uint8_t stroke;       /* 0: the path is filled with its fill rule instead */
+    uint8_t reserved;
+} rrb_stroke_params;
+/* Paint a batch in path order, path p stroked when stroke[p].stroke, else
+ * filled as by rrb_record_path_batch_ex (path_rgb / clip_rects as there; for
+ * Rgb8 hairlines with alpha < 255 the blend is render_span's general arm,
+ * c = div255((255 - a) * dst + a * src), pipe/general.rs:261-312). stroke()
+ * per path: flatten_path, make_dashed_path when a dash array is set, then
+ * make_stroke_path's outline filled nonzero with AA (line_width > 0) or
+ * stroke_narrow's one-pixel spans (line_width 0). Outlines are built on the
+ * host (their round joins call libm atan2 / cos / sin and every segment libm
+ * hypot, whose last bits set the pixels), all filling and compositing on the
+ * device. Replaces the per-path raster::stroke call of PageRenderer::stroke_path
+ * (crates/pdf_interp/src/renderer/page/mod.rs:1201-1246). */
+int rrb_record_stroke_batch(rrb_ctx* ctx, const rrb_path_batch_params* p, const rrb_stroke_params* stroke,
+                            const uint8_t* path_rgb, const double* clip_rects);
+/* What rrb_record_stroke_batch draws for one path, on the host: *kind 0
+ * nothing, 1 the outline (filled nonzero), 2 the polyline of a hairline.
+ * Writes at most cap points to out_pts[2*cap] / out_flags[cap] (either may be
+ * NULL to ask for the size) and the full count to *out_n. */
+int rrb_stroke_outline(const double* pts, const uint8_t* flags, uint64_t n_pts, const rrb_stroke_params* stroke,
+                       double flatness, double* out_pts, uint8_t* out_flags, uint64_t cap, uint64_t* out_n,
+                       int* kind);
+
 /* rgb_to_gray (crates/pdf_raster/src/render.rs:1306-1324) on the device:
  * gray[i] = (2126 r + 7152 g + 722 b + 5000) / 10000 for n_px pixels. */
 int rrb_record_rgb_to_gray(rrb_ctx* ctx, const rrb_buf* rgb, size_t rgb_offset, const rrb_buf* gray,

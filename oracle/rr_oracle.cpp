@@ -864,6 +864,463 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
     delete sc;
 }
 
+// ============================================================================
+// F2: strokes (crates/raster/src/stroke/mod.rs:58-283, stroke/path.rs:40-745).
+// stroke(): flatten_path -> make_dashed_path (dash array set) -> line width
+// 0: stroke_narrow (hairline spans, no AA) / else stroke_wide (outline of
+// make_stroke_path filled nonzero with AA). Stroke adjustment is not restated:
+// the reference's renderer always passes stroke_adjust = false
+// (pdf_interp/src/renderer/page/mod.rs:1217-1227), so no hints are made.
+// ============================================================================
+
+constexpr double BEZIER_CIRCLE = 0.55228475;              // types.rs:45
+constexpr double BEZIER_CIRCLE2 = 0.5 * BEZIER_CIRCLE;    // stroke/path.rs:16
+constexpr double MITER_NEARLY_STRAIGHT = 0.9999;          // stroke/path.rs:22
+constexpr double PI_F64 = 3.141592653589793;              // std::f64::consts::PI
+
+// splash_dist (stroke/path.rs:741-745): f64::hypot, i.e. libm hypot.
+inline double splash_dist(double x0, double y0, double x1, double y1) { return std::hypot(x1 - x0, y1 - y0); }
+
+struct PathView {
+    const double* pts;
+    const uint8_t* flags;
+    size_t n;
+    double x(size_t i) const { return pts[2 * i]; }
+    double y(size_t i) const { return pts[2 * i + 1]; }
+    bool first(size_t i) const { return flags[i] & OR_PF_FIRST; }
+    bool last(size_t i) const { return flags[i] & OR_PF_LAST; }
+    bool closed(size_t i) const { return flags[i] & OR_PF_CLOSED; }
+    bool curve(size_t i) const { return flags[i] & OR_PF_CURVE; }
+};
+
+PathView view_of(const or_path& p) { return PathView{p.pts.data(), p.flags.data(), p.len()}; }
+
+// flatten_path (stroke/path.rs:40-86): curves flattened in user space against
+// flatness^2; builder errors are ignored as the reference ignores them.
+void flatten_path(const PathView& path, double flatness, or_path* out) {
+    const double flatness_sq = flatness * flatness;
+    std::vector<double> flat(2 * (MAX_CURVE_SPLITS + 1));
+    size_t i = 0;
+    while (i < path.n) {
+        if (path.first(i)) {
+            or_path_move_to(out, path.x(i), path.y(i));
+            i += 1;
+        } else if (path.curve(i)) {
+            if (i == 0 || i + 2 >= path.n) break;  // the reference indexes out of bounds here
+            const double cp[8] = {path.x(i - 1), path.y(i - 1), path.x(i), path.y(i),
+                                  path.x(i + 1), path.y(i + 1), path.x(i + 2), path.y(i + 2)};
+            const int32_t k = or_flatten_curve(cp, flatness_sq, flat.data(), MAX_CURVE_SPLITS + 1);
+            for (int32_t j = 0; j < k; ++j) or_path_line_to(out, flat[2 * j], flat[2 * j + 1]);
+            i += 3;
+            if (path.closed(i - 1)) or_path_close(out, 0);
+        } else {
+            or_path_line_to(out, path.x(i), path.y(i));
+            i += 1;
+            if (path.closed(i - 1)) or_path_close(out, 0);
+        }
+    }
+}
+
+// make_dashed_path (stroke/path.rs:107-220).
+void make_dashed_path(const PathView& path, const double* line_dash, size_t n_dash, double line_dash_phase,
+                      or_path* out) {
+    double line_dash_total = 0.0;
+    for (size_t k = 0; k < n_dash; ++k) line_dash_total += line_dash[k];
+    if (n_dash == 0 || line_dash_total < std::numeric_limits<double>::epsilon()) return;
+    double phase = line_dash_phase;
+    {
+        const int32_t periods = splash_floor(phase / line_dash_total);
+        phase -= static_cast<double>(periods) * line_dash_total;
+    }
+    bool dash_start_on = true;
+    size_t dash_start_idx = 0;
+    if (phase > 0.0) {
+        while (dash_start_idx < n_dash && phase >= line_dash[dash_start_idx]) {
+            dash_start_on = !dash_start_on;
+            phase -= line_dash[dash_start_idx];
+            dash_start_idx += 1;
+        }
+        if (dash_start_idx == n_dash) return;
+    }
+    size_t i = 0;
+    while (i < path.n) {
+        size_t j = i;
+        while (j < (path.n > 0 ? path.n - 1 : 0) && !path.last(j)) j += 1;
+        bool dash_on = dash_start_on;
+        size_t dash_idx = dash_start_idx;
+        double dash_dist = line_dash[dash_idx] - phase;
+        bool new_path = true;
+        for (size_t k = i; k < j; ++k) {
+            const double x0 = path.x(k), y0 = path.y(k);
+            const double x1 = path.x(k + 1), y1 = path.y(k + 1);
+            double seg_len = splash_dist(x0, y0, x1, y1);
+            double xa = x0, ya = y0;
+            while (seg_len > 0.0) {
+                if (dash_dist >= seg_len) {
+                    if (dash_on) {
+                        if (new_path) {
+                            or_path_move_to(out, xa, ya);
+                            new_path = false;
+                        }
+                        or_path_line_to(out, x1, y1);
+                    }
+                    dash_dist -= seg_len;
+                    seg_len = 0.0;
+                } else {
+                    const double xb = xa + (dash_dist / seg_len) * (x1 - xa);
+                    const double yb = ya + (dash_dist / seg_len) * (y1 - ya);
+                    if (dash_on) {
+                        if (new_path) {
+                            or_path_move_to(out, xa, ya);
+                            new_path = false;
+                        }
+                        or_path_line_to(out, xb, yb);
+                    }
+                    xa = xb;
+                    ya = yb;
+                    seg_len -= dash_dist;
+                    dash_dist = 0.0;
+                }
+                if (dash_dist <= 0.0) {
+                    dash_on = !dash_on;
+                    dash_idx += 1;
+                    if (dash_idx == n_dash) dash_idx = 0;
+                    dash_dist = line_dash[dash_idx];
+                    new_path = true;
+                }
+            }
+        }
+        i = j + 1;
+    }
+    if (out->len() == 0 && path.n > 0) {
+        bool all_same = true;
+        for (size_t k = 0; k + 1 < path.n; ++k)
+            if (!(path.x(k) == path.x(k + 1) && path.y(k) == path.y(k + 1))) all_same = false;
+        if (all_same) {
+            or_path_move_to(out, path.x(0), path.y(0));
+            or_path_line_to(out, path.x(0), path.y(0));
+        }
+    }
+}
+
+// advance_past_coincident (stroke/path.rs:723-733).
+size_t advance_past_coincident(const PathView& path, size_t start) {
+    size_t i = start;
+    while (!path.last(i) && i + 1 < path.n && path.x(i + 1) == path.x(i) && path.y(i + 1) == path.y(i)) i += 1;
+    return i;
+}
+
+// make_stroke_path (stroke/path.rs:250-706) without stroke-adjust hints.
+void make_stroke_path(const PathView& path, double w, const or_stroke_params& sp, or_path* out) {
+    if (path.n == 0) return;
+    size_t subpath_start0 = 0, subpath_start1 = 0;
+    bool closed = false;
+    size_t i0 = 0;
+    size_t i1 = advance_past_coincident(path, i0);
+    while (i1 < path.n) {
+        const bool first = path.first(i0);
+        if (first) {
+            subpath_start0 = i0;
+            subpath_start1 = i1;
+            closed = path.closed(i0);
+        }
+        (void)subpath_start0;
+        const size_t j0 = i1 + 1;
+        const size_t j1 = j0 < path.n ? advance_past_coincident(path, j0) : j0;
+        if (path.last(i1)) {
+            if (first && sp.line_cap == OR_CAP_ROUND) {
+                const double cx = path.x(i0), cy = path.y(i0);
+                const double r = 0.5 * w;
+                const double bc2w = BEZIER_CIRCLE2 * w;
+                or_path_move_to(out, cx + r, cy);
+                or_path_curve_to(out, cx + r, cy + bc2w, cx + bc2w, cy + r, cx, cy + r);
+                or_path_curve_to(out, cx - bc2w, cy + r, cx - r, cy + bc2w, cx - r, cy);
+                or_path_curve_to(out, cx - r, cy - bc2w, cx - bc2w, cy - r, cx, cy - r);
+                or_path_curve_to(out, cx + bc2w, cy - r, cx + r, cy - bc2w, cx + r, cy);
+                or_path_close(out, 0);
+            }
+            i0 = j0;
+            i1 = j1;
+            continue;
+        }
+        const bool last = path.last(j1);
+        const size_t k0 = last ? subpath_start1 + 1 : j1 + 1;
+        const double seg_dist = splash_dist(path.x(i1), path.y(i1), path.x(j0), path.y(j0));
+        if (seg_dist == 0.0) {
+            i0 = j0;
+            i1 = j1;
+            continue;
+        }
+        const double d = 1.0 / seg_dist;
+        const double dx = d * (path.x(j0) - path.x(i1));
+        const double dy = d * (path.y(j0) - path.y(i1));
+        const double wdx = 0.5 * w * dx;
+        const double wdy = 0.5 * w * dy;
+        const double ix = path.x(i0), iy = path.y(i0);
+        if (or_path_move_to(out, ix - wdy, iy + wdx) != 0) break;
+        if (first && !closed) {
+            switch (sp.line_cap) {
+                case OR_CAP_BUTT:
+                    or_path_line_to(out, ix + wdy, iy - wdx);
+                    break;
+                case OR_CAP_ROUND:
+                    or_path_curve_to(out, ix - wdy - BEZIER_CIRCLE * wdx, iy + wdx - BEZIER_CIRCLE * wdy,
+                                     ix - wdx - BEZIER_CIRCLE * wdy, iy - wdy + BEZIER_CIRCLE * wdx, ix - wdx,
+                                     iy - wdy);
+                    or_path_curve_to(out, ix - wdx + BEZIER_CIRCLE * wdy, iy - wdy - BEZIER_CIRCLE * wdx,
+                                     ix + wdy - BEZIER_CIRCLE * wdx, iy - wdx - BEZIER_CIRCLE * wdy, ix + wdy,
+                                     iy - wdx);
+                    break;
+                default:  // projecting
+                    or_path_line_to(out, ix - wdx - wdy, iy + wdx - wdy);
+                    or_path_line_to(out, ix - wdx + wdy, iy - wdx - wdy);
+                    or_path_line_to(out, ix + wdy, iy - wdx);
+                    break;
+            }
+        } else {
+            or_path_line_to(out, ix + wdy, iy - wdx);
+        }
+        const double jx = path.x(j0), jy = path.y(j0);
+        or_path_line_to(out, jx + wdy, jy - wdx);
+        if (last && !closed) {
+            switch (sp.line_cap) {
+                case OR_CAP_BUTT:
+                    or_path_line_to(out, jx - wdy, jy + wdx);
+                    break;
+                case OR_CAP_ROUND:
+                    or_path_curve_to(out, jx + wdy + BEZIER_CIRCLE * wdx, jy - wdx + BEZIER_CIRCLE * wdy,
+                                     jx + wdx + BEZIER_CIRCLE * wdy, jy + wdy - BEZIER_CIRCLE * wdx, jx + wdx,
+                                     jy + wdy);
+                    or_path_curve_to(out, jx + wdx - BEZIER_CIRCLE * wdy, jy + wdy + BEZIER_CIRCLE * wdx,
+                                     jx - wdy + BEZIER_CIRCLE * wdx, jy + wdx + BEZIER_CIRCLE * wdy, jx - wdy,
+                                     jy + wdx);
+                    break;
+                default:
+                    or_path_line_to(out, jx + wdy + wdx, jy - wdx + wdy);
+                    or_path_line_to(out, jx - wdy + wdx, jy + wdx + wdy);
+                    or_path_line_to(out, jx - wdy, jy + wdx);
+                    break;
+            }
+        } else {
+            or_path_line_to(out, jx - wdy, jy + wdx);
+        }
+        or_path_close(out, 0);  // close(stroke_adjust = false)
+        if (!last || closed) {
+            const double dn = 1.0 / splash_dist(path.x(j1), path.y(j1), path.x(k0), path.y(k0));
+            const double dx_next = dn * (path.x(k0) - path.x(j1));
+            const double dy_next = dn * (path.y(k0) - path.y(j1));
+            const double wdx_next = 0.5 * w * dx_next;
+            const double wdy_next = 0.5 * w * dy_next;
+            const double crossprod = dx * dy_next - dy * dx_next;
+            const double dotprod = -(dx * dx_next + dy * dy_next);
+            const bool has_angle = crossprod != 0.0 || dx * dx_next < 0.0 || dy * dy_next < 0.0;
+            double miter, m;
+            if (dotprod > MITER_NEARLY_STRAIGHT) {
+                miter = (sp.miter_limit + 1.0) * (sp.miter_limit + 1.0);
+                m = 0.0;
+            } else {
+                miter = std::fmax(2.0 / (1.0 - dotprod), 1.0);
+                m = std::sqrt(miter - 1.0);
+            }
+            if (has_angle && sp.line_join == OR_JOIN_ROUND) {
+                if (crossprod < 0.0) {
+                    double angle = std::atan2(dx, -dy);
+                    const double angle_next = std::atan2(dx_next, -dy_next);
+                    if (angle < angle_next) angle = angle + 2.0 * PI_F64;
+                    const double d_angle = (angle - angle_next) / PI_F64;
+                    if (d_angle < 0.501) {
+                        const double kappa = d_angle * BEZIER_CIRCLE * w;
+                        const double cx1 = jx - wdy + kappa * dx, cy1 = jy + wdx + kappa * dy;
+                        const double cx2 = jx - wdy_next - kappa * dx_next, cy2 = jy + wdx_next - kappa * dy_next;
+                        or_path_move_to(out, jx, jy);
+                        or_path_line_to(out, jx - wdy_next, jy + wdx_next);
+                        or_path_curve_to(out, cx2, cy2, cx1, cy1, jx - wdy, jy + wdx);
+                    } else {
+                        const double d_join = splash_dist(-wdy, wdx, -wdy_next, wdx_next);
+                        if (d_join > 0.0) {
+                            const double dx_join = (-wdy_next + wdy) / d_join;
+                            const double dy_join = (wdx_next - wdx) / d_join;
+                            const double xc = jx + 0.5 * w * std::cos(0.5 * (angle + angle_next));
+                            const double yc = jy + 0.5 * w * std::sin(0.5 * (angle + angle_next));
+                            const double kappa = d_angle * BEZIER_CIRCLE2 * w;
+                            const double cx1 = jx - wdy + kappa * dx, cy1 = jy + wdx + kappa * dy;
+                            const double cx2 = xc - kappa * dx_join, cy2 = yc - kappa * dy_join;
+                            const double cx3 = xc + kappa * dx_join, cy3 = yc + kappa * dy_join;
+                            const double cx4 = jx - wdy_next - kappa * dx_next, cy4 = jy + wdx_next - kappa * dy_next;
+                            or_path_move_to(out, jx, jy);
+                            or_path_line_to(out, jx - wdy_next, jy + wdx_next);
+                            or_path_curve_to(out, cx4, cy4, cx3, cy3, xc, yc);
+                            or_path_curve_to(out, cx2, cy2, cx1, cy1, jx - wdy, jy + wdx);
+                        }
+                    }
+                } else {
+                    const double angle = std::atan2(-dx, dy);
+                    double angle_next = std::atan2(-dx_next, dy_next);
+                    if (angle_next < angle) angle_next = angle_next + 2.0 * PI_F64;
+                    const double d_angle = (angle_next - angle) / PI_F64;
+                    if (d_angle < 0.501) {
+                        const double kappa = d_angle * BEZIER_CIRCLE * w;
+                        const double cx1 = jx + wdy + kappa * dx, cy1 = jy - wdx + kappa * dy;
+                        const double cx2 = jx + wdy_next - kappa * dx_next, cy2 = jy - wdx_next - kappa * dy_next;
+                        or_path_move_to(out, jx, jy);
+                        or_path_line_to(out, jx + wdy, jy - wdx);
+                        or_path_curve_to(out, cx1, cy1, cx2, cy2, jx + wdy_next, jy - wdx_next);
+                    } else {
+                        const double d_join = splash_dist(wdy, -wdx, wdy_next, -wdx_next);
+                        if (d_join > 0.0) {
+                            const double dx_join = (wdy_next - wdy) / d_join;
+                            const double dy_join = (-wdx_next + wdx) / d_join;
+                            const double xc = jx + 0.5 * w * std::cos(0.5 * (angle + angle_next));
+                            const double yc = jy + 0.5 * w * std::sin(0.5 * (angle + angle_next));
+                            const double kappa = d_angle * BEZIER_CIRCLE2 * w;
+                            const double cx1 = jx + wdy + kappa * dx, cy1 = jy - wdx + kappa * dy;
+                            const double cx2 = xc - kappa * dx_join, cy2 = yc - kappa * dy_join;
+                            const double cx3 = xc + kappa * dx_join, cy3 = yc + kappa * dy_join;
+                            const double cx4 = jx + wdy_next - kappa * dx_next, cy4 = jy - wdx_next - kappa * dy_next;
+                            or_path_move_to(out, jx, jy);
+                            or_path_line_to(out, jx + wdy, jy - wdx);
+                            or_path_curve_to(out, cx1, cy1, cx2, cy2, xc, yc);
+                            or_path_curve_to(out, cx3, cy3, cx4, cy4, jx + wdy_next, jy - wdx_next);
+                        }
+                    }
+                }
+            } else if (has_angle) {
+                or_path_move_to(out, jx, jy);
+                if (crossprod < 0.0) {
+                    or_path_line_to(out, jx - wdy_next, jy + wdx_next);
+                    if (sp.line_join == OR_JOIN_MITER && std::sqrt(miter) <= sp.miter_limit)
+                        or_path_line_to(out, jx - wdy + wdx * m, jy + wdx + wdy * m);
+                    or_path_line_to(out, jx - wdy, jy + wdx);
+                } else {
+                    or_path_line_to(out, jx + wdy, jy - wdx);
+                    if (sp.line_join == OR_JOIN_MITER && std::sqrt(miter) <= sp.miter_limit)
+                        or_path_line_to(out, jx + wdy + wdx * m, jy - wdx + wdy * m);
+                    or_path_line_to(out, jx + wdy_next, jy - wdx_next);
+                }
+            }
+            or_path_close(out, 0);
+        }
+        i0 = j0;
+        i1 = j1;
+    }
+}
+
+// The path stroke() fills or draws: flattened, then dashed when a dash array
+// is set (stroke/mod.rs:67-78). Returns false when nothing is to be drawn.
+bool stroke_polyline(const PathView& in, const or_stroke_params& sp, double flatness, or_path* out) {
+    if (in.n == 0) return false;
+    or_path flat;
+    flatten_path(in, flatness, &flat);
+    if (sp.n_dash > 0) {
+        make_dashed_path(view_of(flat), sp.dash, static_cast<size_t>(sp.n_dash), sp.dash_phase, out);
+        return out->len() != 0;
+    }
+    *out = flat;
+    return true;
+}
+
+// stroke_narrow (stroke/mod.rs:95-170) + draw_narrow_span (:204-256): spans
+// (y, x0, x1) handed to `span` already clamped and clipped. The clip is the
+// page, or the page and a clip rectangle (rect clips have no path scanners, so
+// Clip::test inside the integer bounds is true).
+template <typename SpanFn>
+void stroke_narrow_impl(int32_t width, int32_t height, const or_path& path, const double m[6], double flatness,
+                        const double* clip_rect, SpanFn span) {
+    const int64_t need = or_xpath_new(path.pts.data(), path.flags.data(), static_cast<int64_t>(path.len()), m,
+                                      flatness, 0, nullptr, 0);
+    std::vector<or_seg> segs(static_cast<size_t>(need));
+    or_xpath_new(path.pts.data(), path.flags.data(), static_cast<int64_t>(path.len()), m, flatness, 0, segs.data(),
+                 need);
+    const ClipRect clip = make_clip(width, height, clip_rect);
+    auto draw = [&](int32_t x0, int32_t x1, int32_t y, bool all_inside) {
+        if (y < 0 || y >= height) return;
+        int32_t sx0, sx1;
+        if (all_inside) {
+            sx0 = std::max(x0, 0);
+            sx1 = std::min(x1, width - 1);
+        } else {
+            sx0 = std::max(x0, clip.x_min_i);
+            sx1 = std::min(x1, clip.x_max_i);
+        }
+        if (sx0 > sx1) return;
+        if (!all_inside && (y < clip.y_min_i || y > clip.y_max_i)) return;  // Clip::test fails on every pixel
+        span(y, sx0, sx1);
+    };
+    for (const or_seg& seg : segs) {
+        double sx0, sy0, sx1, sy1;
+        if (seg.y0 <= seg.y1) {
+            sx0 = seg.x0; sy0 = seg.y0; sx1 = seg.x1; sy1 = seg.y1;
+        } else {
+            sx0 = seg.x1; sy0 = seg.y1; sx1 = seg.x0; sy1 = seg.y0;
+        }
+        const int32_t y0 = splash_floor(sy0), y1 = splash_floor(sy1);
+        const int32_t x0 = splash_floor(sx0), x1 = splash_floor(sx1);
+        const int32_t xl = std::min(x0, x1), xr = std::max(x0, x1);
+        // Clip::test_rect (clip.rs:196-215), right + 1 / bottom + 1 in i32 as the reference computes them.
+        const double r1 = static_cast<double>(static_cast<int32_t>(static_cast<uint32_t>(xr) + 1u));
+        const double b1 = static_cast<double>(static_cast<int32_t>(static_cast<uint32_t>(y1) + 1u));
+        if (r1 <= clip.x_min || static_cast<double>(xl) >= clip.x_max || b1 <= clip.y_min ||
+            static_cast<double>(y0) >= clip.y_max)
+            continue;
+        const bool all_inside = static_cast<double>(xl) >= clip.x_min && r1 <= clip.x_max &&
+                                static_cast<double>(y0) >= clip.y_min && b1 <= clip.y_max;
+        if (y0 == y1) {
+            draw(xl, xr, y0, all_inside);
+            continue;
+        }
+        const double dxdy = seg.dxdy;
+        int32_t cy0 = y0, cx0 = x0, cy1 = y1, cx1 = x1;
+        if (cy0 < clip.y_min_i) {
+            cy0 = clip.y_min_i;
+            cx0 = splash_floor(std::fma(clip.y_min - sy0, dxdy, sx0));
+        }
+        if (cy1 > clip.y_max_i) {
+            cy1 = clip.y_max_i;
+            cx1 = splash_floor(std::fma(clip.y_max - sy0, dxdy, sx0));
+        }
+        int32_t xa = cx0;
+        const bool left_to_right = cx0 <= cx1;
+        for (int32_t y = cy0; y <= cy1; ++y) {
+            int32_t xb;
+            if (y < cy1) xb = splash_floor(std::fma(static_cast<double>(y) + 1.0 - sy0, dxdy, sx0));
+            else xb = left_to_right ? cx1 + 1 : cx1 - 1;
+            int32_t a, b;
+            if (left_to_right) {
+                a = xa;
+                b = xa == xb ? xa : xb - 1;
+            } else if (xa == xb) {
+                a = b = xa;
+            } else {
+                a = xb + 1;
+                b = xa;
+            }
+            draw(a, b, y, all_inside);
+            xa = xb;
+        }
+    }
+}
+
+// One painting operator of a scene: a fill (rule as given) or a stroke.
+template <typename AaSpan, typename SolidSpan>
+void paint_path(int32_t W, int32_t H, const double* pts, const uint8_t* flags, int64_t n, const double m[6],
+                double flatness, int eo, int rowmap, or_stats* st, const or_stroke_params* sp, const double* clip,
+                AaSpan aa_span, SolidSpan solid_span) {
+    if (!sp || !sp->stroke) {
+        fill_path_impl(W, H, pts, flags, n, m, flatness, eo, rowmap, st, aa_span, clip);
+        return;
+    }
+    or_path poly;
+    if (!stroke_polyline(PathView{pts, flags, static_cast<size_t>(n)}, *sp, flatness, &poly)) return;
+    if (sp->line_width == 0.0) {
+        stroke_narrow_impl(W, H, poly, m, flatness, clip, solid_span);
+        return;
+    }
+    or_path outline;
+    make_stroke_path(view_of(poly), sp->line_width, *sp, &outline);
+    fill_path_impl(W, H, outline.pts.data(), outline.flags.data(), static_cast<int64_t>(outline.len()), m, flatness,
+                   0, rowmap, st, aa_span, clip);
+}
+
 // Pages of a scene on up to n_threads workers; rgb == nullptr: Gray8 pages
 // and gray[] sources, else Rgb8 pages (3 bytes per pixel) and rgb[3 * p].
 void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w,
@@ -871,7 +1328,8 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
                        const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
                        const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
                        uint64_t n_paths, const double m[6], double flatness, int rowmap,
-                       int n_threads, or_stats* st, const double* clip = nullptr);
+                       int n_threads, or_stats* st, const double* clip = nullptr,
+                       const or_stroke_params* sp = nullptr);
 
 }  // namespace
 
@@ -915,6 +1373,40 @@ void or_render_scene_ex(uint8_t* arena, const uint64_t* page_off, const uint32_t
                       path_page, n_paths, m, flatness, rowmap, n_threads, st, clip);
 }
 
+void or_render_scene_paint(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                           uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                           const uint8_t* rule, const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha,
+                           const uint32_t* path_page, uint64_t n_paths, const double* clip,
+                           const or_stroke_params* stroke, const double m[6], double flatness, int rowmap,
+                           int n_threads, or_stats* st) {
+    render_scene_impl(arena, page_off, page_w, page_h, n_pages, pts, flags, path_pt_off, rule, gray, rgb, alpha,
+                      path_page, n_paths, m, flatness, rowmap, n_threads, st, clip, stroke);
+}
+
+int or_stroke_outline(const double* pts, const uint8_t* flags, int64_t n, const or_stroke_params* sp,
+                      double flatness, or_path* out) {
+    or_path poly;
+    if (!sp || !stroke_polyline(PathView{pts, flags, static_cast<size_t>(n)}, *sp, flatness, &poly)) return 0;
+    if (sp->line_width == 0.0) {
+        *out = poly;
+        return 2;
+    }
+    make_stroke_path(view_of(poly), sp->line_width, *sp, out);
+    return out->len() ? 1 : 0;
+}
+
+int or_stroke_flatten(const double* pts, const uint8_t* flags, int64_t n, double flatness, or_path* out) {
+    flatten_path(PathView{pts, flags, static_cast<size_t>(n)}, flatness, out);
+    return 0;
+}
+
+int or_stroke_dash(const double* pts, const uint8_t* flags, int64_t n, const double* dash, int32_t n_dash,
+                   double phase, or_path* out) {
+    make_dashed_path(PathView{pts, flags, static_cast<size_t>(n)}, dash, static_cast<size_t>(std::max(n_dash, 0)),
+                     phase, out);
+    return 0;
+}
+
 void or_render_scene_rgb(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
                          uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
                          const uint8_t* rule, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
@@ -933,7 +1425,7 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
                        const uint8_t* flags, const uint64_t* path_pt_off, const uint8_t* rule,
                        const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha, const uint32_t* path_page,
                        uint64_t n_paths, const double m[6], double flatness, int rowmap,
-                       int n_threads, or_stats* st, const double* clip) {
+                       int n_threads, or_stats* st, const double* clip, const or_stroke_params* sp) {
     // Paths of each page, in scene order.
     std::vector<std::vector<uint64_t>> per_page(n_pages);
     for (uint64_t p = 0; p < n_paths; ++p)
@@ -951,24 +1443,34 @@ void render_scene_impl(uint8_t* arena, const uint64_t* page_off, const uint32_t*
                 uint64_t a = path_pt_off[p], b = path_pt_off[p + 1];
                 const int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
                 const double* cp = clip ? clip + 4 * p : nullptr;
+                const or_stroke_params* psp = sp ? sp + p : nullptr;
+                const uint8_t a_in = alpha[p];
                 if (rgb) {
                     const uint8_t* src = rgb + 3 * p;
-                    const uint8_t a_in = alpha[p];
-                    fill_path_impl(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness,
-                                   rule[p] != 0, rowmap, &ls,
-                                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
-                                       or_composite_aa_rgb8_opaque(page + 3 * (static_cast<int64_t>(y) * W + x0), src,
-                                                                   a_in, shape, n);
-                                   },
-                                   cp);
+                    paint_path(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
+                               rowmap, &ls, psp, cp,
+                               [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                                   or_composite_aa_rgb8_opaque(page + 3 * (static_cast<int64_t>(y) * W + x0), src, a_in,
+                                                               shape, n);
+                               },
+                               [&](int32_t y, int32_t x0, int32_t x1) {
+                                   // render_span without shape: simple copy at alpha 255, else
+                                   // the general arm's div255 per channel (pipe/general.rs:261-312).
+                                   uint8_t* d = page + 3 * (static_cast<int64_t>(y) * W + x0);
+                                   for (int64_t i = 0; i < 3 * (static_cast<int64_t>(x1) - x0 + 1); ++i)
+                                       d[i] = or_div255((255u - a_in) * d[i] + a_in * src[i % 3]);
+                               });
                 } else {
-                    const uint8_t g = gray[p], a_in = alpha[p];
-                    fill_path_impl(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness,
-                                   rule[p] != 0, rowmap, &ls,
-                                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
-                                       or_render_span_aa_gray(page + static_cast<int64_t>(y) * W + x0, shape, n, a_in, g);
-                                   },
-                                   cp);
+                    const uint8_t g = gray[p];
+                    paint_path(W, H, pts + 2 * a, flags + a, static_cast<int64_t>(b - a), m, flatness, rule[p] != 0,
+                               rowmap, &ls, psp, cp,
+                               [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                                   or_render_span_aa_gray(page + static_cast<int64_t>(y) * W + x0, shape, n, a_in, g);
+                               },
+                               [&](int32_t y, int32_t x0, int32_t x1) {
+                                   uint8_t* d = page + static_cast<int64_t>(y) * W;
+                                   for (int32_t x = x0; x <= x1; ++x) d[x] = or_div255((255u - a_in) * d[x] + a_in * g);
+                               });
                 }
             }
         }

@@ -170,6 +170,41 @@ void or_render_scene_ex(uint8_t* arena, const uint64_t* page_off, const uint32_t
                         const uint32_t* path_page, uint64_t n_paths, const double* clip, const double m[6],
                         double flatness, int rowmap, int n_threads, or_stats* st);
 
+/* ---- F2: strokes (stroke/mod.rs:58-283, stroke/path.rs:40-745) -------- */
+#define OR_CAP_BUTT 0
+#define OR_CAP_ROUND 1
+#define OR_CAP_PROJECTING 2
+#define OR_JOIN_MITER 0
+#define OR_JOIN_ROUND 1
+#define OR_JOIN_BEVEL 2
+
+/* StrokeParams (stroke/mod.rs:29-48) with stroke_adjust = false and the
+ * scene's flatness; stroke == 0 makes the path an ordinary fill. */
+typedef struct {
+    double line_width, miter_limit, dash_phase;
+    const double* dash;
+    int32_t n_dash;
+    int32_t line_cap, line_join;
+    int32_t stroke;
+} or_stroke_params;
+
+/* flatten_path (stroke/path.rs:40-86) and make_dashed_path (:107-220) into out. */
+int or_stroke_flatten(const double* pts, const uint8_t* flags, int64_t n, double flatness, or_path* out);
+int or_stroke_dash(const double* pts, const uint8_t* flags, int64_t n, const double* dash, int32_t n_dash,
+                   double phase, or_path* out);
+/* What stroke() draws for one path: 0 nothing (no points); 1 out = make_stroke_path's
+ * outline (filled nonzero); 2 out = the flattened (dashed) polyline of a
+ * hairline (line_width 0, drawn by stroke_narrow). */
+int or_stroke_outline(const double* pts, const uint8_t* flags, int64_t n, const or_stroke_params* sp,
+                      double flatness, or_path* out);
+/* or_render_scene_ex where path p is stroked when stroke && stroke[p].stroke. */
+void or_render_scene_paint(uint8_t* arena, const uint64_t* page_off, const uint32_t* page_w, const uint32_t* page_h,
+                           uint32_t n_pages, const double* pts, const uint8_t* flags, const uint64_t* path_pt_off,
+                           const uint8_t* rule, const uint8_t* gray, const uint8_t* rgb, const uint8_t* alpha,
+                           const uint32_t* path_page, uint64_t n_paths, const double* clip,
+                           const or_stroke_params* stroke, const double m[6], double flatness, int rowmap,
+                           int n_threads, or_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,6 +44,16 @@ IDENTITY = (1.0, 0.0, 0.0, 1.0, 0.0, 0.0)
 
 _LIB = None
 
+CAP_BUTT, CAP_ROUND, CAP_PROJECTING = 0, 1, 2
+JOIN_MITER, JOIN_ROUND, JOIN_BEVEL = 0, 1, 2
+
+
+class StrokeParams(C.Structure):
+    """or_stroke_params: StrokeParams (stroke/mod.rs:29-48), stroke_adjust off."""
+    _fields_ = [("line_width", C.c_double), ("miter_limit", C.c_double), ("dash_phase", C.c_double),
+                ("dash", C.POINTER(C.c_double)), ("n_dash", C.c_int32), ("line_cap", C.c_int32),
+                ("line_join", C.c_int32), ("stroke", C.c_int32)]
+
 
 def build(arch: str | None = None) -> Path:
     """Compile the oracle if needed. `arch` overrides -march (default x86-64-v3, portable to any AVX2 host)."""
@@ -106,6 +116,15 @@ def lib() -> C.CDLL:
                                           C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
                                           C.POINTER(U8), C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D),
                                           C.POINTER(D), D, C.c_int, C.c_int, C.POINTER(Stats)]),
+            "or_stroke_flatten": (C.c_int, [C.POINTER(D), C.POINTER(U8), I64, D, VP]),
+            "or_stroke_dash": (C.c_int, [C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D), I32, D, VP]),
+            "or_stroke_outline": (C.c_int, [C.POINTER(D), C.POINTER(U8), I64, C.POINTER(StrokeParams), D, VP]),
+            "or_render_scene_paint": (None, [C.POINTER(U8), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(D), C.POINTER(U8),
+                                             C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
+                                             C.POINTER(U8), C.POINTER(C.c_uint32), C.c_uint64, C.POINTER(D),
+                                             C.POINTER(StrokeParams), C.POINTER(D), D, C.c_int, C.c_int,
+                                             C.POINTER(Stats)]),
             "or_aa_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
             "or_aa_fill_cpu": (None, [C.POINTER(C.c_float), C.c_uint32, C.c_float, C.c_float, C.c_uint32,
                                       C.c_uint32, C.c_int, C.POINTER(U8)]),
@@ -422,3 +441,98 @@ def tile_fill(records, starts, counts, grid_w, width, height, eo=False):
     lib().or_tile_fill(records.ctypes.data, _p(starts, C.c_uint32), _p(counts, C.c_uint32), grid_w, width, height,
                        int(eo), _p(out, C.c_uint8))
     return out.reshape(height, width)
+
+
+# ---- F2: strokes ------------------------------------------------------------------
+def stroke_params(strokes, keep):
+    """StrokeParams array from a list of dicts (None = fill): keys line_width,
+    line_cap, line_join, miter_limit (10), dash (sequence), dash_phase (0)."""
+    arr = (StrokeParams * max(1, len(strokes)))()
+    for i, d in enumerate(strokes):
+        if d is None:
+            continue
+        dash = np.ascontiguousarray(d.get("dash", ()), np.float64)
+        keep.append(dash)
+        arr[i].line_width = float(d["line_width"])
+        arr[i].miter_limit = float(d.get("miter_limit", 10.0))
+        arr[i].dash_phase = float(d.get("dash_phase", 0.0))
+        arr[i].dash = _p(dash, C.c_double) if dash.size else None
+        arr[i].n_dash = int(dash.size)
+        arr[i].line_cap = int(d.get("line_cap", CAP_BUTT))
+        arr[i].line_join = int(d.get("line_join", JOIN_MITER))
+        arr[i].stroke = 1
+    return arr
+
+
+def _path_arrays(pts, flags):
+    p = np.ascontiguousarray(np.reshape(pts, -1), np.float64)
+    f = np.ascontiguousarray(flags, np.uint8)
+    return p, f
+
+
+def _take(h):
+    o = OraclePath.__new__(OraclePath)
+    o.h = h
+    return o.build()
+
+
+def stroke_flatten(pts, flags, flatness=0.1):
+    """flatten_path (stroke/path.rs:40-86): (pts[n,2], flags[n])."""
+    p, f = _path_arrays(pts, flags)
+    h = lib().or_path_new()
+    lib().or_stroke_flatten(_p(p, C.c_double), _p(f, C.c_uint8), f.size, flatness, h)
+    return _take(h)
+
+
+def stroke_dash(pts, flags, dash, phase=0.0):
+    """make_dashed_path (stroke/path.rs:107-220) of an already flat path."""
+    p, f = _path_arrays(pts, flags)
+    d = np.ascontiguousarray(dash, np.float64)
+    h = lib().or_path_new()
+    lib().or_stroke_dash(_p(p, C.c_double), _p(f, C.c_uint8), f.size, _p(d, C.c_double), d.size, phase, h)
+    return _take(h)
+
+
+def stroke_outline(pts, flags, flatness=0.1, **stroke):
+    """What stroke() draws: (kind, pts, flags); kind 0 nothing, 1 the outline
+    make_stroke_path builds (filled nonzero), 2 a hairline polyline."""
+    p, f = _path_arrays(pts, flags)
+    keep = []
+    sp = stroke_params([stroke], keep)
+    h = lib().or_path_new()
+    kind = lib().or_stroke_outline(_p(p, C.c_double), _p(f, C.c_uint8), f.size, sp, flatness, h)
+    pts2, fl2 = _take(h)
+    return kind, pts2, fl2
+
+
+def render_scene_paint(scene, arena: np.ndarray, strokes, rgb=None, clip=None, rowmap=ROWMAP_DOCUMENTED, threads=1,
+                       page_offset=None, flatness=0.1) -> dict:
+    """render_scene_ex where path p is stroked with strokes[p] (a dict as in
+    stroke_params) or filled when strokes[p] is None."""
+    bpp = 1 if rgb is None else 3
+    po = np.ascontiguousarray(bpp * scene.page_offset.astype(np.uint64) if page_offset is None else page_offset,
+                              np.uint64)
+    a = [np.ascontiguousarray(x, t) for x, t in (
+        (scene.page_width, np.uint32), (scene.page_height, np.uint32), (np.reshape(scene.pts, -1), np.float64),
+        (scene.flags, np.uint8), (scene.path_pt_off, np.uint64), (scene.fill_rule, np.uint8),
+        (scene.alpha, np.uint8), (scene.path_page, np.uint32))]
+    gray = np.ascontiguousarray(getattr(scene, "gray", np.zeros(a[5].size, np.uint8)), np.uint8)
+    keep = []
+    sp = stroke_params(list(strokes), keep)
+    rgbp = None
+    if rgb is not None:
+        r = np.ascontiguousarray(np.reshape(rgb, -1), np.uint8)
+        keep.append(r)
+        rgbp = _p(r, C.c_uint8)
+    clipp = None
+    if clip is not None:
+        c = np.ascontiguousarray(np.reshape(clip, -1), np.float64)
+        keep.append(c)
+        clipp = _p(c, C.c_double)
+    st = Stats()
+    lib().or_render_scene_paint(_p(arena, C.c_uint8), _p(po, C.c_uint64), _p(a[0], C.c_uint32),
+                                _p(a[1], C.c_uint32), a[0].size, _p(a[2], C.c_double), _p(a[3], C.c_uint8),
+                                _p(a[4], C.c_uint64), _p(a[5], C.c_uint8), _p(gray, C.c_uint8), rgbp,
+                                _p(a[6], C.c_uint8), _p(a[7], C.c_uint32), a[5].size, clipp, sp, _mat(IDENTITY),
+                                flatness, rowmap, threads, C.byref(st))
+    return st.as_dict()

@@ -21,7 +21,9 @@
 #include <vector>
 
 #include "../../include/rrb.h"
+#include "rrb_hairline.cuh"
 #include "rrb_kernels.cuh"
+#include "rrb_stroke.h"
 
 using namespace rrb;
 
@@ -63,7 +65,7 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
-    Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo;
+    Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
@@ -702,7 +704,7 @@ void release_scratch(rrb_ctx* c) {
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
                       &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
-                      &c->s_chunk_path, &c->s_clip_lo};
+                      &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip};
     for (Scratch* x : all) {
         dev_free(c, x->p, x->cap);
         x->p = nullptr;
@@ -855,6 +857,222 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
     int rc = batch_upload(c, h, B, rgb, clip);
     if (rc) return rc;
     return run_resident(c, B, arena, arena_len, h->rowmap);
+}
+
+// Hairline segments (two-point paths of h, one layer each; see
+// rrb_hairline.cuh) into the device pages: spans per pixel row, then the
+// binning and the tile compositor of fills. clip: host doubles, 4 per segment.
+int run_hairlines(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len, const uint8_t* rgb,
+                  const double* clip) {
+    rrb_batch* B = c->tmp_batch;
+    int rc = batch_upload(c, h, B, rgb, clip);
+    if (rc) return rc;
+    c->launches = 0;
+    std::memset(&c->stats, 0, sizeof c->stats);
+    if (B->n_paths == 0) return RRB_OK;
+    if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
+    const uint32_t tw = c->tuning.tile_w ? c->tuning.tile_w : 64;
+    const uint32_t th = c->tuning.tile_h ? c->tuning.tile_h : 16;
+    uint64_t tiles = 0;
+    set_tiles(B->geom_h, tw, th, tiles);
+    if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
+    const uint32_t NS = static_cast<uint32_t>(B->n_paths), n_pages = B->n_pages;
+    const uint64_t supers = B->supers;
+    const int rowmap = B->rowmap;
+    RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
+                                c->stream));
+    const double* clipd = nullptr;
+    if (clip) {
+        if ((rc = upload(c, c->s_hl_clip, clip, 4 * static_cast<size_t>(NS)))) return rc;
+        clipd = as<double>(c->s_hl_clip);
+    }
+    if ((rc = ensure(c, c->s_info, NS * sizeof(PathInfo)))) return rc;
+    if ((rc = ensure(c, c->s_run_off, (NS + 1ull) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_rows, (NS + 1ull) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_row_idx, sizeof(uint2)))) return rc;
+    if ((rc = ensure(c, c->s_block, (SCAN_MAX_BLOCKS + 1) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
+    if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
+    RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
+    RRB_CUDA(c, cudaMemsetAsync(c->s_rows.p, 0, (NS + 1ull) * sizeof(uint32_t), c->stream));
+    k_hl_count<<<grid_for(c, NS, 128, 16), 128, 0, c->stream>>>(
+        as<double>(B->pts), as<double>(B->mtx), as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph),
+        clipd, as<uint8_t>(B->gray), as<uint8_t>(B->alpha), NS, rowmap, as<PathInfo>(c->s_info),
+        as<uint32_t>(c->s_run_off));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NS))) return rc;
+    if ((rc = read_back(c, as<uint32_t>(c->s_run_off) + NS, sizeof(uint32_t)))) return rc;
+    const uint64_t n_runs = c->h_read[0];
+    if ((rc = ensure(c, c->s_runs, std::max<uint64_t>(1, n_runs) * sizeof(int4)))) return rc;
+    if ((rc = ensure(c, c->s_spans, std::max<uint64_t>(1, n_runs) * sizeof(uint32_t)))) return rc;
+    k_hl_write<<<grid_for(c, NS * 32ull, 256, 8), 256, 0, c->stream>>>(
+        as<double>(B->pts), as<double>(B->mtx), as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph),
+        clipd, NS, rowmap, as<uint32_t>(c->s_run_off), as<PathInfo>(c->s_info), as<int4>(c->s_runs),
+        as<uint32_t>(c->s_spans));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    // Binning and the compositor, as for fills.
+    const uint32_t NSUP = static_cast<uint32_t>(supers);
+    k_super_bin<false><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
+        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, as<uint32_t>(c->s_super_cnt),
+        nullptr, nullptr);
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    if ((rc = scan_u32(c, as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_cnt), NSUP))) return rc;
+    if ((rc = read_back(c, as<uint32_t>(c->s_super_cnt) + NSUP, sizeof(uint32_t)))) return rc;
+    const uint64_t n_pairs = c->h_read[0];
+    if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
+    k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
+        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, nullptr,
+        as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 8),
+                               as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
+                               as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
+                               as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
+                               rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr)))
+        return rc;
+    if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+    BatchCounters hc;
+    std::memcpy(&hc, c->h_read, sizeof hc);
+    c->stats.paths = NS;
+    c->stats.segments = NS;
+    c->stats.spans = n_runs;
+    c->stats.tiles = tiles;
+    c->stats.tile_pairs = n_pairs;
+    c->stats.kernel_launches = c->launches;
+    c->stats.waves = 1;
+    if (hc.err) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "hairline batch capacity exceeded");
+    return RRB_OK;
+}
+
+// One run of consecutive paths of a paint batch that draw the same way
+// (fills and stroke outlines, or hairlines), as a batch of its own over the
+// pages the run touches.
+struct PaintRun {
+    std::vector<double> pts, clip;
+    std::vector<uint8_t> flags, rule, gray, alpha, rgb;
+    std::vector<uint64_t> off{0}, page_off;
+    std::vector<uint32_t> page, pw, ph;
+    uint32_t last_page = UINT32_MAX;
+
+    void clear() {
+        pts.clear();
+        clip.clear();
+        flags.clear();
+        rule.clear();
+        gray.clear();
+        alpha.clear();
+        rgb.clear();
+        off.assign(1, 0);
+        page_off.clear();
+        page.clear();
+        pw.clear();
+        ph.clear();
+        last_page = UINT32_MAX;
+    }
+    // A path of the run: its points, paint and page (pages of the input batch
+    // are renumbered in order of first use).
+    void add(const rrb_path_batch_params* p, uint32_t path, const double* xy, const uint8_t* fl, uint64_t n,
+             uint8_t fill_rule, const uint8_t* path_rgb, const double* clip_rects) {
+        const uint32_t pg = p->path_page[path];
+        if (pg != last_page) {
+            last_page = pg;
+            pw.push_back(p->page_width[pg]);
+            ph.push_back(p->page_height[pg]);
+            page_off.push_back(p->page_offset[pg]);
+        }
+        pts.insert(pts.end(), xy, xy + 2 * n);
+        flags.insert(flags.end(), fl, fl + n);
+        off.push_back(flags.size());
+        rule.push_back(fill_rule);
+        gray.push_back(p->gray[path]);
+        alpha.push_back(p->alpha[path]);
+        page.push_back(static_cast<uint32_t>(pw.size() - 1));
+        if (path_rgb) rgb.insert(rgb.end(), path_rgb + 3 * path, path_rgb + 3 * path + 3);
+        if (clip_rects) clip.insert(clip.end(), clip_rects + 4 * path, clip_rects + 4 * path + 4);
+    }
+    rrb_path_batch_params params(const rrb_path_batch_params* p) const {
+        rrb_path_batch_params q = *p;
+        q.pts = pts.data();
+        q.flags = flags.data();
+        q.n_pts = flags.size();
+        q.path_pt_off = off.data();
+        q.fill_rule = rule.data();
+        q.gray = gray.data();
+        q.alpha = alpha.data();
+        q.path_page = page.data();
+        q.n_paths = rule.size();
+        q.page_width = pw.data();
+        q.page_height = ph.data();
+        q.page_offset = page_off.data();
+        q.n_pages = static_cast<uint32_t>(pw.size());
+        return q;
+    }
+};
+
+int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_params* sp, const uint8_t* path_rgb,
+                const double* clip_rects) {
+    std::string msg;
+    rrb_stroke::Plan plan;
+    int rc = rrb_stroke::plan(p, sp, plan, msg);
+    if (rc) return set_err(c, rc, msg);
+    uint8_t* arena = static_cast<uint8_t*>(p->pages->p);
+    const size_t arena_len = p->pages->len;
+    PaintRun run;
+    int run_kind = -1;  // 0 area (fills and outlines), 1 hairlines
+    auto flush = [&]() -> int {
+        if (run.rule.empty()) return RRB_OK;
+        const rrb_path_batch_params q = run.params(p);
+        const uint8_t* rgb = path_rgb ? run.rgb.data() : nullptr;
+        const double* clip = clip_rects ? run.clip.data() : nullptr;
+        const int r = run_kind == 0 ? run_batch(c, &q, arena, arena_len, rgb, clip)
+                                    : run_hairlines(c, &q, arena, arena_len, rgb, clip);
+        run.clear();
+        return r;
+    };
+    for (uint64_t i = 0; i < p->n_paths; ++i) {
+        const uint8_t k = plan.kind[i];
+        if (k == rrb_stroke::NOTHING) continue;
+        const int want = k == rrb_stroke::HAIRLINE ? 1 : 0;
+        if (want != run_kind && (rc = flush())) return rc;
+        run_kind = want;
+        const uint32_t path = static_cast<uint32_t>(i);
+        if (k == rrb_stroke::FILL) {
+            const uint64_t a = p->path_pt_off[i], b = p->path_pt_off[i + 1];
+            run.add(p, path, p->pts + 2 * a, p->flags + a, b - a, p->fill_rule[i], path_rgb, clip_rects);
+        } else if (k == rrb_stroke::OUTLINE) {
+            const uint64_t a = plan.off[i], b = plan.off[i + 1];
+            run.add(p, path, plan.xy.data() + 2 * a, plan.fl.data() + a, b - a, 0, path_rgb, clip_rects);
+        } else {
+            // The hairline's segments, walked as XPath::new walks a path
+            // without curves and without closing (xpath.rs:162-260): from
+            // each FIRST point through the points up to the next LAST.
+            const double* xy = plan.xy.data() + 2 * plan.off[i];
+            const uint8_t* fl = plan.fl.data() + plan.off[i];
+            const uint64_t n = plan.off[i + 1] - plan.off[i];
+            static const uint8_t kSeg[2] = {RRB_PATH_FIRST, RRB_PATH_LAST};
+            uint64_t j = 0;
+            while (j < n) {
+                if (!(fl[j] & RRB_PATH_FIRST)) {
+                    ++j;
+                    continue;
+                }
+                uint64_t cur = j++;
+                while (j < n) {
+                    const double seg[4] = {xy[2 * cur], xy[2 * cur + 1], xy[2 * j], xy[2 * j + 1]};
+                    run.add(p, path, seg, kSeg, 2, 0, path_rgb, clip_rects);
+                    cur = j;
+                    const bool last = fl[j] & RRB_PATH_LAST;
+                    ++j;
+                    if (last) break;
+                }
+            }
+        }
+    }
+    return flush();
 }
 
 }  // namespace
@@ -1253,6 +1471,27 @@ int rrb_last_stage_times(rrb_ctx* c, rrb_stage_time* out, int cap, int* n) {
     }
     *n = m;
     return RRB_OK;
+}
+
+int rrb_record_stroke_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_params* stroke,
+                            const uint8_t* path_rgb, const double* clip_rects) {
+    if (!c || !p) return RRB_ERR_INVARIANT;
+    if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
+    if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
+    if (p->n_paths && !stroke) return set_err(c, RRB_ERR_INVARIANT, "stroke params array is null");
+    cudaSetDevice(c->device);
+    {
+        std::vector<PageGeom> geom;
+        uint64_t tiles = 0, supers = 0;
+        std::string m;
+        int v = validate_batch(p, p->pages->len, 64, 16, geom, tiles, supers, m, path_rgb ? 3 : 1);
+        if (v) return set_err(c, v, m);
+        if (clip_rects)
+            for (uint64_t k = 0; k < 4 * p->n_paths; ++k)
+                if (!std::isfinite(clip_rects[k])) return set_err(c, RRB_ERR_INVARIANT, "clip rectangles must be finite");
+    }
+    if (p->n_paths == 0) return RRB_OK;
+    return paint_batch(c, p, stroke, path_rgb, clip_rects);
 }
 
 int rrb_record_path_batch_ex(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb,

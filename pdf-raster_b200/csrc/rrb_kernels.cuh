@@ -40,6 +40,11 @@ struct __align__(16) PathInfo {
 };
 
 constexpr uint32_t PI_RECTI = 1u << 17;  // all edges horizontal or vertical, at most RECTI_MAX_EDGES
+// Spans drawn without a shape (hairline strokes): on Rgb8 pages they blend
+// with render_span's general arm c = div255((255 - a) * dst + a * src)
+// (pipe/general.rs:261-312) instead of the AA fast path; on Gray8 pages the
+// two agree (a_src = div255(a * 255) = a).
+constexpr uint32_t PI_SOLID = 1u << 19;
 constexpr uint32_t RECTI_MAX_EDGES = 32;
 
 // Error / status word bits shared by all kernels of a batch.
@@ -1326,6 +1331,16 @@ __device__ __forceinline__ uint32_t rgb_over(uint32_t d, uint32_t a, uint32_t s)
     return out;
 }
 
+// render_span's general arm on an Rgb8 page without alpha plane, per channel
+// div255((255 - a) * dst + a * src) (pipe/general.rs:261-312).
+__device__ __forceinline__ uint32_t rgb_over_div255(uint32_t d, uint32_t a, uint32_t s) {
+    uint32_t out = 0;
+#pragma unroll
+    for (int c = 0; c < 24; c += 8)
+        out |= div255((255u - a) * ((d >> c) & 0xffu) + a * ((s >> c) & 0xffu)) << c;
+    return out;
+}
+
 // a_src of the Rgb8 path: (a_input * shape + 255) >> 8.
 __device__ __forceinline__ uint32_t rgb_a_src(uint32_t alpha, uint32_t shape) { return (alpha * shape + 255u) >> 8; }
 
@@ -1398,7 +1413,8 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
             const uint32_t shape = gamma[min(cov[q], 16)];
             const int k = it * L::PX + q;
             if (RGB) {
-                pix[k] = rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
+                pix[k] = (h.paint & PI_SOLID) ? rgb_over_div255(pix[k], alpha, h.rgb)
+                                              : rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
             } else {
                 const uint32_t a_src = div255(alpha * shape);
                 pix[k] = div255((255u - a_src) * pix[k] + a_src * g);

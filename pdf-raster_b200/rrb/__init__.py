@@ -17,9 +17,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _abi
-from ._abi import (RRB_FILL_EVEN_ODD, RRB_FILL_NONZERO, RRB_ROWMAP_AS_SHIPPED,  # noqa: F401
+from ._abi import (RRB_CAP_BUTT, RRB_CAP_PROJECTING, RRB_CAP_ROUND, RRB_FILL_EVEN_ODD,  # noqa: F401
+                   RRB_FILL_NONZERO, RRB_JOIN_BEVEL, RRB_JOIN_MITER, RRB_JOIN_ROUND, RRB_ROWMAP_AS_SHIPPED,
                    RRB_ROWMAP_DOCUMENTED, BatchStats, PathBatchParams, PathFillParams, RequestResult, SceneParams,
-                   ServerConfig, ServerStats, StageTime, Tuning, VramBudget)
+                   ServerConfig, ServerStats, StageTime, StrokeParams, Tuning, VramBudget)
 
 __all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "Server", "lib",
            "conic_to_cubic", "RRB_FILL_NONZERO", "RRB_FILL_EVEN_ODD", "RRB_ROWMAP_DOCUMENTED",
@@ -391,6 +392,20 @@ class B200Backend:
                                                  None if rgb is None else _ptr(rgb, C.c_uint8),
                                                  None if clip is None else _ptr(clip, C.c_double)))
 
+    def record_stroke_batch(self, params: PathBatchParams, strokes, path_rgb: np.ndarray | None = None,
+                            clip_rects: np.ndarray | None = None):
+        """Paint the batch in path order: path p stroked with strokes[p] (a
+        dict: line_width, line_cap, line_join, miter_limit, dash, dash_phase)
+        or filled when strokes[p] is None. path_rgb / clip_rects as in
+        record_path_batch_ex."""
+        keep = []
+        sp = stroke_params(strokes, keep)
+        rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
+        clip = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
+        self._chk(lib().rrb_record_stroke_batch(self._h, C.byref(params), sp,
+                                                None if rgb is None else _ptr(rgb, C.c_uint8),
+                                                None if clip is None else _ptr(clip, C.c_double)))
+
     def record_rgb_to_gray(self, rgb: DeviceBuffer, gray: DeviceBuffer, n_px: int, rgb_offset: int = 0,
                            gray_offset: int = 0):
         self._chk(lib().rrb_record_rgb_to_gray(self._h, rgb.handle, rgb_offset, gray.handle, gray_offset, n_px))
@@ -555,6 +570,47 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def stroke_params(strokes, keep: list) -> "C.Array":
+    """StrokeParams array, one per path, from dicts (None: fill the path)."""
+    arr = (StrokeParams * max(1, len(strokes)))()
+    for i, d in enumerate(strokes):
+        if d is None:
+            continue
+        dash = np.ascontiguousarray(d.get("dash", ()), np.float64)
+        keep.append(dash)
+        arr[i].line_width = float(d["line_width"])
+        arr[i].miter_limit = float(d.get("miter_limit", 10.0))
+        arr[i].dash_phase = float(d.get("dash_phase", 0.0))
+        arr[i].dash = _ptr(dash, C.c_double) if dash.size else None
+        arr[i].n_dash = int(dash.size)
+        arr[i].line_cap = int(d.get("line_cap", RRB_CAP_BUTT))
+        arr[i].line_join = int(d.get("line_join", RRB_JOIN_MITER))
+        arr[i].stroke = 1
+    return arr
+
+
+def stroke_outline(pts, flags, flatness: float = 0.1, **stroke):
+    """What rrb_record_stroke_batch draws for one path (host): (kind, pts[n, 2],
+    flags[n]); kind 0 nothing, 1 an outline filled nonzero, 2 a hairline polyline."""
+    p = np.ascontiguousarray(np.reshape(pts, -1), np.float64)
+    f = np.ascontiguousarray(flags, np.uint8)
+    keep = []
+    sp = stroke_params([stroke], keep)
+    n, kind = C.c_uint64(), C.c_int()
+    rc = lib().rrb_stroke_outline(_ptr(p, C.c_double), _ptr(f, C.c_uint8), f.size, sp, flatness, None, None, 0,
+                                  C.byref(n), C.byref(kind))
+    if rc:
+        raise BackendError(rc, "rrb_stroke_outline")
+    xy = np.empty(2 * n.value, np.float64)
+    fl = np.empty(n.value, np.uint8)
+    if n.value:
+        rc = lib().rrb_stroke_outline(_ptr(p, C.c_double), _ptr(f, C.c_uint8), f.size, sp, flatness,
+                                      _ptr(xy, C.c_double), _ptr(fl, C.c_uint8), n.value, C.byref(n), C.byref(kind))
+        if rc:
+            raise BackendError(rc, "rrb_stroke_outline")
+    return kind.value, xy.reshape(-1, 2), fl
 
 
 def encode_netpbm(page: np.ndarray) -> bytes:

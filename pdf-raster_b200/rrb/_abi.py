@@ -137,6 +137,16 @@ class ServerCostModel(C.Structure):
                 ("y_mean", C.c_float), ("y_std", C.c_float), ("table", C.POINTER(C.c_int32)), ("policy", C.c_uint32)]
 
 
+RRB_CAP_BUTT, RRB_CAP_ROUND, RRB_CAP_PROJECTING = 0, 1, 2
+RRB_JOIN_MITER, RRB_JOIN_ROUND, RRB_JOIN_BEVEL = 0, 1, 2
+
+
+class StrokeParams(C.Structure):
+    _fields_ = [("line_width", C.c_double), ("miter_limit", C.c_double), ("dash_phase", C.c_double),
+                ("dash", C.POINTER(C.c_double)), ("n_dash", C.c_uint32), ("line_cap", C.c_uint8),
+                ("line_join", C.c_uint8), ("stroke", C.c_uint8), ("reserved", C.c_uint8)]
+
+
 class SceneParams(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32),
@@ -183,6 +193,12 @@ SIGNATURES = {
     "rrb_record_path_batch_ex": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8),
                                            C.POINTER(C.c_double)]),
     "rrb_record_path_batch_rgb": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8)]),
+    "rrb_record_stroke_batch": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(StrokeParams),
+                                          C.POINTER(C.c_uint8), C.POINTER(C.c_double)]),
+    "rrb_stroke_outline": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.c_uint64,
+                                     C.POINTER(StrokeParams), C.c_double, C.POINTER(C.c_double),
+                                     C.POINTER(C.c_uint8), C.c_uint64, C.POINTER(C.c_uint64),
+                                     C.POINTER(C.c_int)]),
     "rrb_record_rgb_to_gray": (C.c_int, [VP, VP, C.c_size_t, VP, C.c_size_t, C.c_uint64]),
     "rrb_record_aa_fill": (C.c_int, [VP, C.POINTER(AaFillParams)]),
     "rrb_aa_fill_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),

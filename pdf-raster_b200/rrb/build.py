@@ -21,13 +21,13 @@ CSRC = ROOT / "csrc"
 INCLUDE = ROOT.parent / "include"
 LIB = PKG_DIR / "librrb.so"
 
-SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "rrb_encode.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp"]
-DEPS = SOURCES + [CSRC / "rrb_kernels.cuh", CSRC / "rrb_device.cuh", INCLUDE / "rrb.h"]
+SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "rrb_encode.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp", CSRC / "rrb_stroke.cpp"]
+DEPS = SOURCES + [CSRC / "rrb_kernels.cuh", CSRC / "rrb_device.cuh", CSRC / "rrb_hairline.cuh", CSRC / "rrb_stroke.h", INCLUDE / "rrb.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC,-O3",
+    "-Xcompiler", "-fPIC,-O3,-ffp-contract=off",
     "-Xptxas", "-O3",
     "-shared",
 ]

@@ -60,6 +60,8 @@ STRUCTS = {
     "rrb_tile_record": ("TileRecord", ["key", "x_enter", "dxdy", "y0_tile", "y1_tile", "sign", "pad", "pad2"]),
     "rrb_tile_fill_params": ("TileFillParams", ["records", "tile_starts", "tile_counts", "coverage", "width",
                                                 "height", "fill_rule"]),
+    "rrb_stroke_params": ("StrokeParams", ["line_width", "miter_limit", "dash_phase", "dash", "n_dash", "line_cap",
+                                           "line_join", "stroke", "reserved"]),
     "rrb_scene_params": ("SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h", "page_scale",
                                          "paths_scale", "path_cap", "reserved"]),
 }
