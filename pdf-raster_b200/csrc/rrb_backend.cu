@@ -879,6 +879,10 @@ int run_hairlines(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, si
     const uint32_t NS = static_cast<uint32_t>(B->n_paths), n_pages = B->n_pages;
     const uint64_t supers = B->supers;
     const int rowmap = B->rowmap;
+    if (rowmap)
+        for (const PageGeom& G : B->geom_h)
+            if (G.h > (1u << 26))
+                return set_err(c, RRB_ERR_INVARIANT, "hairlines under the as-shipped row map need pages <= 2^26 rows");
     RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
                                 c->stream));
     const double* clipd = nullptr;
@@ -898,12 +902,14 @@ int run_hairlines(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, si
     k_hl_count<<<grid_for(c, NS, 128, 16), 128, 0, c->stream>>>(
         as<double>(B->pts), as<double>(B->mtx), as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph),
         clipd, as<uint8_t>(B->gray), as<uint8_t>(B->alpha), NS, rowmap, as<PathInfo>(c->s_info),
-        as<uint32_t>(c->s_run_off));
+        as<uint32_t>(c->s_run_off), as<BatchCounters>(c->s_ctr));
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
+    if ((rc = read_back(c, &as<BatchCounters>(c->s_ctr)->raw_entries, sizeof(uint64_t)))) return rc;
+    uint64_t n_runs;
+    std::memcpy(&n_runs, c->h_read, sizeof n_runs);
+    if (n_runs > 0x7FFFFFFFull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "hairlines cross more than 2^31 pixel rows");
     if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NS))) return rc;
-    if ((rc = read_back(c, as<uint32_t>(c->s_run_off) + NS, sizeof(uint32_t)))) return rc;
-    const uint64_t n_runs = c->h_read[0];
     if ((rc = ensure(c, c->s_runs, std::max<uint64_t>(1, n_runs) * sizeof(int4)))) return rc;
     if ((rc = ensure(c, c->s_spans, std::max<uint64_t>(1, n_runs) * sizeof(uint32_t)))) return rc;
     k_hl_write<<<grid_for(c, NS * 32ull, 256, 8), 256, 0, c->stream>>>(

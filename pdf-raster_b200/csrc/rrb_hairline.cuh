@@ -162,10 +162,12 @@ __global__ void k_hl_count(const double* __restrict__ pts, const double* __restr
                            const uint32_t* __restrict__ seg_page, const uint32_t* __restrict__ page_w,
                            const uint32_t* __restrict__ page_h, const double* __restrict__ clip_rect,
                            const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha, uint32_t n_segs,
-                           int rowmap, PathInfo* __restrict__ info, uint32_t* __restrict__ rows) {
+                           int rowmap, PathInfo* __restrict__ info, uint32_t* __restrict__ rows,
+                           BatchCounters* __restrict__ ctr) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
+    unsigned long long total = 0;
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_segs; s += gridDim.x * blockDim.x) {
         const uint32_t pg = seg_page[s], W = page_w[pg], H = page_h[pg];
         const HlClip clip = hl_clip(W, H, clip_rect ? clip_rect + 4 * s : nullptr);
@@ -194,7 +196,13 @@ __global__ void k_hl_count(const double* __restrict__ pts, const double* __restr
         }
         info[s] = P;
         rows[s] = n;
+        total += n;
     }
+    // The 64-bit total, so the host can refuse a batch whose run count would
+    // overflow the 32-bit offsets before any run is written. Every lane of
+    // every warp reaches this point (blocks are whole warps).
+    for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    if ((threadIdx.x & 31) == 0 && total) atomicAdd(&ctr->raw_entries, total);
 }
 
 // Pass 2, warp per segment: run r = (group, group, cell r, 0 or 1 cells) and
