@@ -474,6 +474,118 @@ def run_rrb(args, rank, local, world):
         dist.destroy_process_group()
 
 
+def run_strokes(args, rank, local, world):
+    """Stroke-heavy page through rrb_record_stroke_batch: host outlines (every
+    cap, join and dash), hairline spans and fills, all composited on the
+    device. A step is one whole call: the host stroker, the upload of the
+    outlines and the device render."""
+    import torch
+
+    import rrb
+    from rrb.strokes import StrokePage
+
+    if world > 1:
+        torch.cuda.set_device(local)
+    page = StrokePage(0, n_paths=args.paths or 20000)
+    backend = rrb.B200Backend(local)
+    pages = backend.alloc_device(page.arena_bytes)
+    keep = []
+    params = rrb.batch_params(page.pts, page.flags, page.path_pt_off, page.fill_rule, page.gray, page.alpha,
+                              page.path_page, page.page_width, page.page_height, page.page_offset, pages, keep=keep)
+    stream = torch.cuda.ExternalStream(backend.stream, device=torch.device("cuda", local))
+
+    def step():
+        backend.begin_page()
+        backend.record_fill_buffer(pages, 255)
+        backend.record_stroke_batch(params, page.strokes)
+        backend.wait_page(backend.submit_page())
+
+    for _ in range(args.warmup):
+        step()
+    backend.set_profiling(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    stage_acc, launches = {}, 0
+    clocks = Clocks(local)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    ev[0].record(stream)
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record(stream)
+        launches += backend.last_batch_stats()["kernel_launches"]
+        for name, (ms, nl) in backend.stage_times().items():
+            a = stage_acc.setdefault(name, [0.0, 0])
+            a[0] += ms
+            a[1] += nl
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    backend.set_profiling(False)
+    total_ms = ev[0].elapsed_time(ev[-1])
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    stats = backend.last_batch_stats()
+    stage_ms = {k: v[0] / args.steps for k, v in stage_acc.items()}
+    device_ms = sum(stage_ms.values())
+    value = page.pixels * world * args.steps / (total_ms / 1e3) / 1e6
+    # End to end: the page arena from pinned host memory and back each step.
+    host_page = pinned_copy(backend, page.blank_arena(), keep)
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    t = time.perf_counter()
+    for _ in range(e2e_steps):
+        backend.begin_page()
+        backend.upload_async(pages, host_page)
+        backend.record_stroke_batch(params, page.strokes)
+        backend.wait_page(backend.submit_page())
+        backend.wait_download(backend.download_async(pages, host_page))
+    e2e_s = time.perf_counter() - t
+    e2e = {"value": page.pixels * world * e2e_steps / e2e_s / 1e6, "unit": "Mpixel/s",
+           "h2d_bytes_per_step": int(page.pts.nbytes + page.flags.nbytes + page.path_pt_off.nbytes + 3 * page.n_paths
+                                     + host_page.nbytes),
+           "d2h_bytes_per_step": int(host_page.nbytes), "steps": e2e_steps,
+           "api": "rrb_record_stroke_batch (C ABI) with the page uploaded from and read back to pinned host memory"}
+    got = np.empty(page.arena_bytes, np.uint8)
+    backend.wait_download(backend.download_async(pages, got))
+    cpu = bit_exact = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import rr_oracle
+        rr_oracle.build()
+        ref = page.blank_arena()
+        t0 = time.perf_counter()
+        ost = rr_oracle.render_scene_paint(page, ref, page.strokes)
+        secs = time.perf_counter() - t0
+        bit_exact = bool(np.array_equal(ref, got) and np.array_equal(ref, np.asarray(host_page)))
+        cpu = {"value": page.pixels / secs / 1e6, "unit": "Mpixel/s", "cores": 1, "kind": "port",
+               "sample": "the whole page (all paths), 1 host thread, C++ restatement of the reference's stroke() "
+                         "and fill path", "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"]}
+    peak, peak_kind = measured_peak()
+    dom = max(stage_ms, key=stage_ms.get) if stage_ms else None
+    roofline = None
+    alg = {"composite": 2 * page.pixels + 4 * stats["spans"] + 8 * stats["aa_rows"],
+           "rows": 32 * stats["segments"] + 8 * stats["aa_rows"] + 4 * stats["spans"]}
+    if dom in alg:
+        waves = max(1, int(stats.get("waves", 1)))
+        dur = stage_ms[dom] / waves / 1e3
+        ach = alg[dom] / waves / dur / 1e9
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": None, "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg[dom] / waves,
+                    "launch_ms": dur * 1e3}
+    backend.free_device(pages)
+    backend.close()
+    if rank == 0:
+        p50, p99 = (float(np.percentile(step_ms, q)) for q in (50, 99))
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded stroke page, seed 0; no public dataset for this path)",
+            "config": {"workload": page.description, "paths": page.n_paths, "pages": 1, "rowmap": "documented",
+                       "l2": "outlines and edge records larger than L2",
+                       "parallelism": f"replicas x{world} (the page on every GPU)"},
+            "device_ms_per_step": device_ms, "outline_segments_per_step": stats["segments"],
+            "p50_page_ms": p50, "p99_page_ms": p99, "bit_exact": bit_exact, "roofline": roofline,
+            "stages_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }), flush=True)
+
+
 def run_fill_ops(args, rank, world):
     """The reference's coverage operators (record_aa_fill / record_tile_fill)
     on the reference's own benchmark shapes (threshold_bench: a w x h square
@@ -649,7 +761,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["rrb", "reference"], default="rrb")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fill_ops"], default="glyphs")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fill_ops", "strokes"], default="glyphs")
     ap.add_argument("--rowmap", type=int, default=0)
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -668,6 +780,8 @@ def main():
         run_serving(args, rank, world)
     elif args.workload == "fill_ops":
         run_fill_ops(args, rank, world)
+    elif args.workload == "strokes":
+        run_strokes(args, rank, local, world)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     else:

@@ -210,7 +210,8 @@ int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info,
 // crates/gpu/src/backend/params.rs:57,334), plus the page geometry the
 // kernels need. No device access.
 int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw, uint32_t th,
-                   std::vector<PageGeom>& geom, uint64_t& tiles, uint64_t& supers, std::string& msg, uint32_t bpp = 1) {
+                   std::vector<PageGeom>& geom, uint64_t& tiles, uint64_t& supers, std::string& msg, uint32_t bpp = 1,
+                   uint8_t max_rule = 1) {
     const uint64_t n_paths = h->n_paths, n_pts = h->n_pts;
     const uint32_t n_pages = h->n_pages;
     tiles = supers = 0;
@@ -252,7 +253,7 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
         uint32_t pg = h->path_page[p];
         if (pg >= n_pages || pg < prev)
             return msg = "path_page must be < n_pages and non-decreasing", RRB_ERR_INVARIANT;
-        if (h->fill_rule[p] > 1) return msg = "fill_rule must be 0 or 1", RRB_ERR_INVARIANT;
+        if (h->fill_rule[p] > max_rule) return msg = "fill_rule must be 0 or 1", RRB_ERR_INVARIANT;
         prev = pg;
     }
     uint64_t p = 0, work = 0;
@@ -290,7 +291,9 @@ struct rrb_batch {
     Scratch rgb;                    // Rgb8 pages: per-path colour r | g << 8 | b << 16
     uint32_t bpp = 1;               // page bytes per pixel: 1 Gray8, 3 Rgb8
     Scratch clip;                   // per-path clip in AA units (int4), when has_clip
+    Scratch clipf;                  // the clip rectangles as given (4 doubles per path), when has_clip
     bool has_clip = false;
+    bool has_hairline = false;      // some paths are hairline segments (RULE_HAIRLINE)
     // Page groups [plan[i], plan[i+1]) that rendered without running out of
     // scratch or cell capacity last time (with plan_wave_points); reused so a
     // resident batch does not fail and split on every render.
@@ -344,7 +347,7 @@ void stage_end(rrb_ctx* c, int k) {
 
 void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
-                      &B->mtx, &B->rgb, &B->clip};
+                      &B->mtx, &B->rgb, &B->clip, &B->clipf};
     for (Scratch* s : all) {
         if (B->view && s != &B->off && s != &B->page && s != &B->geom) {
             s->p = nullptr;
@@ -360,11 +363,12 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
 // Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages;
 // clip (host, 4 doubles per path) clips each path to a device-space rectangle.
 int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr,
-                 const double* clip = nullptr) {
+                 const double* clip = nullptr, bool hairlines = false) {
     std::string msg;
     uint64_t tiles = 0;
     B->bpp = rgb ? 3 : 1;
-    int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg, B->bpp);
+    int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg, B->bpp,
+                           hairlines ? RULE_HAIRLINE : 1);
     if (v) return set_err(c, v, msg);
     B->n_paths = h->n_paths;
     B->n_pts = h->n_pts;
@@ -375,6 +379,9 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     for (const PageGeom& G : B->geom_h)
         B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(B->bpp) * G.w * G.h);
     B->plan.clear();
+    B->has_hairline = false;
+    if (hairlines)
+        for (uint64_t p = 0; p < h->n_paths && !B->has_hairline; ++p) B->has_hairline = h->fill_rule[p] == RULE_HAIRLINE;
     B->page_pt.assign(B->n_pages + 1, 0);
     for (uint32_t pg = 0; pg < B->n_pages; ++pg) B->page_pt[pg] = h->path_pt_off[B->geom_h[pg].path_begin];
     B->page_pt[B->n_pages] = h->n_paths ? h->path_pt_off[h->n_paths] : 0;
@@ -412,6 +419,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
             if (ci[p].z > ci[p].w + 1) ci[p].w = ci[p].z - 1;  // empty row range
         }
         if ((rc = upload(c, B->clip, ci.data(), ci.size()))) return rc;
+        if ((rc = upload(c, B->clipf, clip, 4 * h->n_paths))) return rc;
         RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     if (rgb) {
@@ -458,7 +466,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     k_walk<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
                                                              as<uint64_t>(B->off), NP, as<double>(B->mtx),
                                                              as<uint32_t>(B->page), as<uint32_t>(B->ph),
-                                                             as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces));
+                                                             as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces),
+                                                             B->has_hairline ? as<uint8_t>(B->rule) : nullptr);
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
     if ((rc = scan_u32(c, as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_path_pieces), NP))) return rc;
@@ -515,6 +524,18 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
         chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax, pclip);
     c->launches += 1;
+    // Hairline segments: their layers' PathInfo and run counts (before the
+    // binning, which reads the layers' rectangles).
+    if ((rc = ensure(c, c->s_run_off, (n_paths + 1) * sizeof(uint32_t)))) return rc;
+    const double* hl_clip = B->has_clip ? as<double>(B->clipf) : nullptr;
+    if (B->has_hairline) {
+        k_hl_count<<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
+            as<double>(B->pts), as<uint64_t>(B->off), as<uint8_t>(B->rule), as<double>(B->mtx),
+            as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph), hl_clip, as<uint8_t>(B->gray),
+            as<uint8_t>(B->alpha), NP, rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_run_off),
+            as<BatchCounters>(c->s_ctr));
+        c->launches += 1;
+    }
     stage_end(c, 4);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 5);
@@ -532,7 +553,6 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage(c, 7);
     if ((rc = scan_u32(c, as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_cnt), NSUP))) return rc;
     // Rectilinear paths: runs per path, then their offsets.
-    if ((rc = ensure(c, c->s_run_off, (n_paths + 1) * sizeof(uint32_t)))) return rc;
     k_recti<false><<<grid_for(c, n_paths, 128, 16), 128, 0, c->stream>>>(
         as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, as<uint32_t>(c->s_run_off),
         nullptr, nullptr, nullptr, 0, as<BatchCounters>(c->s_ctr), pclip);
@@ -548,16 +568,22 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                 c->stream));
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 6, as<uint32_t>(c->s_run_off) + NP, 4, cudaMemcpyDeviceToHost,
                                 c->stream));
+    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 8, &as<BatchCounters>(c->s_ctr)->hl_rows, 8, cudaMemcpyDeviceToHost,
+                                c->stream));
     RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     const uint64_t n_groups = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
     const uint64_t n_runs = c->h_read[6];
-    uint64_t raw_entries;
+    uint64_t raw_entries, hl_rows;
     std::memcpy(&raw_entries, c->h_read + 4, 8);
+    std::memcpy(&hl_rows, c->h_read + 8, 8);
+    // The run offsets were scanned in 32 bits: refuse totals that could wrap.
+    if (hl_rows > 0x7FFFFFFFull || n_runs > 0x7FFFFFFFull)
+        return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^31 row runs");
     // ---- stage 3: rows -> coverage cells. An AA row with m merged entries
     // yields at most m/2 + 1 spans, and a pixel row at most 2 cells per span
     // boundary: cells <= 4 * spans <= 2 * raw entries + 4 * AA rows.
     const uint64_t aa_rows = 4 * n_groups;
-    uint64_t cell_cap = 2 * raw_entries + 4 * aa_rows + 1024;
+    uint64_t cell_cap = 2 * raw_entries + 4 * aa_rows + hl_rows + 1024;
     if (cell_cap > 0xFFFFFF00ull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^32 cells");
     if (n_groups > 0x3FFFFFFFull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^30 pixel rows");
     if ((rc = ensure(c, c->s_row_idx, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
@@ -590,6 +616,14 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
             as<PathInfo>(c->s_info), NP, as<Edge>(c->s_edges), as<uint32_t>(B->pw), rowmap, nullptr,
             as<uint32_t>(c->s_run_off), as<int4>(c->s_runs), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
             as<BatchCounters>(c->s_ctr), pclip);
+        c->launches += 1;
+    }
+    if (B->has_hairline && hl_rows) {
+        k_hl_write<<<grid_for(c, n_paths * 32, 256, 8), 256, 0, c->stream>>>(
+            as<double>(B->pts), as<uint64_t>(B->off), as<uint8_t>(B->rule), as<double>(B->mtx),
+            as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph), hl_clip, NP, rowmap,
+            as<uint32_t>(c->s_run_off), as<PathInfo>(c->s_info), as<int4>(c->s_runs), as<uint32_t>(c->s_spans),
+            static_cast<uint32_t>(cell_cap), as<BatchCounters>(c->s_ctr));
         c->launches += 1;
     }
     stage_end(c, 9);
@@ -739,7 +773,9 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     W->bpp = B->bpp;
     if (B->bpp == 3) view(W->rgb, B->rgb, pb * sizeof(uint32_t));
     W->has_clip = B->has_clip;
+    W->has_hairline = B->has_hairline;
     if (B->has_clip) view(W->clip, B->clip, pb * sizeof(int4));
+    if (B->has_clip) view(W->clipf, B->clipf, pb * 4 * sizeof(double));
     int rc;
     if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
     if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
@@ -852,111 +888,16 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
 }
 
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
-              const uint8_t* rgb = nullptr, const double* clip = nullptr) {
+              const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false) {
     rrb_batch* B = c->tmp_batch;
-    int rc = batch_upload(c, h, B, rgb, clip);
+    int rc = batch_upload(c, h, B, rgb, clip, hairlines);
     if (rc) return rc;
     return run_resident(c, B, arena, arena_len, h->rowmap);
 }
 
-// Hairline segments (two-point paths of h, one layer each; see
-// rrb_hairline.cuh) into the device pages: spans per pixel row, then the
-// binning and the tile compositor of fills. clip: host doubles, 4 per segment.
-int run_hairlines(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len, const uint8_t* rgb,
-                  const double* clip) {
-    rrb_batch* B = c->tmp_batch;
-    int rc = batch_upload(c, h, B, rgb, clip);
-    if (rc) return rc;
-    c->launches = 0;
-    std::memset(&c->stats, 0, sizeof c->stats);
-    if (B->n_paths == 0) return RRB_OK;
-    if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
-    const uint32_t tw = c->tuning.tile_w ? c->tuning.tile_w : 64;
-    const uint32_t th = c->tuning.tile_h ? c->tuning.tile_h : 16;
-    uint64_t tiles = 0;
-    set_tiles(B->geom_h, tw, th, tiles);
-    if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
-    const uint32_t NS = static_cast<uint32_t>(B->n_paths), n_pages = B->n_pages;
-    const uint64_t supers = B->supers;
-    const int rowmap = B->rowmap;
-    if (rowmap)
-        for (const PageGeom& G : B->geom_h)
-            if (G.h > (1u << 26))
-                return set_err(c, RRB_ERR_INVARIANT, "hairlines under the as-shipped row map need pages <= 2^26 rows");
-    RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
-                                c->stream));
-    const double* clipd = nullptr;
-    if (clip) {
-        if ((rc = upload(c, c->s_hl_clip, clip, 4 * static_cast<size_t>(NS)))) return rc;
-        clipd = as<double>(c->s_hl_clip);
-    }
-    if ((rc = ensure(c, c->s_info, NS * sizeof(PathInfo)))) return rc;
-    if ((rc = ensure(c, c->s_run_off, (NS + 1ull) * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_rows, (NS + 1ull) * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_row_idx, sizeof(uint2)))) return rc;
-    if ((rc = ensure(c, c->s_block, (SCAN_MAX_BLOCKS + 1) * sizeof(uint32_t)))) return rc;
-    if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
-    if ((rc = ensure(c, c->s_super_cnt, (supers + 1) * sizeof(uint32_t)))) return rc;
-    RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
-    RRB_CUDA(c, cudaMemsetAsync(c->s_rows.p, 0, (NS + 1ull) * sizeof(uint32_t), c->stream));
-    k_hl_count<<<grid_for(c, NS, 128, 16), 128, 0, c->stream>>>(
-        as<double>(B->pts), as<double>(B->mtx), as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph),
-        clipd, as<uint8_t>(B->gray), as<uint8_t>(B->alpha), NS, rowmap, as<PathInfo>(c->s_info),
-        as<uint32_t>(c->s_run_off), as<BatchCounters>(c->s_ctr));
-    c->launches += 1;
-    RRB_CUDA(c, cudaGetLastError());
-    if ((rc = read_back(c, &as<BatchCounters>(c->s_ctr)->raw_entries, sizeof(uint64_t)))) return rc;
-    uint64_t n_runs;
-    std::memcpy(&n_runs, c->h_read, sizeof n_runs);
-    if (n_runs > 0x7FFFFFFFull) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "hairlines cross more than 2^31 pixel rows");
-    if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NS))) return rc;
-    if ((rc = ensure(c, c->s_runs, std::max<uint64_t>(1, n_runs) * sizeof(int4)))) return rc;
-    if ((rc = ensure(c, c->s_spans, std::max<uint64_t>(1, n_runs) * sizeof(uint32_t)))) return rc;
-    k_hl_write<<<grid_for(c, NS * 32ull, 256, 8), 256, 0, c->stream>>>(
-        as<double>(B->pts), as<double>(B->mtx), as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph),
-        clipd, NS, rowmap, as<uint32_t>(c->s_run_off), as<PathInfo>(c->s_info), as<int4>(c->s_runs),
-        as<uint32_t>(c->s_spans));
-    c->launches += 1;
-    RRB_CUDA(c, cudaGetLastError());
-    // Binning and the compositor, as for fills.
-    const uint32_t NSUP = static_cast<uint32_t>(supers);
-    k_super_bin<false><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
-        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, as<uint32_t>(c->s_super_cnt),
-        nullptr, nullptr);
-    c->launches += 1;
-    RRB_CUDA(c, cudaGetLastError());
-    if ((rc = scan_u32(c, as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_cnt), NSUP))) return rc;
-    if ((rc = read_back(c, as<uint32_t>(c->s_super_cnt) + NSUP, sizeof(uint32_t)))) return rc;
-    const uint64_t n_pairs = c->h_read[0];
-    if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
-    k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
-        as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, nullptr,
-        as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list));
-    c->launches += 1;
-    RRB_CUDA(c, cudaGetLastError());
-    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 8),
-                               as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
-                               as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
-                               as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
-                               rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr)))
-        return rc;
-    if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
-    BatchCounters hc;
-    std::memcpy(&hc, c->h_read, sizeof hc);
-    c->stats.paths = NS;
-    c->stats.segments = NS;
-    c->stats.spans = n_runs;
-    c->stats.tiles = tiles;
-    c->stats.tile_pairs = n_pairs;
-    c->stats.kernel_launches = c->launches;
-    c->stats.waves = 1;
-    if (hc.err) return set_err(c, RRB_ERR_POOL_EXHAUSTED, "hairline batch capacity exceeded");
-    return RRB_OK;
-}
-
-// One run of consecutive paths of a paint batch that draw the same way
-// (fills and stroke outlines, or hairlines), as a batch of its own over the
-// pages the run touches.
+// The batch a paint batch renders as: fills, stroke outlines and hairline
+// segments (RULE_HAIRLINE two-point paths) in path order, over the pages that
+// have any.
 struct PaintRun {
     std::vector<double> pts, clip;
     std::vector<uint8_t> flags, rule, gray, alpha, rgb;
@@ -964,21 +905,6 @@ struct PaintRun {
     std::vector<uint32_t> page, pw, ph;
     uint32_t last_page = UINT32_MAX;
 
-    void clear() {
-        pts.clear();
-        clip.clear();
-        flags.clear();
-        rule.clear();
-        gray.clear();
-        alpha.clear();
-        rgb.clear();
-        off.assign(1, 0);
-        page_off.clear();
-        page.clear();
-        pw.clear();
-        ph.clear();
-        last_page = UINT32_MAX;
-    }
     // A path of the run: its points, paint and page (pages of the input batch
     // are renumbered in order of first use).
     void add(const rrb_path_batch_params* p, uint32_t path, const double* xy, const uint8_t* fl, uint64_t n,
@@ -1025,26 +951,10 @@ int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_par
     rrb_stroke::Plan plan;
     int rc = rrb_stroke::plan(p, sp, plan, msg);
     if (rc) return set_err(c, rc, msg);
-    uint8_t* arena = static_cast<uint8_t*>(p->pages->p);
-    const size_t arena_len = p->pages->len;
     PaintRun run;
-    int run_kind = -1;  // 0 area (fills and outlines), 1 hairlines
-    auto flush = [&]() -> int {
-        if (run.rule.empty()) return RRB_OK;
-        const rrb_path_batch_params q = run.params(p);
-        const uint8_t* rgb = path_rgb ? run.rgb.data() : nullptr;
-        const double* clip = clip_rects ? run.clip.data() : nullptr;
-        const int r = run_kind == 0 ? run_batch(c, &q, arena, arena_len, rgb, clip)
-                                    : run_hairlines(c, &q, arena, arena_len, rgb, clip);
-        run.clear();
-        return r;
-    };
     for (uint64_t i = 0; i < p->n_paths; ++i) {
         const uint8_t k = plan.kind[i];
         if (k == rrb_stroke::NOTHING) continue;
-        const int want = k == rrb_stroke::HAIRLINE ? 1 : 0;
-        if (want != run_kind && (rc = flush())) return rc;
-        run_kind = want;
         const uint32_t path = static_cast<uint32_t>(i);
         if (k == rrb_stroke::FILL) {
             const uint64_t a = p->path_pt_off[i], b = p->path_pt_off[i + 1];
@@ -1069,7 +979,7 @@ int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_par
                 uint64_t cur = j++;
                 while (j < n) {
                     const double seg[4] = {xy[2 * cur], xy[2 * cur + 1], xy[2 * j], xy[2 * j + 1]};
-                    run.add(p, path, seg, kSeg, 2, 0, path_rgb, clip_rects);
+                    run.add(p, path, seg, kSeg, 2, RULE_HAIRLINE, path_rgb, clip_rects);
                     cur = j;
                     const bool last = fl[j] & RRB_PATH_LAST;
                     ++j;
@@ -1078,7 +988,12 @@ int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_par
             }
         }
     }
-    return flush();
+    if (run.rule.empty()) return RRB_OK;
+    if (run.rule.size() >= (1ull << 31) || run.flags.size() >= (1ull << 30))
+        return set_err(c, RRB_ERR_POOL_EXHAUSTED, "painted geometry exceeds 2^30 points or 2^31 paths");
+    const rrb_path_batch_params q = run.params(p);
+    return run_batch(c, &q, static_cast<uint8_t*>(p->pages->p), p->pages->len, path_rgb ? run.rgb.data() : nullptr,
+                     clip_rects ? run.clip.data() : nullptr, true);
 }
 
 }  // namespace

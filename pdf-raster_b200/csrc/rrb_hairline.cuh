@@ -10,8 +10,10 @@
 // its pixel rows, each with one coverage-16 cell, composited in segment order
 // by the same tile compositor as fills (k_super_bin + k_composite).
 //
-// Segments arrive as two-point paths (the host walks the flattened and dashed
-// polyline as XPath::new with close_subpaths = false does, xpath.rs:162-260).
+// Segments arrive as two-point paths of the batch with the internal fill rule
+// RULE_HAIRLINE (the host walks the flattened and dashed polyline as
+// XPath::new with close_subpaths = false does, xpath.rs:162-260), so they
+// interleave with fills and stroke outlines in one render, in path order.
 #pragma once
 
 #include "rrb_kernels.cuh"
@@ -53,13 +55,13 @@ struct HlSeg {
     bool flat, inside, ltr;
 };
 
-__device__ __forceinline__ HlSeg hl_segment(const double* __restrict__ pts, const double* __restrict__ m, uint32_t s,
+__device__ __forceinline__ HlSeg hl_segment(const double* __restrict__ pts, const double* __restrict__ m, uint64_t pt,
                                             uint32_t W, uint32_t H, const HlClip& clip) {
     HlSeg g{};
     // add_segment (xpath.rs:324-402) on the transformed endpoints.
     double ax, ay, bx, by;
-    transform(m, pts[4 * s], pts[4 * s + 1], ax, ay);
-    transform(m, pts[4 * s + 2], pts[4 * s + 3], bx, by);
+    transform(m, pts[2 * pt], pts[2 * pt + 1], ax, ay);
+    transform(m, pts[2 * pt + 2], pts[2 * pt + 3], bx, by);
     double x0 = ax, y0 = ay, x1 = bx, y1 = by, dxdy = 0.0;
     if (__double_as_longlong(ay) != __double_as_longlong(by)) {
         const bool vert = __double_as_longlong(ax) == __double_as_longlong(bx);
@@ -156,22 +158,27 @@ __device__ __forceinline__ int2 hl_row_span(const HlSeg& g, int32_t y, uint32_t 
     return make_int2(max(a, clip.x_min_i), min(b, clip.x_max_i));
 }
 
-// Pass 1, thread per segment: rows drawn (one run each) and the layer's
-// PathInfo except its columns.
-__global__ void k_hl_count(const double* __restrict__ pts, const double* __restrict__ mtx,
-                           const uint32_t* __restrict__ seg_page, const uint32_t* __restrict__ page_w,
+// Pass 1, thread per path; hairline segments only (rule RULE_HAIRLINE): the
+// rows drawn (one run each) into run_count, and the layer's PathInfo. Its
+// columns are a bound here (the end columns +-2, in the clip): every span lies
+// between the floors of the segment's x at its rows, which differ from the
+// end columns by at most one; k_hl_write narrows them to the spans.
+__global__ void k_hl_count(const double* __restrict__ pts, const uint64_t* __restrict__ path_pt_off,
+                           const uint8_t* __restrict__ rule, const double* __restrict__ mtx,
+                           const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
                            const uint32_t* __restrict__ page_h, const double* __restrict__ clip_rect,
-                           const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha, uint32_t n_segs,
-                           int rowmap, PathInfo* __restrict__ info, uint32_t* __restrict__ rows,
+                           const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha, uint32_t n_paths,
+                           int rowmap, PathInfo* __restrict__ info, uint32_t* __restrict__ run_count,
                            BatchCounters* __restrict__ ctr) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
     unsigned long long total = 0;
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_segs; s += gridDim.x * blockDim.x) {
-        const uint32_t pg = seg_page[s], W = page_w[pg], H = page_h[pg];
-        const HlClip clip = hl_clip(W, H, clip_rect ? clip_rect + 4 * s : nullptr);
-        const HlSeg g = hl_segment(pts, m, s, W, H, clip);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+        if (rule[p] != RULE_HAIRLINE) continue;
+        const uint32_t pg = path_page[p], W = page_w[pg], H = page_h[pg];
+        const HlClip clip = hl_clip(W, H, clip_rect ? clip_rect + 4 * p : nullptr);
+        const HlSeg g = hl_segment(pts, m, path_pt_off[p], W, H, clip);
         PathInfo P{};
         P.px0 = 1;
         P.px1 = 0;
@@ -179,7 +186,7 @@ __global__ void k_hl_count(const double* __restrict__ pts, const double* __restr
         P.bx1 = P.by1 = 0;
         P.e_begin = P.e_end = 0;
         P.page = pg;
-        P.paint = static_cast<uint32_t>(gray[s]) | (static_cast<uint32_t>(alpha[s]) << 8) | PI_RECTI | PI_SOLID;
+        P.paint = static_cast<uint32_t>(gray[p]) | (static_cast<uint32_t>(alpha[p]) << 8) | PI_RECTI | PI_SOLID;
         uint32_t n = 0;
         if (g.r0 <= g.r1) {
             n = static_cast<uint32_t>(g.r1 - g.r0 + 1);
@@ -190,51 +197,64 @@ __global__ void k_hl_count(const double* __restrict__ pts, const double* __restr
             const int32_t g0 = rowmap ? 4 * g.r0 + 3 : g.r0, g1 = rowmap ? 4 * g.r1 + 3 : g.r1;
             P.y0 = 4 * g0;
             P.y1 = 4 * g1 + 3;
+            const int32_t lo = g.inside ? 0 : clip.x_min_i, hi = g.inside ? static_cast<int32_t>(W) - 1 : clip.x_max_i;
+            const int64_t a = static_cast<int64_t>(min(g.cx0, g.cx1)) - 2, b = static_cast<int64_t>(max(g.cx0, g.cx1)) + 2;
+            P.px0 = static_cast<int32_t>(a > lo ? a : lo);
+            P.px1 = static_cast<int32_t>(b < hi ? b : hi);
         } else {
             P.py0 = P.y0 = 1;
             P.py1 = P.y1 = 0;
         }
-        info[s] = P;
-        rows[s] = n;
+        info[p] = P;
+        run_count[p] = n;
         total += n;
     }
     // The 64-bit total, so the host can refuse a batch whose run count would
     // overflow the 32-bit offsets before any run is written. Every lane of
     // every warp reaches this point (blocks are whole warps).
     for (int o = 16; o; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
-    if ((threadIdx.x & 31) == 0 && total) atomicAdd(&ctr->raw_entries, total);
+    if ((threadIdx.x & 31) == 0 && total) atomicAdd(&ctr->hl_rows, total);
 }
 
-// Pass 2, warp per segment: run r = (group, group, cell r, 0 or 1 cells) and
-// cell r = the row's span at coverage 16; the layer's columns.
-__global__ void k_hl_write(const double* __restrict__ pts, const double* __restrict__ mtx,
-                           const uint32_t* __restrict__ seg_page, const uint32_t* __restrict__ page_w,
+// Pass 2, warp per path; hairline segments only: run r of the layer =
+// (group, group, its cell, 0 or 1 cells), the cell = the row's span at
+// coverage 16 (cells taken from the batch's cell cursor), and the layer's
+// columns narrowed to its spans.
+__global__ void k_hl_write(const double* __restrict__ pts, const uint64_t* __restrict__ path_pt_off,
+                           const uint8_t* __restrict__ rule, const double* __restrict__ mtx,
+                           const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
                            const uint32_t* __restrict__ page_h, const double* __restrict__ clip_rect,
-                           uint32_t n_segs, int rowmap, const uint32_t* __restrict__ run_off,
-                           PathInfo* __restrict__ info, int4* __restrict__ runs, uint32_t* __restrict__ cells) {
+                           uint32_t n_paths, int rowmap, const uint32_t* __restrict__ run_off,
+                           PathInfo* __restrict__ info, int4* __restrict__ runs, uint32_t* __restrict__ cells,
+                           uint32_t cell_cap, BatchCounters* __restrict__ ctr) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < n_segs; s += warps) {
-        const uint32_t pg = seg_page[s], W = page_w[pg], H = page_h[pg];
-        const HlClip clip = hl_clip(W, H, clip_rect ? clip_rect + 4 * s : nullptr);
-        const HlSeg g = hl_segment(pts, m, s, W, H, clip);
-        const uint32_t base = run_off[s];
+    for (uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < n_paths; p += warps) {
+        if (rule[p] != RULE_HAIRLINE) continue;
+        const uint32_t pg = path_page[p], W = page_w[pg], H = page_h[pg];
+        const HlClip clip = hl_clip(W, H, clip_rect ? clip_rect + 4 * p : nullptr);
+        const HlSeg g = hl_segment(pts, m, path_pt_off[p], W, H, clip);
+        const uint32_t base = run_off[p];
+        const uint32_t n = g.r0 <= g.r1 ? static_cast<uint32_t>(g.r1 - g.r0 + 1) : 0u;
+        uint32_t c0 = 0;
+        if (lane == 0 && n) c0 = atomicAdd(&ctr->cell_cursor, n);
+        c0 = __shfl_sync(0xffffffffu, c0, 0);
+        const bool fits = static_cast<uint64_t>(c0) + n <= cell_cap;
+        if (!fits && lane == 0) atomicOr(&ctr->err, ERR_SPAN_CAP);
         int32_t lo = INT32_MAX, hi = INT32_MIN;
-        if (g.r0 <= g.r1) {
-            for (int32_t y = g.r0 + static_cast<int32_t>(lane); y <= g.r1; y += 32) {
-                const int2 sp = hl_row_span(g, y, W, clip);
-                const uint32_t r = base + static_cast<uint32_t>(y - g.r0);
-                const int32_t grp = rowmap ? 4 * y + 3 : y;
-                const bool any = sp.x <= sp.y;
-                runs[r] = make_int4(grp, grp, static_cast<int32_t>(r), any ? 1 : 0);
-                if (any) {
-                    cells[r] = static_cast<uint32_t>(sp.x) | (static_cast<uint32_t>(sp.y - sp.x) << 14) | (15u << 28);
-                    lo = min(lo, sp.x);
-                    hi = max(hi, sp.y);
-                }
+        for (uint32_t k = lane; k < n && fits; k += 32) {
+            const int32_t y = g.r0 + static_cast<int32_t>(k);
+            const int2 sp = hl_row_span(g, y, W, clip);
+            const int32_t grp = rowmap ? 4 * y + 3 : y;
+            const bool any = sp.x <= sp.y;
+            runs[base + k] = make_int4(grp, grp, static_cast<int32_t>(c0 + k), any ? 1 : 0);
+            if (any) {
+                cells[c0 + k] = static_cast<uint32_t>(sp.x) | (static_cast<uint32_t>(sp.y - sp.x) << 14) | (15u << 28);
+                lo = min(lo, sp.x);
+                hi = max(hi, sp.y);
             }
         }
         for (int o = 16; o; o >>= 1) {
@@ -242,10 +262,10 @@ __global__ void k_hl_write(const double* __restrict__ pts, const double* __restr
             hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
         }
         if (lane == 0) {
-            info[s].px0 = lo <= hi ? lo : 1;
-            info[s].px1 = lo <= hi ? hi : 0;
-            info[s].run_off = base;
-            info[s].run_cnt = g.r0 <= g.r1 ? static_cast<uint32_t>(g.r1 - g.r0 + 1) : 0u;
+            info[p].px0 = lo <= hi ? lo : 1;
+            info[p].px1 = lo <= hi ? hi : 0;
+            info[p].run_off = base;
+            info[p].run_cnt = fits ? n : 0u;
         }
     }
 }

@@ -62,7 +62,12 @@ struct BatchCounters {
     uint32_t pad[2];
     unsigned long long raw_entries;  // sum over edges of the rows they cover
     unsigned long long aa_rows;      // sum over paths of y1 - y0 + 1
+    unsigned long long hl_rows;      // hairline segments: pixel rows drawn (one run and one cell each)
 };
+
+// Internal fill-rule value of a hairline segment: a two-point path drawn as
+// stroke_narrow's one-pixel spans, not filled (see rrb_hairline.cuh).
+constexpr uint8_t RULE_HAIRLINE = 2;
 
 // Clip of path p in AA units: columns [x, y) and rows [z, w] — the page, or
 // the page and a clip rectangle (Clip::clip_to_rect) when path_clip is given.
@@ -85,7 +90,7 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
                        const uint64_t* __restrict__ path_pt_off, uint32_t n_paths,
                        const double* __restrict__ mtx, const uint32_t* __restrict__ path_page,
                        const uint32_t* __restrict__ page_h, uint2* __restrict__ pieces,
-                       uint32_t* __restrict__ path_pieces) {
+                       uint32_t* __restrict__ path_pieces, const uint8_t* __restrict__ rule) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -94,6 +99,7 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
         uint32_t n = static_cast<uint32_t>(path_pt_off[p + 1]) - off;
         uint32_t slot = off;
         uint32_t i = 0;
+        if (rule && rule[p] == RULE_HAIRLINE) n = 0;  // hairline segments have no fill edges
         while (i < n) {
             if (flags[off + i] & PF_FIRST) {
                 uint32_t sp = i, cur = i;
@@ -944,6 +950,7 @@ __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edg
     uint32_t nonterm = 0;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
         PathInfo P = info[p];
+        if (P.paint & PI_SOLID) continue;  // hairline layers: runs from k_hl_count / k_hl_write
         if (!(P.paint & PI_RECTI)) {
             if (!WRITE) run_count[p] = 0;
             continue;

@@ -267,7 +267,8 @@ int fill_static(rrb_ctx* c, const rrb_path_fill_params* p, unsigned char* base, 
     const double flat_sq = p->flatness * p->flatness;
 
     // Subpath walk -> pieces (at most one per point).
-    k_walk<<<1, 32, 0, s>>>(pts, flags, hdr->off, 1, hdr->mtx, &hdr->page, &hdr->ph, slots, hdr->path_pieces);
+    k_walk<<<1, 32, 0, s>>>(pts, flags, hdr->off, 1, hdr->mtx, &hdr->page, &hdr->ph, slots, hdr->path_pieces,
+                            nullptr);
     int rc;
     if ((rc = scan_static(c, s, hdr->path_pieces, 1, hdr->block))) return rc;
     uint32_t n_pieces = 0;

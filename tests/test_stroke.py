@@ -312,3 +312,20 @@ def test_hairlines_only_and_bad_params(backend, oracle, rrb_lib):
     with pytest.raises(rrb_lib.BackendError) as e:
         _gpu_paint(backend, rrb_lib, sc)
     assert e.value.status == 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rgb_pages", [False, True])
+def test_stroke_page_matches_oracle(backend, oracle, rrb_lib, rgb_pages):
+    """The benchmark's stroke page generator at Letter @150 dpi: rules, boxes,
+    polylines, curves, dashes and fills interleaved in one batch."""
+    from rrb.strokes import StrokePage
+
+    sp = StrokePage(3, n_paths=2500, w=1275, h=1650)
+    rgb = np.random.default_rng(4).integers(0, 256, (sp.n_paths, 3), dtype=np.uint8) if rgb_pages else None
+    bpp = 3 if rgb_pages else 1
+    exp = np.full(bpp * sp.arena_bytes, 255, np.uint8)
+    oracle.render_scene_paint(sp, exp, sp.strokes, rgb=rgb)
+    got = _gpu_paint(backend, rrb_lib, sp, rgb=rgb)
+    d = np.nonzero(got != exp)[0]
+    assert d.size == 0, f"{d.size} bytes differ, first at {d[:5]}"
