@@ -258,9 +258,11 @@ def _gpu_paint(backend, rrb_lib, sc, rgb=None, clip=None, rowmap=0, tile=(64, 16
     try:
         backend.set_tuning(*tile)
         backend.begin_page()
-        backend.record_fill_buffer(pages, 255)
-        backend.record_stroke_batch(p, sc.strokes, rgb, clip)
-        backend.wait_page(backend.submit_page())
+        try:
+            backend.record_fill_buffer(pages, 255)
+            backend.record_stroke_batch(p, sc.strokes, rgb, clip)
+        finally:
+            backend.wait_page(backend.submit_page())
         got = np.empty(bpp * sc.arena_bytes, np.uint8)
         backend.wait_download(backend.download_async(pages, got))
         return got
