@@ -531,6 +531,7 @@ def run_strokes(args, rank, local, world):
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     t = time.perf_counter()
     for _ in range(e2e_steps):
+        host_page[:] = 255
         backend.begin_page()
         backend.upload_async(pages, host_page)
         backend.record_stroke_batch(params, page.strokes)

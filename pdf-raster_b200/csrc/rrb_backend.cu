@@ -78,6 +78,7 @@ struct rrb_ctx {
     // Per-stage sums over the waves of one resident render.
     float stage_sum_ms[16] = {};
     uint32_t stage_sum_launches[16] = {};
+    rrb_stroke::PaintBatch* paint = nullptr;  // host arrays of rrb_record_stroke_batch, reused
 };
 
 namespace {
@@ -660,7 +661,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                 RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &c->h_read[65], 4,
                                             cudaMemcpyHostToDevice, c->stream));
                 k_groups_slow<<<grid_for(c, slow, 128), 128, 0, c->stream>>>(
-                    as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), as<uint32_t>(B->pw),
+                    as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), gmin, gmax,
+                    as<uint32_t>(B->pw),
                     as<uint2>(c->s_ovf2), ovf_cap, as<int3>(c->s_scratch),
                     static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
                     as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
@@ -895,105 +897,39 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
     return run_resident(c, B, arena, arena_len, h->rowmap);
 }
 
-// The batch a paint batch renders as: fills, stroke outlines and hairline
-// segments (RULE_HAIRLINE two-point paths) in path order, over the pages that
-// have any.
-struct PaintRun {
-    std::vector<double> pts, clip;
-    std::vector<uint8_t> flags, rule, gray, alpha, rgb;
-    std::vector<uint64_t> off{0}, page_off;
-    std::vector<uint32_t> page, pw, ph;
-    uint32_t last_page = UINT32_MAX;
-
-    // A path of the run: its points, paint and page (pages of the input batch
-    // are renumbered in order of first use).
-    void add(const rrb_path_batch_params* p, uint32_t path, const double* xy, const uint8_t* fl, uint64_t n,
-             uint8_t fill_rule, const uint8_t* path_rgb, const double* clip_rects) {
-        const uint32_t pg = p->path_page[path];
-        if (pg != last_page) {
-            last_page = pg;
-            pw.push_back(p->page_width[pg]);
-            ph.push_back(p->page_height[pg]);
-            page_off.push_back(p->page_offset[pg]);
-        }
-        pts.insert(pts.end(), xy, xy + 2 * n);
-        flags.insert(flags.end(), fl, fl + n);
-        off.push_back(flags.size());
-        rule.push_back(fill_rule);
-        gray.push_back(p->gray[path]);
-        alpha.push_back(p->alpha[path]);
-        page.push_back(static_cast<uint32_t>(pw.size() - 1));
-        if (path_rgb) rgb.insert(rgb.end(), path_rgb + 3 * path, path_rgb + 3 * path + 3);
-        if (clip_rects) clip.insert(clip.end(), clip_rects + 4 * path, clip_rects + 4 * path + 4);
+// Page-locked host memory for the paint batch arrays: the upload of the
+// (often large) stroke outlines is then a DMA, and the buffers are reused.
+struct PinnedAlloc : rrb_stroke::HostAlloc {
+    void* alloc(size_t bytes) override {
+        void* p = nullptr;
+        return cudaHostAlloc(&p, std::max<size_t>(bytes, 1), cudaHostAllocDefault) == cudaSuccess ? p : nullptr;
     }
-    rrb_path_batch_params params(const rrb_path_batch_params* p) const {
-        rrb_path_batch_params q = *p;
-        q.pts = pts.data();
-        q.flags = flags.data();
-        q.n_pts = flags.size();
-        q.path_pt_off = off.data();
-        q.fill_rule = rule.data();
-        q.gray = gray.data();
-        q.alpha = alpha.data();
-        q.path_page = page.data();
-        q.n_paths = rule.size();
-        q.page_width = pw.data();
-        q.page_height = ph.data();
-        q.page_offset = page_off.data();
-        q.n_pages = static_cast<uint32_t>(pw.size());
-        return q;
+    void release(void* p) override {
+        if (p) cudaFreeHost(p);
     }
 };
 
 int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_params* sp, const uint8_t* path_rgb,
                 const double* clip_rects) {
     std::string msg;
-    rrb_stroke::Plan plan;
-    int rc = rrb_stroke::plan(p, sp, plan, msg);
+    if (!c->paint) c->paint = new rrb_stroke::PaintBatch();
+    rrb_stroke::PaintBatch& pb = *c->paint;
+    PinnedAlloc alloc;
+    int rc = rrb_stroke::build(p, sp, path_rgb, clip_rects, alloc, pb, msg);
     if (rc) return set_err(c, rc, msg);
-    PaintRun run;
-    for (uint64_t i = 0; i < p->n_paths; ++i) {
-        const uint8_t k = plan.kind[i];
-        if (k == rrb_stroke::NOTHING) continue;
-        const uint32_t path = static_cast<uint32_t>(i);
-        if (k == rrb_stroke::FILL) {
-            const uint64_t a = p->path_pt_off[i], b = p->path_pt_off[i + 1];
-            run.add(p, path, p->pts + 2 * a, p->flags + a, b - a, p->fill_rule[i], path_rgb, clip_rects);
-        } else if (k == rrb_stroke::OUTLINE) {
-            const uint64_t a = plan.off[i], b = plan.off[i + 1];
-            run.add(p, path, plan.xy.data() + 2 * a, plan.fl.data() + a, b - a, 0, path_rgb, clip_rects);
-        } else {
-            // The hairline's segments, walked as XPath::new walks a path
-            // without curves and without closing (xpath.rs:162-260): from
-            // each FIRST point through the points up to the next LAST.
-            const double* xy = plan.xy.data() + 2 * plan.off[i];
-            const uint8_t* fl = plan.fl.data() + plan.off[i];
-            const uint64_t n = plan.off[i + 1] - plan.off[i];
-            static const uint8_t kSeg[2] = {RRB_PATH_FIRST, RRB_PATH_LAST};
-            uint64_t j = 0;
-            while (j < n) {
-                if (!(fl[j] & RRB_PATH_FIRST)) {
-                    ++j;
-                    continue;
-                }
-                uint64_t cur = j++;
-                while (j < n) {
-                    const double seg[4] = {xy[2 * cur], xy[2 * cur + 1], xy[2 * j], xy[2 * j + 1]};
-                    run.add(p, path, seg, kSeg, 2, RULE_HAIRLINE, path_rgb, clip_rects);
-                    cur = j;
-                    const bool last = fl[j] & RRB_PATH_LAST;
-                    ++j;
-                    if (last) break;
-                }
-            }
-        }
-    }
-    if (run.rule.empty()) return RRB_OK;
-    if (run.rule.size() >= (1ull << 31) || run.flags.size() >= (1ull << 30))
-        return set_err(c, RRB_ERR_POOL_EXHAUSTED, "painted geometry exceeds 2^30 points or 2^31 paths");
-    const rrb_path_batch_params q = run.params(p);
-    return run_batch(c, &q, static_cast<uint8_t*>(p->pages->p), p->pages->len, path_rgb ? run.rgb.data() : nullptr,
-                     clip_rects ? run.clip.data() : nullptr, true);
+    if (pb.n_paths == 0) return RRB_OK;
+    rrb_path_batch_params q = *p;
+    q.pts = pb.pts.p;
+    q.flags = pb.flags.p;
+    q.n_pts = pb.n_pts;
+    q.path_pt_off = pb.off.p;
+    q.fill_rule = pb.rule.p;
+    q.gray = pb.gray.p;
+    q.alpha = pb.alpha.p;
+    q.path_page = pb.page.p;
+    q.n_paths = pb.n_paths;
+    return run_batch(c, &q, static_cast<uint8_t*>(p->pages->p), p->pages->len, path_rgb ? pb.rgb.p : nullptr,
+                     clip_rects ? pb.clip.p : nullptr, true);
 }
 
 }  // namespace
@@ -1095,6 +1031,11 @@ int rrb_destroy(rrb_ctx* c) {
             cudaEventDestroy(c->timer->end[k]);
         }
         delete c->timer;
+    }
+    if (c->paint) {
+        PinnedAlloc alloc;
+        c->paint->release(alloc);
+        delete c->paint;
     }
     for (auto& kv : c->fences) cudaEventDestroy(kv.second);
     for (cudaEvent_t ev : c->free_events) cudaEventDestroy(ev);

@@ -1161,7 +1161,8 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
 // pixel row, the four sub-row lists in a global scratch slice of 4 x the
 // path's edge count.
 __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off,
-                              const Edge* __restrict__ edges, const uint32_t* __restrict__ page_w,
+                              const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
+                              const int32_t* __restrict__ gmax, const uint32_t* __restrict__ page_w,
                               const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
                               uint32_t scratch_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
                               uint32_t cell_cap, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
@@ -1181,24 +1182,42 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
         const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
         int n4[4] = {0, 0, 0, 0};
+        // One pass over the path's edges builds the four sub-rows' entry
+        // lists, each in edge order (merging into its own last entry);
+        // aligned 32-edge groups whose row bounds miss the pixel row are skipped.
+        const int32_t rlo = max(4 * g, P.y0), rhi = min(4 * g + 3, P.y1);
+        for (uint32_t j = P.e_begin; j < P.e_end;) {
+            const uint32_t grp = j >> 5;
+            const uint32_t jend = min(P.e_end, (grp + 1) << 5);
+            if (gmax[grp] < rlo || gmin[grp] > rhi) {
+                j = jend;
+                continue;
+            }
+            for (; j < jend; ++j) {
+                const Edge E = edges[j];
+                if ((E.flags & EF_EMPTY) || E.row1 < rlo || E.row0 > rhi) continue;
+                const int32_t r0 = max(rlo, E.row0), r1 = min(rhi, E.row1);
+                for (int32_t r = r0; r <= r1; ++r) {
+                    const int sub = r - 4 * g;
+                    int3* L = scratch + sb + static_cast<uint32_t>(sub) * ne;
+                    int& n = n4[sub];
+                    int32_t elo, ehi, ec;
+                    edge_entry(E, r, elo, ehi, ec);
+                    if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
+                        L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
+                        L[n - 1].x = min(L[n - 1].x, elo);
+                        L[n - 1].y = max(L[n - 1].y, ehi);
+                    } else {
+                        L[n++] = make_int3(elo, ehi, ec);
+                    }
+                }
+            }
+        }
         for (int sub = 0; sub < 4; ++sub) {
             const int32_t r = 4 * g + sub;
             if (r < P.y0 || r > P.y1) continue;
             int3* L = scratch + sb + static_cast<uint32_t>(sub) * ne;
-            int n = 0;
-            for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
-                const Edge E = edges[j];
-                if ((E.flags & EF_EMPTY) || r < E.row0 || r > E.row1) continue;
-                int32_t elo, ehi, ec;
-                edge_entry(E, r, elo, ehi, ec);
-                if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
-                    L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
-                    L[n - 1].x = min(L[n - 1].x, elo);
-                    L[n - 1].y = max(L[n - 1].y, ehi);
-                } else {
-                    L[n++] = make_int3(elo, ehi, ec);
-                }
-            }
+            int n = n4[sub];
             // Stable sort by x0 (a row of more than 20 entries: see the tie note in the oracle).
             for (int a = 1; a < n; ++a) {
                 const int3 t = L[a];

@@ -497,76 +497,190 @@ int check_params(const rrb_stroke_params& sp, std::string& msg) {
     return RRB_OK;
 }
 
-int plan(const rrb_path_batch_params* p, const rrb_stroke_params* sp, Plan& out, std::string& msg) {
+namespace {
+
+// Runs fn(worker) on up to `want` threads (the calling thread is one).
+template <typename Fn>
+void parallel(unsigned want, Fn fn) {
+    if (want <= 1) {
+        fn();
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(want - 1);
+    for (unsigned t = 1; t < want; ++t) th.emplace_back(fn);
+    fn();
+    for (auto& t : th) t.join();
+}
+
+// Hairline segments of a polyline, walked as XPath::new walks a path without
+// curves and without closing (xpath.rs:162-260): from each FIRST point
+// through the points up to the next LAST. emit(a, b) gets point indices.
+template <typename Emit>
+uint32_t hairline_segments(const uint8_t* fl, uint64_t n, Emit emit) {
+    uint32_t k = 0;
+    uint64_t j = 0;
+    while (j < n) {
+        if (!(fl[j] & RRB_PATH_FIRST)) {
+            ++j;
+            continue;
+        }
+        uint64_t cur = j++;
+        while (j < n) {
+            emit(cur, j);
+            ++k;
+            cur = j;
+            const bool last = fl[j] & RRB_PATH_LAST;
+            ++j;
+            if (last) break;
+        }
+    }
+    return k;
+}
+
+}  // namespace
+
+int build(const rrb_path_batch_params* p, const rrb_stroke_params* sp, const uint8_t* path_rgb,
+          const double* clip_rects, HostAlloc& alloc, PaintBatch& out, std::string& msg) {
     const uint64_t n = p->n_paths;
-    out.kind.assign(n, NOTHING);
-    out.off.assign(n + 1, 0);
-    out.xy.clear();
-    out.fl.clear();
+    out.n_paths = out.n_pts = 0;
     for (uint64_t i = 0; i < n; ++i) {
         const int rc = check_params(sp[i], msg);
         if (rc) return rc;
     }
     constexpr uint64_t kChunk = 64;
     const uint64_t n_chunks = (n + kChunk - 1) / kChunk;
-    struct Chunk {
-        std::vector<double> xy;
-        std::vector<uint8_t> fl;
-        std::vector<uint64_t> len;  // points per path of the chunk
-    };
-    std::vector<Chunk> chunks(n_chunks);
+    if (out.chunks.size() < n_chunks) out.chunks.resize(n_chunks);
+    const double flatness = std::max(p->flatness, 0.0);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = static_cast<unsigned>(std::min<uint64_t>(std::min(hw, 32u), n_chunks));
+    // Pass 1: stroke each chunk's paths into its own buffers; count the
+    // output paths and points.
     std::atomic<uint64_t> next{0};
-    auto work = [&]() {
+    parallel(nt, [&]() {
         Scratch s;
         for (;;) {
             const uint64_t c = next.fetch_add(1);
             if (c >= n_chunks) return;
-            Chunk& ch = chunks[c];
+            Chunk& ch = out.chunks[c];
             const uint64_t b = c * kChunk, e = std::min(n, b + kChunk);
+            ch.xy.clear();
+            ch.fl.clear();
+            ch.kind.assign(e - b, NOTHING);
             ch.len.assign(e - b, 0);
+            ch.segs.assign(e - b, 0);
+            ch.out_paths = ch.out_pts = 0;
             for (uint64_t i = b; i < e; ++i) {
+                const uint64_t a0 = p->path_pt_off[i], a1 = p->path_pt_off[i + 1];
+                const size_t k = i - b;
                 if (!sp[i].stroke) {
-                    out.kind[i] = FILL;
+                    ch.kind[k] = a1 > a0 ? FILL : NOTHING;
+                    if (a1 > a0) {
+                        ch.out_paths += 1;
+                        ch.out_pts += a1 - a0;
+                    }
                     continue;
                 }
-                const uint64_t a0 = p->path_pt_off[i], a1 = p->path_pt_off[i + 1];
                 const size_t before = ch.fl.size();
-                out.kind[i] = static_cast<uint8_t>(
-                    stroke_one(Pts{p->pts + 2 * a0, p->flags + a0, static_cast<size_t>(a1 - a0)}, sp[i],
-                               std::max(p->flatness, 0.0), s, ch.xy, ch.fl));
-                ch.len[i - b] = ch.fl.size() - before;
-                if (ch.len[i - b] == 0) out.kind[i] = NOTHING;
+                int kind = stroke_one(Pts{p->pts + 2 * a0, p->flags + a0, static_cast<size_t>(a1 - a0)}, sp[i],
+                                      flatness, s, ch.xy, ch.fl);
+                ch.len[k] = ch.fl.size() - before;
+                if (ch.len[k] == 0) kind = NOTHING;
+                ch.kind[k] = static_cast<uint8_t>(kind);
+                if (kind == OUTLINE) {
+                    ch.out_paths += 1;
+                    ch.out_pts += ch.len[k];
+                } else if (kind == HAIRLINE) {
+                    ch.segs[k] = hairline_segments(ch.fl.data() + before, ch.len[k], [](uint64_t, uint64_t) {});
+                    ch.out_paths += ch.segs[k];
+                    ch.out_pts += 2ull * ch.segs[k];
+                }
             }
         }
-    };
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned nt = static_cast<unsigned>(std::min<uint64_t>(std::min(hw, 32u), n_chunks));
-    if (nt <= 1) {
-        work();
-    } else {
-        std::vector<std::thread> th;
-        th.reserve(nt);
-        for (unsigned t = 0; t < nt; ++t) th.emplace_back(work);
-        for (auto& t : th) t.join();
-    }
-    uint64_t total = 0;
+    });
+    // Offsets of each chunk's output.
+    std::vector<uint64_t> path_at(n_chunks + 1, 0), pt_at(n_chunks + 1, 0);
     for (uint64_t c = 0; c < n_chunks; ++c) {
-        const uint64_t b = c * kChunk;
-        for (size_t k = 0; k < chunks[c].len.size(); ++k) {
-            out.off[b + k] = total;
-            total += chunks[c].len[k];
+        path_at[c + 1] = path_at[c] + out.chunks[c].out_paths;
+        pt_at[c + 1] = pt_at[c] + out.chunks[c].out_pts;
+    }
+    const uint64_t np = path_at[n_chunks], npt = pt_at[n_chunks];
+    if (npt >= (1ull << 30) || np >= (1ull << 31))
+        return msg = "painted geometry exceeds 2^30 points or 2^31 paths", RRB_ERR_POOL_EXHAUSTED;
+    out.n_paths = np;
+    out.n_pts = npt;
+    if (np == 0) return RRB_OK;
+    out.pts.reserve(alloc, 2 * npt);
+    out.flags.reserve(alloc, npt);
+    out.off.reserve(alloc, np + 1);
+    out.rule.reserve(alloc, np);
+    out.gray.reserve(alloc, np);
+    out.alpha.reserve(alloc, np);
+    out.page.reserve(alloc, np);
+    if (path_rgb) out.rgb.reserve(alloc, 3 * np);
+    if (clip_rects) out.clip.reserve(alloc, 4 * np);
+    if (!out.pts.p || !out.flags.p || !out.off.p || !out.rule.p || !out.gray.p || !out.alpha.p || !out.page.p ||
+        (path_rgb && !out.rgb.p) || (clip_rects && !out.clip.p))
+        return msg = "out of host memory for the paint batch", RRB_ERR_OUT_OF_MEMORY;
+    out.off.p[np] = npt;
+    // Pass 2: every chunk writes its output paths at its offsets.
+    next = 0;
+    parallel(nt, [&]() {
+        for (;;) {
+            const uint64_t c = next.fetch_add(1);
+            if (c >= n_chunks) return;
+            const Chunk& ch = out.chunks[c];
+            uint64_t q = path_at[c], at = pt_at[c], g = 0;  // output path, output point, chunk geometry point
+            const uint64_t b = c * kChunk, e = std::min(n, b + kChunk);
+            auto meta = [&](uint64_t i, uint8_t rule) {
+                out.off.p[q] = at;
+                out.rule.p[q] = rule;
+                out.gray.p[q] = p->gray[i];
+                out.alpha.p[q] = p->alpha[i];
+                out.page.p[q] = p->path_page[i];
+                if (path_rgb) std::memcpy(out.rgb.p + 3 * q, path_rgb + 3 * i, 3);
+                if (clip_rects) std::memcpy(out.clip.p + 4 * q, clip_rects + 4 * i, 4 * sizeof(double));
+                ++q;
+            };
+            for (uint64_t i = b; i < e; ++i) {
+                const size_t k = i - b;
+                switch (ch.kind[k]) {
+                    case FILL: {
+                        const uint64_t a0 = p->path_pt_off[i], m = p->path_pt_off[i + 1] - a0;
+                        meta(i, p->fill_rule[i]);
+                        std::memcpy(out.pts.p + 2 * at, p->pts + 2 * a0, 2 * m * sizeof(double));
+                        std::memcpy(out.flags.p + at, p->flags + a0, m);
+                        at += m;
+                        break;
+                    }
+                    case OUTLINE:
+                        meta(i, 0);
+                        std::memcpy(out.pts.p + 2 * at, ch.xy.data() + 2 * g, 2 * ch.len[k] * sizeof(double));
+                        std::memcpy(out.flags.p + at, ch.fl.data() + g, ch.len[k]);
+                        at += ch.len[k];
+                        break;
+                    case HAIRLINE: {
+                        const double* xy = ch.xy.data() + 2 * g;
+                        hairline_segments(ch.fl.data() + g, ch.len[k], [&](uint64_t a, uint64_t bb) {
+                            meta(i, kRuleHairline);
+                            double* o = out.pts.p + 2 * at;
+                            o[0] = xy[2 * a];
+                            o[1] = xy[2 * a + 1];
+                            o[2] = xy[2 * bb];
+                            o[3] = xy[2 * bb + 1];
+                            out.flags.p[at] = RRB_PATH_FIRST;
+                            out.flags.p[at + 1] = RRB_PATH_LAST;
+                            at += 2;
+                        });
+                        break;
+                    }
+                    default:
+                        break;
+                }
+                g += ch.len[k];
+            }
         }
-    }
-    out.off[n] = total;
-    if (total >= (1ull << 30)) return msg = "stroke outlines exceed 2^30 points", RRB_ERR_POOL_EXHAUSTED;
-    out.xy.resize(2 * total);
-    out.fl.resize(total);
-    for (uint64_t c = 0; c < n_chunks; ++c) {
-        if (chunks[c].fl.empty()) continue;
-        const uint64_t at = out.off[c * kChunk];
-        std::memcpy(out.xy.data() + 2 * at, chunks[c].xy.data(), chunks[c].xy.size() * sizeof(double));
-        std::memcpy(out.fl.data() + at, chunks[c].fl.data(), chunks[c].fl.size());
-    }
+    });
     return RRB_OK;
 }
 

@@ -17,18 +17,78 @@ enum Kind : uint8_t {
     FILL = 3,      // not a stroke: the input path, filled with its own rule
 };
 
-// Geometry of a paint batch: kind per path, and for outlines and hairlines
-// their points at [off[p], off[p+1]) of xy (x, y pairs) / fl (path flags).
-struct Plan {
-    std::vector<uint8_t> kind;
-    std::vector<uint64_t> off;
-    std::vector<double> xy;
+// Internal fill-rule value of a hairline segment in a paint batch (the
+// device pipeline's RULE_HAIRLINE).
+constexpr uint8_t kRuleHairline = 2;
+
+// Source of host memory for the batch arrays (the backend hands out
+// page-locked memory, so the upload is a DMA).
+struct HostAlloc {
+    virtual void* alloc(size_t bytes) = 0;
+    virtual void release(void* p) = 0;
+    virtual ~HostAlloc() = default;
+};
+
+template <typename T>
+struct HostArray {
+    T* p = nullptr;
+    size_t cap = 0;
+    void reserve(HostAlloc& a, size_t n) {
+        if (n <= cap) return;
+        a.release(p);
+        p = nullptr;
+        cap = 0;
+        p = static_cast<T*>(a.alloc(n * sizeof(T)));
+        if (p) cap = n;
+    }
+    void release(HostAlloc& a) {
+        a.release(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// Geometry a worker made for one chunk of consecutive paths (reused from
+// call to call, so steady-state calls allocate nothing).
+struct Chunk {
+    std::vector<double> xy;       // outline / hairline points of the chunk's paths
     std::vector<uint8_t> fl;
+    std::vector<uint8_t> kind;    // per path
+    std::vector<uint64_t> len;    // per path: points in xy / fl
+    std::vector<uint32_t> segs;   // per path: hairline segments
+    uint64_t out_paths = 0, out_pts = 0;
+};
+
+// The batch the device renders for a paint batch: fills (the input paths),
+// stroke outlines (rule nonzero) and hairline segments (two-point paths with
+// rule kRuleHairline), in path order, with their paint, page and clip.
+struct PaintBatch {
+    HostArray<double> pts, clip;
+    HostArray<uint8_t> flags, rule, gray, alpha, rgb;
+    HostArray<uint64_t> off;
+    HostArray<uint32_t> page;
+    uint64_t n_paths = 0, n_pts = 0;
+    std::vector<Chunk> chunks;
+    void release(HostAlloc& a) {
+        pts.release(a);
+        clip.release(a);
+        flags.release(a);
+        rule.release(a);
+        gray.release(a);
+        alpha.release(a);
+        rgb.release(a);
+        off.release(a);
+        page.release(a);
+    }
 };
 
 // Checks one path's stroke parameters (params.validate() style).
 int check_params(const rrb_stroke_params& sp, std::string& msg);
-// Strokes every path of p with sp[p] (host threads over chunks of paths).
-int plan(const rrb_path_batch_params* p, const rrb_stroke_params* sp, Plan& out, std::string& msg);
+// Strokes every path of p with sp[p] and lays out the batch to render:
+// host threads stroke chunks of paths, then write the chunks' output paths
+// at their offsets. path_rgb / clip_rects (per input path, or null) are
+// carried to the output paths.
+int build(const rrb_path_batch_params* p, const rrb_stroke_params* sp, const uint8_t* path_rgb,
+          const double* clip_rects, HostAlloc& alloc, PaintBatch& out, std::string& msg);
 
 }  // namespace rrb_stroke
