@@ -1173,8 +1173,9 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
         const int32_t g = static_cast<int32_t>(ovf[k].y);
         const PathInfo P = info[p];
         const uint32_t ne = P.e_end - P.e_begin;
-        const uint32_t sb = atomicAdd(&ctr->scratch_cursor, 4u * ne);
-        if (static_cast<uint64_t>(sb) + 4ull * ne > scratch_cap) {
+        // Four sub-row lists of up to ne entries, and one list of merge-sort temporary.
+        const uint32_t sb = atomicAdd(&ctr->scratch_cursor, 5u * ne);
+        if (static_cast<uint64_t>(sb) + 5ull * ne > scratch_cap) {
             atomicOr(&ctr->err, ERR_SCRATCH_CAP);
             continue;
         }
@@ -1218,15 +1219,28 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
             if (r < P.y0 || r > P.y1) continue;
             int3* L = scratch + sb + static_cast<uint32_t>(sub) * ne;
             int n = n4[sub];
-            // Stable sort by x0 (a row of more than 20 entries: see the tie note in the oracle).
-            for (int a = 1; a < n; ++a) {
-                const int3 t = L[a];
-                int b = a;
-                while (b > 0 && t.x < L[b - 1].x) {
-                    L[b] = L[b - 1];
-                    --b;
+            // Stable sort by x0 (a row of more than 20 entries: see the tie
+            // note in the oracle): bottom-up merge sort through the temporary
+            // list, skipped when the entries already come in order.
+            bool sorted = true;
+            for (int a = 1; a < n && sorted; ++a) sorted = L[a - 1].x <= L[a].x;
+            if (!sorted) {
+                int3* A = L;
+                int3* T = scratch + sb + 4u * ne;
+                for (int w = 1; w < n; w *= 2) {
+                    for (int lo = 0; lo < n; lo += 2 * w) {
+                        const int mid = min(lo + w, n), hi = min(lo + 2 * w, n);
+                        int i = lo, j = mid, k = lo;
+                        while (i < mid && j < hi) T[k++] = A[j].x < A[i].x ? A[j++] : A[i++];
+                        while (i < mid) T[k++] = A[i++];
+                        while (j < hi) T[k++] = A[j++];
+                    }
+                    int3* t = A;
+                    A = T;
+                    T = t;
                 }
-                L[b] = t;
+                if (A != L)
+                    for (int a = 0; a < n; ++a) L[a] = A[a];
             }
             n4[sub] = walk_row(
                 n, mask, aa_width, cx.x, cx.y,
