@@ -79,6 +79,7 @@ struct rrb_ctx {
     float stage_sum_ms[16] = {};
     uint32_t stage_sum_launches[16] = {};
     rrb_stroke::PaintBatch* paint = nullptr;  // host arrays of rrb_record_stroke_batch, reused
+    cudaStream_t copy_stream = nullptr;       // streamed batches: point uploads ahead of the render
 };
 
 namespace {
@@ -364,7 +365,7 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
 // Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages;
 // clip (host, 4 doubles per path) clips each path to a device-space rectangle.
 int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr,
-                 const double* clip = nullptr, bool hairlines = false) {
+                 const double* clip = nullptr, bool hairlines = false, bool defer_points = false) {
     std::string msg;
     uint64_t tiles = 0;
     B->bpp = rgb ? 3 : 1;
@@ -388,8 +389,14 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     B->page_pt[B->n_pages] = h->n_paths ? h->path_pt_off[h->n_paths] : 0;
     if (B->n_paths == 0) return RRB_OK;
     int rc;
-    if ((rc = upload(c, B->pts, h->pts, 2 * h->n_pts))) return rc;
-    if ((rc = upload(c, B->flags, h->flags, h->n_pts))) return rc;
+    if (defer_points) {
+        // The caller copies the points itself, range by range (run_streamed).
+        if ((rc = ensure(c, B->pts, 2 * h->n_pts * sizeof(double)))) return rc;
+        if ((rc = ensure(c, B->flags, h->n_pts))) return rc;
+    } else {
+        if ((rc = upload(c, B->pts, h->pts, 2 * h->n_pts))) return rc;
+        if ((rc = upload(c, B->flags, h->flags, h->n_pts))) return rc;
+    }
     if ((rc = upload(c, B->off, h->path_pt_off, h->n_paths + 1))) return rc;
     if ((rc = upload(c, B->rule, h->fill_rule, h->n_paths))) return rc;
     if ((rc = upload(c, B->gray, h->gray, h->n_paths))) return rc;
@@ -889,11 +896,176 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
     return RRB_OK;
 }
 
+// Paths [pa, pb) of B as a batch of their own (a path-range wave): the pages
+// they lie on, each keeping only those paths. Rendering consecutive path
+// ranges one after another composites every page in path order, the same
+// pixels as one pass. ptb / pte: the range's first point and end.
+int make_path_wave(rrb_ctx* c, rrb_batch* B, uint32_t pa, uint32_t pb, uint64_t ptb, uint64_t pte, rrb_batch* W) {
+    auto page_of = [&](uint32_t path) {  // the page whose path range holds `path`
+        uint32_t lo = 0, hi = B->n_pages;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (B->geom_h[mid].path_begin <= path) lo = mid;
+            else hi = mid;
+        }
+        while (lo + 1 < B->n_pages && B->geom_h[lo].path_end <= path) ++lo;
+        return lo;
+    };
+    const uint32_t pg0 = page_of(pa), pg1 = page_of(pb - 1) + 1;
+    W->view = true;
+    W->n_paths = pb - pa;
+    W->n_pts = pte - ptb;
+    W->n_pages = pg1 - pg0;
+    W->flat_sq = B->flat_sq;
+    W->rowmap = B->rowmap;
+    W->arena_need = B->arena_need;
+    W->bpp = B->bpp;
+    W->has_clip = B->has_clip;
+    W->has_hairline = B->has_hairline;
+    auto view = [](Scratch& dst, const Scratch& src, size_t byte_off) {
+        dst.p = static_cast<char*>(src.p) + byte_off;
+        dst.cap = 0;
+    };
+    view(W->pts, B->pts, 2 * ptb * sizeof(double));
+    view(W->flags, B->flags, ptb);
+    view(W->rule, B->rule, pa);
+    view(W->gray, B->gray, pa);
+    view(W->alpha, B->alpha, pa);
+    view(W->pw, B->pw, pg0 * sizeof(uint32_t));
+    view(W->ph, B->ph, pg0 * sizeof(uint32_t));
+    view(W->mtx, B->mtx, 0);
+    if (B->bpp == 3) view(W->rgb, B->rgb, pa * sizeof(uint32_t));
+    if (B->has_clip) {
+        view(W->clip, B->clip, pa * sizeof(int4));
+        view(W->clipf, B->clipf, pa * 4 * sizeof(double));
+    }
+    int rc;
+    if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
+    if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
+    if ((rc = ensure(c, W->geom, W->n_pages * sizeof(PageGeom)))) return rc;
+    k_rebase_paths<<<grid_for(c, W->n_paths + 1, 256), 256, 0, c->stream>>>(
+        as<uint64_t>(B->off) + pa, as<uint64_t>(W->off), ptb, as<uint32_t>(B->page) + pa, as<uint32_t>(W->page), pg0,
+        static_cast<uint32_t>(W->n_paths));
+    c->launches += 1;
+    RRB_CUDA(c, cudaGetLastError());
+    W->geom_h.assign(B->geom_h.begin() + pg0, B->geom_h.begin() + pg1);
+    for (PageGeom& G : W->geom_h) {
+        G.path_begin = std::min(std::max(G.path_begin, pa), pb) - pa;
+        G.path_end = std::max(std::min(G.path_end, pb), pa) - pa;
+        if (G.path_end < G.path_begin) G.path_end = G.path_begin;
+    }
+    set_binning(W->geom_h, W->supers);
+    W->page_pt.clear();
+    W->plan.clear();
+    return RRB_OK;
+}
+
+// Path range [pa, pb) of B; a range that runs out of memory or cell capacity
+// is split in two (its composite had not run, so the pages are untouched).
+int run_path_range(rrb_ctx* c, rrb_batch* B, const uint64_t* path_pt_off, uint32_t pa, uint32_t pb, uint8_t* arena,
+                   size_t arena_len, int rowmap, rrb_batch_stats& acc, int depth) {
+    int rc = make_path_wave(c, B, pa, pb, path_pt_off[pa], path_pt_off[pb], c->wave_batch);
+    if (!rc) rc = run_resident_one(c, c->wave_batch, arena, arena_len, rowmap);
+    if (rc == RRB_OK) {
+        const rrb_batch_stats& s = c->stats;
+        acc.paths += s.paths;
+        acc.pieces += s.pieces;
+        acc.segments += s.segments;
+        acc.aa_rows += s.aa_rows;
+        acc.spans += s.spans;
+        acc.row_overflows += s.row_overflows;
+        acc.tiles += s.tiles;
+        acc.tile_pairs += s.tile_pairs;
+        acc.nonterminating_rows += s.nonterminating_rows;
+        acc.kernel_launches += s.kernel_launches;
+        acc.waves += 1;
+        for (int k = 0; k < 16; ++k) {
+            c->stage_sum_ms[k] += c->stage_ms[k];
+            c->stage_sum_launches[k] += c->stage_launches[k];
+        }
+        return RRB_OK;
+    }
+    const bool splittable = (rc == RRB_ERR_OUT_OF_MEMORY || rc == RRB_ERR_POOL_EXHAUSTED) && pb - pa > 1 && depth < 24;
+    if (!splittable) return rc;
+    cudaGetLastError();
+    if (rc == RRB_ERR_OUT_OF_MEMORY) release_scratch(c);
+    const uint32_t mid = pa + (pb - pa) / 2;
+    if ((rc = run_path_range(c, B, path_pt_off, pa, mid, arena, arena_len, rowmap, acc, depth + 1))) return rc;
+    return run_path_range(c, B, path_pt_off, mid, pb, arena, arena_len, rowmap, acc, depth + 1);
+}
+
+// Points per batch from which host batches in page-locked memory are
+// streamed: their points are copied range by range on a second stream while
+// the ranges before them render, so the upload hides behind the render.
+constexpr uint64_t kStreamMinPoints = 4ull << 20;
+constexpr uint64_t kStreamRanges = 6;
+
+bool page_locked(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8_t* arena, size_t arena_len) {
+    if (!c->copy_stream) RRB_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    // Ranges of consecutive paths of about n_pts / kStreamRanges points each.
+    const uint64_t target = std::max<uint64_t>(1ull << 20, (h->n_pts + kStreamRanges - 1) / kStreamRanges);
+    std::vector<uint32_t> cut{0};
+    for (uint64_t p = 1; p < h->n_paths; ++p)
+        if (h->path_pt_off[p] - h->path_pt_off[cut.back()] >= target) cut.push_back(static_cast<uint32_t>(p));
+    cut.push_back(static_cast<uint32_t>(h->n_paths));
+    const size_t nr = cut.size() - 1;
+    std::vector<cudaEvent_t> ev(nr + 1, nullptr);
+    for (auto& e : ev) RRB_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    auto done = [&](int rc) {
+        cudaStreamSynchronize(c->copy_stream);  // no copy from the caller's memory may outlive the call
+        for (auto& e : ev) cudaEventDestroy(e);
+        return rc;
+    };
+    // The copies start once the device is done with the previous batch in these buffers.
+    RRB_CUDA(c, cudaEventRecord(ev[nr], c->stream));
+    RRB_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev[nr], 0));
+    for (size_t r = 0; r < nr; ++r) {
+        const uint64_t a = h->path_pt_off[cut[r]], b = h->path_pt_off[cut[r + 1]];
+        if (b > a) {
+            if (cudaMemcpyAsync(as<double>(B->pts) + 2 * a, h->pts + 2 * a, 2 * (b - a) * sizeof(double),
+                                cudaMemcpyHostToDevice, c->copy_stream) != cudaSuccess ||
+                cudaMemcpyAsync(as<uint8_t>(B->flags) + a, h->flags + a, b - a, cudaMemcpyHostToDevice,
+                                c->copy_stream) != cudaSuccess)
+                return done(set_err(c, RRB_ERR_DEVICE, "point upload failed"));
+        }
+        if (cudaEventRecord(ev[r], c->copy_stream) != cudaSuccess) return done(set_err(c, RRB_ERR_DEVICE, "event"));
+    }
+    rrb_batch_stats acc{};
+    const uint64_t grows0 = c->scratch_grows;
+    std::memset(c->stage_sum_ms, 0, sizeof c->stage_sum_ms);
+    std::memset(c->stage_sum_launches, 0, sizeof c->stage_sum_launches);
+    for (size_t r = 0; r < nr; ++r) {
+        if (cudaStreamWaitEvent(c->stream, ev[r], 0) != cudaSuccess) return done(set_err(c, RRB_ERR_DEVICE, "event"));
+        const int rc = run_path_range(c, B, h->path_pt_off, cut[r], cut[r + 1], arena, arena_len, h->rowmap, acc, 0);
+        if (rc) {
+            c->stats = acc;
+            return done(rc);
+        }
+    }
+    c->stats = acc;
+    c->stats.scratch_grows = c->scratch_grows - grows0;
+    std::memcpy(c->stage_ms, c->stage_sum_ms, sizeof c->stage_ms);
+    std::memcpy(c->stage_launches, c->stage_sum_launches, sizeof c->stage_launches);
+    return done(RRB_OK);
+}
+
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
               const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false) {
     rrb_batch* B = c->tmp_batch;
-    int rc = batch_upload(c, h, B, rgb, clip, hairlines);
+    const bool streamed = h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
+                          page_locked(h->flags);
+    int rc = batch_upload(c, h, B, rgb, clip, hairlines, streamed);
     if (rc) return rc;
+    if (streamed) return run_streamed(c, h, B, arena, arena_len);
     return run_resident(c, B, arena, arena_len, h->rowmap);
 }
 
@@ -1040,6 +1212,7 @@ int rrb_destroy(rrb_ctx* c) {
     for (auto& kv : c->fences) cudaEventDestroy(kv.second);
     for (cudaEvent_t ev : c->free_events) cudaEventDestroy(ev);
     if (c->h_read) cudaFreeHost(c->h_read);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     cudaStreamDestroy(c->stream);
     delete c;
     return RRB_OK;
