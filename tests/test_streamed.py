@@ -19,7 +19,7 @@ def _pinned(backend, arr, bufs):
 
 SCENES = {
     "glyphs_one_page": dict(kind=1, seed=3, n_paths=20000),
-    "mixed_8_pages": dict(kind=2, seed=5, n_pages=8, page_scale=0.15, paths_scale=0.7),
+    "mixed_8_pages": dict(kind=2, seed=5, n_pages=8, page_scale=0.15, paths_scale=0.8),
 }
 
 
