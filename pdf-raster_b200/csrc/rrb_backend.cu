@@ -1058,10 +1058,13 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
     return done(RRB_OK);
 }
 
+// stream: allow the streamed form. Paint batches do not stream: their points
+// are built on the host first, and their slow rows (one thread per row, a
+// few long ones) cost more split over ranges than the copy they would hide.
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
-              const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false) {
+              const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false, bool stream = true) {
     rrb_batch* B = c->tmp_batch;
-    const bool streamed = h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
+    const bool streamed = stream && h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
                           page_locked(h->flags);
     int rc = batch_upload(c, h, B, rgb, clip, hairlines, streamed);
     if (rc) return rc;
@@ -1101,7 +1104,7 @@ int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_par
     q.path_page = pb.page.p;
     q.n_paths = pb.n_paths;
     return run_batch(c, &q, static_cast<uint8_t*>(p->pages->p), p->pages->len, path_rgb ? pb.rgb.p : nullptr,
-                     clip_rects ? pb.clip.p : nullptr, true);
+                     clip_rects ? pb.clip.p : nullptr, true, false);
 }
 
 }  // namespace
