@@ -667,7 +667,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                             cudaMemcpyHostToDevice, c->stream));
                 RRB_CUDA(c, cudaMemcpyAsync(&as<BatchCounters>(c->s_ctr)->scratch_cursor, &c->h_read[65], 4,
                                             cudaMemcpyHostToDevice, c->stream));
-                k_groups_slow<<<grid_for(c, slow, 128), 128, 0, c->stream>>>(
+                k_groups_slow<<<grid_for(c, slow * 32, SLOW_WARPS * 32, 16), SLOW_WARPS * 32, 0, c->stream>>>(
                     as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), gmin, gmax,
                     as<uint32_t>(B->pw),
                     as<uint2>(c->s_ovf2), ovf_cap, as<int3>(c->s_scratch),

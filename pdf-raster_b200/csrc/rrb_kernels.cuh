@@ -1160,60 +1160,92 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
 // Pixel rows with a sub-row whose merged list exceeded MID_K: one thread per
 // pixel row, the four sub-row lists in a global scratch slice of 4 x the
 // path's edge count.
+constexpr int SLOW_WARPS = 4;  // warps per block of k_groups_slow
+
 __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t* __restrict__ group_off,
                               const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
                               const int32_t* __restrict__ gmax, const uint32_t* __restrict__ page_w,
                               const uint2* __restrict__ ovf, uint32_t ovf_cap, int3* __restrict__ scratch,
                               uint32_t scratch_cap, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
                               uint32_t cell_cap, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
+    // One warp per overflowing pixel row. The warp loads the path's edges 32
+    // at a time (aligned groups whose row bounds miss the row are skipped) and
+    // stages each lane's entries for the four AA sub-rows in shared memory;
+    // lanes 0-3 then fold them, in edge order, into their sub-row's list
+    // (merging into the list's last entry as fill_intersections does). Lane 0
+    // sorts, walks and writes the cells.
+    __shared__ int3 stage[SLOW_WARPS][4][32];
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t n_ovf = min(ctr->ovf2_count, ovf_cap);
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     uint32_t nonterm = 0;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_ovf; k += gridDim.x * blockDim.x) {
+    for (uint32_t k = blockIdx.x * (blockDim.x >> 5) + wib; k < n_ovf; k += warps) {
         const uint32_t p = ovf[k].x;
         const int32_t g = static_cast<int32_t>(ovf[k].y);
         const PathInfo P = info[p];
         const uint32_t ne = P.e_end - P.e_begin;
         // Four sub-row lists of up to ne entries, and one list of merge-sort temporary.
-        const uint32_t sb = atomicAdd(&ctr->scratch_cursor, 5u * ne);
+        uint32_t sb = 0;
+        if (lane == 0) sb = atomicAdd(&ctr->scratch_cursor, 5u * ne);
+        sb = __shfl_sync(0xffffffffu, sb, 0);
         if (static_cast<uint64_t>(sb) + 5ull * ne > scratch_cap) {
-            atomicOr(&ctr->err, ERR_SCRATCH_CAP);
+            if (lane == 0) atomicOr(&ctr->err, ERR_SCRATCH_CAP);
             continue;
         }
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
         const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
-        int n4[4] = {0, 0, 0, 0};
-        // One pass over the path's edges builds the four sub-rows' entry
-        // lists, each in edge order (merging into its own last entry);
-        // aligned 32-edge groups whose row bounds miss the pixel row are skipped.
         const int32_t rlo = max(4 * g, P.y0), rhi = min(4 * g + 3, P.y1);
-        for (uint32_t j = P.e_begin; j < P.e_end;) {
-            const uint32_t grp = j >> 5;
-            const uint32_t jend = min(P.e_end, (grp + 1) << 5);
-            if (gmax[grp] < rlo || gmin[grp] > rhi) {
-                j = jend;
-                continue;
-            }
-            for (; j < jend; ++j) {
+        // Lane s < 4: sub-row s's list length and its last entry (not yet stored).
+        int n_s = 0;
+        int3 last = make_int3(0, 0, 0);
+        bool has_last = false;
+        int3* const Ls = scratch + sb + min(lane, 3u) * ne;
+        for (uint32_t base = P.e_begin & ~31u; base < P.e_end; base += 32) {
+            const uint32_t grp = base >> 5;
+            if (gmax[grp] < rlo || gmin[grp] > rhi) continue;
+            const uint32_t j = base + lane;
+            uint32_t bits = 0;  // sub-rows this lane's edge has an entry in
+            if (j >= P.e_begin && j < P.e_end) {
                 const Edge E = edges[j];
-                if ((E.flags & EF_EMPTY) || E.row1 < rlo || E.row0 > rhi) continue;
-                const int32_t r0 = max(rlo, E.row0), r1 = min(rhi, E.row1);
-                for (int32_t r = r0; r <= r1; ++r) {
-                    const int sub = r - 4 * g;
-                    int3* L = scratch + sb + static_cast<uint32_t>(sub) * ne;
-                    int& n = n4[sub];
-                    int32_t elo, ehi, ec;
-                    edge_entry(E, r, elo, ehi, ec);
-                    if (n > 0 && sat_inc(L[n - 1].y) >= elo && L[n - 1].x <= sat_inc(ehi)) {
-                        L[n - 1].z = static_cast<int32_t>(static_cast<uint32_t>(L[n - 1].z) + static_cast<uint32_t>(ec));
-                        L[n - 1].x = min(L[n - 1].x, elo);
-                        L[n - 1].y = max(L[n - 1].y, ehi);
-                    } else {
-                        L[n++] = make_int3(elo, ehi, ec);
+                if (!(E.flags & EF_EMPTY) && E.row1 >= rlo && E.row0 <= rhi) {
+                    const int32_t r0 = max(rlo, E.row0), r1 = min(rhi, E.row1);
+                    for (int32_t r = r0; r <= r1; ++r) {
+                        int32_t elo, ehi, ec;
+                        edge_entry(E, r, elo, ehi, ec);
+                        stage[wib][r - 4 * g][lane] = make_int3(elo, ehi, ec);
+                        bits |= 1u << (r - 4 * g);
                     }
                 }
             }
+            const uint32_t m0 = __ballot_sync(0xffffffffu, bits & 1), m1 = __ballot_sync(0xffffffffu, bits & 2);
+            const uint32_t m2 = __ballot_sync(0xffffffffu, bits & 4), m3 = __ballot_sync(0xffffffffu, bits & 8);
+            __syncwarp();
+            if (lane < 4) {
+                uint32_t m = lane == 0 ? m0 : lane == 1 ? m1 : lane == 2 ? m2 : m3;
+                while (m) {
+                    const int q = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int3 e = stage[wib][lane][q];
+                    if (has_last && sat_inc(last.y) >= e.x && last.x <= sat_inc(e.y)) {
+                        last.z = static_cast<int32_t>(static_cast<uint32_t>(last.z) + static_cast<uint32_t>(e.z));
+                        last.x = min(last.x, e.x);
+                        last.y = max(last.y, e.y);
+                    } else {
+                        if (has_last) Ls[n_s++] = last;
+                        last = e;
+                        has_last = true;
+                    }
+                }
+            }
+            __syncwarp();
         }
+        if (lane < 4 && has_last) Ls[n_s++] = last;
+        int n4[4];
+#pragma unroll
+        for (int sub = 0; sub < 4; ++sub) n4[sub] = __shfl_sync(0xffffffffu, n_s, sub);
+        __syncwarp();
+        if (lane != 0) continue;
         for (int sub = 0; sub < 4; ++sub) {
             const int32_t r = 4 * g + sub;
             if (r < P.y0 || r > P.y1) continue;
