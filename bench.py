@@ -396,9 +396,18 @@ def run_rrb(args, rank, local, world):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
     h2d = sum(int(h[k].nbytes) for k in h) + int(host_page.nbytes)
+    # The host link alone: the same bytes as one pinned copy, for the bound e2e meets.
+    scratch = backend.alloc_device(int(h["pts"].nbytes))
+    backend.wait_transfer(backend.upload_async(scratch, h["pts"]))
+    t = time.perf_counter()
+    for _ in range(3):
+        backend.wait_transfer(backend.upload_async(scratch, h["pts"]))
+    link_gbs = 3 * h["pts"].nbytes / (time.perf_counter() - t) / 1e9
+    backend.free_device(scratch)
     e2e = {"value": job_px * e2e_steps / e2e_s / 1e6, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": int(host_page.nbytes), "steps": e2e_steps,
-           "api": "rrb_render_pages_host (C ABI), pinned host buffers"}
+           "api": "rrb_render_pages_host (C ABI), pinned host buffers",
+           "h2d_link_gbs": link_gbs, "h2d_bound_ms": h2d / link_gbs / 1e6}
 
     # ---- parity check and CPU baseline (rank 0, N = 1)
     gpu_page = np.empty(scene.arena_bytes, np.uint8)
