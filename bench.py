@@ -188,8 +188,21 @@ def run_reference(args, rank, world):
     import rr_oracle
     import rrb
     rr_oracle.build()
-    kw, desc = WORKLOADS[args.workload]
-    scene = rrb.Scene(**kw)
+    if args.workload == "fill_ops":
+        print(json.dumps({"impl": "reference", "unavailable": "the fill_ops line times aa_fill_cpu (the "
+                                                             "reference's own CPU coverage) as its cpu_baseline"}))
+        return
+    render = rr_oracle.render_scene
+    if args.workload == "strokes":
+        from rrb.strokes import StrokePage
+        scene = StrokePage(0, n_paths=args.paths or 20000)
+        desc = scene.description
+
+        def render(work, arena, threads=1):
+            return rr_oracle.render_scene_paint(work, arena, work.strokes, threads=threads)
+    else:
+        kw, desc = WORKLOADS[args.workload]
+        scene = rrb.Scene(**kw)
     sample_desc, work = "the page", scene
     px_per_copy = scene.pixels
     if scene.n_pages > 1:
@@ -211,8 +224,7 @@ def run_reference(args, rank, world):
     def step():
         for a in arenas:
             a.fill(255)
-        ts = [threading.Thread(target=rr_oracle.render_scene, args=(work, a), kwargs=dict(threads=1))
-              for a in arenas]
+        ts = [threading.Thread(target=render, args=(work, a), kwargs=dict(threads=1)) for a in arenas]
         t = time.perf_counter()
         for x in ts:
             x.start()
@@ -788,12 +800,12 @@ def main():
     rank, local, world = dist_env()
     if args.serving:
         run_serving(args, rank, world)
+    elif args.impl == "reference":
+        run_reference(args, rank, world)
     elif args.workload == "fill_ops":
         run_fill_ops(args, rank, world)
     elif args.workload == "strokes":
         run_strokes(args, rank, local, world)
-    elif args.impl == "reference":
-        run_reference(args, rank, world)
     else:
         run_rrb(args, rank, local, world)
 
