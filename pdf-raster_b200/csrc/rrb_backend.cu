@@ -527,8 +527,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         as<int4>(c->s_piece_box), as<unsigned long long>(c->s_piece_raw));
     c->launches += 1;
     k_group_bounds<<<grid_for(c, (n_edges + 31) / 32, 256), 256, 0, c->stream>>>(
-        as<uint32_t>(c->s_edge_off), as<int4>(c->s_piece_box), as<Edge>(c->s_edges), NPC,
-        static_cast<uint32_t>(n_edges), gmin, gmax);
+        as<uint32_t>(c->s_edge_off), as<int4>(c->s_piece_box), NPC, static_cast<uint32_t>(n_edges), gmin, gmax);
     c->launches += 1;
     stage_end(c, 3);
     const int chunk_rows = 32;

@@ -479,13 +479,12 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
 }
 
 // Row bounds of each aligned group of 32 edges (the skip test of the row
-// stage): min row0 / max row1 over the group's non-empty edges. A piece whose
-// edges all lie in the group contributes its row range; the edges of a piece
-// that straddles the group's ends are read. Thread per group; its pieces by
-// binary search in edge_off.
+// stage), from the row ranges of the pieces whose edges the group holds: a
+// superset of the group's own edge rows, which only makes the skip test
+// skip less. Thread per group; its pieces by binary search in edge_off.
 __global__ void k_group_bounds(const uint32_t* __restrict__ edge_off, const int4* __restrict__ piece_box,
-                               const Edge* __restrict__ edges, uint32_t n_pieces, uint32_t n_edges,
-                               int32_t* __restrict__ gmin, int32_t* __restrict__ gmax) {
+                               uint32_t n_pieces, uint32_t n_edges, int32_t* __restrict__ gmin,
+                               int32_t* __restrict__ gmax) {
     const uint32_t n_groups = (n_edges + 31) / 32;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
         const uint32_t e0 = 32 * g, e1 = min(e0 + 32, n_edges);
@@ -497,20 +496,10 @@ __global__ void k_group_bounds(const uint32_t* __restrict__ edge_off, const int4
         }
         int32_t g0 = INT32_MAX, g1 = INT32_MIN;
         for (uint32_t k = lo; k < n_pieces && edge_off[k] < e1; ++k) {
-            const uint32_t a = edge_off[k], b = edge_off[k + 1];
-            if (b <= e0) continue;
-            if (a >= e0 && b <= e1) {
-                const int4 bx = piece_box[k];
-                g0 = min(g0, bx.x);
-                g1 = max(g1, bx.y);
-            } else {
-                for (uint32_t j = max(a, e0); j < min(b, e1); ++j) {
-                    const Edge e = edges[j];
-                    if (e.flags & EF_EMPTY) continue;
-                    g0 = min(g0, e.row0);
-                    g1 = max(g1, e.row1);
-                }
-            }
+            if (edge_off[k + 1] <= e0) continue;
+            const int4 b = piece_box[k];
+            g0 = min(g0, b.x);
+            g1 = max(g1, b.y);
         }
         gmin[g] = g0;
         gmax[g] = g1;
