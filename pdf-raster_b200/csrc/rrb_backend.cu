@@ -524,10 +524,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     k_seg_write<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
         static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo,
-        as<int4>(c->s_piece_box), as<unsigned long long>(c->s_piece_raw));
-    c->launches += 1;
-    k_group_bounds<<<grid_for(c, (n_edges + 31) / 32, 256), 256, 0, c->stream>>>(
-        as<uint32_t>(c->s_edge_off), as<int4>(c->s_piece_box), NPC, static_cast<uint32_t>(n_edges), gmin, gmax);
+        as<int4>(c->s_piece_box), as<unsigned long long>(c->s_piece_raw), gmin, gmax);
     c->launches += 1;
     stage_end(c, 3);
     const int chunk_rows = 32;

@@ -187,13 +187,14 @@ __global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restr
 
 // Edge records per piece slot, at edge_off[slot].
 // With piece_box != nullptr it also reduces each piece's edges for
-// k_path_bbox_pieces and k_group_bounds (row range, AA column range, row
-// entries, sloped or not).
+// k_path_bbox_pieces (row range, AA column range, row entries, sloped or not)
+// and folds their rows into the 32-edge group bounds gmin / gmax.
 __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
                             uint32_t edge_cap, Edge* __restrict__ edges,
                             const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo,
-                            int4* __restrict__ piece_box = nullptr, unsigned long long* __restrict__ piece_raw = nullptr) {
+                            int4* __restrict__ piece_box = nullptr, unsigned long long* __restrict__ piece_raw = nullptr,
+                            int32_t* __restrict__ gmin = nullptr, int32_t* __restrict__ gmax = nullptr) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -211,6 +212,14 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
         int32_t by0 = INT32_MAX, by1 = INT32_MIN, bxl = INT32_MAX, bxh = INT32_MIN;
         unsigned long long raw = 0;
         bool sloped = false;
+        uint32_t grp = 0xffffffffu;
+        int32_t g0 = INT32_MAX, g1 = INT32_MIN;
+        auto flush_group = [&]() {
+            if (grp != 0xffffffffu && g0 <= g1) {
+                atomicMin(&gmin[grp], g0);
+                atomicMax(&gmax[grp], g1);
+            }
+        };
         auto put = [&](uint32_t k, const Edge& e) {
             edges[k] = e;
             if (!sum || (e.flags & EF_EMPTY)) return;
@@ -222,6 +231,15 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
             bxh = max(bxh, hi);
             raw += static_cast<unsigned long long>(e.row1 - e.row0 + 1);
             sloped = sloped || (e.flags & EF_KIND_MASK) == EK_SLOPED;
+            if ((k >> 5) != grp) {
+                flush_group();
+                grp = k >> 5;
+                g0 = e.row0;
+                g1 = e.row1;
+            } else {
+                g0 = min(g0, e.row0);
+                g1 = max(g1, e.row1);
+            }
         };
         if (kind == PK_LINE || kind == PK_CLOSE) {
             double x1, y1;
@@ -242,6 +260,7 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
             });
         }
         if (sum) {
+            flush_group();
             piece_box[s] = make_int4(by0, by1, bxl, bxh);
             piece_raw[s] = raw | (sloped ? (1ull << 63) : 0ull);
         }
@@ -478,38 +497,11 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
     }
 }
 
-// Row bounds of each aligned group of 32 edges (the skip test of the row
-// stage), from the row ranges of the pieces whose edges the group holds: a
-// superset of the group's own edge rows, which only makes the skip test
-// skip less. Thread per group; its pieces by binary search in edge_off.
-__global__ void k_group_bounds(const uint32_t* __restrict__ edge_off, const int4* __restrict__ piece_box,
-                               uint32_t n_pieces, uint32_t n_edges, int32_t* __restrict__ gmin,
-                               int32_t* __restrict__ gmax) {
-    const uint32_t n_groups = (n_edges + 31) / 32;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < n_groups; g += gridDim.x * blockDim.x) {
-        const uint32_t e0 = 32 * g, e1 = min(e0 + 32, n_edges);
-        uint32_t lo = 0, hi = n_pieces;  // the last piece whose first edge is <= e0
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (edge_off[mid] <= e0) lo = mid;
-            else hi = mid;
-        }
-        int32_t g0 = INT32_MAX, g1 = INT32_MIN;
-        for (uint32_t k = lo; k < n_pieces && edge_off[k] < e1; ++k) {
-            if (edge_off[k + 1] <= e0) continue;
-            const int4 b = piece_box[k];
-            g0 = min(g0, b.x);
-            g1 = max(g1, b.y);
-        }
-        gmin[g] = g0;
-        gmax[g] = g1;
-    }
-}
-
 // The same PathInfo from the per-piece reductions k_seg_write leaves
 // (piece_box = (y0, y1, xl, xh) of the piece's non-empty edges, piece_raw =
 // their row entries, bit 63 set when one is sloped): one warp per path reads
-// 24 bytes per piece instead of 32 per edge.
+// 24 bytes per piece instead of 32 per edge. The 32-edge group bounds were
+// taken by k_seg_write too.
 __global__ void k_path_bbox_pieces(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
                                    const int4* __restrict__ piece_box, const unsigned long long* __restrict__ piece_raw,
                                    uint32_t n_paths, const uint8_t* __restrict__ rule,
