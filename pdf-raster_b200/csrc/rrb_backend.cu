@@ -65,7 +65,7 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
-    Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip, s_piece_box, s_piece_raw;
+    Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
@@ -518,22 +518,19 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     // 0x7f7f7f7f / 0x80808080: beyond any AA row, so they act as +inf / -inf.
     RRB_CUDA(c, cudaMemsetAsync(gmin, 0x7f, n_egroups * sizeof(int32_t), c->stream));
     RRB_CUDA(c, cudaMemsetAsync(gmax, 0x80, n_egroups * sizeof(int32_t), c->stream));
-    if ((rc = ensure(c, c->s_piece_box, std::max<uint64_t>(1, n_pieces) * sizeof(int4)))) return rc;
-    if ((rc = ensure(c, c->s_piece_raw, std::max<uint64_t>(1, n_pieces) * sizeof(unsigned long long)))) return rc;
     stage(c, 3);
     k_seg_write<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
-        static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo,
-        as<int4>(c->s_piece_box), as<unsigned long long>(c->s_piece_raw), gmin, gmax);
+        static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo);
     c->launches += 1;
     stage_end(c, 3);
     const int chunk_rows = 32;
     stage(c, 4);
-    k_path_bbox_pieces<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(
-        as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<int4>(c->s_piece_box),
-        as<unsigned long long>(c->s_piece_raw), NP, as<uint8_t>(B->rule), as<uint8_t>(B->gray), as<uint8_t>(B->alpha),
-        as<uint32_t>(B->page), as<uint32_t>(B->pw), as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info),
-        as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks), chunk_rows, as<BatchCounters>(c->s_ctr), pclip);
+    k_path_bbox<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(
+        as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
+        as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
+        as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
+        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax, pclip);
     c->launches += 1;
     // Hairline segments: their layers' PathInfo and run counts (before the
     // binning, which reads the layers' rectangles).
@@ -750,7 +747,7 @@ void release_scratch(rrb_ctx* c) {
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
                       &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
-                      &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip, &c->s_piece_box, &c->s_piece_raw};
+                      &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip};
     for (Scratch* x : all) {
         dev_free(c, x->p, x->cap);
         x->p = nullptr;

@@ -186,15 +186,10 @@ __global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restr
 }
 
 // Edge records per piece slot, at edge_off[slot].
-// With piece_box != nullptr it also reduces each piece's edges for
-// k_path_bbox_pieces (row range, AA column range, row entries, sloped or not)
-// and folds their rows into the 32-edge group bounds gmin / gmax.
 __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
                             uint32_t edge_cap, Edge* __restrict__ edges,
-                            const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo,
-                            int4* __restrict__ piece_box = nullptr, unsigned long long* __restrict__ piece_raw = nullptr,
-                            int32_t* __restrict__ gmin = nullptr, int32_t* __restrict__ gmax = nullptr) {
+                            const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -208,43 +203,10 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
         uint32_t j = pc.y & 0x3fffffffu;
         double x0, y0;
         load_tpt(pts, m, pc.x, x0, y0);
-        const bool sum = piece_box != nullptr;
-        int32_t by0 = INT32_MAX, by1 = INT32_MIN, bxl = INT32_MAX, bxh = INT32_MIN;
-        unsigned long long raw = 0;
-        bool sloped = false;
-        uint32_t grp = 0xffffffffu;
-        int32_t g0 = INT32_MAX, g1 = INT32_MIN;
-        auto flush_group = [&]() {
-            if (grp != 0xffffffffu && g0 <= g1) {
-                atomicMin(&gmin[grp], g0);
-                atomicMax(&gmax[grp], g1);
-            }
-        };
-        auto put = [&](uint32_t k, const Edge& e) {
-            edges[k] = e;
-            if (!sum || (e.flags & EF_EMPTY)) return;
-            int32_t lo, hi;
-            edge_xrange(e, lo, hi);
-            by0 = min(by0, e.row0);
-            by1 = max(by1, e.row1);
-            bxl = min(bxl, lo);
-            bxh = max(bxh, hi);
-            raw += static_cast<unsigned long long>(e.row1 - e.row0 + 1);
-            sloped = sloped || (e.flags & EF_KIND_MASK) == EK_SLOPED;
-            if ((k >> 5) != grp) {
-                flush_group();
-                grp = k >> 5;
-                g0 = e.row0;
-                g1 = e.row1;
-            } else {
-                g0 = min(g0, e.row0);
-                g1 = max(g1, e.row1);
-            }
-        };
         if (kind == PK_LINE || kind == PK_CLOSE) {
             double x1, y1;
             load_tpt(pts, m, j, x1, y1);
-            if (base < edge_cap) put(base, make_edge(x0, y0, x1, y1, clo, chi));
+            if (base < edge_cap) edges[base] = make_edge(x0, y0, x1, y1, clo, chi);
         } else {
             double x1, y1, x2, y2, x3, y3;
             load_tpt(pts, m, j, x1, y1);
@@ -253,16 +215,11 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
             double cx = x0, cy = y0;
             uint32_t k = base;
             flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [&](double fx, double fy) {
-                if (k < edge_cap) put(k, make_edge(cx, cy, fx, fy, clo, chi));
+                if (k < edge_cap) edges[k] = make_edge(cx, cy, fx, fy, clo, chi);
                 ++k;
                 cx = fx;
                 cy = fy;
             });
-        }
-        if (sum) {
-            flush_group();
-            piece_box[s] = make_int4(by0, by1, bxl, bxh);
-            piece_raw[s] = raw | (sloped ? (1ull << 63) : 0ull);
         }
     }
 }
@@ -353,74 +310,6 @@ __global__ void k_scan_down(const uint32_t* __restrict__ in, uint32_t* __restric
     if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = block_sums[SCAN_MAX_BLOCKS];
 }
 
-// The PathInfo of path p from its edges' reductions (row range y0..y1, AA
-// column range xl..xh, raw row entries, all edges axis-aligned), with its
-// pixel rectangle under the clip and row map, and its row-stage sizes.
-__device__ __forceinline__ void write_path_info(uint32_t p, uint32_t eb, uint32_t ee, int32_t y0, int32_t y1,
-                                                int32_t xl, int32_t xh, unsigned long long raw, bool axis_only,
-                                                const uint8_t* __restrict__ rule, const uint8_t* __restrict__ gray,
-                                                const uint8_t* __restrict__ alpha, const uint32_t* __restrict__ path_page,
-                                                const uint32_t* __restrict__ page_w, const uint32_t* __restrict__ page_h,
-                                                int rowmap, PathInfo* __restrict__ info,
-                                                uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
-                                                int chunk_rows, BatchCounters* __restrict__ ctr,
-                                                const int4* __restrict__ path_clip) {
-    if (raw) atomicAdd(&ctr->raw_entries, raw);
-    if (y0 <= y1) atomicAdd(&ctr->aa_rows, static_cast<unsigned long long>(y1 - y0 + 1));
-    uint32_t pg = path_page[p];
-    int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
-    PathInfo pi;
-    pi.e_begin = eb;
-    pi.e_end = ee;
-    pi.paint = uint32_t(gray[p]) | (uint32_t(alpha[p]) << 8) | (uint32_t(rule[p] ? 1 : 0) << 16);
-    pi.page = pg;
-    pi.run_off = pi.run_cnt = 0;
-    pi.bx0 = 1;
-    pi.bx1 = 0;
-    pi.by0 = 1;
-    pi.by1 = 0;
-    const bool recti = axis_only && y0 <= y1 && ee - eb <= RECTI_MAX_EDGES;
-    if (recti) pi.paint |= PI_RECTI;
-    uint32_t rows = 0, groups = 0;
-    if (y0 <= y1) {
-        pi.y0 = y0;
-        pi.y1 = y1;
-        rows = static_cast<uint32_t>(y1 - (y0 & ~3) + 1);     // rows of the 4-aligned chunks
-        groups = static_cast<uint32_t>((y1 >> 2) - (y0 >> 2) + 1);
-        // Pixel columns: spans cover AA columns [max(x0, lo), min(x1+1, hi)).
-        const int4 clp = path_clip_of(path_clip, p, 4 * W, 4 * H);
-        int32_t cl = max(xl, clp.x), ch = min(xh, clp.y - 1);
-        pi.px0 = cl >> 2;
-        pi.px1 = ch >> 2;
-        if (xh < clp.x || xl >= clp.y || clp.x >= clp.y) {
-            pi.px0 = 1;
-            pi.px1 = 0;
-        }
-        // Pixel rows under the row map.
-        if (rowmap == 0) {
-            pi.py0 = y0 >> 2;
-            pi.py1 = y1 >> 2;
-        } else {
-            pi.py0 = y0 >> 2;
-            int32_t t = y1 - 12;
-            pi.py1 = t >= 0 ? (t >> 4) : -1;
-        }
-        pi.py0 = max(pi.py0, 0);
-        pi.py1 = min(pi.py1, H - 1);
-    } else {
-        pi.y0 = 1;
-        pi.y1 = 0;
-        pi.px0 = 1;
-        pi.px1 = 0;
-        pi.py0 = 1;
-        pi.py1 = 0;
-    }
-    info[p] = pi;
-    // Rectilinear paths skip the row stage: k_recti builds their row runs.
-    path_groups[p] = recti ? 0u : groups;
-    path_chunks[p] = recti ? 0u : (rows + chunk_rows - 1) / chunk_rows;
-}
-
 // ---------------------------------------------------------------------------
 // Path bounding box (XPathScanner::new, scanner/mod.rs:131-180): one warp per
 // path reduces its edges to the AA row range and AA column range, then maps
@@ -491,55 +380,62 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
             xh = max(xh, __shfl_xor_sync(0xffffffffu, xh, o));
             raw += __shfl_xor_sync(0xffffffffu, raw, o);
         }
-        if (lane == 0)
-            write_path_info(p, eb, ee, y0, y1, xl, xh, raw, axis_only, rule, gray, alpha, path_page, page_w, page_h,
-                            rowmap, info, path_groups, path_chunks, chunk_rows, ctr, path_clip);
-    }
-}
-
-// The same PathInfo from the per-piece reductions k_seg_write leaves
-// (piece_box = (y0, y1, xl, xh) of the piece's non-empty edges, piece_raw =
-// their row entries, bit 63 set when one is sloped): one warp per path reads
-// 24 bytes per piece instead of 32 per edge. The 32-edge group bounds were
-// taken by k_seg_write too.
-__global__ void k_path_bbox_pieces(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
-                                   const int4* __restrict__ piece_box, const unsigned long long* __restrict__ piece_raw,
-                                   uint32_t n_paths, const uint8_t* __restrict__ rule,
-                                   const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha,
-                                   const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
-                                   const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
-                                   uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
-                                   int chunk_rows, BatchCounters* __restrict__ ctr, const int4* __restrict__ path_clip) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t p = warp_g; p < n_paths; p += nwarps) {
-        const uint32_t pb = piece_off[p], pe = piece_off[p + 1];
-        int32_t y0 = INT32_MAX, y1 = INT32_MIN, xl = INT32_MAX, xh = INT32_MIN;
-        unsigned long long raw = 0;
-        bool axis_only = true;
-        for (uint32_t k = pb + lane; k < pe; k += 32) {
-            const int4 b = piece_box[k];
-            const unsigned long long r = piece_raw[k];
-            y0 = min(y0, b.x);
-            y1 = max(y1, b.y);
-            xl = min(xl, b.z);
-            xh = max(xh, b.w);
-            raw += r & ~(1ull << 63);
-            axis_only = axis_only && !(r >> 63);
+        if (lane == 0) {
+            if (raw) atomicAdd(&ctr->raw_entries, raw);
+            if (y0 <= y1) atomicAdd(&ctr->aa_rows, static_cast<unsigned long long>(y1 - y0 + 1));
+            uint32_t pg = path_page[p];
+            int32_t W = static_cast<int32_t>(page_w[pg]), H = static_cast<int32_t>(page_h[pg]);
+            PathInfo pi;
+            pi.e_begin = eb;
+            pi.e_end = ee;
+            pi.paint = uint32_t(gray[p]) | (uint32_t(alpha[p]) << 8) | (uint32_t(rule[p] ? 1 : 0) << 16);
+            pi.page = pg;
+            pi.run_off = pi.run_cnt = 0;
+            pi.bx0 = 1;
+            pi.bx1 = 0;
+            pi.by0 = 1;
+            pi.by1 = 0;
+            const bool recti = axis_only && y0 <= y1 && ee - eb <= RECTI_MAX_EDGES;
+            if (recti) pi.paint |= PI_RECTI;
+            uint32_t rows = 0, groups = 0;
+            if (y0 <= y1) {
+                pi.y0 = y0;
+                pi.y1 = y1;
+                rows = static_cast<uint32_t>(y1 - (y0 & ~3) + 1);     // rows of the 4-aligned chunks
+                groups = static_cast<uint32_t>((y1 >> 2) - (y0 >> 2) + 1);
+                // Pixel columns: spans cover AA columns [max(x0, lo), min(x1+1, hi)).
+                const int4 clp = path_clip_of(path_clip, p, 4 * W, 4 * H);
+                int32_t cl = max(xl, clp.x), ch = min(xh, clp.y - 1);
+                pi.px0 = cl >> 2;
+                pi.px1 = ch >> 2;
+                if (xh < clp.x || xl >= clp.y || clp.x >= clp.y) {
+                    pi.px0 = 1;
+                    pi.px1 = 0;
+                }
+                // Pixel rows under the row map.
+                if (rowmap == 0) {
+                    pi.py0 = y0 >> 2;
+                    pi.py1 = y1 >> 2;
+                } else {
+                    pi.py0 = y0 >> 2;
+                    int32_t t = y1 - 12;
+                    pi.py1 = t >= 0 ? (t >> 4) : -1;
+                }
+                pi.py0 = max(pi.py0, 0);
+                pi.py1 = min(pi.py1, H - 1);
+            } else {
+                pi.y0 = 1;
+                pi.y1 = 0;
+                pi.px0 = 1;
+                pi.px1 = 0;
+                pi.py0 = 1;
+                pi.py1 = 0;
+            }
+            info[p] = pi;
+            // Rectilinear paths skip the row stage: k_recti builds their row runs.
+            path_groups[p] = recti ? 0u : groups;
+            path_chunks[p] = recti ? 0u : (rows + chunk_rows - 1) / chunk_rows;
         }
-        for (int o = 16; o; o >>= 1) {
-            y0 = min(y0, __shfl_xor_sync(0xffffffffu, y0, o));
-            y1 = max(y1, __shfl_xor_sync(0xffffffffu, y1, o));
-            xl = min(xl, __shfl_xor_sync(0xffffffffu, xl, o));
-            xh = max(xh, __shfl_xor_sync(0xffffffffu, xh, o));
-            raw += __shfl_xor_sync(0xffffffffu, raw, o);
-        }
-        axis_only = __all_sync(0xffffffffu, axis_only);
-        if (lane == 0)
-            write_path_info(p, edge_off[pb], edge_off[pe], y0, y1, xl, xh, raw, axis_only, rule, gray, alpha,
-                            path_page, page_w, page_h, rowmap, info, path_groups, path_chunks, chunk_rows, ctr,
-                            path_clip);
     }
 }
 
