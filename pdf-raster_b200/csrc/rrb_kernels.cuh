@@ -100,21 +100,6 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
         uint32_t slot = off;
         uint32_t i = 0;
         if (rule && rule[p] == RULE_HAIRLINE) n = 0;  // hairline segments have no fill edges
-        // The closing segment of a subpath depends on its transformed end
-        // points; their loads are issued when the subpath ends and the test
-        // is made one subpath later, so the loads' latency overlaps the next
-        // subpath's walk instead of stalling it. The slot is reserved at once
-        // and becomes an empty piece (PK_NONE) when no closing segment is due.
-        bool pend = false;
-        uint32_t pend_slot = 0;
-        double psx = 0, psy = 0, pcx = 0, pcy = 0;
-        auto resolve = [&]() {
-            double sx, sy, cx, cy;
-            transform(m, psx, psy, sx, sy);
-            transform(m, pcx, pcy, cx, cy);
-            if (!(fabs(dsub(cx, sx)) > 1e-10 || fabs(dsub(cy, sy)) > 1e-10))
-                pieces[pend_slot] = make_uint2(0u, PK_NONE << 30);
-        };
         while (i < n) {
             if (flags[off + i] & PF_FIRST) {
                 uint32_t sp = i, cur = i;
@@ -133,19 +118,15 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
                         if (f & PF_LAST) break;
                     }
                 }
-                if (pend) resolve();
-                pend = true;
-                pend_slot = slot;
-                pieces[slot++] = make_uint2(off + cur, (PK_CLOSE << 30) | (off + sp));
-                psx = pts[2 * (off + sp)];
-                psy = pts[2 * (off + sp) + 1];
-                pcx = pts[2 * (off + cur)];
-                pcy = pts[2 * (off + cur) + 1];
+                double sx, sy, cx, cy;
+                transform(m, pts[2 * (off + sp)], pts[2 * (off + sp) + 1], sx, sy);
+                transform(m, pts[2 * (off + cur)], pts[2 * (off + cur) + 1], cx, cy);
+                if (fabs(dsub(cx, sx)) > 1e-10 || fabs(dsub(cy, sy)) > 1e-10)
+                    pieces[slot++] = make_uint2(off + cur, (PK_CLOSE << 30) | (off + sp));
             } else {
                 ++i;
             }
         }
-        if (pend) resolve();
         path_pieces[p] = slot - off;
     }
 }
