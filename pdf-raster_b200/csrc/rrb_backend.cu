@@ -487,7 +487,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if (pclip && (rc = ensure(c, c->s_clip_lo, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
     uint32_t* clip_lo = pclip ? as<uint32_t>(c->s_clip_lo) : nullptr;
     if ((rc = ensure(c, c->s_edge_off, (n_pieces + 1) * sizeof(uint32_t)))) return rc;
-    k_compact_pieces<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(
+    k_compact_pieces<<<grid_for(c, n_paths * 32, 256, 16), 256, 0, c->stream>>>(
         as<uint64_t>(B->off), as<uint32_t>(c->s_path_pieces), NP, as<uint32_t>(B->page), as<uint32_t>(B->ph),
         as<uint2>(c->s_slots), as<uint2>(c->s_pieces), as<uint32_t>(c->s_clip), pclip, clip_lo);
     c->launches += 1;

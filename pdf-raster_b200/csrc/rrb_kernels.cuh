@@ -139,7 +139,11 @@ __global__ void k_compact_pieces(const uint64_t* __restrict__ path_pt_off, const
                                  const uint32_t* __restrict__ page_h, const uint2* __restrict__ slots,
                                  uint2* __restrict__ pieces, uint32_t* __restrict__ piece_clip,
                                  const int4* __restrict__ path_clip, uint32_t* __restrict__ piece_clip_lo) {
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
+    // One warp per path: its lanes copy the pieces (long stroke outlines have
+    // thousands) in coalesced strides.
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_paths; p += warps) {
         const uint32_t src = static_cast<uint32_t>(path_pt_off[p]);
         const uint32_t dst = piece_off[p], n = piece_off[p + 1] - dst;
         uint32_t clip_hi = 4u * page_h[path_page[p]] - 1u, clip_lo = 0;
@@ -148,7 +152,7 @@ __global__ void k_compact_pieces(const uint64_t* __restrict__ path_pt_off, const
             clip_lo = static_cast<uint32_t>(cl.z);
             clip_hi = static_cast<uint32_t>(cl.w);
         }
-        for (uint32_t k = 0; k < n; ++k) {
+        for (uint32_t k = lane; k < n; k += 32) {
             pieces[dst + k] = slots[src + k];
             piece_clip[dst + k] = clip_hi;
             if (piece_clip_lo) piece_clip_lo[dst + k] = clip_lo;
