@@ -471,11 +471,19 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if ((rc = ensure(c, c->s_ctr, sizeof(BatchCounters)))) return rc;
     RRB_CUDA(c, cudaMemsetAsync(c->s_ctr.p, 0, sizeof(BatchCounters), c->stream));
     stage(c, 0);
+    // Paths of up to kLongWalk points: a thread each; longer ones: a warp each.
+    constexpr uint32_t kLongWalk = 64;
     k_walk<<<grid_for(c, n_paths, 128, 32), 128, 0, c->stream>>>(as<double>(B->pts), as<uint8_t>(B->flags),
                                                              as<uint64_t>(B->off), NP, as<double>(B->mtx),
                                                              as<uint32_t>(B->page), as<uint32_t>(B->ph),
                                                              as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces),
-                                                             B->has_hairline ? as<uint8_t>(B->rule) : nullptr);
+                                                             B->has_hairline ? as<uint8_t>(B->rule) : nullptr,
+                                                             kLongWalk);
+    c->launches += 1;
+    k_walk_long<<<grid_for(c, n_paths * 32, 256, 16), 256, 0, c->stream>>>(
+        as<double>(B->pts), as<uint8_t>(B->flags), as<uint64_t>(B->off), NP, as<double>(B->mtx),
+        as<uint2>(c->s_slots), as<uint32_t>(c->s_path_pieces), B->has_hairline ? as<uint8_t>(B->rule) : nullptr,
+        kLongWalk);
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
     if ((rc = scan_u32(c, as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_path_pieces), NP))) return rc;

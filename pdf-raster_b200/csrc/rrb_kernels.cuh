@@ -90,13 +90,15 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
                        const uint64_t* __restrict__ path_pt_off, uint32_t n_paths,
                        const double* __restrict__ mtx, const uint32_t* __restrict__ path_page,
                        const uint32_t* __restrict__ page_h, uint2* __restrict__ pieces,
-                       uint32_t* __restrict__ path_pieces, const uint8_t* __restrict__ rule) {
+                       uint32_t* __restrict__ path_pieces, const uint8_t* __restrict__ rule,
+                       uint32_t long_min = 0xffffffffu) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n_paths; p += gridDim.x * blockDim.x) {
         uint32_t off = static_cast<uint32_t>(path_pt_off[p]);
         uint32_t n = static_cast<uint32_t>(path_pt_off[p + 1]) - off;
+        if (n >= long_min) continue;  // walked by k_walk_long
         uint32_t slot = off;
         uint32_t i = 0;
         if (rule && rule[p] == RULE_HAIRLINE) n = 0;  // hairline segments have no fill edges
@@ -128,6 +130,154 @@ __global__ void k_walk(const double* __restrict__ pts, const uint8_t* __restrict
             }
         }
         path_pieces[p] = slot - off;
+    }
+}
+
+// The same walk for paths of at least long_min points, one warp per path.
+// A serial walk of a long path (stroke outlines have thousands of points)
+// keeps one lane busy while its warp's other paths are done, and its lanes
+// diverge at every subpath end. Here each point's part in the walk is read
+// from its neighbours' flags, which is exact when the path is well formed:
+// it starts with FIRST; CURVE points come in pairs after a non-CURVE point
+// and before a non-CURVE end point; no FIRST point is a control or end point;
+// no two consecutive points are FIRST; and a point after which the walk
+// breaks (an inner line point with LAST) is followed by a FIRST point. Then
+// the walk examines every point but control and end points of curves:
+//   start (FIRST, and the first point or just after a break): no piece;
+//   first control point of a curve: CURVE piece from the point before;
+//   any other examined point: LINE piece from the point before, and a break
+//   when it has LAST (the end point of a curve is never tested for LAST,
+//   xpath.rs:210-234);
+// and the closing test of a walk-subpath runs at each break and at the last
+// point, against the latest start. The warp scans 32 points at a time for
+// the latest start and the piece slots. A path that is not well formed is
+// walked serially by lane 0.
+__global__ void k_walk_long(const double* __restrict__ pts, const uint8_t* __restrict__ flags,
+                            const uint64_t* __restrict__ path_pt_off, uint32_t n_paths,
+                            const double* __restrict__ mtx, uint2* __restrict__ pieces,
+                            uint32_t* __restrict__ path_pieces, const uint8_t* __restrict__ rule,
+                            uint32_t long_min) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_paths; p += warps) {
+        const uint32_t off = static_cast<uint32_t>(path_pt_off[p]);
+        const uint32_t n = static_cast<uint32_t>(path_pt_off[p + 1]) - off;
+        if (n < long_min) continue;
+        if (rule && rule[p] == RULE_HAIRLINE) {
+            if (lane == 0) path_pieces[p] = 0;
+            continue;
+        }
+        const uint8_t* F = flags + off;
+        auto fl = [&](int64_t i) -> uint32_t { return (i >= 0 && i < static_cast<int64_t>(n)) ? F[i] : 0u; };
+        // Well-formedness, 32 points at a time.
+        bool ok = true;
+        for (uint32_t b = 0; b < n && ok; b += 32) {
+            const int64_t i = static_cast<int64_t>(b) + lane;
+            bool good = true;
+            if (i < static_cast<int64_t>(n)) {
+                const uint32_t f0 = fl(i), fm1 = fl(i - 1), fm2 = fl(i - 2), fp1 = fl(i + 1), fp2 = fl(i + 2);
+                const bool curve = f0 & PF_CURVE, pc = fm1 & PF_CURVE;
+                const bool ctrl1 = curve && !pc, ctrl2 = curve && pc, endpt = !curve && pc;
+                const bool lin = !curve && !endpt;
+                const bool prev_lin = i >= 1 && !pc && !(fm2 & PF_CURVE);
+                const bool start = (f0 & PF_FIRST) && (i == 0 || (prev_lin && (fm1 & PF_LAST)));
+                if (i == 0 && !(f0 & PF_FIRST)) good = false;
+                if ((f0 & PF_FIRST) && (curve || endpt)) good = false;
+                if (ctrl1 && !(i >= 1 && i + 2 < static_cast<int64_t>(n) && (fp1 & PF_CURVE) && !(fp2 & PF_CURVE)))
+                    good = false;
+                if (ctrl2 && !(i >= 2 && !(fm2 & PF_CURVE))) good = false;
+                if ((f0 & PF_FIRST) && (fm1 & PF_FIRST) && i >= 1) good = false;
+                if (lin && !start && (f0 & PF_LAST) && i + 1 < static_cast<int64_t>(n) && !(fp1 & PF_FIRST))
+                    good = false;
+            }
+            ok = __all_sync(0xffffffffu, good);
+        }
+        if (!ok) {
+            // Serial walk of a path that is not well formed (the k_walk loop).
+            if (lane == 0) {
+                uint32_t slot = off, i = 0;
+                while (i < n) {
+                    if (F[i] & PF_FIRST) {
+                        uint32_t sp = i, cur = i;
+                        ++i;
+                        while (i < n) {
+                            const uint8_t f = F[i];
+                            if (f & PF_CURVE) {
+                                if (i + 2 >= n) break;
+                                pieces[slot++] = make_uint2(off + cur, (PK_CURVE << 30) | (off + i));
+                                cur = i + 2;
+                                i += 3;
+                            } else {
+                                pieces[slot++] = make_uint2(off + cur, (PK_LINE << 30) | (off + i));
+                                cur = i;
+                                ++i;
+                                if (f & PF_LAST) break;
+                            }
+                        }
+                        double sx, sy, cx, cy;
+                        transform(m, pts[2 * (off + sp)], pts[2 * (off + sp) + 1], sx, sy);
+                        transform(m, pts[2 * (off + cur)], pts[2 * (off + cur) + 1], cx, cy);
+                        if (fabs(dsub(cx, sx)) > 1e-10 || fabs(dsub(cy, sy)) > 1e-10)
+                            pieces[slot++] = make_uint2(off + cur, (PK_CLOSE << 30) | (off + sp));
+                    } else {
+                        ++i;
+                    }
+                }
+                path_pieces[p] = slot - off;
+            }
+            continue;
+        }
+        uint32_t slot_base = off;
+        int64_t last_start = -1;
+        for (uint32_t b = 0; b < n; b += 32) {
+            const int64_t i = static_cast<int64_t>(b) + lane;
+            const bool valid = i < static_cast<int64_t>(n);
+            bool piece = false, is_curve = false, close_ev = false, start = false;
+            if (valid) {
+                const uint32_t f0 = fl(i), fm1 = fl(i - 1), fm2 = fl(i - 2);
+                const bool curve = f0 & PF_CURVE, pc = fm1 & PF_CURVE;
+                const bool ctrl1 = curve && !pc, endpt = !curve && pc;
+                const bool lin = !curve && !endpt;
+                const bool prev_lin = i >= 1 && !pc && !(fm2 & PF_CURVE);
+                start = (f0 & PF_FIRST) && (i == 0 || (prev_lin && (fm1 & PF_LAST)));
+                is_curve = ctrl1;
+                piece = ctrl1 || (lin && !start);
+                const bool brk = lin && !start && (f0 & PF_LAST);
+                close_ev = brk || (i == static_cast<int64_t>(n) - 1);
+            }
+            // The latest start at or before each point.
+            int64_t sp = start ? i : -1;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t t = __shfl_up_sync(0xffffffffu, sp, o);
+                if (static_cast<int>(lane) >= o) sp = max(sp, t);
+            }
+            sp = max(sp, last_start);
+            bool close = false;
+            if (close_ev && sp >= 0) {
+                double sx, sy, cx, cy;
+                transform(m, pts[2 * (off + sp)], pts[2 * (off + sp) + 1], sx, sy);
+                transform(m, pts[2 * (off + i)], pts[2 * (off + i) + 1], cx, cy);
+                close = fabs(dsub(cx, sx)) > 1e-10 || fabs(dsub(cy, sy)) > 1e-10;
+            }
+            const uint32_t cnt = (piece ? 1u : 0u) + (close ? 1u : 0u);
+            uint32_t incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (static_cast<int>(lane) >= o) incl += t;
+            }
+            uint32_t at = slot_base + incl - cnt;
+            if (piece)
+                pieces[at++] = make_uint2(off + static_cast<uint32_t>(i - 1),
+                                          ((is_curve ? PK_CURVE : PK_LINE) << 30) | (off + static_cast<uint32_t>(i)));
+            if (close)
+                pieces[at] = make_uint2(off + static_cast<uint32_t>(i), (PK_CLOSE << 30) | (off + static_cast<uint32_t>(sp)));
+            slot_base += __shfl_sync(0xffffffffu, incl, 31);
+            last_start = __shfl_sync(0xffffffffu, sp, 31);
+        }
+        if (lane == 0) path_pieces[p] = slot_base - off;
     }
 }
 
