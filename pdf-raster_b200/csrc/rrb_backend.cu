@@ -43,7 +43,7 @@ struct Scratch {
     size_t cap = 0;
 };
 
-constexpr int KCAP = 16;        // merged Intersect entries per AA row kept in shared memory
+constexpr int KCAP = 12;        // merged Intersect entries per AA row kept in shared memory
 constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
 
 }  // namespace

@@ -677,7 +677,7 @@ __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* _
 // The merged list lives in shared memory (KCAP entries per row); rows that
 // overflow go to k_rows_slow.
 // ---------------------------------------------------------------------------
-constexpr int ROWS_WARPS = 4;
+constexpr int ROWS_WARPS = 8;
 
 // 32x32 bit-matrix transpose across a warp: on entry bit j of lane i is
 // A[i][j]; on exit bit j of lane i is A[j][i]. Five butterfly stages, each
