@@ -108,7 +108,7 @@ class Clocks:
 # kernel on the glyph page reduced to 30,000 paths (10,979,156 segments, edge
 # records larger than L2), scaled to a full launch by its segment count.
 GLYPH_DRAM_BYTES_PER_SEGMENT = {
-    "rows": (387_620_864 + 43_667_712) / 10_979_156,
+    "rows": (386_763_520 + 43_189_504) / 10_979_156,
     "seg_write": (169_890_304 + 404_720_384) / 10_979_156,
 }
 
