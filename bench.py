@@ -602,7 +602,8 @@ def run_strokes(args, rank, local, world):
             "config": {"workload": page.description, "paths": page.n_paths, "pages": 1, "rowmap": "documented",
                        "l2": "outlines and edge records larger than L2",
                        "parallelism": f"replicas x{world} (the page on every GPU)"},
-            "device_ms_per_step": device_ms, "outline_segments_per_step": stats["segments"],
+            "device_ms_per_step": device_ms, "host_ms_per_step": stats["host_ns"] / 1e6,
+            "outline_segments_per_step": stats["segments"],
             "p50_page_ms": p50, "p99_page_ms": p99, "bit_exact": bit_exact, "roofline": roofline,
             "stages_ms": stage_ms, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         }), flush=True)

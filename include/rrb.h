@@ -360,6 +360,8 @@ typedef struct {
     uint64_t kernel_launches;               /* kernels launched by the last record call */
     uint64_t scratch_grows;                 /* scratch buffers the call had to (re)allocate */
     uint64_t waves;                         /* page groups the batch was rendered in */
+    uint64_t host_ns;                       /* host time of the call before its first kernel: validation,
+                                               stroke outlines, staging and enqueued uploads */
 } rrb_batch_stats;
 int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
 

@@ -1069,15 +1069,22 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
 // stream: allow the streamed form. Paint batches do not stream: their points
 // are built on the host first, and their slow rows (one thread per row, a
 // few long ones) cost more split over ranges than the copy they would hide.
+// t0: when the caller's own host work began (default: now); the stats'
+// host_ns is the time from it to the first kernel.
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
-              const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false, bool stream = true) {
+              const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false, bool stream = true,
+              const std::chrono::steady_clock::time_point* t0 = nullptr) {
+    const auto start = t0 ? *t0 : std::chrono::steady_clock::now();
     rrb_batch* B = c->tmp_batch;
     const bool streamed = stream && h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
                           page_locked(h->flags);
     int rc = batch_upload(c, h, B, rgb, clip, hairlines, streamed);
     if (rc) return rc;
-    if (streamed) return run_streamed(c, h, B, arena, arena_len);
-    return run_resident(c, B, arena, arena_len, h->rowmap);
+    const uint64_t host_ns = static_cast<uint64_t>(
+        std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start).count());
+    rc = streamed ? run_streamed(c, h, B, arena, arena_len) : run_resident(c, B, arena, arena_len, h->rowmap);
+    c->stats.host_ns = host_ns;
+    return rc;
 }
 
 // Page-locked host memory for the paint batch arrays: the upload of the
@@ -1094,6 +1101,7 @@ struct PinnedAlloc : rrb_stroke::HostAlloc {
 
 int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_params* sp, const uint8_t* path_rgb,
                 const double* clip_rects) {
+    const auto t0 = std::chrono::steady_clock::now();
     std::string msg;
     if (!c->paint) c->paint = new rrb_stroke::PaintBatch();
     rrb_stroke::PaintBatch& pb = *c->paint;
@@ -1112,7 +1120,7 @@ int paint_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rrb_stroke_par
     q.path_page = pb.page.p;
     q.n_paths = pb.n_paths;
     return run_batch(c, &q, static_cast<uint8_t*>(p->pages->p), p->pages->len, path_rgb ? pb.rgb.p : nullptr,
-                     clip_rects ? pb.clip.p : nullptr, true, false);
+                     clip_rects ? pb.clip.p : nullptr, true, false, &t0);
 }
 
 }  // namespace

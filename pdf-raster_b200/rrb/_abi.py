@@ -108,7 +108,7 @@ class Tuning(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles", "tile_pairs",
-        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves")]
+        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves", "host_ns")]
 
 
 class StageTime(C.Structure):

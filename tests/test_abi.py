@@ -48,7 +48,7 @@ STRUCTS = {
     "rrb_tuning": ("Tuning", ["tile_w", "tile_h", "rows_per_chunk", "wave_points", "reserved"]),
     "rrb_batch_stats": ("BatchStats", ["paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles",
                                        "tile_pairs", "nonterminating_rows", "kernel_launches", "scratch_grows",
-                                       "waves"]),
+                                       "waves", "host_ns"]),
     "rrb_stage_time": ("StageTime", ["name", "ms", "launches"]),
     "rrb_server_config": ("ServerConfig", ["device", "workers", "mem_budget_bytes", "max_batch_pages", "tile_w",
                                            "tile_h", "predict_threads", "reserved"]),
