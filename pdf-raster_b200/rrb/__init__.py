@@ -396,10 +396,12 @@ class B200Backend:
                             clip_rects: np.ndarray | None = None):
         """Paint the batch in path order: path p stroked with strokes[p] (a
         dict: line_width, line_cap, line_join, miter_limit, dash, dash_phase)
-        or filled when strokes[p] is None. path_rgb / clip_rects as in
+        or filled when strokes[p] is None; or strokes = an array made once by
+        stroke_params (kept alive by the caller). path_rgb / clip_rects as in
         record_path_batch_ex."""
         keep = []
-        sp = stroke_params(strokes, keep)
+        # A prebuilt array (stroke_params(...)) is passed as it is; a list of dicts is converted.
+        sp = strokes if isinstance(strokes, C.Array) else stroke_params(strokes, keep)
         rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
         clip = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
         self._chk(lib().rrb_record_stroke_batch(self._h, C.byref(params), sp,
