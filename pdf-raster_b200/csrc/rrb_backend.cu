@@ -44,6 +44,7 @@ struct Scratch {
 };
 
 constexpr int KCAP = 12;        // merged Intersect entries per AA row kept in shared memory
+constexpr int KCAP_WIDE = 16;   // the same for the 4-warp row-stage shape
 constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
 
 }  // namespace
@@ -301,6 +302,11 @@ struct rrb_batch {
     // resident batch does not fail and split on every render.
     std::vector<uint32_t> plan;
     uint64_t plan_wave_points = 0;
+    // Row-stage shape (0: 12 entries x 8 warps, 1: 16 entries x 4 warps). A
+    // resident batch renders once with each (renders that grew scratch do not
+    // count) and keeps the faster.
+    uint8_t row_shape = 0, shape_state = 0;
+    double shape_ms[2] = {0.0, 0.0};
     std::vector<PageGeom> geom_h;
     std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
     bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
@@ -381,6 +387,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     for (const PageGeom& G : B->geom_h)
         B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(B->bpp) * G.w * G.h);
     B->plan.clear();
+    B->row_shape = B->shape_state = 0;
     B->has_hairline = false;
     if (hairlines)
         for (uint64_t p = 0; p < h->n_paths && !B->has_hairline; ++p) B->has_hairline = h->fill_rule[p] == RULE_HAIRLINE;
@@ -619,12 +626,22 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         k_chunk_paths<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(as<uint32_t>(c->s_chunks), NP,
                                                                             as<uint32_t>(c->s_chunk_path));
         c->launches += 1;
-        int g = grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16);
-        k_rows<KCAP><<<g, ROWS_WARPS * 32, 0, c->stream>>>(
-            as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
-            gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
-            static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
-            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
+        // Two shapes of the row stage: 12 list entries per AA row with 8 warps
+        // per block (the default), or 16 entries with 4 warps, which sends
+        // fewer rows to k_groups_mid (pages whose rows carry more crossings).
+        if (B->row_shape == 1) {
+            k_rows<KCAP_WIDE, 4><<<grid_for(c, n_chunks * 32, 4 * 32, 16), 4 * 32, 0, c->stream>>>(
+                as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
+                gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+                static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
+                as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
+        } else {
+            k_rows<KCAP><<<grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16), ROWS_WARPS * 32, 0, c->stream>>>(
+                as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
+                gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
+                static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
+                as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
+        }
         c->launches += 1;
     }
     if (n_runs) {
@@ -791,6 +808,7 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     if (B->bpp == 3) view(W->rgb, B->rgb, pb * sizeof(uint32_t));
     W->has_clip = B->has_clip;
     W->has_hairline = B->has_hairline;
+    W->row_shape = B->row_shape;
     if (B->has_clip) view(W->clip, B->clip, pb * sizeof(int4));
     if (B->has_clip) view(W->clipf, B->clipf, pb * 4 * sizeof(double));
     int rc;
@@ -858,7 +876,23 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
     return run_pages(c, B, mid, pg1, arena, arena_len, rowmap, acc, depth + 1, done_plan);
 }
 
+int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap);
+
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
+    if (B->shape_state >= 2) return run_resident_waves(c, B, arena, arena_len, rowmap);
+    B->row_shape = B->shape_state;  // trying shape 0, then shape 1
+    const uint64_t g0 = c->scratch_grows;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = run_resident_waves(c, B, arena, arena_len, rowmap);
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (rc == RRB_OK && c->scratch_grows == g0) {
+        B->shape_ms[B->shape_state] = ms;
+        if (++B->shape_state == 2) B->row_shape = B->shape_ms[1] < B->shape_ms[0] ? 1 : 0;
+    }
+    return rc;
+}
+
+int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     rrb_batch_stats acc{};
     const uint64_t grows0 = c->scratch_grows;
     struct Done {
@@ -930,6 +964,7 @@ int make_path_wave(rrb_ctx* c, rrb_batch* B, uint32_t pa, uint32_t pb, uint64_t 
     W->bpp = B->bpp;
     W->has_clip = B->has_clip;
     W->has_hairline = B->has_hairline;
+    W->row_shape = B->row_shape;
     auto view = [](Scratch& dst, const Scratch& src, size_t byte_off) {
         dst.p = static_cast<char*>(src.p) + byte_off;
         dst.cap = 0;

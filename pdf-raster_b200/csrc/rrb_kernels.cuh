@@ -952,22 +952,22 @@ __global__ void k_chunk_paths(const uint32_t* __restrict__ chunk_off, uint32_t n
 // Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the four
 // sub-rows of one pixel row; their spans are merged into coverage cells by
 // lane 4k. Pixel rows with a list over KCAP go to k_groups_mid.
-template <int KCAP>
-__global__ void __launch_bounds__(ROWS_WARPS * 32) k_rows(
+template <int KCAP, int WARPS = ROWS_WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
     const Edge* __restrict__ edges, const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax,
     const uint32_t* __restrict__ page_w, uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
     uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr,
     const uint32_t* __restrict__ chunk_path, const int4* __restrict__ path_clip) {
-    __shared__ int32_t sx0[ROWS_WARPS][KCAP * 32];
-    __shared__ int32_t sx1[ROWS_WARPS][KCAP * 32];
-    __shared__ int32_t scn[ROWS_WARPS][KCAP * 32];
-    __shared__ int32_t sedge[ROWS_WARPS][8][32];
-    __shared__ int32_t sns[ROWS_WARPS][32];
+    __shared__ int32_t sx0[WARPS][KCAP * 32];
+    __shared__ int32_t sx1[WARPS][KCAP * 32];
+    __shared__ int32_t scn[WARPS][KCAP * 32];
+    __shared__ int32_t sedge[WARPS][8][32];
+    __shared__ int32_t sns[WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
-    for (uint32_t c = blockIdx.x * ROWS_WARPS + w; c < total_chunks; c += gridDim.x * ROWS_WARPS) {
+    for (uint32_t c = blockIdx.x * WARPS + w; c < total_chunks; c += gridDim.x * WARPS) {
         const uint32_t p = chunk_path[c];  // path owning chunk c
         const PathInfo P = info[p];
         const int32_t chunk_lo = (P.y0 & ~3) + static_cast<int32_t>(c - chunk_off[p]) * 32;
