@@ -1041,7 +1041,7 @@ int run_path_range(rrb_ctx* c, rrb_batch* B, const uint64_t* path_pt_off, uint32
 // streamed: their points are copied range by range on a second stream while
 // the ranges before them render, so the upload hides behind the render.
 constexpr uint64_t kStreamMinPoints = 4ull << 20;
-constexpr uint64_t kStreamRanges = 6;
+constexpr uint64_t kStreamRanges = 4;
 
 bool page_locked(const void* p) {
     cudaPointerAttributes a{};
