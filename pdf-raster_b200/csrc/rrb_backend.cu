@@ -1054,11 +1054,16 @@ bool page_locked(const void* p) {
 
 int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8_t* arena, size_t arena_len) {
     if (!c->copy_stream) RRB_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
-    // Ranges of consecutive paths of about n_pts / kStreamRanges points each.
-    const uint64_t target = std::max<uint64_t>(1ull << 20, (h->n_pts + kStreamRanges - 1) / kStreamRanges);
+    // Ranges of consecutive paths: a first one of about a tenth of the
+    // points (the render starts once its copy lands), then kStreamRanges - 1
+    // equal ones (copies run a little faster than renders, so they stay ahead).
+    const uint64_t first = std::max<uint64_t>(1ull << 20, h->n_pts / 10);
+    const uint64_t target = std::max<uint64_t>(
+        1ull << 20, (h->n_pts - std::min(first, h->n_pts) + kStreamRanges - 2) / (kStreamRanges - 1));
     std::vector<uint32_t> cut{0};
     for (uint64_t p = 1; p < h->n_paths; ++p)
-        if (h->path_pt_off[p] - h->path_pt_off[cut.back()] >= target) cut.push_back(static_cast<uint32_t>(p));
+        if (h->path_pt_off[p] - h->path_pt_off[cut.back()] >= (cut.size() == 1 ? first : target))
+            cut.push_back(static_cast<uint32_t>(p));
     cut.push_back(static_cast<uint32_t>(h->n_paths));
     const size_t nr = cut.size() - 1;
     std::vector<cudaEvent_t> ev(nr + 1, nullptr);
