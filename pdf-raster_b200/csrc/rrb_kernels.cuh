@@ -1500,6 +1500,8 @@ struct HitRows {
     uint32_t cell0[ITERS];
 };
 
+constexpr uint32_t kFewRuns = 4;  // rectilinear paths with at most this many runs: no search
+
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
                                                const uint2* __restrict__ gidx, const int4* __restrict__ runs,
@@ -1516,11 +1518,23 @@ __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int
         if (rowok) {
             if (h.paint & PI_RECTI) {
                 // Runs cover [g0, g1] in order: the last run starting at or before grp.
-                uint32_t lo = 0, hi = h.run_cnt;
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (runs[h.goff + mid].x <= grp) lo = mid;
-                    else hi = mid;
+                uint32_t lo = 0;
+                if (h.run_cnt <= kFewRuns) {
+                    // A rectangle has a handful of runs: their starts are loaded
+                    // at once instead of by a chain of dependent search steps.
+                    int32_t s[kFewRuns - 1];
+#pragma unroll
+                    for (uint32_t q = 1; q < kFewRuns; ++q) s[q - 1] = q < h.run_cnt ? runs[h.goff + q].x : INT32_MAX;
+#pragma unroll
+                    for (uint32_t q = 1; q < kFewRuns; ++q)
+                        if (s[q - 1] <= grp) lo = q;
+                } else {
+                    uint32_t hi = h.run_cnt;
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (runs[h.goff + mid].x <= grp) lo = mid;
+                        else hi = mid;
+                    }
                 }
                 const int4 rn = runs[h.goff + lo];
                 if (rn.x <= grp && grp <= rn.y) ix = make_uint2(static_cast<uint32_t>(rn.z), static_cast<uint32_t>(rn.w));
