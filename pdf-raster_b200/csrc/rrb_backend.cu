@@ -189,20 +189,29 @@ bool valid_tile(uint32_t w, uint32_t h) {
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
                      uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
                      const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, const int4* runs,
-                     uint8_t* arena, int rowmap, const BatchCounters* ctr, const uint32_t* path_rgb) {
-#define RRB_COMP(TW, TH, RGB)                                                                                  \
-    k_composite<TW, TH, RGB><<<grid, COMP_THREADS, 0, c->stream>>>(info, geom, n_pages, n_tiles, SUPER, SUPER, \
-                                                                   super_off, super_list, row_off, row_idx,    \
-                                                                   spans, runs, arena, rowmap, ctr, path_rgb)
+                     uint8_t* arena, int rowmap, const BatchCounters* ctr, const uint32_t* path_rgb,
+                     bool rectilinear) {
+#define RRB_COMP(TW, TH, RGB, FEW)                                                                           \
+    k_composite<TW, TH, RGB, FEW><<<grid, COMP_THREADS, 0, c->stream>>>(                                      \
+        info, geom, n_pages, n_tiles, SUPER, SUPER, super_off, super_list, row_off, row_idx, spans, runs, arena, \
+        rowmap, ctr, path_rgb)
+#define RRB_COMP_SHAPE(RGB, FEW)                                  \
+    do {                                                          \
+        if (tw == 64 && th == 16) RRB_COMP(64, 16, RGB, FEW);     \
+        else if (tw == 32 && th == 32) RRB_COMP(32, 32, RGB, FEW); \
+        else RRB_COMP(16, 16, RGB, FEW);                          \
+    } while (0)
+    // Batches with rectilinear paths (rectangles) use the variant with the
+    // direct cell lookup for their rows; others keep the plain kernel, whose
+    // register allocation the extra path would disturb.
     if (path_rgb) {
-        if (tw == 64 && th == 16) RRB_COMP(64, 16, true);
-        else if (tw == 32 && th == 32) RRB_COMP(32, 32, true);
-        else RRB_COMP(16, 16, true);
+        if (rectilinear) RRB_COMP_SHAPE(true, true);
+        else RRB_COMP_SHAPE(true, false);
     } else {
-        if (tw == 64 && th == 16) RRB_COMP(64, 16, false);
-        else if (tw == 32 && th == 32) RRB_COMP(32, 32, false);
-        else RRB_COMP(16, 16, false);
+        if (rectilinear) RRB_COMP_SHAPE(false, true);
+        else RRB_COMP_SHAPE(false, false);
     }
+#undef RRB_COMP_SHAPE
 #undef RRB_COMP
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
@@ -719,7 +728,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
                                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
-                               rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr)))
+                               rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr,
+                               n_runs > 0)))
         return rc;
     stage_end(c, 11);
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;

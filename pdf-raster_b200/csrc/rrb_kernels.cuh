@@ -1500,7 +1500,8 @@ struct HitRows {
     uint32_t cell0[ITERS];
 };
 
-constexpr uint32_t kFewRuns = 4;  // rectilinear paths with at most this many runs: no search
+constexpr uint32_t kFewRuns = 4;   // rectilinear paths with at most this many runs: no search
+constexpr uint32_t kFewCells = 4;  // rectilinear rows with at most this many cells: direct lookup
 
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
@@ -1584,7 +1585,8 @@ __device__ __forceinline__ uint32_t rgb_over_div255(uint32_t d, uint32_t a, uint
 // a_src of the Rgb8 path: (a_input * shape + 255) >> 8.
 __device__ __forceinline__ uint32_t rgb_a_src(uint32_t alpha, uint32_t shape) { return (alpha * shape + 255u) >> 8; }
 
-template <int TW, int TH, bool RGB>
+// FEW: the batch has rectilinear paths, whose rows take the direct lookup.
+template <int TW, int TH, bool RGB, bool FEW>
 __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitRows<TW, TH>& hr, int X0,
                                                     const uint32_t* __restrict__ cells, const uint8_t* gamma,
                                                     int32_t (*mark)[TW], uint32_t (&pix)[TH * TW / COMP_THREADS]) {
@@ -1598,11 +1600,54 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 #pragma unroll
     for (int it = 0; it < ITERS; ++it) {
         const uint2 ix = hr.ix[it];
-        uint32_t nb = (ix.y + L::LPR - 1) / L::LPR;
-        for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
         int32_t cov[L::PX];
 #pragma unroll
         for (int q = 0; q < L::PX; ++q) cov[q] = 0;
+        // Rectilinear paths (rectangle edges crossing the tile) have at most a
+        // few cells per pixel row, held in the row's first lanes (cell0): each
+        // pixel takes the last cell that reaches into the tile and starts
+        // (clipped to the tile) at or before it, and is covered if it lies
+        // before that cell's end — the rule of the marking pass below,
+        // without shared memory.
+        bool few = false;
+        if constexpr (FEW) few = (h.paint & PI_RECTI) && __all_sync(0xffffffffu, ix.y <= kFewCells);
+        if (few) {
+            uint32_t sel[L::PX];
+            bool has[L::PX];
+#pragma unroll
+            for (int q = 0; q < L::PX; ++q) {
+                sel[q] = 0;
+                has[q] = false;
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kFewCells; ++k) {
+                const uint32_t c = __shfl_sync(0xffffffffu, hr.cell0[it], static_cast<int>(k), L::LPR);
+                const int32_t x0 = static_cast<int32_t>(c & 0x3fffu);
+                const int32_t x1 = x0 + static_cast<int32_t>((c >> 14) & 0x3fffu) + 1;
+                const int32_t sx = max(x0, X0);
+                const bool marks = k < ix.y && sx < min(x1, X0 + TW);
+#pragma unroll
+                for (int q = 0; q < L::PX; ++q) {
+                    if (marks && sx <= X0 + col + q) {
+                        sel[q] = c;
+                        has[q] = true;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < L::PX; ++q) {
+                const int32_t x0 = static_cast<int32_t>(sel[q] & 0x3fffu);
+                const int32_t x1 = x0 + static_cast<int32_t>((sel[q] >> 14) & 0x3fffu) + 1;
+                if (has[q] && X0 + col + q < x1) cov[q] = static_cast<int32_t>(sel[q] >> 28) + 1;
+            }
+        }
+        // Otherwise the clipped cell starts are marked in shared memory, LPR
+        // cells at a time, and each pixel takes a prefix max across its row.
+        uint32_t nb = 0;
+        if (!few) {
+            nb = (ix.y + L::LPR - 1) / L::LPR;
+            for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
+        }
         for (uint32_t bt = 0; bt < nb; ++bt) {
 #pragma unroll
             for (int q = 0; q < L::PX; ++q) mark[w * L::RPW + slot][q * L::LPR + sub] = -1;
@@ -1665,7 +1710,7 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 
 // RGB: the pages are Rgb8 (3 bytes per pixel) and path_rgb[p] is path p's
 // colour; otherwise Gray8 pages painted with each path's gray.
-template <int TW, int TH, bool RGB>
+template <int TW, int TH, bool RGB, bool FEW>
 __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
@@ -1835,7 +1880,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 }
                 if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
                 if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
-                composite_path_rows<TW, TH, RGB>(hits[k], cur, X0, cells, gamma, mark, pix);
+                composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
                 nxt = nxt2;
                 ++k;
