@@ -269,12 +269,19 @@ size_t skip_same(const Pts& p, size_t i) {
 }
 
 // Round join arcs (stroke/path.rs:461-584) at vertex (jx, jy) between the
-// segment with unit direction (dx, dy) and the next one (nx, ny).
+// segment with unit direction (dx, dy) and the next one (nx, ny). The join
+// takes each direction's angle as atan2(x, -y) on a left turn (kind 1) or
+// atan2(-x, y) otherwise (kind 0). a_kind / a_val: the current segment's
+// angle when the previous join already took it in this join's kind (-1:
+// none); an_kind / an_val receive the next segment's, for the next join.
 void round_join(Sink& out, double jx, double jy, double w, double dx, double dy, double wdx, double wdy, double nx,
-                double ny, double wnx, double wny, double cross) {
+                double ny, double wnx, double wny, double cross, int a_kind, double a_val, int& an_kind,
+                double& an_val) {
     if (cross < 0.0) {
-        double a = std::atan2(dx, -dy);
+        double a = a_kind == 1 ? a_val : std::atan2(dx, -dy);
         const double an = std::atan2(nx, -ny);
+        an_kind = 1;
+        an_val = an;
         if (a < an) a = a + 2.0 * kPi;
         const double da = (a - an) / kPi;
         if (da < 0.501) {
@@ -298,8 +305,10 @@ void round_join(Sink& out, double jx, double jy, double w, double dx, double dy,
                   jy + wdx);
         return;
     }
-    const double a = std::atan2(-dx, dy);
+    const double a = a_kind == 0 ? a_val : std::atan2(-dx, dy);
     double an = std::atan2(-nx, ny);
+    an_kind = 0;
+    an_val = an;
     if (an < a) an = an + 2.0 * kPi;
     const double da = (an - a) / kPi;
     if (da < 0.501) {
@@ -363,6 +372,16 @@ void end_cap(Sink& out, int kind, double x, double y, double wdx, double wdy) {
 // subpath) a closed join piece; the nonzero fill of their union is the stroke.
 void outline_path(const Pts& p, double w, const rrb_stroke_params& sp, Sink& out) {
     if (p.n == 0) return;
+    // The segment a join turns into is the next iteration's segment: its
+    // length (hypot) and, after a round join, its angle (atan2) are kept,
+    // keyed by the segment's end-point indices, so a reuse is the same libm
+    // call on the same points.
+    struct {
+        size_t a = SIZE_MAX, b = SIZE_MAX;
+        double len = 0.0;
+        int ang_kind = -1;
+        double ang = 0.0;
+    } next;
     size_t sub1 = 0;
     bool closed = false;
     size_t i0 = 0, i1 = skip_same(p, 0);
@@ -391,7 +410,8 @@ void outline_path(const Pts& p, double w, const rrb_stroke_params& sp, Sink& out
         }
         const bool last = p.has(j1, RRB_PATH_LAST);
         const size_t k0 = last ? sub1 + 1 : j1 + 1;
-        const double len = seg_len(p.x(i1), p.y(i1), p.x(j0), p.y(j0));
+        const bool known = next.a == i1 && next.b == j0;
+        const double len = known ? next.len : seg_len(p.x(i1), p.y(i1), p.x(j0), p.y(j0));
         if (len == 0.0) {
             i0 = j0;
             i1 = j1;
@@ -409,7 +429,10 @@ void outline_path(const Pts& p, double w, const rrb_stroke_params& sp, Sink& out
         else out.line(jx - wdy, jy + wdx);
         out.close();
         if (!last || closed) {
-            const double inv_n = 1.0 / seg_len(p.x(j1), p.y(j1), p.x(k0), p.y(k0));
+            const double nlen = seg_len(p.x(j1), p.y(j1), p.x(k0), p.y(k0));
+            const double inv_n = 1.0 / nlen;
+            int an_kind = -1;
+            double an_val = 0.0;
             const double nx = inv_n * (p.x(k0) - p.x(j1)), ny = inv_n * (p.y(k0) - p.y(j1));
             const double wnx = 0.5 * w * nx, wny = 0.5 * w * ny;
             const double cross = dx * ny - dy * nx;
@@ -421,7 +444,8 @@ void outline_path(const Pts& p, double w, const rrb_stroke_params& sp, Sink& out
                 m = std::sqrt(miter - 1.0);
             }
             if (angle && sp.line_join == RRB_JOIN_ROUND) {
-                round_join(out, jx, jy, w, dx, dy, wdx, wdy, nx, ny, wnx, wny, cross);
+                round_join(out, jx, jy, w, dx, dy, wdx, wdy, nx, ny, wnx, wny, cross, known ? next.ang_kind : -1,
+                           next.ang, an_kind, an_val);
             } else if (angle) {
                 const bool apex = sp.line_join == RRB_JOIN_MITER && std::sqrt(miter) <= sp.miter_limit;
                 out.move(jx, jy);
@@ -436,6 +460,11 @@ void outline_path(const Pts& p, double w, const rrb_stroke_params& sp, Sink& out
                 }
             }
             out.close();
+            next.a = j1;
+            next.b = k0;
+            next.len = nlen;
+            next.ang_kind = an_kind;
+            next.ang = an_val;
         }
         i0 = j0;
         i1 = j1;

@@ -211,6 +211,37 @@ def test_host_outline_matches_oracle(oracle, rrb_lib):
     assert kinds == {1, 2} or kinds == {0, 1, 2}
 
 
+def test_host_outline_round_join_chains_match_oracle(oracle, rrb_lib):
+    """Long chains of round joins, where the builder reuses each segment's
+    length and join angle for the next join: smooth curves turning one way,
+    zigzags turning both ways, collinear vertices (no join drawn) between
+    turns, and closed subpaths whose last join turns into the first segment."""
+    rng = np.random.default_rng(23)
+    cases = []
+    for _ in range(60):  # curves flattened into many short segments
+        c = rng.uniform(20, 180, 2)
+        pts, fl = [c], [1]
+        for _ in range(int(rng.integers(1, 5))):
+            pts += [c + rng.normal(0, 40, 2), c + rng.normal(0, 40, 2), c + rng.normal(0, 60, 2)]
+            fl += [8, 8, 0]
+            c = pts[-1]
+        fl[-1] |= 2
+        cases.append((np.array(pts, float), np.array(fl, np.uint8)))
+    for _ in range(60):  # zigzags with collinear runs, some closed
+        n = int(rng.integers(4, 40))
+        xs = np.cumsum(rng.uniform(1, 15, n))
+        ys = rng.choice([-6.0, 0.0, 0.0, 6.0], n) + 50
+        sub = [tuple(p) for p in np.stack([xs, ys], 1)]
+        cases.append(_path(sub, closed=(0,) if rng.random() < 0.4 else ()))
+    for pts, fl in cases:
+        for w in (0.5, 2.0, 9.0):
+            st = dict(line_width=w, line_join=RJOIN, line_cap=int(rng.integers(0, 3)))
+            a = rrb_lib.stroke_outline(pts, fl, flatness=0.1, **st)
+            b = oracle.stroke_outline(pts, fl, flatness=0.1, **st)
+            assert a[0] == b[0] == 1
+            assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
+
+
 def test_host_outline_rejects_bad_params(rrb_lib):
     pts, fl = _path([(0, 0), (10, 0)])
     for bad in (dict(line_width=-1.0), dict(line_width=float("nan")), dict(line_width=1.0, line_cap=3),
