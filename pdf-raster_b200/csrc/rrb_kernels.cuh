@@ -702,8 +702,8 @@ __device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? 
 // at aa_width as in the reference) in place over the entry arrays. Returns the
 // span count.
 template <typename Get, typename Put>
-__device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, int32_t lo, int32_t hi, Get get, Put put,
-                                        uint32_t& nonterm) {
+__host__ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, int32_t lo, int32_t hi,
+                                                 Get get, Put put, uint32_t& nonterm) {
     int32_t count = 0, xx = 0;
     int i = 0, ns = 0;
     bool have = false;
@@ -768,7 +768,7 @@ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa_width, i
 // coverage > 0; at most one per boundary plus one run per gap, i.e. at most
 // 2 x (number of boundaries). Cell: x0 (bits 0-13) | len-1 (14-27) | cov-1 (28-31).
 template <typename Bound, typename Put>
-__device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bound, Put put) {
+__host__ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bound, Put put) {
     int bi[4] = {0, 0, 0, 0};
     int depth = 0, nc = 0;
     int32_t prev_px = -1;

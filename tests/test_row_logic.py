@@ -1,0 +1,168 @@
+"""The row stage's per-row logic on the CPU: walk_row (the winding walk of
+render_aa_line, scanner/mod.rs:393-467) and sweep_cells (the 4x4 coverage of
+draw_aa_line, fill/mod.rs:344-401, computed from spans) are __host__
+__device__ functions; tests/row_logic_shim.cu calls the same source on the
+host. Each is checked against the oracle on seeded paths: every AA row's spans
+must set exactly the oracle's AaBuf bits, and every pixel row's cells must give
+the oracle's 0..16 coverage per pixel.
+"""
+
+import ctypes as C
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+SHIM = ROOT / "tests" / "row_logic_shim.cu"
+
+
+@pytest.fixture(scope="module")
+def shim(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(nvcc).exists():
+        pytest.skip("nvcc not found")
+    out = tmp_path_factory.mktemp("row_logic") / "librow_logic.so"
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17", "-shared",
+                    "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-o", str(out), str(SHIM)],
+                   check=True, cwd=str(ROOT))
+    lib = C.CDLL(str(out))
+    i32p = C.POINTER(C.c_int32)
+    lib.rl_walk_row.argtypes = [i32p, i32p, i32p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, i32p, i32p,
+                                C.POINTER(C.c_uint32)]
+    lib.rl_walk_row.restype = C.c_int
+    lib.rl_sweep_cells.argtypes = [i32p, i32p, i32p, C.c_int, C.POINTER(C.c_uint32)]
+    lib.rl_sweep_cells.restype = C.c_int
+    return lib
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+def walk(shim, row, eo, aa_width):
+    """Spans (x0, x1 exclusive) of one AA row's sorted entries, and whether it ran out."""
+    n = len(row)
+    x0 = _i32([r[0] for r in row] or [0])
+    x1 = _i32([r[1] for r in row] or [0])
+    cn = _i32([r[2] for r in row] or [0])
+    s0 = np.zeros(max(1, n), np.int32)
+    s1 = np.zeros(max(1, n), np.int32)
+    nt = C.c_uint32()
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    ns = shim.rl_walk_row(p(x0), p(x1), p(cn), n, int(eo), aa_width, 0, aa_width, p(s0), p(s1), C.byref(nt))
+    return list(zip(s0[:ns].tolist(), s1[:ns].tolist())), nt.value
+
+
+def sweep(shim, spans4):
+    """Cells of one pixel row from its four AA rows' spans, expanded to coverage per pixel."""
+    stride = max(1, max(len(s) for s in spans4))
+    x0 = np.zeros(4 * stride, np.int32)
+    x1 = np.zeros(4 * stride, np.int32)
+    for k, sp in enumerate(spans4):
+        for i, (a, b) in enumerate(sp):
+            x0[k * stride + i], x1[k * stride + i] = a, b
+    n4 = _i32([len(s) for s in spans4])
+    cells = np.zeros(4 * max(1, int(n4.sum())), np.uint32)
+    p = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    nc = shim.rl_sweep_cells(p(n4), p(x0), p(x1), stride, cells.ctypes.data_as(C.POINTER(C.c_uint32)))
+    assert nc <= 4 * int(n4.sum())
+    return cells[:nc]
+
+
+def coverage_of(cells, width):
+    cov = np.zeros(width, np.int32)
+    last = -1
+    for c in cells.tolist():
+        x0, ln, cv = c & 0x3FFF, ((c >> 14) & 0x3FFF) + 1, (c >> 28) + 1
+        assert x0 > last, "cells sorted and disjoint"
+        last = x0 + ln - 1
+        cov[x0:min(width, x0 + ln)] = cv
+    return cov
+
+
+def random_path(rng, w, h, closed=True):
+    """1-3 subpaths of lines and cubics, vertices partly outside the page;
+    closed=False leaves every subpath open (no return to its first point)."""
+    pts, fl = [], []
+    for _ in range(int(rng.integers(1, 4))):
+        start = len(fl)
+        cur = rng.uniform([-5, -5], [w + 5, h + 5])
+        pts.append(cur)
+        fl.append(1)
+        for _ in range(int(rng.integers(2, 9))):
+            nxt = rng.uniform([-8, -8], [w + 8, h + 8])
+            if rng.random() < 0.35:
+                pts += [cur + rng.normal(0, 12, 2), nxt + rng.normal(0, 12, 2), nxt]
+                fl += [8, 8, 0]
+            else:
+                pts.append(nxt)
+                fl.append(0)
+            cur = nxt
+        if closed:
+            if not np.array_equal(pts[start], pts[-1]):
+                pts.append(np.array(pts[start], float))
+                fl.append(0)
+            fl[start] |= 4
+            fl[-1] |= 4
+        fl[-1] |= 2
+    return np.array(pts, float), np.array(fl, np.uint8)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_walk_and_sweep_match_oracle(oracle, shim, seed):
+    rng = np.random.default_rng(seed)
+    W, H = 48, 40
+    aw = 4 * W
+    rows_checked = ran_out = 0
+    for i in range(40):
+        # Open paths without the implicit close leave rows whose winding never returns to 0.
+        close = i % 5 != 4
+        pts, fl = random_path(rng, W, H, closed=close)
+        eo = bool(i % 3 == 0)
+        segs = oracle.xpath_new(pts, fl, flatness=0.25, close=close, aa_scale=True)
+        sc = oracle.Scanner(segs, eo, 0, 4 * H - 1)
+        for y in range(H):
+            bits, _, st = sc.render_aa_line(aw, y)
+            spans4, nt_sum = [], 0
+            for k in range(4):
+                spans, nt = walk(shim, sc.row(4 * y + k), eo, aw)
+                line = np.zeros(aw, bool)
+                for a, b in spans:
+                    assert 0 <= a < b <= aw
+                    line[a:b] = True
+                assert np.array_equal(np.packbits(line), bits[k]), (i, y, k)
+                spans4.append(spans)
+                nt_sum += nt
+            assert nt_sum == st.nonterminating_rows
+            ran_out += nt_sum
+            want = oracle.aa_coverage_span(bits, 0, W).astype(np.int32)
+            assert np.array_equal(coverage_of(sweep(shim, spans4), W), want), (i, y)
+            rows_checked += 1
+    assert rows_checked == 40 * H
+    if seed == 0:
+        assert ran_out > 0  # the open paths exercised the unclosed-span arm
+
+
+def test_sweep_cell_edges(oracle, shim):
+    """Spans ending on pixel boundaries, one-column spans, spans covering a
+    whole pixel in one sub-row only, and empty sub-rows."""
+    cases = [
+        [[(0, 4)], [(0, 4)], [(0, 4)], [(0, 4)]],
+        [[(3, 5)], [], [(4, 8)], [(7, 8)]],
+        [[(1, 2), (5, 6), (9, 10)], [(0, 12)], [], [(2, 3)]],
+        [[(0, 40)], [(0, 40)], [(0, 40)], [(0, 39)]],
+        [[], [], [], []],
+    ]
+    W = 12
+    for spans4 in cases:
+        bits = np.zeros((4, (4 * W + 7) // 8), np.uint8)
+        for k, sp in enumerate(spans4):
+            line = np.zeros(4 * W, bool)
+            for a, b in sp:
+                line[a:b] = True
+            bits[k] = np.packbits(line)
+        want = oracle.aa_coverage_span(bits, 0, W).astype(np.int32)
+        assert np.array_equal(coverage_of(sweep(shim, spans4), W), want), spans4
