@@ -5,9 +5,15 @@
 // ...) so nvcc cannot contract it into an FMA; every f64::mul_add of the
 // reference is __fma_rn. That keeps flattening and segment set-up bit-exact
 // with the reference CPU rasterizer independently of -fmad.
+//
+// The functions are __host__ __device__: compiled for the host (the CPU
+// tests do, with -ffp-contract=off) the same operations are plain IEEE
+// double operations and std::fma, which round the same way.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
+#include <cstring>
 
 namespace rrb {
 
@@ -22,16 +28,34 @@ constexpr uint8_t PF_FIRST = 0x01, PF_LAST = 0x02, PF_CLOSED = 0x04, PF_CURVE = 
 constexpr int EK_HORIZ = 0, EK_VERT = 1, EK_SLOPED = 2;
 constexpr int EF_KIND_MASK = 3, EF_POSITIVE = 4, EF_FIRST_ZERO = 8, EF_EMPTY = 16;
 
+#ifdef __CUDA_ARCH__
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ double dfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ unsigned long long bits_of(double x) { return __double_as_longlong(x); }
+__device__ __forceinline__ bool is_pos_inf(double x) { return x == __longlong_as_double(0x7ff0000000000000LL); }
+__device__ __forceinline__ int32_t trunc_i32(double x) { return __double2int_rz(x); }
+#else
+inline double dadd(double a, double b) { return a + b; }
+inline double dsub(double a, double b) { return a - b; }
+inline double dmul(double a, double b) { return a * b; }
+inline double ddiv(double a, double b) { return a / b; }
+inline double dfma(double a, double b, double c) { return std::fma(a, b, c); }
+inline unsigned long long bits_of(double x) {
+    unsigned long long b;
+    std::memcpy(&b, &x, sizeof b);
+    return b;
+}
+inline bool is_pos_inf(double x) { return x == HUGE_VAL; }
+inline int32_t trunc_i32(double x) { return static_cast<int32_t>(x); }  // |x| < 2^31 at every call
+#endif
 
 // f64::midpoint (Rust std): (a+b)/2 when both |a|,|b| <= f64::MAX/2. x/2
 // and x*0.5 are the same correctly rounded value of the same real number, so
 // the halving is a multiplication.
-__device__ __forceinline__ double midpoint(double a, double b) {
+__host__ __device__ __forceinline__ double midpoint(double a, double b) {
     const double HI = 8.98846567431157854e+307;   // f64::MAX / 2
     const double LO = 4.45014771701440277e-308;   // f64::MIN_POSITIVE * 2
     double aa = fabs(a), ab = fabs(b);
@@ -42,29 +66,29 @@ __device__ __forceinline__ double midpoint(double a, double b) {
 }
 
 // saturate_f64_to_i32 / splash_floor (crates/color/src/convert.rs:221-265).
-__device__ __forceinline__ int32_t sat_i32_of_integral(double x) {
-    if (!isfinite(x)) return x == __longlong_as_double(0x7ff0000000000000LL) ? INT32_MAX : INT32_MIN;
+__host__ __device__ __forceinline__ int32_t sat_i32_of_integral(double x) {
+    if (!isfinite(x)) return is_pos_inf(x) ? INT32_MAX : INT32_MIN;
     if (x >= 2147483647.0) return INT32_MAX;
     if (x <= -2147483648.0) return INT32_MIN;
     return static_cast<int32_t>(x);
 }
-__device__ __forceinline__ int32_t splash_floor(double x) { return sat_i32_of_integral(floor(x)); }
+__host__ __device__ __forceinline__ int32_t splash_floor(double x) { return sat_i32_of_integral(floor(x)); }
 
 // fp_from_f64 (crates/raster/src/scanner/mod.rs:51-66): truncating 16.16.
-__device__ __forceinline__ int32_t fp_from_f64(double x) {
+__host__ __device__ __forceinline__ int32_t fp_from_f64(double x) {
     double fp = dmul(x, 65536.0);
     if (fp >= 2147483647.0) return INT32_MAX;
     if (fp <= -2147483648.0) return INT32_MIN;
     if (isnan(fp)) return 0;
-    return __double2int_rz(fp);
+    return trunc_i32(fp);
 }
 
-__device__ __forceinline__ int32_t sat_i64_to_i32(long long v) {
+__host__ __device__ __forceinline__ int32_t sat_i64_to_i32(long long v) {
     return v > INT32_MAX ? INT32_MAX : (v < INT32_MIN ? INT32_MIN : static_cast<int32_t>(v));
 }
 
 // transform (crates/raster/src/xpath.rs:421-426).
-__device__ __forceinline__ void transform(const double* m, double x, double y, double& ox, double& oy) {
+__host__ __device__ __forceinline__ void transform(const double* m, double x, double y, double& ox, double& oy) {
     ox = dfma(x, m[0], dfma(y, m[2], m[4]));
     oy = dfma(x, m[1], dfma(y, m[3], m[5]));
 }
@@ -84,15 +108,15 @@ struct __align__(16) Edge {
 // add_segment (xpath.rs:324-402) + aa_scale (xpath.rs:283-303) + the
 // per-segment set-up of count/fill_intersections, clipped to AA rows
 // [clip_lo, clip_hi].
-__device__ __forceinline__ Edge make_edge(double x0, double y0, double x1, double y1, int32_t clip_lo,
-                                          int32_t clip_hi) {
+__host__ __device__ __forceinline__ Edge make_edge(double x0, double y0, double x1, double y1, int32_t clip_lo,
+                                                   int32_t clip_hi) {
     Edge e;
     e.dfp = 0;
     e.cmin = 0;
     e.cmax = 0;
     e.b = 0;
-    unsigned long long by0 = __double_as_longlong(y0), by1 = __double_as_longlong(y1);
-    unsigned long long bx0 = __double_as_longlong(x0), bx1 = __double_as_longlong(x1);
+    unsigned long long by0 = bits_of(y0), by1 = bits_of(y1);
+    unsigned long long bx0 = bits_of(x0), bx1 = bits_of(x1);
     if (by0 == by1) {
         // HORIZ: never flipped, dxdy = 0; aa_scale then multiplies by 4.
         double sx0 = dmul(x0, 4.0), sx1 = dmul(x1, 4.0), sy = dmul(y0, 4.0);
@@ -175,7 +199,7 @@ __device__ __forceinline__ Edge make_edge(double x0, double y0, double x1, doubl
 // of fill_intersections' stepping. The saturating accumulator
 // xx1_fp += dxdy_fp is monotone, so after k steps it equals the exact sum
 // clamped to the i32 range.
-__device__ __forceinline__ void edge_entry(const Edge& e, int32_t r, int32_t& lo, int32_t& hi, int32_t& c) {
+__host__ __device__ __forceinline__ void edge_entry(const Edge& e, int32_t r, int32_t& lo, int32_t& hi, int32_t& c) {
     int kind = e.flags & EF_KIND_MASK;
     if (kind == EK_HORIZ) {
         lo = e.a;
@@ -204,7 +228,7 @@ __device__ __forceinline__ void edge_entry(const Edge& e, int32_t r, int32_t& lo
 }
 
 // AA column range [lo, hi] of the entries an edge can produce.
-__device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo, int32_t& hi) {
+__host__ __device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo, int32_t& hi) {
     int kind = e.flags & EF_KIND_MASK;
     if (kind == EK_HORIZ) {
         lo = e.a;
@@ -226,20 +250,21 @@ __device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo, int32_t&
 // most log2(1024) = 10 halves are pending. Same operations in the same
 // order as the reference, hence the same points.
 // (a+b)/2 for operands known to be within +-f64::MAX/2 (midpoint's first branch).
-__device__ __forceinline__ double midpoint_in_range(double a, double b) { return dmul(dadd(a, b), 0.5); }
+__host__ __device__ __forceinline__ double midpoint_in_range(double a, double b) { return dmul(dadd(a, b), 0.5); }
 
 template <bool IN_RANGE, typename Emit>
-__device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
-                                                  double p2y, double p3x, double p3y, double flat_sq, Emit& emit);
+__host__ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                           double p2y, double p3x, double p3y, double flat_sq,
+                                                           Emit& emit);
 
 // Every point the subdivision computes is a midpoint of two earlier points,
 // i.e. a convex combination of the four control points, so when all control
 // coordinates lie within +-f64::MAX/2 every midpoint call takes the (a+b)/2
 // branch: the check is made once per curve and the loop runs branch-free.
 template <typename Emit>
-__device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x, double p1y, double p2x,
-                                             double p2y, double p3x, double p3y, double flat_sq,
-                                             Emit emit) {
+__host__ __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                      double p2y, double p3x, double p3y, double flat_sq,
+                                                      Emit emit) {
     const double HI = 8.98846567431157854e+307;
     const double m = fmax(fmax(fmax(fabs(p0x), fabs(p0y)), fmax(fabs(p1x), fabs(p1y))),
                           fmax(fmax(fabs(p2x), fabs(p2y)), fmax(fabs(p3x), fabs(p3y))));
@@ -248,8 +273,9 @@ __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x,
 }
 
 template <bool IN_RANGE, typename Emit>
-__device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
-                                                  double p2y, double p3x, double p3y, double flat_sq, Emit& emit) {
+__host__ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                           double p2y, double p3x, double p3y, double flat_sq,
+                                                           Emit& emit) {
     auto mid = [](double a, double b) { return IN_RANGE ? midpoint_in_range(a, b) : midpoint(a, b); };
     double sx[FLATTEN_STACK][6];
     int sidx[FLATTEN_STACK];
@@ -314,7 +340,7 @@ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double
 }
 
 // div255 (crates/color/src/convert.rs:50-58).
-__device__ __forceinline__ uint32_t div255(uint32_t x) {
+__host__ __device__ __forceinline__ uint32_t div255(uint32_t x) {
     uint32_t s = (x + (x >> 8) + 0x80u) >> 8;
     return s > 255u ? 255u : s;
 }

@@ -1,9 +1,12 @@
-// Host entry points over two device functions of the row stage, for the CPU
-// tests (tests/test_row_logic.py): walk_row (the winding walk of one AA row
-// into spans) and sweep_cells (four AA rows' spans into a pixel row's
-// coverage cells). Both are __host__ __device__; the kernels run the same
-// source on the GPU.
+// Host entry points over device functions of the fill path, for the CPU
+// tests (tests/test_row_logic.py): flatten_curve, make_edge and edge_entry
+// (segment set-up and per-row entries), walk_row (the winding walk of one AA
+// row into spans) and sweep_cells (four AA rows' spans into a pixel row's
+// coverage cells). All are __host__ __device__; the kernels run the same
+// source on the GPU. Build with -ffp-contract=off for the host so that no
+// multiply-add is fused where the device's explicit rounding keeps them apart.
 #include <cstdint>
+#include <cstring>
 
 #include "../pdf-raster_b200/csrc/rrb_kernels.cuh"
 
@@ -57,4 +60,56 @@ extern "C" int rl_sweep_cells(const int32_t* n4, const int32_t* span_x0, const i
                               uint32_t* cells) {
     const int n[4] = {n4[0], n4[1], n4[2], n4[3]};
     return rrb::sweep_cells(n, Bounds{span_x0, span_x1, stride}, CellOut{cells});
+}
+
+// flatten_curve (the device's flattening of one cubic): writes up to cap
+// points (x, y) of the subdivision and returns their count.
+namespace {
+struct PointsOut {
+    double* out;
+    int cap;
+    int* n;
+    __host__ __device__ void operator()(double x, double y) const {
+        if (*n < cap) {
+            out[2 * *n] = x;
+            out[2 * *n + 1] = y;
+        }
+        ++*n;
+    }
+};
+}  // namespace
+
+extern "C" int rl_flatten_curve(const double* c, double flat_sq, double* out, int cap) {
+    int n = 0;
+    rrb::flatten_curve(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], flat_sq, PointsOut{out, cap, &n});
+    return n;
+}
+
+// make_edge of each segment (x0, y0, x1, y1 in device space, as the walk
+// produces them) clipped to AA rows [clip_lo, clip_hi]: 8 int32 per edge.
+extern "C" void rl_make_edges(const double* segs, int n, int32_t clip_lo, int32_t clip_hi, int32_t* out) {
+    for (int i = 0; i < n; ++i) {
+        const rrb::Edge e = rrb::make_edge(segs[4 * i], segs[4 * i + 1], segs[4 * i + 2], segs[4 * i + 3], clip_lo,
+                                           clip_hi);
+        std::memcpy(out + 8 * i, &e, sizeof e);
+    }
+}
+
+// edge_entry of every edge that covers AA row r, in edge order: (edge index,
+// lo, hi, count) per entry; returns the entry count.
+extern "C" int rl_row_entries(const int32_t* edges, int n, int32_t r, int32_t* out) {
+    int k = 0;
+    for (int i = 0; i < n; ++i) {
+        rrb::Edge e;
+        std::memcpy(&e, edges + 8 * i, sizeof e);
+        if ((e.flags & rrb::EF_EMPTY) || r < e.row0 || r > e.row1) continue;
+        int32_t lo, hi, c;
+        rrb::edge_entry(e, r, lo, hi, c);
+        out[4 * k] = i;
+        out[4 * k + 1] = lo;
+        out[4 * k + 2] = hi;
+        out[4 * k + 3] = c;
+        ++k;
+    }
+    return k;
 }

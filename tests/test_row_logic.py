@@ -1,10 +1,12 @@
-"""The row stage's per-row logic on the CPU: walk_row (the winding walk of
-render_aa_line, scanner/mod.rs:393-467) and sweep_cells (the 4x4 coverage of
-draw_aa_line, fill/mod.rs:344-401, computed from spans) are __host__
-__device__ functions; tests/row_logic_shim.cu calls the same source on the
-host. Each is checked against the oracle on seeded paths: every AA row's spans
-must set exactly the oracle's AaBuf bits, and every pixel row's cells must give
-the oracle's 0..16 coverage per pixel.
+"""Device logic of the fill path on the CPU. flatten_curve (flatten.rs:109-215),
+make_edge + edge_entry (add_segment, aa_scale and fill_intersections,
+xpath.rs:283-402, scanner/mod.rs:511-587), walk_row (render_aa_line,
+scanner/mod.rs:393-467) and sweep_cells (the 4x4 coverage of draw_aa_line,
+fill/mod.rs:344-401, from spans) are __host__ __device__ functions;
+tests/row_logic_shim.cu calls the same source on the host. Each is checked
+against the oracle on seeded inputs: flattened points bit for bit, every AA
+row's merged and sorted entries, every AA row's spans against the oracle's
+AaBuf bits, and every pixel row's cells against its 0..16 coverage.
 """
 
 import ctypes as C
@@ -26,7 +28,7 @@ def shim(tmp_path_factory):
         pytest.skip("nvcc not found")
     out = tmp_path_factory.mktemp("row_logic") / "librow_logic.so"
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17", "-shared",
-                    "-Xcompiler", "-fPIC", "-I", str(ROOT / "include"), "-o", str(out), str(SHIM)],
+                    "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", str(ROOT / "include"), "-o", str(out), str(SHIM)],
                    check=True, cwd=str(ROOT))
     lib = C.CDLL(str(out))
     i32p = C.POINTER(C.c_int32)
@@ -35,6 +37,13 @@ def shim(tmp_path_factory):
     lib.rl_walk_row.restype = C.c_int
     lib.rl_sweep_cells.argtypes = [i32p, i32p, i32p, C.c_int, C.POINTER(C.c_uint32)]
     lib.rl_sweep_cells.restype = C.c_int
+    dp = C.POINTER(C.c_double)
+    lib.rl_flatten_curve.argtypes = [dp, C.c_double, dp, C.c_int]
+    lib.rl_flatten_curve.restype = C.c_int
+    lib.rl_make_edges.argtypes = [dp, C.c_int, C.c_int32, C.c_int32, i32p]
+    lib.rl_make_edges.restype = None
+    lib.rl_row_entries.argtypes = [i32p, C.c_int, C.c_int32, i32p]
+    lib.rl_row_entries.restype = C.c_int
     return lib
 
 
@@ -166,3 +175,66 @@ def test_sweep_cell_edges(oracle, shim):
             bits[k] = np.packbits(line)
         want = oracle.aa_coverage_span(bits, 0, W).astype(np.int32)
         assert np.array_equal(coverage_of(sweep(shim, spans4), W), want), spans4
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def test_flatten_curve_matches_oracle(oracle, shim):
+    """The same points, bit for bit, for ordinary, tiny, huge (beyond f64::MAX/2,
+    the midpoint's other branches) and degenerate cubics."""
+    rng = np.random.default_rng(5)
+    out = np.zeros(2 * 1025, np.float64)
+    for i in range(3000):
+        scale = [1e-3, 1.0, 40.0, 3000.0, 1e308][i % 5]
+        c = np.clip(rng.normal(0, 1, 8), -1.5, 1.5) * scale
+        if i % 7 == 0:
+            c[2:4] = c[0:2]  # a control point on the start
+        if i % 11 == 0:
+            c[:] = c[0]  # all four points equal
+        fsq = [0.01, 0.25, 1.0][i % 3]
+        n = shim.rl_flatten_curve(_dp(np.ascontiguousarray(c)), fsq, _dp(out), 1025)
+        want = oracle.flatten_curve(c[0:2], c[2:4], c[4:6], c[6:8], fsq)
+        assert n == len(want), i
+        assert np.array_equal(out[: 2 * n].view(np.uint64), np.ascontiguousarray(want).reshape(-1).view(np.uint64)), i
+
+
+def _sat_inc(v):
+    return v if v == 2**31 - 1 else v + 1
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_row_entries_match_scanner(oracle, shim, seed):
+    """Per AA row: the entries of make_edge + edge_entry, merged in segment
+    order with the last entry written (write_intersect) and stably sorted, are
+    the oracle scanner's row."""
+    rng = np.random.default_rng(seed)
+    W, H = 48, 40
+    for i in range(30):
+        pts, fl = random_path(rng, W, H)
+        segs = oracle.xpath_new(pts, fl, flatness=0.25, close=True)
+        # Segments in walk order: add_segment stored flipped ones (OR_XF_FLIPPED = 4) with y0 <= y1.
+        ends = np.array([(s.x1, s.y1, s.x0, s.y0) if s.flags & 4 else (s.x0, s.y0, s.x1, s.y1) for s in segs],
+                        np.float64).reshape(-1)
+        edges = np.zeros(8 * max(1, len(segs)), np.int32)
+        shim.rl_make_edges(_dp(ends), len(segs), 0, 4 * H - 1, _ip(edges))
+        scaled = oracle.xpath_new(pts, fl, flatness=0.25, close=True, aa_scale=True)
+        sc = oracle.Scanner(scaled, bool(i % 2), 0, 4 * H - 1)
+        buf = np.zeros(4 * max(1, len(segs)), np.int32)
+        for r in range(4 * H):
+            k = shim.rl_row_entries(_ip(edges), len(segs), r, _ip(buf))
+            row = []
+            for j in range(k):
+                lo, hi, c = (int(v) for v in buf[4 * j + 1: 4 * j + 4])
+                if row and _sat_inc(row[-1][1]) >= lo and row[-1][0] <= _sat_inc(hi):
+                    a, b, cc = row[-1]
+                    row[-1] = (min(a, lo), max(b, hi), (cc + c + 2**31) % 2**32 - 2**31)
+                else:
+                    row.append((lo, hi, c))
+            row.sort(key=lambda e: e[0])  # stable, as the device's insertion sort
+            assert row == [tuple(e) for e in sc.row(r)], (i, r)
