@@ -27,7 +27,7 @@ struct HlClip {
     int32_t x_min_i, y_min_i, x_max_i, y_max_i;
 };
 
-__device__ __forceinline__ HlClip hl_clip(uint32_t W, uint32_t H, const double* __restrict__ rect) {
+__host__ __device__ __forceinline__ HlClip hl_clip(uint32_t W, uint32_t H, const double* __restrict__ rect) {
     HlClip c{0.0, 0.0, static_cast<double>(W), static_cast<double>(H), 0, 0, 0, 0};
     if (rect) {
         c.x_min = fmax(c.x_min, fmin(rect[0], rect[2]));
@@ -42,7 +42,7 @@ __device__ __forceinline__ HlClip hl_clip(uint32_t W, uint32_t H, const double* 
     return c;
 }
 
-__device__ __forceinline__ int32_t wrap_add(int32_t a, int32_t b) {
+__host__ __device__ __forceinline__ int32_t wrap_add(int32_t a, int32_t b) {
     return static_cast<int32_t>(static_cast<uint32_t>(a) + static_cast<uint32_t>(b));
 }
 
@@ -55,16 +55,16 @@ struct HlSeg {
     bool flat, inside, ltr;
 };
 
-__device__ __forceinline__ HlSeg hl_segment(const double* __restrict__ pts, const double* __restrict__ m, uint64_t pt,
-                                            uint32_t W, uint32_t H, const HlClip& clip) {
+__host__ __device__ __forceinline__ HlSeg hl_segment(const double* __restrict__ pts, const double* __restrict__ m,
+                                                     uint64_t pt, uint32_t W, uint32_t H, const HlClip& clip) {
     HlSeg g{};
     // add_segment (xpath.rs:324-402) on the transformed endpoints.
     double ax, ay, bx, by;
     transform(m, pts[2 * pt], pts[2 * pt + 1], ax, ay);
     transform(m, pts[2 * pt + 2], pts[2 * pt + 3], bx, by);
     double x0 = ax, y0 = ay, x1 = bx, y1 = by, dxdy = 0.0;
-    if (__double_as_longlong(ay) != __double_as_longlong(by)) {
-        const bool vert = __double_as_longlong(ax) == __double_as_longlong(bx);
+    if (bits_of(ay) != bits_of(by)) {
+        const bool vert = bits_of(ax) == bits_of(bx);
         dxdy = vert ? 0.0 : ddiv(dsub(bx, ax), dsub(by, ay));
         if (ay > by) {
             x0 = bx;
@@ -133,7 +133,7 @@ __device__ __forceinline__ HlSeg hl_segment(const double* __restrict__ pts, cons
 
 // The clamped span of row y (cy0 <= y <= cy1) as draw_narrow_span paints it;
 // x0 > x1 when nothing is painted.
-__device__ __forceinline__ int2 hl_row_span(const HlSeg& g, int32_t y, uint32_t W, const HlClip& clip) {
+__host__ __device__ __forceinline__ int2 hl_row_span(const HlSeg& g, int32_t y, uint32_t W, const HlClip& clip) {
     int32_t a, b;
     if (g.flat) {
         a = g.cx0;

@@ -1,14 +1,14 @@
 // Host entry points over device functions of the fill path, for the CPU
 // tests (tests/test_row_logic.py): flatten_curve, make_edge and edge_entry
 // (segment set-up and per-row entries), walk_row (the winding walk of one AA
-// row into spans) and sweep_cells (four AA rows' spans into a pixel row's
-// coverage cells). All are __host__ __device__; the kernels run the same
+// row into spans), sweep_cells (four AA rows' spans into a pixel row's
+// coverage cells) and the hairline spans (hl_clip, hl_segment, hl_row_span). All are __host__ __device__; the kernels run the same
 // source on the GPU. Build with -ffp-contract=off for the host so that no
 // multiply-add is fused where the device's explicit rounding keeps them apart.
 #include <cstdint>
 #include <cstring>
 
-#include "../pdf-raster_b200/csrc/rrb_kernels.cuh"
+#include "../pdf-raster_b200/csrc/rrb_hairline.cuh"
 
 namespace {
 
@@ -109,6 +109,25 @@ extern "C" int rl_row_entries(const int32_t* edges, int n, int32_t r, int32_t* o
         out[4 * k + 1] = lo;
         out[4 * k + 2] = hi;
         out[4 * k + 3] = c;
+        ++k;
+    }
+    return k;
+}
+
+// The pixel spans one hairline segment (x0, y0) -> (x1, y1) paints on a W x H
+// page, clipped to rect (x_min, y_min, x_max, y_max; null: the page): (row,
+// first, last) per painted row; returns the count.
+extern "C" int rl_hairline_spans(const double* seg, uint32_t W, uint32_t H, const double* rect, int32_t* out) {
+    const double m[6] = {1.0, 0.0, 0.0, 1.0, 0.0, 0.0};
+    const rrb::HlClip clip = rrb::hl_clip(W, H, rect);
+    const rrb::HlSeg g = rrb::hl_segment(seg, m, 0, W, H, clip);
+    int k = 0;
+    for (int32_t y = g.r0; y <= g.r1; ++y) {
+        const int2 sp = rrb::hl_row_span(g, y, W, clip);
+        if (sp.x > sp.y) continue;
+        out[3 * k] = y;
+        out[3 * k + 1] = sp.x;
+        out[3 * k + 2] = sp.y;
         ++k;
     }
     return k;

@@ -6,7 +6,9 @@ fill/mod.rs:344-401, from spans) are __host__ __device__ functions;
 tests/row_logic_shim.cu calls the same source on the host. Each is checked
 against the oracle on seeded inputs: flattened points bit for bit, every AA
 row's merged and sorted entries, every AA row's spans against the oracle's
-AaBuf bits, and every pixel row's cells against its 0..16 coverage.
+AaBuf bits, and every pixel row's cells against its 0..16 coverage. The
+hairline span functions (stroke_narrow / draw_narrow_span,
+stroke/mod.rs:95-256) are checked by the pages they paint.
 """
 
 import ctypes as C
@@ -44,6 +46,8 @@ def shim(tmp_path_factory):
     lib.rl_make_edges.restype = None
     lib.rl_row_entries.argtypes = [i32p, C.c_int, C.c_int32, i32p]
     lib.rl_row_entries.restype = C.c_int
+    lib.rl_hairline_spans.argtypes = [dp, C.c_uint32, C.c_uint32, dp, i32p]
+    lib.rl_hairline_spans.restype = C.c_int
     return lib
 
 
@@ -238,3 +242,48 @@ def test_row_entries_match_scanner(oracle, shim, seed):
                     row.append((lo, hi, c))
             row.sort(key=lambda e: e[0])  # stable, as the device's insertion sort
             assert row == [tuple(e) for e in sc.row(r)], (i, r)
+
+
+class _OnePath:
+    def __init__(self, pts, w, h):
+        self.pts = np.asarray(pts, np.float64)
+        self.flags = np.array([1, 2], np.uint8)
+        self.path_pt_off = np.array([0, 2], np.uint64)
+        self.fill_rule = np.zeros(1, np.uint8)
+        self.gray = np.zeros(1, np.uint8)
+        self.alpha = np.full(1, 255, np.uint8)
+        self.path_page = np.zeros(1, np.uint32)
+        self.page_width, self.page_height = np.array([w], np.uint32), np.array([h], np.uint32)
+        self.page_offset = np.zeros(1, np.uint64)
+
+
+def test_hairline_spans_match_oracle(oracle, shim):
+    """One-segment hairlines (sloped, flat, vertical, short, partly or wholly
+    off the page, with and without a clip rectangle): the spans of hl_segment
+    and hl_row_span paint the oracle's page."""
+    rng = np.random.default_rng(9)
+    W, H = 40, 30
+    out = np.zeros(3 * 4096, np.int32)
+    for i in range(2000):
+        p = rng.uniform([-12, -12], [W + 12, H + 12], (2, 2))
+        if i % 6 == 1:
+            p[1, 1] = p[0, 1]  # flat
+        if i % 6 == 2:
+            p[1, 0] = p[0, 0]  # vertical
+        if i % 6 == 3:
+            p[1] = p[0] + rng.normal(0, 0.7, 2)  # short
+        rect = None
+        if i % 3 == 0:
+            a, b = rng.uniform([-5, -5], [W + 5, H + 5], (2, 2))
+            rect = np.array([a[0], a[1], b[0], b[1]], np.float64)
+        want = np.full(W * H, 255, np.uint8)
+        oracle.render_scene_paint(_OnePath(p, W, H), want, [dict(line_width=0.0)],
+                                  clip=None if rect is None else rect.reshape(1, 4))
+        seg = np.ascontiguousarray(p.reshape(-1))
+        k = shim.rl_hairline_spans(_dp(seg), W, H, None if rect is None else _dp(rect), _ip(out))
+        got = np.full((H, W), 255, np.uint8)
+        for j in range(k):
+            y, a, b = (int(v) for v in out[3 * j: 3 * j + 3])
+            assert 0 <= y < H and 0 <= a <= b < W, (i, y, a, b)
+            got[y, a: b + 1] = 0
+        assert np.array_equal(got, want.reshape(H, W)), i
