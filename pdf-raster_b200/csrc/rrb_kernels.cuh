@@ -694,7 +694,7 @@ __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
     return x;
 }
 
-__device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? v : v + 1; }
+__host__ __device__ __forceinline__ int32_t sat_inc(int32_t v) { return v == INT32_MAX ? v : v + 1; }
 
 // Winding walk of render_aa_line (scanner/mod.rs:393-467) for one AA row over
 // its sorted entries, emitting the union of the covered spans clamped to the
@@ -1047,9 +1047,9 @@ constexpr int RECTI_MAX_EVENTS = 4 * RECTI_MAX_EDGES + 2;
 constexpr int RECTI_MAX_SPANS = RECTI_MAX_EDGES / 2 + 1;
 
 // Spans of AA row r of a rectilinear path (fold, sort, walk over <= 32 edges).
-__device__ __forceinline__ int recti_row_spans(const PathInfo& P, const Edge* __restrict__ edges, int32_t r,
-                                               int32_t aa_width, int32_t lo, int32_t hi, int32_t* sx0, int32_t* sx1,
-                                               uint32_t& nonterm) {
+__host__ __device__ __forceinline__ int recti_row_spans(const PathInfo& P, const Edge* __restrict__ edges,
+                                                        int32_t r, int32_t aa_width, int32_t lo, int32_t hi,
+                                                        int32_t* sx0, int32_t* sx1, uint32_t& nonterm) {
     int32_t x0s[RECTI_MAX_EDGES], x1s[RECTI_MAX_EDGES], cs[RECTI_MAX_EDGES];
     int n = 0;
     for (uint32_t j = P.e_begin; j < P.e_end; ++j) {

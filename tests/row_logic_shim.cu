@@ -2,7 +2,8 @@
 // tests (tests/test_row_logic.py): flatten_curve, make_edge and edge_entry
 // (segment set-up and per-row entries), walk_row (the winding walk of one AA
 // row into spans), sweep_cells (four AA rows' spans into a pixel row's
-// coverage cells) and the hairline spans (hl_clip, hl_segment, hl_row_span). All are __host__ __device__; the kernels run the same
+// coverage cells), recti_row_spans (rectilinear paths) and the hairline spans
+// (hl_clip, hl_segment, hl_row_span). All are __host__ __device__; the kernels run the same
 // source on the GPU. Build with -ffp-contract=off for the host so that no
 // multiply-add is fused where the device's explicit rounding keeps them apart.
 #include <cstdint>
@@ -131,4 +132,19 @@ extern "C" int rl_hairline_spans(const double* seg, uint32_t W, uint32_t H, cons
         ++k;
     }
     return k;
+}
+
+// recti_row_spans (the row stage of rectilinear paths) over n edges of one
+// path with fill rule eo: AA row r's spans clipped to [lo, hi); returns the count.
+extern "C" int rl_recti_spans(const int32_t* edges, int n, int eo, int32_t r, int32_t aa_width, int32_t lo,
+                              int32_t hi, int32_t* span_x0, int32_t* span_x1, uint32_t* nonterminating) {
+    rrb::PathInfo P{};
+    P.e_begin = 0;
+    P.e_end = static_cast<uint32_t>(n);
+    P.paint = eo ? (1u << 16) : 0u;
+    uint32_t nt = 0;
+    const int ns = rrb::recti_row_spans(P, reinterpret_cast<const rrb::Edge*>(edges), r, aa_width, lo, hi, span_x0,
+                                        span_x1, nt);
+    *nonterminating = nt;
+    return ns;
 }

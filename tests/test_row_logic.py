@@ -48,6 +48,9 @@ def shim(tmp_path_factory):
     lib.rl_row_entries.restype = C.c_int
     lib.rl_hairline_spans.argtypes = [dp, C.c_uint32, C.c_uint32, dp, i32p]
     lib.rl_hairline_spans.restype = C.c_int
+    lib.rl_recti_spans.argtypes = [i32p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p,
+                                   C.POINTER(C.c_uint32)]
+    lib.rl_recti_spans.restype = C.c_int
     return lib
 
 
@@ -287,3 +290,56 @@ def test_hairline_spans_match_oracle(oracle, shim):
             assert 0 <= y < H and 0 <= a <= b < W, (i, y, a, b)
             got[y, a: b + 1] = 0
         assert np.array_equal(got, want.reshape(H, W)), i
+
+
+def test_recti_row_spans_match_oracle(oracle, shim):
+    """Rectilinear paths (1-4 rectangles with fractional corners, some
+    overlapping or reversed, nonzero and even-odd): recti_row_spans sets every
+    AA row's bits as render_aa_line does."""
+    rng = np.random.default_rng(13)
+    W, H = 40, 32
+    aw = 4 * W
+    s0 = np.zeros(64, np.int32)
+    s1 = np.zeros(64, np.int32)
+    nt = C.c_uint32()
+    for i in range(150):
+        subs = []
+        for _ in range(int(rng.integers(1, 5))):
+            x0, y0 = rng.uniform([-6, -6], [W + 2, H + 2])
+            x1, y1 = x0 + rng.uniform(0.3, 25), y0 + rng.uniform(0.3, 20)
+            corners = [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
+            if rng.random() < 0.4:
+                corners = corners[::-1]  # the other winding direction
+            subs.append(corners)
+        pts, fl = _path_closed(subs)
+        eo = bool(i % 2)
+        segs = oracle.xpath_new(pts, fl, flatness=0.25, close=True)
+        assert len(segs) <= 32
+        ends = np.array([(s.x1, s.y1, s.x0, s.y0) if s.flags & 4 else (s.x0, s.y0, s.x1, s.y1) for s in segs],
+                        np.float64).reshape(-1)
+        edges = np.zeros(8 * max(1, len(segs)), np.int32)
+        shim.rl_make_edges(_dp(ends), len(segs), 0, 4 * H - 1, _ip(edges))
+        sc = oracle.Scanner(oracle.xpath_new(pts, fl, flatness=0.25, close=True, aa_scale=True), eo, 0, 4 * H - 1)
+        for y in range(H):
+            bits, _, _ = sc.render_aa_line(aw, y)
+            for k in range(4):
+                ns = shim.rl_recti_spans(_ip(edges), len(segs), int(eo), 4 * y + k, aw, 0, aw, _ip(s0), _ip(s1),
+                                         C.byref(nt))
+                line = np.zeros(aw, bool)
+                for a, b in zip(s0[:ns].tolist(), s1[:ns].tolist()):
+                    line[a:b] = True
+                assert np.array_equal(np.packbits(line), bits[k]), (i, y, k)
+
+
+def _path_closed(subpaths):
+    pts, fl = [], []
+    for sp in subpaths:
+        start = len(fl)
+        for j, p in enumerate(sp):
+            pts.append(p)
+            fl.append(1 if j == 0 else 0)
+        pts.append(sp[0])
+        fl.append(0)
+        fl[start] |= 4
+        fl[-1] |= 4 | 2
+    return np.array(pts, float), np.array(fl, np.uint8)
