@@ -779,10 +779,93 @@ ClipRect make_clip(int32_t width, int32_t height, const double* rect) {
     return c;
 }
 
+// Clip::recompute_int_bounds (clip.rs:266-271).
+void recompute_int_bounds(ClipRect& c) {
+    c.x_min_i = splash_floor(c.x_min);
+    c.y_min_i = splash_floor(c.y_min);
+    c.x_max_i = splash_ceil(c.x_max) - 1;
+    c.y_max_i = splash_ceil(c.y_max) - 1;
+}
+
+// detect_rect (clip.rs:322-359): exactly four segments, two carrying VERT and
+// two carrying HORIZ (a zero-length segment carries both), give the box of
+// the vertical segments' x and the horizontal segments' y.
+bool detect_rect(const std::vector<or_seg>& segs, double& x0, double& y0, double& x1, double& y1) {
+    if (segs.size() != 4) return false;
+    int verts = 0, horizs = 0;
+    for (const or_seg& g : segs) {
+        if (g.flags & OR_XF_VERT) ++verts;
+        if (g.flags & OR_XF_HORIZ) ++horizs;
+    }
+    if (verts != 2 || horizs != 2) return false;
+    x0 = INFINITY;
+    x1 = -INFINITY;
+    y0 = INFINITY;
+    y1 = -INFINITY;
+    for (const or_seg& g : segs) {
+        if (g.flags & OR_XF_VERT) {
+            x0 = std::fmin(std::fmin(x0, g.x0), g.x1);  // f64::min ignores a NaN operand, as fmin does
+            x1 = std::fmax(std::fmax(x1, g.x0), g.x1);
+        }
+        if (g.flags & OR_XF_HORIZ) {
+            y0 = std::fmin(std::fmin(y0, g.y0), g.y1);
+            y1 = std::fmax(std::fmax(y1, g.y0), g.y1);
+        }
+    }
+    return true;
+}
+
+// A clip region: the rectangle and the path-clip scanners pushed by
+// clip_to_path (clip.rs:141-176).
+struct ClipState {
+    ClipRect r;
+    std::vector<or_scanner*> scanners;
+    ClipState() = default;
+    ClipState(const ClipState&) = delete;
+    ClipState& operator=(const ClipState&) = delete;
+    ~ClipState() {
+        for (or_scanner* sc : scanners) or_scanner_free(sc);
+    }
+};
+
+// Clip::clip_to_path (clip.rs:141-176) with the renderer's XPath: built with
+// close_subpaths = true and without aa_scale (pdf_interp/src/renderer/page/
+// mod.rs:1003-1009). An empty path empties the clip; a detected rectangle
+// becomes clip_to_rect (clip.rs:119-127); otherwise a scanner over AA rows
+// [4 y_min_i, 4 (y_max_i + 1) - 1] is pushed.
+void clip_to_path(ClipState& cs, const double* pts, const uint8_t* flags, int64_t n, const double m[6],
+                  double flatness, int eo, or_stats* st) {
+    const int64_t need = or_xpath_new(pts, flags, n, m, flatness, 1, nullptr, 0);
+    std::vector<or_seg> segs(static_cast<size_t>(need));
+    if (need) or_xpath_new(pts, flags, n, m, flatness, 1, segs.data(), need);
+    ClipRect& c = cs.r;
+    if (segs.empty()) {
+        c.x_max = c.x_min - 1.0;
+        c.y_max = c.y_min - 1.0;
+        recompute_int_bounds(c);
+        return;
+    }
+    double rx0, ry0, rx1, ry1;
+    if (detect_rect(segs, rx0, ry0, rx1, ry1)) {
+        c.x_min = std::fmax(c.x_min, std::fmin(rx0, rx1));
+        c.x_max = std::fmin(c.x_max, std::fmax(rx0, rx1));
+        c.y_min = std::fmax(c.y_min, std::fmin(ry0, ry1));
+        c.y_max = std::fmin(c.y_max, std::fmax(ry0, ry1));
+        recompute_int_bounds(c);
+        return;
+    }
+    const int32_t y_lo = c.y_min_i * AA_SIZE, y_hi = (c.y_max_i + 1) * AA_SIZE - 1;
+    cs.scanners.push_back(or_scanner_new(segs.data(), need, eo, y_lo, y_hi, st));
+}
+
+// clip_state: when given, the clip (rectangle and path scanners) instead of
+// the page and clip_rect. With path scanners the fill is never AllInside
+// (clip.rs:210-216) and clip_aa_line lets every scanner render the AA rows
+// of the same row argument into the buffer (clip.rs:246-254).
 template <typename Span>
 void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint8_t* flags, int64_t n_pts,
                     const double m[6], double flatness, int eo, int rowmap, or_stats* st, Span span,
-                    const double* clip_rect = nullptr) {
+                    const double* clip_rect = nullptr, const ClipState* clip_state = nullptr) {
     if (n_pts == 0) return;
     if (st) st->paths++;
     // XPath::new with close_subpaths = true, then aa_scale.
@@ -792,7 +875,8 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
     or_xpath_aa_scale(segs.data(), need);
     if (st) st->segments += static_cast<uint64_t>(need);
     // Clip integer bounds (the page, or the page and a clip rectangle).
-    const ClipRect cr = make_clip(width, height, clip_rect);
+    const ClipRect cr = clip_state ? clip_state->r : make_clip(width, height, clip_rect);
+    const bool has_paths = clip_state && !clip_state->scanners.empty();
     int32_t clip_x_min_i = cr.x_min_i, clip_y_min_i = cr.y_min_i;
     int32_t clip_x_max_i = cr.x_max_i;
     int32_t clip_y_max_i = cr.y_max_i;
@@ -814,7 +898,7 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
         return;
     }
     bool all_inside = static_cast<double>(left) >= cx_min && static_cast<double>(right + 1) <= cx_max &&
-                      static_cast<double>(top) >= cy_min && static_cast<double>(bottom + 1) <= cy_max;
+                      static_cast<double>(top) >= cy_min && static_cast<double>(bottom + 1) <= cy_max && !has_paths;
     int64_t aa_width = static_cast<int64_t>(width) * AA_SIZE;
     int64_t rb = (aa_width + 7) / 8;
     std::vector<uint8_t> aa_buf(static_cast<size_t>(rb * AA_SIZE), 0);
@@ -833,8 +917,17 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
         if (!any) return;
         span(y, x0, shape.data(), cnt);
     };
-    auto clip_aa_line = [&](int32_t* x0, int32_t* x1) {
-        // Clip::clip_aa_line (clip.rs:246-254) with no path-clip scanners.
+    auto clip_aa_line = [&](int32_t row_arg, int32_t* x0, int32_t* x1) {
+        // Clip::clip_aa_line (clip.rs:246-254): each path-clip scanner's
+        // render_aa_line clears the buffer and draws its own coverage.
+        if (has_paths) {
+            int32_t cx[2];
+            for (const or_scanner* cs : clip_state->scanners) {
+                or_render_aa_line(cs, aa_buf.data(), aa_width, row_arg, cx, st);
+                *x0 = cx[0];
+                *x1 = cx[1];
+            }
+        }
         *x0 = std::max(*x0, clip_x_min_i);
         *x1 = std::min(*x1, clip_x_max_i);
     };
@@ -846,7 +939,7 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
             int32_t y = aa_y / AA_SIZE;
             int32_t aa_row = aa_y % AA_SIZE;
             or_render_aa_line(sc, aa_buf.data(), aa_width, aa_y, xr, st);
-            if (!all_inside) clip_aa_line(&xr[0], &xr[1]);
+            if (!all_inside) clip_aa_line(aa_y, &xr[0], &xr[1]);
             if (aa_row == AA_SIZE - 1) {
                 if (xr[0] <= xr[1] && y >= 0 && y < height) draw(xr[0], xr[1], y);
                 std::fill(aa_buf.begin(), aa_buf.end(), 0);
@@ -857,7 +950,7 @@ void fill_path_impl(int32_t width, int32_t height, const double* pts, const uint
         int32_t y0 = sc->y_min / AA_SIZE, y1 = sc->y_max / AA_SIZE;
         for (int32_t y = y0; y <= y1; ++y) {
             or_render_aa_line(sc, aa_buf.data(), aa_width, y, xr, st);
-            if (!all_inside) clip_aa_line(&xr[0], &xr[1]);
+            if (!all_inside) clip_aa_line(y, &xr[0], &xr[1]);
             if (xr[0] <= xr[1] && y >= 0 && y < height) draw(xr[0], xr[1], y);
         }
     }
@@ -1342,6 +1435,20 @@ void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pt
                    [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
                        or_render_span_aa_gray(page + static_cast<int64_t>(y) * width + x0, shape, n, alpha, gray);
                    });
+}
+
+void or_fill_path_clip_path(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                            int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
+                            int rowmap, const double* clip_rect, const double* clip_pts, const uint8_t* clip_flags,
+                            int64_t clip_n, int clip_eo, or_stats* st) {
+    ClipState cs;
+    cs.r = make_clip(width, height, clip_rect);
+    clip_to_path(cs, clip_pts, clip_flags, clip_n, m, flatness, clip_eo, st);
+    fill_path_impl(width, height, pts, flags, n_pts, m, flatness, eo, rowmap, st,
+                   [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
+                       or_render_span_aa_gray(page + static_cast<int64_t>(y) * width + x0, shape, n, alpha, gray);
+                   },
+                   nullptr, &cs);
 }
 
 void or_fill_path_rgb(uint8_t* page_rgb, int32_t width, int32_t height, const double* pts, const uint8_t* flags,

@@ -135,6 +135,14 @@ void or_rgb_to_gray(const uint8_t* rgb, uint8_t* gray, int64_t n_px);
 void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pts,
                   const uint8_t* flags, int64_t n_pts, const double m[6], double flatness, int eo,
                   uint8_t gray, uint8_t alpha, int rowmap, or_stats* st);
+/* fill_impl under a clip made by Clip::new(0, 0, W, H), clip_to_rect(clip_rect)
+ * when given, then clip_to_path of the clip path (clip.rs:141-176, its XPath
+ * built as the renderer builds it: close_subpaths, no aa_scale,
+ * pdf_interp/src/renderer/page/mod.rs:1003-1009) with rule clip_eo. */
+void or_fill_path_clip_path(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                            int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
+                            int rowmap, const double* clip_rect, const double* clip_pts, const uint8_t* clip_flags,
+                            int64_t clip_n, int clip_eo, or_stats* st);
 
 /* The same fill onto an Rgb8 page (3 bytes per pixel, row stride 3 * width)
  * with a solid RGB source, through composite_aa_rgb8_opaque (A12). */

@@ -101,6 +101,9 @@ def lib() -> C.CDLL:
             "or_rgb_to_gray": (None, [C.POINTER(U8), C.POINTER(U8), I64]),
             "or_fill_path": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D), D,
                                     C.c_int, U8, U8, C.c_int, C.POINTER(Stats)]),
+            "or_fill_path_clip_path": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D),
+                                              D, C.c_int, U8, U8, C.c_int, C.POINTER(D), C.POINTER(D), C.POINTER(U8),
+                                              I64, C.c_int, C.POINTER(Stats)]),
             "or_render_scene": (None, [C.POINTER(U8), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                        C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(D), C.POINTER(U8),
                                        C.POINTER(C.c_uint64), C.POINTER(U8), C.POINTER(U8), C.POINTER(U8),
@@ -318,6 +321,24 @@ def fill_path(page: np.ndarray, pts, flags, eo=False, gray=0, alpha=255, rowmap=
     lib().or_fill_path(_p(page, C.c_uint8), page.shape[1], page.shape[0], _p(pts, C.c_double),
                        _p(flags, C.c_uint8), flags.size, _mat(matrix), flatness, int(eo), gray, alpha, rowmap,
                        C.byref(st))
+    return st.as_dict()
+
+
+def fill_path_clip_path(page: np.ndarray, pts, flags, clip_pts, clip_flags, clip_eo=False, eo=False, gray=0,
+                        alpha=255, rowmap=ROWMAP_DOCUMENTED, clip_rect=None, matrix=IDENTITY, flatness=0.1) -> dict:
+    """fill_impl on a (H, W) u8 page in place under the page clip, clip_to_rect(clip_rect) when given, and
+    clip_to_path of (clip_pts, clip_flags) with rule clip_eo, as the renderer clips (XPath without aa_scale)."""
+    assert page.dtype == np.uint8 and page.flags["C_CONTIGUOUS"] and page.ndim == 2
+    pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    cpts = np.ascontiguousarray(clip_pts, np.float64).reshape(-1)
+    cfl = np.ascontiguousarray(clip_flags, np.uint8)
+    rect = None if clip_rect is None else np.ascontiguousarray(clip_rect, np.float64).reshape(4)
+    st = Stats()
+    lib().or_fill_path_clip_path(_p(page, C.c_uint8), page.shape[1], page.shape[0], _p(pts, C.c_double),
+                                 _p(flags, C.c_uint8), flags.size, _mat(matrix), flatness, int(eo), gray, alpha, rowmap,
+                                 None if rect is None else _p(rect, C.c_double), _p(cpts, C.c_double),
+                                 _p(cfl, C.c_uint8), cfl.size, int(clip_eo), C.byref(st))
     return st.as_dict()
 
 
