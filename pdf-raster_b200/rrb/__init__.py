@@ -19,7 +19,8 @@ import numpy as np
 from . import _abi
 from ._abi import (RRB_CAP_BUTT, RRB_CAP_PROJECTING, RRB_CAP_ROUND, RRB_FILL_EVEN_ODD,  # noqa: F401
                    RRB_FILL_NONZERO, RRB_JOIN_BEVEL, RRB_JOIN_MITER, RRB_JOIN_ROUND, RRB_ROWMAP_AS_SHIPPED,
-                   RRB_ROWMAP_DOCUMENTED, BatchStats, PathBatchParams, PathFillParams, RequestResult, SceneParams,
+                   RRB_ROWMAP_DOCUMENTED, BatchStats, ClipPath, PathBatchParams, PathFillParams, RequestResult,
+                   SceneParams,
                    ServerConfig, ServerStats, StageTime, StrokeParams, Tuning, VramBudget)
 
 __all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "Server", "lib",
@@ -392,6 +393,27 @@ class B200Backend:
                                                  None if rgb is None else _ptr(rgb, C.c_uint8),
                                                  None if clip is None else _ptr(clip, C.c_double)))
 
+    def record_path_batch_clip_paths(self, params: PathBatchParams, clip_paths, clip_rects: np.ndarray | None = None,
+                                     path_rgb: np.ndarray | None = None):
+        """The batch with a clip path per fill (clip_paths[p] = (pts, flags, even_odd) or None) and optional
+        clip rectangles: rrb_lower_clip_paths, then rrb_record_path_batch_ex on the lowered batch."""
+        low = lower_clip_paths(params, clip_paths, clip_rects)
+        n = int(params.n_paths)
+        asa = np.ctypeslib.as_array
+        src = low["src_path"]
+        gray = asa(params.gray, shape=(max(1, n),))[:n][src]
+        alpha = asa(params.alpha, shape=(max(1, n),))[:n][src]
+        page = asa(params.path_page, shape=(max(1, n),))[:n][src]
+        keep = []
+        npg = int(params.n_pages)
+        lowered = batch_params(low["pts"], low["flags"], low["path_pt_off"], low["fill_rule"], gray, alpha, page,
+                               asa(params.page_width, shape=(npg,)).copy(), asa(params.page_height, shape=(npg,)).copy(),
+                               asa(params.page_offset, shape=(npg,)).copy(), None, flatness=params.flatness,
+                               rowmap=params.rowmap, keep=keep)
+        lowered.pages = params.pages
+        rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1, 3)[src]
+        self.record_path_batch_ex(lowered, rgb, low["clip_rects"])
+
     def record_stroke_batch(self, params: PathBatchParams, strokes, path_rgb: np.ndarray | None = None,
                             clip_rects: np.ndarray | None = None):
         """Paint the batch in path order: path p stroked with strokes[p] (a
@@ -591,6 +613,49 @@ def stroke_params(strokes, keep: list) -> "C.Array":
         arr[i].line_join = int(d.get("line_join", RRB_JOIN_MITER))
         arr[i].stroke = 1
     return arr
+
+
+def lower_clip_paths(params: PathBatchParams, clip_paths, clip_rects=None) -> dict:
+    """rrb_lower_clip_paths (host): the batch with clip_paths[p] = (pts, flags, even_odd) or None per path and
+    optional clip_rects [n_paths, 4], as a rectangle-clipped batch: dict of pts [n, 2], flags, path_pt_off,
+    fill_rule, src_path (the input path of each lowered path) and clip_rects [m, 4]."""
+    n = int(params.n_paths)
+    keep = []
+    cps = None
+    if clip_paths is not None:
+        cps = (ClipPath * max(1, n))()
+        for i, c in enumerate(clip_paths):
+            if c is None:
+                continue
+            pts, fl, eo = c
+            a = np.ascontiguousarray(pts, np.float64).reshape(-1)
+            f = np.ascontiguousarray(fl, np.uint8)
+            keep += [a, f]
+            cps[i].pts = _ptr(a, C.c_double)
+            cps[i].flags = _ptr(f, C.c_uint8)
+            cps[i].n_pts = f.size
+            cps[i].even_odd = int(bool(eo))
+    rect = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
+    rp = None if rect is None else _ptr(rect, C.c_double)
+    npt, npa = C.c_uint64(), C.c_uint64()
+    rc = lib().rrb_lower_clip_paths(C.byref(params), rp, cps, None, None, 0, None, None, None, None, 0,
+                                    C.byref(npt), C.byref(npa))
+    if rc:
+        raise BackendError(rc, "rrb_lower_clip_paths")
+    m, k = npt.value, npa.value
+    pts = np.zeros(2 * max(1, m), np.float64)
+    fl = np.zeros(max(1, m), np.uint8)
+    off = np.zeros(k + 1, np.uint64)
+    src = np.zeros(max(1, k), np.uint64)
+    rule = np.zeros(max(1, k), np.uint8)
+    rects = np.zeros(4 * max(1, k), np.float64)
+    rc = lib().rrb_lower_clip_paths(C.byref(params), rp, cps, _ptr(pts, C.c_double), _ptr(fl, C.c_uint8), m,
+                                    _ptr(off, C.c_uint64), _ptr(src, C.c_uint64), _ptr(rule, C.c_uint8),
+                                    _ptr(rects, C.c_double), k + 1, C.byref(npt), C.byref(npa))
+    if rc:
+        raise BackendError(rc, "rrb_lower_clip_paths")
+    return dict(pts=pts[: 2 * m].reshape(m, 2), flags=fl[:m], path_pt_off=off, fill_rule=rule[:k],
+                src_path=src[:k].astype(np.int64), clip_rects=rects[: 4 * k].reshape(k, 4))
 
 
 def stroke_outline(pts, flags, flatness: float = 0.1, **stroke):

@@ -147,6 +147,11 @@ class StrokeParams(C.Structure):
                 ("line_join", C.c_uint8), ("stroke", C.c_uint8), ("reserved", C.c_uint8)]
 
 
+class ClipPath(C.Structure):
+    _fields_ = [("pts", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_uint8)), ("n_pts", C.c_uint64),
+                ("even_odd", C.c_uint8), ("reserved", C.c_uint8 * 7)]
+
+
 class SceneParams(C.Structure):
     _fields_ = [
         ("kind", C.c_uint32),
@@ -190,6 +195,11 @@ SIGNATURES = {
     "rrb_wait_page": (C.c_int, [VP, C.c_uint64, C.c_uint64]),
     "rrb_record_path_fill": (C.c_int, [VP, C.POINTER(PathFillParams)]),
     "rrb_record_path_fill_static": (C.c_int, [VP, C.POINTER(PathFillParams)]),
+    "rrb_lower_clip_paths": (C.c_int, [C.POINTER(PathBatchParams), C.POINTER(C.c_double), C.POINTER(ClipPath),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.c_uint64,
+                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint8),
+                                       C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_uint64)]),
     "rrb_record_path_batch_ex": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8),
                                            C.POINTER(C.c_double)]),
     "rrb_record_path_batch_rgb": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8)]),

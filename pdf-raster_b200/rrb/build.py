@@ -21,7 +21,7 @@ CSRC = ROOT / "csrc"
 INCLUDE = ROOT.parent / "include"
 LIB = PKG_DIR / "librrb.so"
 
-SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "rrb_encode.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp", CSRC / "rrb_stroke.cpp"]
+SOURCES = [CSRC / "rrb_backend.cu", CSRC / "rrb_static.cu", CSRC / "rrb_fills.cu", CSRC / "rrb_mlp.cu", CSRC / "rrb_features.cpp", CSRC / "rrb_encode.cpp", CSRC / "path_scene.cpp", CSRC / "rrb_server.cpp", CSRC / "rrb_stroke.cpp", CSRC / "rrb_clip.cu"]
 DEPS = SOURCES + [CSRC / "rrb_kernels.cuh", CSRC / "rrb_device.cuh", CSRC / "rrb_hairline.cuh", CSRC / "rrb_stroke.h", INCLUDE / "rrb.h"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,170 @@
+"""F3 clip paths through the product: rrb_lower_clip_paths lowers a batch with
+a clip path per fill onto the rectangle-clipped batch of
+rrb_record_path_batch_ex (a fill under a clip path paints the clip path at a
+quarter of its size, in its paint and the clip's rule, on its pixel rows:
+Clip::clip_aa_line, crates/raster/src/clip.rs:246-254, with the clip's XPath
+built without aa_scale, pdf_interp/src/renderer/page/mod.rs:1003-1009).
+
+CPU: the lowered batch rendered by the oracle's rectangle-clip renderer equals
+the oracle's literal clip-path fill (or_fill_path_clip_path), path after path
+on one page. GPU: the device's page for the same batch, through the C ABI.
+"""
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+W, H = 72, 56
+
+
+def _poly(points, closed=True):
+    pts = [tuple(p) for p in points]
+    fl = [1] + [0] * (len(pts) - 1)
+    if closed:
+        if pts[0] != pts[-1]:
+            pts.append(pts[0])
+            fl.append(0)
+        fl[0] |= 4
+        fl[-1] |= 4
+    fl[-1] |= 2
+    return np.array(pts, float), np.array(fl, np.uint8)
+
+
+def _random_poly(rng, n, lo, hi, rmax=30):
+    c = rng.uniform(lo, hi)
+    ang = np.sort(rng.uniform(0, 2 * np.pi, n))
+    r = rng.uniform(3, rmax, n)
+    return _poly(np.stack([c[0] + r * np.cos(ang), c[1] + r * np.sin(ang)], 1))
+
+
+def _random_curvy(rng, n, lo, hi):
+    c = rng.uniform(lo, hi)
+    ang = np.sort(rng.uniform(0, 2 * np.pi, n))
+    r = rng.uniform(5, 40, n)
+    v = np.stack([c[0] + r * np.cos(ang), c[1] + r * np.sin(ang)], 1)
+    pts, fl = [v[0]], [1]
+    for k in range(n):
+        a, b = v[k], v[(k + 1) % n]
+        pts += [a + rng.normal(0, 10, 2), b + rng.normal(0, 10, 2), b]
+        fl += [8, 8, 0]
+    fl[0] |= 4
+    fl[-1] |= 4 | 2
+    return np.array(pts, float), np.array(fl, np.uint8)
+
+
+class _Scene:
+    def __init__(self, paths, rule, gray, alpha):
+        self.pts = np.concatenate([p for p, _ in paths]).reshape(-1, 2)
+        self.flags = np.concatenate([f for _, f in paths])
+        self.path_pt_off = np.cumsum([0] + [len(f) for _, f in paths]).astype(np.uint64)
+        self.fill_rule = np.asarray(rule, np.uint8)
+        self.gray = np.asarray(gray, np.uint8)
+        self.alpha = np.asarray(alpha, np.uint8)
+        self.path_page = np.zeros(len(paths), np.uint32)
+        self.page_width, self.page_height = np.array([W], np.uint32), np.array([H], np.uint32)
+        self.page_offset = np.zeros(1, np.uint64)
+        self.n_paths = len(paths)
+
+
+def _batch(rng, n_paths):
+    """Paths, paint, clip rectangles and clip paths of one seeded batch."""
+    paths, rule, gray, alpha, rects, clips = [], [], [], [], [], []
+    for i in range(n_paths):
+        paths.append(_random_poly(rng, int(rng.integers(3, 9)), [6, 6], [66, 50]))
+        rule.append(int(rng.random() < 0.3))
+        gray.append(int(rng.integers(0, 256)))
+        alpha.append(int(rng.choice([255, int(rng.integers(40, 255))])))
+        kind = i % 6
+        rect = None
+        if kind in (1, 3):
+            x0, y0 = rng.uniform(-5, 50, 2)
+            rect = [x0, y0, x0 + rng.uniform(3, 40), y0 + rng.uniform(3, 30)]
+        rects.append(rect if rect is not None else [-1e9, -1e9, 1e9, 1e9])
+        if kind in (2, 3):
+            cp = _random_poly(rng, int(rng.integers(3, 9)), [20, 20], [260, 200], rmax=90)
+        elif kind == 4:
+            cp = _random_curvy(rng, int(rng.integers(2, 5)), [40, 40], [240, 180])
+        elif kind == 5:  # a rectangle: detect_rect makes it a rectangle clip
+            x0, y0 = rng.uniform(0, 50, 2)
+            w = rng.uniform(4, 30)
+            cp = _poly([(x0, y0), (x0 + w, y0), (x0 + w, y0 + 15), (x0, y0 + 15)])
+        else:
+            cp = None
+        clips.append(None if cp is None else (cp[0], cp[1], bool(rng.random() < 0.5)))
+    return paths, rule, gray, alpha, np.array(rects, float), clips
+
+
+def _expected(oracle, paths, rule, gray, alpha, rects, clips):
+    page = np.full((H, W), 255, np.uint8)
+    for i, (p, f) in enumerate(paths):
+        r = rects[i]
+        if clips[i] is not None:
+            cp, cf, ceo = clips[i]
+            oracle.fill_path_clip_path(page, p, f, cp, cf, clip_eo=ceo, eo=bool(rule[i]), gray=gray[i],
+                                       alpha=alpha[i], clip_rect=r)
+        else:
+            flat = page.reshape(-1)
+            oracle.render_scene_ex(_Scene([(p, f)], [rule[i]], [gray[i]], [alpha[i]]), flat, clip=r.reshape(1, 4))
+    return page
+
+
+def _params(rrb_lib, paths, rule, gray, alpha, keep, pages=None):
+    s = _Scene(paths, rule, gray, alpha)
+    return rrb_lib.batch_params(s.pts, s.flags, s.path_pt_off, s.fill_rule, s.gray, s.alpha, s.path_page,
+                                s.page_width, s.page_height, s.page_offset, pages, keep=keep), s
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_lowered_batch_paints_the_oracle_clip(oracle, rrb_lib, seed):
+    rng = np.random.default_rng(seed)
+    paths, rule, gray, alpha, rects, clips = _batch(rng, 18)
+    keep = []
+    params, s = _params(rrb_lib, paths, rule, gray, alpha, keep)
+    low = rrb_lib.lower_clip_paths(params, clips, rects)
+    src = low["src_path"]
+    lowered = SimpleNamespace(pts=low["pts"], flags=low["flags"], path_pt_off=low["path_pt_off"],
+                              fill_rule=low["fill_rule"], gray=s.gray[src], alpha=s.alpha[src],
+                              path_page=np.zeros(len(src), np.uint32), page_width=s.page_width,
+                              page_height=s.page_height, page_offset=s.page_offset)
+    got = np.full(W * H, 255, np.uint8)
+    oracle.render_scene_ex(lowered, got, clip=low["clip_rects"])
+    exp = _expected(oracle, paths, rule, gray, alpha, rects, clips)
+    assert np.array_equal(got.reshape(H, W), exp)
+    assert (exp != 255).any()
+
+
+def test_lowering_needs_identity_and_documented_rows(rrb_lib):
+    p, f = _poly([(1, 1), (20, 3), (9, 18)])
+    keep = []
+    params, _ = _params(rrb_lib, [(p, f)], [0], [0], [255], keep)
+    params.matrix[0] = 2.0
+    with pytest.raises(rrb_lib.BackendError):
+        rrb_lib.lower_clip_paths(params, [(p, f, False)])
+    params.matrix[0] = 1.0
+    params.rowmap = rrb_lib.RRB_ROWMAP_AS_SHIPPED
+    with pytest.raises(rrb_lib.BackendError):
+        rrb_lib.lower_clip_paths(params, [(p, f, False)])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_clip_paths_on_the_device_match_oracle(backend, oracle, rrb_lib, seed):
+    rng = np.random.default_rng(seed)
+    paths, rule, gray, alpha, rects, clips = _batch(rng, 18)
+    exp = _expected(oracle, paths, rule, gray, alpha, rects, clips)
+    pages = backend.alloc_device(W * H)
+    keep = []
+    params, _ = _params(rrb_lib, paths, rule, gray, alpha, keep, pages)
+    try:
+        backend.begin_page()
+        try:
+            backend.record_fill_buffer(pages, 255)
+            backend.record_path_batch_clip_paths(params, clips, rects)
+        finally:
+            backend.wait_page(backend.submit_page())
+        got = np.empty(W * H, np.uint8)
+        backend.wait_download(backend.download_async(pages, got))
+    finally:
+        backend.free_device(pages)
+    assert np.array_equal(got.reshape(H, W), exp)
