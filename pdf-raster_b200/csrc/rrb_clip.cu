@@ -223,7 +223,8 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
                                     uint64_t pts_cap, uint64_t* out_path_pt_off, uint64_t* out_src_path,
                                     uint8_t* out_rule, double* out_clip_rects, uint64_t paths_cap,
                                     uint64_t* n_pts_out, uint64_t* n_paths_out) {
-    if (!p || !n_pts_out || !n_paths_out || (p->n_paths && (!p->path_pt_off || !p->fill_rule || !p->path_page)))
+    if (!p || !n_pts_out || !n_paths_out || (p->n_paths && (!p->path_pt_off || !p->fill_rule || !p->path_page)) ||
+        (p->n_pts && (!p->pts || !p->flags)) || (p->n_pages && (!p->page_width || !p->page_height)))
         return RRB_ERR_INVARIANT;
     static const double kIdentity[6] = {1.0, 0.0, 0.0, 1.0, 0.0, 0.0};
     for (int k = 0; k < 6; ++k)

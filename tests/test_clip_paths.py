@@ -145,6 +145,14 @@ def test_lowering_needs_identity_and_documented_rows(rrb_lib):
     params.rowmap = rrb_lib.RRB_ROWMAP_AS_SHIPPED
     with pytest.raises(rrb_lib.BackendError):
         rrb_lib.lower_clip_paths(params, [(p, f, False)])
+    params.rowmap = rrb_lib.RRB_ROWMAP_DOCUMENTED
+    params.path_page[0] = 3  # no such page
+    with pytest.raises(rrb_lib.BackendError):
+        rrb_lib.lower_clip_paths(params, [(p, f, False)])
+    params.path_page[0] = 0
+    params.pts = None  # points missing
+    with pytest.raises(rrb_lib.BackendError):
+        rrb_lib.lower_clip_paths(params, [(p, f, False)])
 
 
 @pytest.mark.gpu
