@@ -260,19 +260,23 @@ int rrb_record_path_batch_rgb(rrb_ctx* ctx, const rrb_path_batch_params* p, cons
 int rrb_record_path_batch_ex(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb,
                              const double* clip_rects);
 /* ---- clip paths (W / W* on a path that is not an axis-aligned rectangle) ----
- * A clip path of one fill: points and PathBuilder flags in user space (the
- * batch matrix applies); n_pts 0 for none. */
-typedef struct {
+ * A fill's clip paths: points and PathBuilder flags in user space (the batch
+ * matrix applies), applied in order from the first through `next` as
+ * successive Clip::clip_to_path calls. An entry without points and without a
+ * `next` means no clip path; an entry without points in a stack is an empty
+ * path, which lets nothing through (clip.rs:142-148). */
+typedef struct rrb_clip_path_s {
     const double* pts;
     const uint8_t* flags;
     uint64_t n_pts;
     uint8_t even_odd;     /* W* */
     uint8_t reserved[7];
+    const struct rrb_clip_path_s* next;
 } rrb_clip_path;
 /* Host only; no counterpart in the reference, which clips inside fill_impl.
  * Lowers a batch whose path i is clipped to its page, clip_rects[4i..4i+3]
- * (when clip_rects != NULL) and clip_paths[i] (when clip_paths != NULL and
- * its n_pts > 0) onto a batch for rrb_record_path_batch_ex with clip
+ * (when clip_rects != NULL) and the clip paths of clip_paths[i] (when
+ * clip_paths != NULL) onto a batch for rrb_record_path_batch_ex with clip
  * rectangles. The pixels are the reference's: Clip::clip_aa_line
  * (crates/raster/src/clip.rs:246-254) lets the clip path's scanner draw its
  * own coverage into the fill's AA lines, and the renderer builds the clip's
@@ -281,14 +285,15 @@ typedef struct {
  * size, in the fill's paint and the clip's rule, on the fill's pixel rows
  * (nothing when the fill's box lies outside the clip rectangle); a clip path
  * that detect_rect (clip.rs:322-359) finds to be a rectangle clips as that
- * rectangle. Lowered path k comes from input path out_src_path[k] (its gray,
+ * rectangle; of a stack, the last other clip path is drawn (each clip
+ * scanner overwrites the AA lines in turn) within the intersection of the
+ * rectangles. Lowered path k comes from input path out_src_path[k] (its gray,
  * alpha, page and colour), has fill rule out_rule[k] and clip rectangle
  * out_clip_rects[4k..4k+3]; its points are out_pts / out_flags from
  * out_path_pt_off[k] to out_path_pt_off[k + 1]. Any output may be NULL;
  * *n_pts_out and *n_paths_out always receive the sizes, and
  * RRB_ERR_POOL_EXHAUSTED says an output was too small. Needs the identity
- * matrix (the renderer's DEVICE_MATRIX) and RRB_ROWMAP_DOCUMENTED; one clip
- * path per fill. */
+ * matrix (the renderer's DEVICE_MATRIX) and RRB_ROWMAP_DOCUMENTED. */
 int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double* clip_rects, const rrb_clip_path* clip_paths,
                          double* out_pts, uint8_t* out_flags, uint64_t pts_cap, uint64_t* out_path_pt_off,
                          uint64_t* out_src_path, uint8_t* out_rule, double* out_clip_rects, uint64_t paths_cap,

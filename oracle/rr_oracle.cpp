@@ -1437,18 +1437,27 @@ void or_fill_path(uint8_t* page, int32_t width, int32_t height, const double* pt
                    });
 }
 
-void or_fill_path_clip_path(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
-                            int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
-                            int rowmap, const double* clip_rect, const double* clip_pts, const uint8_t* clip_flags,
-                            int64_t clip_n, int clip_eo, or_stats* st) {
+void or_fill_path_clip_paths(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                             int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
+                             int rowmap, const double* clip_rect, int64_t n_clips, const double* const* clip_pts,
+                             const uint8_t* const* clip_flags, const int64_t* clip_n, const int* clip_eo,
+                             or_stats* st) {
     ClipState cs;
     cs.r = make_clip(width, height, clip_rect);
-    clip_to_path(cs, clip_pts, clip_flags, clip_n, m, flatness, clip_eo, st);
+    for (int64_t k = 0; k < n_clips; ++k) clip_to_path(cs, clip_pts[k], clip_flags[k], clip_n[k], m, flatness, clip_eo[k], st);
     fill_path_impl(width, height, pts, flags, n_pts, m, flatness, eo, rowmap, st,
                    [&](int32_t y, int32_t x0, const uint8_t* shape, int64_t n) {
                        or_render_span_aa_gray(page + static_cast<int64_t>(y) * width + x0, shape, n, alpha, gray);
                    },
                    nullptr, &cs);
+}
+
+void or_fill_path_clip_path(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                            int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
+                            int rowmap, const double* clip_rect, const double* clip_pts, const uint8_t* clip_flags,
+                            int64_t clip_n, int clip_eo, or_stats* st) {
+    or_fill_path_clip_paths(page, width, height, pts, flags, n_pts, m, flatness, eo, gray, alpha, rowmap, clip_rect, 1,
+                            &clip_pts, &clip_flags, &clip_n, &clip_eo, st);
 }
 
 void or_fill_path_rgb(uint8_t* page_rgb, int32_t width, int32_t height, const double* pts, const uint8_t* flags,

@@ -143,6 +143,13 @@ void or_fill_path_clip_path(uint8_t* page, int32_t width, int32_t height, const 
                             int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
                             int rowmap, const double* clip_rect, const double* clip_pts, const uint8_t* clip_flags,
                             int64_t clip_n, int clip_eo, or_stats* st);
+/* The same under a stack of clip paths, clip_to_path applied in order
+ * (clip_pts[k] / clip_flags[k] / clip_n[k] / clip_eo[k]). */
+void or_fill_path_clip_paths(uint8_t* page, int32_t width, int32_t height, const double* pts, const uint8_t* flags,
+                             int64_t n_pts, const double m[6], double flatness, int eo, uint8_t gray, uint8_t alpha,
+                             int rowmap, const double* clip_rect, int64_t n_clips, const double* const* clip_pts,
+                             const uint8_t* const* clip_flags, const int64_t* clip_n, const int* clip_eo,
+                             or_stats* st);
 
 /* The same fill onto an Rgb8 page (3 bytes per pixel, row stride 3 * width)
  * with a solid RGB source, through composite_aa_rgb8_opaque (A12). */

@@ -101,6 +101,10 @@ def lib() -> C.CDLL:
             "or_rgb_to_gray": (None, [C.POINTER(U8), C.POINTER(U8), I64]),
             "or_fill_path": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D), D,
                                     C.c_int, U8, U8, C.c_int, C.POINTER(Stats)]),
+            "or_fill_path_clip_paths": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64,
+                                               C.POINTER(D), D, C.c_int, U8, U8, C.c_int, C.POINTER(D), I64,
+                                               C.POINTER(C.POINTER(D)), C.POINTER(C.POINTER(U8)), C.POINTER(I64),
+                                               C.POINTER(C.c_int), C.POINTER(Stats)]),
             "or_fill_path_clip_path": (None, [C.POINTER(U8), I32, I32, C.POINTER(D), C.POINTER(U8), I64, C.POINTER(D),
                                               D, C.c_int, U8, U8, C.c_int, C.POINTER(D), C.POINTER(D), C.POINTER(U8),
                                               I64, C.c_int, C.POINTER(Stats)]),
@@ -339,6 +343,28 @@ def fill_path_clip_path(page: np.ndarray, pts, flags, clip_pts, clip_flags, clip
                                  _p(flags, C.c_uint8), flags.size, _mat(matrix), flatness, int(eo), gray, alpha, rowmap,
                                  None if rect is None else _p(rect, C.c_double), _p(cpts, C.c_double),
                                  _p(cfl, C.c_uint8), cfl.size, int(clip_eo), C.byref(st))
+    return st.as_dict()
+
+
+def fill_path_clip_paths(page: np.ndarray, pts, flags, clips, eo=False, gray=0, alpha=255,
+                         rowmap=ROWMAP_DOCUMENTED, clip_rect=None, matrix=IDENTITY, flatness=0.1) -> dict:
+    """fill_path_clip_path under a stack of clip paths: clips = [(pts, flags, even_odd), ...], applied in order."""
+    assert page.dtype == np.uint8 and page.flags["C_CONTIGUOUS"] and page.ndim == 2
+    pts = np.ascontiguousarray(pts, np.float64).reshape(-1)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    cp = [np.ascontiguousarray(c[0], np.float64).reshape(-1) for c in clips]
+    cf = [np.ascontiguousarray(c[1], np.uint8) for c in clips]
+    n = len(clips)
+    pp = (C.POINTER(C.c_double) * max(1, n))(*[_p(a, C.c_double) for a in cp])
+    fp = (C.POINTER(C.c_uint8) * max(1, n))(*[_p(a, C.c_uint8) for a in cf])
+    ns = (C.c_int64 * max(1, n))(*[a.size for a in cf])
+    eos = (C.c_int * max(1, n))(*[int(bool(c[2])) for c in clips])
+    rect = None if clip_rect is None else np.ascontiguousarray(clip_rect, np.float64).reshape(4)
+    st = Stats()
+    lib().or_fill_path_clip_paths(_p(page, C.c_uint8), page.shape[1], page.shape[0], _p(pts, C.c_double),
+                                  _p(flags, C.c_uint8), flags.size, _mat(matrix), flatness, int(eo), gray, alpha,
+                                  rowmap, None if rect is None else _p(rect, C.c_double), n, pp, fp, ns, eos,
+                                  C.byref(st))
     return st.as_dict()
 
 

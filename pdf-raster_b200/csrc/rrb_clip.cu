@@ -23,8 +23,9 @@
 // clip's columns and the fill's pixel rows (the documented row map: one
 // render_aa_line per pixel row). A clip path that detect_rect (clip.rs:
 // 322-359) reduces to a rectangle becomes a rectangle clip of the fill itself.
-// One clip path per fill; the batch matrix must be the identity, as the
-// renderer's DEVICE_MATRIX is (page/mod.rs:177).
+// Of a stack of clip paths the last one that is not a rectangle is drawn:
+// every scanner renders the same AA line in turn. The batch matrix must be
+// the identity, as the renderer's DEVICE_MATRIX is (page/mod.rs:177).
 
 #include <cmath>
 #include <cstdint>
@@ -245,23 +246,41 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
             const double* r = clip_rects + 4 * i;
             c.clip_to(r[0], r[1], r[2], r[3]);
         }
-        const rrb_clip_path* cp = clip_paths ? clip_paths + i : nullptr;
-        const bool has_clip = cp && cp->n_pts > 0;
-        if (!has_clip) {
-            // No clip path: the fill itself under its rectangle.
-            const uint64_t first = o.n_pts;
-            for (uint64_t k = a; k < b; ++k) o.point(p->pts[2 * k], p->pts[2 * k + 1], p->flags[k]);
-            o.path(i, p->fill_rule[i], c, c.y_min, c.y_max, first);
-            continue;
-        }
-        if (!cp->pts || !cp->flags) return RRB_ERR_INVARIANT;
+        const rrb_clip_path* head = clip_paths ? clip_paths + i : nullptr;
+        const bool has_clip = head && (head->n_pts > 0 || head->next);
+        // The stack in order: empty paths empty the clip, rectangles narrow it,
+        // and the last other clip path is the one whose coverage is drawn.
+        bool have_path = false, emptied = false, eo_last = false;
         segs.clear();
         starts.clear();
-        xpath_segments(cp->pts, cp->flags, cp->n_pts, p->matrix, flat_sq, segs, starts);
-        if (segs.empty()) continue;  // an empty clip path: nothing passes (clip.rs:142-148)
-        double rx0, ry0, rx1, ry1;
-        if (detect_rect(segs, rx0, ry0, rx1, ry1)) {
-            c.clip_to(rx0, ry0, rx1, ry1);
+        int depth = 0;
+        for (const rrb_clip_path* e = has_clip ? head : nullptr; e; e = e->next) {
+            if (++depth > 4096) return RRB_ERR_INVARIANT;  // a cycle
+            if (e->n_pts && (!e->pts || !e->flags)) return RRB_ERR_INVARIANT;
+            std::vector<Seg> es;
+            std::vector<size_t> est;
+            if (e->n_pts) xpath_segments(e->pts, e->flags, e->n_pts, p->matrix, flat_sq, es, est);
+            if (es.empty()) {
+                emptied = true;  // clip.rs:142-148
+                continue;
+            }
+            double rx0, ry0, rx1, ry1;
+            if (detect_rect(es, rx0, ry0, rx1, ry1)) {
+                c.clip_to(rx0, ry0, rx1, ry1);
+                continue;
+            }
+            segs.swap(es);
+            starts.swap(est);
+            eo_last = e->even_odd != 0;
+            have_path = true;
+        }
+        // A clip with no integer column or row paints nothing (test_rect is
+        // AllOutside, or the clamped span is empty). The device would read an
+        // inverted rectangle as its normalised corners, so such paths are
+        // dropped; an inverted one with a column left (floor(x_min) ==
+        // ceil(x_max) - 1) normalises to the same integer bounds.
+        if (emptied || c.x_min_i > c.x_max_i || c.y_min_i > c.y_max_i) continue;
+        if (!have_path) {
             const uint64_t first = o.n_pts;
             for (uint64_t k = a; k < b; ++k) o.point(p->pts[2 * k], p->pts[2 * k + 1], p->flags[k]);
             o.path(i, p->fill_rule[i], c, c.y_min, c.y_max, first);
@@ -288,7 +307,7 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
                 o.point(rrb::dmul(segs[e].x1, 0.25), rrb::dmul(segs[e].y1, 0.25), e + 1 == e1 ? PF_LAST : 0);
         }
         // Rows top..bottom of the fill's loop (clamped to the page by the device).
-        o.path(i, cp->even_odd ? 1 : 0, c, static_cast<double>(top), static_cast<double>(bottom) + 1.0, first);
+        o.path(i, eo_last ? 1 : 0, c, static_cast<double>(top), static_cast<double>(bottom) + 1.0, first);
     }
     if (out_path_pt_off && o.n_paths < paths_cap) out_path_pt_off[o.n_paths] = o.n_pts;
     *n_pts_out = o.n_pts;

@@ -395,8 +395,8 @@ class B200Backend:
 
     def record_path_batch_clip_paths(self, params: PathBatchParams, clip_paths, clip_rects: np.ndarray | None = None,
                                      path_rgb: np.ndarray | None = None):
-        """The batch with a clip path per fill (clip_paths[p] = (pts, flags, even_odd) or None) and optional
-        clip rectangles: rrb_lower_clip_paths, then rrb_record_path_batch_ex on the lowered batch."""
+        """The batch with clip paths per fill (clip_paths[p] = None, (pts, flags, even_odd) or a list of them)
+        and optional clip rectangles: rrb_lower_clip_paths, then rrb_record_path_batch_ex on the lowered batch."""
         low = lower_clip_paths(params, clip_paths, clip_rects)
         n = int(params.n_paths)
         asa = np.ctypeslib.as_array
@@ -616,25 +616,40 @@ def stroke_params(strokes, keep: list) -> "C.Array":
 
 
 def lower_clip_paths(params: PathBatchParams, clip_paths, clip_rects=None) -> dict:
-    """rrb_lower_clip_paths (host): the batch with clip_paths[p] = (pts, flags, even_odd) or None per path and
-    optional clip_rects [n_paths, 4], as a rectangle-clipped batch: dict of pts [n, 2], flags, path_pt_off,
-    fill_rule, src_path (the input path of each lowered path) and clip_rects [m, 4]."""
+    """rrb_lower_clip_paths (host): the batch with clip_paths[p] = None, (pts, flags, even_odd), or a list of
+    them (a stack applied in order) per path and optional clip_rects [n_paths, 4], as a rectangle-clipped
+    batch: dict of pts [n, 2], flags, path_pt_off, fill_rule, src_path (the input path of each lowered path)
+    and clip_rects [m, 4]."""
     n = int(params.n_paths)
     keep = []
     cps = None
+
+    def fill(entry, c):
+        pts, fl, eo = c
+        a = np.ascontiguousarray(pts, np.float64).reshape(-1)
+        f = np.ascontiguousarray(fl, np.uint8)
+        keep.extend((a, f))
+        entry.pts = _ptr(a, C.c_double) if f.size else None
+        entry.flags = _ptr(f, C.c_uint8) if f.size else None
+        entry.n_pts = f.size
+        entry.even_odd = int(bool(eo))
+
     if clip_paths is not None:
         cps = (ClipPath * max(1, n))()
         for i, c in enumerate(clip_paths):
             if c is None:
                 continue
-            pts, fl, eo = c
-            a = np.ascontiguousarray(pts, np.float64).reshape(-1)
-            f = np.ascontiguousarray(fl, np.uint8)
-            keep += [a, f]
-            cps[i].pts = _ptr(a, C.c_double)
-            cps[i].flags = _ptr(f, C.c_uint8)
-            cps[i].n_pts = f.size
-            cps[i].even_odd = int(bool(eo))
+            stack = list(c) if isinstance(c, list) else [c]
+            fill(cps[i], stack[0])
+            if len(stack) > 1:
+                rest = (ClipPath * (len(stack) - 1))()
+                keep.append(rest)
+                for j, cj in enumerate(stack[1:]):
+                    fill(rest[j], cj)
+                prev = cps[i]
+                for j in range(len(stack) - 1):
+                    prev.next = C.pointer(rest[j])
+                    prev = rest[j]
     rect = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
     rp = None if rect is None else _ptr(rect, C.c_double)
     npt, npa = C.c_uint64(), C.c_uint64()

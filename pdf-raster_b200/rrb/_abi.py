@@ -148,8 +148,11 @@ class StrokeParams(C.Structure):
 
 
 class ClipPath(C.Structure):
-    _fields_ = [("pts", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_uint8)), ("n_pts", C.c_uint64),
-                ("even_odd", C.c_uint8), ("reserved", C.c_uint8 * 7)]
+    pass
+
+
+ClipPath._fields_ = [("pts", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_uint8)), ("n_pts", C.c_uint64),
+                     ("even_odd", C.c_uint8), ("reserved", C.c_uint8 * 7), ("next", C.POINTER(ClipPath))]
 
 
 class SceneParams(C.Structure):

@@ -95,11 +95,33 @@ def _batch(rng, n_paths):
     return paths, rule, gray, alpha, np.array(rects, float), clips
 
 
+def _batch_stacks(rng, n_paths):
+    """Clip stacks (lists of clip paths) and clip rectangles off the page."""
+    paths, rule, gray, alpha, rects, clips = [], [], [], [], [], []
+    empty = (np.zeros((0, 2)), np.zeros(0, np.uint8), False)
+    for i in range(n_paths):
+        paths.append(_random_poly(rng, int(rng.integers(3, 9)), [6, 6], [66, 50]))
+        rule.append(int(rng.random() < 0.3))
+        gray.append(int(rng.integers(0, 256)))
+        alpha.append(int(rng.choice([255, int(rng.integers(40, 255))])))
+        a = _random_poly(rng, 6, [20, 20], [260, 200], rmax=90) + (bool(rng.random() < 0.5),)
+        b = _random_curvy(rng, 3, [40, 40], [240, 180]) + (bool(rng.random() < 0.5),)
+        x0, y0 = rng.uniform(0, 50, 2)
+        r = _poly([(x0, y0), (x0 + 25, y0), (x0 + 25, y0 + 18), (x0, y0 + 18)]) + (False,)
+        kind = i % 6
+        clips.append([[a, b], [r, a], [a, r], [a, empty, b], [r], None][kind])
+        rects.append([-30.0, 5.0, -2.0, 40.0] if i % 7 == 3 else [-1e9, -1e9, 1e9, 1e9])
+    return paths, rule, gray, alpha, np.array(rects, float), clips
+
+
 def _expected(oracle, paths, rule, gray, alpha, rects, clips):
     page = np.full((H, W), 255, np.uint8)
     for i, (p, f) in enumerate(paths):
         r = rects[i]
-        if clips[i] is not None:
+        if isinstance(clips[i], list):
+            oracle.fill_path_clip_paths(page, p, f, clips[i], eo=bool(rule[i]), gray=gray[i], alpha=alpha[i],
+                                        clip_rect=r)
+        elif clips[i] is not None:
             cp, cf, ceo = clips[i]
             oracle.fill_path_clip_path(page, p, f, cp, cf, clip_eo=ceo, eo=bool(rule[i]), gray=gray[i],
                                        alpha=alpha[i], clip_rect=r)
@@ -115,10 +137,10 @@ def _params(rrb_lib, paths, rule, gray, alpha, keep, pages=None):
                                 s.page_width, s.page_height, s.page_offset, pages, keep=keep), s
 
 
-@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 10, 11, 12])
 def test_lowered_batch_paints_the_oracle_clip(oracle, rrb_lib, seed):
     rng = np.random.default_rng(seed)
-    paths, rule, gray, alpha, rects, clips = _batch(rng, 18)
+    paths, rule, gray, alpha, rects, clips = (_batch if seed < 10 else _batch_stacks)(rng, 18)
     keep = []
     params, s = _params(rrb_lib, paths, rule, gray, alpha, keep)
     low = rrb_lib.lower_clip_paths(params, clips, rects)
@@ -132,6 +154,21 @@ def test_lowered_batch_paints_the_oracle_clip(oracle, rrb_lib, seed):
     exp = _expected(oracle, paths, rule, gray, alpha, rects, clips)
     assert np.array_equal(got.reshape(H, W), exp)
     assert (exp != 255).any()
+
+
+def test_disjoint_rectangles_paint_nothing(oracle, rrb_lib):
+    """A clip rectangle and a rectangle clip path that do not meet leave an
+    inverted rectangle, which is empty; the lowering drops the fill (the
+    device would read the inverted corners as a rectangle)."""
+    p, f = _poly([(2, 2), (60, 4), (50, 50), (3, 40)])
+    rect_path = _poly([(20, 5), (40, 5), (40, 30), (20, 30)]) + (False,)
+    keep = []
+    params, _ = _params(rrb_lib, [(p, f)], [0], [0], [255], keep)
+    low = rrb_lib.lower_clip_paths(params, [rect_path], np.array([[0.0, 0.0, 10.0, 56.0]]))
+    assert len(low["src_path"]) == 0
+    page = np.full((H, W), 255, np.uint8)
+    oracle.fill_path_clip_paths(page, p, f, [rect_path], clip_rect=[0.0, 0.0, 10.0, 56.0])
+    assert (page == 255).all()
 
 
 def test_lowering_needs_identity_and_documented_rows(rrb_lib):

@@ -142,3 +142,28 @@ def test_clip_path_output_depends_on_the_fill_rows_only(oracle, rowmap):
             assert np.array_equal(a, b), i
             compared += 1
     assert compared >= 30
+
+
+def test_clip_path_stacks(oracle):
+    """A stack of clip paths (successive W): each scanner overwrites the AA
+    lines, so the last non-rectangular clip path is drawn; rectangle clip
+    paths narrow the rectangle wherever they stand; an empty path lets
+    nothing through."""
+    rng = np.random.default_rng(4)
+    for i in range(30):
+        pts, fl = _random_poly(rng, int(rng.integers(3, 9)), [8, 8], [56, 40])
+        ca = _random_poly(rng, 6, [20, 20], [200, 150]) + (bool(i % 2),)
+        cb = _random_curvy(rng, 3, [30, 30], [200, 150]) + (False,)
+        x0, y0 = rng.uniform(0, 30, 2)
+        rect = (x0, y0, x0 + rng.uniform(5, 30), y0 + rng.uniform(5, 20))
+        rp = _poly([(rect[0], rect[1]), (rect[2], rect[1]), (rect[2], rect[3]), (rect[0], rect[3])]) + (False,)
+        ref = np.full((H, W), 255, np.uint8)
+        oracle.fill_path_clip_path(ref, pts, fl, cb[0], cb[1], clip_eo=cb[2], gray=9, clip_rect=rect)
+        for stack in ([ca, rp, cb], [rp, ca, cb], [ca, cb, rp]):
+            got = np.full((H, W), 255, np.uint8)
+            oracle.fill_path_clip_paths(got, pts, fl, stack, gray=9)
+            assert np.array_equal(got, ref), (i, len(stack))
+        empty = (np.zeros((0, 2)), np.zeros(0, np.uint8), False)
+        got = np.full((H, W), 255, np.uint8)
+        oracle.fill_path_clip_paths(got, pts, fl, [ca, empty, cb], gray=9)
+        assert (got == 255).all()
