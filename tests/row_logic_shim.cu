@@ -2,14 +2,16 @@
 // tests (tests/test_row_logic.py): flatten_curve, make_edge and edge_entry
 // (segment set-up and per-row entries), walk_row (the winding walk of one AA
 // row into spans), sweep_cells (four AA rows' spans into a pixel row's
-// coverage cells), recti_row_spans (rectilinear paths) and the hairline spans
-// (hl_clip, hl_segment, hl_row_span). All are __host__ __device__; the kernels run the same
+// coverage cells), recti_row_spans (rectilinear paths), the hairline spans
+// (hl_clip, hl_segment, hl_row_span) and the host XPath walk of the clip-path
+// lowering (rrb_clip.cu, included here for its internal functions). All are __host__ __device__; the kernels run the same
 // source on the GPU. Build with -ffp-contract=off for the host so that no
 // multiply-add is fused where the device's explicit rounding keeps them apart.
 #include <cstdint>
 #include <cstring>
 
 #include "../pdf-raster_b200/csrc/rrb_hairline.cuh"
+#include "../pdf-raster_b200/csrc/rrb_clip.cu"
 
 namespace {
 
@@ -147,4 +149,20 @@ extern "C" int rl_recti_spans(const int32_t* edges, int n, int eo, int32_t r, in
                                         span_x1, nt);
     *nonterminating = nt;
     return ns;
+}
+
+// The clip-path lowering's XPath walk (xpath_segments in rrb_clip.cu): up to
+// cap segments (x0, y0, x1, y1) in device space; returns the count.
+extern "C" int64_t rl_xpath_segments(const double* pts, const uint8_t* flags, uint64_t n, const double* m,
+                                     double flatness, double* out, int64_t cap) {
+    std::vector<Seg> segs;
+    std::vector<size_t> starts;
+    xpath_segments(pts, flags, n, m, rrb::dmul(flatness, flatness), segs, starts);
+    for (size_t k = 0; k < segs.size() && static_cast<int64_t>(k) < cap; ++k) {
+        out[4 * k] = segs[k].x0;
+        out[4 * k + 1] = segs[k].y0;
+        out[4 * k + 2] = segs[k].x1;
+        out[4 * k + 3] = segs[k].y1;
+    }
+    return static_cast<int64_t>(segs.size());
 }

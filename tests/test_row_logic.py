@@ -51,6 +51,8 @@ def shim(tmp_path_factory):
     lib.rl_recti_spans.argtypes = [i32p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p,
                                    C.POINTER(C.c_uint32)]
     lib.rl_recti_spans.restype = C.c_int
+    lib.rl_xpath_segments.argtypes = [dp, C.POINTER(C.c_uint8), C.c_uint64, dp, C.c_double, dp, C.c_int64]
+    lib.rl_xpath_segments.restype = C.c_int64
     return lib
 
 
@@ -343,3 +345,35 @@ def _path_closed(subpaths):
         fl[start] |= 4
         fl[-1] |= 4 | 2
     return np.array(pts, float), np.array(fl, np.uint8)
+
+
+def test_host_xpath_walk_matches_oracle(oracle, shim):
+    """The clip-path lowering's host walk (k_walk + k_seg_write restated) gives
+    XPath::new's segments bit for bit: lines, cubics, subpaths that close by
+    a segment or within 1e-10, a curve end marked LAST (the walk runs on into
+    the next subpath), transforms and flatness."""
+    rng = np.random.default_rng(17)
+    out = np.zeros(4 * 20000, np.float64)
+    for i in range(400):
+        pts, fl = random_path(rng, 60, 50, closed=i % 4 != 3)
+        if i % 9 == 0 and (fl & 8).any():
+            j = int(np.nonzero(fl & 8)[0][-1]) + 1  # the end point after the last control pair
+            if j < len(fl):
+                fl = fl.copy()
+                fl[j] |= 2
+        if i % 11 == 0:
+            pts = pts.copy()
+            pts[-1] = pts[0] + rng.choice([0.0, 3e-11, -5e-11, 2e-10], 2)
+        m = (1.0, 0.0, 0.0, 1.0, 0.0, 0.0) if i % 3 else tuple(rng.normal(0, 1, 6))
+        flat = float(rng.choice([0.1, 0.3, 1.0]))
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1)
+        f = np.ascontiguousarray(fl, np.uint8)
+        mm = np.array(m, np.float64)
+        n = shim.rl_xpath_segments(_dp(p), f.ctypes.data_as(C.POINTER(C.c_uint8)), f.size, _dp(mm), flat, _dp(out),
+                                   20000)
+        want = oracle.xpath_new(pts, fl, matrix=m, flatness=flat, close=True)
+        assert n == len(want), i
+        # add_segment stores flipped segments with y0 <= y1 (OR_XF_FLIPPED = 4): compare in walk order.
+        exp = np.array([(s.x1, s.y1, s.x0, s.y0) if s.flags & 4 else (s.x0, s.y0, s.x1, s.y1) for s in want],
+                       np.float64).reshape(-1)
+        assert np.array_equal(out[: 4 * n].view(np.uint64), exp.view(np.uint64)), i
