@@ -1,25 +1,34 @@
 """Benchmark of the B200 anti-aliased fill (one JSON line on rank 0).
 
-Workload (default): the glyph-dense text page — 150,000 quadratic glyph paths
-(2 contours on average, 12-60 quadratic segments each, 8-12 pt em at 300 dpi)
-on 60 baselines of one 2550x3300 u8 page initialised to 255, seed 0. A step
-renders the whole page: fill the page with 255, flatten every path in FP64,
-build the AA rows, bin paths to tiles and composite them in order.
+Workload (default): the mixed batch — 64 u8 pages whose sizes are drawn from
+{A4, Letter, A3} x {150, 300, 600} dpi (1.17 Gpixel in all), 662,271 paths:
+30% glyph outlines, 40% polygons, 30% axis-aligned rectangles covering 5-80%
+of their page, alpha 32-255, seed 0 — rendered in ONE submission. A step
+fills the pages with 255, flattens every path in FP64, builds the AA rows,
+bins paths to tiles and composites them in order. `--workload glyphs` is the
+glyph-dense text page (150,000 glyphs on one Letter @300 dpi page),
+`--workload polygons` the 2,000-path polygon page.
 
   value  Mpixel/s with the path inputs already resident in device memory
          (rrb_batch_upload once, rrb_record_batch per step), timed with CUDA
          events on the backend's own stream, max over ranks.
   e2e    the same metric through rrb_render_pages_host with pinned HOST
-         buffers: the path arrays and the page go host->device and the page
-         comes back every step.
+         buffers: the path arrays and the pages go host->device and the pages
+         come back every step.
+  bit_exact  every page of the batch against the CPU oracle: the mixed batch
+         by the SHA-256 of each page that the oracle rendered
+         (tests/golden/mixed_batch_digests.json), one-page workloads by the
+         oracle's page itself.
 
-Multi-GPU: pages are independent, so N ranks render N page replicas with no
-collective on the data path (weak scaling); only the timing barrier and the
+Multi-GPU: pages are independent, so N ranks split a multi-page batch's pages
+(strong scaling) or render replicas of a one-page workload (weak scaling),
+with no collective on the data path; only the timing barrier and the
 max-over-ranks reduction use torch.distributed.
 
 `--impl reference` times the reference CPU scanline rasterizer's
-restatement (oracle/, the reference itself is Rust and cannot be built here)
-on the host cores: each step renders one copy of the page per thread.
+restatement (oracle/; the reference itself is Rust and cannot be built here)
+on the host cores, page-parallel as the reference's per-page workers: each
+thread renders the leading paths of its own page of the batch.
 """
 
 from __future__ import annotations
@@ -45,9 +54,9 @@ WORKLOADS = {
                "glyph-dense text page: 150,000 quadratic glyph paths (2 contours avg, 12-60 quads each, "
                "8-12 pt em @300 dpi, 60 baselines) on one 2550x3300 u8 page (Letter @300 dpi), NZ, gray 0, alpha 255"),
     "mixed": (dict(kind=2, seed=0),
-              "mixed pages in one batch: 64 u8 pages of {A4, Letter, A3} x {150, 300, 600} dpi, log-normal path "
-              "count (median 5,000, sigma 1.2, cap 50,000) of 30% glyphs / 40% polygons / 30% axis-aligned "
-              "rectangles covering 5-80% of the page, alpha 32-255"),
+              "mixed pages in one batch: 64 u8 pages of {A4, Letter, A3} x {150, 300, 600} dpi (1.17 Gpixel), "
+              "log-normal path count (median 5,000, sigma 1.2, cap 50,000; 662,271 paths) of 30% glyphs / 40% "
+              "polygons / 30% axis-aligned rectangles covering 5-80% of the page, alpha 32-255, one submission"),
     "polygons": (dict(kind=0, seed=0),
                  "polygon page: 2,000 closed paths (1-3 contours x 4-32 line/cubic segments, jittered circles, "
                  "log-normal radius) on one 2550x3300 u8 page, NZ 70% / EO 30%, opaque"),
@@ -163,22 +172,75 @@ def oracle_prefix(page, arena, budget_s):
     return done, spent, ties
 
 
-def oracle_pages(scene, budget_s=20.0, page_budget_s=5.0):
-    """A bounded CPU sample of a multi-page batch: pages in batch order, each
-    rendered by the oracle on one thread for at most page_budget_s (its
-    leading paths), until budget_s in all. Returns
-    [(page, sub-scene, arena, paths done, seconds, tie rows)]."""
-    from rrb.shard import SceneShard
-    out, spent = [], 0.0
-    for pg in range(scene.n_pages):
-        sub = SceneShard(scene, pages=(pg, pg + 1))
-        a = sub.blank_arena()
-        done, secs, ties = oracle_prefix(sub, a, page_budget_s)
-        out.append((pg, sub, a, done, secs, ties))
-        spent += secs
-        if spent >= budget_s:
-            break
-    return out
+class PageParallelSample:
+    """A bounded sample of a multi-page batch for the CPU oracle, page-parallel
+    as the reference renders pages (one page per rayon worker): thread t takes
+    page t of the batch (pages reused when threads outnumber them) and renders
+    its leading paths. calibrate() finds, on all threads at once, how many
+    leading paths each renders in about budget_s; step() renders exactly those
+    paths on every thread and returns the wall time; credited_px is each
+    page's pixels times the share of its paths sampled, summed."""
+
+    def __init__(self, scene, threads, budget_s):
+        from rrb.shard import SceneShard
+        self.threads = max(1, threads)
+        self.subs = [SceneShard(scene, pages=(t % scene.n_pages, t % scene.n_pages + 1)) for t in range(self.threads)]
+        ks = [0] * self.threads
+
+        def cal(t):
+            ks[t], _, _ = oracle_prefix(self.subs[t], self.subs[t].blank_arena(), budget_s)
+
+        _run_threads(cal, self.threads)
+        self.work = [PathRange(self.subs[t], 0, max(1, ks[t])) for t in range(self.threads)]
+        self.paths = [w.fill_rule.size for w in self.work]
+        self.credited_px = sum(sub.pixels * k / max(1, sub.n_paths) for sub, k in zip(self.subs, self.paths))
+        self.arenas = [np.full(int(w.page_width[0]) * int(w.page_height[0]), 255, np.uint8) for w in self.work]
+
+    def step(self) -> float:
+        import rr_oracle
+        for a in self.arenas:
+            a.fill(255)
+        t = time.perf_counter()
+        _run_threads(lambda k: rr_oracle.render_scene(self.work[k], self.arenas[k]), self.threads)
+        return time.perf_counter() - t
+
+    def describe(self) -> str:
+        return (f"{self.threads} host threads at once, thread t on page t of the batch (its first "
+                f"{min(self.paths)}-{max(self.paths)} paths, the number each thread renders in about the budget), "
+                "credited with each page's pixels times the share of its paths rendered")
+
+
+def _run_threads(fn, n):
+    ts = [threading.Thread(target=fn, args=(k,)) for k in range(n)]
+    for x in ts:
+        x.start()
+    for x in ts:
+        x.join()
+
+
+def batch_digests_check(scene, pages_arena) -> dict | None:
+    """Compare every page of the mixed batch with the oracle's pinned SHA-256
+    digests (tests/golden/mixed_batch_digests.json, made by
+    tests/golden/make_batch_digests.py); None when the scene is not that batch."""
+    import hashlib
+    path = ROOT / "tests" / "golden" / "mixed_batch_digests.json"
+    if not path.exists() or scene.n_pages != 64:
+        return None
+    doc = json.loads(path.read_text())
+    recs = doc["records"]
+    ok, bad = 0, []
+    for rec in recs:
+        pg = rec["page"]
+        o, w, h = int(scene.page_offset[pg]), int(scene.page_width[pg]), int(scene.page_height[pg])
+        if (w, h) != (rec["width"], rec["height"]):
+            return None
+        d = hashlib.sha256(np.ascontiguousarray(pages_arena[o:o + w * h]).tobytes()).hexdigest()
+        if d == rec["page_sha256"]:
+            ok += 1
+        else:
+            bad.append(pg)
+    return {"pages_checked": len(recs), "pages_bit_exact": ok, "pages_differing": bad,
+            "reference": "SHA-256 of each page rendered by the CPU oracle (tests/golden/mixed_batch_digests.json)"}
 
 
 def run_reference(args, rank, world):
@@ -203,47 +265,40 @@ def run_reference(args, rank, world):
     else:
         kw, desc = WORKLOADS[args.workload]
         scene = rrb.Scene(**kw)
-    sample_desc, work = "the page", scene
-    px_per_copy = scene.pixels
-    if scene.n_pages > 1:
-        # A bounded sample of the batch: the leading paths of its first page
-        # that one thread renders in about 3 s, credited with that share of
-        # the page's pixels (pixels x paths done / paths on the page).
-        from rrb.shard import SceneShard
-        page0 = SceneShard(scene, pages=(0, 1))
-        k, _, _ = oracle_prefix(page0, page0.blank_arena(), 3.0)
-        work = PathRange(page0, 0, k)
-        px_per_copy = page0.pixels * k / max(1, page0.n_paths)
-        sample_desc = (f"the first {k} of {page0.n_paths} paths of the batch's first page, credited with "
-                       f"{k}/{page0.n_paths} of its pixels")
     cores = os.cpu_count() or 1
     threads = max(1, min(cores, args.ref_threads))
-    arenas = [scene.blank_arena() if work is scene else np.full(int(work.page_width[0]) * int(work.page_height[0]),
-                                                                  255, np.uint8) for _ in range(threads)]
+    if scene.n_pages > 1:
+        # Page-parallel on the host cores: each thread renders the leading
+        # paths of its own page (about 2 s of work each per step).
+        sample = PageParallelSample(scene, threads, 2.0)
+        step, px_per_step, sample_desc = sample.step, sample.credited_px, sample.describe()
+        pages_per_step = threads
+    else:
+        arenas = [scene.blank_arena() for _ in range(threads)]
 
-    def step():
-        for a in arenas:
-            a.fill(255)
-        ts = [threading.Thread(target=render, args=(work, a), kwargs=dict(threads=1)) for a in arenas]
-        t = time.perf_counter()
-        for x in ts:
-            x.start()
-        for x in ts:
-            x.join()
-        return time.perf_counter() - t
+        def step():
+            for a in arenas:
+                a.fill(255)
+            t = time.perf_counter()
+            _run_threads(lambda k: render(scene, arenas[k], threads=1), threads)
+            return time.perf_counter() - t
 
+        px_per_step = scene.pixels * threads
+        sample_desc = (f"{threads} copies of the page per step, one per host thread (the reference renders one "
+                       "page per worker)")
+        pages_per_step = threads
     for _ in range(args.warmup):
         step()
     times = [step() for _ in range(args.steps)]
     total = sum(times)
-    mpx = px_per_copy * threads * args.steps / total / 1e6
-    sample = (f"{threads} copies of {sample_desc} per step, one per host thread (page-parallel, as the "
-              "reference's per-page workers)")
+    mpx = px_per_step * args.steps / total / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": mpx, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded)", "config": {"workload": desc, "pages_per_step": threads},
-            "cpu_baseline": {"value": mpx, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": sample},
+            "data": "synthetic (seeded)", "config": {"workload": desc, "pages_per_step": pages_per_step},
+            "cpu_baseline": {"value": mpx, "unit": "Mpixel/s", "cores": threads, "kind": "port",
+                             "sample": sample_desc,
+                             "coverage_tier": ["scalar", "avx2", "avx512_bitalg"][rr_oracle.coverage_tier()]},
             "e2e": {"value": mpx, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -337,10 +392,10 @@ def run_rrb(args, rank, local, world):
     stage_ms = {k: v[0] / args.steps for k, v in stage_acc.items()}
     dom = max(stage_ms, key=stage_ms.get)
     alg = {
-        # page read + written once, each span (4 B) and AA-row index entry (8 B) read once
-        "composite": 2 * px + 4 * stats["spans"] + 8 * stats["aa_rows"],
-        # each edge record (32 B) read once, row index (8 B/row) and spans (4 B) written once
-        "rows": 32 * stats["segments"] + 8 * stats["aa_rows"] + 4 * stats["spans"],
+        # page read + written once, each coverage cell (4 B) and pixel-row index entry (8 B) read once
+        "composite": 2 * px + 4 * stats["spans"] + 8 * stats["row_groups"],
+        # each edge record (32 B) read once, pixel-row index (8 B/entry) and cells (4 B) written once
+        "rows": 32 * stats["segments"] + 8 * stats["row_groups"] + 4 * stats["spans"],
         # path points (16 B) + flags read, edge records written
         "seg_write": 17 * scene.n_pts + 32 * stats["segments"],
         "seg_count": 17 * scene.n_pts + 4 * scene.n_pts,
@@ -431,41 +486,27 @@ def run_rrb(args, rank, local, world):
         bit_exact = bool(np.array_equal(ref, np.asarray(host_page)) and np.array_equal(ref, gpu_page))
         cpu = {"value": px / secs / 1e6, "unit": "Mpixel/s", "cores": 1, "kind": "port",
                "sample": "the whole page (all paths), 1 host thread, C++ restatement of the reference CPU path",
-               "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"]}
-    elif rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = oracle_pages(scene, budget_s=15.0, page_budget_s=5.0)
-        bit_exact, spx, est, secs, ties, whole = True, 0, 0.0, 0.0, 0, 0
-        hp = np.asarray(host_page)
-        for pg, sub, ref, done, s_, t_ in sample:
-            spx += sub.pixels
-            secs += s_
-            est += s_ * sub.n_paths / max(1, done)  # the page's time at the sample's paths-per-second
-            ties += t_
-            if done == sub.n_paths:
-                whole += 1
-                lo, hi = sub.arena_base, sub.arena_base + sub.arena_bytes
-                bit_exact &= bool(np.array_equal(ref, hp[lo:hi]) and np.array_equal(ref, gpu_page[lo:hi]))
-        # Parity on whole pages as well: the pages with the fewest points,
-        # while they take the oracle about 10 s in all.
-        from rrb.shard import SceneShard
-        pts_per_page = np.diff(np.append(scene.path_pt_off[np.searchsorted(scene.path_page, np.arange(scene.n_pages))],
-                                         scene.path_pt_off[-1]).astype(np.int64))
-        checked = 0.0
-        for pg in np.argsort(pts_per_page, kind="stable"):
-            if checked >= 10.0:
-                break
-            sub = SceneShard(scene, pages=(int(pg), int(pg) + 1))
-            ref, secs_pg, _ = oracle_page(sub)
-            checked += secs_pg
-            lo, hi = sub.arena_base, sub.arena_base + sub.arena_bytes
-            bit_exact &= bool(np.array_equal(ref, hp[lo:hi]) and np.array_equal(ref, gpu_page[lo:hi]))
-            whole += 1
-        cpu = {"value": spx / est / 1e6 if est > 0 else None, "unit": "Mpixel/s", "cores": 1, "kind": "port",
-               "sample": f"the first {len(sample)} of {scene.n_pages} pages, each for at most 5 s of its leading "
-                         "paths (page time extrapolated by its path count), 1 host thread, C++ restatement of "
-                         f"the reference CPU path; bit_exact covers {whole} whole pages (those sampled whole and the "
-                         "pages with the fewest points)",
-               "seconds": secs, "unpinned_tie_rows": ties}
+               "seconds": secs, "unpinned_tie_rows": ost["unpinned_tie_rows"],
+               "coverage_tier": ["scalar", "avx2", "avx512_bitalg"][__import__("rr_oracle").coverage_tier()]}
+    parity = None
+    if scene.n_pages > 1 and not sharded:
+        # Every page of the batch, device and end-to-end arenas, against the
+        # oracle's pinned page digests.
+        parity = batch_digests_check(scene, gpu_page)
+        e2e_parity = batch_digests_check(scene, np.asarray(host_page))
+        if parity is not None:
+            bit_exact = (parity["pages_bit_exact"] == parity["pages_checked"] and e2e_parity is not None and
+                         e2e_parity["pages_bit_exact"] == e2e_parity["pages_checked"])
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and scene.n_pages > 1:
+        import rr_oracle
+        rr_oracle.build()
+        threads = max(1, min(os.cpu_count() or 1, args.ref_threads))
+        sample = PageParallelSample(scene, threads, 2.0)
+        secs = sample.step()
+        cpu = {"value": sample.credited_px / secs / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
+               "sample": sample.describe() + "; C++ restatement of the reference CPU path, page-parallel",
+               "seconds": secs,
+               "coverage_tier": ["scalar", "avx2", "avx512_bitalg"][rr_oracle.coverage_tier()]}
     batch.free()
     if rank == 0:
         p50, p99 = (float(np.percentile(step_ms, q)) for q in (50, 99))
@@ -484,7 +525,7 @@ def run_rrb(args, rank, local, world):
             "edges_per_s": edges_s, "segments_per_step": stats["segments"],
             "input_segments_per_step": scene.n_lines + scene.n_cubics,
             "p50_page_ms": p50, "p99_page_ms": p99,
-            "plain_per_path": plain, "bit_exact": bit_exact,
+            "plain_per_path": plain, "bit_exact": bit_exact, "parity": parity,
             "roofline": roofline, "stages_ms": stage_ms,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         }
@@ -584,8 +625,8 @@ def run_strokes(args, rank, local, world):
     peak, peak_kind = measured_peak()
     dom = max(stage_ms, key=stage_ms.get) if stage_ms else None
     roofline = None
-    alg = {"composite": 2 * page.pixels + 4 * stats["spans"] + 8 * stats["aa_rows"],
-           "rows": 32 * stats["segments"] + 8 * stats["aa_rows"] + 4 * stats["spans"]}
+    alg = {"composite": 2 * page.pixels + 4 * stats["spans"] + 8 * stats["row_groups"],
+           "rows": 32 * stats["segments"] + 8 * stats["row_groups"] + 4 * stats["spans"]}
     if dom in alg:
         waves = max(1, int(stats.get("waves", 1)))
         dur = stage_ms[dom] / waves / 1e3
@@ -787,7 +828,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["rrb", "reference"], default="rrb")
-    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fill_ops", "strokes"], default="glyphs")
+    ap.add_argument("--workload", choices=list(WORKLOADS) + ["fill_ops", "strokes"], default="mixed")
     ap.add_argument("--rowmap", type=int, default=0)
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -5,8 +5,8 @@
  * backends: every entry point mirrors one method of the reference trait
  * `GpuBackend` (crates/gpu/src/backend/mod.rs:216-503) or one of its
  * parameter structs (crates/gpu/src/backend/params.rs), with plain pointers,
- * sizes and an int status instead of Rust types. A Rust `impl GpuBackend for
- * B200Backend` binds these symbols one to one.
+ * sizes and an int status instead of Rust types, so a Rust
+ * `impl GpuBackend for B200Backend` can bind these symbols one to one.
  *
  * Status codes mirror `BackendError` (mod.rs:35-72) plus a timeout and a
  * device error. The text of the last failure is available from
@@ -402,6 +402,8 @@ typedef struct {
     uint64_t waves;                         /* page groups the batch was rendered in */
     uint64_t host_ns;                       /* host time of the call before its first kernel: validation,
                                                stroke outlines, staging and enqueued uploads */
+    uint64_t row_groups;                    /* pixel-row index entries written by the row stage */
+    uint64_t host_syncs;                    /* times the call waited on its stream for a device-side size */
 } rrb_batch_stats;
 int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
 
@@ -538,32 +540,6 @@ const double* rrb_path_pts(const rrb_path* p);
 const uint8_t* rrb_path_flags(const rrb_path* p);
 void rrb_conic_to_cubic(double p0x, double p0y, double pcx, double pcy, double p3x, double p3y,
                         double out[4]);
-
-/* ---- seeded synthetic scenes (the benchmark workloads) ----------------------
- * kind 0: polygon page (2,000 paths of 1-3 contours x 4-32 line/cubic
- *         segments on jittered circles, NZ 70% / EO 30%, opaque);
- * kind 1: glyph-dense text page (150,000 quadratic glyphs on 60 baselines);
- * kind 2: mixed pages of uneven size (30% glyphs, 40% polygons, 30% rects,
- *         alpha 32-255). Zero fields take the defaults of each kind. */
-typedef struct {
-    uint32_t kind;
-    uint64_t seed;
-    uint32_t n_pages;      /* kind 2 (default 64); kinds 0/1 always 1 */
-    uint32_t n_paths;      /* kinds 0/1: paths on the page; kind 2: 0 = log-normal count */
-    uint32_t page_w, page_h; /* kinds 0/1 page size (default 2550x3300) */
-    double page_scale;     /* kind 2: page dimensions multiplied by this (default 1) */
-    double paths_scale;    /* kind 2: median path count multiplied by this (default 1) */
-    uint32_t path_cap;     /* kind 2: max paths per page (default 50,000) */
-    uint32_t reserved;
-} rrb_scene_params;
-typedef struct rrb_scene rrb_scene;
-int rrb_scene_generate(const rrb_scene_params* p, rrb_scene** out);
-void rrb_scene_free(rrb_scene* s);
-/* Fills a batch view of the scene (pages = NULL, caller binds a device arena). */
-void rrb_scene_view(const rrb_scene* s, rrb_path_batch_params* out);
-uint64_t rrb_scene_arena_bytes(const rrb_scene* s);
-/* Input segment counts of the scene: [lines, cubics, points]. */
-void rrb_scene_counts(const rrb_scene* s, uint64_t out[3]);
 
 #ifdef __cplusplus
 }

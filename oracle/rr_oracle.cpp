@@ -8,6 +8,8 @@
 
 #include "rr_oracle.h"
 
+#include <immintrin.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -693,10 +695,19 @@ void or_render_aa_line(const or_scanner* s, uint8_t* aa_buf, int64_t aa_width, i
     out[1] = (xx_max - 1) / AA_SIZE;
 }
 
-// aa_coverage_span_scalar (crates/raster/src/simd/aa_coverage.rs:51-69): the
-// SIMD tiers (:310-471) compute the same per-nibble popcounts.
-void or_aa_coverage_span(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape,
-                         int64_t n) {
+// aa_coverage_span (crates/raster/src/simd/aa_coverage.rs:490-514): the
+// coverage count 0..16 of output pixels x0 .. x0+n-1 from the four AaBuf
+// sub-rows (row_bytes apart). Pixel x is nibble x & 1 of byte x >> 1 of each
+// row (even pixel = high nibble). The reference dispatches on the host CPU:
+// an odd x0 goes to the scalar loop; otherwise the AVX-512 BITALG tier when
+// avx512bitalg and avx512bw are present, else the AVX2 tier, else scalar.
+// All tiers count the same bits; the SIMD ones take whole chunks of row bytes
+// (64 for AVX-512, 32 for AVX2: coverage_chunk_params, :84-93) and leave the
+// rest of the span to the scalar loop, as the reference does.
+namespace {
+
+// aa_coverage_span_scalar (:51-69).
+void coverage_scalar(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape, int64_t n) {
     for (int64_t i = 0; i < n; ++i) {
         int64_t x = x0 + i;
         int64_t bi = x >> 1;
@@ -709,6 +720,90 @@ void or_aa_coverage_span(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, u
         }
         shape[i] = static_cast<uint8_t>(c);
     }
+}
+
+// Writes even pixel 2k <- hi[k], odd pixel 2k+1 <- lo[k] for the first
+// min(2 * bytes, n) pixels of a chunk.
+inline void interleave(const uint8_t* hi, const uint8_t* lo, int bytes, uint8_t* shape, int64_t n) {
+    for (int k = 0; k < bytes; ++k) {
+        if (2 * k < n) shape[2 * k] = hi[k];
+        if (2 * k + 1 < n) shape[2 * k + 1] = lo[k];
+    }
+}
+
+// AVX2 tier (:310-380): a 16-entry nibble-popcount table looked up with a
+// byte shuffle, 32 row bytes (64 pixels) per step.
+__attribute__((target("avx2"))) void coverage_avx2(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0,
+                                                    uint8_t* shape, int64_t n) {
+    const int64_t b0 = x0 >> 1, chunks = ((n + 1) / 2) / 32;
+    const __m256i table = _mm256_setr_epi8(0, 1, 1, 2, 1, 2, 2, 3, 1, 2, 2, 3, 2, 3, 3, 4,
+                                           0, 1, 1, 2, 1, 2, 2, 3, 1, 2, 2, 3, 2, 3, 3, 4);
+    const __m256i low4 = _mm256_set1_epi8(0x0f);
+    alignas(32) uint8_t hi[32], lo[32];
+    for (int64_t c = 0; c < chunks; ++c) {
+        __m256i acc_hi = _mm256_setzero_si256(), acc_lo = _mm256_setzero_si256();
+        for (int r = 0; r < 4; ++r) {
+            const __m256i v = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(aa_buf + r * row_bytes + b0 + 32 * c));
+            acc_hi = _mm256_add_epi8(acc_hi, _mm256_shuffle_epi8(table, _mm256_and_si256(_mm256_srli_epi16(v, 4), low4)));
+            acc_lo = _mm256_add_epi8(acc_lo, _mm256_shuffle_epi8(table, _mm256_and_si256(v, low4)));
+        }
+        _mm256_store_si256(reinterpret_cast<__m256i*>(hi), acc_hi);
+        _mm256_store_si256(reinterpret_cast<__m256i*>(lo), acc_lo);
+        interleave(hi, lo, 32, shape + 64 * c, n - 64 * c);
+    }
+    if (64 * chunks < n) coverage_scalar(aa_buf, row_bytes, x0 + 64 * chunks, shape + 64 * chunks, n - 64 * chunks);
+}
+
+// AVX-512 BITALG tier (:403-471): a per-byte popcount of each isolated
+// nibble, 64 row bytes (128 pixels) per step.
+__attribute__((target("avx512f,avx512bw,avx512bitalg"))) void coverage_avx512(const uint8_t* aa_buf,
+                                                                              int64_t row_bytes, int64_t x0,
+                                                                              uint8_t* shape, int64_t n) {
+    const int64_t b0 = x0 >> 1, chunks = ((n + 1) / 2) / 64;
+    const __m512i low4 = _mm512_set1_epi8(0x0f);
+    alignas(64) uint8_t hi[64], lo[64];
+    for (int64_t c = 0; c < chunks; ++c) {
+        __m512i acc_hi = _mm512_setzero_si512(), acc_lo = _mm512_setzero_si512();
+        for (int r = 0; r < 4; ++r) {
+            const __m512i v = _mm512_loadu_si512(aa_buf + r * row_bytes + b0 + 64 * c);
+            acc_hi = _mm512_add_epi8(acc_hi, _mm512_popcnt_epi8(_mm512_and_si512(_mm512_srli_epi16(v, 4), low4)));
+            acc_lo = _mm512_add_epi8(acc_lo, _mm512_popcnt_epi8(_mm512_and_si512(v, low4)));
+        }
+        _mm512_store_si512(hi, acc_hi);
+        _mm512_store_si512(lo, acc_lo);
+        interleave(hi, lo, 64, shape + 128 * c, n - 128 * c);
+    }
+    if (128 * chunks < n) coverage_scalar(aa_buf, row_bytes, x0 + 128 * chunks, shape + 128 * chunks, n - 128 * chunks);
+}
+
+int detect_tier() {
+    __builtin_cpu_init();
+    if (__builtin_cpu_supports("avx512bitalg") && __builtin_cpu_supports("avx512bw")) return 2;
+    if (__builtin_cpu_supports("avx2")) return 1;
+    return 0;
+}
+
+const int g_tier = detect_tier();
+
+}  // namespace
+
+// The tier dispatch uses on this host: 2 AVX-512 BITALG, 1 AVX2, 0 scalar.
+int or_coverage_tier(void) { return g_tier; }
+
+// One tier explicitly (for the scalar-vs-SIMD agreement check); a tier the
+// host lacks falls back to the best one it has. Odd x0 is always scalar.
+void or_aa_coverage_span_tier(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape, int64_t n,
+                              int tier) {
+    if (n <= 0) return;
+    if (tier > g_tier) tier = g_tier;
+    if ((x0 & 1) || tier == 0) coverage_scalar(aa_buf, row_bytes, x0, shape, n);
+    else if (tier == 2) coverage_avx512(aa_buf, row_bytes, x0, shape, n);
+    else coverage_avx2(aa_buf, row_bytes, x0, shape, n);
+}
+
+void or_aa_coverage_span(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape,
+                         int64_t n) {
+    or_aa_coverage_span_tier(aa_buf, row_bytes, x0, shape, n, g_tier);
 }
 
 const uint8_t* or_aa_gamma(void) { return AA_GAMMA; }

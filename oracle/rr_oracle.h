@@ -117,6 +117,11 @@ void or_render_aa_line(const or_scanner* s, uint8_t* aa_buf, int64_t aa_width, i
 void or_aabuf_set_span(uint8_t* aa_buf, int64_t aa_width, int64_t row, int64_t x0, int64_t x1);
 
 /* ---- A10, A11: coverage, gamma, compositing ---------------------------- */
+/* The coverage tier dispatch picks on this host (2 AVX-512 BITALG, 1 AVX2,
+ * 0 scalar), and one tier run explicitly (scalar-vs-SIMD agreement). */
+int or_coverage_tier(void);
+void or_aa_coverage_span_tier(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape, int64_t n,
+                              int tier);
 void or_aa_coverage_span(const uint8_t* aa_buf, int64_t row_bytes, int64_t x0, uint8_t* shape,
                          int64_t n);
 const uint8_t* or_aa_gamma(void);

@@ -94,6 +94,8 @@ def lib() -> C.CDLL:
             "or_render_aa_line": (None, [VP, C.POINTER(U8), I64, I32, C.POINTER(I32), C.POINTER(Stats)]),
             "or_aabuf_set_span": (None, [C.POINTER(U8), I64, I64, I64, I64]),
             "or_aa_coverage_span": (None, [C.POINTER(U8), I64, I64, C.POINTER(U8), I64]),
+            "or_aa_coverage_span_tier": (None, [C.POINTER(U8), I64, I64, C.POINTER(U8), I64, C.c_int]),
+            "or_coverage_tier": (C.c_int, []),
             "or_aa_gamma": (C.POINTER(U8), []),
             "or_div255": (U8, [C.c_uint32]),
             "or_render_span_aa_gray": (None, [C.POINTER(U8), C.POINTER(U8), I64, U8, U8]),
@@ -284,6 +286,19 @@ def aa_coverage_span(rows4: np.ndarray, x0: int, n: int) -> np.ndarray:
     rows4 = np.ascontiguousarray(rows4, np.uint8)
     out = np.zeros(n, np.uint8)
     lib().or_aa_coverage_span(_p(rows4, C.c_uint8), rows4.shape[1], x0, _p(out, C.c_uint8), n)
+    return out
+
+
+def coverage_tier() -> int:
+    """The coverage tier the oracle dispatches to on this host: 2 AVX-512 BITALG, 1 AVX2, 0 scalar."""
+    return int(lib().or_coverage_tier())
+
+
+def aa_coverage_span_tier(rows4: np.ndarray, x0: int, n: int, tier: int) -> np.ndarray:
+    """aa_coverage_span through one tier (0 scalar, 1 AVX2, 2 AVX-512 BITALG; capped at the host's best)."""
+    rows4 = np.ascontiguousarray(rows4, np.uint8)
+    out = np.zeros(n, np.uint8)
+    lib().or_aa_coverage_span_tier(_p(rows4, C.c_uint8), rows4.shape[1], x0, _p(out, C.c_uint8), n, tier)
     return out
 
 

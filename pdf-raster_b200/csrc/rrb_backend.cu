@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/rrb.h"
+#include "rrb_device_scope.h"
 #include "rrb_hairline.cuh"
 #include "rrb_kernels.cuh"
 #include "rrb_stroke.h"
@@ -65,11 +66,13 @@ struct rrb_ctx {
     // Batch scratch.
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
+    Scratch s_super_start;  // per supertile: one past its last opaque full layer
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
     Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
+    uint64_t host_syncs = 0;  // stream waits for device-side sizes in the current run_resident_one
     uint64_t scratch_grows = 0;  // ensure() reallocations since the last record call began
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
     struct rrb_batch* wave_batch = nullptr; // view of a group of pages of a larger batch
@@ -177,6 +180,7 @@ int upload(rrb_ctx* c, Scratch& s, const T* src, size_t count) {
 }
 
 int read_back(rrb_ctx* c, const void* dev, size_t bytes) {
+    ++c->host_syncs;
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
     RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     return RRB_OK;
@@ -190,11 +194,11 @@ int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info,
                      uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
                      const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, const int4* runs,
                      uint8_t* arena, int rowmap, const BatchCounters* ctr, const uint32_t* path_rgb,
-                     bool rectilinear) {
+                     bool rectilinear, const uint32_t* super_start) {
 #define RRB_COMP(TW, TH, RGB, FEW)                                                                           \
     k_composite<TW, TH, RGB, FEW><<<grid, COMP_THREADS, 0, c->stream>>>(                                      \
         info, geom, n_pages, n_tiles, SUPER, SUPER, super_off, super_list, row_off, row_idx, spans, runs, arena, \
-        rowmap, ctr, path_rgb)
+        rowmap, ctr, path_rgb, super_start)
 #define RRB_COMP_SHAPE(RGB, FEW)                                  \
     do {                                                          \
         if (tw == 64 && th == 16) RRB_COMP(64, 16, RGB, FEW);     \
@@ -247,7 +251,9 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
         uint32_t w = h->page_width[pg], ht = h->page_height[pg];
         if (w == 0 || ht == 0 || w > 16383 || ht > (1u << 28))
             return msg = "page width must be 1..16383 and height 1..2^28", RRB_ERR_INVARIANT;
-        if (h->page_offset[pg] + static_cast<uint64_t>(bpp) * w * ht > arena_len)
+        // Overflow-safe form of offset + bytes > arena_len (an offset near 2^64 must not wrap).
+        const uint64_t page_bytes = static_cast<uint64_t>(bpp) * w * ht;
+        if (h->page_offset[pg] > arena_len || page_bytes > arena_len - h->page_offset[pg])
             return msg = "page extends past the page buffer", RRB_ERR_INVARIANT;
         PageGeom& G = geom[pg];
         G.w = w;
@@ -460,6 +466,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
 // The pipeline over a device-resident batch into the device page arena.
 int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     c->launches = 0;
+    c->host_syncs = 0;
     std::memset(&c->stats, 0, sizeof c->stats);
     std::memset(c->stage_ms, 0, sizeof c->stage_ms);
     std::memset(c->stage_launches, 0, sizeof c->stage_launches);
@@ -578,7 +585,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage(c, 6);
     k_super_bin<false><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
         as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, as<uint32_t>(c->s_super_cnt),
-        nullptr, nullptr);
+        nullptr, nullptr, nullptr);
     c->launches += 1;
     stage_end(c, 6);
     RRB_CUDA(c, cudaGetLastError());
@@ -602,6 +609,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                 c->stream));
     RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 8, &as<BatchCounters>(c->s_ctr)->hl_rows, 8, cudaMemcpyDeviceToHost,
                                 c->stream));
+    ++c->host_syncs;
     RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     const uint64_t n_groups = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
     const uint64_t n_runs = c->h_read[6];
@@ -623,10 +631,15 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if ((rc = ensure(c, c->s_ovf, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_super_list, std::max<uint64_t>(1, n_pairs) * sizeof(uint32_t)))) return rc;
     if ((rc = ensure(c, c->s_runs, std::max<uint64_t>(1, n_runs) * sizeof(int4)))) return rc;
+    const PageGeom& last_page = B->geom_h[n_pages - 1];
+    const uint64_t n_super_tiles =
+        last_page.super_base + static_cast<uint64_t>(last_page.nsx) * ((last_page.h + SUPER - 1) / SUPER);
+    if ((rc = ensure(c, c->s_super_start, n_super_tiles * sizeof(uint32_t)))) return rc;
+    RRB_CUDA(c, cudaMemsetAsync(c->s_super_start.p, 0, n_super_tiles * sizeof(uint32_t), c->stream));
     stage(c, 8);
     k_super_bin<true><<<grid_for(c, supers * 32, 256), 256, 0, c->stream>>>(
         as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, NSUP, SUPER, SUPER, nullptr,
-        as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list));
+        as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_super_start));
     c->launches += 1;
     stage_end(c, 8);
     stage(c, 9);
@@ -729,7 +742,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
                                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
                                rowmap, as<BatchCounters>(c->s_ctr), B->bpp == 3 ? as<uint32_t>(B->rgb) : nullptr,
-                               n_runs > 0)))
+                               n_runs > 0, as<uint32_t>(c->s_super_start))))
         return rc;
     stage_end(c, 11);
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
@@ -745,6 +758,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     c->stats.tile_pairs = n_pairs;
     c->stats.nonterminating_rows = hc.nonterminating;
     c->stats.kernel_launches = c->launches;
+    c->stats.row_groups = n_groups;
+    c->stats.host_syncs = c->host_syncs;
     if (c->timer && c->timer->on) {
         // The final read_back synchronised the stream: every event is complete.
         for (int k = 0; k < kStages; ++k) {
@@ -780,7 +795,7 @@ void set_binning(std::vector<PageGeom>& geom, uint64_t& supers_out) {
 void release_scratch(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
-                      &c->s_super_cnt, &c->s_super_list, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
+                      &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip};
     for (Scratch* x : all) {
@@ -866,6 +881,8 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
         acc.tile_pairs += s.tile_pairs;
         acc.nonterminating_rows += s.nonterminating_rows;
         acc.kernel_launches += s.kernel_launches;
+        acc.row_groups += s.row_groups;
+        acc.host_syncs += s.host_syncs;
         acc.waves += 1;
         for (int k = 0; k < 16; ++k) {
             c->stage_sum_ms[k] += c->stage_ms[k];
@@ -1031,6 +1048,8 @@ int run_path_range(rrb_ctx* c, rrb_batch* B, const uint64_t* path_pt_off, uint32
         acc.tile_pairs += s.tile_pairs;
         acc.nonterminating_rows += s.nonterminating_rows;
         acc.kernel_launches += s.kernel_launches;
+        acc.row_groups += s.row_groups;
+        acc.host_syncs += s.host_syncs;
         acc.waves += 1;
         for (int k = 0; k < 16; ++k) {
             c->stage_sum_ms[k] += c->stage_ms[k];
@@ -1218,7 +1237,8 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
     rrb_ctx* c = new rrb_ctx();
     c->device = device;
     c->budget = mem_budget_bytes;
-    cudaError_t e = cudaSetDevice(device);
+    const rrb_host::DeviceScope dev_scope(device);
+    cudaError_t e = dev_scope.status();
     if (e != cudaSuccess) {
         delete c;
         return RRB_ERR_DEVICE;
@@ -1248,11 +1268,11 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
 
 int rrb_destroy(rrb_ctx* c) {
     if (!c) return RRB_OK;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pts, &c->s_flags, &c->s_off, &c->s_rule, &c->s_gray, &c->s_alpha, &c->s_page,
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
-                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list,
+                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list, &c->s_super_start,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo};
@@ -1292,7 +1312,7 @@ const char* rrb_last_error_message(const rrb_ctx* c) { return c ? c->err.c_str()
 int rrb_alloc_device(rrb_ctx* c, size_t size, rrb_buf** out) {
     if (!c || !out) return RRB_ERR_INVARIANT;
     if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_device called with size = 0");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     void* p = nullptr;
     int rc = dev_alloc(c, size, &p);
     if (rc) return rc;
@@ -1302,6 +1322,7 @@ int rrb_alloc_device(rrb_ctx* c, size_t size, rrb_buf** out) {
 
 int rrb_alloc_device_zeroed(rrb_ctx* c, size_t size, rrb_buf** out) {
     if (!c || !out) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_device_zeroed called with size = 0");
     int rc = rrb_alloc_device(c, size, out);
     if (rc) return rc;
@@ -1315,7 +1336,7 @@ void* rrb_device_ptr(const rrb_buf* b) { return b ? b->p : nullptr; }
 
 int rrb_free_device(rrb_ctx* c, rrb_buf* b) {
     if (!c || !b) return RRB_ERR_INVARIANT;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     cudaStreamSynchronize(c->stream);
     dev_free(c, b->p, b->len);
     delete b;
@@ -1324,6 +1345,7 @@ int rrb_free_device(rrb_ctx* c, rrb_buf* b) {
 
 int rrb_alloc_host_pinned(rrb_ctx* c, size_t size, rrb_host_buf** out) {
     if (!c || !out) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (size == 0) return set_err(c, RRB_ERR_ZERO_SIZE_ALLOC, "alloc_host_pinned called with size = 0");
     void* p = nullptr;
     RRB_CUDA(c, cudaMallocHost(&p, size));
@@ -1335,6 +1357,7 @@ void* rrb_host_ptr(const rrb_host_buf* b) { return b ? b->p : nullptr; }
 
 int rrb_free_host_pinned(rrb_ctx* c, rrb_host_buf* b) {
     if (!c || !b) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     cudaStreamSynchronize(c->stream);
     cudaFreeHost(b->p);
     delete b;
@@ -1381,7 +1404,7 @@ int rrb_upload_async(rrb_ctx* c, const rrb_buf* dst, size_t off, const void* src
     if (!c || !dst || (!src && len)) return RRB_ERR_INVARIANT;
     if (off > dst->len || len > dst->len - off)
         return set_err(c, RRB_ERR_INVARIANT, "upload exceeds the device buffer");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (len) RRB_CUDA(c, cudaMemcpyAsync(static_cast<char*>(dst->p) + off, src, len, cudaMemcpyHostToDevice, c->stream));
     return record_fence(c, out);
 }
@@ -1390,7 +1413,7 @@ int rrb_download_async(rrb_ctx* c, const rrb_buf* src, size_t off, void* dst, si
     if (!c || !src || (!dst && len)) return RRB_ERR_INVARIANT;
     if (off > src->len || len > src->len - off)
         return set_err(c, RRB_ERR_INVARIANT, "download exceeds the device buffer");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (len) RRB_CUDA(c, cudaMemcpyAsync(dst, static_cast<const char*>(src->p) + off, len, cudaMemcpyDeviceToHost, c->stream));
     return record_fence(c, out);
 }
@@ -1401,7 +1424,7 @@ int rrb_wait_transfer(rrb_ctx* c, rrb_fence f, uint64_t t) { return c ? wait_fen
 
 int rrb_detect_vram_budget(rrb_ctx* c, rrb_vram_budget* out) {
     if (!c || !out) return RRB_ERR_INVARIANT;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     size_t fr = 0, tot = 0;
     RRB_CUDA(c, cudaMemGetInfo(&fr, &tot));
     out->total_bytes = tot;
@@ -1420,6 +1443,7 @@ int rrb_begin_page(rrb_ctx* c) {
 
 int rrb_record_zero_buffer(rrb_ctx* c, const rrb_buf* b) {
     if (!c || !b) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     RRB_CUDA(c, cudaMemsetAsync(b->p, 0, b->len, c->stream));
     return RRB_OK;
@@ -1462,7 +1486,7 @@ int rrb_record_path_batch(rrb_ctx* c, const rrb_path_batch_params* p) {
     if (!c || !p) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len);
 }
 
@@ -1510,7 +1534,7 @@ int rrb_record_path_fill(rrb_ctx* c, const rrb_path_fill_params* p) {
 
 int rrb_batch_upload(rrb_ctx* c, const rrb_path_batch_params* p, rrb_batch** out) {
     if (!c || !p || !out) return RRB_ERR_INVARIANT;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     rrb_batch* B = new rrb_batch();
     int rc = batch_upload(c, p, B);
     if (rc) {
@@ -1526,13 +1550,13 @@ int rrb_batch_upload(rrb_ctx* c, const rrb_path_batch_params* p, rrb_batch** out
 int rrb_record_batch(rrb_ctx* c, rrb_batch* B, const rrb_buf* pages, int rowmap) {
     if (!c || !B || !pages) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     return run_resident(c, B, static_cast<uint8_t*>(pages->p), pages->len, rowmap);
 }
 
 int rrb_batch_free(rrb_ctx* c, rrb_batch* B) {
     if (!c || !B) return RRB_ERR_INVARIANT;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     cudaStreamSynchronize(c->stream);
     free_batch_bufs(c, B);
     delete B;
@@ -1541,6 +1565,7 @@ int rrb_batch_free(rrb_ctx* c, rrb_batch* B) {
 
 int rrb_record_fill_buffer(rrb_ctx* c, const rrb_buf* b, size_t off, size_t len, uint8_t value) {
     if (!c || !b) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (off > b->len || len > b->len - off) return set_err(c, RRB_ERR_INVARIANT, "fill exceeds the device buffer");
     RRB_CUDA(c, cudaMemsetAsync(static_cast<char*>(b->p) + off, value, len, c->stream));
@@ -1551,6 +1576,7 @@ void* rrb_stream(rrb_ctx* c) { return c ? static_cast<void*>(c->stream) : nullpt
 
 int rrb_set_profiling(rrb_ctx* c, int enable) {
     if (!c) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(c->device);
     if (!c->timer) {
         c->timer = new StageTimer();
         for (int k = 0; k < kStages; ++k) {
@@ -1583,7 +1609,7 @@ int rrb_record_stroke_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rr
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
     if (p->n_paths && !stroke) return set_err(c, RRB_ERR_INVARIANT, "stroke params array is null");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     {
         std::vector<PageGeom> geom;
         uint64_t tiles = 0, supers = 0;
@@ -1603,7 +1629,7 @@ int rrb_record_path_batch_ex(rrb_ctx* c, const rrb_path_batch_params* p, const u
     if (!c || !p) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     {
         std::vector<PageGeom> geom;
         uint64_t tiles = 0, supers = 0;
@@ -1626,10 +1652,11 @@ int rrb_record_rgb_to_gray(rrb_ctx* c, const rrb_buf* rgb, size_t rgb_offset, co
                            size_t gray_offset, uint64_t n_px) {
     if (!c || !rgb || !gray) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
-    if (rgb_offset + 3 * n_px > rgb->len || gray_offset + n_px > gray->len)
+    if (rgb_offset > rgb->len || n_px > (rgb->len - rgb_offset) / 3 || gray_offset > gray->len ||
+        n_px > gray->len - gray_offset)
         return set_err(c, RRB_ERR_INVARIANT, "rgb_to_gray range past a buffer");
     if (!n_px) return RRB_OK;
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     k_rgb_to_gray<<<grid_for(c, n_px, 256), 256, 0, c->stream>>>(static_cast<const uint8_t*>(rgb->p) + rgb_offset,
                                                                 static_cast<uint8_t*>(gray->p) + gray_offset, n_px);
     RRB_CUDA(c, cudaGetLastError());
@@ -1639,7 +1666,7 @@ int rrb_record_rgb_to_gray(rrb_ctx* c, const rrb_buf* rgb, size_t rgb_offset, co
 int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len) {
     if (!c || !p || !host_pages || !p->pages) return RRB_ERR_INVARIANT;
     if (len > p->pages->len) return set_err(c, RRB_ERR_INVARIANT, "host pages larger than the device arena");
-    cudaSetDevice(c->device);
+    const rrb_host::DeviceScope dev_scope(c->device);
     RRB_CUDA(c, cudaMemcpyAsync(p->pages->p, host_pages, len, cudaMemcpyHostToDevice, c->stream));
     int rc = rrb_begin_page(c);
     if (rc) return rc;

@@ -41,6 +41,7 @@
 #include <string>
 
 #include "../../include/rrb.h"
+#include "rrb_device_scope.h"
 
 int rrb_ctx_device(const rrb_ctx* c);
 bool rrb_ctx_page_open(const rrb_ctx* c);
@@ -477,9 +478,11 @@ __global__ void k_tile_ranges(const uint32_t* __restrict__ keys, uint32_t n, uin
         }                                                                                                \
     } while (0)
 
-int begin(rrb_ctx* c) {
+// Checks shared by the coverage operators; `dev` is the status of the
+// caller's DeviceScope (the context's device made current for the call).
+int begin(rrb_ctx* c, cudaError_t dev) {
     if (!rrb_ctx_page_open(c)) return rrb_ctx_fail(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
-    FILL_CUDA(c, cudaSetDevice(rrb_ctx_device(c)));
+    FILL_CUDA(c, dev);
     return RRB_OK;
 }
 
@@ -521,8 +524,9 @@ void rrb_aa_fill_jitter(float* x, float* y) {
 
 int rrb_record_aa_fill(rrb_ctx* c, const rrb_aa_fill_params* p) {
     if (!c || !p) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(rrb_ctx_device(c));
     int rc;
-    if ((rc = begin(c)) || (rc = check_cov(c, p->coverage, p->width, p->height)) ||
+    if ((rc = begin(c, dev_scope.status())) || (rc = check_cov(c, p->coverage, p->width, p->height)) ||
         (rc = check_segs(c, p->segs, p->n_segs)))
         return rc;
     if (!p->width || !p->height) return RRB_OK;
@@ -542,8 +546,9 @@ int rrb_record_aa_fill(rrb_ctx* c, const rrb_aa_fill_params* p) {
 
 int rrb_record_tile_fill(rrb_ctx* c, const rrb_tile_fill_params* p) {
     if (!c || !p) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(rrb_ctx_device(c));
     int rc;
-    if ((rc = begin(c)) || (rc = check_cov(c, p->coverage, p->width, p->height))) return rc;
+    if ((rc = begin(c, dev_scope.status())) || (rc = check_cov(c, p->coverage, p->width, p->height))) return rc;
     if (!p->width || !p->height) return RRB_OK;
     const uint32_t gw = (p->width + TILE - 1) / TILE, gh = (p->height + TILE - 1) / TILE;
     const uint64_t tiles = static_cast<uint64_t>(gw) * gh;
@@ -562,8 +567,9 @@ int rrb_record_tile_fill(rrb_ctx* c, const rrb_tile_fill_params* p) {
 
 int rrb_record_tile_fill_segs(rrb_ctx* c, const rrb_aa_fill_params* p, uint64_t* n_records) {
     if (!c || !p) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(rrb_ctx_device(c));
     int rc;
-    if ((rc = begin(c)) || (rc = check_cov(c, p->coverage, p->width, p->height)) ||
+    if ((rc = begin(c, dev_scope.status())) || (rc = check_cov(c, p->coverage, p->width, p->height)) ||
         (rc = check_segs(c, p->segs, p->n_segs)))
         return rc;
     if (n_records) *n_records = 0;

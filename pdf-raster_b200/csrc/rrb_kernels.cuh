@@ -45,6 +45,14 @@ constexpr uint32_t PI_RECTI = 1u << 17;  // all edges horizontal or vertical, at
 // (pipe/general.rs:261-312) instead of the AA fast path; on Gray8 pages the
 // two agree (a_src = div255(a * 255) = a).
 constexpr uint32_t PI_SOLID = 1u << 19;
+// A rectilinear path whose every AA row in [y0, y1] holds the same single
+// span [S0, S1) of AA columns (an axis-aligned rectangle): the coverage of
+// pixel (x, y) is cx * cy, cx = |[4x, 4x+4) n [S0, S1)| and cy = the number
+// of the pixel row's AA rows inside [y0, y1] — draw_aa_line's nibble popcount
+// summed over four identical sub-rows. Such a path keeps S0 in run_off, S1 in
+// run_cnt and the AA rows it paints in [y0, y1] (set by k_recti), and has no
+// runs or cells: the composite evaluates its coverage directly.
+constexpr uint32_t PI_BOX = 1u << 20;
 constexpr uint32_t RECTI_MAX_EDGES = 32;
 
 // Error / status word bits shared by all kernels of a batch.
@@ -634,10 +642,16 @@ __device__ __forceinline__ uint32_t find_page_work(const PageGeom* pg, uint32_t 
 // paths of block b that overlap s, in path order. Work items of one
 // supertile are consecutive, so after an exclusive scan of the counts the
 // supertile's list is the contiguous range [off(s,0), off(s,nblk)).
+// The writing pass also records in super_start[s] one past the list position
+// of the last opaque path whose solid box holds the whole supertile (clipped
+// to the page): compositing of every tile of s can start there, since that
+// layer sets each of its pixels to the path's colour (super_start zeroed
+// beforehand; 0 = no such path).
 template <bool WRITE>
 __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages,
                             uint32_t n_work, int stw, int sth, uint32_t* __restrict__ work_count,
-                            const uint32_t* __restrict__ work_off, uint32_t* __restrict__ super_list) {
+                            const uint32_t* __restrict__ work_off, uint32_t* __restrict__ super_list,
+                            uint32_t* __restrict__ super_start) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -652,6 +666,8 @@ __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* _
         uint32_t pe = min(G.path_end, pb + BIN_BLOCK);
         uint32_t cnt = 0;
         uint32_t base = WRITE ? work_off[q] : 0u;
+        const int32_t cx1 = min(x1, static_cast<int32_t>(G.w) - 1), cy1 = min(y1, static_cast<int32_t>(G.h) - 1);
+        uint32_t opaque_end = 0;  // one past the list position of the last opaque full layer seen
         for (uint32_t j = pb; j < pe; j += 32) {
             uint32_t qq = j + lane;
             bool hit = false;
@@ -661,10 +677,23 @@ __global__ void k_super_bin(const PathInfo* __restrict__ info, const PageGeom* _
                 hit = r.x <= r.y && r.z <= r.w && r.x <= x1 && r.y >= x0 && r.z <= y1 && r.w >= y0;
             }
             uint32_t m = __ballot_sync(0xffffffffu, hit);
-            if (WRITE && hit) super_list[base + cnt + __popc(m & lanemask_lt())] = qq;
+            if (WRITE && hit) {
+                const uint32_t pos = base + cnt + __popc(m & lanemask_lt());
+                super_list[pos] = qq;
+                static_assert(offsetof(PathInfo, paint) == 32 && offsetof(PathInfo, bx0) == 48, "int4 loads");
+                const uint32_t paint = reinterpret_cast<const uint4*>(&info[qq])[2].x;
+                if (((paint >> 8) & 0xffu) == 255u) {
+                    const int4 b = reinterpret_cast<const int4*>(&info[qq])[3];  // bx0, bx1, by0, by1
+                    if (b.x <= x0 && b.y >= cx1 && b.z <= y0 && b.w >= cy1) opaque_end = max(opaque_end, pos + 1);
+                }
+            }
             cnt += __popc(m);
         }
         if (!WRITE && lane == 0) work_count[q] = cnt;
+        if (WRITE) {
+            for (int o = 16; o; o >>= 1) opaque_end = max(opaque_end, __shfl_xor_sync(0xffffffffu, opaque_end, o));
+            if (lane == 0 && opaque_end) atomicMax(&super_start[G.super_base + sl], opaque_end);
+        }
     }
 }
 
@@ -1096,6 +1125,76 @@ __host__ __device__ __forceinline__ int recti_row_spans(const PathInfo& P, const
         nonterm);
 }
 
+// Event rows of a rectilinear path, sorted and unique, within [y0, y1 + 1]:
+// its first row, the row after its last; a horizontal edge's row and the row
+// after; a vertical edge's first row, the row after it and the row after its
+// last. All AA rows of one band [ev[b], ev[b+1]) have the same merged entries.
+__host__ __device__ __forceinline__ int recti_events(const PathInfo& P, const Edge* __restrict__ edges, int32_t* ev) {
+    int nev = 0;
+    auto push = [&](int32_t v) {
+        if (v >= P.y0 && v <= P.y1 + 1) ev[nev++] = v;
+    };
+    push(P.y0);
+    push(P.y1 + 1);
+    for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
+        const Edge E = edges[j];
+        if (E.flags & EF_EMPTY) continue;
+        push(E.row0);
+        push(E.row0 + 1);
+        if ((E.flags & EF_KIND_MASK) == EK_VERT) push(E.row1 + 1);
+    }
+    for (int a = 1; a < nev; ++a) {
+        const int32_t t = ev[a];
+        int b = a;
+        while (b > 0 && t < ev[b - 1]) {
+            ev[b] = ev[b - 1];
+            --b;
+        }
+        ev[b] = t;
+    }
+    int m = 0;
+    for (int a = 0; a < nev; ++a)
+        if (m == 0 || ev[a] != ev[m - 1]) ev[m++] = ev[a];
+    return m;
+}
+
+// Whether a rectilinear path is a box (PI_BOX): the bands of identical AA
+// rows [ev[b], ev[b+1]) that paint anything are consecutive, each has exactly
+// one span, the same in all of them, and every row's winding closes. Returns
+// the span [s0, s1) and the painted AA rows [r0, r1]. (A rectangle's first
+// and last AA rows paint nothing: their merged entry has a zero count.)
+__host__ __device__ __forceinline__ bool recti_box(const PathInfo& P, const Edge* __restrict__ edges,
+                                                   const int32_t* ev, int nev, int32_t aa_width, int32_t lo,
+                                                   int32_t hi, int32_t& s0, int32_t& s1, int32_t& r0, int32_t& r1) {
+    bool seen = false, ended = false;
+    for (int b = 0; b + 1 < nev; ++b) {
+        int32_t a0[RECTI_MAX_SPANS], a1[RECTI_MAX_SPANS];
+        uint32_t open_rows = 0;
+        const int n = recti_row_spans(P, edges, ev[b], aa_width, lo, hi, a0, a1, open_rows);
+        if (open_rows || n > 1) return false;
+        if (n == 0) {
+            ended = seen;
+            continue;
+        }
+        if (ended) return false;  // painted bands with a gap between them
+        if (!seen) {
+            s0 = a0[0];
+            s1 = a1[0];
+            r0 = ev[b];
+            seen = true;
+        } else if (a0[0] != s0 || a1[0] != s1) {
+            return false;
+        }
+        r1 = ev[b + 1] - 1;
+    }
+    return seen && s0 < s1;
+}
+
+// Floor of a / b for b > 0.
+__host__ __device__ __forceinline__ int32_t floor_div(int32_t a, int32_t b) {
+    return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
 template <bool WRITE>
 __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edge* __restrict__ edges,
                         const uint32_t* __restrict__ page_w, int rowmap, uint32_t* __restrict__ run_count,
@@ -1109,34 +1208,9 @@ __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edg
             if (!WRITE) run_count[p] = 0;
             continue;
         }
-        // Event rows, sorted and unique, within [y0, y1 + 1].
+        if (WRITE && (P.paint & PI_BOX)) continue;  // boxes have no runs or cells
         int32_t ev[RECTI_MAX_EVENTS];
-        int nev = 0;
-        auto push = [&](int32_t v) {
-            if (v >= P.y0 && v <= P.y1 + 1) ev[nev++] = v;
-        };
-        push(P.y0);
-        push(P.y1 + 1);
-        for (uint32_t j = P.e_begin; j < P.e_end; ++j) {
-            const Edge E = edges[j];
-            if (E.flags & EF_EMPTY) continue;
-            push(E.row0);
-            push(E.row0 + 1);
-            if ((E.flags & EF_KIND_MASK) == EK_VERT) push(E.row1 + 1);
-        }
-        for (int a = 1; a < nev; ++a) {
-            const int32_t t = ev[a];
-            int b = a;
-            while (b > 0 && t < ev[b - 1]) {
-                ev[b] = ev[b - 1];
-                --b;
-            }
-            ev[b] = t;
-        }
-        int m = 0;
-        for (int a = 0; a < nev; ++a)
-            if (m == 0 || ev[a] != ev[m - 1]) ev[m++] = ev[a];
-        nev = m;  // ev[0] = y0, ev[nev-1] = y1 + 1
+        const int nev = recti_events(P, edges, ev);  // ev[0] = y0, ev[nev-1] = y1 + 1
         auto band_of = [&](int32_t r) {  // last k with ev[k] <= r
             int lo = 0, hi = nev - 1;
             while (hi - lo > 1) {
@@ -1149,6 +1223,38 @@ __global__ void k_recti(PathInfo* __restrict__ info, uint32_t n_paths, const Edg
         const int32_t g0 = P.y0 >> 2, g1 = P.y1 >> 2;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
         const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
+        if (!WRITE) {
+            int32_t s0 = 0, s1 = 0, r0 = 0, r1 = -1;
+            if (recti_box(P, edges, ev, nev, aa_width, cx.x, cx.y, s0, s1, r0, r1)) {
+                // Solid box: pixels whose four AA columns and whose AA rows under
+                // the row map all lie inside the box.
+                int32_t by0, by1;
+                if (rowmap == 0) {
+                    by0 = floor_div(r0 + 3, 4);
+                    by1 = floor_div(r1 + 1, 4) - 1;
+                } else {  // pixel row y shows AA rows 16y+12 .. 16y+15
+                    by0 = floor_div(r0 - 12 + 15, 16);
+                    by1 = floor_div(r1 - 15, 16);
+                }
+                by0 = max(by0, P.py0);
+                by1 = min(by1, P.py1);
+                const int32_t bx0 = floor_div(s0 + 3, 4), bx1 = floor_div(s1, 4) - 1;
+                // From here on a box's y0, y1 are the AA rows it paints.
+                info[p].y0 = r0;
+                info[p].y1 = r1;
+                info[p].paint = P.paint | PI_BOX;
+                info[p].run_off = static_cast<uint32_t>(s0);
+                info[p].run_cnt = static_cast<uint32_t>(s1);
+                if (bx0 <= bx1 && by0 <= by1) {
+                    info[p].bx0 = bx0;
+                    info[p].bx1 = bx1;
+                    info[p].by0 = by0;
+                    info[p].by1 = by1;
+                }
+                run_count[p] = 0;
+                continue;
+            }
+        }
         uint32_t nrun = 0;
         uint32_t ro = WRITE ? run_off[p] : 0u;
         int32_t best_rows = 0, bx0 = 1, bx1 = 0, bg0 = 1, bg1 = 0;
@@ -1500,6 +1606,15 @@ struct HitRows {
     uint32_t cell0[ITERS];
 };
 
+// A box hit (PI_BOX): its coverage over this thread's pixels is cx * cy,
+// from the box's AA columns [S0, S1) (h.goff, h.run_cnt) and AA rows
+// [h.g0, h.g1]; the pixel row y shows AA rows 4y..4y+3 (documented row map)
+// or 16y+12..16y+15 (as-shipped). No loads: every operand is in the hit.
+// Then AA_GAMMA and the blend of composite_path_rows.
+template <int TW, int TH, bool RGB>
+__device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int X0, int Y0, const uint8_t* gamma,
+                                              uint32_t (&pix)[TH * TW / COMP_THREADS]);
+
 constexpr uint32_t kFewRuns = 4;   // rectilinear paths with at most this many runs: no search
 constexpr uint32_t kFewCells = 4;  // rectilinear rows with at most this many cells: direct lookup
 
@@ -1514,7 +1629,7 @@ __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int
     for (int it = 0; it < HitRows<TW, TH>::ITERS; ++it) {
         const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
         const int32_t grp = rowmap ? 4 * y + 3 : y;
-        const bool rowok = y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
+        const bool rowok = !(h.paint & PI_BOX) && y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
         uint2 ix = make_uint2(0u, 0u);
         if (rowok) {
             if (h.paint & PI_RECTI) {
@@ -1708,6 +1823,42 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
     }
 }
 
+template <int TW, int TH, bool RGB>
+__device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int X0, int Y0, const uint8_t* gamma,
+                                              uint32_t (&pix)[TH * TW / COMP_THREADS]) {
+    using L = CompLayout<TW>;
+    constexpr int ITERS = HitRows<TW, TH>::ITERS;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int slot = lane / L::LPR, col = (lane % L::LPR) * L::PX;
+    const int32_t S0 = static_cast<int32_t>(h.goff), S1 = static_cast<int32_t>(h.run_cnt);
+    const uint32_t g = h.paint & 0xff, alpha = (h.paint >> 8) & 0xff;
+    int32_t cx[L::PX];
+#pragma unroll
+    for (int q = 0; q < L::PX; ++q) {
+        const int32_t a = 4 * (X0 + col + q);
+        cx[q] = max(0, min(a + 4, S1) - max(a, S0));
+    }
+#pragma unroll
+    for (int it = 0; it < ITERS; ++it) {
+        const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
+        const int32_t r = rowmap ? 16 * y + 12 : 4 * y;
+        const int32_t cy = (y >= h.py0 && y <= h.py1) ? max(0, min(r + 4, h.g1 + 1) - max(r, h.g0)) : 0;
+#pragma unroll
+        for (int q = 0; q < L::PX; ++q) {
+            const int32_t cov = cx[q] * cy;
+            if (cov == 0) continue;
+            const uint32_t shape = gamma[cov];
+            const int k = it * L::PX + q;
+            if (RGB) {
+                pix[k] = rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
+            } else {
+                const uint32_t a_src = div255(alpha * shape);
+                pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
+            }
+        }
+    }
+}
+
 // RGB: the pages are Rgb8 (3 bytes per pixel) and path_rgb[p] is path p's
 // colour; otherwise Gray8 pages painted with each path's gray.
 template <int TW, int TH, bool RGB, bool FEW>
@@ -1716,7 +1867,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
     const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
     const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr,
-    const uint32_t* __restrict__ path_rgb) {
+    const uint32_t* __restrict__ path_rgb, const uint32_t* __restrict__ super_start) {
     using L = CompLayout<TW>;
     constexpr int ITERS = TH / (L::NW * L::RPW);
     constexpr int NPIX = TH * TW / COMP_THREADS;
@@ -1725,12 +1876,15 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     __shared__ uint32_t wcnt[L::NW];
     __shared__ uint8_t gamma[17];
     __shared__ int32_t mark[L::NW * L::RPW][TW];
-    __shared__ uint8_t lut[RGB ? 768 : 256];
+    // Two maps, used in turn: a run's map is written while no thread can still
+    // be reading the one before it (one barrier per run).
+    __shared__ uint8_t lut[2][RGB ? 768 : 256];
     __shared__ uint32_t red[L::NW];
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int col = (lane % L::LPR) * L::PX;
+    int lut_sel = 0;
     for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
         const uint32_t pg = find_page_by(pages, n_pages, t, false);
         const PageGeom G = pages[pg];
@@ -1761,6 +1915,8 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
         const uint32_t sx = static_cast<uint32_t>(X0 / stw), sy = static_cast<uint32_t>(Y0 / sth);
         const uint32_t q0 = G.work_base + (sy * G.nsx + sx) * G.nblk;
         const uint32_t l0 = super_off[q0], l1 = super_off[q0 + G.nblk];
+        // The supertile's last opaque full layer (position + 1, or 0).
+        const uint32_t s_open = super_start[G.super_base + sy * G.nsx + sx];
         // The tile clipped to the page: a path whose solid box holds it covers
         // every pixel that matters with coverage 16.
         const int TX1 = min(X0 + TW, W) - 1, TY1 = min(Y0 + TH, H) - 1;
@@ -1772,8 +1928,10 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
         // (255 * s + 255) >> 8 = s), so compositing starts there.
         uint32_t start = l0;
         {
-            uint32_t best = 0;
-            for (uint32_t c0 = l0; c0 < l1; c0 += COMP_CHUNK) {
+            // Only layers from the supertile's opaque start on can start the tile.
+            uint32_t best = s_open;
+            const uint32_t scan0 = s_open ? s_open : l0;
+            for (uint32_t c0 = scan0; c0 < l1; c0 += COMP_CHUNK) {
                 const uint32_t q = c0 + threadIdx.x;
                 if (q < l1) {
                     const PathInfo P = info[super_list[q]];
@@ -1809,8 +1967,9 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
             if (hit) {
                 const uint32_t pos = before + __popc(m & lanemask_lt());
                 HitInfo hi;
-                hi.g0 = P.y0 >> 2;
-                hi.g1 = P.y1 >> 2;
+                const bool box = (P.paint & PI_BOX) != 0;  // boxes keep AA rows, the others pixel-row groups
+                hi.g0 = box ? P.y0 : P.y0 >> 2;
+                hi.g1 = box ? P.y1 : P.y1 >> 2;
                 hi.py0 = P.py0;
                 hi.py1 = P.py1;
                 hi.goff = (P.paint & PI_RECTI) ? P.run_off : group_off[super_list[q]];
@@ -1841,34 +2000,36 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                     if (RGB) {
                         // One map per channel (each channel composes on its own).
                         if (m - k >= 2) {
-                            __syncthreads();  // the previous maps' readers are done
+                            uint8_t* map = lut[lut_sel];
+                            lut_sel ^= 1;
                             uint32_t v = threadIdx.x | (threadIdx.x << 8) | (threadIdx.x << 16);
                             for (uint32_t i = k; i < m; ++i)
                                 v = rgb_over(v, rgb_a_src((hits[i].paint >> 8) & 0xff, 255u), hits[i].rgb);
-                            lut[threadIdx.x] = static_cast<uint8_t>(v);
-                            lut[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
-                            lut[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
+                            map[threadIdx.x] = static_cast<uint8_t>(v);
+                            map[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
+                            map[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
                             __syncthreads();
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j)
-                                pix[j] = lut[pix[j] & 0xffu] | (uint32_t(lut[256 + ((pix[j] >> 8) & 0xffu)]) << 8) |
-                                         (uint32_t(lut[512 + (pix[j] >> 16)]) << 16);
+                                pix[j] = map[pix[j] & 0xffu] | (uint32_t(map[256 + ((pix[j] >> 8) & 0xffu)]) << 8) |
+                                         (uint32_t(map[512 + (pix[j] >> 16)]) << 16);
                         } else {
                             const uint32_t a = rgb_a_src((hits[k].paint >> 8) & 0xff, 255u), s = hits[k].rgb;
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j) pix[j] = rgb_over(pix[j], a, s);
                         }
                     } else if (m - k >= 2) {
-                        __syncthreads();  // the previous map's readers are done
+                        uint8_t* map = lut[lut_sel];
+                        lut_sel ^= 1;
                         uint32_t v = threadIdx.x;
                         for (uint32_t i = k; i < m; ++i) {
                             const uint32_t a = (hits[i].paint >> 8) & 0xff, gg = hits[i].paint & 0xff;
                             v = div255((255u - a) * v + a * gg);  // a_src = div255(a * AA_GAMMA[16]) = a
                         }
-                        lut[threadIdx.x] = static_cast<uint8_t>(v);
+                        map[threadIdx.x] = static_cast<uint8_t>(v);
                         __syncthreads();
 #pragma unroll
-                        for (int j = 0; j < NPIX; ++j) pix[j] = lut[pix[j]];
+                        for (int j = 0; j < NPIX; ++j) pix[j] = map[pix[j]];
                     } else {
                         const uint32_t a = (hits[k].paint >> 8) & 0xff, gg = hits[k].paint & 0xff;
 #pragma unroll
@@ -1880,7 +2041,8 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 }
                 if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
                 if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
-                composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
+                if (hits[k].paint & PI_BOX) composite_box<TW, TH, RGB>(hits[k], rowmap, X0, Y0, gamma, pix);
+                else composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
                 nxt = nxt2;
                 ++k;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/rrb.h"
+#include "rrb_device_scope.h"
 
 namespace {
 
@@ -160,7 +161,8 @@ extern "C" {
 
 int rrb_mlp_create(int device, uint64_t seed, rrb_mlp** out) {
     if (!out) return RRB_ERR_INVARIANT;
-    if (cudaSetDevice(device) != cudaSuccess) return RRB_ERR_DEVICE;
+    const rrb_host::DeviceScope dev_scope(device);
+    if (dev_scope.status() != cudaSuccess) return RRB_ERR_DEVICE;
     rrb_mlp* m = new rrb_mlp();
     m->device = device;
     bool ok = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) == cudaSuccess;
@@ -186,7 +188,7 @@ int rrb_mlp_create(int device, uint64_t seed, rrb_mlp** out) {
 
 int rrb_mlp_destroy(rrb_mlp* m) {
     if (!m) return RRB_OK;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     if (m->stream) cudaStreamSynchronize(m->stream);
     float* bufs[] = {m->d_params, m->d_grad, m->d_m, m->d_v, m->d_loss, m->d_x, m->d_y, m->d_out};
     for (float* b : bufs) cudaFree(b);
@@ -197,7 +199,7 @@ int rrb_mlp_destroy(rrb_mlp* m) {
 
 int rrb_mlp_set_params(rrb_mlp* m, const float* params) {
     if (!m || !params) return RRB_ERR_INVARIANT;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     if (cudaMemcpyAsync(m->d_params, params, NPARAM * sizeof(float), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
         cudaMemsetAsync(m->d_grad, 0, NPARAM * sizeof(float), m->stream) != cudaSuccess ||
         cudaMemsetAsync(m->d_m, 0, NPARAM * sizeof(float), m->stream) != cudaSuccess ||
@@ -209,7 +211,7 @@ int rrb_mlp_set_params(rrb_mlp* m, const float* params) {
 
 int rrb_mlp_get_params(rrb_mlp* m, float* params) {
     if (!m || !params) return RRB_ERR_INVARIANT;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     if (cudaMemcpyAsync(params, m->d_params, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, m->stream) != cudaSuccess)
         return RRB_ERR_DEVICE;
     return cudaStreamSynchronize(m->stream) == cudaSuccess ? RRB_OK : RRB_ERR_DEVICE;
@@ -217,7 +219,7 @@ int rrb_mlp_get_params(rrb_mlp* m, float* params) {
 
 int rrb_mlp_loss_grad(rrb_mlp* m, const float* X, const float* y, uint32_t n, float* grad_out, float* loss_out) {
     if (!m || !X || !y || !n) return RRB_ERR_INVARIANT;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     int rc = ensure_io(m, n);
     if (rc) return rc;
     cudaMemcpyAsync(m->d_x, X, static_cast<size_t>(n) * IN * sizeof(float), cudaMemcpyHostToDevice, m->stream);
@@ -238,7 +240,7 @@ int rrb_mlp_loss_grad(rrb_mlp* m, const float* X, const float* y, uint32_t n, fl
 int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32_t epochs, uint32_t batch,
                   float lr, uint64_t seed, float* final_loss) {
     if (!m || !X || !y || !n || !epochs) return RRB_ERR_INVARIANT;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     int rc = ensure_io(m, n);
     if (rc) return rc;
     if (!batch || batch > n) batch = n;
@@ -284,7 +286,7 @@ int rrb_mlp_train(rrb_mlp* m, const float* X, const float* y, uint32_t n, uint32
 
 int rrb_mlp_predict(rrb_mlp* m, const float* X, uint32_t n, float* out) {
     if (!m || !X || !out || !n) return RRB_ERR_INVARIANT;
-    cudaSetDevice(m->device);
+    const rrb_host::DeviceScope dev_scope(m->device);
     int rc = ensure_io(m, n);
     if (rc) return rc;
     cudaMemcpyAsync(m->d_x, X, static_cast<size_t>(n) * IN * sizeof(float), cudaMemcpyHostToDevice, m->stream);

@@ -35,6 +35,7 @@
 #include <string>
 
 #include "../../include/rrb.h"
+#include "rrb_device_scope.h"
 
 // The pipeline's kernels with internal linkage in this translation unit: this
 // module carries its own copies, so it can load apart from the main one.
@@ -342,7 +343,8 @@ extern "C" int rrb_record_path_fill_static(rrb_ctx* c, const rrb_path_fill_param
         if (!std::isfinite(p->matrix[i])) return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "matrix must be finite");
     if (p->width == 0 || p->height == 0 || p->width > 16383 || p->height > (1u << 28))
         return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "page width must be 1..16383 and height 1..2^28");
-    if (p->page_offset + static_cast<uint64_t>(p->width) * p->height > rrb_device_buffer_len(p->page))
+    const uint64_t page_len = rrb_device_buffer_len(p->page);
+    if (p->page_offset > page_len || static_cast<uint64_t>(p->width) * p->height > page_len - p->page_offset)
         return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
     if (p->n_pts > kMaxPoints) {
         char msg[160];
@@ -353,7 +355,8 @@ extern "C" int rrb_record_path_fill_static(rrb_ctx* c, const rrb_path_fill_param
     if (p->n_pts == 0) return RRB_OK;
     std::lock_guard<std::mutex> lk(g_lock);
     const int device = rrb_ctx_device(c);
-    RRB_STATIC_CUDA(c, cudaSetDevice(device));
+    const rrb_host::DeviceScope dev_scope(device);
+    RRB_STATIC_CUDA(c, dev_scope.status());
     DeviceScratch* d = nullptr;
     int rc = scratch_for(c, device, d);
     if (rc) return rc;

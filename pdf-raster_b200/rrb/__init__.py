@@ -20,7 +20,6 @@ from . import _abi
 from ._abi import (RRB_CAP_BUTT, RRB_CAP_PROJECTING, RRB_CAP_ROUND, RRB_FILL_EVEN_ODD,  # noqa: F401
                    RRB_FILL_NONZERO, RRB_JOIN_BEVEL, RRB_JOIN_MITER, RRB_JOIN_ROUND, RRB_ROWMAP_AS_SHIPPED,
                    RRB_ROWMAP_DOCUMENTED, BatchStats, ClipPath, PathBatchParams, PathFillParams, RequestResult,
-                   SceneParams,
                    ServerConfig, ServerStats, StageTime, StrokeParams, Tuning, VramBudget)
 
 __all__ = ["B200Backend", "BackendError", "DeviceBuffer", "PinnedBuffer", "Scene", "PathBuilder", "Server", "lib",
@@ -115,59 +114,7 @@ def conic_to_cubic(p0, pc, p3):
     return (out[0], out[1]), (out[2], out[3])
 
 
-class Scene:
-    """A seeded synthetic workload (kind 0 polygons, 1 glyphs, 2 mixed pages).
-
-    Arrays are numpy views of the generator's memory (valid while the Scene lives).
-    """
-
-    def __init__(self, kind: int, seed: int = 0, **kw):
-        p = SceneParams(kind=kind, seed=seed)
-        for k, v in kw.items():
-            setattr(p, k, v)
-        h = C.c_void_p()
-        rc = lib().rrb_scene_generate(C.byref(p), C.byref(h))
-        if rc:
-            raise BackendError(rc, "scene generation failed")
-        self._h = h.value
-        self.view = PathBatchParams()
-        lib().rrb_scene_view(self._h, C.byref(self.view))
-        v = self.view
-        self.n_paths = int(v.n_paths)
-        self.n_pts = int(v.n_pts)
-        self.n_pages = int(v.n_pages)
-        asa = np.ctypeslib.as_array
-        self.pts = asa(v.pts, shape=(self.n_pts * 2,)).reshape(self.n_pts, 2) if self.n_pts else np.zeros((0, 2))
-        self.flags = asa(v.flags, shape=(self.n_pts,)) if self.n_pts else np.zeros(0, np.uint8)
-        self.path_pt_off = asa(v.path_pt_off, shape=(self.n_paths + 1,))
-        self.fill_rule = asa(v.fill_rule, shape=(self.n_paths,))
-        self.gray = asa(v.gray, shape=(self.n_paths,))
-        self.alpha = asa(v.alpha, shape=(self.n_paths,))
-        self.path_page = asa(v.path_page, shape=(self.n_paths,))
-        self.page_width = asa(v.page_width, shape=(self.n_pages,))
-        self.page_height = asa(v.page_height, shape=(self.n_pages,))
-        self.page_offset = asa(v.page_offset, shape=(self.n_pages,))
-        self.arena_bytes = int(lib().rrb_scene_arena_bytes(self._h))
-        cnt = (C.c_uint64 * 3)()
-        lib().rrb_scene_counts(self._h, cnt)
-        self.n_lines, self.n_cubics = int(cnt[0]), int(cnt[1])
-
-    def __del__(self):
-        h, self._h = getattr(self, "_h", None), None
-        if h:
-            lib().rrb_scene_free(h)
-
-    @property
-    def pixels(self) -> int:
-        return int(np.sum(self.page_width.astype(np.int64) * self.page_height.astype(np.int64)))
-
-    def blank_arena(self, value: int = 255) -> np.ndarray:
-        """Host page arena initialised to `value` (white pages)."""
-        return np.full(self.arena_bytes, value, dtype=np.uint8)
-
-    def page(self, arena: np.ndarray, i: int) -> np.ndarray:
-        o, w, h = int(self.page_offset[i]), int(self.page_width[i]), int(self.page_height[i])
-        return arena[o:o + w * h].reshape(h, w)
+from .scenes import Scene  # noqa: E402  (the seeded workloads; librrb_scenes.so)
 
 
 def batch_params(pts, flags, path_pt_off, fill_rule, gray, alpha, path_page, page_width, page_height,

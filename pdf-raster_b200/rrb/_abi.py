@@ -108,7 +108,7 @@ class Tuning(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles", "tile_pairs",
-        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves", "host_ns")]
+        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves", "host_ns", "row_groups", "host_syncs")]
 
 
 class StageTime(C.Structure):
@@ -153,21 +153,6 @@ class ClipPath(C.Structure):
 
 ClipPath._fields_ = [("pts", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_uint8)), ("n_pts", C.c_uint64),
                      ("even_odd", C.c_uint8), ("reserved", C.c_uint8 * 7), ("next", C.POINTER(ClipPath))]
-
-
-class SceneParams(C.Structure):
-    _fields_ = [
-        ("kind", C.c_uint32),
-        ("seed", C.c_uint64),
-        ("n_pages", C.c_uint32),
-        ("n_paths", C.c_uint32),
-        ("page_w", C.c_uint32),
-        ("page_h", C.c_uint32),
-        ("page_scale", C.c_double),
-        ("paths_scale", C.c_double),
-        ("path_cap", C.c_uint32),
-        ("reserved", C.c_uint32),
-    ]
 
 
 # Every exported symbol of include/rrb.h with its signature: (restype, argtypes).
@@ -265,11 +250,6 @@ SIGNATURES = {
     "rrb_path_pts": (C.POINTER(C.c_double), [VP]),
     "rrb_path_flags": (C.POINTER(C.c_uint8), [VP]),
     "rrb_conic_to_cubic": (None, [C.c_double] * 6 + [C.POINTER(C.c_double)]),
-    "rrb_scene_generate": (C.c_int, [C.POINTER(SceneParams), C.POINTER(VP)]),
-    "rrb_scene_free": (None, [VP]),
-    "rrb_scene_view": (None, [VP, C.POINTER(PathBatchParams)]),
-    "rrb_scene_arena_bytes": (C.c_uint64, [VP]),
-    "rrb_scene_counts": (None, [VP, C.POINTER(C.c_uint64)]),
 }
 
 _LIB = None

@@ -151,6 +151,24 @@ extern "C" int rl_recti_spans(const int32_t* edges, int n, int eo, int32_t r, in
     return ns;
 }
 
+// The box test of rectilinear paths (recti_events + recti_box, PI_BOX) over n
+// edges whose AA rows span [y0, y1]: 1, the span [out[0], out[1]) of AA
+// columns and the painted AA rows [out[2], out[3]] when every painted AA row
+// holds that one span, else 0.
+extern "C" int rl_recti_box(const int32_t* edges, int n, int eo, int32_t y0, int32_t y1, int32_t aa_width,
+                            int32_t lo, int32_t hi, int32_t* out) {
+    rrb::PathInfo P{};
+    P.e_begin = 0;
+    P.e_end = static_cast<uint32_t>(n);
+    P.paint = eo ? (1u << 16) : 0u;
+    P.y0 = y0;
+    P.y1 = y1;
+    const rrb::Edge* e = reinterpret_cast<const rrb::Edge*>(edges);
+    int32_t ev[rrb::RECTI_MAX_EVENTS];
+    const int nev = rrb::recti_events(P, e, ev);
+    return rrb::recti_box(P, e, ev, nev, aa_width, lo, hi, out[0], out[1], out[2], out[3]) ? 1 : 0;
+}
+
 // The clip-path lowering's XPath walk (xpath_segments in rrb_clip.cu): up to
 // cap segments (x0, y0, x1, y1) in device space; returns the count.
 extern "C" int64_t rl_xpath_segments(const double* pts, const uint8_t* flags, uint64_t n, const double* m,

@@ -7,6 +7,7 @@ of crates/gpu/src/backend/params.rs:978-1075).
 import ctypes as C
 import re
 import subprocess
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -14,10 +15,11 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "rrb.h"
+SCENES_HEADER = ROOT / "include" / "rrb_scenes.h"
 
 
-def declared_functions():
-    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+def declared_functions(header=HEADER):
+    text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
     return sorted(set(re.findall(r"^[A-Za-z_][\w\s\*]*?\b(rrb_\w+)\s*\(", text, flags=re.M)))
 
 
@@ -29,6 +31,22 @@ def test_library_exports_every_declared_symbol(rrb_lib):
     assert not missing, missing
     from rrb import _abi
     assert sorted(_abi.SIGNATURES) == names  # every declaration has a ctypes binding
+
+
+def test_scene_library_exports_its_header_and_is_separate(rrb_lib):
+    """librrb_scenes.so exports rrb_scenes.h; the backend library does not
+    carry the generator, and generating a scene maps no backend library."""
+    from rrb import scenes
+    names = declared_functions(SCENES_HEADER)
+    assert names == sorted(scenes.SIGNATURES)
+    lib = scenes.lib()
+    assert all(hasattr(lib, n) for n in names)
+    assert not any(hasattr(rrb_lib.lib(), n) for n in names)
+    code = ("import sys; sys.path.insert(0, %r); from rrb.scenes import Scene; s = Scene(2, 1, n_pages=1, "
+            "page_scale=0.05, paths_scale=0.01); print(s.n_paths); "
+            "print(any('librrb.so' in l for l in open('/proc/self/maps')))" % str(ROOT / "pdf-raster_b200"))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout.split()
+    assert int(out[0]) > 0 and out[1] == "False"
 
 
 def test_version_and_status_names(rrb_lib):
@@ -48,7 +66,7 @@ STRUCTS = {
     "rrb_tuning": ("Tuning", ["tile_w", "tile_h", "rows_per_chunk", "wave_points", "reserved"]),
     "rrb_batch_stats": ("BatchStats", ["paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles",
                                        "tile_pairs", "nonterminating_rows", "kernel_launches", "scratch_grows",
-                                       "waves", "host_ns"]),
+                                       "waves", "host_ns", "row_groups", "host_syncs"]),
     "rrb_stage_time": ("StageTime", ["name", "ms", "launches"]),
     "rrb_server_config": ("ServerConfig", ["device", "workers", "mem_budget_bytes", "max_batch_pages", "tile_w",
                                            "tile_h", "predict_threads", "reserved"]),
@@ -62,14 +80,15 @@ STRUCTS = {
                                                 "height", "fill_rule"]),
     "rrb_stroke_params": ("StrokeParams", ["line_width", "miter_limit", "dash_phase", "dash", "n_dash", "line_cap",
                                            "line_join", "stroke", "reserved"]),
-    "rrb_scene_params": ("SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h", "page_scale",
-                                         "paths_scale", "path_cap", "reserved"]),
+    "rrb_scene_params": ("scenes.SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h",
+                                                "page_scale", "paths_scale", "path_cap", "reserved"]),
 }
 
 
 def test_struct_layouts_match_c_compiler(rrb_lib, tmp_path):
     from rrb import _abi
-    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', f'#include "{SCENES_HEADER}"',
+             "int main(void){"]
     for cname, (_, fields) in STRUCTS.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
         for f in fields:
@@ -81,8 +100,9 @@ def test_struct_layouts_match_c_compiler(rrb_lib, tmp_path):
     subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(src)], check=True)
     out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
                                                          check=True).stdout.splitlines())
+    from rrb import scenes
     for cname, (pyname, fields) in STRUCTS.items():
-        st = getattr(_abi, pyname)
+        st = getattr(scenes, pyname.split(".")[1]) if pyname.startswith("scenes.") else getattr(_abi, pyname)
         assert C.sizeof(st) == int(out[f"{cname} size"]), cname
         for f in fields:
             assert getattr(st, f).offset == int(out[f"{cname}.{f}"]), (cname, f)
@@ -149,7 +169,7 @@ def test_scene_generator_is_seeded(rrb_lib):
     m = rrb_lib.Scene(2, seed=0, n_pages=5, page_scale=0.1, paths_scale=0.01)
     assert m.n_pages == 5 and np.all(np.diff(m.path_page.astype(np.int64)) >= 0)
     assert m.alpha.min() >= 32
-    with pytest.raises(rrb_lib.BackendError):
+    with pytest.raises(ValueError):
         rrb_lib.Scene(9)
 
 

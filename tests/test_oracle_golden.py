@@ -253,6 +253,31 @@ def test_coverage_matches_popcount(O, x0, n):
     assert np.array_equal(got, exp)
 
 
+@pytest.mark.parametrize("tier", [1, 2])
+def test_coverage_simd_tier_matches_scalar(O, tier):
+    # avx2_coverage_matches_scalar / avx512_coverage_matches_scalar (aa_coverage.rs:684-717):
+    # TIER_TEST_N = 300 pixels of the dispatch test rows, the SIMD tier against the scalar
+    # loop; plus every even and odd x0 up to 8 and spans that end inside, on and past a chunk.
+    if O.coverage_tier() < tier:
+        pytest.skip(f"host lacks coverage tier {tier}")
+    rng = np.random.default_rng(tier)
+    for x0, n in [(0, 300)] + [(x, k) for x in range(9) for k in (1, 63, 64, 127, 128, 129, 255, 256, 257, 700)]:
+        rb = (x0 + n + 1) // 2
+        i = np.arange(rb, dtype=np.uint16)
+        rows = np.stack([((i * m + a) & 0xFF) for m, a in ((0x37, 0), (0x53, 0), (0x17, 0))] +
+                        [(~i) & 0xFF]).astype(np.uint8)
+        for r in (rows, rng.integers(0, 256, rows.shape, dtype=np.uint8)):
+            assert np.array_equal(O.aa_coverage_span_tier(r, x0, n, tier), O.aa_coverage_span_tier(r, x0, n, 0)), \
+                (tier, x0, n)
+
+
+def test_coverage_dispatch_uses_the_hosts_best_tier(O):
+    # dispatch_coverage (aa_coverage.rs:497-514): AVX-512 BITALG when present, else AVX2.
+    flags = open("/proc/cpuinfo").read().split("flags")[1].split("\n")[0].split()
+    want = 2 if {"avx512_bitalg", "avx512bw"} <= set(flags) else (1 if "avx2" in flags else 0)
+    assert O.coverage_tier() == want
+
+
 # ---- div255 (crates/color/src/convert.rs:316-345) -------------------------------------
 
 def test_div255_exhaustive(O):

@@ -51,6 +51,8 @@ def shim(tmp_path_factory):
     lib.rl_recti_spans.argtypes = [i32p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p,
                                    C.POINTER(C.c_uint32)]
     lib.rl_recti_spans.restype = C.c_int
+    lib.rl_recti_box.argtypes = [i32p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p]
+    lib.rl_recti_box.restype = C.c_int
     lib.rl_xpath_segments.argtypes = [dp, C.POINTER(C.c_uint8), C.c_uint64, dp, C.c_double, dp, C.c_int64]
     lib.rl_xpath_segments.restype = C.c_int64
     return lib
@@ -331,6 +333,73 @@ def test_recti_row_spans_match_oracle(oracle, shim):
                 for a, b in zip(s0[:ns].tolist(), s1[:ns].tolist()):
                     line[a:b] = True
                 assert np.array_equal(np.packbits(line), bits[k]), (i, y, k)
+
+
+def test_box_coverage_matches_oracle(oracle, shim):
+    """Rectangles (fractional corners, partly off the page, either winding,
+    both rules) and other rectilinear paths: whenever the box test
+    (recti_events + recti_box) accepts a path, the composite's closed form
+    cx * cy reproduces every pixel the oracle paints, under both row maps;
+    single on-page rectangles are always accepted, and paths whose rows differ
+    are refused."""
+    rng = np.random.default_rng(29)
+    W, H = 48, 40
+    aw = 4 * W
+    gamma = oracle.aa_gamma()
+    inv = {255 - int(g): k for k, g in enumerate(gamma)}  # page value after one opaque black layer -> coverage
+    out = np.zeros(4, np.int32)
+    boxes = refused = 0
+    for i in range(300):
+        kind = i % 3
+        subs = []
+        x0, y0 = rng.uniform([-8, -8], [W + 2, H + 2])
+        x1, y1 = x0 + rng.uniform(0.2, 30), y0 + rng.uniform(0.2, 26)
+        subs.append([(x0, y0), (x1, y0), (x1, y1), (x0, y1)])
+        if kind == 1:  # a second rectangle beside or below: an L, a stack or two disjoint boxes
+            a0, b0 = rng.uniform([-4, -4], [W, H])
+            a1, b1 = a0 + rng.uniform(0.5, 20), b0 + rng.uniform(0.5, 15)
+            if rng.random() < 0.3:
+                a0, a1 = x0, x1  # stacked on the same columns: still one box where the two touch or overlap
+            subs.append([(a0, b0), (a1, b0), (a1, b1), (a0, b1)])
+        if kind == 2 and rng.random() < 0.5:
+            subs[0] = subs[0][::-1]
+        pts, fl = _path_closed(subs)
+        eo = bool(rng.integers(0, 2))
+        segs = oracle.xpath_new(pts, fl, flatness=0.1, close=True)
+        ends = np.array([(s.x1, s.y1, s.x0, s.y0) if s.flags & 4 else (s.x0, s.y0, s.x1, s.y1) for s in segs],
+                        np.float64).reshape(-1)
+        edges = np.zeros(8 * max(1, len(segs)), np.int32)
+        shim.rl_make_edges(_dp(ends), len(segs), 0, 4 * H - 1, _ip(edges))
+        e = edges.reshape(-1, 8)[: len(segs)]
+        live = e[(e[:, 2] & 16) == 0]
+        if not len(live) or np.any((live[:, 2] & 3) == 2):
+            continue  # no rows on the page, or a sloped edge (not a rectilinear path)
+        ay0, ay1 = int(live[:, 0].min()), int(live[:, 1].max())
+        is_box = shim.rl_recti_box(_ip(edges), len(segs), int(eo), ay0, ay1, aw, 0, aw, _ip(out))
+        on_page = kind != 1 and 0 <= x0 and x1 <= W and 0 <= y0 and y1 <= H
+        # Edges in adjacent AA columns (or rows) merge into one zero-count entry
+        # that paints nothing, so only rectangles at least two AA units across
+        # must be boxes.
+        if on_page and np.floor(4 * x1) - np.floor(4 * x0) >= 2 and np.floor(4 * y1) - np.floor(4 * y0) >= 2:
+            assert is_box, (i, subs)
+        for rowmap in (0, 1):
+            page = np.full((H, W), 255, np.uint8)
+            oracle.fill_path(page, pts, fl, eo=eo, gray=0, alpha=255, rowmap=rowmap)
+            cov = np.vectorize(inv.get)(page)
+            if is_box:
+                s0, s1, r0, r1 = (int(v) for v in out)
+                assert ay0 <= r0 <= r1 <= ay1
+                xs = 4 * np.arange(W)
+                cx = np.clip(np.minimum(xs + 4, s1) - np.maximum(xs, s0), 0, None)
+                ys = 16 * np.arange(H) + 12 if rowmap else 4 * np.arange(H)
+                cy = np.clip(np.minimum(ys + 4, r1 + 1) - np.maximum(ys, r0), 0, None)
+                if rowmap:  # the shipped loop visits pixel row y only when AA row 4y+3 is in the scanner's range
+                    vis = 4 * np.arange(H) + 3
+                    cy[(vis < ay0) | (vis > ay1)] = 0
+                assert np.array_equal(cov, np.outer(cy, cx)), (i, rowmap, subs)
+        boxes += bool(is_box)
+        refused += not is_box
+    assert boxes > 150 and refused > 20
 
 
 def _path_closed(subpaths):
