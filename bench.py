@@ -745,28 +745,34 @@ def run_fill_ops(args, rank, world):
     be.close()
 
 
-def page_requests(rrb, scene):
-    """One request per page of `scene`: (params, keep-alive arrays, page bytes)."""
+SERVING_POOL = 128  # requests 0..127 render the pages pinned in tests/golden/serving_request_digests.json
+
+
+def request_pool(rrb, n):
+    """The pages serving requests 0..n-1 ask for: request r is one page of the
+    mixed-page generator seeded by its id (kind 2, seed r, one page). Returns
+    [(params, scene kept alive, page bytes, pinned SHA-256 or None)]."""
+    pinned = {}
+    path = ROOT / "tests" / "golden" / "serving_request_digests.json"
+    if path.exists():
+        pinned = {r["request"]: r["page_sha256"] for r in json.loads(path.read_text())["records"]}
     out = []
-    for pg in range(scene.n_pages):
-        idx = np.nonzero(scene.path_page == pg)[0]
-        a, b = int(scene.path_pt_off[idx[0]]), int(scene.path_pt_off[idx[-1] + 1])
-        keep = []
-        w, h = int(scene.page_width[pg]), int(scene.page_height[pg])
-        p = rrb.batch_params(scene.pts[a:b], scene.flags[a:b], scene.path_pt_off[idx[0]:idx[-1] + 2] - a,
-                             scene.fill_rule[idx], scene.gray[idx], scene.alpha[idx], np.zeros(len(idx), np.uint32),
-                             [w], [h], [0], None, keep=keep)
-        out.append((p, keep, w * h))
+    for r in range(n):
+        sc = rrb.Scene(kind=2, seed=r, n_pages=1)
+        sc.view.pages = None
+        out.append((sc.view, sc, int(sc.page_width[0]) * int(sc.page_height[0]), pinned.get(r)))
     return out
 
 
 def serve_rates(srv, reqs, rates, n_req, seed=0):
-    """Poisson arrivals at each rate; latency percentiles of the completed requests."""
+    """Poisson arrivals at each rate, request i rendering pool page i mod len(pool);
+    latency percentiles of the completed requests and the number whose page
+    equals the oracle's pinned digest."""
+    import hashlib
     rng = np.random.default_rng(seed)
     out = []
     for rate in rates:
         gaps = rng.exponential(1.0 / rate, n_req)
-        outs = [np.empty(reqs[i % len(reqs)][2], np.uint8) for i in range(n_req)]
         tickets = []
         t0 = time.perf_counter()
         due = t0
@@ -775,50 +781,67 @@ def serve_rates(srv, reqs, rates, n_req, seed=0):
             dt = due - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-            p, k, _ = reqs[i % len(reqs)]
-            tickets.append(srv.submit(p, outs[i], keep=k))
-        res = [srv.wait(t) for t in tickets]
-        lat = [r["latency_ns"] / 1e6 for r in res]
+            p, k, n, _ = reqs[i % len(reqs)]
+            page = np.empty(n, np.uint8)
+            tickets.append((srv.submit(p, page, keep=k), page, i % len(reqs)))
+        res, exact, checked = [], 0, 0
+        for t, page, r in tickets:
+            res.append(srv.wait(t))
         wall = time.perf_counter() - t0
+        for t, page, r in tickets:
+            d = reqs[r][3]
+            if d is not None:
+                checked += 1
+                exact += hashlib.sha256(page.tobytes()).hexdigest() == d
+        lat = [x["latency_ns"] / 1e6 for x in res]
         px = sum(reqs[i % len(reqs)][2] for i in range(n_req))
         out.append({"rate_pages_s": rate, "requests": n_req, "completed_pages_s": n_req / wall,
                     "mpixel_s": px / wall / 1e6, "p50_ms": float(np.percentile(lat, 50)),
                     "p95_ms": float(np.percentile(lat, 95)), "p99_ms": float(np.percentile(lat, 99)),
-                    "mean_ms": float(np.mean(lat))})
+                    "mean_ms": float(np.mean(lat)), "bit_exact_requests": f"{exact}/{checked}"})
     return out
 
 
 def run_serving(args, rank, world):
-    """Poisson page-render requests against the continuous-batching server,
-    first in arrival order with the default tile, then with the cost model
-    (shortest predicted first, tile shape per batch from the model)."""
+    """Poisson page-render requests against the continuous-batching server
+    under three scheduling policies: arrival order with the default 64x16
+    tile; the autotuner's table (tile shape per batch from page size and edge
+    density, arrival order); the learned cost model (tile shape per batch and
+    shortest-predicted-first admission, falling back to the table). Every
+    request's page is checked against the oracle's pinned digest."""
     if rank != 0:
         return
     import rrb
     from rrb.autotune import CostModel
-    scene = rrb.Scene(kind=2, seed=0)
-    reqs = page_requests(rrb, scene)
+    reqs = request_pool(rrb, min(args.requests, SERVING_POOL))
     rates = [float(r) for r in args.rates.split(",")]
     model_path = Path(args.cost_model)
-    policies = ["arrival_order"] + (["cost_model"] if model_path.exists() else [])
+    model = CostModel.load(model_path) if model_path.exists() else None
+    policies = ["arrival_order"] + (["autotuner_table", "cost_model"] if model is not None else [])
     report = {}
     for policy in policies:
         with rrb.Server(workers=args.workers, mem_budget=args.mem_budget_gb << 30, max_batch_pages=64) as srv:
             if policy == "cost_model":
-                srv.set_cost_model(CostModel.load(model_path))
-            # warm-up: every distinct page, queued at once, twice (scratch reaches its working size)
-            for _ in range(2):
-                warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n in reqs]
-                for t in warm:
-                    srv.wait(t)
+                srv.set_cost_model(model)
+            elif policy == "autotuner_table":
+                srv.set_cost_model(table=model.table, shortest_first=False)
+            # warm-up: every distinct page, queued at once (scratch reaches its working size)
+            warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n, _ in reqs]
+            for t in warm:
+                srv.wait(t)
             report[policy] = {"rates": serve_rates(srv, reqs, rates, args.requests), "server_stats": srv.stats()}
     best = report.get("cost_model", report["arrival_order"])
     line = {"metric": "p99 page latency under Poisson load (continuous batching)", "unit": "ms",
             "value": best["rates"][-1]["p99_ms"], "higher_is_better": False, "n_gpus": 1,
-            "config": {"workload": "requests = single pages of the mixed 64-page scene (seed 0), cycled",
+            "config": {"workload": f"request r = one page of the mixed-page generator seeded by r (kind 2, seed r); "
+                                   f"requests cycle through the {len(reqs)} pages pinned by the oracle",
                        "workers": args.workers, "mem_budget_gb": args.mem_budget_gb,
-                       "cost_model": str(model_path) if model_path.exists() else None},
+                       "cost_model": str(model_path) if model is not None else None},
             "serving": report}
+    if model is not None:
+        line["model_vs_table"] = {r_m["rate_pages_s"]: {"mpixel_s": r_m["mpixel_s"] / max(1e-9, r_t["mpixel_s"]),
+                                                       "p99": r_m["p99_ms"] / max(1e-9, r_t["p99_ms"])}
+                                  for r_m, r_t in zip(report["cost_model"]["rates"], report["autotuner_table"]["rates"])}
     print(json.dumps(line), flush=True)
 
 

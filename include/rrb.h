@@ -259,6 +259,16 @@ int rrb_record_path_batch_rgb(rrb_ctx* ctx, const rrb_path_batch_params* p, cons
  * rectangular W/W* clip path (detect_rect, clip.rs:130-140). */
 int rrb_record_path_batch_ex(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb,
                              const double* clip_rects);
+/* rrb_record_path_batch_ex with, under RRB_ROWMAP_AS_SHIPPED, the pixel rows
+ * the shipped driver loop visits given per path: visit_rows[2p..2p+1] =
+ * [v0, v1] (host int32; NULL: each path's own, the rows y whose AA row 4y+3
+ * lies in its scanner range, fill/mod.rs:176-203). Path p then draws pixel
+ * rows v0 .. v1 from its AA rows 16y+12 .. 16y+15. This is how a clip path
+ * paints on its fill's rows (rrb_lower_clip_paths); the documented row map
+ * ignores visit_rows. No counterpart in the reference, which clips inside
+ * fill_impl. */
+int rrb_record_path_batch_visit(rrb_ctx* ctx, const rrb_path_batch_params* p, const uint8_t* path_rgb,
+                                const double* clip_rects, const int32_t* visit_rows);
 /* ---- clip paths (W / W* on a path that is not an axis-aligned rectangle) ----
  * A fill's clip paths: points and PathBuilder flags in user space (the batch
  * matrix applies), applied in order from the first through `next` as
@@ -289,15 +299,22 @@ typedef struct rrb_clip_path_s {
  * scanner overwrites the AA lines in turn) within the intersection of the
  * rectangles. Lowered path k comes from input path out_src_path[k] (its gray,
  * alpha, page and colour), has fill rule out_rule[k] and clip rectangle
- * out_clip_rects[4k..4k+3]; its points are out_pts / out_flags from
- * out_path_pt_off[k] to out_path_pt_off[k + 1]. Any output may be NULL;
- * *n_pts_out and *n_paths_out always receive the sizes, and
- * RRB_ERR_POOL_EXHAUSTED says an output was too small. Needs the identity
- * matrix (the renderer's DEVICE_MATRIX) and RRB_ROWMAP_DOCUMENTED. */
+ * out_clip_rects[4k..4k+3], and visits pixel rows out_visit_rows[2k..2k+1]
+ * under the as-shipped row map (see rrb_record_path_batch_visit); its points
+ * are out_pts / out_flags from out_path_pt_off[k] to out_path_pt_off[k + 1].
+ * Under RRB_ROWMAP_DOCUMENTED a clipped fill draws one render_aa_line per
+ * pixel row of the fill, so the lowered path is clipped to the fill's rows;
+ * under RRB_ROWMAP_AS_SHIPPED the loop visits the pixel rows y whose AA row
+ * 4y+3 lies in the fill's scanner range and shows the clip scanner's rows
+ * 16y+12 .. 16y+15, so the lowered path keeps the clip scanner's rows and
+ * gets the fill's visited rows. Any output may be NULL; *n_pts_out and
+ * *n_paths_out always receive the sizes, and RRB_ERR_POOL_EXHAUSTED says an
+ * output was too small. Needs the identity matrix (the renderer's
+ * DEVICE_MATRIX). */
 int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double* clip_rects, const rrb_clip_path* clip_paths,
                          double* out_pts, uint8_t* out_flags, uint64_t pts_cap, uint64_t* out_path_pt_off,
-                         uint64_t* out_src_path, uint8_t* out_rule, double* out_clip_rects, uint64_t paths_cap,
-                         uint64_t* n_pts_out, uint64_t* n_paths_out);
+                         uint64_t* out_src_path, uint8_t* out_rule, double* out_clip_rects, int32_t* out_visit_rows,
+                         uint64_t paths_cap, uint64_t* n_pts_out, uint64_t* n_paths_out);
 
 /* ---- strokes (crates/raster/src/stroke/mod.rs:58-283, stroke/path.rs) ----
  * StrokeParams (stroke/mod.rs:29-48) of one path. The flatness is the batch's

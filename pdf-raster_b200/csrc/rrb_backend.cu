@@ -67,6 +67,7 @@ struct rrb_ctx {
     Scratch s_pts, s_flags, s_off, s_rule, s_gray, s_alpha, s_page, s_geom, s_pw, s_ph, s_mtx;
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_super_start;  // per supertile: one past its last opaque full layer
+    Scratch s_big;          // piece slots of curves flattened by a warp each
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
     Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
@@ -193,7 +194,7 @@ bool valid_tile(uint32_t w, uint32_t h) {
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
                      uint32_t n_pages, uint32_t n_tiles, const uint32_t* super_off, const uint32_t* super_list,
                      const uint32_t* row_off, const uint2* row_idx, const uint32_t* spans, const int4* runs,
-                     uint8_t* arena, int rowmap, const BatchCounters* ctr, const uint32_t* path_rgb,
+                     uint8_t* arena, int rowmap, BatchCounters* ctr, const uint32_t* path_rgb,
                      bool rectilinear, const uint32_t* super_start) {
 #define RRB_COMP(TW, TH, RGB, FEW)                                                                           \
     k_composite<TW, TH, RGB, FEW><<<grid, COMP_THREADS, 0, c->stream>>>(                                      \
@@ -311,6 +312,8 @@ struct rrb_batch {
     Scratch clip;                   // per-path clip in AA units (int4), when has_clip
     Scratch clipf;                  // the clip rectangles as given (4 doubles per path), when has_clip
     bool has_clip = false;
+    Scratch visit;                  // per-path visited pixel rows (int2) under the shipped row map, when has_visit
+    bool has_visit = false;
     bool has_hairline = false;      // some paths are hairline segments (RULE_HAIRLINE)
     // Page groups [plan[i], plan[i+1]) that rendered without running out of
     // scratch or cell capacity last time (with plan_wave_points); reused so a
@@ -370,7 +373,7 @@ void stage_end(rrb_ctx* c, int k) {
 
 void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
     Scratch* all[] = {&B->pts, &B->flags, &B->off, &B->rule, &B->gray, &B->alpha, &B->page, &B->geom, &B->pw, &B->ph,
-                      &B->mtx, &B->rgb, &B->clip, &B->clipf};
+                      &B->mtx, &B->rgb, &B->clip, &B->clipf, &B->visit};
     for (Scratch* s : all) {
         if (B->view && s != &B->off && s != &B->page && s != &B->geom) {
             s->p = nullptr;
@@ -386,7 +389,8 @@ void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
 // Upload a batch's inputs. rgb (host, 3 bytes per path) selects Rgb8 pages;
 // clip (host, 4 doubles per path) clips each path to a device-space rectangle.
 int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const uint8_t* rgb = nullptr,
-                 const double* clip = nullptr, bool hairlines = false, bool defer_points = false) {
+                 const double* clip = nullptr, bool hairlines = false, bool defer_points = false,
+                 const int32_t* visit = nullptr) {
     std::string msg;
     uint64_t tiles = 0;
     B->bpp = rgb ? 3 : 1;
@@ -450,6 +454,11 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
         }
         if ((rc = upload(c, B->clip, ci.data(), ci.size()))) return rc;
         if ((rc = upload(c, B->clipf, clip, 4 * h->n_paths))) return rc;
+        RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    B->has_visit = visit != nullptr && h->rowmap == RRB_ROWMAP_AS_SHIPPED;
+    if (B->has_visit) {
+        if ((rc = upload(c, B->visit, reinterpret_cast<const int2*>(visit), h->n_paths))) return rc;
         RRB_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     if (rgb) {
@@ -525,10 +534,15 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage_end(c, 0);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 1);
-    k_seg_count<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces), NPC,
-                                                                   as<double>(B->mtx), flat_sq,
-                                                                   as<uint32_t>(c->s_edge_off));
-    c->launches += 1;
+    // Curves of more than CURVE_BIG segments: listed here, counted by a warp each.
+    if ((rc = ensure(c, c->s_big, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
+    k_seg_count<true><<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
+        as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
+        as<uint32_t>(c->s_big), as<BatchCounters>(c->s_ctr));
+    k_seg_count_big<<<c->sm_count * 16, 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces),
+                                                            as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_big),
+                                                            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_edge_off));
+    c->launches += 2;
     stage_end(c, 1);
     RRB_CUDA(c, cudaGetLastError());
     stage(c, 2);
@@ -550,10 +564,14 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     RRB_CUDA(c, cudaMemsetAsync(gmin, 0x7f, n_egroups * sizeof(int32_t), c->stream));
     RRB_CUDA(c, cudaMemsetAsync(gmax, 0x80, n_egroups * sizeof(int32_t), c->stream));
     stage(c, 3);
-    k_seg_write<<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
+    k_seg_write<true><<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
         static_cast<uint32_t>(n_edges), as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo);
-    c->launches += 1;
+    k_seg_write_big<<<c->sm_count * 16, 128, 0, c->stream>>>(
+        as<double>(B->pts), as<uint2>(c->s_pieces), as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_big),
+        as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_edge_off), static_cast<uint32_t>(n_edges),
+        as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo);
+    c->launches += 2;
     stage_end(c, 3);
     const int chunk_rows = 32;
     stage(c, 4);
@@ -561,7 +579,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_edge_off), as<Edge>(c->s_edges), NP, as<uint8_t>(B->rule),
         as<uint8_t>(B->gray), as<uint8_t>(B->alpha), as<uint32_t>(B->page), as<uint32_t>(B->pw),
         as<uint32_t>(B->ph), rowmap, as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<uint32_t>(c->s_chunks),
-        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax, pclip);
+        chunk_rows, as<BatchCounters>(c->s_ctr), gmin, gmax, pclip, B->has_visit ? as<int2>(B->visit) : nullptr);
     c->launches += 1;
     // Hairline segments: their layers' PathInfo and run counts (before the
     // binning, which reads the layers' rectangles).
@@ -737,7 +755,9 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     }
     // ---- stage 4: composite
     stage(c, 11);
-    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 8),
+    // Persistent: as many CTAs as fit on the device at once (4 per SM), taking
+    // tiles from the work queue.
+    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 4),
                                as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
                                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
@@ -795,7 +815,7 @@ void set_binning(std::vector<PageGeom>& geom, uint64_t& supers_out) {
 void release_scratch(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
-                      &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
+                      &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip};
     for (Scratch* x : all) {
@@ -836,6 +856,8 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     W->row_shape = B->row_shape;
     if (B->has_clip) view(W->clip, B->clip, pb * sizeof(int4));
     if (B->has_clip) view(W->clipf, B->clipf, pb * 4 * sizeof(double));
+    W->has_visit = B->has_visit;
+    if (B->has_visit) view(W->visit, B->visit, pb * sizeof(int2));
     int rc;
     if ((rc = ensure(c, W->off, (W->n_paths + 1) * sizeof(uint64_t)))) return rc;
     if ((rc = ensure(c, W->page, std::max<uint64_t>(1, W->n_paths) * sizeof(uint32_t)))) return rc;
@@ -1005,6 +1027,8 @@ int make_path_wave(rrb_ctx* c, rrb_batch* B, uint32_t pa, uint32_t pb, uint64_t 
     view(W->ph, B->ph, pg0 * sizeof(uint32_t));
     view(W->mtx, B->mtx, 0);
     if (B->bpp == 3) view(W->rgb, B->rgb, pa * sizeof(uint32_t));
+    W->has_visit = B->has_visit;
+    if (B->has_visit) view(W->visit, B->visit, pa * sizeof(int2));
     if (B->has_clip) {
         view(W->clip, B->clip, pa * sizeof(int4));
         view(W->clipf, B->clipf, pa * 4 * sizeof(double));
@@ -1142,12 +1166,12 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
 // host_ns is the time from it to the first kernel.
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
               const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false, bool stream = true,
-              const std::chrono::steady_clock::time_point* t0 = nullptr) {
+              const std::chrono::steady_clock::time_point* t0 = nullptr, const int32_t* visit = nullptr) {
     const auto start = t0 ? *t0 : std::chrono::steady_clock::now();
     rrb_batch* B = c->tmp_batch;
     const bool streamed = stream && h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
                           page_locked(h->flags);
-    int rc = batch_upload(c, h, B, rgb, clip, hairlines, streamed);
+    int rc = batch_upload(c, h, B, rgb, clip, hairlines, streamed, visit);
     if (rc) return rc;
     const uint64_t host_ns = static_cast<uint64_t>(
         std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start).count());
@@ -1272,7 +1296,7 @@ int rrb_destroy(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pts, &c->s_flags, &c->s_off, &c->s_rule, &c->s_gray, &c->s_alpha, &c->s_page,
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
-                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list, &c->s_super_start,
+                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo};
@@ -1626,6 +1650,11 @@ int rrb_record_stroke_batch(rrb_ctx* c, const rrb_path_batch_params* p, const rr
 
 int rrb_record_path_batch_ex(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb,
                              const double* clip_rects) {
+    return rrb_record_path_batch_visit(c, p, path_rgb, clip_rects, nullptr);
+}
+
+int rrb_record_path_batch_visit(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb,
+                                const double* clip_rects, const int32_t* visit_rows) {
     if (!c || !p) return RRB_ERR_INVARIANT;
     if (!c->in_page) return set_err(c, RRB_ERR_STATE, "record_* outside begin_page/submit_page");
     if (!p->pages) return set_err(c, RRB_ERR_INVARIANT, "pages buffer is null");
@@ -1639,7 +1668,8 @@ int rrb_record_path_batch_ex(rrb_ctx* c, const rrb_path_batch_params* p, const u
     }
     static const uint8_t kNone[3] = {0, 0, 0};
     const uint8_t* rgb = path_rgb ? (p->n_paths ? path_rgb : kNone) : nullptr;
-    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, rgb, p->n_paths ? clip_rects : nullptr);
+    return run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, rgb, p->n_paths ? clip_rects : nullptr,
+                     false, true, nullptr, p->n_paths ? visit_rows : nullptr);
 }
 
 int rrb_record_path_batch_rgb(rrb_ctx* c, const rrb_path_batch_params* p, const uint8_t* path_rgb) {

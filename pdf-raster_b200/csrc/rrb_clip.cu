@@ -18,11 +18,23 @@
 // The lowering. Per clipped fill, the clip path's XPath segments (walked and
 // flattened here exactly as k_walk and k_seg_write do) become a polyline whose
 // points are divided by 4 (exact); the device's make_edge multiplies them back
-// by 4, so its edges are the clip scanner's segments. That polyline is filled
-// with the clip's rule and the fill's paint, clipped to the rectangle of the
-// clip's columns and the fill's pixel rows (the documented row map: one
-// render_aa_line per pixel row). A clip path that detect_rect (clip.rs:
-// 322-359) reduces to a rectangle becomes a rectangle clip of the fill itself.
+// by 4, so its edges are the clip scanner's segments and its AA rows are the
+// clip scanner's rows. That polyline is filled with the clip's rule and the
+// fill's paint, within the clip's columns. Which pixel rows it draws depends
+// on the row map:
+// - documented (one render_aa_line per pixel row y of the fill): the fill's
+//   pixel rows, each showing the clip scanner's rows 4y .. 4y+3; the lowered
+//   path is clipped to the fill's rows;
+// - as shipped (fill/mod.rs:176-203: the loop runs over the fill's AA rows
+//   and draws pixel row y = aa_y / 4 at aa_y % 4 == 3 after the clip scanner
+//   rendered "row" aa_y, i.e. its rows 16y+12 .. 16y+15): the rows y with
+//   4y+3 in the fill's scanner range, each showing the clip scanner's rows
+//   16y+12 .. 16y+15 inside that scanner's own range (the clip rectangle's
+//   rows when clip_to_path built it, clip.rs:152-171). The lowered path keeps
+//   those rows as its clip and gets the fill's visited rows as visit rows
+//   (rrb_record_path_batch_visit).
+// A clip path that detect_rect (clip.rs:322-359) reduces to a rectangle
+// becomes a rectangle clip of the fill itself.
 // Of a stack of clip paths the last one that is not a rectangle is drawn:
 // every scanner renders the same AA line in turn. The batch matrix must be
 // the identity, as the renderer's DEVICE_MATRIX is (page/mod.rs:177).
@@ -181,6 +193,9 @@ bool scanner_box(const std::vector<Seg>& segs, int32_t clip_lo, int32_t clip_hi,
     return y_min <= y_max;
 }
 
+// Visit rows meaning "the path's own" (rrb_record_path_batch_visit).
+constexpr int32_t kOwnRows = INT32_MIN;
+
 struct Out {
     double* pts;
     uint8_t* flags;
@@ -189,6 +204,7 @@ struct Out {
     uint64_t* src_path;
     uint8_t* rule;
     double* clip_rects;
+    int32_t* visit_rows;
     uint64_t paths_cap;
     uint64_t n_pts = 0, n_paths = 0;
 
@@ -200,7 +216,9 @@ struct Out {
         if (flags && n_pts < pts_cap) flags[n_pts] = f;
         ++n_pts;
     }
-    void path(uint64_t src, uint8_t r, const Rect& c, double y0, double y1, uint64_t first_pt) {
+    // visit v0 = kOwnRows: the path's own visited rows.
+    void path(uint64_t src, uint8_t r, const Rect& c, double y0, double y1, uint64_t first_pt,
+              int32_t v0 = kOwnRows, int32_t v1 = kOwnRows) {
         if (n_paths < paths_cap) {
             if (path_pt_off) path_pt_off[n_paths] = first_pt;
             if (src_path) src_path[n_paths] = src;
@@ -212,6 +230,10 @@ struct Out {
                 q[2] = c.x_max;
                 q[3] = y1;
             }
+            if (visit_rows) {
+                visit_rows[2 * n_paths] = v0;
+                visit_rows[2 * n_paths + 1] = v1;
+            }
         }
         ++n_paths;
     }
@@ -222,17 +244,19 @@ struct Out {
 extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double* clip_rects,
                                     const rrb_clip_path* clip_paths, double* out_pts, uint8_t* out_flags,
                                     uint64_t pts_cap, uint64_t* out_path_pt_off, uint64_t* out_src_path,
-                                    uint8_t* out_rule, double* out_clip_rects, uint64_t paths_cap,
-                                    uint64_t* n_pts_out, uint64_t* n_paths_out) {
+                                    uint8_t* out_rule, double* out_clip_rects, int32_t* out_visit_rows,
+                                    uint64_t paths_cap, uint64_t* n_pts_out, uint64_t* n_paths_out) {
     if (!p || !n_pts_out || !n_paths_out || (p->n_paths && (!p->path_pt_off || !p->fill_rule || !p->path_page)) ||
         (p->n_pts && (!p->pts || !p->flags)) || (p->n_pages && (!p->page_width || !p->page_height)))
         return RRB_ERR_INVARIANT;
     static const double kIdentity[6] = {1.0, 0.0, 0.0, 1.0, 0.0, 0.0};
     for (int k = 0; k < 6; ++k)
         if (!same_bits(p->matrix[k], kIdentity[k])) return RRB_ERR_INVARIANT;
-    if (p->rowmap != RRB_ROWMAP_DOCUMENTED) return RRB_ERR_INVARIANT;
+    if (p->rowmap > RRB_ROWMAP_AS_SHIPPED) return RRB_ERR_INVARIANT;
+    const bool shipped = p->rowmap == RRB_ROWMAP_AS_SHIPPED;
     const double flat_sq = rrb::dmul(p->flatness, p->flatness);
-    Out o{out_pts, out_flags, pts_cap, out_path_pt_off, out_src_path, out_rule, out_clip_rects, paths_cap};
+    Out o{out_pts, out_flags, pts_cap, out_path_pt_off, out_src_path, out_rule, out_clip_rects, out_visit_rows,
+          paths_cap};
     std::vector<Seg> segs;
     std::vector<size_t> starts;
     for (uint64_t i = 0; i < p->n_paths; ++i) {
@@ -251,6 +275,7 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
         // The stack in order: empty paths empty the clip, rectangles narrow it,
         // and the last other clip path is the one whose coverage is drawn.
         bool have_path = false, emptied = false, eo_last = false;
+        Rect c_scan = c;  // the clip rectangle when the drawn clip path's scanner was built
         segs.clear();
         starts.clear();
         int depth = 0;
@@ -273,6 +298,7 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
             starts.swap(est);
             eo_last = e->even_odd != 0;
             have_path = true;
+            c_scan = c;
         }
         // A clip with no integer column or row paints nothing (test_rect is
         // AllOutside, or the clamped span is empty). The device would read an
@@ -306,8 +332,13 @@ extern "C" int rrb_lower_clip_paths(const rrb_path_batch_params* p, const double
             for (size_t e = e0; e < e1; ++e)
                 o.point(rrb::dmul(segs[e].x1, 0.25), rrb::dmul(segs[e].y1, 0.25), e + 1 == e1 ? PF_LAST : 0);
         }
-        // Rows top..bottom of the fill's loop (clamped to the page by the device).
-        o.path(i, eo_last ? 1 : 0, c, static_cast<double>(top), static_cast<double>(bottom) + 1.0, first);
+        if (shipped) {
+            // The clip scanner's rows; the fill's visited pixel rows: 4y + 3 in [sy0, sy1].
+            o.path(i, eo_last ? 1 : 0, c, c_scan.y_min, c_scan.y_max, first, sy0 >> 2, floor_div(sy1 - 3, 4));
+        } else {
+            // Rows top..bottom of the fill's loop (clamped to the page by the device).
+            o.path(i, eo_last ? 1 : 0, c, static_cast<double>(top), static_cast<double>(bottom) + 1.0, first);
+        }
     }
     if (out_path_pt_off && o.n_paths < paths_cap) out_path_pt_off[o.n_paths] = o.n_pts;
     *n_pts_out = o.n_pts;

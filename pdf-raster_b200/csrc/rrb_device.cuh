@@ -195,6 +195,11 @@ __host__ __device__ __forceinline__ Edge make_edge(double x0, double y0, double 
     return e;
 }
 
+// Floor of a / b for b > 0.
+__host__ __device__ __forceinline__ int32_t floor_div(int32_t a, int32_t b) {
+    return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
 // Intersect entry of edge `e` on AA row r (row0 <= r <= row1): the closed form
 // of fill_intersections' stepping. The saturating accumulator
 // xx1_fp += dxdy_fp is monotone, so after k steps it equals the exact sum
@@ -253,56 +258,104 @@ __host__ __device__ __forceinline__ void edge_xrange(const Edge& e, int32_t& lo,
 __host__ __device__ __forceinline__ double midpoint_in_range(double a, double b) { return dmul(dadd(a, b), 0.5); }
 
 template <bool IN_RANGE, typename Emit>
-__host__ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
-                                                           double p2y, double p3x, double p3y, double flat_sq,
-                                                           Emit& emit);
+__host__ __device__ __forceinline__ int flatten_range_impl(double c0x, double c0y, double c1x, double c1y, double c2x,
+                                                           double c2y, double r3x, double r3y, int pp_lo, int pp_hi,
+                                                           double flat_sq, int limit, Emit& emit);
 
 // Every point the subdivision computes is a midpoint of two earlier points,
 // i.e. a convex combination of the four control points, so when all control
 // coordinates lie within +-f64::MAX/2 every midpoint call takes the (a+b)/2
 // branch: the check is made once per curve and the loop runs branch-free.
+__host__ __device__ __forceinline__ bool curve_in_range(double p0x, double p0y, double p1x, double p1y, double p2x,
+                                                        double p2y, double p3x, double p3y) {
+    const double HI = 8.98846567431157854e+307;
+    const double m = fmax(fmax(fmax(fabs(p0x), fabs(p0y)), fmax(fabs(p1x), fabs(p1y))),
+                          fmax(fmax(fabs(p2x), fabs(p2y)), fmax(fabs(p3x), fabs(p3y))));
+    return m <= HI;
+}
+
 template <typename Emit>
 __host__ __device__ __forceinline__ int flatten_curve(double p0x, double p0y, double p1x, double p1y, double p2x,
                                                       double p2y, double p3x, double p3y, double flat_sq,
                                                       Emit emit) {
-    const double HI = 8.98846567431157854e+307;
-    const double m = fmax(fmax(fmax(fabs(p0x), fabs(p0y)), fmax(fabs(p1x), fabs(p1y))),
-                          fmax(fmax(fabs(p2x), fabs(p2y)), fmax(fabs(p3x), fabs(p3y))));
-    if (m <= HI) return flatten_curve_impl<true>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, flat_sq, emit);
-    return flatten_curve_impl<false>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, flat_sq, emit);
+    if (curve_in_range(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y))
+        return flatten_range_impl<true>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, 0, MAX_CURVE_SPLITS, flat_sq, 0, emit);
+    return flatten_range_impl<false>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, 0, MAX_CURVE_SPLITS, flat_sq, 0, emit);
 }
 
-template <bool IN_RANGE, typename Emit>
-__host__ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0y, double p1x, double p1y, double p2x,
-                                                           double p2y, double p3x, double p3y, double flat_sq,
-                                                           Emit& emit) {
+// The segment count of a curve, or limit + 1 as soon as it exceeds limit.
+__host__ __device__ __forceinline__ int flatten_count_capped(double p0x, double p0y, double p1x, double p1y,
+                                                             double p2x, double p2y, double p3x, double p3y,
+                                                             double flat_sq, int limit) {
+    auto none = [](double, double) {};
+    if (curve_in_range(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y))
+        return flatten_range_impl<true>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, 0, MAX_CURVE_SPLITS, flat_sq, limit,
+                                        none);
+    return flatten_range_impl<false>(p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y, 0, MAX_CURVE_SPLITS, flat_sq, limit,
+                                     none);
+}
+
+// One node of the subdivision: the piece of the curve between two slots,
+// start point c0, control points c1, c2 and endpoint r3.
+struct CurveNode {
+    double c0x, c0y, c1x, c1y, c2x, c2y, r3x, r3y;
+};
+
+// flatten_curve's leaf test of a node: its chord midpoint against both
+// control points.
+template <bool IN_RANGE>
+__host__ __device__ __forceinline__ bool node_is_flat(const CurveNode& n, double flat_sq) {
     auto mid = [](double a, double b) { return IN_RANGE ? midpoint_in_range(a, b) : midpoint(a, b); };
+    const double mx = mid(n.c0x, n.r3x), my = mid(n.c0y, n.r3y);
+    const double dx1 = dsub(n.c1x, mx), dy1 = dsub(n.c1y, my);
+    const double dx2 = dsub(n.c2x, mx), dy2 = dsub(n.c2y, my);
+    const double d1 = dfma(dx1, dx1, dmul(dy1, dy1));
+    const double d2 = dfma(dx2, dx2, dmul(dy2, dy2));
+    return d1 <= flat_sq && d2 <= flat_sq;
+}
+
+// flatten_curve's split of a node into its two halves.
+template <bool IN_RANGE>
+__host__ __device__ __forceinline__ void node_split(const CurveNode& n, CurveNode& left, CurveNode& right) {
+    auto mid = [](double a, double b) { return IN_RANGE ? midpoint_in_range(a, b) : midpoint(a, b); };
+    const double xl1 = mid(n.c0x, n.c1x), yl1 = mid(n.c0y, n.c1y);
+    const double xh = mid(n.c1x, n.c2x), yh = mid(n.c1y, n.c2y);
+    const double xl2 = mid(xl1, xh), yl2 = mid(yl1, yh);
+    const double xr2 = mid(n.c2x, n.r3x), yr2 = mid(n.c2y, n.r3y);
+    const double xr1 = mid(xh, xr2), yr1 = mid(yh, yr2);
+    const double xr0 = mid(xl2, xr1), yr0 = mid(yl2, yr1);
+    left = CurveNode{n.c0x, n.c0y, xl1, yl1, xl2, yl2, xr0, yr0};
+    right = CurveNode{xr0, yr0, xr1, yr1, xr2, yr2, n.r3x, n.r3y};
+}
+
+// The subdivision restricted to the node over slots [pp_lo, pp_hi) with start
+// c0, controls c1, c2 and endpoint r3: emits the endpoint of every leaf in
+// order and returns their number (flatten_curve is the whole curve, slots
+// [0, 1024)). limit > 0: stops once more than limit leaves are found,
+// returning limit + 1.
+template <bool IN_RANGE, typename Emit>
+__host__ __device__ __forceinline__ int flatten_range_impl(double c0x, double c0y, double c1x, double c1y, double c2x,
+                                                           double c2y, double r3x, double r3y, int pp_lo, int pp_hi,
+                                                           double flat_sq, int limit, Emit& emit) {
     double sx[FLATTEN_STACK][6];
     int sidx[FLATTEN_STACK];
     int top = 0;
-    double c0x = p0x, c0y = p0y, c1x = p1x, c1y = p1y, c2x = p2x, c2y = p2y;
-    int pp1 = 0;
+    int pp1 = pp_lo;
     int count = 0;
-    while (pp1 < MAX_CURVE_SPLITS) {
+    while (pp1 < pp_hi) {
         int pp2;
-        double xr3, yr3;
+        CurveNode n;
         if (top > 0) {
             pp2 = sidx[top - 1];
-            xr3 = sx[top - 1][0];
-            yr3 = sx[top - 1][1];
+            n = CurveNode{c0x, c0y, c1x, c1y, c2x, c2y, sx[top - 1][0], sx[top - 1][1]};
         } else {
-            pp2 = MAX_CURVE_SPLITS;
-            xr3 = p3x;
-            yr3 = p3y;
+            pp2 = pp_hi;
+            n = CurveNode{c0x, c0y, c1x, c1y, c2x, c2y, r3x, r3y};
         }
-        double mx = mid(c0x, xr3), my = mid(c0y, yr3);
-        double dx1 = dsub(c1x, mx), dy1 = dsub(c1y, my);
-        double dx2 = dsub(c2x, mx), dy2 = dsub(c2y, my);
-        double d1 = dfma(dx1, dx1, dmul(dy1, dy1));
-        double d2 = dfma(dx2, dx2, dmul(dy2, dy2));
-        if (pp2 - pp1 == 1 || (d1 <= flat_sq && d2 <= flat_sq)) {
-            emit(xr3, yr3);
+        if (pp2 - pp1 == 1 || node_is_flat<IN_RANGE>(n, flat_sq)) {
+            emit(n.r3x, n.r3y);
             ++count;
+            if (limit > 0 && count > limit) return count;
             pp1 = pp2;
             if (top > 0) {
                 --top;
@@ -314,29 +367,79 @@ __host__ __device__ __forceinline__ int flatten_curve_impl(double p0x, double p0
                 c2y = sx[top][5];
             }
         } else {
-            double xl1 = mid(c0x, c1x), yl1 = mid(c0y, c1y);
-            double xh = mid(c1x, c2x), yh = mid(c1y, c2y);
-            double xl2 = mid(xl1, xh), yl2 = mid(yl1, yh);
-            double xr2 = mid(c2x, xr3), yr2 = mid(c2y, yr3);
-            double xr1 = mid(xh, xr2), yr1 = mid(yh, yr2);
-            double xr0 = mid(xl2, xr1), yr0 = mid(yl2, yr1);
-            int pp3 = (pp1 + pp2) >> 1;
+            CurveNode l, r;
+            node_split<IN_RANGE>(n, l, r);
+            const int pp3 = (pp1 + pp2) >> 1;
             // pp2 - pp1 >= 2 here, so fewer than FLATTEN_STACK halves are pending.
-            sx[top][0] = xr0;
-            sx[top][1] = yr0;
-            sx[top][2] = xr1;
-            sx[top][3] = yr1;
-            sx[top][4] = xr2;
-            sx[top][5] = yr2;
+            sx[top][0] = r.c0x;
+            sx[top][1] = r.c0y;
+            sx[top][2] = r.c1x;
+            sx[top][3] = r.c1y;
+            sx[top][4] = r.c2x;
+            sx[top][5] = r.c2y;
             sidx[top] = pp3;
             ++top;
-            c1x = xl1;
-            c1y = yl1;
-            c2x = xl2;
-            c2y = yl2;
+            c1x = l.c1x;
+            c1y = l.c1y;
+            c2x = l.c2x;
+            c2y = l.c2y;
         }
     }
     return count;
+}
+
+// A curve split among the 32 lanes of a warp: lane l takes the subtree of
+// slots [32 l, 32 l + 32), the node the sequential subdivision reaches after
+// five halvings. Each lane walks down from the root with node_is_flat and
+// node_split, so the node it reaches (and every point below it) is computed
+// by the same operations on the same values as in flatten_curve. If an
+// ancestor is a leaf, the lane whose subtree starts at that leaf's first slot
+// emits it (mode 1: the segment c0 -> r3 of `node`) and the others emit
+// nothing (mode 2); otherwise (mode 0) the lane flattens `node` over its
+// slots with flatten_range_impl. In lane order the leaves are the curve's
+// leaves in order.
+constexpr int CURVE_LANE_DEPTH = 5;
+constexpr int CURVE_LANE_SLOTS = MAX_CURVE_SPLITS >> CURVE_LANE_DEPTH;  // 32
+
+template <bool IN_RANGE>
+__host__ __device__ __forceinline__ int curve_lane_node(const CurveNode& root, int lane, double flat_sq,
+                                                        CurveNode& node) {
+    node = root;
+    int lo = 0, hi = MAX_CURVE_SPLITS;
+    const int target = lane * CURVE_LANE_SLOTS;
+    for (int d = 0; d < CURVE_LANE_DEPTH; ++d) {
+        if (node_is_flat<IN_RANGE>(node, flat_sq)) return target == lo ? 1 : 2;  // hi - lo >= 64 here
+        CurveNode l, r;
+        node_split<IN_RANGE>(node, l, r);
+        const int mid = (lo + hi) >> 1;
+        if (target < mid) {
+            node = l;
+            hi = mid;
+        } else {
+            node = r;
+            lo = mid;
+        }
+    }
+    return 0;
+}
+
+// The leaves of lane `lane` of a curve (see curve_lane_node): emits their
+// endpoints and returns their number; c0 receives the lane's first start point.
+template <bool IN_RANGE, typename Emit>
+__host__ __device__ __forceinline__ int curve_lane_flatten(const CurveNode& root, int lane, double flat_sq,
+                                                           double& c0x, double& c0y, Emit& emit) {
+    CurveNode n;
+    const int mode = curve_lane_node<IN_RANGE>(root, lane, flat_sq, n);
+    c0x = n.c0x;
+    c0y = n.c0y;
+    if (mode == 2) return 0;
+    if (mode == 1) {
+        emit(n.r3x, n.r3y);
+        return 1;
+    }
+    const int lo = lane * CURVE_LANE_SLOTS;
+    return flatten_range_impl<IN_RANGE>(n.c0x, n.c0y, n.c1x, n.c1y, n.c2x, n.c2y, n.r3x, n.r3y, lo,
+                                        lo + CURVE_LANE_SLOTS, flat_sq, 0, emit);
 }
 
 // div255 (crates/color/src/convert.rs:50-58).

@@ -67,7 +67,8 @@ struct BatchCounters {
     uint32_t scratch_cursor;
     uint32_t nonterminating;
     uint32_t ovf2_count;
-    uint32_t pad[2];
+    uint32_t tile_cursor;  // k_composite's work queue: the next tile to take
+    uint32_t big_curves;   // curves flattened by a warp each (k_seg_count's big_list)
     unsigned long long raw_entries;  // sum over edges of the rows they cover
     unsigned long long aa_rows;      // sum over paths of y1 - y0 + 1
     unsigned long long hl_rows;      // hairline segments: pixel rows drawn (one run and one cell each)
@@ -322,16 +323,28 @@ __device__ __forceinline__ void load_tpt(const double* pts, const double* m, uin
     transform(m, pts[2 * i], pts[2 * i + 1], x, y);
 }
 
-// Segments per piece slot.
+// Curves of more than this many segments are flattened by a warp each
+// (k_seg_count_big / k_seg_write_big): thread-per-curve work is that long.
+constexpr int CURVE_BIG = 32;
+
+// Segments per piece slot. SPLIT: a curve with more than CURVE_BIG segments
+// is counted 0 here and appended to big_list (big-curve count in
+// ctr->big_curves) for k_seg_count_big.
+template <bool SPLIT>
 __global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
-                            const double* __restrict__ mtx, double flat_sq, uint32_t* __restrict__ counts) {
+                            const double* __restrict__ mtx, double flat_sq, uint32_t* __restrict__ counts,
+                            uint32_t* __restrict__ big_list, BatchCounters* __restrict__ ctr) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
-    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
-        uint2 pc = pieces[s];
+    // Whole warps step together (blockDim is a multiple of 32), so the ballot
+    // below sees all 32 lanes.
+    for (uint32_t s0 = blockIdx.x * blockDim.x; s0 < n_slots; s0 += gridDim.x * blockDim.x) {
+        const uint32_t s = s0 + threadIdx.x;
+        const uint2 pc = s < n_slots ? pieces[s] : make_uint2(0u, 0u);
         uint32_t kind = pc.y >> 30;
         uint32_t c = 0;
+        bool big = false;
         if (kind == PK_LINE || kind == PK_CLOSE) {
             c = 1;
         } else if (kind == PK_CURVE) {
@@ -341,13 +354,68 @@ __global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restr
             load_tpt(pts, m, i, x1, y1);
             load_tpt(pts, m, i + 1, x2, y2);
             load_tpt(pts, m, i + 2, x3, y3);
-            c = flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [](double, double) {});
+            if (SPLIT) {
+                c = static_cast<uint32_t>(flatten_count_capped(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, CURVE_BIG));
+                big = c > static_cast<uint32_t>(CURVE_BIG);
+                if (big) c = 0;
+            } else {
+                c = flatten_curve(x0, y0, x1, y1, x2, y2, x3, y3, flat_sq, [](double, double) {});
+            }
         }
-        counts[s] = c;
+        if (s < n_slots) counts[s] = c;
+        if (SPLIT) {
+            const uint32_t bm = __ballot_sync(0xffffffffu, big);
+            if (bm) {
+                const int lead = __ffs(bm) - 1;
+                uint32_t base = 0;
+                if (static_cast<int>(threadIdx.x & 31) == lead) base = atomicAdd(&ctr->big_curves, __popc(bm));
+                base = __shfl_sync(0xffffffffu, base, lead);
+                if (big) big_list[base + __popc(bm & lanemask_lt())] = s;
+            }
+        }
     }
 }
 
-// Edge records per piece slot, at edge_off[slot].
+__device__ __forceinline__ CurveNode load_curve(const double* pts, const double* m, const uint2 pc) {
+    const uint32_t i = pc.y & 0x3fffffffu;
+    CurveNode r;
+    load_tpt(pts, m, pc.x, r.c0x, r.c0y);
+    load_tpt(pts, m, i, r.c1x, r.c1y);
+    load_tpt(pts, m, i + 1, r.c2x, r.c2y);
+    load_tpt(pts, m, i + 2, r.r3x, r.r3y);
+    return r;
+}
+
+__device__ __forceinline__ bool curve_root_in_range(const CurveNode& r) {
+    return curve_in_range(r.c0x, r.c0y, r.c1x, r.c1y, r.c2x, r.c2y, r.r3x, r.r3y);
+}
+
+// One warp per big curve (k_seg_count's big_list): each lane counts the
+// leaves of its subtree (curve_lane_flatten); the sum is the curve's count.
+__global__ void k_seg_count_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
+                                const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
+                                const BatchCounters* __restrict__ ctr, uint32_t* __restrict__ counts) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_big = ctr->big_curves;
+    const uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = warp_g; q < n_big; q += nwarps) {
+        const uint32_t s = big_list[q];
+        const CurveNode root = load_curve(pts, m, pieces[s]);
+        auto none = [](double, double) {};
+        double cx, cy;
+        int c = curve_root_in_range(root) ? curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, none)
+                                          : curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, none);
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) counts[s] = static_cast<uint32_t>(c);
+    }
+}
+
+// Edge records per piece slot, at edge_off[slot]. SPLIT: curves with more
+// than CURVE_BIG segments are left to k_seg_write_big.
+template <bool SPLIT>
 __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
                             uint32_t edge_cap, Edge* __restrict__ edges,
@@ -360,6 +428,7 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
         uint32_t kind = pc.y >> 30;
         if (kind == PK_NONE) continue;
         uint32_t base = edge_off[s];
+        if (SPLIT && kind == PK_CURVE && edge_off[s + 1] - base > static_cast<uint32_t>(CURVE_BIG)) continue;
         int32_t chi = static_cast<int32_t>(slot_clip_hi[s]);
         const int32_t clo = slot_clip_lo ? static_cast<int32_t>(slot_clip_lo[s]) : 0;
         uint32_t j = pc.y & 0x3fffffffu;
@@ -382,6 +451,50 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
                 cx = fx;
                 cy = fy;
             });
+        }
+    }
+}
+
+// One warp per big curve: each lane counts its subtree's leaves, an
+// exclusive scan over the lanes places them, and each lane writes the edge
+// records of its leaves from its subtree's start point on.
+__global__ void k_seg_write_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
+                                const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
+                                const BatchCounters* __restrict__ ctr, const uint32_t* __restrict__ edge_off,
+                                uint32_t edge_cap, Edge* __restrict__ edges,
+                                const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo) {
+    __shared__ double m[6];
+    if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t n_big = ctr->big_curves;
+    const uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t q = warp_g; q < n_big; q += nwarps) {
+        const uint32_t s = big_list[q];
+        const CurveNode root = load_curve(pts, m, pieces[s]);
+        const bool in_range = curve_root_in_range(root);
+        const int32_t chi = static_cast<int32_t>(slot_clip_hi[s]);
+        const int32_t clo = slot_clip_lo ? static_cast<int32_t>(slot_clip_lo[s]) : 0;
+        auto none = [](double, double) {};
+        double cx, cy;
+        const int mine = in_range ? curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, none)
+                                  : curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, none);
+        int incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        uint32_t k = edge_off[s] + static_cast<uint32_t>(incl - mine);
+        auto emit = [&](double fx, double fy) {
+            if (k < edge_cap) edges[k] = make_edge(cx, cy, fx, fy, clo, chi);
+            ++k;
+            cx = fx;
+            cy = fy;
+        };
+        if (mine) {
+            double sx0, sy0;
+            if (in_range) curve_lane_flatten<true>(root, lane, flat_sq, sx0, sy0, emit);
+            else curve_lane_flatten<false>(root, lane, flat_sq, sx0, sy0, emit);
         }
     }
 }
@@ -475,7 +588,9 @@ __global__ void k_scan_down(const uint32_t* __restrict__ in, uint32_t* __restric
 // ---------------------------------------------------------------------------
 // Path bounding box (XPathScanner::new, scanner/mod.rs:131-180): one warp per
 // path reduces its edges to the AA row range and AA column range, then maps
-// them to the pixel rectangle the row map can touch.
+// them to the pixel rectangle the row map can touch. path_visit (optional,
+// read under the as-shipped row map only) gives per path the pixel rows the
+// shipped driver loop visits when they come from another path's AA range.
 // ---------------------------------------------------------------------------
 __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
                             const Edge* __restrict__ edges, uint32_t n_paths, const uint8_t* __restrict__ rule,
@@ -484,7 +599,8 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                             const uint32_t* __restrict__ page_h, int rowmap, PathInfo* __restrict__ info,
                             uint32_t* __restrict__ path_groups, uint32_t* __restrict__ path_chunks,
                             int chunk_rows, BatchCounters* __restrict__ ctr, int32_t* __restrict__ gmin,
-                            int32_t* __restrict__ gmax, const int4* __restrict__ path_clip) {
+                            int32_t* __restrict__ gmax, const int4* __restrict__ path_clip,
+                            const int2* __restrict__ path_visit) {
     int lane = threadIdx.x & 31;
     uint32_t warp_g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -582,6 +698,13 @@ __global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32
                     pi.py0 = y0 >> 2;
                     int32_t t = y1 - 12;
                     pi.py1 = t >= 0 ? (t >> 4) : -1;
+                    // The shipped loop visits the pixel rows of another path's AA
+                    // range (a clip path drawn on its fill's rows): those rows,
+                    // up to the last one with content of this path.
+                    if (path_visit && path_visit[p].x != INT32_MIN) {  // INT32_MIN: the path's own rows
+                        pi.py0 = path_visit[p].x;
+                        pi.py1 = min(pi.py1, path_visit[p].y);
+                    }
                 }
                 pi.py0 = max(pi.py0, 0);
                 pi.py1 = min(pi.py1, H - 1);
@@ -1188,11 +1311,6 @@ __host__ __device__ __forceinline__ bool recti_box(const PathInfo& P, const Edge
         r1 = ev[b + 1] - 1;
     }
     return seen && s0 < s1;
-}
-
-// Floor of a / b for b > 0.
-__host__ __device__ __forceinline__ int32_t floor_div(int32_t a, int32_t b) {
-    return a >= 0 ? a / b : -((-a + b - 1) / b);
 }
 
 template <bool WRITE>
@@ -1866,7 +1984,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
     const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
-    const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, const BatchCounters* __restrict__ ctr,
+    const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, BatchCounters* __restrict__ ctr,
     const uint32_t* __restrict__ path_rgb, const uint32_t* __restrict__ super_start) {
     using L = CompLayout<TW>;
     constexpr int ITERS = TH / (L::NW * L::RPW);
@@ -1880,12 +1998,22 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     // be reading the one before it (one barrier per run).
     __shared__ uint8_t lut[2][RGB ? 768 : 256];
     __shared__ uint32_t red[L::NW];
+    __shared__ uint32_t next_tile;
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int col = (lane % L::LPR) * L::PX;
     int lut_sel = 0;
-    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    // Persistent CTAs take tiles from a work queue (ctr->tile_cursor, zeroed
+    // with the batch counters): a tile's cost ranges from nothing to
+    // thousands of layers, so tiles go to whichever CTA is free.
+    auto take = [&]() {
+        __syncthreads();  // every thread is done with the previous index
+        if (threadIdx.x == 0) next_tile = atomicAdd(&ctr->tile_cursor, 1u);
+        __syncthreads();
+        return next_tile;
+    };
+    for (uint32_t t = take(); t < n_tiles; t = take()) {
         const uint32_t pg = find_page_by(pages, n_pages, t, false);
         const PageGeom G = pages[pg];
         const uint32_t lt = t - G.tile_base;

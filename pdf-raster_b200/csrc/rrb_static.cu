@@ -277,7 +277,8 @@ int fill_static(rrb_ctx* c, const rrb_path_fill_params* p, unsigned char* base, 
     if (n_pieces == 0) return RRB_OK;
     k_compact_pieces<<<1, 32, 0, s>>>(hdr->off, hdr->path_pieces, 1, &hdr->page, &hdr->ph, slots, pieces, clip,
                                       nullptr, nullptr);
-    k_seg_count<<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off);
+    k_seg_count<false><<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off,
+                                                                nullptr, &hdr->ctr);
     if ((rc = scan_static(c, s, edge_off, n_pieces, hdr->block))) return rc;
     uint32_t n_edges = 0;
     if ((rc = read_u32(c, s, edge_off + n_pieces, n_edges))) return rc;
@@ -294,11 +295,11 @@ int fill_static(rrb_ctx* c, const rrb_path_fill_params* p, unsigned char* base, 
     const uint32_t groups = n_edges / 32 + 1;
     RRB_STATIC_CUDA(c, cudaMemsetAsync(gmin, 0x7f, groups * sizeof(int32_t), s));  // +inf rows
     RRB_STATIC_CUDA(c, cudaMemsetAsync(gmax, 0x80, groups * sizeof(int32_t), s));  // -inf rows
-    k_seg_write<<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off, n_edges,
+    k_seg_write<false><<<grid(n_pieces, 128, 32), 128, 0, s>>>(pts, pieces, n_pieces, hdr->mtx, flat_sq, edge_off, n_edges,
                                                          edges, clip, nullptr);
     k_path_bbox<<<1, 32, 0, s>>>(hdr->path_pieces, edge_off, edges, 1, &hdr->rule, &hdr->gray, &hdr->alpha,
                                  &hdr->page, &hdr->pw, &hdr->ph, p->rowmap, &hdr->info, hdr->rows, hdr->chunks, 32,
-                                 &hdr->ctr, gmin, gmax, nullptr);
+                                 &hdr->ctr, gmin, gmax, nullptr, nullptr);
     RRB_STATIC_CUDA(c, cudaGetLastError());
 
     // Rows -> cells, then the blend (skipped on the device if a limit was hit).

@@ -332,13 +332,22 @@ class B200Backend:
         self._chk(lib().rrb_record_path_batch_rgb(self._h, C.byref(params), _ptr(rgb, C.c_uint8)))
 
     def record_path_batch_ex(self, params: PathBatchParams, path_rgb: np.ndarray | None = None,
-                             clip_rects: np.ndarray | None = None):
-        """Gray or (path_rgb) Rgb8 pages; clip_rects [n_paths, 4] device-space (x0, y0, x1, y1) or None."""
+                             clip_rects: np.ndarray | None = None, visit_rows: np.ndarray | None = None):
+        """Gray or (path_rgb) Rgb8 pages; clip_rects [n_paths, 4] device-space (x0, y0, x1, y1) or None;
+        visit_rows [n_paths, 2] pixel rows the shipped row map's loop visits per path (INT32_MIN: its own),
+        or None (rrb_record_path_batch_visit)."""
         rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)
         clip = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
-        self._chk(lib().rrb_record_path_batch_ex(self._h, C.byref(params),
-                                                 None if rgb is None else _ptr(rgb, C.c_uint8),
-                                                 None if clip is None else _ptr(clip, C.c_double)))
+        if visit_rows is None:
+            self._chk(lib().rrb_record_path_batch_ex(self._h, C.byref(params),
+                                                     None if rgb is None else _ptr(rgb, C.c_uint8),
+                                                     None if clip is None else _ptr(clip, C.c_double)))
+            return
+        vis = np.ascontiguousarray(visit_rows, np.int32).reshape(-1)
+        self._chk(lib().rrb_record_path_batch_visit(self._h, C.byref(params),
+                                                    None if rgb is None else _ptr(rgb, C.c_uint8),
+                                                    None if clip is None else _ptr(clip, C.c_double),
+                                                    _ptr(vis, C.c_int32)))
 
     def record_path_batch_clip_paths(self, params: PathBatchParams, clip_paths, clip_rects: np.ndarray | None = None,
                                      path_rgb: np.ndarray | None = None):
@@ -359,7 +368,7 @@ class B200Backend:
                                rowmap=params.rowmap, keep=keep)
         lowered.pages = params.pages
         rgb = None if path_rgb is None else np.ascontiguousarray(path_rgb, np.uint8).reshape(-1, 3)[src]
-        self.record_path_batch_ex(lowered, rgb, low["clip_rects"])
+        self.record_path_batch_ex(lowered, rgb, low["clip_rects"], low["visit_rows"])
 
     def record_stroke_batch(self, params: PathBatchParams, strokes, path_rgb: np.ndarray | None = None,
                             clip_rects: np.ndarray | None = None):
@@ -565,8 +574,9 @@ def stroke_params(strokes, keep: list) -> "C.Array":
 def lower_clip_paths(params: PathBatchParams, clip_paths, clip_rects=None) -> dict:
     """rrb_lower_clip_paths (host): the batch with clip_paths[p] = None, (pts, flags, even_odd), or a list of
     them (a stack applied in order) per path and optional clip_rects [n_paths, 4], as a rectangle-clipped
-    batch: dict of pts [n, 2], flags, path_pt_off, fill_rule, src_path (the input path of each lowered path)
-    and clip_rects [m, 4]."""
+    batch: dict of pts [n, 2], flags, path_pt_off, fill_rule, src_path (the input path of each lowered path),
+    clip_rects [m, 4] and visit_rows [m, 2] (the pixel rows the shipped row map's loop visits; INT32_MIN: the
+    path's own)."""
     n = int(params.n_paths)
     keep = []
     cps = None
@@ -600,7 +610,7 @@ def lower_clip_paths(params: PathBatchParams, clip_paths, clip_rects=None) -> di
     rect = None if clip_rects is None else np.ascontiguousarray(clip_rects, np.float64).reshape(-1)
     rp = None if rect is None else _ptr(rect, C.c_double)
     npt, npa = C.c_uint64(), C.c_uint64()
-    rc = lib().rrb_lower_clip_paths(C.byref(params), rp, cps, None, None, 0, None, None, None, None, 0,
+    rc = lib().rrb_lower_clip_paths(C.byref(params), rp, cps, None, None, 0, None, None, None, None, None, 0,
                                     C.byref(npt), C.byref(npa))
     if rc:
         raise BackendError(rc, "rrb_lower_clip_paths")
@@ -611,13 +621,16 @@ def lower_clip_paths(params: PathBatchParams, clip_paths, clip_rects=None) -> di
     src = np.zeros(max(1, k), np.uint64)
     rule = np.zeros(max(1, k), np.uint8)
     rects = np.zeros(4 * max(1, k), np.float64)
+    visit = np.zeros(2 * max(1, k), np.int32)
     rc = lib().rrb_lower_clip_paths(C.byref(params), rp, cps, _ptr(pts, C.c_double), _ptr(fl, C.c_uint8), m,
                                     _ptr(off, C.c_uint64), _ptr(src, C.c_uint64), _ptr(rule, C.c_uint8),
-                                    _ptr(rects, C.c_double), k + 1, C.byref(npt), C.byref(npa))
+                                    _ptr(rects, C.c_double), _ptr(visit, C.c_int32), k + 1, C.byref(npt),
+                                    C.byref(npa))
     if rc:
         raise BackendError(rc, "rrb_lower_clip_paths")
     return dict(pts=pts[: 2 * m].reshape(m, 2), flags=fl[:m], path_pt_off=off, fill_rule=rule[:k],
-                src_path=src[:k].astype(np.int64), clip_rects=rects[: 4 * k].reshape(k, 4))
+                src_path=src[:k].astype(np.int64), clip_rects=rects[: 4 * k].reshape(k, 4),
+                visit_rows=visit[: 2 * k].reshape(k, 2))
 
 
 def stroke_outline(pts, flags, flatness: float = 0.1, **stroke):

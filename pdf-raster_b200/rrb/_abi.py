@@ -186,10 +186,12 @@ SIGNATURES = {
     "rrb_lower_clip_paths": (C.c_int, [C.POINTER(PathBatchParams), C.POINTER(C.c_double), C.POINTER(ClipPath),
                                        C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.c_uint64,
                                        C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint8),
-                                       C.POINTER(C.c_double), C.c_uint64, C.POINTER(C.c_uint64),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int32), C.c_uint64, C.POINTER(C.c_uint64),
                                        C.POINTER(C.c_uint64)]),
     "rrb_record_path_batch_ex": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8),
                                            C.POINTER(C.c_double)]),
+    "rrb_record_path_batch_visit": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8),
+                                              C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "rrb_record_path_batch_rgb": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(C.c_uint8)]),
     "rrb_record_stroke_batch": (C.c_int, [VP, C.POINTER(PathBatchParams), C.POINTER(StrokeParams),
                                           C.POINTER(C.c_uint8), C.POINTER(C.c_double)]),

@@ -88,6 +88,26 @@ extern "C" int rl_flatten_curve(const double* c, double flat_sq, double* out, in
     return n;
 }
 
+// A curve flattened the way k_seg_count_big / k_seg_write_big split it over
+// a warp: lanes 0..31 in turn (curve_lane_flatten), their leaves' endpoints
+// concatenated; starts[l] receives lane l's first start point and counts[l]
+// its number of leaves. Returns the total.
+extern "C" int rl_flatten_curve_lanes(const double* c, double flat_sq, double* out, int cap, double* starts,
+                                      int* counts) {
+    int n = 0;
+    const rrb::CurveNode root{c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]};
+    const bool in_range = rrb::curve_in_range(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7]);
+    for (int lane = 0; lane < 32; ++lane) {
+        PointsOut emit{out, cap, &n};
+        double sx, sy;
+        counts[lane] = in_range ? rrb::curve_lane_flatten<true>(root, lane, flat_sq, sx, sy, emit)
+                                : rrb::curve_lane_flatten<false>(root, lane, flat_sq, sx, sy, emit);
+        starts[2 * lane] = sx;
+        starts[2 * lane + 1] = sy;
+    }
+    return n;
+}
+
 // make_edge of each segment (x0, y0, x1, y1 in device space, as the walk
 // produces them) clipped to AA rows [clip_lo, clip_hi]: 8 int32 per edge.
 extern "C" void rl_make_edges(const double* segs, int n, int32_t clip_lo, int32_t clip_hi, int32_t* out) {

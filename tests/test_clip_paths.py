@@ -7,7 +7,10 @@ built without aa_scale, pdf_interp/src/renderer/page/mod.rs:1003-1009).
 
 CPU: the lowered batch rendered by the oracle's rectangle-clip renderer equals
 the oracle's literal clip-path fill (or_fill_path_clip_path), path after path
-on one page. GPU: the device's page for the same batch, through the C ABI.
+on one page (documented row map: the oracle's batch renderer has no visited-
+row override). GPU: the device's page for the same batch, through the C ABI,
+under both row maps — under the shipped one a clip path draws the clip
+scanner's rows 16y+12 .. 16y+15 on the pixel rows its fill's loop visits.
 """
 
 from types import SimpleNamespace
@@ -114,20 +117,21 @@ def _batch_stacks(rng, n_paths):
     return paths, rule, gray, alpha, np.array(rects, float), clips
 
 
-def _expected(oracle, paths, rule, gray, alpha, rects, clips):
+def _expected(oracle, paths, rule, gray, alpha, rects, clips, rowmap=0):
     page = np.full((H, W), 255, np.uint8)
     for i, (p, f) in enumerate(paths):
         r = rects[i]
         if isinstance(clips[i], list):
             oracle.fill_path_clip_paths(page, p, f, clips[i], eo=bool(rule[i]), gray=gray[i], alpha=alpha[i],
-                                        clip_rect=r)
+                                        clip_rect=r, rowmap=rowmap)
         elif clips[i] is not None:
             cp, cf, ceo = clips[i]
             oracle.fill_path_clip_path(page, p, f, cp, cf, clip_eo=ceo, eo=bool(rule[i]), gray=gray[i],
-                                       alpha=alpha[i], clip_rect=r)
+                                       alpha=alpha[i], clip_rect=r, rowmap=rowmap)
         else:
             flat = page.reshape(-1)
-            oracle.render_scene_ex(_Scene([(p, f)], [rule[i]], [gray[i]], [alpha[i]]), flat, clip=r.reshape(1, 4))
+            oracle.render_scene_ex(_Scene([(p, f)], [rule[i]], [gray[i]], [alpha[i]]), flat, clip=r.reshape(1, 4),
+                                   rowmap=rowmap)
     return page
 
 
@@ -171,7 +175,7 @@ def test_disjoint_rectangles_paint_nothing(oracle, rrb_lib):
     assert (page == 255).all()
 
 
-def test_lowering_needs_identity_and_documented_rows(rrb_lib):
+def test_lowering_needs_identity_and_a_known_row_map(rrb_lib):
     p, f = _poly([(1, 1), (20, 3), (9, 18)])
     keep = []
     params, _ = _params(rrb_lib, [(p, f)], [0], [0], [255], keep)
@@ -179,7 +183,7 @@ def test_lowering_needs_identity_and_documented_rows(rrb_lib):
     with pytest.raises(rrb_lib.BackendError):
         rrb_lib.lower_clip_paths(params, [(p, f, False)])
     params.matrix[0] = 1.0
-    params.rowmap = rrb_lib.RRB_ROWMAP_AS_SHIPPED
+    params.rowmap = 2
     with pytest.raises(rrb_lib.BackendError):
         rrb_lib.lower_clip_paths(params, [(p, f, False)])
     params.rowmap = rrb_lib.RRB_ROWMAP_DOCUMENTED
@@ -213,3 +217,57 @@ def test_clip_paths_on_the_device_match_oracle(backend, oracle, rrb_lib, seed):
     finally:
         backend.free_device(pages)
     assert np.array_equal(got.reshape(H, W), exp)
+
+
+def test_shipped_lowering_visits_the_fills_rows(oracle, rrb_lib):
+    """Under the shipped row map a lowered clip path keeps the clip scanner's
+    rows as its clip and gets the fill's visited rows: the pixel rows y whose
+    AA row 4y+3 lies in the fill's scanner range; paths without a clip path
+    keep their own rows (INT32_MIN)."""
+    rng = np.random.default_rng(5)
+    paths, rule, gray, alpha, rects, clips = _batch(rng, 12)
+    keep = []
+    params, s = _params(rrb_lib, paths, rule, gray, alpha, keep)
+    params.rowmap = rrb_lib.RRB_ROWMAP_AS_SHIPPED
+    low = rrb_lib.lower_clip_paths(params, clips, rects)
+    own = np.iinfo(np.int32).min
+    checked = 0
+    for k, i in enumerate(low["src_path"]):
+        v0, v1 = (int(v) for v in low["visit_rows"][k])
+        if i % 6 not in (2, 3, 4):  # no clip path, or a rectangle one (detect_rect)
+            assert v0 == own
+            continue
+        r = rects[i]
+        y_lo = int(np.floor(max(0.0, min(r[1], r[3]))))
+        y_hi = int(np.ceil(min(float(H), max(r[1], r[3])))) - 1
+        sc = oracle.Scanner(oracle.xpath_new(paths[i][0], paths[i][1], aa_scale=True), bool(rule[i]), 4 * y_lo,
+                            4 * (y_hi + 1) - 1)
+        b = sc.bounds()
+        assert v0 == b["y_min"] >> 2 and v1 == (b["y_max"] - 3) // 4, (i, v0, v1, b)
+        checked += 1
+    assert checked >= 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [0, 1, 10, 11])
+def test_clip_paths_on_the_device_match_oracle_as_shipped(backend, oracle, rrb_lib, seed):
+    rng = np.random.default_rng(seed)
+    paths, rule, gray, alpha, rects, clips = (_batch if seed < 10 else _batch_stacks)(rng, 18)
+    exp = _expected(oracle, paths, rule, gray, alpha, rects, clips, rowmap=1)
+    pages = backend.alloc_device(W * H)
+    keep = []
+    params, _ = _params(rrb_lib, paths, rule, gray, alpha, keep, pages)
+    params.rowmap = rrb_lib.RRB_ROWMAP_AS_SHIPPED
+    try:
+        backend.begin_page()
+        try:
+            backend.record_fill_buffer(pages, 255)
+            backend.record_path_batch_clip_paths(params, clips, rects)
+        finally:
+            backend.wait_page(backend.submit_page())
+        got = np.empty(W * H, np.uint8)
+        backend.wait_download(backend.download_async(pages, got))
+    finally:
+        backend.free_device(pages)
+    assert np.array_equal(got.reshape(H, W), exp)
+    assert (exp != 255).any()

@@ -42,6 +42,8 @@ def shim(tmp_path_factory):
     dp = C.POINTER(C.c_double)
     lib.rl_flatten_curve.argtypes = [dp, C.c_double, dp, C.c_int]
     lib.rl_flatten_curve.restype = C.c_int
+    lib.rl_flatten_curve_lanes.argtypes = [dp, C.c_double, dp, C.c_int, dp, C.POINTER(C.c_int)]
+    lib.rl_flatten_curve_lanes.restype = C.c_int
     lib.rl_make_edges.argtypes = [dp, C.c_int, C.c_int32, C.c_int32, i32p]
     lib.rl_make_edges.restype = None
     lib.rl_row_entries.argtypes = [i32p, C.c_int, C.c_int32, i32p]
@@ -213,6 +215,39 @@ def test_flatten_curve_matches_oracle(oracle, shim):
         want = oracle.flatten_curve(c[0:2], c[2:4], c[4:6], c[6:8], fsq)
         assert n == len(want), i
         assert np.array_equal(out[: 2 * n].view(np.uint64), np.ascontiguousarray(want).reshape(-1).view(np.uint64)), i
+
+
+def test_flatten_split_over_lanes_matches_oracle(oracle, shim):
+    """A curve split over the 32 lanes of a warp (the depth-5 subtrees of the
+    subdivision, how k_seg_count_big / k_seg_write_big flatten curves of more
+    than 32 segments) yields flatten_curve's points bit for bit, and each
+    lane's first start point is the previous lane's last endpoint (or the
+    curve's start)."""
+    rng = np.random.default_rng(17)
+    out = np.zeros(2 * 1025, np.float64)
+    starts = np.zeros(64, np.float64)
+    counts = (C.c_int * 32)()
+    seen_big = 0
+    for i in range(3000):
+        scale = [1e-3, 1.0, 40.0, 3000.0, 1e308, 1e5][i % 6]
+        c = np.clip(rng.normal(0, 1, 8), -1.5, 1.5) * scale
+        if i % 7 == 0:
+            c[2:4] = c[0:2]
+        if i % 13 == 0:
+            c[:] = c[0]
+        fsq = [0.01, 0.25, 1.0, 1e-6][i % 4]
+        n = shim.rl_flatten_curve_lanes(_dp(np.ascontiguousarray(c)), fsq, _dp(out), 1025, _dp(starts), counts)
+        want = np.ascontiguousarray(oracle.flatten_curve(c[0:2], c[2:4], c[4:6], c[6:8], fsq)).reshape(-1)
+        assert n == len(want) // 2, i
+        assert np.array_equal(out[: 2 * n].view(np.uint64), want.view(np.uint64)), i
+        k, prev = 0, c[0:2]
+        for lane in range(32):
+            if counts[lane]:
+                assert np.array_equal(starts[2 * lane: 2 * lane + 2].view(np.uint64), np.asarray(prev).view(np.uint64))
+                k += counts[lane]
+                prev = want[2 * k - 2: 2 * k]
+        seen_big += n > 32
+    assert seen_big > 300
 
 
 def _sat_inc(v):
