@@ -329,6 +329,12 @@ def run_rrb(args, rank, local, world):
         kw = dict(kw, n_paths=args.paths)
         desc += f" [reduced to {args.paths} paths]"
     full_scene = rrb.Scene(**kw)
+    if args.pages:
+        # A page range of a multi-page batch (profiling captures of a reduced case).
+        from rrb.shard import SceneShard
+        p0, p1 = (int(v) for v in args.pages.split(":"))
+        full_scene = SceneShard(full_scene, pages=(p0, p1))
+        desc += f" [pages {p0}:{p1} only]"
     # Several pages and several ranks: each rank renders its share of the
     # pages (strong scaling over the fixed batch); one page: replicas (weak).
     sharded = world > 1 and full_scene.n_pages > 1
@@ -858,6 +864,7 @@ def main():
     ap.add_argument("--ref-threads", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
+    ap.add_argument("--pages", default="", help="a:b, render only pages [a, b) of the batch (profiling runs)")
     ap.add_argument("--serving", action="store_true", help="Poisson request load against the server")
     ap.add_argument("--rates", default="50,200,1000,2000")
     ap.add_argument("--requests", type=int, default=128)

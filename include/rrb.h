@@ -163,7 +163,11 @@ int rrb_record_path_fill(rrb_ctx* ctx, const rrb_path_fill_params* p);
  * finished and concurrent callers run one after another. Like
  * rrb_record_path_fill it must come between rrb_begin_page and
  * rrb_submit_page, runs on the context's stream and has finished when it
- * returns. It does not update rrb_last_batch_stats. */
+ * returns: between its stages it waits on that stream to read sizes back
+ * from the device (up to four times per call). It does not update
+ * rrb_last_batch_stats. As every entry point, it makes the context's device
+ * current for the call and then restores the calling thread's current
+ * context (a thread that had none keeps the context's device current). */
 #define RRB_STATIC_SCRATCH_BYTES (32u << 20)
 #define RRB_STATIC_MAX_POINTS (1u << 16)
 #define RRB_STATIC_MAX_EDGES (1u << 18)

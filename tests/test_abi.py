@@ -213,6 +213,18 @@ def test_validation_rejects_short_page_buffer(rrb_lib):
     assert rc == 4 and "page buffer" in msg
 
 
+def test_validation_rejects_a_page_offset_that_would_wrap(rrb_lib):
+    """page_offset + page bytes computed in 64 bits must not wrap around and
+    pass: an offset of 2^64 - 11 is past any buffer."""
+    keep = []
+    p, n = _valid_batch(rrb_lib, keep)
+    off = np.array([np.iinfo(np.uint64).max - 10], np.uint64)
+    keep.append(off)
+    p.page_offset = off.ctypes.data_as(C.POINTER(C.c_uint64))
+    rc, msg = _validate(rrb_lib, p, n)
+    assert rc == 4 and "page buffer" in msg
+
+
 def test_no_device_fails_loudly(rrb_lib):
     """Without a CUDA device the backend raises; it never renders on the CPU."""
     try:

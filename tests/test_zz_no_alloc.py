@@ -1,6 +1,7 @@
 """rrb_record_path_fill_static through the C ABI: the same pixels as
-rrb_record_path_fill on consecutive calls, no device allocation, and the
-documented limits rejected with the page untouched.
+rrb_record_path_fill on consecutive calls and as the CPU oracle, no device
+allocation, and every documented limit (points, edges, crossings per AA row,
+coverage cells) rejected with the page untouched.
 
 Collected last on purpose: it must hold both in a fresh process (the first
 call sets up the static scratch array) and after every other test.
@@ -96,6 +97,19 @@ def test_static_fill_matches_record_path_fill_on_consecutive_calls(rrb_lib, page
     assert not np.array_equal(ref, init)
 
 
+def test_static_fill_matches_the_oracle(rrb_lib, oracle, pages):
+    """The static entry point against the CPU oracle directly: every case
+    composited in order onto a fresh copy of the same initial page."""
+    be, _, b, init = pages
+    be.upload_async(b, init)
+    exp = init.copy().reshape(H, W)
+    for name, pts, fl, rule, gray, alpha, rowmap in _cases(rrb_lib):
+        got = _render(be, b, be.record_path_fill_static, pts, fl, rule, gray, alpha, rowmap)
+        oracle.fill_path(exp, pts, fl, eo=bool(rule), gray=gray, alpha=alpha, rowmap=rowmap)
+        d = np.nonzero(got != exp.reshape(-1))[0]
+        assert d.size == 0, f"{name}: {d.size} pixels differ from the oracle, first at {d[:5]}"
+
+
 def test_static_fill_twice_in_a_row_matches(rrb_lib, pages):
     be, a, b, _ = pages
     name, pts, fl, rule, gray, alpha, rowmap = _cases(rrb_lib)[0]
@@ -142,6 +156,59 @@ def test_static_fill_limits_leave_the_page_untouched(rrb_lib, pages):
     # The entry point still works after a rejection.
     name, pts, fl, rule, gray, alpha, rowmap = _cases(rrb_lib)[1]
     _render(be, b, be.record_path_fill_static, pts, fl, rule, gray, alpha, rowmap)
+
+
+def test_static_fill_edge_limit_leaves_the_page_untouched(rrb_lib, pages):
+    """A path of 300 huge cubics flattens to 1,024 edges each, past
+    RRB_STATIC_MAX_EDGES (262,144): rejected after the count, page untouched."""
+    be, _, b, _ = pages
+    before = np.empty(W * H, np.uint8)
+    be.wait_download(be.download_async(b, before))
+    ops = [("move_to", 10.0, 10.0)]
+    for k in range(300):
+        s = 1e6 * (1 + (k % 3))
+        ops.append(("curve_to", -s, s, s, -s, 10.0 + k % 7, 10.0 + k % 5))
+    ops.append(("close",))
+    pts, fl = _builder_path(rrb_lib, ops)
+    with pytest.raises(rrb_lib.BackendError) as e:
+        _render(be, b, be.record_path_fill_static, pts, fl, 0, 0, 255, 0)
+    assert e.value.status == 3 and "edges" in str(e.value)
+    after = np.empty(W * H, np.uint8)
+    be.wait_download(be.download_async(b, after))
+    assert np.array_equal(before, after)
+
+
+def test_static_fill_cell_limit_leaves_the_page_untouched(rrb_lib, pages):
+    """A comb of 60 teeth (122 merged crossings per AA row, under the row
+    limit) on a page 20,000 rows tall needs more coverage cells than
+    RRB_STATIC_MAX_CELLS: found on the device, the blend is skipped, the page
+    keeps its bytes and the call reports the cell limit."""
+    be = pages[0]
+    w2, h2 = W, 20000
+    ops = [("move_to", 2.0, 2.0)]
+    x = 2.0
+    for _ in range(60):
+        ops += [("line_to", x + 0.7, 2.0), ("line_to", x + 0.7, h2 - 8.0), ("line_to", x + 1.3, h2 - 8.0),
+                ("line_to", x + 1.3, 2.0)]
+        x += 1.45
+    ops += [("line_to", x, 2.0), ("line_to", x, h2 - 2.0), ("line_to", 2.0, h2 - 2.0), ("close",)]
+    pts, fl = _builder_path(rrb_lib, ops)
+    buf = be.alloc_device(w2 * h2)
+    try:
+        init = np.random.default_rng(8).integers(0, 256, w2 * h2, dtype=np.uint8)
+        be.upload_async(buf, init)
+        be.begin_page()
+        try:
+            with pytest.raises(rrb_lib.BackendError) as e:
+                be.record_path_fill_static(pts, fl, buf, w2, h2, fill_rule=1, gray=0, alpha=255, rowmap=0)
+        finally:
+            be.wait_page(be.submit_page())
+        assert e.value.status == 3 and "coverage cells" in str(e.value)
+        after = np.empty(w2 * h2, np.uint8)
+        be.wait_download(be.download_async(buf, after))
+        assert np.array_equal(init, after)
+    finally:
+        be.free_device(buf)
 
 
 def test_static_fill_outside_a_page_is_a_state_error(rrb_lib, pages):
