@@ -1,6 +1,6 @@
 """Extract the aa_fill sample offsets from the reference source as a fixture.
 
-    python tests/golden/make_jitter.py [path/to/reference]
+    python tests/golden/make_jitter.py path/to/reference
 
 Reads the HALTON2 / HALTON3 tables of crates/gpu/src/fill.rs (the jitter of
 the reference's aa_fill operator) as text and writes aa_fill_jitter.json:
@@ -26,7 +26,9 @@ def table(src: str, name: str) -> list[str]:
 
 
 def main():
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_jitter.py path/to/reference (the rasterrocket source tree)")
+    ref = Path(sys.argv[1])
     src = (ref / "crates/gpu/src/fill.rs").read_text()
     out = {"source": "crates/gpu/src/fill.rs HALTON2 / HALTON3", "x": table(src, "HALTON2"),
            "y": table(src, "HALTON3")}
