@@ -180,11 +180,11 @@ def test_static_fill_edge_limit_leaves_the_page_untouched(rrb_lib, pages):
 
 def test_static_fill_cell_limit_leaves_the_page_untouched(rrb_lib, pages):
     """A comb of 60 teeth (122 merged crossings per AA row, under the row
-    limit) on a page 20,000 rows tall needs more coverage cells than
+    limit) on a page 60,000 rows tall needs more coverage cells than
     RRB_STATIC_MAX_CELLS: found on the device, the blend is skipped, the page
     keeps its bytes and the call reports the cell limit."""
     be = pages[0]
-    w2, h2 = W, 20000
+    w2, h2 = W, 60000  # about 120 cells per pixel row: some 7 M cells
     ops = [("move_to", 2.0, 2.0)]
     x = 2.0
     for _ in range(60):
