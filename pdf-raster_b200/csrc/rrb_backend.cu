@@ -74,6 +74,16 @@ struct rrb_ctx {
     uint32_t* h_read = nullptr;  // pinned readback area
     uint64_t launches = 0;
     uint64_t host_syncs = 0;  // stream waits for device-side sizes in the current run_resident_one
+    // Replays with cached sizes: each wave's counters are copied here (page-
+    // locked, one slot per wave) and read after the render's one wait.
+    rrb::BatchCounters* h_waves = nullptr;
+    uint32_t h_waves_cap = 0;
+    bool deferred = false;  // the last run_resident_one left its counters in h_waves
+    // Page-locked staging of the page geometry of a render's waves (wave i at
+    // its first page): a copy from pageable memory would wait on the stream.
+    rrb::PageGeom* h_geom = nullptr;
+    uint32_t h_geom_cap = 0;
+    uint32_t geom_slot = 0;  // where the next run_resident_one stages its geometry
     uint64_t scratch_grows = 0;  // ensure() reallocations since the last record call began
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
     struct rrb_batch* wave_batch = nullptr; // view of a group of pages of a larger batch
@@ -303,6 +313,23 @@ void set_tiles(std::vector<PageGeom>& geom, uint32_t tw, uint32_t th, uint64_t& 
 
 }  // namespace
 
+// The sizes one render of a wave found on the device between its stages. A
+// resident batch renders the same inputs every time, so a later render of
+// the same wave with the same tile shape, row-stage shape and row map finds
+// the same sizes: it takes them from here and launches every stage without
+// waiting on the stream.
+struct WaveSizes {
+    bool valid = false;
+    uint32_t tw = 0, th = 0;
+    uint8_t row_shape = 0;
+    int rowmap = -1;
+    uint64_t n_pieces = 0, n_edges = 0, n_groups = 0, n_chunks = 0, n_pairs = 0, n_runs = 0;
+    uint64_t raw_entries = 0, hl_rows = 0, mid = 0, slow = 0, slow_need = 0;
+    bool matches(uint32_t w, uint32_t h, uint8_t rs, int rm) const {
+        return valid && tw == w && th == h && row_shape == rs && rowmap == rm;
+    }
+};
+
 // A batch whose inputs live in device memory: uploaded once, rendered any
 // number of times (the serving loop keeps these resident).
 struct rrb_batch {
@@ -320,6 +347,8 @@ struct rrb_batch {
     // resident batch does not fail and split on every render.
     std::vector<uint32_t> plan;
     uint64_t plan_wave_points = 0;
+    // Per wave of `plan`: the sizes its last render found on the device.
+    std::vector<WaveSizes> sizes;
     // Row-stage shape (0: 12 entries x 8 warps, 1: 16 entries x 4 warps). A
     // resident batch renders once with each (renders that grew scratch do not
     // count) and keeps the faster.
@@ -345,11 +374,16 @@ constexpr int kStages = sizeof(kStageNames) / sizeof(kStageNames[0]);
 
 }  // namespace
 
+// Events of up to kTimedWaves waves of one render: a render whose waves do
+// not wait on the stream (a replay with cached sizes) reads them all after
+// its one synchronisation.
+constexpr int kTimedWaves = 64;
 struct StageTimer {
     bool on = false;
-    cudaEvent_t begin[kStages] = {}, end[kStages] = {};
-    bool used[kStages] = {};
-    uint32_t launches[kStages] = {};
+    int slot = 0;  // the wave whose events are being recorded
+    cudaEvent_t begin[kTimedWaves][kStages] = {}, end[kTimedWaves][kStages] = {};
+    bool used[kTimedWaves][kStages] = {};
+    uint32_t launches[kTimedWaves][kStages] = {};
     uint64_t launch_mark = 0;
 };
 
@@ -359,16 +393,16 @@ namespace {
 void stage(rrb_ctx* c, int k) {
     StageTimer* t = c->timer;
     if (!t || !t->on || k >= kStages) return;
-    cudaEventRecord(t->begin[k], c->stream);
-    t->used[k] = true;
+    cudaEventRecord(t->begin[t->slot][k], c->stream);
+    t->used[t->slot][k] = true;
     t->launch_mark = c->launches;
 }
 
 void stage_end(rrb_ctx* c, int k) {
     StageTimer* t = c->timer;
     if (!t || !t->on || k >= kStages) return;
-    cudaEventRecord(t->end[k], c->stream);
-    t->launches[k] = static_cast<uint32_t>(c->launches - t->launch_mark);
+    cudaEventRecord(t->end[t->slot][k], c->stream);
+    t->launches[t->slot][k] = static_cast<uint32_t>(c->launches - t->launch_mark);
 }
 
 void free_batch_bufs(rrb_ctx* c, rrb_batch* B) {
@@ -397,6 +431,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     int v = validate_batch(h, SIZE_MAX, 64, 16, B->geom_h, tiles, B->supers, msg, B->bpp,
                            hairlines ? RULE_HAIRLINE : 1);
     if (v) return set_err(c, v, msg);
+    B->sizes.clear();  // new inputs: no render has seen their sizes
     B->n_paths = h->n_paths;
     B->n_pts = h->n_pts;
     B->n_pages = h->n_pages;
@@ -473,13 +508,20 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
 }
 
 // The pipeline over a device-resident batch into the device page arena.
-int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
+// ws: the wave's cached sizes (see WaveSizes), or nullptr. When they match,
+// every stage is launched without waiting on the stream, and the counters
+// are copied into the page-locked slot c->h_waves[slot] for the caller to
+// read after its one wait (c->deferred is set); otherwise the sizes are read
+// back between the stages and, if ws is given, stored there.
+int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap,
+                     WaveSizes* ws = nullptr, uint32_t slot = 0) {
     c->launches = 0;
     c->host_syncs = 0;
+    c->deferred = false;
     std::memset(&c->stats, 0, sizeof c->stats);
     std::memset(c->stage_ms, 0, sizeof c->stage_ms);
     std::memset(c->stage_launches, 0, sizeof c->stage_launches);
-    if (c->timer) std::memset(c->timer->used, 0, sizeof c->timer->used);
+    if (c->timer) std::memset(c->timer->used[c->timer->slot], 0, sizeof c->timer->used[0]);
     if (B->n_paths == 0) return RRB_OK;
     if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
     if (rowmap < 0 || rowmap > 1) return set_err(c, RRB_ERR_INVARIANT, "rowmap must be 0 or 1");
@@ -488,14 +530,21 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     uint64_t tiles = 0;
     set_tiles(B->geom_h, tw, th, tiles);
     if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
+    const bool cached = ws && ws->matches(tw, th, B->row_shape, rowmap) && slot < c->h_waves_cap;
     const uint64_t n_paths = B->n_paths, n_pts = B->n_pts, supers = B->supers;
     const uint32_t n_pages = B->n_pages;
     const uint32_t NP = static_cast<uint32_t>(n_paths);
     const double flat_sq = B->flat_sq;
     const int4* pclip = B->has_clip ? as<int4>(B->clip) : nullptr;
     int rc;
-    RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
-                                c->stream));
+    if (cached && c->h_geom && c->geom_slot + n_pages <= c->h_geom_cap) {
+        PageGeom* st = c->h_geom + c->geom_slot;
+        std::memcpy(st, B->geom_h.data(), n_pages * sizeof(PageGeom));
+        RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, st, n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice, c->stream));
+    } else {
+        RRB_CUDA(c, cudaMemcpyAsync(B->geom.p, B->geom_h.data(), n_pages * sizeof(PageGeom), cudaMemcpyHostToDevice,
+                                    c->stream));
+    }
     // ---- stage 1: walk, compact pieces, flatten counts, edge offsets
     if ((rc = ensure(c, c->s_slots, n_pts * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_path_pieces, (n_paths + 1) * sizeof(uint32_t)))) return rc;
@@ -519,8 +568,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     c->launches += 1;
     RRB_CUDA(c, cudaGetLastError());
     if ((rc = scan_u32(c, as<uint32_t>(c->s_path_pieces), as<uint32_t>(c->s_path_pieces), NP))) return rc;
-    if ((rc = read_back(c, as<uint32_t>(c->s_path_pieces) + NP, sizeof(uint32_t)))) return rc;
-    const uint64_t n_pieces = c->h_read[0];
+    if (!cached && (rc = read_back(c, as<uint32_t>(c->s_path_pieces) + NP, sizeof(uint32_t)))) return rc;
+    const uint64_t n_pieces = cached ? ws->n_pieces : c->h_read[0];
     const uint32_t NPC = static_cast<uint32_t>(n_pieces);
     if ((rc = ensure(c, c->s_pieces, std::max<uint64_t>(1, n_pieces) * sizeof(uint2)))) return rc;
     if ((rc = ensure(c, c->s_clip, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
@@ -548,8 +597,8 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage(c, 2);
     if ((rc = scan_u32(c, as<uint32_t>(c->s_edge_off), as<uint32_t>(c->s_edge_off), NPC))) return rc;
     stage_end(c, 2);
-    if ((rc = read_back(c, as<uint32_t>(c->s_edge_off) + NPC, sizeof(uint32_t)))) return rc;
-    const uint64_t n_edges = c->h_read[0];
+    if (!cached && (rc = read_back(c, as<uint32_t>(c->s_edge_off) + NPC, sizeof(uint32_t)))) return rc;
+    const uint64_t n_edges = cached ? ws->n_edges : c->h_read[0];
     // ---- stage 2: edges, path boxes, row/chunk offsets, supertile bins
     if ((rc = ensure(c, c->s_edges, std::max<uint64_t>(1, n_edges) * sizeof(Edge)))) return rc;
     if ((rc = ensure(c, c->s_info, n_paths * sizeof(PathInfo)))) return rc;
@@ -617,23 +666,36 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     RRB_CUDA(c, cudaGetLastError());
     if ((rc = scan_u32(c, as<uint32_t>(c->s_run_off), as<uint32_t>(c->s_run_off), NP))) return rc;
     stage_end(c, 7);
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 0, as<uint32_t>(c->s_rows) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 1, as<uint32_t>(c->s_chunks) + NP, 4, cudaMemcpyDeviceToHost, c->stream));
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 2, as<uint32_t>(c->s_super_cnt) + NSUP, 4, cudaMemcpyDeviceToHost,
-                                c->stream));
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 4, &as<BatchCounters>(c->s_ctr)->raw_entries, 8, cudaMemcpyDeviceToHost,
-                                c->stream));
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 6, as<uint32_t>(c->s_run_off) + NP, 4, cudaMemcpyDeviceToHost,
-                                c->stream));
-    RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 8, &as<BatchCounters>(c->s_ctr)->hl_rows, 8, cudaMemcpyDeviceToHost,
-                                c->stream));
-    ++c->host_syncs;
-    RRB_CUDA(c, cudaStreamSynchronize(c->stream));
-    const uint64_t n_groups = c->h_read[0], n_chunks = c->h_read[1], n_pairs = c->h_read[2];
-    const uint64_t n_runs = c->h_read[6];
-    uint64_t raw_entries, hl_rows;
-    std::memcpy(&raw_entries, c->h_read + 4, 8);
-    std::memcpy(&hl_rows, c->h_read + 8, 8);
+    uint64_t n_groups, n_chunks, n_pairs, n_runs, raw_entries, hl_rows;
+    if (cached) {
+        n_groups = ws->n_groups;
+        n_chunks = ws->n_chunks;
+        n_pairs = ws->n_pairs;
+        n_runs = ws->n_runs;
+        raw_entries = ws->raw_entries;
+        hl_rows = ws->hl_rows;
+    } else {
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 0, as<uint32_t>(c->s_rows) + NP, 4, cudaMemcpyDeviceToHost,
+                                    c->stream));
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 1, as<uint32_t>(c->s_chunks) + NP, 4, cudaMemcpyDeviceToHost,
+                                    c->stream));
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 2, as<uint32_t>(c->s_super_cnt) + NSUP, 4, cudaMemcpyDeviceToHost,
+                                    c->stream));
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 4, &as<BatchCounters>(c->s_ctr)->raw_entries, 8,
+                                    cudaMemcpyDeviceToHost, c->stream));
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 6, as<uint32_t>(c->s_run_off) + NP, 4, cudaMemcpyDeviceToHost,
+                                    c->stream));
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_read + 8, &as<BatchCounters>(c->s_ctr)->hl_rows, 8, cudaMemcpyDeviceToHost,
+                                    c->stream));
+        ++c->host_syncs;
+        RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        n_groups = c->h_read[0];
+        n_chunks = c->h_read[1];
+        n_pairs = c->h_read[2];
+        n_runs = c->h_read[6];
+        std::memcpy(&raw_entries, c->h_read + 4, 8);
+        std::memcpy(&hl_rows, c->h_read + 8, 8);
+    }
     // The run offsets were scanned in 32 bits: refuse totals that could wrap.
     if (hl_rows > 0x7FFFFFFFull || n_runs > 0x7FFFFFFFull)
         return set_err(c, RRB_ERR_POOL_EXHAUSTED, "batch needs more than 2^31 row runs");
@@ -703,11 +765,15 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     RRB_CUDA(c, cudaGetLastError());
     // Overflowing pixel rows, if any: the warp-per-row middle path, then the
     // sequential path for rows longer than its shared lists.
-    if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
     BatchCounters hc;
-    std::memcpy(&hc, c->h_read, sizeof hc);
+    std::memset(&hc, 0, sizeof hc);
+    if (!cached) {
+        if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+        std::memcpy(&hc, c->h_read, sizeof hc);
+    }
     const uint32_t ovf_cap = static_cast<uint32_t>(std::max<uint64_t>(1, n_groups));
-    const uint64_t mid = std::min<uint64_t>(hc.ovf_count, n_groups);
+    const uint64_t mid = cached ? ws->mid : std::min<uint64_t>(hc.ovf_count, n_groups);
+    uint64_t slow = 0, slow_need = 0;
     if (mid) {
         if ((rc = ensure(c, c->s_ovf2, std::max<uint64_t>(1, n_groups) * sizeof(uint2)))) return rc;
         stage(c, 10);
@@ -717,10 +783,25 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
             static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf2), as<BatchCounters>(c->s_ctr), pclip);
         c->launches += 1;
         RRB_CUDA(c, cudaGetLastError());
-        if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
-        std::memcpy(&hc, c->h_read, sizeof hc);
-        const uint64_t slow = std::min<uint64_t>(hc.ovf2_count, n_groups);
-        if (slow) {
+        if (!cached) {
+            if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
+            std::memcpy(&hc, c->h_read, sizeof hc);
+        }
+        slow = cached ? ws->slow : std::min<uint64_t>(hc.ovf2_count, n_groups);
+        if (slow && cached) {
+            // The scratch the last render settled on; the cursors are where the
+            // faster paths left them on the device.
+            slow_need = ws->slow_need;
+            if ((rc = ensure(c, c->s_scratch, slow_need * sizeof(int3)))) return rc;
+            k_groups_slow<<<grid_for(c, slow * 32, SLOW_WARPS * 32, 16), SLOW_WARPS * 32, 0, c->stream>>>(
+                as<PathInfo>(c->s_info), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges), gmin, gmax,
+                as<uint32_t>(B->pw), as<uint2>(c->s_ovf2), ovf_cap, as<int3>(c->s_scratch),
+                static_cast<uint32_t>(std::min<uint64_t>(c->s_scratch.cap / sizeof(int3), 0xFFFFFFFFull)),
+                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), static_cast<uint32_t>(cell_cap),
+                as<BatchCounters>(c->s_ctr), pclip);
+            c->launches += 1;
+            RRB_CUDA(c, cudaGetLastError());
+        } else if (slow) {
             uint64_t need = std::min<uint64_t>(slow * 4096 + 4 * n_edges, 0x7FFFFFFFull);
             // Every attempt re-runs all slow rows, so it restarts the cell
             // allocation where the faster paths left it.
@@ -743,6 +824,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                 RRB_CUDA(c, cudaGetLastError());
                 if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
                 std::memcpy(&hc, c->h_read, sizeof hc);
+                slow_need = need;
                 if (!(hc.err & ERR_SCRATCH_CAP)) break;
                 // Not enough scratch: grow to what was asked for and run again.
                 need = std::min<uint64_t>(static_cast<uint64_t>(hc.scratch_cursor) + 4 * n_edges, 0x7FFFFFFFull);
@@ -765,8 +847,42 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                                n_runs > 0, as<uint32_t>(c->s_super_start))))
         return rc;
     stage_end(c, 11);
+    c->stats.paths = n_paths;
+    c->stats.pieces = n_pieces;
+    c->stats.segments = n_edges;
+    c->stats.tiles = tiles;
+    c->stats.tile_pairs = n_pairs;
+    c->stats.kernel_launches = c->launches;
+    c->stats.row_groups = n_groups;
+    if (cached) {
+        // The counters go to this wave's page-locked slot; the caller reads
+        // them (and the stage events) after its one wait on the stream.
+        RRB_CUDA(c, cudaMemcpyAsync(c->h_waves + slot, c->s_ctr.p, sizeof(BatchCounters), cudaMemcpyDeviceToHost,
+                                    c->stream));
+        c->deferred = true;
+        c->stats.host_syncs = c->host_syncs;
+        return RRB_OK;
+    }
     if ((rc = read_back(c, as<BatchCounters>(c->s_ctr), sizeof(BatchCounters)))) return rc;
     std::memcpy(&hc, c->h_read, sizeof hc);
+    if (ws && !hc.err) {
+        ws->valid = true;
+        ws->tw = tw;
+        ws->th = th;
+        ws->row_shape = B->row_shape;
+        ws->rowmap = rowmap;
+        ws->n_pieces = n_pieces;
+        ws->n_edges = n_edges;
+        ws->n_groups = n_groups;
+        ws->n_chunks = n_chunks;
+        ws->n_pairs = n_pairs;
+        ws->n_runs = n_runs;
+        ws->raw_entries = raw_entries;
+        ws->hl_rows = hl_rows;
+        ws->mid = mid;
+        ws->slow = slow;
+        ws->slow_need = slow_need;
+    }
     c->stats.paths = n_paths;
     c->stats.pieces = n_pieces;
     c->stats.segments = n_edges;
@@ -782,11 +898,12 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     c->stats.host_syncs = c->host_syncs;
     if (c->timer && c->timer->on) {
         // The final read_back synchronised the stream: every event is complete.
+        const int sl = c->timer->slot;
         for (int k = 0; k < kStages; ++k) {
             float ms = 0.f;
-            if (c->timer->used[k]) cudaEventElapsedTime(&ms, c->timer->begin[k], c->timer->end[k]);
+            if (c->timer->used[sl][k]) cudaEventElapsedTime(&ms, c->timer->begin[sl][k], c->timer->end[sl][k]);
             c->stage_ms[k] = ms;
-            c->stage_launches[k] = c->timer->used[k] ? c->timer->launches[k] : 0;
+            c->stage_launches[k] = c->timer->used[sl][k] ? c->timer->launches[sl][k] : 0;
         }
     }
     if (hc.err) {
@@ -882,14 +999,17 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
 // in half and retried.
 constexpr uint64_t kWavePoints = 40ull << 20;
 
+// ws / slot: the wave's cached sizes and counter slot (run_resident_one);
+// the halves of a wave that had to be split get none.
 int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* arena, size_t arena_len, int rowmap,
-              rrb_batch_stats& acc, int depth, std::vector<uint32_t>& done_plan) {
+              rrb_batch_stats& acc, int depth, std::vector<uint32_t>& done_plan, WaveSizes* ws = nullptr,
+              uint32_t slot = 0) {
     int rc;
     if (pg0 == 0 && pg1 == B->n_pages) {
-        rc = run_resident_one(c, B, arena, arena_len, rowmap);
+        rc = run_resident_one(c, B, arena, arena_len, rowmap, ws, slot);
     } else {
         rc = make_wave(c, B, pg0, pg1, c->wave_batch);
-        if (!rc) rc = run_resident_one(c, c->wave_batch, arena, arena_len, rowmap);
+        if (!rc) rc = run_resident_one(c, c->wave_batch, arena, arena_len, rowmap, ws, slot);
     }
     if (rc == RRB_OK) {
         const rrb_batch_stats& s = c->stats;
@@ -953,7 +1073,9 @@ int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_le
     // Wave plan: the groups that worked last time, else consecutive pages up
     // to wave_pts points each (any group that fails is split in two).
     std::vector<uint32_t> plan;
-    if (!B->plan.empty() && B->plan_wave_points == wave_pts && B->plan.back() == B->n_pages) {
+    const bool reused = !B->plan.empty() && B->plan_wave_points == wave_pts && B->plan.back() == B->n_pages;
+    if (!reused) B->sizes.clear();  // sizes belong to the plan's waves
+    if (reused) {
         plan = B->plan;
     } else if (B->n_paths == 0 || B->n_pts <= wave_pts) {
         plan = {0, B->n_pages};
@@ -969,15 +1091,83 @@ int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_le
     }
     std::memset(c->stage_sum_ms, 0, sizeof c->stage_sum_ms);
     std::memset(c->stage_sum_launches, 0, sizeof c->stage_sum_launches);
-    std::vector<uint32_t> done_plan{plan.front()};
-    for (size_t i = 0; i + 1 < plan.size(); ++i) {
-        int rc = run_pages(c, B, plan[i], plan[i + 1], arena, arena_len, rowmap, acc, 0, done_plan);
+    // Waves whose sizes the last render of this plan found: launched without
+    // waiting on the stream, their counters read after one wait at the end.
+    const size_t n_waves = plan.size() - 1;
+    if (B->sizes.size() != n_waves) B->sizes.assign(n_waves, WaveSizes{});
+    if (c->h_waves_cap < n_waves) {
+        if (c->h_waves) cudaFreeHost(c->h_waves);
+        c->h_waves = nullptr;
+        c->h_waves_cap = 0;
+        void* h = nullptr;
+        if (cudaMallocHost(&h, std::max<size_t>(n_waves, 8) * sizeof(BatchCounters)) == cudaSuccess) {
+            c->h_waves = static_cast<BatchCounters*>(h);
+            c->h_waves_cap = static_cast<uint32_t>(std::max<size_t>(n_waves, 8));
+        } else {
+            cudaGetLastError();  // no slots: every wave reads its sizes back
+        }
+    }
+    if (c->h_geom_cap < B->n_pages) {
+        if (c->h_geom) cudaFreeHost(c->h_geom);
+        c->h_geom = nullptr;
+        c->h_geom_cap = 0;
+        void* h = nullptr;
+        if (cudaMallocHost(&h, std::max<size_t>(B->n_pages, 64) * sizeof(PageGeom)) == cudaSuccess) {
+            c->h_geom = static_cast<PageGeom*>(h);
+            c->h_geom_cap = static_cast<uint32_t>(std::max<size_t>(B->n_pages, 64));
+        } else {
+            cudaGetLastError();  // geometry then comes from pageable memory
+        }
+    }
+    std::vector<uint32_t> done_plan{plan.front()}, deferred;
+    for (size_t i = 0; i < n_waves; ++i) {
+        const uint32_t slot = static_cast<uint32_t>(i);
+        if (c->timer) c->timer->slot = static_cast<int>(std::min<size_t>(i, kTimedWaves - 1));
+        c->geom_slot = plan[i];
+        int rc = run_pages(c, B, plan[i], plan[i + 1], arena, arena_len, rowmap, acc, 0, done_plan, &B->sizes[i],
+                           slot);
         if (rc) {
             c->stats = acc;
             B->plan.clear();
+            B->sizes.clear();
+            if (c->timer) c->timer->slot = 0;
             return rc;
         }
+        if (c->deferred) deferred.push_back(slot);
     }
+    if (c->timer) c->timer->slot = 0;
+    if (!deferred.empty()) {
+        // The render's one wait: then every deferred wave's counters and events.
+        ++acc.host_syncs;
+        RRB_CUDA(c, cudaStreamSynchronize(c->stream));
+        uint32_t err = 0;
+        for (uint32_t w : deferred) {
+            const BatchCounters& hc = c->h_waves[w];
+            err |= hc.err;
+            acc.aa_rows += hc.aa_rows;
+            acc.spans += hc.cell_cursor;
+            acc.row_overflows += hc.ovf_count;
+            acc.nonterminating_rows += hc.nonterminating;
+            if (c->timer && c->timer->on) {
+                const int sl = static_cast<int>(std::min<uint32_t>(w, kTimedWaves - 1));
+                for (int k = 0; k < kStages; ++k) {
+                    float ms = 0.f;
+                    if (c->timer->used[sl][k]) cudaEventElapsedTime(&ms, c->timer->begin[sl][k], c->timer->end[sl][k]);
+                    c->stage_sum_ms[k] += ms;
+                    c->stage_sum_launches[k] += c->timer->used[sl][k] ? c->timer->launches[sl][k] : 0;
+                }
+            }
+        }
+        if (err) {
+            // Cannot happen for the inputs the sizes came from; drop them.
+            B->sizes.clear();
+            c->stats = acc;
+            char buf[128];
+            std::snprintf(buf, sizeof buf, "batch capacity exceeded on a replay (error bits 0x%x)", err);
+            return set_err(c, RRB_ERR_POOL_EXHAUSTED, buf);
+        }
+    }
+    if (done_plan != plan) B->sizes.assign(done_plan.size() - 1, WaveSizes{});  // waves were split
     B->plan = done_plan;
     B->plan_wave_points = wave_pts;
     c->stats = acc;
@@ -1311,12 +1501,15 @@ int rrb_destroy(rrb_ctx* c) {
         delete c->wave_batch;
     }
     if (c->timer) {
-        for (int k = 0; k < kStages; ++k) {
-            cudaEventDestroy(c->timer->begin[k]);
-            cudaEventDestroy(c->timer->end[k]);
-        }
+        for (int w = 0; w < kTimedWaves; ++w)
+            for (int k = 0; k < kStages; ++k) {
+                cudaEventDestroy(c->timer->begin[w][k]);
+                cudaEventDestroy(c->timer->end[w][k]);
+            }
         delete c->timer;
     }
+    if (c->h_waves) cudaFreeHost(c->h_waves);
+    if (c->h_geom) cudaFreeHost(c->h_geom);
     if (c->paint) {
         PinnedAlloc alloc;
         c->paint->release(alloc);
@@ -1603,10 +1796,11 @@ int rrb_set_profiling(rrb_ctx* c, int enable) {
     const rrb_host::DeviceScope dev_scope(c->device);
     if (!c->timer) {
         c->timer = new StageTimer();
-        for (int k = 0; k < kStages; ++k) {
-            RRB_CUDA(c, cudaEventCreate(&c->timer->begin[k]));
-            RRB_CUDA(c, cudaEventCreate(&c->timer->end[k]));
-        }
+        for (int w = 0; w < kTimedWaves; ++w)
+            for (int k = 0; k < kStages; ++k) {
+                RRB_CUDA(c, cudaEventCreate(&c->timer->begin[w][k]));
+                RRB_CUDA(c, cudaEventCreate(&c->timer->end[w][k]));
+            }
     }
     c->timer->on = enable != 0;
     return RRB_OK;

@@ -73,6 +73,7 @@ class SceneShard:
         from . import batch_params
 
         sh = range_arrays(scene, *pages) if pages is not None else shard_arrays(scene, rank, world)
+        self._scene = scene  # the arrays below can be views of the scene's memory: keep it alive
         self.arena_base = int(sh["arena_base"])
         self.pages_range = sh["pages"]
         for k in ("pts", "flags", "path_pt_off", "fill_rule", "gray", "alpha", "path_page", "page_width",
