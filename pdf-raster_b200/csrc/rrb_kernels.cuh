@@ -982,9 +982,15 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
     int n = 0;
     bool has_last = false;
     int32_t lx0 = 0, lx1 = 0, lc = 0;
-    for (uint32_t eb = P.e_begin & ~31u; eb < P.e_end; eb += 32) {
-        const uint32_t gi = eb >> 5;
-        if (gmin[gi] > hi || gmax[gi] < lo) continue;  // no edge of this group touches the rows
+    // 32 groups' bounds at a time, one per lane: the warp visits only the
+    // groups whose rows meet [lo, hi], in ascending order.
+    for (uint32_t gb = P.e_begin >> 5; 32ull * gb < P.e_end; gb += 32) {
+      const uint32_t gl = gb + lane;
+      const bool g_hit = 32ull * gl < P.e_end && !(gmin[gl] > hi || gmax[gl] < lo);
+      uint32_t gm = __ballot_sync(0xffffffffu, g_hit);
+      while (gm) {
+        const uint32_t eb = (gb + static_cast<uint32_t>(__ffs(gm) - 1)) << 5;
+        gm &= gm - 1;
         const uint32_t j = eb + lane;
         Edge e;
         bool hit = false;
@@ -1045,6 +1051,7 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
             }
         }
         __syncwarp();
+      }
     }
     if (has_last) {
         if (n < K) {
@@ -1579,9 +1586,15 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
         int3 last = make_int3(0, 0, 0);
         bool has_last = false;
         int3* const Ls = scratch + sb + min(lane, 3u) * ne;
-        for (uint32_t base = P.e_begin & ~31u; base < P.e_end; base += 32) {
-            const uint32_t grp = base >> 5;
-            if (gmax[grp] < rlo || gmin[grp] > rhi) continue;
+        // 32 groups' bounds at a time, one per lane; only groups meeting the
+        // pixel row's AA rows are visited, in ascending order.
+        for (uint32_t gb = P.e_begin >> 5; 32ull * gb < P.e_end; gb += 32) {
+          const uint32_t gl = gb + lane;
+          const bool g_hit = 32ull * gl < P.e_end && !(gmax[gl] < rlo || gmin[gl] > rhi);
+          uint32_t gm = __ballot_sync(0xffffffffu, g_hit);
+          while (gm) {
+            const uint32_t base = (gb + static_cast<uint32_t>(__ffs(gm) - 1)) << 5;
+            gm &= gm - 1;
             const uint32_t j = base + lane;
             uint32_t bits = 0;  // sub-rows this lane's edge has an entry in
             if (j >= P.e_begin && j < P.e_end) {
@@ -1617,6 +1630,7 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
                 }
             }
             __syncwarp();
+          }
         }
         if (lane < 4 && has_last) Ls[n_s++] = last;
         int n4[4];
@@ -1997,9 +2011,16 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     // Two maps, used in turn: a run's map is written while no thread can still
     // be reading the one before it (one barrier per run).
     __shared__ uint8_t lut[2][RGB ? 768 : 256];
+    // Gray pages: the values a run of full-tile layers meets. A tile holds few
+    // distinct values, so the run's map is composed for those alone: every
+    // thread marks its pixels' values, warp 0 lists and clears the marks and
+    // composes the layers for each listed value (seen[] is all zero between runs).
+    __shared__ __align__(8) uint8_t seen[RGB ? 8 : 256];
+    __shared__ uint8_t vals[RGB ? 4 : 256];
     __shared__ uint32_t red[L::NW];
     __shared__ uint32_t next_tile;
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
+    if (!RGB) seen[threadIdx.x] = 0;  // COMP_THREADS == 256; ordered before use by take()'s barrier
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int col = (lane % L::LPR) * L::PX;
@@ -2149,12 +2170,37 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                     } else if (m - k >= 2) {
                         uint8_t* map = lut[lut_sel];
                         lut_sel ^= 1;
-                        uint32_t v = threadIdx.x;
-                        for (uint32_t i = k; i < m; ++i) {
-                            const uint32_t a = (hits[i].paint >> 8) & 0xff, gg = hits[i].paint & 0xff;
-                            v = div255((255u - a) * v + a * gg);  // a_src = div255(a * AA_GAMMA[16]) = a
+#pragma unroll
+                        for (int j = 0; j < NPIX; ++j) seen[pix[j]] = 1;
+                        __syncthreads();
+                        if (w == 0) {
+                            // List the marked values (lane l owns seen[8l .. 8l+7]) and clear them.
+                            const uint2 wd = reinterpret_cast<const uint2*>(seen)[lane];
+                            const uint32_t n_mine = __popc(__vcmpne4(wd.x, 0u)) / 8 + __popc(__vcmpne4(wd.y, 0u)) / 8;
+                            uint32_t at = n_mine;
+                            for (int o = 1; o < 32; o <<= 1) {
+                                const uint32_t t = __shfl_up_sync(0xffffffffu, at, o);
+                                if (lane >= o) at += t;
+                            }
+                            const uint32_t n_vals = __shfl_sync(0xffffffffu, at, 31);
+                            at -= n_mine;
+#pragma unroll
+                            for (int b = 0; b < 8; ++b) {
+                                const uint32_t byte = ((b < 4 ? wd.x : wd.y) >> (8 * (b & 3))) & 0xffu;
+                                if (byte) vals[at++] = static_cast<uint8_t>(8 * lane + b);
+                            }
+                            reinterpret_cast<uint2*>(seen)[lane] = make_uint2(0u, 0u);
+                            __syncwarp();
+                            for (uint32_t q = lane; q < n_vals; q += 32) {
+                                const uint32_t v0 = vals[q];
+                                uint32_t v = v0;
+                                for (uint32_t i = k; i < m; ++i) {
+                                    const uint32_t a = (hits[i].paint >> 8) & 0xff, gg = hits[i].paint & 0xff;
+                                    v = div255((255u - a) * v + a * gg);  // a_src = div255(a * AA_GAMMA[16]) = a
+                                }
+                                map[v0] = static_cast<uint8_t>(v);
+                            }
                         }
-                        map[threadIdx.x] = static_cast<uint8_t>(v);
                         __syncthreads();
 #pragma unroll
                         for (int j = 0; j < NPIX; ++j) pix[j] = map[pix[j]];
