@@ -85,16 +85,57 @@ uint64_t estimate_bytes(const rrb_path_batch_params& p) {
     return 3 * pages + p.n_pts * (17 + 112) + p.n_paths * 256 + (1u << 20);
 }
 
+// A growable array in page-locked host memory (rrb_alloc_host_pinned): the
+// batch upload from it is a DMA, and a batch of 4 Mi points or more streams
+// its path ranges to the device while earlier ranges render.
+template <typename T>
+struct PinnedVec {
+    rrb_ctx* c = nullptr;
+    rrb_host_buf* buf = nullptr;
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    ~PinnedVec() {
+        if (buf) rrb_free_host_pinned(c, buf);
+    }
+    bool reserve(size_t want) {
+        if (want <= cap) return true;
+        size_t nc = std::max<size_t>(want, cap + cap / 2 + 1024);
+        rrb_host_buf* nb = nullptr;
+        if (rrb_alloc_host_pinned(c, nc * sizeof(T), &nb)) return false;
+        T* np = static_cast<T*>(rrb_host_ptr(nb));
+        if (n) std::memcpy(np, p, n * sizeof(T));
+        if (buf) rrb_free_host_pinned(c, buf);
+        buf = nb;
+        p = np;
+        cap = nc;
+        return true;
+    }
+    bool append(const T* src, size_t k) {
+        if (!reserve(n + k)) return false;
+        if (k) std::memcpy(p + n, src, k * sizeof(T));
+        n += k;
+        return true;
+    }
+    bool push(T v) { return append(&v, 1); }
+    void clear() { n = 0; }
+    T* data() { return p; }
+    size_t size() const { return n; }
+};
+
 struct Staging {
-    std::vector<double> pts;
-    std::vector<uint8_t> flags, rule, gray, alpha;
-    std::vector<uint64_t> off, page_off;
-    std::vector<uint32_t> path_page, pw, ph;
+    PinnedVec<double> pts;
+    PinnedVec<uint8_t> flags, rule, gray, alpha;
+    PinnedVec<uint64_t> off, page_off;
+    PinnedVec<uint32_t> path_page, pw, ph;
+    void bind(rrb_ctx* c) {
+        pts.c = flags.c = rule.c = gray.c = alpha.c = off.c = page_off.c = path_page.c = pw.c = ph.c = c;
+    }
 };
 
 void worker(rrb_server* s, int wi) {
     rrb_ctx* c = s->ctx[wi];
     Staging st;
+    st.bind(c);
     rrb_buf* arena = nullptr;
     size_t arena_cap = 0;
     for (;;) {
@@ -162,33 +203,33 @@ void worker(rrb_server* s, int wi) {
         };
         // Concatenate the requests into one batch over one device arena.
         st.pts.clear(); st.flags.clear(); st.rule.clear(); st.gray.clear(); st.alpha.clear();
-        st.off.assign(1, 0); st.page_off.clear(); st.path_page.clear(); st.pw.clear(); st.ph.clear();
+        st.off.clear(); st.page_off.clear(); st.path_page.clear(); st.pw.clear(); st.ph.clear();
         std::vector<uint64_t> req_arena_off;
         uint64_t arena_len = 0;
         uint32_t page_base = 0;
+        bool staged = st.off.push(0);
         for (Request* r : batch) {
             const rrb_path_batch_params& p = r->p;
             req_arena_off.push_back(arena_len);
             const uint64_t pt_base = st.flags.size();
-            st.pts.insert(st.pts.end(), p.pts, p.pts + 2 * p.n_pts);
-            st.flags.insert(st.flags.end(), p.flags, p.flags + p.n_pts);
+            staged = staged && st.pts.append(p.pts, 2 * p.n_pts) && st.flags.append(p.flags, p.n_pts) &&
+                     st.off.reserve(st.off.size() + p.n_paths) && st.path_page.reserve(st.path_page.size() + p.n_paths);
+            if (!staged) break;
             for (uint64_t i = 0; i < p.n_paths; ++i) {
-                st.off.push_back(pt_base + p.path_pt_off[i + 1]);
-                st.path_page.push_back(page_base + p.path_page[i]);
+                st.off.p[st.off.n++] = pt_base + p.path_pt_off[i + 1];
+                st.path_page.p[st.path_page.n++] = page_base + p.path_page[i];
             }
-            st.rule.insert(st.rule.end(), p.fill_rule, p.fill_rule + p.n_paths);
-            st.gray.insert(st.gray.end(), p.gray, p.gray + p.n_paths);
-            st.alpha.insert(st.alpha.end(), p.alpha, p.alpha + p.n_paths);
-            for (uint32_t i = 0; i < p.n_pages; ++i) {
-                st.pw.push_back(p.page_width[i]);
-                st.ph.push_back(p.page_height[i]);
-                st.page_off.push_back(arena_len + p.page_offset[i]);
-            }
+            staged = st.rule.append(p.fill_rule, p.n_paths) && st.gray.append(p.gray, p.n_paths) &&
+                     st.alpha.append(p.alpha, p.n_paths);
+            for (uint32_t i = 0; i < p.n_pages && staged; ++i)
+                staged = st.pw.push(p.page_width[i]) && st.ph.push(p.page_height[i]) &&
+                         st.page_off.push(arena_len + p.page_offset[i]);
+            if (!staged) break;
             arena_len += (r->out_len + 255) & ~size_t(255);
             page_base += p.n_pages;
         }
-        int rc = RRB_OK;
-        if (arena_len > arena_cap) {
+        int rc = staged ? RRB_OK : RRB_ERR_OUT_OF_MEMORY;
+        if (!rc && arena_len > arena_cap) {
             if (arena) rrb_free_device(c, arena);
             arena = nullptr;
             arena_cap = 0;
