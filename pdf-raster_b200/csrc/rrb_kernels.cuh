@@ -2005,6 +2005,9 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     constexpr int NPIX = TH * TW / COMP_THREADS;
     static_assert(ITERS * L::PX == NPIX, "tile shape must cover the CTA exactly");
     __shared__ HitInfo hits[COMP_CHUNK];
+    // Gray pages: per hit, the full-coverage blend's constants packed as
+    // (255 - a) | a * g << 8 (a_src = div255(a * AA_GAMMA[16]) = a).
+    __shared__ uint32_t hcoef[RGB ? 1 : COMP_CHUNK];
     __shared__ uint32_t wcnt[L::NW];
     __shared__ uint8_t gamma[17];
     __shared__ int32_t mark[L::NW * L::RPW][TW];
@@ -2126,6 +2129,10 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 hi.rgb = RGB ? path_rgb[super_list[q]] : 0u;
                 hi.paint = P.paint | (full_over(P) ? HIT_FULL : 0u);
                 hits[pos] = hi;
+                if (!RGB) {
+                    const uint32_t a = (P.paint >> 8) & 0xffu, g = P.paint & 0xffu;
+                    hcoef[pos] = (255u - a) | ((a * g) << 8);
+                }
             }
             __syncthreads();
             // Software pipeline over the hits: the index entries of hit k+2 and
@@ -2133,12 +2140,18 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
             // A run of layers covering the whole tile is applied as one 256-entry
             // map (one blend per thread per layer) instead of per pixel.
             HitRows<TW, TH> cur, nxt, nxt2;
-            auto prime = [&](uint32_t k) {
-                if (k < total) {
-                    load_hit_index<TW, TH>(hits[k], rowmap, Y0, H, gidx, runs, cur);
-                    load_hit_cells<TW, TH>(cells, cur);
-                }
+            // Index entries of hits k and k+1, then (once they have landed) the
+            // first cells of hit k.
+            auto prime_index = [&](uint32_t k) {
+                if (k < total) load_hit_index<TW, TH>(hits[k], rowmap, Y0, H, gidx, runs, cur);
                 if (k + 1 < total) load_hit_index<TW, TH>(hits[k + 1], rowmap, Y0, H, gidx, runs, nxt);
+            };
+            auto prime_cells = [&](uint32_t k) {
+                if (k < total) load_hit_cells<TW, TH>(cells, cur);
+            };
+            auto prime = [&](uint32_t k) {
+                prime_index(k);
+                prime_cells(k);
             };
             prime(0);
             uint32_t k = 0;
@@ -2146,6 +2159,10 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 if (hits[k].paint & HIT_FULL) {
                     uint32_t m = k + 1;
                     while (m < total && (hits[m].paint & HIT_FULL)) ++m;
+                    // The index loads of the hits after the run go out now and
+                    // land while the run is composed; their cell loads follow
+                    // before the run's last barrier.
+                    prime_index(m);
                     if (RGB) {
                         // One map per channel (each channel composes on its own).
                         if (m - k >= 2) {
@@ -2157,6 +2174,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                             map[threadIdx.x] = static_cast<uint8_t>(v);
                             map[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
                             map[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
+                            prime_cells(m);
                             __syncthreads();
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j)
@@ -2166,6 +2184,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                             const uint32_t a = rgb_a_src((hits[k].paint >> 8) & 0xff, 255u), s = hits[k].rgb;
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j) pix[j] = rgb_over(pix[j], a, s);
+                            prime_cells(m);
                         }
                     } else if (m - k >= 2) {
                         uint8_t* map = lut[lut_sel];
@@ -2194,13 +2213,17 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                             for (uint32_t q = lane; q < n_vals; q += 32) {
                                 const uint32_t v0 = vals[q];
                                 uint32_t v = v0;
+                                // div255 of x <= 255 * 255 needs no clamp.
+#pragma unroll 4
                                 for (uint32_t i = k; i < m; ++i) {
-                                    const uint32_t a = (hits[i].paint >> 8) & 0xff, gg = hits[i].paint & 0xff;
-                                    v = div255((255u - a) * v + a * gg);  // a_src = div255(a * AA_GAMMA[16]) = a
+                                    const uint32_t cf = hcoef[i];
+                                    const uint32_t x = (cf & 0xffu) * v + (cf >> 8);
+                                    v = (x + (x >> 8) + 0x80u) >> 8;
                                 }
                                 map[v0] = static_cast<uint8_t>(v);
                             }
                         }
+                        prime_cells(m);
                         __syncthreads();
 #pragma unroll
                         for (int j = 0; j < NPIX; ++j) pix[j] = map[pix[j]];
@@ -2208,9 +2231,9 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                         const uint32_t a = (hits[k].paint >> 8) & 0xff, gg = hits[k].paint & 0xff;
 #pragma unroll
                         for (int j = 0; j < NPIX; ++j) pix[j] = div255((255u - a) * pix[j] + a * gg);
+                        prime_cells(m);
                     }
                     k = m;
-                    prime(k);
                     continue;
                 }
                 if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
