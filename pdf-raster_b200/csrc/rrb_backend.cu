@@ -84,6 +84,10 @@ struct rrb_ctx {
     rrb::PageGeom* h_geom = nullptr;
     uint32_t h_geom_cap = 0;
     uint32_t geom_slot = 0;  // where the next run_resident_one stages its geometry
+    // Set while the pages are still on their way up (rrb_render_pages_host):
+    // the next composite waits for this event first.
+    cudaEvent_t pages_up = nullptr;
+    bool wait_pages_up = false;
     uint64_t scratch_grows = 0;  // ensure() reallocations since the last record call began
     struct rrb_batch* tmp_batch = nullptr;  // inputs of rrb_record_path_batch
     struct rrb_batch* wave_batch = nullptr; // view of a group of pages of a larger batch
@@ -837,6 +841,10 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     }
     // ---- stage 4: composite
     stage(c, 11);
+    if (c->wait_pages_up) {  // the first composite of a host render: its pages must have landed
+        RRB_CUDA(c, cudaStreamWaitEvent(c->stream, c->pages_up, 0));
+        c->wait_pages_up = false;
+    }
     // Persistent: as many CTAs as fit on the device at once (4 per SM), taking
     // tiles from the work queue.
     if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 4),
@@ -1295,7 +1303,18 @@ bool page_locked(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
-int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8_t* arena, size_t arena_len) {
+// Host pages of rrb_render_pages_host: up before the render, down after it.
+struct HostPages {
+    uint8_t* p = nullptr;
+    size_t len = 0;
+};
+
+// io (optional): the streamed render also moves the pages. They go up on the
+// copy stream behind the first range's points, and the first composite
+// waits for them; each page goes down as soon as the last range with a path
+// on it has composited, while later ranges render.
+int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8_t* arena, size_t arena_len,
+                 const HostPages* io = nullptr) {
     if (!c->copy_stream) RRB_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     // Ranges of consecutive paths: a first one of about a tenth of the
     // points (the render starts once its copy lands), then kStreamRanges - 1
@@ -1309,7 +1328,9 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
             cut.push_back(static_cast<uint32_t>(p));
     cut.push_back(static_cast<uint32_t>(h->n_paths));
     const size_t nr = cut.size() - 1;
-    std::vector<cudaEvent_t> ev(nr + 1, nullptr);
+    // ev[0 .. nr-1]: range r's points landed; ev[nr]: previous work done;
+    // ev[nr+1]: pages landed; ev[nr+2 ..]: range r composited.
+    std::vector<cudaEvent_t> ev(2 * nr + 2, nullptr);
     for (auto& e : ev) RRB_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     auto done = [&](int rc) {
         cudaStreamSynchronize(c->copy_stream);  // no copy from the caller's memory may outlive the call
@@ -1329,7 +1350,29 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
                 return done(set_err(c, RRB_ERR_DEVICE, "point upload failed"));
         }
         if (cudaEventRecord(ev[r], c->copy_stream) != cudaSuccess) return done(set_err(c, RRB_ERR_DEVICE, "event"));
+        if (r == 0 && io) {
+            if (cudaMemcpyAsync(arena, io->p, io->len, cudaMemcpyHostToDevice, c->copy_stream) != cudaSuccess ||
+                cudaEventRecord(ev[nr + 1], c->copy_stream) != cudaSuccess)
+                return done(set_err(c, RRB_ERR_DEVICE, "page upload failed"));
+            c->pages_up = ev[nr + 1];
+            c->wait_pages_up = true;
+        }
     }
+    uint32_t next_down = 0;  // first page not yet on its way down
+    auto send_down = [&](uint32_t upto, cudaEvent_t after) -> bool {
+        if (!io || next_down >= upto) return true;
+        if (cudaEventRecord(after, c->stream) != cudaSuccess || cudaStreamWaitEvent(c->copy_stream, after, 0) != cudaSuccess)
+            return false;
+        for (; next_down < upto; ++next_down) {
+            const uint64_t off = h->page_offset[next_down];
+            const uint64_t bytes = static_cast<uint64_t>(B->bpp) * h->page_width[next_down] * h->page_height[next_down];
+            const uint64_t end = std::min<uint64_t>(off + bytes, io->len);
+            if (off < end && cudaMemcpyAsync(io->p + off, arena + off, end - off, cudaMemcpyDeviceToHost,
+                                             c->copy_stream) != cudaSuccess)
+                return false;
+        }
+        return true;
+    };
     rrb_batch_stats acc{};
     const uint64_t grows0 = c->scratch_grows;
     std::memset(c->stage_sum_ms, 0, sizeof c->stage_sum_ms);
@@ -1338,9 +1381,19 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
         if (cudaStreamWaitEvent(c->stream, ev[r], 0) != cudaSuccess) return done(set_err(c, RRB_ERR_DEVICE, "event"));
         const int rc = run_path_range(c, B, h->path_pt_off, cut[r], cut[r + 1], arena, arena_len, h->rowmap, acc, 0);
         if (rc) {
+            c->wait_pages_up = false;
             c->stats = acc;
             return done(rc);
         }
+        // Pages whose paths all lie in ranges 0..r are final.
+        uint32_t upto = next_down;
+        while (upto < B->n_pages && (r + 1 == nr || B->geom_h[upto].path_end <= cut[r + 1])) ++upto;
+        if (!send_down(upto, ev[nr + 2 + r])) return done(set_err(c, RRB_ERR_DEVICE, "page download failed"));
+    }
+    if (c->wait_pages_up) {  // no range reached a composite: the pages still go up and come back
+        RRB_CUDA(c, cudaStreamWaitEvent(c->stream, c->pages_up, 0));
+        c->wait_pages_up = false;
+        if (!send_down(B->n_pages, ev[2 * nr + 1])) return done(set_err(c, RRB_ERR_DEVICE, "page download failed"));
     }
     c->stats = acc;
     c->stats.scratch_grows = c->scratch_grows - grows0;
@@ -1354,9 +1407,12 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
 // few long ones) cost more split over ranges than the copy they would hide.
 // t0: when the caller's own host work began (default: now); the stats'
 // host_ns is the time from it to the first kernel.
+// io (optional): host pages to upload before and download after the render
+// (overlapped with it when the batch streams).
 int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t arena_len,
               const uint8_t* rgb = nullptr, const double* clip = nullptr, bool hairlines = false, bool stream = true,
-              const std::chrono::steady_clock::time_point* t0 = nullptr, const int32_t* visit = nullptr) {
+              const std::chrono::steady_clock::time_point* t0 = nullptr, const int32_t* visit = nullptr,
+              const HostPages* io = nullptr) {
     const auto start = t0 ? *t0 : std::chrono::steady_clock::now();
     rrb_batch* B = c->tmp_batch;
     const bool streamed = stream && h->n_paths > 1 && h->n_pts >= kStreamMinPoints && page_locked(h->pts) &&
@@ -1365,7 +1421,13 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
     if (rc) return rc;
     const uint64_t host_ns = static_cast<uint64_t>(
         std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - start).count());
-    rc = streamed ? run_streamed(c, h, B, arena, arena_len) : run_resident(c, B, arena, arena_len, h->rowmap);
+    if (streamed) {
+        rc = run_streamed(c, h, B, arena, arena_len, io);
+    } else {
+        if (io) RRB_CUDA(c, cudaMemcpyAsync(arena, io->p, io->len, cudaMemcpyHostToDevice, c->stream));
+        rc = run_resident(c, B, arena, arena_len, h->rowmap);
+        if (io && !rc) RRB_CUDA(c, cudaMemcpyAsync(io->p, arena, io->len, cudaMemcpyDeviceToHost, c->stream));
+    }
     c->stats.host_ns = host_ns;
     return rc;
 }
@@ -1891,15 +1953,17 @@ int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* h
     if (!c || !p || !host_pages || !p->pages) return RRB_ERR_INVARIANT;
     if (len > p->pages->len) return set_err(c, RRB_ERR_INVARIANT, "host pages larger than the device arena");
     const rrb_host::DeviceScope dev_scope(c->device);
-    RRB_CUDA(c, cudaMemcpyAsync(p->pages->p, host_pages, len, cudaMemcpyHostToDevice, c->stream));
     int rc = rrb_begin_page(c);
     if (rc) return rc;
-    rc = rrb_record_path_batch(c, p);
+    // The pages travel inside the render: overlapped with it when the batch
+    // streams (page-locked points), before and after it otherwise.
+    const HostPages io{host_pages, len};
+    rc = run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, nullptr, nullptr, false, true, nullptr,
+                   nullptr, &io);
     rrb_fence f = 0;
     int rc2 = rrb_submit_page(c, &f);
     if (rc) return rc;
     if (rc2) return rc2;
-    RRB_CUDA(c, cudaMemcpyAsync(host_pages, p->pages->p, len, cudaMemcpyDeviceToHost, c->stream));
     return rrb_wait_page(c, f, 0) ? RRB_ERR_DEVICE : (cudaStreamSynchronize(c->stream) == cudaSuccess ? RRB_OK : RRB_ERR_DEVICE);
 }
 
