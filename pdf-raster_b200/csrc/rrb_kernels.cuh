@@ -2013,21 +2013,17 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     __shared__ int32_t mark[L::NW * L::RPW][TW];
     // Two maps, used in turn: a run's map is written while no thread can still
     // be reading the one before it (one barrier per run).
-    __shared__ uint8_t lut[2][RGB ? 768 : 4];  // Rgb8 pages: the run's three channel maps
-    // Gray pages: a run of full-tile layers is composed per warp, for the few
-    // distinct values of that warp's own pixels: the warp marks them, lists
-    // and clears the marks, composes the layers for each listed value into
-    // its own map and applies it. No block barrier; other warps' chains fill
-    // the SM meanwhile. seen[w][] is all zero between runs.
-    __shared__ __align__(8) uint8_t seen[RGB ? 1 : L::NW][256];
-    __shared__ uint8_t vals[RGB ? 1 : L::NW][256];
-    __shared__ uint8_t wmap[RGB ? 1 : L::NW][256];
+    __shared__ uint8_t lut[2][RGB ? 768 : 256];
+    // Gray pages: the values a run of full-tile layers meets. A tile holds few
+    // distinct values, so the run's map is composed for those alone: every
+    // thread marks its pixels' values, warp 0 lists and clears the marks and
+    // composes the layers for each listed value (seen[] is all zero between runs).
+    __shared__ __align__(8) uint8_t seen[RGB ? 8 : 256];
+    __shared__ uint8_t vals[RGB ? 4 : 256];
     __shared__ uint32_t red[L::NW];
     __shared__ uint32_t next_tile;
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
-    if (!RGB) {
-        for (int q = threadIdx.x; q < L::NW * 256; q += COMP_THREADS) (&seen[0][0])[q] = 0;  // before take()'s barrier
-    }
+    if (!RGB) seen[threadIdx.x] = 0;  // COMP_THREADS == 256; ordered before use by take()'s barrier
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int col = (lane % L::LPR) * L::PX;
@@ -2191,46 +2187,46 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                             prime_cells(m);
                         }
                     } else if (m - k >= 2) {
-                        uint8_t* ws = seen[w];
-                        uint8_t* wv = vals[w];
-                        uint8_t* wm = wmap[w];
+                        uint8_t* map = lut[lut_sel];
+                        lut_sel ^= 1;
 #pragma unroll
-                        for (int j = 0; j < NPIX; ++j) ws[pix[j]] = 1;
-                        __syncwarp();
-                        // List the marked values (lane l owns ws[8l .. 8l+7]) and clear them.
-                        const uint2 wd = reinterpret_cast<const uint2*>(ws)[lane];
-                        const uint32_t n_mine = __popc(__vcmpne4(wd.x, 0u)) / 8 + __popc(__vcmpne4(wd.y, 0u)) / 8;
-                        uint32_t at = n_mine;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const uint32_t t = __shfl_up_sync(0xffffffffu, at, o);
-                            if (lane >= o) at += t;
-                        }
-                        const uint32_t n_vals = __shfl_sync(0xffffffffu, at, 31);
-                        at -= n_mine;
-#pragma unroll
-                        for (int b = 0; b < 8; ++b) {
-                            const uint32_t byte = ((b < 4 ? wd.x : wd.y) >> (8 * (b & 3))) & 0xffu;
-                            if (byte) wv[at++] = static_cast<uint8_t>(8 * lane + b);
-                        }
-                        reinterpret_cast<uint2*>(ws)[lane] = make_uint2(0u, 0u);
-                        __syncwarp();
-                        for (uint32_t q = lane; q < n_vals; q += 32) {
-                            const uint32_t v0 = wv[q];
-                            uint32_t v = v0;
-                            // div255 of x <= 255 * 255 needs no clamp.
-#pragma unroll 4
-                            for (uint32_t i = k; i < m; ++i) {
-                                const uint32_t cf = hcoef[i];
-                                const uint32_t x = (cf & 0xffu) * v + (cf >> 8);
-                                v = (x + (x >> 8) + 0x80u) >> 8;
+                        for (int j = 0; j < NPIX; ++j) seen[pix[j]] = 1;
+                        __syncthreads();
+                        if (w == 0) {
+                            // List the marked values (lane l owns seen[8l .. 8l+7]) and clear them.
+                            const uint2 wd = reinterpret_cast<const uint2*>(seen)[lane];
+                            const uint32_t n_mine = __popc(__vcmpne4(wd.x, 0u)) / 8 + __popc(__vcmpne4(wd.y, 0u)) / 8;
+                            uint32_t at = n_mine;
+                            for (int o = 1; o < 32; o <<= 1) {
+                                const uint32_t t = __shfl_up_sync(0xffffffffu, at, o);
+                                if (lane >= o) at += t;
                             }
-                            wm[v0] = static_cast<uint8_t>(v);
+                            const uint32_t n_vals = __shfl_sync(0xffffffffu, at, 31);
+                            at -= n_mine;
+#pragma unroll
+                            for (int b = 0; b < 8; ++b) {
+                                const uint32_t byte = ((b < 4 ? wd.x : wd.y) >> (8 * (b & 3))) & 0xffu;
+                                if (byte) vals[at++] = static_cast<uint8_t>(8 * lane + b);
+                            }
+                            reinterpret_cast<uint2*>(seen)[lane] = make_uint2(0u, 0u);
+                            __syncwarp();
+                            for (uint32_t q = lane; q < n_vals; q += 32) {
+                                const uint32_t v0 = vals[q];
+                                uint32_t v = v0;
+                                // div255 of x <= 255 * 255 needs no clamp.
+#pragma unroll 4
+                                for (uint32_t i = k; i < m; ++i) {
+                                    const uint32_t cf = hcoef[i];
+                                    const uint32_t x = (cf & 0xffu) * v + (cf >> 8);
+                                    v = (x + (x >> 8) + 0x80u) >> 8;
+                                }
+                                map[v0] = static_cast<uint8_t>(v);
+                            }
                         }
                         prime_cells(m);
-                        __syncwarp();
+                        __syncthreads();
 #pragma unroll
-                        for (int j = 0; j < NPIX; ++j) pix[j] = wm[pix[j]];
+                        for (int j = 0; j < NPIX; ++j) pix[j] = map[pix[j]];
                     } else {
                         const uint32_t a = (hits[k].paint >> 8) & 0xff, gg = hits[k].paint & 0xff;
 #pragma unroll

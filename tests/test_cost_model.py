@@ -135,8 +135,11 @@ def test_host_forward_equals_device_forward(rrb_lib):
 def test_trained_model_beats_the_default_tile_on_held_out_pages(rrb_lib):
     """The committed model (trained on 50,100 (page, tile) pairs) against the
     5,000 held-out pages of the sweep: its per-page tile choice costs less
-    measured device time than the fixed 64x16 default, about as little as the
-    autotuner table, and its time predictions stay within 20% on average."""
+    measured device time than the fixed 64x16 default (the method without a
+    tuner), and its time predictions stay within 20% on average. It does NOT
+    beat the autotuner table on tile choice: the table is within 0.7% of the
+    best shape per page, and the model's choices cost 0.2% more than the
+    table's (model_vs_table 0.998); this pins that it stays within 2% of it."""
     from pathlib import Path
 
     from rrb.autotune import CostModel, evaluate
@@ -147,7 +150,7 @@ def test_trained_model_beats_the_default_tile_on_held_out_pages(rrb_lib):
     rep = evaluate(model, d["X"], d["ms"])
     assert rep["pages"] == 5000
     assert rep["model_vs_default"] > 1.05
-    assert rep["model_vs_table"] > 0.98
+    assert 0.98 < rep["model_vs_table"] < 1.0 + 1e-3  # as good as the table, not better
     assert rep["mape"] < 0.2
     # The device and host forward passes give the same choices.
     X = d["X"][:200]
