@@ -735,19 +735,19 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         // Two shapes of the row stage: 12 list entries per AA row with 8 warps
         // per block (the default), or 16 entries with 4 warps, which sends
         // fewer rows to k_groups_mid (pages whose rows carry more crossings).
-        if (B->row_shape == 1) {
-            k_rows<KCAP_WIDE, 4><<<grid_for(c, n_chunks * 32, 4 * 32, 16), 4 * 32, 0, c->stream>>>(
+        auto rows = [&](auto kernel, int warps, size_t smem) -> int {
+            RRB_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem)));
+            kernel<<<grid_for(c, n_chunks * 32, warps * 32, 16), warps * 32, smem, c->stream>>>(
                 as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
                 gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
                 static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
                 as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
-        } else {
-            k_rows<KCAP><<<grid_for(c, n_chunks * 32, ROWS_WARPS * 32, 16), ROWS_WARPS * 32, 0, c->stream>>>(
-                as<PathInfo>(c->s_info), as<uint32_t>(c->s_chunks), as<uint32_t>(c->s_rows), as<Edge>(c->s_edges),
-                gmin, gmax, as<uint32_t>(B->pw), NP, as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans),
-                static_cast<uint32_t>(cell_cap), as<uint2>(c->s_ovf), static_cast<uint32_t>(std::max<uint64_t>(1, n_groups)),
-                as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
-        }
+            return RRB_OK;
+        };
+        if (B->row_shape == 1) rc = rows(k_rows<KCAP_WIDE, 4>, 4, rows_smem_bytes<KCAP_WIDE, 4>());
+        else rc = rows(k_rows<KCAP, ROWS_WARPS>, ROWS_WARPS, rows_smem_bytes<KCAP, ROWS_WARPS>());
+        if (rc) return rc;
         c->launches += 1;
     }
     if (n_runs) {

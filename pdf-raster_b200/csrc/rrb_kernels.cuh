@@ -921,23 +921,40 @@ __host__ __device__ __forceinline__ int walk_row(int n, int32_t mask, int32_t aa
 // 2 x (number of boundaries). Cell: x0 (bits 0-13) | len-1 (14-27) | cov-1 (28-31).
 template <typename Bound, typename Put>
 __host__ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bound, Put put) {
-    int bi[4] = {0, 0, 0, 0};
+    // Each list's next boundary (INT32_MAX once the list is used up) and its
+    // index (bit 0: a span end). The sweep takes the least head, lowest list
+    // first among equal ones, and reloads only that list's head.
+    int bi[4];
+    int32_t hd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        bi[k] = 0;
+        hd[k] = n[k] > 0 ? bound(k, 0, false) : INT32_MAX;
+    }
     int depth = 0, nc = 0;
     int32_t prev_px = -1;
     auto next = [&](int& kmin) -> int32_t {
-        int32_t best = INT32_MAX;
-        kmin = -1;
+        int32_t best = hd[0];
+        kmin = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (bi[k] < 2 * n[k]) {
-                const int32_t v = bound(k, bi[k] >> 1, (bi[k] & 1) != 0);
-                if (v < best) {
-                    best = v;
-                    kmin = k;
-                }
+        for (int k = 1; k < 4; ++k) {
+            if (hd[k] < best) {
+                best = hd[k];
+                kmin = k;
             }
         }
+        if (best == INT32_MAX) kmin = -1;
         return best;
+    };
+    auto advance = [&](int kk) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k == kk) {
+                depth += (bi[k] & 1) ? -1 : 1;
+                ++bi[k];
+                hd[k] = bi[k] < 2 * n[k] ? bound(k, bi[k] >> 1, (bi[k] & 1) != 0) : INT32_MAX;
+            }
+        }
     };
     auto emit = [&](int32_t x0, int32_t len, int32_t cov) {
         put(nc++, static_cast<uint32_t>(x0) | (static_cast<uint32_t>(len - 1) << 14) |
@@ -952,8 +969,7 @@ __host__ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bou
         while (k >= 0 && b < 4 * px + 4) {
             cov += depth * (b - col);
             col = b;
-            depth += (bi[k] & 1) ? -1 : 1;
-            ++bi[k];
+            advance(k);
             b = next(k);
         }
         cov += depth * (4 * px + 4 - col);
@@ -972,16 +988,51 @@ __host__ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bou
 // sees its entries in segment order and the write_intersect merge (merge only
 // with the last entry written to the row, scanner/mod.rs:600-642) is exact.
 // Groups of 32 edges whose row range misses [lo, hi] are skipped from the
-// per-group bounds gmin/gmax. Returns the entry count; entries past K are
-// counted but not stored (the caller treats n > K as overflow).
-template <int K, int LS>
+// per-group bounds gmin/gmax. GS groups are staged at once (sedge holds GS x
+// 32 edges) and folded in one loop, so the warp runs as many fold steps as
+// its busiest row has entries in those groups together, not per group.
+// Returns the entry count; entries past K are counted but not stored (the
+// caller treats n > K as overflow).
+template <int K, int LS, int GS = 1>
 __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t hi, int32_t r, bool valid,
                                           const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
-                                          const int32_t* __restrict__ gmax, int32_t (*sedge)[32], int32_t* x0s,
+                                          const int32_t* __restrict__ gmax, int32_t (*sedge)[32 * GS], int32_t* x0s,
                                           int32_t* x1s, int32_t* cns, int lane) {
+    static_assert(GS == 1 || GS == 2, "one or two staged edge groups");
     int n = 0;
     bool has_last = false;
     int32_t lx0 = 0, lx1 = 0, lc = 0;
+    auto fold = [&](int bb) {
+        Edge E;
+        E.row0 = sedge[0][bb];
+        E.row1 = sedge[1][bb];
+        E.flags = sedge[2][bb];
+        E.a = sedge[3][bb];
+        E.b = sedge[4][bb];
+        E.dfp = sedge[5][bb];
+        E.cmin = sedge[6][bb];
+        E.cmax = sedge[7][bb];
+        int32_t elo, ehi, ec;
+        edge_entry(E, r, elo, ehi, ec);
+        if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
+            lc = static_cast<int32_t>(static_cast<uint32_t>(lc) + static_cast<uint32_t>(ec));
+            lx0 = min(lx0, elo);
+            lx1 = max(lx1, ehi);
+        } else {
+            if (has_last) {
+                if (n < K) {
+                    x0s[n * LS + lane] = lx0;
+                    x1s[n * LS + lane] = lx1;
+                    cns[n * LS + lane] = lc;
+                }
+                ++n;
+            }
+            lx0 = elo;
+            lx1 = ehi;
+            lc = ec;
+            has_last = true;
+        }
+    };
     // 32 groups' bounds at a time, one per lane: the warp visits only the
     // groups whose rows meet [lo, hi], in ascending order.
     for (uint32_t gb = P.e_begin >> 5; 32ull * gb < P.e_end; gb += 32) {
@@ -989,65 +1040,56 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
       const bool g_hit = 32ull * gl < P.e_end && !(gmin[gl] > hi || gmax[gl] < lo);
       uint32_t gm = __ballot_sync(0xffffffffu, g_hit);
       while (gm) {
-        const uint32_t eb = (gb + static_cast<uint32_t>(__ffs(gm) - 1)) << 5;
-        gm &= gm - 1;
-        const uint32_t j = eb + lane;
-        Edge e;
-        bool hit = false;
-        if (j >= P.e_begin && j < P.e_end) {
-            e = edges[j];
-            hit = !(e.flags & EF_EMPTY) && e.row0 <= hi && e.row1 >= lo;
-        }
-        if (!__any_sync(0xffffffffu, hit)) continue;
-        if (hit) {
-            sedge[0][lane] = e.row0;
-            sedge[1][lane] = e.row1;
-            sedge[2][lane] = e.flags;
-            sedge[3][lane] = e.a;
-            sedge[4][lane] = e.b;
-            sedge[5][lane] = e.dfp;
-            sedge[6][lane] = e.cmin;
-            sedge[7][lane] = e.cmax;
+        uint32_t mine[GS];
+#pragma unroll
+        for (int s = 0; s < GS; ++s) {
+            mine[s] = 0;
+            // The next group with an edge on [lo, hi] goes to slot s.
+            while (gm) {
+                const uint32_t eb = (gb + static_cast<uint32_t>(__ffs(gm) - 1)) << 5;
+                gm &= gm - 1;
+                const uint32_t j = eb + lane;
+                Edge e;
+                bool hit = false;
+                if (j >= P.e_begin && j < P.e_end) {
+                    e = edges[j];
+                    hit = !(e.flags & EF_EMPTY) && e.row0 <= hi && e.row1 >= lo;
+                }
+                if (!__any_sync(0xffffffffu, hit)) continue;
+                uint32_t rows_of_edge = 0;
+                if (hit) {
+                    const int q = 32 * s + lane;
+                    sedge[0][q] = e.row0;
+                    sedge[1][q] = e.row1;
+                    sedge[2][q] = e.flags;
+                    sedge[3][q] = e.a;
+                    sedge[4][q] = e.b;
+                    sedge[5][q] = e.dfp;
+                    sedge[6][q] = e.cmin;
+                    sedge[7][q] = e.cmax;
+                    const int32_t ra = max(e.row0, lo) - lo, rb = min(e.row1, hi) - lo;
+                    rows_of_edge = (0xffffffffu >> (31 - rb)) & (0xffffffffu << ra);
+                }
+                mine[s] = warp_transpose32(rows_of_edge, lane);
+                break;
+            }
+            if (!valid) mine[s] = 0;
         }
         __syncwarp();
-        uint32_t rows_of_edge = 0;
-        if (hit) {
-            const int32_t ra = max(e.row0, lo) - lo, rb = min(e.row1, hi) - lo;
-            rows_of_edge = (0xffffffffu >> (31 - rb)) & (0xffffffffu << ra);
-        }
-        uint32_t mine = warp_transpose32(rows_of_edge, lane);
-        if (!valid) mine = 0;
-        while (mine) {
-            const int bb = __ffs(mine) - 1;
-            mine &= mine - 1;
-            Edge E;
-            E.row0 = sedge[0][bb];
-            E.row1 = sedge[1][bb];
-            E.flags = sedge[2][bb];
-            E.a = sedge[3][bb];
-            E.b = sedge[4][bb];
-            E.dfp = sedge[5][bb];
-            E.cmin = sedge[6][bb];
-            E.cmax = sedge[7][bb];
-            int32_t elo, ehi, ec;
-            edge_entry(E, r, elo, ehi, ec);
-            if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
-                lc = static_cast<int32_t>(static_cast<uint32_t>(lc) + static_cast<uint32_t>(ec));
-                lx0 = min(lx0, elo);
-                lx1 = max(lx1, ehi);
-            } else {
-                if (has_last) {
-                    if (n < K) {
-                        x0s[n * LS + lane] = lx0;
-                        x1s[n * LS + lane] = lx1;
-                        cns[n * LS + lane] = lc;
-                    }
-                    ++n;
-                }
-                lx0 = elo;
-                lx1 = ehi;
-                lc = ec;
-                has_last = true;
+        if constexpr (GS == 1) {
+            uint32_t m = mine[0];
+            while (m) {
+                const int bb = __ffs(m) - 1;
+                m &= m - 1;
+                fold(bb);
+            }
+        } else {
+            // Slot 0's group precedes slot 1's: bit order is edge order.
+            uint64_t m = (static_cast<uint64_t>(mine[1]) << 32) | mine[0];
+            while (m) {
+                const int bb = __ffsll(static_cast<long long>(m)) - 1;
+                m &= m - 1;
+                fold(bb);
             }
         }
         __syncwarp();
@@ -1111,6 +1153,14 @@ __global__ void k_chunk_paths(const uint32_t* __restrict__ chunk_off, uint32_t n
 // Chunks start on a multiple of 4 AA rows, so lanes 4k..4k+3 are the four
 // sub-rows of one pixel row; their spans are merged into coverage cells by
 // lane 4k. Pixel rows with a list over KCAP go to k_groups_mid.
+// k_rows' shared memory (dynamic: it exceeds the 48 KB of static shared
+// memory): per warp the three entry lists, two staged edge groups and the
+// span counts.
+template <int KCAP, int WARPS>
+constexpr size_t rows_smem_bytes() {
+    return sizeof(int32_t) * WARPS * (3 * KCAP * 32 + 8 * 64 + 32);
+}
+
 template <int KCAP, int WARPS = ROWS_WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
@@ -1118,11 +1168,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_rows(
     const uint32_t* __restrict__ page_w, uint32_t n_paths, uint2* __restrict__ group_idx, uint32_t* __restrict__ cells,
     uint32_t cell_cap, uint2* __restrict__ ovf, uint32_t ovf_cap, BatchCounters* __restrict__ ctr,
     const uint32_t* __restrict__ chunk_path, const int4* __restrict__ path_clip) {
-    __shared__ int32_t sx0[WARPS][KCAP * 32];
-    __shared__ int32_t sx1[WARPS][KCAP * 32];
-    __shared__ int32_t scn[WARPS][KCAP * 32];
-    __shared__ int32_t sedge[WARPS][8][32];
-    __shared__ int32_t sns[WARPS][32];
+    extern __shared__ __align__(16) int32_t rows_smem[];
+    constexpr int LIST = WARPS * KCAP * 32;
+    auto sx0 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem);
+    auto sx1 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + LIST);
+    auto scn = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + 2 * LIST);
+    auto sedge = reinterpret_cast<int32_t (*)[8][64]>(rows_smem + 3 * LIST);
+    auto sns = reinterpret_cast<int32_t (*)[32]>(rows_smem + 3 * LIST + WARPS * 8 * 64);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
@@ -1135,8 +1187,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_rows(
         const bool valid = r >= P.y0 && r <= chunk_hi;
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
-        const int n = gather_row<KCAP, 32>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
-                                           sx1[w], scn[w], lane);
+        const int n = gather_row<KCAP, 32, 2>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
+                                              sx1[w], scn[w], lane);
         const bool overflow = valid && n > KCAP;
         int ns = 0;
         const int2 cx = path_clip ? make_int2(path_clip[p].x, path_clip[p].y) : make_int2(0, aa_width);
@@ -1761,7 +1813,8 @@ __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int
     for (int it = 0; it < HitRows<TW, TH>::ITERS; ++it) {
         const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
         const int32_t grp = rowmap ? 4 * y + 3 : y;
-        const bool rowok = !(h.paint & PI_BOX) && y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 && grp <= h.g1;
+        const bool rowok = !(h.paint & (PI_BOX | HIT_FULL)) && y >= h.py0 && y <= h.py1 && y < H && grp >= h.g0 &&
+                           grp <= h.g1;
         uint2 ix = make_uint2(0u, 0u);
         if (rowok) {
             if (h.paint & PI_RECTI) {
@@ -2021,6 +2074,8 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     __shared__ __align__(8) uint8_t seen[RGB ? 8 : 256];
     __shared__ uint8_t vals[RGB ? 4 : 256];
     __shared__ uint32_t red[L::NW];
+    // Bit k: hit k of the chunk is not a full-tile layer (where a run of full layers ends).
+    __shared__ uint32_t partial[COMP_CHUNK / 32];
     __shared__ uint32_t next_tile;
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
     if (!RGB) seen[threadIdx.x] = 0;  // COMP_THREADS == 256; ordered before use by take()'s barrier
@@ -2108,6 +2163,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
             }
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) wcnt[w] = __popc(m);
+            if (threadIdx.x < COMP_CHUNK / 32) partial[threadIdx.x] = 0u;
             __syncthreads();
             uint32_t before = 0, total = 0;
 #pragma unroll
@@ -2127,8 +2183,10 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 hi.goff = (P.paint & PI_RECTI) ? P.run_off : group_off[super_list[q]];
                 hi.run_cnt = P.run_cnt;
                 hi.rgb = RGB ? path_rgb[super_list[q]] : 0u;
-                hi.paint = P.paint | (full_over(P) ? HIT_FULL : 0u);
+                const bool full = full_over(P);
+                hi.paint = P.paint | (full ? HIT_FULL : 0u);
                 hits[pos] = hi;
+                if (!full) atomicOr(&partial[pos >> 5], 1u << (pos & 31));
                 if (!RGB) {
                     const uint32_t a = (P.paint >> 8) & 0xffu, g = P.paint & 0xffu;
                     hcoef[pos] = (255u - a) | ((a * g) << 8);
@@ -2154,11 +2212,17 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 prime_cells(k);
             };
             prime(0);
+            // The first hit at or after `from` that is not a full-tile layer (or total).
+            auto next_partial = [&](uint32_t from) {
+                uint32_t wd = from >> 5;
+                uint32_t b = from < total ? partial[wd] & (0xffffffffu << (from & 31)) : 0u;
+                while (!b && 32 * (wd + 1) < total) b = partial[++wd];
+                return b ? 32 * wd + static_cast<uint32_t>(__ffs(b) - 1) : total;
+            };
             uint32_t k = 0;
             while (k < total) {
                 if (hits[k].paint & HIT_FULL) {
-                    uint32_t m = k + 1;
-                    while (m < total && (hits[m].paint & HIT_FULL)) ++m;
+                    const uint32_t m = next_partial(k + 1);
                     // The index loads of the hits after the run go out now and
                     // land while the run is composed; their cell loads follow
                     // before the run's last barrier.
