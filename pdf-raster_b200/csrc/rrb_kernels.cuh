@@ -1910,7 +1910,10 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
         // before that cell's end — the rule of the marking pass below,
         // without shared memory.
         bool few = false;
-        if constexpr (FEW) few = (h.paint & PI_RECTI) && __all_sync(0xffffffffu, ix.y <= kFewCells);
+        if constexpr (FEW) {
+            if constexpr (L::RPW > 1) few = (h.paint & PI_RECTI) && __all_sync(0xffffffffu, ix.y <= kFewCells);
+            else few = (h.paint & PI_RECTI) && ix.y <= kFewCells;
+        }
         if (few) {
             uint32_t sel[L::PX];
             bool has[L::PX];
@@ -1946,7 +1949,9 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
         uint32_t nb = 0;
         if (!few) {
             nb = (ix.y + L::LPR - 1) / L::LPR;
-            for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
+            // With one pixel row per warp step every lane holds the same entry.
+            if constexpr (L::RPW > 1)
+                for (int o = 16; o; o >>= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, o));
         }
         for (uint32_t bt = 0; bt < nb; ++bt) {
 #pragma unroll
