@@ -1801,6 +1801,7 @@ __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int 
 
 constexpr uint32_t kFewRuns = 4;   // rectilinear paths with at most this many runs: no search
 constexpr uint32_t kFewCells = 4;  // rectilinear rows with at most this many cells: direct lookup
+constexpr int kLoopCells = 6;      // rows with at most this many cells in the tile: tested one by one
 
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
@@ -1942,6 +1943,34 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
                 const int32_t x0 = static_cast<int32_t>(sel[q] & 0x3fffu);
                 const int32_t x1 = x0 + static_cast<int32_t>((sel[q] >> 14) & 0x3fffu) + 1;
                 if (has[q] && X0 + col + q < x1) cov[q] = static_cast<int32_t>(sel[q] >> 28) + 1;
+            }
+        }
+        // A warp holding one pixel row whose cells all sit in its lanes
+        // (cell0): when few of them reach into the tile, each pixel tests
+        // those few directly (cells are sorted and disjoint, so the one that
+        // contains a pixel is the last one starting at or before it).
+        if constexpr (L::RPW == 1) {
+            if (!few && ix.y <= static_cast<uint32_t>(L::LPR)) {
+                const uint32_t c = hr.cell0[it];
+                const int32_t x0 = static_cast<int32_t>(c & 0x3fffu);
+                const int32_t x1 = x0 + static_cast<int32_t>((c >> 14) & 0x3fffu) + 1;
+                const bool in_tile = static_cast<uint32_t>(sub) < ix.y && max(x0, X0) < min(x1, X0 + TW);
+                uint32_t bm = __ballot_sync(0xffffffffu, in_tile);
+                if (__popc(bm) <= kLoopCells) {
+                    while (bm) {
+                        const int t = __ffs(bm) - 1;
+                        bm &= bm - 1;
+                        const uint32_t cc = __shfl_sync(0xffffffffu, c, t);
+                        const int32_t cx0 = static_cast<int32_t>(cc & 0x3fffu);
+                        const int32_t cx1 = cx0 + static_cast<int32_t>((cc >> 14) & 0x3fffu) + 1;
+#pragma unroll
+                        for (int q = 0; q < L::PX; ++q) {
+                            const int32_t x = X0 + col + q;
+                            if (x >= cx0 && x < cx1) cov[q] = static_cast<int32_t>(cc >> 28) + 1;
+                        }
+                    }
+                    few = true;  // done: skip the marking pass
+                }
             }
         }
         // Otherwise the clipped cell starts are marked in shared memory, LPR
