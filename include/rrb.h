@@ -401,13 +401,20 @@ int rrb_last_stage_times(rrb_ctx* ctx, rrb_stage_time* out, int cap, int* n);
  * first violated invariant is written to msg. */
 int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, char* msg, size_t msg_len);
 
-/* Per-batch tuning knobs (tile shape etc.); 0 fields keep the defaults.
- * Tile shapes accepted: 16x16, 32x32, 64x16. */
+/* Per-batch tuning knobs (tile shape etc.); 0 fields keep the current
+ * values. Tile shapes accepted: 16x16, 32x32, 64x16, 128x16.
+ * auto_tile: 1 = a device-resident batch (rrb_record_batch) chooses its tile
+ * shape by trial: its first renders run 64x16 and 128x16, each with both
+ * row-stage shapes, and it keeps the fastest (by CUDA events; renders that
+ * grew scratch are repeated). 2 = every batch uses tile_w x tile_h (resident
+ * batches still try both row-stage shapes). The default is 1 with 64x16 for
+ * batches that are not resident. Giving a tile shape without auto_tile sets 2. */
 typedef struct {
     uint32_t tile_w, tile_h;
     uint32_t rows_per_chunk;    /* AA rows per row-kernel work item: 32 */
     uint32_t wave_points;       /* path points per wave of pages (0 = default, 40 Mi) */
-    uint32_t reserved[4];
+    uint32_t auto_tile;         /* 0 = keep, 1 = on, 2 = off */
+    uint32_t reserved[3];
 } rrb_tuning;
 int rrb_set_tuning(rrb_ctx* ctx, const rrb_tuning* t);
 int rrb_get_tuning(rrb_ctx* ctx, rrb_tuning* t);
@@ -425,6 +432,9 @@ typedef struct {
                                                stroke outlines, staging and enqueued uploads */
     uint64_t row_groups;                    /* pixel-row index entries written by the row stage */
     uint64_t host_syncs;                    /* times the call waited on its stream for a device-side size */
+    uint64_t tile_w, tile_h;                /* tile shape of the render */
+    uint64_t row_shape;                     /* row-stage shape: 0 = 12 entries x 8 warps, 1 = 16 x 4 */
+    uint64_t trials_left;                   /* resident batches: tuning trials still to run (0: settled) */
 } rrb_batch_stats;
 int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
 

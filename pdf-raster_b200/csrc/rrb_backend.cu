@@ -99,6 +99,8 @@ struct rrb_ctx {
     uint32_t stage_sum_launches[16] = {};
     rrb_stroke::PaintBatch* paint = nullptr;  // host arrays of rrb_record_stroke_batch, reused
     cudaStream_t copy_stream = nullptr;       // streamed batches: point uploads ahead of the render
+    uint64_t tuning_epoch = 0;                // bumped by rrb_set_tuning: resident batches re-run their trials
+    cudaEvent_t trial_ev[2] = {nullptr, nullptr};  // timing of a resident batch's trial render
 };
 
 namespace {
@@ -202,7 +204,7 @@ int read_back(rrb_ctx* c, const void* dev, size_t bytes) {
 }
 
 bool valid_tile(uint32_t w, uint32_t h) {
-    return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16);
+    return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16) || (w == 128 && h == 16);
 }
 
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
@@ -217,6 +219,7 @@ int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info,
 #define RRB_COMP_SHAPE(RGB, FEW)                                  \
     do {                                                          \
         if (tw == 64 && th == 16) RRB_COMP(64, 16, RGB, FEW);     \
+        else if (tw == 128 && th == 16) RRB_COMP(128, 16, RGB, FEW); \
         else if (tw == 32 && th == 32) RRB_COMP(32, 32, RGB, FEW); \
         else RRB_COMP(16, 16, RGB, FEW);                          \
     } while (0)
@@ -250,7 +253,7 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
     if (!(h->flatness >= 0.0)) return msg = "flatness must be >= 0", RRB_ERR_INVARIANT;
     for (int i = 0; i < 6; ++i)
         if (!std::isfinite(h->matrix[i])) return msg = "matrix must be finite", RRB_ERR_INVARIANT;
-    if (!valid_tile(tw, th)) return msg = "tile shape must be 16x16, 32x32 or 64x16", RRB_ERR_INVARIANT;
+    if (!valid_tile(tw, th)) return msg = "tile shape must be 16x16, 32x32, 64x16 or 128x16", RRB_ERR_INVARIANT;
     if (n_paths == 0) return RRB_OK;
     if (!h->pts || !h->flags || !h->path_pt_off || !h->fill_rule || !h->gray || !h->alpha || !h->path_page ||
         !h->page_width || !h->page_height || !h->page_offset || !n_pages)
@@ -353,11 +356,21 @@ struct rrb_batch {
     uint64_t plan_wave_points = 0;
     // Per wave of `plan`: the sizes its last render found on the device.
     std::vector<WaveSizes> sizes;
-    // Row-stage shape (0: 12 entries x 8 warps, 1: 16 entries x 4 warps). A
-    // resident batch renders once with each (renders that grew scratch do not
-    // count) and keeps the faster.
-    uint8_t row_shape = 0, shape_state = 0;
-    double shape_ms[2] = {0.0, 0.0};
+    // Row-stage shape (0: 12 entries x 8 warps, 1: 16 entries x 4 warps) and
+    // tile shape (0 x 0: the context's) of the next render. A resident batch
+    // renders once with each candidate pair (both row shapes; with automatic
+    // tiles both of 64x16 and 128x16), timed by events on its stream, repeats
+    // a trial whose render grew scratch, and keeps the fastest pair.
+    uint8_t row_shape = 0;
+    uint32_t tile_w = 0, tile_h = 0;
+    struct Trial {
+        uint32_t tw, th;
+        uint8_t rs;
+        float ms;
+    };
+    std::vector<Trial> trials;  // empty: not planned yet
+    size_t trial = 0;           // next trial to run (trials.size(): settled)
+    uint64_t trial_epoch = ~0ull;
     std::vector<PageGeom> geom_h;
     std::vector<uint64_t> page_pt;  // first point of each page's paths (n_pages + 1)
     bool view = false;              // a wave: inputs point into another batch (only off/page/geom owned)
@@ -445,7 +458,11 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     for (const PageGeom& G : B->geom_h)
         B->arena_need = std::max<uint64_t>(B->arena_need, G.offset + static_cast<uint64_t>(B->bpp) * G.w * G.h);
     B->plan.clear();
-    B->row_shape = B->shape_state = 0;
+    B->row_shape = 0;
+    B->tile_w = B->tile_h = 0;
+    B->trials.clear();
+    B->trial = 0;
+    B->trial_epoch = ~0ull;
     B->has_hairline = false;
     if (hairlines)
         for (uint64_t p = 0; p < h->n_paths && !B->has_hairline; ++p) B->has_hairline = h->fill_rule[p] == RULE_HAIRLINE;
@@ -529,8 +546,11 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if (B->n_paths == 0) return RRB_OK;
     if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
     if (rowmap < 0 || rowmap > 1) return set_err(c, RRB_ERR_INVARIANT, "rowmap must be 0 or 1");
-    const uint32_t tw = c->tuning.tile_w ? c->tuning.tile_w : 64;
-    const uint32_t th = c->tuning.tile_h ? c->tuning.tile_h : 16;
+    const uint32_t tw = B->tile_w ? B->tile_w : (c->tuning.tile_w ? c->tuning.tile_w : 64);
+    const uint32_t th = B->tile_h ? B->tile_h : (c->tuning.tile_h ? c->tuning.tile_h : 16);
+    c->stats.tile_w = tw;
+    c->stats.tile_h = th;
+    c->stats.row_shape = B->row_shape;
     uint64_t tiles = 0;
     set_tiles(B->geom_h, tw, th, tiles);
     if (tiles >= (1ull << 31)) return set_err(c, RRB_ERR_INVARIANT, "too many tiles");
@@ -979,6 +999,8 @@ int make_wave(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, rrb_batch* W
     W->has_clip = B->has_clip;
     W->has_hairline = B->has_hairline;
     W->row_shape = B->row_shape;
+    W->tile_w = B->tile_w;
+    W->tile_h = B->tile_h;
     if (B->has_clip) view(W->clip, B->clip, pb * sizeof(int4));
     if (B->has_clip) view(W->clipf, B->clipf, pb * 4 * sizeof(double));
     W->has_visit = B->has_visit;
@@ -1034,6 +1056,9 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
         acc.row_groups += s.row_groups;
         acc.host_syncs += s.host_syncs;
         acc.waves += 1;
+        acc.tile_w = s.tile_w;
+        acc.tile_h = s.tile_h;
+        acc.row_shape = s.row_shape;
         for (int k = 0; k < 16; ++k) {
             c->stage_sum_ms[k] += c->stage_ms[k];
             c->stage_sum_launches[k] += c->stage_launches[k];
@@ -1056,17 +1081,56 @@ int run_pages(rrb_ctx* c, rrb_batch* B, uint32_t pg0, uint32_t pg1, uint8_t* are
 int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap);
 
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
-    if (B->shape_state >= 2) return run_resident_waves(c, B, arena, arena_len, rowmap);
-    B->row_shape = B->shape_state;  // trying shape 0, then shape 1
-    const uint64_t g0 = c->scratch_grows;
-    const auto t0 = std::chrono::steady_clock::now();
-    const int rc = run_resident_waves(c, B, arena, arena_len, rowmap);
-    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    if (rc == RRB_OK && c->scratch_grows == g0) {
-        B->shape_ms[B->shape_state] = ms;
-        if (++B->shape_state == 2) B->row_shape = B->shape_ms[1] < B->shape_ms[0] ? 1 : 0;
+    if (B->trial_epoch != c->tuning_epoch) {
+        // Plan the trials: both row-stage shapes, for the context's tile shape
+        // or, with automatic tiles, for 64x16 and for 128x16.
+        B->trial_epoch = c->tuning_epoch;
+        B->trials.clear();
+        B->trial = 0;
+        const uint32_t cw = c->tuning.tile_w ? c->tuning.tile_w : 64, ch = c->tuning.tile_h ? c->tuning.tile_h : 16;
+        if (c->tuning.auto_tile == 1) {
+            for (uint32_t tw : {64u, 128u})
+                for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({tw, 16u, rs, 0.f});
+        } else {
+            for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({cw, ch, rs, 0.f});
+        }
     }
-    return rc;
+    auto settled = [&]() {
+        c->stats.trials_left = B->trials.size() - B->trial;
+    };
+    if (B->trial >= B->trials.size()) {
+        const int rc = run_resident_waves(c, B, arena, arena_len, rowmap);
+        settled();
+        return rc;
+    }
+    const rrb_batch::Trial& T = B->trials[B->trial];
+    B->tile_w = T.tw;
+    B->tile_h = T.th;
+    B->row_shape = T.rs;
+    for (cudaEvent_t& e : c->trial_ev)
+        if (!e) RRB_CUDA(c, cudaEventCreate(&e));
+    const uint64_t g0 = c->scratch_grows;
+    RRB_CUDA(c, cudaEventRecord(c->trial_ev[0], c->stream));
+    const int rc = run_resident_waves(c, B, arena, arena_len, rowmap);
+    if (rc != RRB_OK) return rc;
+    RRB_CUDA(c, cudaEventRecord(c->trial_ev[1], c->stream));
+    ++c->stats.host_syncs;
+    RRB_CUDA(c, cudaEventSynchronize(c->trial_ev[1]));
+    float ms = 0.f;
+    RRB_CUDA(c, cudaEventElapsedTime(&ms, c->trial_ev[0], c->trial_ev[1]));
+    if (c->scratch_grows == g0) {  // a render that grew scratch is repeated
+        B->trials[B->trial].ms = ms;
+        if (++B->trial == B->trials.size()) {
+            size_t best = 0;
+            for (size_t k = 1; k < B->trials.size(); ++k)
+                if (B->trials[k].ms < B->trials[best].ms) best = k;
+            B->tile_w = B->trials[best].tw;
+            B->tile_h = B->trials[best].th;
+            B->row_shape = B->trials[best].rs;
+        }
+    }
+    settled();
+    return RRB_OK;
 }
 
 int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
@@ -1212,6 +1276,8 @@ int make_path_wave(rrb_ctx* c, rrb_batch* B, uint32_t pa, uint32_t pb, uint64_t 
     W->has_clip = B->has_clip;
     W->has_hairline = B->has_hairline;
     W->row_shape = B->row_shape;
+    W->tile_w = B->tile_w;
+    W->tile_h = B->tile_h;
     auto view = [](Scratch& dst, const Scratch& src, size_t byte_off) {
         dst.p = static_cast<char*>(src.p) + byte_off;
         dst.cap = 0;
@@ -1273,6 +1339,9 @@ int run_path_range(rrb_ctx* c, rrb_batch* B, const uint64_t* path_pt_off, uint32
         acc.row_groups += s.row_groups;
         acc.host_syncs += s.host_syncs;
         acc.waves += 1;
+        acc.tile_w = s.tile_w;
+        acc.tile_h = s.tile_h;
+        acc.row_shape = s.row_shape;
         for (int k = 0; k < 16; ++k) {
             c->stage_sum_ms[k] += c->stage_ms[k];
             c->stage_sum_launches[k] += c->stage_launches[k];
@@ -1538,6 +1607,7 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
     c->tuning.tile_w = 64;
     c->tuning.tile_h = 16;
     c->tuning.rows_per_chunk = 32;
+    c->tuning.auto_tile = 1;
     *out = c;
     return RRB_OK;
 }
@@ -1554,6 +1624,8 @@ int rrb_destroy(rrb_ctx* c) {
                       &c->s_chunk_path, &c->s_clip_lo};
     for (Scratch* s : all) dev_free(c, s->p, s->cap);
     for (Scratch& s : c->s_fill) dev_free(c, s.p, s.cap);
+    for (cudaEvent_t e : c->trial_ev)
+        if (e) cudaEventDestroy(e);
     if (c->tmp_batch) {
         free_batch_bufs(c, c->tmp_batch);
         delete c->tmp_batch;
@@ -1742,10 +1814,14 @@ int rrb_wait_page(rrb_ctx* c, rrb_fence f, uint64_t timeout_ns) {
 int rrb_set_tuning(rrb_ctx* c, const rrb_tuning* t) {
     if (!c || !t) return RRB_ERR_INVARIANT;
     uint32_t w = t->tile_w ? t->tile_w : c->tuning.tile_w, h = t->tile_h ? t->tile_h : c->tuning.tile_h;
-    if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32 or 64x16");
+    if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32, 64x16 or 128x16");
+    if (t->auto_tile > 2) return set_err(c, RRB_ERR_INVARIANT, "auto_tile must be 0, 1 or 2");
     c->tuning.tile_w = w;
     c->tuning.tile_h = h;
+    if (t->auto_tile) c->tuning.auto_tile = t->auto_tile;
+    else if (t->tile_w || t->tile_h) c->tuning.auto_tile = 2;  // an explicit tile shape
     if (t->wave_points != 0xFFFFFFFFu) c->tuning.wave_points = t->wave_points;  // all ones: keep
+    ++c->tuning_epoch;
     return RRB_OK;
 }
 

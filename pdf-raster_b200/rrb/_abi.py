@@ -102,13 +102,14 @@ class PathBatchParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("rows_per_chunk", C.c_uint32),
-                ("wave_points", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("wave_points", C.c_uint32), ("auto_tile", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class BatchStats(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles", "tile_pairs",
-        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves", "host_ns", "row_groups", "host_syncs")]
+        "nonterminating_rows", "kernel_launches", "scratch_grows", "waves", "host_ns", "row_groups", "host_syncs",
+        "tile_w", "tile_h", "row_shape", "trials_left")]
 
 
 class StageTime(C.Structure):

@@ -63,10 +63,11 @@ STRUCTS = {
                                                   "alpha", "path_page", "n_paths", "page_width", "page_height",
                                                   "page_offset", "n_pages", "pages", "matrix", "flatness", "rowmap"]),
     "rrb_vram_budget": ("VramBudget", ["total_bytes", "free_bytes", "budget_bytes", "used_bytes"]),
-    "rrb_tuning": ("Tuning", ["tile_w", "tile_h", "rows_per_chunk", "wave_points", "reserved"]),
+    "rrb_tuning": ("Tuning", ["tile_w", "tile_h", "rows_per_chunk", "wave_points", "auto_tile", "reserved"]),
     "rrb_batch_stats": ("BatchStats", ["paths", "pieces", "segments", "aa_rows", "spans", "row_overflows", "tiles",
                                        "tile_pairs", "nonterminating_rows", "kernel_launches", "scratch_grows",
-                                       "waves", "host_ns", "row_groups", "host_syncs"]),
+                                       "waves", "host_ns", "row_groups", "host_syncs", "tile_w", "tile_h",
+                                       "row_shape", "trials_left"]),
     "rrb_stage_time": ("StageTime", ["name", "ms", "launches"]),
     "rrb_server_config": ("ServerConfig", ["device", "workers", "mem_budget_bytes", "max_batch_pages", "tile_w",
                                            "tile_h", "predict_threads", "reserved"]),

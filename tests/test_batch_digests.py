@@ -69,7 +69,7 @@ def test_serving_digests_pin_the_generated_inputs(rrb_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tile", [(64, 16), (32, 32), (16, 16)])
+@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (32, 32), (16, 16)])
 def test_mixed_batch_every_page_bit_exact(backend, mixed_scene, tile):
     """All 64 pages of the 1.17-Gpixel mixed batch, rendered in one submission,
     equal the oracle's pages (by digest) under each tile shape."""
@@ -90,7 +90,7 @@ def test_mixed_batch_every_page_bit_exact(backend, mixed_scene, tile):
         got = np.empty(s.arena_bytes, np.uint8)
         backend.wait_download(backend.download_async(pages, got))
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
         backend.free_device(pages)
     bad = [rec["page"] for rec in doc["records"] if _page_sha(got, s, rec["page"]) != rec["page_sha256"]]
     assert not bad, f"pages differing from the oracle: {bad}"

@@ -86,7 +86,7 @@ def test_clipped_batches_match_oracle(backend, oracle, rrb_lib, name, rowmap, rg
             d = np.nonzero(got != exp)[0]
             assert d.size == 0, f"{name} tile {tile}: {d.size} bytes differ, first at {d[:5]}"
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
         backend.free_device(pages)
 
 

@@ -139,7 +139,7 @@ def test_small_scenes(backend, oracle, rrb_lib, name, rowmap):
     assert np.array_equal(got, exp), _diff(got, exp)
 
 
-@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16)])
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16)])
 def test_tile_shapes_agree(backend, oracle, rrb_lib, tile):
     s = rrb_lib.Scene(kind=2, seed=9, n_pages=3, page_scale=0.12, paths_scale=0.04)
     exp, _ = _oracle_arena(oracle, s, 0)
@@ -147,7 +147,7 @@ def test_tile_shapes_agree(backend, oracle, rrb_lib, tile):
     try:
         got = _gpu_arena(backend, s, 0)
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
     assert np.array_equal(got, exp), _diff(got, exp)
 
 
@@ -295,7 +295,7 @@ def _stacked_rects(rrb, W, H, n, seed):
 
 
 @pytest.mark.parametrize("rowmap", ROWMAPS)
-@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16)])
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16)])
 def test_stacked_rectangles(backend, oracle, rrb_lib, rowmap, tile):
     W, H = 211, 157
     pts, flags, off, rule, gray, alpha = _stacked_rects(rrb_lib, W, H, 60, seed=7)
@@ -312,7 +312,7 @@ def test_stacked_rectangles(backend, oracle, rrb_lib, rowmap, tile):
         got = init.copy()
         backend.render_pages_host(p, got)
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
         backend.free_device(buf)
     assert np.array_equal(got, exp), _diff(got, exp)
 

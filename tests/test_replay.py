@@ -28,7 +28,7 @@ def _render(backend, batch, pages, n):
     return got, backend.last_batch_stats()
 
 
-@pytest.mark.parametrize("tile", [(64, 16), (32, 32)])
+@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (32, 32)])
 def test_replays_keep_pixels_and_stats_and_wait_once(backend, oracle, rrb_lib, tile):
     s = rrb_lib.Scene(kind=2, seed=23, n_pages=6, page_scale=0.25, paths_scale=0.1)
     exp = s.blank_arena()
@@ -56,7 +56,7 @@ def test_replays_keep_pixels_and_stats_and_wait_once(backend, oracle, rrb_lib, t
             assert last[key] == first[key], key
     finally:
         batch.free()
-        backend.set_tuning(64, 16, wave_points=0)
+        backend.set_tuning(64, 16, wave_points=0, auto_tile=True)
         backend.free_device(pages)
 
 
@@ -76,3 +76,43 @@ def test_new_inputs_are_not_replayed(backend, oracle, rrb_lib):
             assert backend.last_batch_stats()["host_syncs"] >= 3
     finally:
         backend.free_device(pages)
+
+
+def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
+    """With automatic tiles a resident batch renders once with each of 64x16
+    and 128x16 under both row-stage shapes, then keeps the fastest pair and
+    replays it: every render, trials included, gives the oracle's pages."""
+    s = rrb_lib.Scene(kind=2, seed=29, n_pages=3, page_scale=0.3, paths_scale=0.1)
+    exp = s.blank_arena()
+    oracle.render_scene(s, exp, threads=4)
+    pages = backend.alloc_device(s.arena_bytes)
+    backend.set_tuning(64, 16, auto_tile=True)
+    assert backend.get_tuning().auto_tile == 1
+    s.view.pages = None
+    batch = backend.batch_upload(s.view)
+    try:
+        seen = set()
+        for k in range(12):
+            got, st = _render(backend, batch, pages, s.arena_bytes)
+            assert np.array_equal(got, exp), f"render {k} ({st['tile_w']}x{st['tile_h']}, rows {st['row_shape']})"
+            seen.add((st["tile_w"], st["tile_h"], st["row_shape"]))
+            if st["trials_left"] == 0 and st["host_syncs"] == 1:
+                break
+        assert {(64, 16, 0), (64, 16, 1), (128, 16, 0), (128, 16, 1)} <= seen
+        assert st["trials_left"] == 0 and st["host_syncs"] == 1  # settled and replaying
+        assert (st["tile_w"], st["tile_h"]) in {(64, 16), (128, 16)}
+    finally:
+        batch.free()
+        backend.set_tuning(64, 16, auto_tile=True)
+        backend.free_device(pages)
+
+
+def test_explicit_tile_turns_automatic_tiles_off(backend):
+    backend.set_tuning(32, 32)
+    try:
+        t = backend.get_tuning()
+        assert (t.tile_w, t.tile_h, t.auto_tile) == (32, 32, 2)
+        backend.set_tuning(auto_tile=True)
+        assert backend.get_tuning().auto_tile == 1
+    finally:
+        backend.set_tuning(64, 16, auto_tile=True)

@@ -78,7 +78,7 @@ def test_rgb_pages_match_oracle(backend, oracle, rrb_lib, name, rowmap):
             d = np.nonzero(got != exp)[0]
             assert d.size == 0, f"{name} tile {tile}: {d.size} bytes differ, first at {d[:5]}"
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
         backend.free_device(pages)
 
 
@@ -136,7 +136,7 @@ def test_rgb_full_tile_layers_and_luma(backend, oracle, rrb_lib):
             backend.wait_download(backend.download_async(gray, g))
             assert np.array_equal(g, oracle.rgb_to_gray(exp))
     finally:
-        backend.set_tuning(64, 16)
+        backend.set_tuning(64, 16, auto_tile=True)
         backend.free_device(pages)
         backend.free_device(gray)
 
