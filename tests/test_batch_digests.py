@@ -103,19 +103,20 @@ def test_every_serving_request_bit_exact(rrb_lib):
     equals the oracle's page for its seed."""
     doc = _load(SERVING)
     recs = doc["records"]
+    burst = 32  # bounds the host memory held by queued requests
     with rrb_lib.Server(workers=2, max_batch_pages=16) as srv:
-        pending = []
-        for rec in recs:
-            sc = rrb_lib.Scene(kind=2, seed=rec["request"], n_pages=1)
-            sc.view.pages = None
-            out = sc.blank_arena(0)
-            pending.append((rec, sc, out, srv.submit(sc.view, out, init=255, keep=sc)))
-            if len(pending) >= 32:  # bound the host memory held by queued requests
-                rec0, sc0, out0, t0 = pending.pop(0)
-                srv.wait(t0)
-                assert _page_sha(out0, sc0) == rec0["page_sha256"], rec0["request"]
-        for rec, sc, out, t in pending:
-            srv.wait(t)
-            assert _page_sha(out, sc) == rec["page_sha256"], rec["request"]
+        for b0 in range(0, len(recs), burst):
+            # Generate a burst's scenes first, then submit them back to back:
+            # generating between submits would leave the workers idle, and
+            # every request would go out alone.
+            group = []
+            for rec in recs[b0:b0 + burst]:
+                sc = rrb_lib.Scene(kind=2, seed=rec["request"], n_pages=1)
+                sc.view.pages = None
+                group.append((rec, sc, sc.blank_arena(0)))
+            pending = [(rec, sc, out, srv.submit(sc.view, out, init=255, keep=sc)) for rec, sc, out in group]
+            for rec, sc, out, t in pending:
+                srv.wait(t)
+                assert _page_sha(out, sc) == rec["page_sha256"], rec["request"]
         st = srv.stats()
     assert st["completed"] == len(recs) and st["batches"] < len(recs)
