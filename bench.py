@@ -344,6 +344,10 @@ def run_rrb(args, rank, local, world):
     else:
         scene = full_scene
     backend = rrb.B200Backend(local)
+    if args.tile:
+        # A fixed tile shape (profiling runs): no tile trials.
+        tw, th = (int(v) for v in args.tile.split("x"))
+        backend.set_tuning(tw, th)
     tuning = backend.get_tuning()
     pages = backend.alloc_device(scene.arena_bytes)
     scene.view.pages = None
@@ -358,7 +362,7 @@ def run_rrb(args, rank, local, world):
 
     # Tuning renders (untimed, before the warm-up): the resident batch tries
     # each tile shape x row-stage shape and keeps the fastest.
-    for _ in range(16):
+    for _ in range(24):
         step()
         if backend.last_batch_stats()["trials_left"] == 0:
             break
@@ -530,7 +534,7 @@ def run_rrb(args, rank, local, world):
             "data": "synthetic (seeded generator, seed 0; no public dataset for this path)",
             "config": {"workload": desc, "paths": full_scene.n_paths, "pages": full_scene.n_pages,
                        "rowmap": ["documented", "as_shipped"][args.rowmap],
-                       "tile": f"{stats['tile_w']}x{stats['tile_h']} (chosen by trial among 64x16 and 128x16)"
+                       "tile": f"{stats['tile_w']}x{stats['tile_h']} (chosen by trial among 64x16, 128x16 and 128x32)"
                                if tuning.auto_tile == 1 else f"{stats['tile_w']}x{stats['tile_h']}",
                        "row_stage": "12 entries x 8 warps" if stats["row_shape"] == 0 else "16 entries x 4 warps",
                        "l2": f"inputs larger than L2 ({16 * scene.n_pts / 1e6:.0f} MB of path points)",
@@ -898,6 +902,7 @@ def main():
     ap.add_argument("--ref-threads", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
+    ap.add_argument("--tile", default="", help="WxH, a fixed tile shape instead of the trials (profiling runs)")
     ap.add_argument("--pages", default="", help="a:b, render only pages [a, b) of the batch (profiling runs)")
     ap.add_argument("--serving", action="store_true", help="Poisson request load against the server")
     ap.add_argument("--rates", default="50,200,1000,2000")

@@ -402,9 +402,9 @@ int rrb_last_stage_times(rrb_ctx* ctx, rrb_stage_time* out, int cap, int* n);
 int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, char* msg, size_t msg_len);
 
 /* Per-batch tuning knobs (tile shape etc.); 0 fields keep the current
- * values. Tile shapes accepted: 16x16, 32x32, 64x16, 128x16.
+ * values. Tile shapes accepted: 16x16, 32x32, 64x16, 128x16, 128x32.
  * auto_tile: 1 = a device-resident batch (rrb_record_batch) chooses its tile
- * shape by trial: its first renders run 64x16 and 128x16, each with both
+ * shape by trial: its first renders run 64x16, 128x16 and 128x32, each with both
  * row-stage shapes, and it keeps the fastest (by CUDA events; renders that
  * grew scratch are repeated). 2 = every batch uses tile_w x tile_h (resident
  * batches still try both row-stage shapes). The default is 1 with 64x16 for

@@ -204,7 +204,8 @@ int read_back(rrb_ctx* c, const void* dev, size_t bytes) {
 }
 
 bool valid_tile(uint32_t w, uint32_t h) {
-    return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16) || (w == 128 && h == 16);
+    return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16) || (w == 128 && h == 16) ||
+           (w == 128 && h == 32);
 }
 
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
@@ -213,13 +214,14 @@ int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info,
                      uint8_t* arena, int rowmap, BatchCounters* ctr, const uint32_t* path_rgb,
                      bool rectilinear, const uint32_t* super_start) {
 #define RRB_COMP(TW, TH, RGB, FEW)                                                                           \
-    k_composite<TW, TH, RGB, FEW><<<grid, COMP_THREADS, 0, c->stream>>>(                                      \
+    k_composite<TW, TH, RGB, FEW><<<grid, comp_threads(TW, TH), 0, c->stream>>>(                              \
         info, geom, n_pages, n_tiles, SUPER, SUPER, super_off, super_list, row_off, row_idx, spans, runs, arena, \
         rowmap, ctr, path_rgb, super_start)
 #define RRB_COMP_SHAPE(RGB, FEW)                                  \
     do {                                                          \
         if (tw == 64 && th == 16) RRB_COMP(64, 16, RGB, FEW);     \
         else if (tw == 128 && th == 16) RRB_COMP(128, 16, RGB, FEW); \
+        else if (tw == 128 && th == 32) RRB_COMP(128, 32, RGB, FEW); \
         else if (tw == 32 && th == 32) RRB_COMP(32, 32, RGB, FEW); \
         else RRB_COMP(16, 16, RGB, FEW);                          \
     } while (0)
@@ -253,7 +255,7 @@ int validate_batch(const rrb_path_batch_params* h, size_t arena_len, uint32_t tw
     if (!(h->flatness >= 0.0)) return msg = "flatness must be >= 0", RRB_ERR_INVARIANT;
     for (int i = 0; i < 6; ++i)
         if (!std::isfinite(h->matrix[i])) return msg = "matrix must be finite", RRB_ERR_INVARIANT;
-    if (!valid_tile(tw, th)) return msg = "tile shape must be 16x16, 32x32, 64x16 or 128x16", RRB_ERR_INVARIANT;
+    if (!valid_tile(tw, th)) return msg = "tile shape must be 16x16, 32x32, 64x16, 128x16 or 128x32", RRB_ERR_INVARIANT;
     if (n_paths == 0) return RRB_OK;
     if (!h->pts || !h->flags || !h->path_pt_off || !h->fill_rule || !h->gray || !h->alpha || !h->path_page ||
         !h->page_width || !h->page_height || !h->page_offset || !n_pages)
@@ -865,9 +867,10 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         RRB_CUDA(c, cudaStreamWaitEvent(c->stream, c->pages_up, 0));
         c->wait_pages_up = false;
     }
-    // Persistent: as many CTAs as fit on the device at once (4 per SM), taking
-    // tiles from the work queue.
-    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, 4),
+    // Persistent: as many CTAs as fit on the device at once (the CTAs per SM
+    // the composite is compiled for), taking tiles from the work queue.
+    const int comp_per_sm = comp_ctas_per_sm(static_cast<int>(tw), static_cast<int>(th));
+    if ((rc = launch_composite(c, static_cast<int>(tw), static_cast<int>(th), grid_for(c, tiles, 1, comp_per_sm),
                                as<PathInfo>(c->s_info), as<PageGeom>(B->geom), n_pages, static_cast<uint32_t>(tiles),
                                as<uint32_t>(c->s_super_cnt), as<uint32_t>(c->s_super_list), as<uint32_t>(c->s_rows),
                                as<uint2>(c->s_row_idx), as<uint32_t>(c->s_spans), as<int4>(c->s_runs), arena,
@@ -1083,14 +1086,15 @@ int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_le
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     if (B->trial_epoch != c->tuning_epoch) {
         // Plan the trials: both row-stage shapes, for the context's tile shape
-        // or, with automatic tiles, for 64x16 and for 128x16.
+        // or, with automatic tiles, for 64x16, 128x16 and 128x32.
         B->trial_epoch = c->tuning_epoch;
         B->trials.clear();
         B->trial = 0;
         const uint32_t cw = c->tuning.tile_w ? c->tuning.tile_w : 64, ch = c->tuning.tile_h ? c->tuning.tile_h : 16;
         if (c->tuning.auto_tile == 1) {
-            for (uint32_t tw : {64u, 128u})
-                for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({tw, 16u, rs, 0.f});
+            const uint32_t shapes[3][2] = {{64u, 16u}, {128u, 16u}, {128u, 32u}};
+            for (const auto& t : shapes)
+                for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({t[0], t[1], rs, 0.f});
         } else {
             for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({cw, ch, rs, 0.f});
         }
@@ -1814,7 +1818,7 @@ int rrb_wait_page(rrb_ctx* c, rrb_fence f, uint64_t timeout_ns) {
 int rrb_set_tuning(rrb_ctx* c, const rrb_tuning* t) {
     if (!c || !t) return RRB_ERR_INVARIANT;
     uint32_t w = t->tile_w ? t->tile_w : c->tuning.tile_w, h = t->tile_h ? t->tile_h : c->tuning.tile_h;
-    if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32, 64x16 or 128x16");
+    if (!valid_tile(w, h)) return set_err(c, RRB_ERR_INVARIANT, "tile shape must be 16x16, 32x32, 64x16, 128x16 or 128x32");
     if (t->auto_tile > 2) return set_err(c, RRB_ERR_INVARIANT, "auto_tile must be 0, 1 or 2");
     c->tuning.tile_w = w;
     c->tuning.tile_h = h;

@@ -1759,8 +1759,24 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
 // sub-row span lists -> AA_GAMMA -> div255 source-over), and the tile is
 // stored once.
 // ---------------------------------------------------------------------------
-constexpr int COMP_THREADS = 256;
-constexpr int COMP_CHUNK = 256;
+// Tiles of 4,096 pixels or more run RRB_COMP_BIG_THREADS threads per CTA
+// (512: a thread holds 8 pixels, as in the smaller tiles' 256-thread CTAs).
+// The composite is compiled for RRB_COMP_SM_THREADS resident threads per SM,
+// which sets its register budget: 1280 threads (five 256-thread CTAs, 48
+// registers) ran the 64-page mixed batch's composite 5% faster than 1024 (64
+// registers) and 4% faster than 1536 (40), spills included.
+#ifndef RRB_COMP_BIG_THREADS
+#define RRB_COMP_BIG_THREADS 512
+#endif
+#ifndef RRB_COMP_SM_THREADS
+#define RRB_COMP_SM_THREADS 1280
+#endif
+__host__ __device__ constexpr int comp_threads(int tw, int th) {
+    return tw * th >= 4096 ? RRB_COMP_BIG_THREADS : 256;
+}
+__host__ __device__ constexpr int comp_ctas_per_sm(int tw, int th) {
+    return RRB_COMP_SM_THREADS / comp_threads(tw, th) > 0 ? RRB_COMP_SM_THREADS / comp_threads(tw, th) : 1;
+}
 
 __constant__ uint8_t c_gamma[17] = {0, 4, 11, 21, 32, 45, 59, 74, 90, 108, 126, 145, 166, 187, 209, 231, 255};
 
@@ -1772,12 +1788,14 @@ struct HitInfo {
 
 constexpr uint32_t HIT_FULL = 1u << 18;  // every pixel of this tile has coverage 16 for this path
 
-template <int TW>
+template <int TW, int TH>
 struct CompLayout {
-    static constexpr int LPR = TW < 32 ? TW : 32;  // lanes per pixel row
-    static constexpr int PX = TW / LPR;            // pixels per lane
-    static constexpr int RPW = 32 / LPR;           // rows per warp step
-    static constexpr int NW = COMP_THREADS / 32;
+    static constexpr int NT = comp_threads(TW, TH);  // threads per CTA = candidates per chunk
+    static constexpr int LPR = TW < 32 ? TW : 32;      // lanes per pixel row
+    static constexpr int PX = TW / LPR;                // pixels per lane
+    static constexpr int RPW = 32 / LPR;               // rows per warp step
+    static constexpr int NW = NT / 32;
+    static constexpr int NPIX = TW * TH / NT;          // pixels per thread
 };
 
 // Loads of one hit for this thread's tile rows: the pixel row's entry in the
@@ -1785,7 +1803,7 @@ struct CompLayout {
 // first cell. k_composite issues them two and one hits ahead of use.
 template <int TW, int TH>
 struct HitRows {
-    static constexpr int ITERS = TH / (CompLayout<TW>::NW * CompLayout<TW>::RPW);
+    static constexpr int ITERS = TH / (CompLayout<TW, TH>::NW * CompLayout<TW, TH>::RPW);
     uint2 ix[ITERS];
     uint32_t cell0[ITERS];
 };
@@ -1797,17 +1815,18 @@ struct HitRows {
 // Then AA_GAMMA and the blend of composite_path_rows.
 template <int TW, int TH, bool RGB>
 __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int X0, int Y0, const uint8_t* gamma,
-                                              uint32_t (&pix)[TH * TW / COMP_THREADS]);
+                                              uint32_t (&pix)[CompLayout<TW, TH>::NPIX]);
 
 constexpr uint32_t kFewRuns = 4;   // rectilinear paths with at most this many runs: no search
 constexpr uint32_t kFewCells = 4;  // rectilinear rows with at most this many cells: direct lookup
 constexpr int kLoopCells = 6;      // rows with at most this many cells in the tile: tested one by one
+constexpr uint32_t kDirectRun = 4; // runs of at most this many full-tile layers: blended per pixel
 
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int Y0, int H,
                                                const uint2* __restrict__ gidx, const int4* __restrict__ runs,
                                                HitRows<TW, TH>& hr) {
-    using L = CompLayout<TW>;
+    using L = CompLayout<TW, TH>;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int slot = lane / L::LPR;
 #pragma unroll
@@ -1850,7 +1869,7 @@ __device__ __forceinline__ void load_hit_index(const HitInfo& h, int rowmap, int
 
 template <int TW, int TH>
 __device__ __forceinline__ void load_hit_cells(const uint32_t* __restrict__ cells, HitRows<TW, TH>& hr) {
-    using L = CompLayout<TW>;
+    using L = CompLayout<TW, TH>;
     const int sub = (threadIdx.x & 31) % L::LPR;
 #pragma unroll
     for (int it = 0; it < HitRows<TW, TH>::ITERS; ++it)
@@ -1886,12 +1905,28 @@ __device__ __forceinline__ uint32_t rgb_over_div255(uint32_t d, uint32_t a, uint
 // a_src of the Rgb8 path: (a_input * shape + 255) >> 8.
 __device__ __forceinline__ uint32_t rgb_a_src(uint32_t alpha, uint32_t shape) { return (alpha * shape + 255u) >> 8; }
 
+// div255 for x <= 255 * 255, where its clamp never applies: every product
+// of two bytes and every source-over sum (255 - a) * d + a * s.
+__device__ __forceinline__ uint32_t div255_small(uint32_t x) { return (x + (x >> 8) + 0x80u) >> 8; }
+
+// Source-over of one Gray8 pixel at AA coverage cov (1..16): a_src =
+// div255(alpha * AA_GAMMA[cov]), then div255((255 - a_src) * d + a_src * g).
+// Full coverage takes the hit's constants: AA_GAMMA[16] = 255 and
+// div255(alpha * 255) = alpha, so a_src = alpha (inv16 = 255 - alpha,
+// ag16 = alpha * g).
+__device__ __forceinline__ uint32_t gray_over(uint32_t d, int32_t cov, const uint8_t* gamma, uint32_t alpha,
+                                              uint32_t g, uint32_t inv16, uint32_t ag16) {
+    if (cov >= 16) return div255_small(inv16 * d + ag16);
+    const uint32_t a_src = div255_small(alpha * gamma[cov]);
+    return div255_small((255u - a_src) * d + a_src * g);
+}
+
 // FEW: the batch has rectilinear paths, whose rows take the direct lookup.
 template <int TW, int TH, bool RGB, bool FEW>
 __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitRows<TW, TH>& hr, int X0,
                                                     const uint32_t* __restrict__ cells, const uint8_t* gamma,
-                                                    int32_t (*mark)[TW], uint32_t (&pix)[TH * TW / COMP_THREADS]) {
-    using L = CompLayout<TW>;
+                                                    int32_t (*mark)[TW], uint32_t (&pix)[CompLayout<TW, TH>::NPIX]) {
+    using L = CompLayout<TW, TH>;
     constexpr int ITERS = HitRows<TW, TH>::ITERS;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane % L::LPR;
@@ -2029,14 +2064,13 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 #pragma unroll
         for (int q = 0; q < L::PX; ++q) {
             if (cov[q] == 0) continue;
-            const uint32_t shape = gamma[min(cov[q], 16)];
             const int k = it * L::PX + q;
             if (RGB) {
+                const uint32_t shape = gamma[min(cov[q], 16)];
                 pix[k] = (h.paint & PI_SOLID) ? rgb_over_div255(pix[k], alpha, h.rgb)
                                               : rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
             } else {
-                const uint32_t a_src = div255(alpha * shape);
-                pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
+                pix[k] = gray_over(pix[k], cov[q], gamma, alpha, g, 255u - alpha, alpha * g);
             }
         }
     }
@@ -2044,8 +2078,8 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 
 template <int TW, int TH, bool RGB>
 __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int X0, int Y0, const uint8_t* gamma,
-                                              uint32_t (&pix)[TH * TW / COMP_THREADS]) {
-    using L = CompLayout<TW>;
+                                              uint32_t (&pix)[CompLayout<TW, TH>::NPIX]) {
+    using L = CompLayout<TW, TH>;
     constexpr int ITERS = HitRows<TW, TH>::ITERS;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int slot = lane / L::LPR, col = (lane % L::LPR) * L::PX;
@@ -2066,13 +2100,11 @@ __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int 
         for (int q = 0; q < L::PX; ++q) {
             const int32_t cov = cx[q] * cy;
             if (cov == 0) continue;
-            const uint32_t shape = gamma[cov];
             const int k = it * L::PX + q;
             if (RGB) {
-                pix[k] = rgb_over(pix[k], rgb_a_src(alpha, shape), h.rgb);
+                pix[k] = rgb_over(pix[k], rgb_a_src(alpha, gamma[cov]), h.rgb);
             } else {
-                const uint32_t a_src = div255(alpha * shape);
-                pix[k] = div255((255u - a_src) * pix[k] + a_src * g);
+                pix[k] = gray_over(pix[k], cov, gamma, alpha, g, 255u - alpha, alpha * g);
             }
         }
     }
@@ -2081,15 +2113,16 @@ __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int 
 // RGB: the pages are Rgb8 (3 bytes per pixel) and path_rgb[p] is path p's
 // colour; otherwise Gray8 pages painted with each path's gray.
 template <int TW, int TH, bool RGB, bool FEW>
-__global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
+__global__ void __launch_bounds__(comp_threads(TW, TH), comp_ctas_per_sm(TW, TH)) k_composite(
     const PathInfo* __restrict__ info, const PageGeom* __restrict__ pages, uint32_t n_pages, uint32_t n_tiles,
     int stw, int sth, const uint32_t* __restrict__ super_off, const uint32_t* __restrict__ super_list,
     const uint32_t* __restrict__ group_off, const uint2* __restrict__ gidx, const uint32_t* __restrict__ cells,
     const int4* __restrict__ runs, uint8_t* __restrict__ arena, int rowmap, BatchCounters* __restrict__ ctr,
     const uint32_t* __restrict__ path_rgb, const uint32_t* __restrict__ super_start) {
-    using L = CompLayout<TW>;
+    using L = CompLayout<TW, TH>;
     constexpr int ITERS = TH / (L::NW * L::RPW);
-    constexpr int NPIX = TH * TW / COMP_THREADS;
+    constexpr int NPIX = L::NPIX;
+    constexpr int COMP_CHUNK = L::NT;
     static_assert(ITERS * L::PX == NPIX, "tile shape must cover the CTA exactly");
     __shared__ HitInfo hits[COMP_CHUNK];
     // Gray pages: per hit, the full-coverage blend's constants packed as
@@ -2110,9 +2143,12 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
     __shared__ uint32_t red[L::NW];
     // Bit k: hit k of the chunk is not a full-tile layer (where a run of full layers ends).
     __shared__ uint32_t partial[COMP_CHUNK / 32];
+    // Bit k: hit k reads coverage cells (neither a full-tile layer nor a box):
+    // the hits the load pipeline runs over.
+    __shared__ uint32_t pathbits[COMP_CHUNK / 32];
     __shared__ uint32_t next_tile;
     if (threadIdx.x < 17) gamma[threadIdx.x] = c_gamma[threadIdx.x];
-    if (!RGB) seen[threadIdx.x] = 0;  // COMP_THREADS == 256; ordered before use by take()'s barrier
+    if (!RGB && threadIdx.x < 256) seen[threadIdx.x] = 0;  // ordered before use by take()'s barrier
     if (ctr->err) return;  // a capacity overflow upstream: leave the pages untouched
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int col = (lane % L::LPR) * L::PX;
@@ -2197,7 +2233,7 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
             }
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) wcnt[w] = __popc(m);
-            if (threadIdx.x < COMP_CHUNK / 32) partial[threadIdx.x] = 0u;
+            if (threadIdx.x < COMP_CHUNK / 32) partial[threadIdx.x] = pathbits[threadIdx.x] = 0u;
             __syncthreads();
             uint32_t before = 0, total = 0;
 #pragma unroll
@@ -2221,58 +2257,50 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                 hi.paint = P.paint | (full ? HIT_FULL : 0u);
                 hits[pos] = hi;
                 if (!full) atomicOr(&partial[pos >> 5], 1u << (pos & 31));
+                if (!full && !box) atomicOr(&pathbits[pos >> 5], 1u << (pos & 31));
                 if (!RGB) {
                     const uint32_t a = (P.paint >> 8) & 0xffu, g = P.paint & 0xffu;
                     hcoef[pos] = (255u - a) | ((a * g) << 8);
                 }
             }
             __syncthreads();
-            // Software pipeline over the hits: the index entries of hit k+2 and
-            // the first cells of hit k+1 are in flight while hit k is blended.
+            // The first hit at or after `from` whose bit is set in bits[] (or total).
+            auto next_set = [&](const uint32_t* bits, uint32_t from) {
+                uint32_t wd = from >> 5;
+                uint32_t b = from < total ? bits[wd] & (0xffffffffu << (from & 31)) : 0u;
+                while (!b && 32 * (wd + 1) < total) b = bits[++wd];
+                return b ? 32 * wd + static_cast<uint32_t>(__ffs(b) - 1) : total;
+            };
+            // Software pipeline over the hits that read cells (path hits): the
+            // index entries of the path hit after next and the first cells of
+            // the next one are in flight while a path hit is blended, and across
+            // the boxes and full-tile runs between them, which load nothing.
             // A run of layers covering the whole tile is applied as one 256-entry
             // map (one blend per thread per layer) instead of per pixel.
             HitRows<TW, TH> cur, nxt, nxt2;
-            // Index entries of hits k and k+1, then (once they have landed) the
-            // first cells of hit k.
-            auto prime_index = [&](uint32_t k) {
-                if (k < total) load_hit_index<TW, TH>(hits[k], rowmap, Y0, H, gidx, runs, cur);
-                if (k + 1 < total) load_hit_index<TW, TH>(hits[k + 1], rowmap, Y0, H, gidx, runs, nxt);
-            };
-            auto prime_cells = [&](uint32_t k) {
-                if (k < total) load_hit_cells<TW, TH>(cells, cur);
-            };
-            auto prime = [&](uint32_t k) {
-                prime_index(k);
-                prime_cells(k);
-            };
-            prime(0);
-            // The first hit at or after `from` that is not a full-tile layer (or total).
-            auto next_partial = [&](uint32_t from) {
-                uint32_t wd = from >> 5;
-                uint32_t b = from < total ? partial[wd] & (0xffffffffu << (from & 31)) : 0u;
-                while (!b && 32 * (wd + 1) < total) b = partial[++wd];
-                return b ? 32 * wd + static_cast<uint32_t>(__ffs(b) - 1) : total;
-            };
+            const uint32_t p0 = next_set(pathbits, 0);
+            uint32_t p1 = p0 < total ? next_set(pathbits, p0 + 1) : total;  // the path hit after the next one
+            if (p0 < total) load_hit_index<TW, TH>(hits[p0], rowmap, Y0, H, gidx, runs, cur);
+            if (p1 < total) load_hit_index<TW, TH>(hits[p1], rowmap, Y0, H, gidx, runs, nxt);
+            if (p0 < total) load_hit_cells<TW, TH>(cells, cur);
             uint32_t k = 0;
             while (k < total) {
-                if (hits[k].paint & HIT_FULL) {
-                    const uint32_t m = next_partial(k + 1);
-                    // The index loads of the hits after the run go out now and
-                    // land while the run is composed; their cell loads follow
-                    // before the run's last barrier.
-                    prime_index(m);
+                const uint32_t kpaint = hits[k].paint;
+                if (kpaint & HIT_FULL) {
+                    const uint32_t m = next_set(partial, k + 1);
                     if (RGB) {
                         // One map per channel (each channel composes on its own).
                         if (m - k >= 2) {
                             uint8_t* map = lut[lut_sel];
                             lut_sel ^= 1;
-                            uint32_t v = threadIdx.x | (threadIdx.x << 8) | (threadIdx.x << 16);
-                            for (uint32_t i = k; i < m; ++i)
-                                v = rgb_over(v, rgb_a_src((hits[i].paint >> 8) & 0xff, 255u), hits[i].rgb);
-                            map[threadIdx.x] = static_cast<uint8_t>(v);
-                            map[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
-                            map[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
-                            prime_cells(m);
+                            if (threadIdx.x < 256) {
+                                uint32_t v = threadIdx.x | (threadIdx.x << 8) | (threadIdx.x << 16);
+                                for (uint32_t i = k; i < m; ++i)
+                                    v = rgb_over(v, rgb_a_src((hits[i].paint >> 8) & 0xff, 255u), hits[i].rgb);
+                                map[threadIdx.x] = static_cast<uint8_t>(v);
+                                map[256 + threadIdx.x] = static_cast<uint8_t>(v >> 8);
+                                map[512 + threadIdx.x] = static_cast<uint8_t>(v >> 16);
+                            }
                             __syncthreads();
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j)
@@ -2282,9 +2310,8 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                             const uint32_t a = rgb_a_src((hits[k].paint >> 8) & 0xff, 255u), s = hits[k].rgb;
 #pragma unroll
                             for (int j = 0; j < NPIX; ++j) pix[j] = rgb_over(pix[j], a, s);
-                            prime_cells(m);
                         }
-                    } else if (m - k >= 2) {
+                    } else if (m - k > kDirectRun) {
                         uint8_t* map = lut[lut_sel];
                         lut_sel ^= 1;
 #pragma unroll
@@ -2321,25 +2348,35 @@ __global__ void __launch_bounds__(COMP_THREADS, 4) k_composite(
                                 map[v0] = static_cast<uint8_t>(v);
                             }
                         }
-                        prime_cells(m);
                         __syncthreads();
 #pragma unroll
                         for (int j = 0; j < NPIX; ++j) pix[j] = map[pix[j]];
                     } else {
-                        const uint32_t a = (hits[k].paint >> 8) & 0xff, gg = hits[k].paint & 0xff;
+                        // A short run: each pixel takes the layers one by one
+                        // (no map, no barrier).
+                        for (uint32_t i = k; i < m; ++i) {
+                            const uint32_t cf = hcoef[i], inv = cf & 0xffu, ag = cf >> 8;
 #pragma unroll
-                        for (int j = 0; j < NPIX; ++j) pix[j] = div255((255u - a) * pix[j] + a * gg);
-                        prime_cells(m);
+                            for (int j = 0; j < NPIX; ++j) pix[j] = div255_small(inv * pix[j] + ag);
+                        }
                     }
                     k = m;
                     continue;
                 }
-                if (k + 2 < total) load_hit_index<TW, TH>(hits[k + 2], rowmap, Y0, H, gidx, runs, nxt2);
-                if (k + 1 < total) load_hit_cells<TW, TH>(cells, nxt);
-                if (hits[k].paint & PI_BOX) composite_box<TW, TH, RGB>(hits[k], rowmap, X0, Y0, gamma, pix);
-                else composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
+                if (kpaint & PI_BOX) {
+                    composite_box<TW, TH, RGB>(hits[k], rowmap, X0, Y0, gamma, pix);
+                    ++k;
+                    continue;
+                }
+                // A path hit (k is the pipeline's current one): the index loads
+                // of the path hit after p1 and the cells of p1 go out first.
+                const uint32_t p2 = p1 < total ? next_set(pathbits, p1 + 1) : total;
+                if (p2 < total) load_hit_index<TW, TH>(hits[p2], rowmap, Y0, H, gidx, runs, nxt2);
+                if (p1 < total) load_hit_cells<TW, TH>(cells, nxt);
+                composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
                 nxt = nxt2;
+                p1 = p2;
                 ++k;
             }
             __syncthreads();

@@ -428,8 +428,8 @@ class B200Backend:
     # ---- tuning / stats
     def set_tuning(self, tile_w: int = 0, tile_h: int = 0, wave_points: int | None = None,
                    auto_tile: bool | None = None):
-        """Tile shape (16x16 / 32x32 / 64x16 / 128x16) and, if given, path points per page wave
-        (0 = default). auto_tile: resident batches choose 64x16 or 128x16 by trial (a given tile
+        """Tile shape (16x16 / 32x32 / 64x16 / 128x16 / 128x32) and, if given, path points per page wave
+        (0 = default). auto_tile: resident batches choose 64x16, 128x16 or 128x32 by trial (a given tile
         shape turns it off unless auto_tile is passed)."""
         auto = 0 if auto_tile is None else (1 if auto_tile else 2)
         t = Tuning(tile_w=tile_w, tile_h=tile_h, wave_points=0xFFFFFFFF if wave_points is None else wave_points,

@@ -69,7 +69,7 @@ def test_serving_digests_pin_the_generated_inputs(rrb_lib):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (32, 32), (16, 16)])
+@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (128, 32), (32, 32), (16, 16)])
 def test_mixed_batch_every_page_bit_exact(backend, mixed_scene, tile):
     """All 64 pages of the 1.17-Gpixel mixed batch, rendered in one submission,
     equal the oracle's pages (by digest) under each tile shape."""

@@ -139,7 +139,7 @@ def test_small_scenes(backend, oracle, rrb_lib, name, rowmap):
     assert np.array_equal(got, exp), _diff(got, exp)
 
 
-@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16)])
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16), (128, 32)])
 def test_tile_shapes_agree(backend, oracle, rrb_lib, tile):
     s = rrb_lib.Scene(kind=2, seed=9, n_pages=3, page_scale=0.12, paths_scale=0.04)
     exp, _ = _oracle_arena(oracle, s, 0)
@@ -295,7 +295,7 @@ def _stacked_rects(rrb, W, H, n, seed):
 
 
 @pytest.mark.parametrize("rowmap", ROWMAPS)
-@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16)])
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16), (128, 32)])
 def test_stacked_rectangles(backend, oracle, rrb_lib, rowmap, tile):
     W, H = 211, 157
     pts, flags, off, rule, gray, alpha = _stacked_rects(rrb_lib, W, H, 60, seed=7)

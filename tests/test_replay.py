@@ -28,7 +28,7 @@ def _render(backend, batch, pages, n):
     return got, backend.last_batch_stats()
 
 
-@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (32, 32)])
+@pytest.mark.parametrize("tile", [(64, 16), (128, 16), (128, 32), (32, 32)])
 def test_replays_keep_pixels_and_stats_and_wait_once(backend, oracle, rrb_lib, tile):
     s = rrb_lib.Scene(kind=2, seed=23, n_pages=6, page_scale=0.25, paths_scale=0.1)
     exp = s.blank_arena()
@@ -79,8 +79,8 @@ def test_new_inputs_are_not_replayed(backend, oracle, rrb_lib):
 
 
 def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
-    """With automatic tiles a resident batch renders once with each of 64x16
-    and 128x16 under both row-stage shapes, then keeps the fastest pair and
+    """With automatic tiles a resident batch renders once with each of 64x16,
+    128x16 and 128x32 under both row-stage shapes, then keeps the fastest pair and
     replays it: every render, trials included, gives the oracle's pages."""
     s = rrb_lib.Scene(kind=2, seed=29, n_pages=3, page_scale=0.3, paths_scale=0.1)
     exp = s.blank_arena()
@@ -92,15 +92,15 @@ def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
     batch = backend.batch_upload(s.view)
     try:
         seen = set()
-        for k in range(12):
+        for k in range(16):
             got, st = _render(backend, batch, pages, s.arena_bytes)
             assert np.array_equal(got, exp), f"render {k} ({st['tile_w']}x{st['tile_h']}, rows {st['row_shape']})"
             seen.add((st["tile_w"], st["tile_h"], st["row_shape"]))
             if st["trials_left"] == 0 and st["host_syncs"] == 1:
                 break
-        assert {(64, 16, 0), (64, 16, 1), (128, 16, 0), (128, 16, 1)} <= seen
+        assert {(64, 16, 0), (64, 16, 1), (128, 16, 0), (128, 16, 1), (128, 32, 0), (128, 32, 1)} <= seen
         assert st["trials_left"] == 0 and st["host_syncs"] == 1  # settled and replaying
-        assert (st["tile_w"], st["tile_h"]) in {(64, 16), (128, 16)}
+        assert (st["tile_w"], st["tile_h"]) in {(64, 16), (128, 16), (128, 32)}
     finally:
         batch.free()
         backend.set_tuning(64, 16, auto_tile=True)

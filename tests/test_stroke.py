@@ -304,7 +304,7 @@ def _gpu_paint(backend, rrb_lib, sc, rgb=None, clip=None, rowmap=0, tile=(64, 16
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("rowmap", [0, 1])
-@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16)])
+@pytest.mark.parametrize("tile", [(16, 16), (32, 32), (64, 16), (128, 16), (128, 32)])
 def test_stroke_batch_matches_oracle(backend, oracle, rrb_lib, rowmap, tile):
     sc = StrokeScene(5, n_paths=300, n_pages=2)
     exp = np.full(sc.arena_bytes, 255, np.uint8)
