@@ -122,6 +122,15 @@ GLYPH_DRAM_BYTES_PER_SEGMENT = {
 }
 
 
+# DRAM bytes per page pixel of the composite on the mixed batch:
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
+# k_composite<128, 16> on page 0 of the batch alone (3508x4961, 17,589 paths;
+# its cells and row index larger than L2), scaled to a launch by its pixels.
+MIXED_DRAM_BYTES_PER_PIXEL = {
+    "composite": (92_163_328 + 14_567_936) / (3508 * 4961),
+}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -425,12 +434,16 @@ def run_rrb(args, rank, local, world):
         dur = stage_ms[dom] / waves / 1e3
         ach = alg_b / waves / dur / 1e9
         per_seg = GLYPH_DRAM_BYTES_PER_SEGMENT.get(dom) if args.workload == "glyphs" else None
-        traffic = per_seg * stats["segments"] / waves if per_seg else None
+        per_px = MIXED_DRAM_BYTES_PER_PIXEL.get(dom) if args.workload == "mixed" else None
+        traffic = (per_seg * stats["segments"] / waves if per_seg else
+                   per_px * px / waves if per_px else None)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                     "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
                     "algorithmic_bytes_per_launch": alg_b / waves, "launch_ms": dur * 1e3,
                     "traffic_source": ("ncu capture of the glyph page at 30,000 paths, scaled by segments"
-                                       if traffic else None)}
+                                       if per_seg else
+                                       "ncu capture of page 0 of the batch alone, scaled by pixels"
+                                       if per_px else None)}
 
     # ---- plain per-path form on a sample of paths (one record_path_fill per path)
     plain = None
