@@ -12,9 +12,9 @@ glyph-dense text page (150,000 glyphs on one Letter @300 dpi page),
   value  Mpixel/s with the path inputs already resident in device memory
          (rrb_batch_upload once, rrb_record_batch per step), timed with CUDA
          events on the backend's own stream, max over ranks.
-  e2e    the same metric through rrb_render_pages_host with pinned HOST
-         buffers: the path arrays and the pages go host->device and the pages
-         come back every step.
+  e2e    the same metric through rrb_render_pages_host_init with pinned HOST
+         buffers: the path arrays go host->device, the pages start white on
+         the device and come back to the host every step.
   bit_exact  every page of the batch against the CPU oracle: the mixed batch
          by the SHA-256 of each page that the oracle rendered
          (tests/golden/mixed_batch_digests.json), one-page workloads by the
@@ -478,20 +478,21 @@ def run_rrb(args, rank, local, world):
                               rowmap=args.rowmap)
     host_page = pinned_copy(backend, scene.blank_arena(), keep)
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
-    host_page[:] = 255
-    backend.render_pages_host(params, host_page)  # warm
+    # The pages start white (255), as the workload defines them: the device
+    # fills them (rrb_render_pages_host_init), so only the path arrays go up
+    # and the rendered pages come down.
+    backend.render_pages_host(params, host_page, init=255)  # warm
     if dist:
         dist.barrier()
     t = time.perf_counter()
     for _ in range(e2e_steps):
-        host_page[:] = 255
-        backend.render_pages_host(params, host_page)
+        backend.render_pages_host(params, host_page, init=255)
     e2e_s = time.perf_counter() - t
     if dist:
         tt = torch.tensor([e2e_s], device=f"cuda:{local}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_s = float(tt.item())
-    h2d = sum(int(h[k].nbytes) for k in h) + int(host_page.nbytes)
+    h2d = sum(int(h[k].nbytes) for k in h)
     # The host link alone: the same bytes as one pinned copy, for the bound e2e meets.
     scratch = backend.alloc_device(int(h["pts"].nbytes))
     backend.wait_transfer(backend.upload_async(scratch, h["pts"]))
@@ -502,7 +503,7 @@ def run_rrb(args, rank, local, world):
     backend.free_device(scratch)
     e2e = {"value": job_px * e2e_steps / e2e_s / 1e6, "unit": "Mpixel/s", "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": int(host_page.nbytes), "steps": e2e_steps,
-           "api": "rrb_render_pages_host (C ABI), pinned host buffers",
+           "api": "rrb_render_pages_host_init (C ABI, pages filled with 255 on the device), pinned host buffers",
            "h2d_link_gbs": link_gbs, "h2d_bound_ms": h2d / link_gbs / 1e6}
 
     # ---- parity check and CPU baseline (rank 0, N = 1)
@@ -795,10 +796,12 @@ def request_pool(rrb, n):
     return out
 
 
-def serve_rates(srv, reqs, rates, n_req, seed=0):
-    """Poisson arrivals at each rate, request i rendering pool page i mod len(pool);
-    latency percentiles of the completed requests and the number whose page
-    equals the oracle's pinned digest."""
+def serve_rates(srv, reqs, rates, n_req, outs, seed=0):
+    """Poisson arrivals at each rate, request i rendering pool page i mod len(pool)
+    into outs[i mod len(pool)] (at most len(pool) requests per rate, so no two
+    requests in flight share a buffer); latency percentiles of the completed
+    requests and the number whose page equals the oracle's pinned digest."""
+    assert n_req <= len(reqs)
     import hashlib
     rng = np.random.default_rng(seed)
     out = []
@@ -813,7 +816,8 @@ def serve_rates(srv, reqs, rates, n_req, seed=0):
             if dt > 0:
                 time.sleep(dt)
             p, k, n, _ = reqs[i % len(reqs)]
-            page = np.empty(n, np.uint8)
+            page = outs[i % len(reqs)]
+            page.fill(0)
             tickets.append((srv.submit(p, page, keep=k), page, i % len(reqs)))
         res, exact, checked = [], 0, 0
         for t, page, r in tickets:
@@ -846,6 +850,11 @@ def run_serving(args, rank, world):
     from rrb.autotune import CostModel
     reqs = request_pool(rrb, min(args.requests, SERVING_POOL))
     rates = [float(r) for r in args.rates.split(",")]
+    # Each pool page's result buffer, page-locked (as a serving client would
+    # keep its result buffers) and reused by every request for that page.
+    pin_ctx = rrb.B200Backend(0)
+    pin_bufs = [pin_ctx.alloc_host_pinned(n) for _, _, n, _ in reqs]
+    pin_outs = [b.array()[:n] for b, (_, _, n, _) in zip(pin_bufs, reqs)]
     model_path = Path(args.cost_model)
     model = CostModel.load(model_path) if model_path.exists() else None
     policies = ["arrival_order"] + (["autotuner_table", "cost_model"] if model is not None else [])
@@ -857,12 +866,14 @@ def run_serving(args, rank, world):
             elif policy == "autotuner_table":
                 srv.set_cost_model(table=model.table, shortest_first=False)
             # warm-up: every distinct page, queued at once (scratch reaches its working size)
-            warm = [srv.submit(p, np.empty(n, np.uint8), keep=k) for p, k, n, _ in reqs]
+            warm = [srv.submit(p, o, keep=k) for (p, k, n, _), o in zip(reqs, pin_outs)]
             for t in warm:
                 srv.wait(t)
             # The same pages queued at once again, timed: the rate of full batches
             # with no arrival gaps, which the Poisson rates are measured against.
-            outs = [np.empty(n, np.uint8) for _, _, n, _ in reqs]
+            outs = pin_outs
+            for o in outs:
+                o.fill(0)
             t0 = time.perf_counter()
             burst = [srv.submit(p, o, keep=k) for (p, k, n, _), o in zip(reqs, outs)]
             for t in burst:
@@ -874,7 +885,7 @@ def run_serving(args, rank, world):
                         for (_, _, _, d), o in zip(reqs, outs))
             rep = {"burst": {"pages": len(reqs), "pages_s": len(reqs) / wall, "mpixel_s": px / wall / 1e6,
                              "bit_exact_requests": f"{exact}/{sum(d is not None for *_, d in reqs)}"},
-                   "rates": serve_rates(srv, reqs, rates, args.requests), "server_stats": srv.stats()}
+                   "rates": serve_rates(srv, reqs, rates, min(args.requests, len(reqs)), pin_outs), "server_stats": srv.stats()}
             for r in rep["rates"]:
                 r["vs_burst_pages_s"] = r["completed_pages_s"] / rep["burst"]["pages_s"]
             report[policy] = rep

@@ -442,6 +442,12 @@ int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);
  * records the batch, downloads the pages and waits (one call, end to end). */
 int rrb_render_pages_host(rrb_ctx* ctx, const rrb_path_batch_params* p, uint8_t* host_pages,
                           size_t host_pages_len);
+/* The same for pages that start blank: the device fills its pages with
+ * init_value (0..255) instead of uploading host_pages, then renders and
+ * downloads them into host_pages (the renderer's fresh pages, e.g. white
+ * 255, without a host fill or a page upload). */
+int rrb_render_pages_host_init(rrb_ctx* ctx, const rrb_path_batch_params* p, uint8_t* host_pages,
+                               size_t host_pages_len, int init_value);
 
 /* ---- serving: continuous batching of page renders --------------------------
  * Worker threads, each with its own context and stream, form batches from the

@@ -46,6 +46,7 @@ struct Scratch {
 
 constexpr int KCAP = 12;        // merged Intersect entries per AA row kept in shared memory
 constexpr int KCAP_WIDE = 16;   // the same for the 4-warp row-stage shape
+constexpr uint64_t kLaneCountCurves = 1ull << 22;  // big curves whose lane counts are kept (128 MiB)
 constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
 
 }  // namespace
@@ -68,6 +69,7 @@ struct rrb_ctx {
     Scratch s_pieces, s_clip, s_edge_off, s_edges, s_info, s_rows, s_chunks, s_super_cnt, s_super_list;
     Scratch s_super_start;  // per supertile: one past its last opaque full layer
     Scratch s_big;          // piece slots of curves flattened by a warp each
+    Scratch s_lanes;        // per big curve: each lane's segment count (u8 x 32), from the count pass
     Scratch s_row_idx, s_spans, s_ovf, s_scratch, s_ctr, s_block, s_stats, s_groups, s_slots, s_path_pieces, s_ovf2;
     Scratch s_run_off, s_runs, s_chunk_path, s_clip_lo, s_hl_clip;
     Scratch s_fill[8];           // scratch of the aa_fill / tile_fill operators (rrb_fills.cu)
@@ -99,6 +101,7 @@ struct rrb_ctx {
     uint32_t stage_sum_launches[16] = {};
     rrb_stroke::PaintBatch* paint = nullptr;  // host arrays of rrb_record_stroke_batch, reused
     cudaStream_t copy_stream = nullptr;       // streamed batches: point uploads ahead of the render
+    cudaStream_t down_stream = nullptr;       // host page renders: page downloads beside the uploads
     uint64_t tuning_epoch = 0;                // bumped by rrb_set_tuning: resident batches re-run their trials
     cudaEvent_t trial_ev[2] = {nullptr, nullptr};  // timing of a resident batch's trial render
 };
@@ -611,12 +614,17 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     stage(c, 1);
     // Curves of more than CURVE_BIG segments: listed here, counted by a warp each.
     if ((rc = ensure(c, c->s_big, std::max<uint64_t>(1, n_pieces) * sizeof(uint32_t)))) return rc;
+    // Lane counts of the first lane_cap big curves: the write pass places each
+    // lane's leaves from them instead of counting again (later curves recount).
+    const uint32_t lane_cap = static_cast<uint32_t>(std::min<uint64_t>(n_pieces, kLaneCountCurves));
+    if ((rc = ensure(c, c->s_lanes, std::max<uint64_t>(1, lane_cap) * CURVE_LANES))) return rc;
     k_seg_count<true><<<grid_for(c, n_pieces, 128, 32), 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), NPC, as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_edge_off),
         as<uint32_t>(c->s_big), as<BatchCounters>(c->s_ctr));
     k_seg_count_big<<<c->sm_count * 16, 128, 0, c->stream>>>(as<double>(B->pts), as<uint2>(c->s_pieces),
                                                             as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_big),
-                                                            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_edge_off));
+                                                            as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_edge_off),
+                                                            as<uint8_t>(c->s_lanes), lane_cap);
     c->launches += 2;
     stage_end(c, 1);
     RRB_CUDA(c, cudaGetLastError());
@@ -645,7 +653,7 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     k_seg_write_big<<<c->sm_count * 16, 128, 0, c->stream>>>(
         as<double>(B->pts), as<uint2>(c->s_pieces), as<double>(B->mtx), flat_sq, as<uint32_t>(c->s_big),
         as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_edge_off), static_cast<uint32_t>(n_edges),
-        as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo);
+        as<Edge>(c->s_edges), as<uint32_t>(c->s_clip), clip_lo, as<uint8_t>(c->s_lanes), lane_cap);
     c->launches += 2;
     stage_end(c, 3);
     const int chunk_rows = 32;
@@ -963,7 +971,7 @@ void set_binning(std::vector<PageGeom>& geom, uint64_t& supers_out) {
 void release_scratch(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pieces, &c->s_clip, &c->s_edge_off, &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks,
-                      &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
+                      &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big, &c->s_lanes, &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo, &c->s_hl_clip};
     for (Scratch* x : all) {
@@ -1376,19 +1384,24 @@ bool page_locked(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
-// Host pages of rrb_render_pages_host: up before the render, down after it.
+// Host pages of rrb_render_pages_host: up before the render (or, with
+// init >= 0, filled with that byte on the device instead), down after it.
 struct HostPages {
     uint8_t* p = nullptr;
     size_t len = 0;
+    int init = -1;
 };
 
 // io (optional): the streamed render also moves the pages. They go up on the
 // copy stream behind the first range's points, and the first composite
-// waits for them; each page goes down as soon as the last range with a path
-// on it has composited, while later ranges render.
+// waits for them (pages filled on the device instead: a fill ahead of the
+// first range); each page goes down on its own stream, beside the uploads,
+// as soon as the last range with a path on it has composited, while later
+// ranges render.
 int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8_t* arena, size_t arena_len,
                  const HostPages* io = nullptr) {
     if (!c->copy_stream) RRB_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    if (io && !c->down_stream) RRB_CUDA(c, cudaStreamCreateWithFlags(&c->down_stream, cudaStreamNonBlocking));
     // Ranges of consecutive paths: a first one of about a tenth of the
     // points (the render starts once its copy lands), then kStreamRanges - 1
     // equal ones (copies run a little faster than renders, so they stay ahead).
@@ -1407,12 +1420,14 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
     for (auto& e : ev) RRB_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     auto done = [&](int rc) {
         cudaStreamSynchronize(c->copy_stream);  // no copy from the caller's memory may outlive the call
+        if (io) cudaStreamSynchronize(c->down_stream);
         for (auto& e : ev) cudaEventDestroy(e);
         return rc;
     };
     // The copies start once the device is done with the previous batch in these buffers.
     RRB_CUDA(c, cudaEventRecord(ev[nr], c->stream));
     RRB_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev[nr], 0));
+    if (io && io->init >= 0) RRB_CUDA(c, cudaMemsetAsync(arena, io->init, io->len, c->stream));
     for (size_t r = 0; r < nr; ++r) {
         const uint64_t a = h->path_pt_off[cut[r]], b = h->path_pt_off[cut[r + 1]];
         if (b > a) {
@@ -1423,7 +1438,7 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
                 return done(set_err(c, RRB_ERR_DEVICE, "point upload failed"));
         }
         if (cudaEventRecord(ev[r], c->copy_stream) != cudaSuccess) return done(set_err(c, RRB_ERR_DEVICE, "event"));
-        if (r == 0 && io) {
+        if (r == 0 && io && io->init < 0) {
             if (cudaMemcpyAsync(arena, io->p, io->len, cudaMemcpyHostToDevice, c->copy_stream) != cudaSuccess ||
                 cudaEventRecord(ev[nr + 1], c->copy_stream) != cudaSuccess)
                 return done(set_err(c, RRB_ERR_DEVICE, "page upload failed"));
@@ -1434,14 +1449,14 @@ int run_streamed(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, uint8
     uint32_t next_down = 0;  // first page not yet on its way down
     auto send_down = [&](uint32_t upto, cudaEvent_t after) -> bool {
         if (!io || next_down >= upto) return true;
-        if (cudaEventRecord(after, c->stream) != cudaSuccess || cudaStreamWaitEvent(c->copy_stream, after, 0) != cudaSuccess)
+        if (cudaEventRecord(after, c->stream) != cudaSuccess || cudaStreamWaitEvent(c->down_stream, after, 0) != cudaSuccess)
             return false;
         for (; next_down < upto; ++next_down) {
             const uint64_t off = h->page_offset[next_down];
             const uint64_t bytes = static_cast<uint64_t>(B->bpp) * h->page_width[next_down] * h->page_height[next_down];
             const uint64_t end = std::min<uint64_t>(off + bytes, io->len);
             if (off < end && cudaMemcpyAsync(io->p + off, arena + off, end - off, cudaMemcpyDeviceToHost,
-                                             c->copy_stream) != cudaSuccess)
+                                             c->down_stream) != cudaSuccess)
                 return false;
         }
         return true;
@@ -1497,7 +1512,8 @@ int run_batch(rrb_ctx* c, const rrb_path_batch_params* h, uint8_t* arena, size_t
     if (streamed) {
         rc = run_streamed(c, h, B, arena, arena_len, io);
     } else {
-        if (io) RRB_CUDA(c, cudaMemcpyAsync(arena, io->p, io->len, cudaMemcpyHostToDevice, c->stream));
+        if (io && io->init >= 0) RRB_CUDA(c, cudaMemsetAsync(arena, io->init, io->len, c->stream));
+        else if (io) RRB_CUDA(c, cudaMemcpyAsync(arena, io->p, io->len, cudaMemcpyHostToDevice, c->stream));
         rc = run_resident(c, B, arena, arena_len, h->rowmap);
         if (io && !rc) RRB_CUDA(c, cudaMemcpyAsync(io->p, arena, io->len, cudaMemcpyDeviceToHost, c->stream));
     }
@@ -1622,7 +1638,7 @@ int rrb_destroy(rrb_ctx* c) {
     cudaStreamSynchronize(c->stream);
     Scratch* all[] = {&c->s_pts, &c->s_flags, &c->s_off, &c->s_rule, &c->s_gray, &c->s_alpha, &c->s_page,
                       &c->s_geom, &c->s_pw, &c->s_ph, &c->s_mtx, &c->s_pieces, &c->s_clip, &c->s_edge_off,
-                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big,
+                      &c->s_edges, &c->s_info, &c->s_rows, &c->s_chunks, &c->s_super_cnt, &c->s_super_list, &c->s_super_start, &c->s_big, &c->s_lanes,
                       &c->s_row_idx, &c->s_spans, &c->s_ovf, &c->s_scratch, &c->s_ctr, &c->s_block, &c->s_stats,
                       &c->s_groups, &c->s_slots, &c->s_path_pieces, &c->s_ovf2, &c->s_run_off, &c->s_runs,
                       &c->s_chunk_path, &c->s_clip_lo};
@@ -1657,6 +1673,7 @@ int rrb_destroy(rrb_ctx* c) {
     for (cudaEvent_t ev : c->free_events) cudaEventDestroy(ev);
     if (c->h_read) cudaFreeHost(c->h_read);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->down_stream) cudaStreamDestroy(c->down_stream);
     cudaStreamDestroy(c->stream);
     delete c;
     return RRB_OK;
@@ -2029,15 +2046,17 @@ int rrb_record_rgb_to_gray(rrb_ctx* c, const rrb_buf* rgb, size_t rgb_offset, co
     return RRB_OK;
 }
 
-int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len) {
+namespace {
+int render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len, int init) {
     if (!c || !p || !host_pages || !p->pages) return RRB_ERR_INVARIANT;
     if (len > p->pages->len) return set_err(c, RRB_ERR_INVARIANT, "host pages larger than the device arena");
+    if (init > 255) return set_err(c, RRB_ERR_INVARIANT, "init_value must be 0..255");
     const rrb_host::DeviceScope dev_scope(c->device);
     int rc = rrb_begin_page(c);
     if (rc) return rc;
     // The pages travel inside the render: overlapped with it when the batch
     // streams (page-locked points), before and after it otherwise.
-    const HostPages io{host_pages, len};
+    const HostPages io{host_pages, len, init < 0 ? -1 : init};
     rc = run_batch(c, p, static_cast<uint8_t*>(p->pages->p), p->pages->len, nullptr, nullptr, false, true, nullptr,
                    nullptr, &io);
     rrb_fence f = 0;
@@ -2045,6 +2064,17 @@ int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* h
     if (rc) return rc;
     if (rc2) return rc2;
     return rrb_wait_page(c, f, 0) ? RRB_ERR_DEVICE : (cudaStreamSynchronize(c->stream) == cudaSuccess ? RRB_OK : RRB_ERR_DEVICE);
+}
+}  // namespace
+
+int rrb_render_pages_host(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len) {
+    return render_pages_host(c, p, host_pages, len, -1);
+}
+
+int rrb_render_pages_host_init(rrb_ctx* c, const rrb_path_batch_params* p, uint8_t* host_pages, size_t len,
+                               int init_value) {
+    if (init_value < 0) return c ? set_err(c, RRB_ERR_INVARIANT, "init_value must be 0..255") : RRB_ERR_INVARIANT;
+    return render_pages_host(c, p, host_pages, len, init_value);
 }
 
 }  // extern "C"

@@ -219,13 +219,15 @@ __host__ __device__ __forceinline__ void edge_entry(const Edge& e, int32_t r, in
         return;
     }
     long long k = static_cast<long long>(r) - e.row0;
-    int32_t x1v = sat_i64_to_i32(static_cast<long long>(e.b) + k * e.dfp);
+    // The exact sums after k and k - 1 steps (|k * dfp| < 2^62: no overflow).
+    const long long s1 = static_cast<long long>(e.b) + k * e.dfp;
+    int32_t x1v = sat_i64_to_i32(s1);
     int32_t px1 = min(max(x1v, e.cmin), e.cmax) >> 16;
     int32_t px0;
     if (k == 0) {
         px0 = e.a;
     } else {
-        int32_t x0v = sat_i64_to_i32(static_cast<long long>(e.b) + (k - 1) * e.dfp);
+        int32_t x0v = sat_i64_to_i32(s1 - e.dfp);
         px0 = min(max(x0v, e.cmin), e.cmax) >> 16;
     }
     lo = min(px0, px1);

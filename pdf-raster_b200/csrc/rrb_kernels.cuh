@@ -392,9 +392,12 @@ __device__ __forceinline__ bool curve_root_in_range(const CurveNode& r) {
 
 // One warp per big curve (k_seg_count's big_list): each lane counts the
 // leaves of its subtree (curve_lane_flatten); the sum is the curve's count.
+constexpr int CURVE_LANES = 32;  // lanes per big curve; each lane's count is at most CURVE_LANE_SLOTS
+
 __global__ void k_seg_count_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
                                 const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
-                                const BatchCounters* __restrict__ ctr, uint32_t* __restrict__ counts) {
+                                const BatchCounters* __restrict__ ctr, uint32_t* __restrict__ counts,
+                                uint8_t* __restrict__ lane_cnt, uint32_t lane_cap) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -408,6 +411,7 @@ __global__ void k_seg_count_big(const double* __restrict__ pts, const uint2* __r
         double cx, cy;
         int c = curve_root_in_range(root) ? curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, none)
                                           : curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, none);
+        if (q < lane_cap) lane_cnt[static_cast<uint64_t>(q) * CURVE_LANES + lane] = static_cast<uint8_t>(c);
         for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
         if (lane == 0) counts[s] = static_cast<uint32_t>(c);
     }
@@ -455,14 +459,16 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
     }
 }
 
-// One warp per big curve: each lane counts its subtree's leaves, an
-// exclusive scan over the lanes places them, and each lane writes the edge
-// records of its leaves from its subtree's start point on.
+// One warp per big curve: each lane's count of its subtree's leaves (kept by
+// k_seg_count_big for the first lane_cap curves, counted again for the
+// rest), an exclusive scan over the lanes places them, and each lane writes
+// the edge records of its leaves from its subtree's start point on.
 __global__ void k_seg_write_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
                                 const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
                                 const BatchCounters* __restrict__ ctr, const uint32_t* __restrict__ edge_off,
                                 uint32_t edge_cap, Edge* __restrict__ edges,
-                                const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo) {
+                                const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo,
+                                const uint8_t* __restrict__ lane_cnt, uint32_t lane_cap) {
     __shared__ double m[6];
     if (threadIdx.x < 6) m[threadIdx.x] = mtx[threadIdx.x];
     __syncthreads();
@@ -476,9 +482,11 @@ __global__ void k_seg_write_big(const double* __restrict__ pts, const uint2* __r
         const int32_t chi = static_cast<int32_t>(slot_clip_hi[s]);
         const int32_t clo = slot_clip_lo ? static_cast<int32_t>(slot_clip_lo[s]) : 0;
         auto none = [](double, double) {};
-        double cx, cy;
-        const int mine = in_range ? curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, none)
-                                  : curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, none);
+        double cx = 0.0, cy = 0.0;
+        int mine;
+        if (q < lane_cap) mine = lane_cnt[static_cast<uint64_t>(q) * CURVE_LANES + lane];
+        else mine = in_range ? curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, none)
+                             : curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, none);
         int incl = mine;
         for (int o = 1; o < 32; o <<= 1) {
             const int t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -492,9 +500,10 @@ __global__ void k_seg_write_big(const double* __restrict__ pts, const uint2* __r
             cy = fy;
         };
         if (mine) {
-            double sx0, sy0;
-            if (in_range) curve_lane_flatten<true>(root, lane, flat_sq, sx0, sy0, emit);
-            else curve_lane_flatten<false>(root, lane, flat_sq, sx0, sy0, emit);
+            // The flatten sets (cx, cy) to the lane's start point before its
+            // first leaf is emitted.
+            if (in_range) curve_lane_flatten<true>(root, lane, flat_sq, cx, cy, emit);
+            else curve_lane_flatten<false>(root, lane, flat_sq, cx, cy, emit);
         }
     }
 }
@@ -996,22 +1005,14 @@ __host__ __device__ __forceinline__ int sweep_cells(const int (&n)[4], Bound bou
 template <int K, int LS, int GS = 1>
 __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t hi, int32_t r, bool valid,
                                           const Edge* __restrict__ edges, const int32_t* __restrict__ gmin,
-                                          const int32_t* __restrict__ gmax, int32_t (*sedge)[32 * GS], int32_t* x0s,
+                                          const int32_t* __restrict__ gmax, Edge* sedge, int32_t* x0s,
                                           int32_t* x1s, int32_t* cns, int lane) {
     static_assert(GS == 1 || GS == 2, "one or two staged edge groups");
     int n = 0;
     bool has_last = false;
     int32_t lx0 = 0, lx1 = 0, lc = 0;
     auto fold = [&](int bb) {
-        Edge E;
-        E.row0 = sedge[0][bb];
-        E.row1 = sedge[1][bb];
-        E.flags = sedge[2][bb];
-        E.a = sedge[3][bb];
-        E.b = sedge[4][bb];
-        E.dfp = sedge[5][bb];
-        E.cmin = sedge[6][bb];
-        E.cmax = sedge[7][bb];
+        const Edge E = sedge[bb];  // two 16-byte shared loads
         int32_t elo, ehi, ec;
         edge_entry(E, r, elo, ehi, ec);
         if (has_last && sat_inc(lx1) >= elo && lx0 <= sat_inc(ehi)) {
@@ -1059,14 +1060,7 @@ __device__ __forceinline__ int gather_row(const PathInfo& P, int32_t lo, int32_t
                 uint32_t rows_of_edge = 0;
                 if (hit) {
                     const int q = 32 * s + lane;
-                    sedge[0][q] = e.row0;
-                    sedge[1][q] = e.row1;
-                    sedge[2][q] = e.flags;
-                    sedge[3][q] = e.a;
-                    sedge[4][q] = e.b;
-                    sedge[5][q] = e.dfp;
-                    sedge[6][q] = e.cmin;
-                    sedge[7][q] = e.cmax;
+                    sedge[q] = e;
                     const int32_t ra = max(e.row0, lo) - lo, rb = min(e.row1, hi) - lo;
                     rows_of_edge = (0xffffffffu >> (31 - rb)) & (0xffffffffu << ra);
                 }
@@ -1173,7 +1167,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_rows(
     auto sx0 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem);
     auto sx1 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + LIST);
     auto scn = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + 2 * LIST);
-    auto sedge = reinterpret_cast<int32_t (*)[8][64]>(rows_smem + 3 * LIST);
+    auto sedge = reinterpret_cast<Edge (*)[64]>(rows_smem + 3 * LIST);  // 16-byte aligned: LIST is a multiple of 4
     auto sns = reinterpret_cast<int32_t (*)[32]>(rows_smem + 3 * LIST + WARPS * 8 * 64);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
@@ -1541,7 +1535,7 @@ __global__ void __launch_bounds__(MID_WARPS * 32) k_groups_mid(
     __shared__ int32_t sx0[MID_WARPS][MID_K * 4];
     __shared__ int32_t sx1[MID_WARPS][MID_K * 4];
     __shared__ int32_t scn[MID_WARPS][MID_K * 4];
-    __shared__ int32_t sedge[MID_WARPS][8][32];
+    __shared__ Edge sedge[MID_WARPS][32];
     __shared__ int32_t sns[MID_WARPS][4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n_ovf = min(ctr->ovf_count, ovf_cap);

@@ -15,6 +15,7 @@
 // tile shape of least predicted total time (autotuner table as fallback).
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -47,6 +48,7 @@ struct Request {
 };
 
 constexpr uint32_t kTiles[3][2] = {{16, 16}, {32, 32}, {64, 16}};
+constexpr size_t kStageThreads = 8;  // host threads per worker that copy a batch's requests into staging
 
 }  // namespace
 
@@ -78,11 +80,14 @@ namespace {
 
 // Device bytes a request needs while it is on the device: its pages, its
 // inputs, and the intermediate edge / row data (about 3.5 edges of 32 B per
-// input point on curve-heavy content, and a few bytes per pixel row).
+// input point on curve-heavy content, and a few bytes per pixel row), plus
+// the 32 lane counts kept per curve flattened by a warp (at most one curve
+// per point, at most 4 Mi curves).
 uint64_t estimate_bytes(const rrb_path_batch_params& p) {
     uint64_t pages = 0;
     for (uint32_t i = 0; i < p.n_pages; ++i) pages += static_cast<uint64_t>(p.page_width[i]) * p.page_height[i];
-    return 3 * pages + p.n_pts * (17 + 112) + p.n_paths * 256 + (1u << 20);
+    return 3 * pages + p.n_pts * (17 + 112) + std::min<uint64_t>(p.n_pts, 1ull << 22) * 32 + p.n_paths * 256 +
+           (1u << 20);
 }
 
 // A growable array in page-locked host memory (rrb_alloc_host_pinned): the
@@ -117,6 +122,12 @@ struct PinnedVec {
         return true;
     }
     bool push(T v) { return append(&v, 1); }
+    // Size n (contents past the old size undefined): callers then fill it.
+    bool resize(size_t k) {
+        if (!reserve(k)) return false;
+        n = k;
+        return true;
+    }
     void clear() { n = 0; }
     T* data() { return p; }
     size_t size() const { return n; }
@@ -201,32 +212,60 @@ void worker(rrb_server* s, int wi) {
         auto ns_since = [](Clock::time_point a) {
             return static_cast<uint64_t>(std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - a).count());
         };
-        // Concatenate the requests into one batch over one device arena.
-        st.pts.clear(); st.flags.clear(); st.rule.clear(); st.gray.clear(); st.alpha.clear();
-        st.off.clear(); st.page_off.clear(); st.path_page.clear(); st.pw.clear(); st.ph.clear();
-        std::vector<uint64_t> req_arena_off;
+        // Concatenate the requests into one batch over one device arena:
+        // each request's place in the staging arrays first, then the copies,
+        // requests spread over host threads (the batch's points are most of
+        // its bytes, and one thread's memcpy is well below the host link).
+        const size_t nb = batch.size();
+        std::vector<uint64_t> req_arena_off(nb), req_pt(nb + 1), req_path(nb + 1), req_page(nb + 1);
         uint64_t arena_len = 0;
-        uint32_t page_base = 0;
-        bool staged = st.off.push(0);
-        for (Request* r : batch) {
-            const rrb_path_batch_params& p = r->p;
-            req_arena_off.push_back(arena_len);
-            const uint64_t pt_base = st.flags.size();
-            staged = staged && st.pts.append(p.pts, 2 * p.n_pts) && st.flags.append(p.flags, p.n_pts) &&
-                     st.off.reserve(st.off.size() + p.n_paths) && st.path_page.reserve(st.path_page.size() + p.n_paths);
-            if (!staged) break;
-            for (uint64_t i = 0; i < p.n_paths; ++i) {
-                st.off.p[st.off.n++] = pt_base + p.path_pt_off[i + 1];
-                st.path_page.p[st.path_page.n++] = page_base + p.path_page[i];
-            }
-            staged = st.rule.append(p.fill_rule, p.n_paths) && st.gray.append(p.gray, p.n_paths) &&
-                     st.alpha.append(p.alpha, p.n_paths);
-            for (uint32_t i = 0; i < p.n_pages && staged; ++i)
-                staged = st.pw.push(p.page_width[i]) && st.ph.push(p.page_height[i]) &&
-                         st.page_off.push(arena_len + p.page_offset[i]);
-            if (!staged) break;
-            arena_len += (r->out_len + 255) & ~size_t(255);
-            page_base += p.n_pages;
+        for (size_t k = 0; k < nb; ++k) {
+            const rrb_path_batch_params& p = batch[k]->p;
+            req_arena_off[k] = arena_len;
+            req_pt[k + 1] = req_pt[k] + p.n_pts;
+            req_path[k + 1] = req_path[k] + p.n_paths;
+            req_page[k + 1] = req_page[k] + p.n_pages;
+            arena_len += (batch[k]->out_len + 255) & ~size_t(255);
+        }
+        bool staged = st.pts.resize(2 * req_pt[nb]) && st.flags.resize(req_pt[nb]) &&
+                      st.off.resize(req_path[nb] + 1) && st.path_page.resize(req_path[nb]) &&
+                      st.rule.resize(req_path[nb]) && st.gray.resize(req_path[nb]) &&
+                      st.alpha.resize(req_path[nb]) && st.pw.resize(req_page[nb]) && st.ph.resize(req_page[nb]) &&
+                      st.page_off.resize(req_page[nb]);
+        if (staged) {
+            st.off.p[0] = 0;
+            auto copy_req = [&](size_t k) {
+                const rrb_path_batch_params& p = batch[k]->p;
+                const uint64_t pt0 = req_pt[k], pa0 = req_path[k], pg0 = req_page[k];
+                if (p.n_pts) {
+                    std::memcpy(st.pts.p + 2 * pt0, p.pts, 2 * p.n_pts * sizeof(double));
+                    std::memcpy(st.flags.p + pt0, p.flags, p.n_pts);
+                }
+                for (uint64_t i = 0; i < p.n_paths; ++i) {
+                    st.off.p[pa0 + i + 1] = pt0 + p.path_pt_off[i + 1];
+                    st.path_page.p[pa0 + i] = static_cast<uint32_t>(pg0) + p.path_page[i];
+                }
+                if (p.n_paths) {
+                    std::memcpy(st.rule.p + pa0, p.fill_rule, p.n_paths);
+                    std::memcpy(st.gray.p + pa0, p.gray, p.n_paths);
+                    std::memcpy(st.alpha.p + pa0, p.alpha, p.n_paths);
+                }
+                for (uint32_t i = 0; i < p.n_pages; ++i) {
+                    st.pw.p[pg0 + i] = p.page_width[i];
+                    st.ph.p[pg0 + i] = p.page_height[i];
+                    st.page_off.p[pg0 + i] = req_arena_off[k] + p.page_offset[i];
+                }
+            };
+            // Threads take requests in turn; a small batch stays on this thread.
+            const size_t nt = std::min<size_t>({nb, kStageThreads, req_pt[nb] / (1u << 18) + 1});
+            std::atomic<size_t> next{0};
+            auto run = [&]() {
+                for (size_t k = next.fetch_add(1); k < nb; k = next.fetch_add(1)) copy_req(k);
+            };
+            std::vector<std::thread> helpers;
+            for (size_t t = 1; t < nt; ++t) helpers.emplace_back(run);
+            run();
+            for (std::thread& h : helpers) h.join();
         }
         int rc = staged ? RRB_OK : RRB_ERR_OUT_OF_MEMORY;
         if (!rc && arena_len > arena_cap) {
@@ -265,11 +304,11 @@ void worker(rrb_server* s, int wi) {
         if (!rc) rc = rrb_wait_page(c, f, 0);
         const uint64_t render = ns_since(t_render);
         const auto t_down = Clock::now();
-        for (size_t k = 0; k < batch.size() && !rc; ++k) {
-            rrb_fence df = 0;
+        // Every request's pages go down in stream order; one wait for the last.
+        rrb_fence df = 0;
+        for (size_t k = 0; k < batch.size() && !rc; ++k)
             rc = rrb_download_async(c, arena, req_arena_off[k], batch[k]->out, batch[k]->out_len, &df);
-            if (!rc) rc = rrb_wait_download(c, df);
-        }
+        if (!rc && df) rc = rrb_wait_download(c, df);
         const auto t_done = Clock::now();
         const uint64_t down = ns_since(t_down);
         {

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_static_rows(const PathInfo* 
     __shared__ int32_t sx0[kRowWarps][kRowK * 4];
     __shared__ int32_t sx1[kRowWarps][kRowK * 4];
     __shared__ int32_t scn[kRowWarps][kRowK * 4];
-    __shared__ int32_t sedge[kRowWarps][8][32];
+    __shared__ Edge sedge[kRowWarps][32];
     __shared__ int32_t sns[kRowWarps][4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const PathInfo P = info[0];

@@ -393,9 +393,16 @@ class B200Backend:
     def record_path_batch(self, params: PathBatchParams):
         self._chk(lib().rrb_record_path_batch(self._h, C.byref(params)))
 
-    def render_pages_host(self, params: PathBatchParams, host_pages: np.ndarray):
+    def render_pages_host(self, params: PathBatchParams, host_pages: np.ndarray, init: int | None = None):
+        """Render onto host pages in one call: their content goes up, the pages come back. With
+        init (0..255) the pages start as that byte, filled on the device (no page upload)."""
         assert host_pages.dtype == np.uint8 and host_pages.flags["C_CONTIGUOUS"]
-        self._chk(lib().rrb_render_pages_host(self._h, C.byref(params), host_pages.ctypes.data, host_pages.nbytes))
+        if init is None:
+            self._chk(lib().rrb_render_pages_host(self._h, C.byref(params), host_pages.ctypes.data,
+                                                  host_pages.nbytes))
+        else:
+            self._chk(lib().rrb_render_pages_host_init(self._h, C.byref(params), host_pages.ctypes.data,
+                                                       host_pages.nbytes, int(init)))
 
     def record_fill_buffer(self, buf: DeviceBuffer, value: int, offset: int = 0, length: int | None = None):
         n = buf.size - offset if length is None else length

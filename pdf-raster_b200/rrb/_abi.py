@@ -218,6 +218,7 @@ SIGNATURES = {
     "rrb_last_stage_times": (C.c_int, [VP, C.POINTER(StageTime), C.c_int, C.POINTER(C.c_int)]),
     "rrb_validate_path_batch": (C.c_int, [C.POINTER(PathBatchParams), C.c_size_t, C.c_char_p, C.c_size_t]),
     "rrb_render_pages_host": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t]),
+    "rrb_render_pages_host_init": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t, C.c_int]),
     "rrb_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(VP)]),
     "rrb_server_submit": (C.c_int, [VP, C.POINTER(PathBatchParams), VP, C.c_size_t, C.c_uint8,
                                     C.POINTER(C.c_uint64)]),

@@ -51,6 +51,20 @@ def test_streamed_batch_matches_oracle(backend, oracle, rrb_lib, name):
         host2 = s.blank_arena()
         backend.render_pages_host(q, host2)
         assert np.array_equal(host2, exp)
+        # Pages filled on the device (init 255) instead of uploaded: the host
+        # buffer's old page content is ignored, streamed and from pageable
+        # memory (arena bytes outside every page are not written back).
+        def pages_equal(got):
+            return all(np.array_equal(got[o:o + w * h], exp[o:o + w * h])
+                       for o, w, h in zip(s.page_offset.tolist(), s.page_width.tolist(), s.page_height.tolist()))
+
+        host[:] = 7
+        backend.render_pages_host(p, host, init=255)
+        assert backend.last_batch_stats()["waves"] > 1
+        assert pages_equal(np.asarray(host))
+        host2[:] = 7
+        backend.render_pages_host(q, host2, init=255)
+        assert pages_equal(host2)
     finally:
         backend.free_device(pages)
         for b in bufs:
