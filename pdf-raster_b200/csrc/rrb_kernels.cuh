@@ -1930,6 +1930,9 @@ __device__ __forceinline__ void composite_path_rows(const HitInfo& h, const HitR
 #pragma unroll
     for (int it = 0; it < ITERS; ++it) {
         const uint2 ix = hr.ix[it];
+        // No cells in this warp's row(s) of the tile: nothing to do (a vote,
+        // so the shuffles below stay warp-uniform when a warp holds 2 rows).
+        if (__all_sync(0xffffffffu, ix.y == 0u)) continue;
         int32_t cov[L::PX];
 #pragma unroll
         for (int q = 0; q < L::PX; ++q) cov[q] = 0;
@@ -2090,6 +2093,7 @@ __device__ __forceinline__ void composite_box(const HitInfo& h, int rowmap, int 
         const int y = Y0 + (w * L::RPW + slot) + it * L::NW * L::RPW;
         const int32_t r = rowmap ? 16 * y + 12 : 4 * y;
         const int32_t cy = (y >= h.py0 && y <= h.py1) ? max(0, min(r + 4, h.g1 + 1) - max(r, h.g0)) : 0;
+        if (cy == 0) continue;  // the box misses this row
 #pragma unroll
         for (int q = 0; q < L::PX; ++q) {
             const int32_t cov = cx[q] * cy;
