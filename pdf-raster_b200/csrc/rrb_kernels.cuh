@@ -394,7 +394,20 @@ __device__ __forceinline__ bool curve_root_in_range(const CurveNode& r) {
 // leaves of its subtree (curve_lane_flatten); the sum is the curve's count.
 constexpr int CURVE_LANES = 32;  // lanes per big curve; each lane's count is at most CURVE_LANE_SLOTS
 
-__global__ void k_seg_count_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
+// The big-curve kernels run 128-thread CTAs; RRB_BIG_CURVE_CTAS > 0 asks the
+// compiler to fit that many per SM (a register budget). 8 (64 registers)
+// took the mixed batch's flatten + records from 15.9 to 14.8 ms against the
+// unbounded 96 registers; 6 (80 registers) gave 15.4.
+#ifndef RRB_BIG_CURVE_CTAS
+#define RRB_BIG_CURVE_CTAS 8
+#endif
+#if RRB_BIG_CURVE_CTAS > 0
+#define RRB_BIG_CURVE_BOUNDS __launch_bounds__(128, RRB_BIG_CURVE_CTAS)
+#else
+#define RRB_BIG_CURVE_BOUNDS
+#endif
+
+__global__ void RRB_BIG_CURVE_BOUNDS k_seg_count_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
                                 const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
                                 const BatchCounters* __restrict__ ctr, uint32_t* __restrict__ counts,
                                 uint8_t* __restrict__ lane_cnt, uint32_t lane_cap) {
@@ -463,7 +476,7 @@ __global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restr
 // k_seg_count_big for the first lane_cap curves, counted again for the
 // rest), an exclusive scan over the lanes places them, and each lane writes
 // the edge records of its leaves from its subtree's start point on.
-__global__ void k_seg_write_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
+__global__ void RRB_BIG_CURVE_BOUNDS k_seg_write_big(const double* __restrict__ pts, const uint2* __restrict__ pieces,
                                 const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ big_list,
                                 const BatchCounters* __restrict__ ctr, const uint32_t* __restrict__ edge_off,
                                 uint32_t edge_cap, Edge* __restrict__ edges,
