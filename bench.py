@@ -127,7 +127,7 @@ GLYPH_DRAM_BYTES_PER_SEGMENT = {
 # k_composite<128, 16> on page 0 of the batch alone (3508x4961, 17,589 paths;
 # its cells and row index larger than L2), scaled to a launch by its pixels.
 MIXED_DRAM_BYTES_PER_PIXEL = {
-    "composite": (92_163_328 + 14_567_936) / (3508 * 4961),
+    "composite": (92_113_664 + 15_584_256) / (3508 * 4961),
 }
 
 

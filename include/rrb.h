@@ -407,8 +407,10 @@ int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, ch
  * shape by trial: its first renders run 64x16, 128x16 and 128x32, each with both
  * row-stage shapes, and it keeps the fastest (by CUDA events; renders that
  * grew scratch are repeated). 2 = every batch uses tile_w x tile_h (resident
- * batches still try both row-stage shapes). The default is 1 with 64x16 for
- * batches that are not resident. Giving a tile shape without auto_tile sets 2. */
+ * batches still try both row-stage shapes). With 1, batches that are not
+ * resident use the tile shape the context's last resident batch settled on
+ * (64x16 before any, and again after each rrb_set_tuning). The default is 1.
+ * Giving a tile shape without auto_tile sets 2. */
 typedef struct {
     uint32_t tile_w, tile_h;
     uint32_t rows_per_chunk;    /* AA rows per row-kernel work item: 32 */

@@ -103,6 +103,10 @@ struct rrb_ctx {
     cudaStream_t copy_stream = nullptr;       // streamed batches: point uploads ahead of the render
     cudaStream_t down_stream = nullptr;       // host page renders: page downloads beside the uploads
     uint64_t tuning_epoch = 0;                // bumped by rrb_set_tuning: resident batches re-run their trials
+    // With automatic tiles: the tile shape the last resident batch settled on
+    // by its trials (0: none yet, 64x16), the default of batches uploaded per
+    // call on this context until another batch settles or the tuning changes.
+    uint32_t settled_tw = 0, settled_th = 0;
     cudaEvent_t trial_ev[2] = {nullptr, nullptr};  // timing of a resident batch's trial render
 };
 
@@ -209,6 +213,32 @@ int read_back(rrb_ctx* c, const void* dev, size_t bytes) {
 bool valid_tile(uint32_t w, uint32_t h) {
     return (w == 16 && h == 16) || (w == 32 && h == 32) || (w == 64 && h == 16) || (w == 128 && h == 16) ||
            (w == 128 && h == 32);
+}
+
+// The kernels a resident batch's trials choose between, loaded when the
+// context is made: with CUDA's lazy module loading the first launch of a
+// kernel also loads it, and that time would land inside the first trial
+// render that uses it, making that tile or row shape look slower.
+void preload_trial_kernels() {
+    cudaFuncAttributes a{};
+#define RRB_PRELOAD(...) cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(__VA_ARGS__))
+#define RRB_PRELOAD_COMP(TW, TH)                      \
+    do {                                              \
+        RRB_PRELOAD(k_composite<TW, TH, false, false>); \
+        RRB_PRELOAD(k_composite<TW, TH, false, true>);  \
+        RRB_PRELOAD(k_composite<TW, TH, true, false>);  \
+        RRB_PRELOAD(k_composite<TW, TH, true, true>);   \
+    } while (0)
+    RRB_PRELOAD_COMP(16, 16);
+    RRB_PRELOAD_COMP(32, 32);
+    RRB_PRELOAD_COMP(64, 16);
+    RRB_PRELOAD_COMP(128, 16);
+    RRB_PRELOAD_COMP(128, 32);
+    RRB_PRELOAD(k_rows<KCAP, ROWS_WARPS>);
+    RRB_PRELOAD(k_rows<KCAP_WIDE, 4>);
+#undef RRB_PRELOAD_COMP
+#undef RRB_PRELOAD
+    cudaGetLastError();
 }
 
 int launch_composite(rrb_ctx* c, int tw, int th, int grid, const PathInfo* info, const PageGeom* geom,
@@ -551,8 +581,9 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
     if (B->n_paths == 0) return RRB_OK;
     if (B->arena_need > arena_len) return set_err(c, RRB_ERR_INVARIANT, "page extends past the page buffer");
     if (rowmap < 0 || rowmap > 1) return set_err(c, RRB_ERR_INVARIANT, "rowmap must be 0 or 1");
-    const uint32_t tw = B->tile_w ? B->tile_w : (c->tuning.tile_w ? c->tuning.tile_w : 64);
-    const uint32_t th = B->tile_h ? B->tile_h : (c->tuning.tile_h ? c->tuning.tile_h : 16);
+    const bool settled = c->tuning.auto_tile == 1 && c->settled_tw;
+    const uint32_t tw = B->tile_w ? B->tile_w : settled ? c->settled_tw : (c->tuning.tile_w ? c->tuning.tile_w : 64);
+    const uint32_t th = B->tile_h ? B->tile_h : settled ? c->settled_th : (c->tuning.tile_h ? c->tuning.tile_h : 16);
     c->stats.tile_w = tw;
     c->stats.tile_h = th;
     c->stats.row_shape = B->row_shape;
@@ -1100,7 +1131,11 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
         B->trial = 0;
         const uint32_t cw = c->tuning.tile_w ? c->tuning.tile_w : 64, ch = c->tuning.tile_h ? c->tuning.tile_h : 16;
         if (c->tuning.auto_tile == 1) {
-            const uint32_t shapes[3][2] = {{64u, 16u}, {128u, 16u}, {128u, 32u}};
+            // The shape the context last settled on goes first: a batch
+            // uploaded per call renders once, with the first trial's shapes.
+            uint32_t shapes[3][2] = {{64u, 16u}, {128u, 16u}, {128u, 32u}};
+            for (int k = 1; k < 3; ++k)
+                if (shapes[k][0] == c->settled_tw && shapes[k][1] == c->settled_th) std::swap(shapes[0], shapes[k]);
             for (const auto& t : shapes)
                 for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({t[0], t[1], rs, 0.f});
         } else {
@@ -1139,6 +1174,10 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
             B->tile_w = B->trials[best].tw;
             B->tile_h = B->trials[best].th;
             B->row_shape = B->trials[best].rs;
+            if (c->tuning.auto_tile == 1) {
+                c->settled_tw = B->tile_w;
+                c->settled_th = B->tile_h;
+            }
         }
     }
     settled();
@@ -1624,6 +1663,7 @@ int rrb_init(int device, uint64_t mem_budget_bytes, rrb_ctx** out) {
     }
     c->tmp_batch = new rrb_batch();
     c->wave_batch = new rrb_batch();
+    preload_trial_kernels();
     c->tuning.tile_w = 64;
     c->tuning.tile_h = 16;
     c->tuning.rows_per_chunk = 32;
@@ -1843,6 +1883,7 @@ int rrb_set_tuning(rrb_ctx* c, const rrb_tuning* t) {
     else if (t->tile_w || t->tile_h) c->tuning.auto_tile = 2;  // an explicit tile shape
     if (t->wave_points != 0xFFFFFFFFu) c->tuning.wave_points = t->wave_points;  // all ones: keep
     ++c->tuning_epoch;
+    c->settled_tw = c->settled_th = 0;
     return RRB_OK;
 }
 

@@ -101,6 +101,20 @@ def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
         assert {(64, 16, 0), (64, 16, 1), (128, 16, 0), (128, 16, 1), (128, 32, 0), (128, 32, 1)} <= seen
         assert st["trials_left"] == 0 and st["host_syncs"] == 1  # settled and replaying
         assert (st["tile_w"], st["tile_h"]) in {(64, 16), (128, 16), (128, 32)}
+        # A batch uploaded per call on this context then takes the settled tile shape.
+        settled = (st["tile_w"], st["tile_h"])
+        keep = []
+        p = rrb_lib.batch_params(s.pts, s.flags, s.path_pt_off, s.fill_rule, s.gray, s.alpha, s.path_page,
+                                 s.page_width, s.page_height, s.page_offset, pages, keep=keep)
+        backend.begin_page()
+        backend.record_fill_buffer(pages, 255)
+        backend.record_path_batch(p)
+        backend.wait_page(backend.submit_page())
+        st2 = backend.last_batch_stats()
+        assert (st2["tile_w"], st2["tile_h"]) == settled
+        got = np.empty(s.arena_bytes, np.uint8)
+        backend.wait_download(backend.download_async(pages, got))
+        assert np.array_equal(got, exp)
     finally:
         batch.free()
         backend.set_tuning(64, 16, auto_tile=True)
