@@ -131,6 +131,13 @@ MIXED_DRAM_BYTES_PER_PIXEL = {
 }
 
 
+# Row-stage shapes (rrb_batch_stats.row_shape): list entries per AA row x
+# warps per block x 32-edge groups staged per warp.
+ROW_STAGES = ["12 entries x 8 warps, 512 edges staged per block", "16 entries x 4 warps, 256 edges per block",
+              "12 entries x 8 warps, 256 edges per block", "8 entries x 16 warps, 1024 edges per block",
+              "16 entries x 4 warps, 128 edges per block"]
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -550,7 +557,7 @@ def run_rrb(args, rank, local, world):
                        "rowmap": ["documented", "as_shipped"][args.rowmap],
                        "tile": f"{stats['tile_w']}x{stats['tile_h']} (chosen by trial among 64x16, 128x16 and 128x32)"
                                if tuning.auto_tile == 1 else f"{stats['tile_w']}x{stats['tile_h']}",
-                       "row_stage": "12 entries x 8 warps" if stats["row_shape"] == 0 else "16 entries x 4 warps",
+                       "row_stage": ROW_STAGES[int(stats["row_shape"])],
                        "l2": f"inputs larger than L2 ({16 * scene.n_pts / 1e6:.0f} MB of path points)",
                        "parallelism": (f"pages sharded over {world} GPUs" if sharded
                                        else f"replicas x{world} (the page on every GPU)")},

@@ -404,10 +404,11 @@ int rrb_validate_path_batch(const rrb_path_batch_params* p, size_t pages_len, ch
 /* Per-batch tuning knobs (tile shape etc.); 0 fields keep the current
  * values. Tile shapes accepted: 16x16, 32x32, 64x16, 128x16, 128x32.
  * auto_tile: 1 = a device-resident batch (rrb_record_batch) chooses its tile
- * shape by trial: its first renders run 64x16, 128x16 and 128x32, each with both
- * row-stage shapes, and it keeps the fastest (by CUDA events; renders that
- * grew scratch are repeated). 2 = every batch uses tile_w x tile_h (resident
- * batches still try both row-stage shapes). With 1, batches that are not
+ * shape by trial: its first renders run 64x16, 128x16 and 128x32 with row-stage
+ * shape 0, then the other row-stage shapes with the fastest of those tiles, and
+ * it keeps the fastest pair (by CUDA events; renders that grew scratch are
+ * repeated). 2 = every batch uses tile_w x tile_h (resident batches still try
+ * every row-stage shape). With 1, batches that are not
  * resident use the tile shape the context's last resident batch settled on
  * (64x16 before any, and again after each rrb_set_tuning). The default is 1.
  * Giving a tile shape without auto_tile sets 2. */
@@ -435,7 +436,9 @@ typedef struct {
     uint64_t row_groups;                    /* pixel-row index entries written by the row stage */
     uint64_t host_syncs;                    /* times the call waited on its stream for a device-side size */
     uint64_t tile_w, tile_h;                /* tile shape of the render */
-    uint64_t row_shape;                     /* row-stage shape: 0 = 12 entries x 8 warps, 1 = 16 x 4 */
+    uint64_t row_shape;                     /* row-stage shape (entries per AA row x warps x edge groups per
+                                               warp): 0 = 12x8x2, 1 = 16x4x2, 2 = 12x8x1, 3 = 8x16x2,
+                                               4 = 16x4x1 */
     uint64_t trials_left;                   /* resident batches: tuning trials still to run (0: settled) */
 } rrb_batch_stats;
 int rrb_last_batch_stats(rrb_ctx* ctx, rrb_batch_stats* out);

@@ -45,7 +45,11 @@ struct Scratch {
 };
 
 constexpr int KCAP = 12;        // merged Intersect entries per AA row kept in shared memory
-constexpr int KCAP_WIDE = 16;   // the same for the 4-warp row-stage shape
+constexpr int KCAP_WIDE = 16;   // the same for the 4-warp row-stage shapes
+// Row-stage shapes (rrb_batch::row_shape): entries per AA row kept in shared
+// memory x warps per block x 32-edge groups a warp stages at once; a block
+// stages warps x groups x 32 edges (512, 256, 256, 1024, 128).
+constexpr int kRowShapes = 5;
 constexpr uint64_t kLaneCountCurves = 1ull << 22;  // big curves whose lane counts are kept (128 MiB)
 constexpr int SUPER = 256;      // supertile edge in pixels (a multiple of every tile shape)
 
@@ -236,6 +240,9 @@ void preload_trial_kernels() {
     RRB_PRELOAD_COMP(128, 32);
     RRB_PRELOAD(k_rows<KCAP, ROWS_WARPS>);
     RRB_PRELOAD(k_rows<KCAP_WIDE, 4>);
+    RRB_PRELOAD(k_rows<KCAP, ROWS_WARPS, 1>);
+    RRB_PRELOAD(k_rows<8, 16>);
+    RRB_PRELOAD(k_rows<KCAP_WIDE, 4, 1>);
 #undef RRB_PRELOAD_COMP
 #undef RRB_PRELOAD
     cudaGetLastError();
@@ -391,11 +398,12 @@ struct rrb_batch {
     uint64_t plan_wave_points = 0;
     // Per wave of `plan`: the sizes its last render found on the device.
     std::vector<WaveSizes> sizes;
-    // Row-stage shape (0: 12 entries x 8 warps, 1: 16 entries x 4 warps) and
-    // tile shape (0 x 0: the context's) of the next render. A resident batch
-    // renders once with each candidate pair (both row shapes; with automatic
-    // tiles both of 64x16 and 128x16), timed by events on its stream, repeats
-    // a trial whose render grew scratch, and keeps the fastest pair.
+    // Row-stage shape (kRowShapes of them, 0 the default) and tile shape (0 x 0:
+    // the context's) of the next render. A resident batch renders once per
+    // trial, timed by events on its stream (a trial whose render grew scratch
+    // is repeated): first each candidate tile shape with row shape 0 (with
+    // automatic tiles 64x16, 128x16 and 128x32; else the context's), then the
+    // other row shapes with the fastest tile; it keeps the fastest pair.
     uint8_t row_shape = 0;
     uint32_t tile_w = 0, tile_h = 0;
     struct Trial {
@@ -404,6 +412,7 @@ struct rrb_batch {
         float ms;
     };
     std::vector<Trial> trials;  // empty: not planned yet
+    bool row_trials_planned = false;  // the second phase (row shapes) is in trials
     size_t trial = 0;           // next trial to run (trials.size(): settled)
     uint64_t trial_epoch = ~0ull;
     std::vector<PageGeom> geom_h;
@@ -498,6 +507,7 @@ int batch_upload(rrb_ctx* c, const rrb_path_batch_params* h, rrb_batch* B, const
     B->trials.clear();
     B->trial = 0;
     B->trial_epoch = ~0ull;
+    B->row_trials_planned = false;
     B->has_hairline = false;
     if (hairlines)
         for (uint64_t p = 0; p < h->n_paths && !B->has_hairline; ++p) B->has_hairline = h->fill_rule[p] == RULE_HAIRLINE;
@@ -793,9 +803,10 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
         k_chunk_paths<<<grid_for(c, n_paths * 32, 256), 256, 0, c->stream>>>(as<uint32_t>(c->s_chunks), NP,
                                                                             as<uint32_t>(c->s_chunk_path));
         c->launches += 1;
-        // Two shapes of the row stage: 12 list entries per AA row with 8 warps
-        // per block (the default), or 16 entries with 4 warps, which sends
-        // fewer rows to k_groups_mid (pages whose rows carry more crossings).
+        // Shapes of the row stage: 12 list entries per AA row with 8 warps per
+        // block (the default), 16 entries with 4 warps (fewer rows go to
+        // k_groups_mid: pages whose rows carry more crossings), 8 entries with
+        // 16 warps, each with one or two edge groups staged per warp.
         auto rows = [&](auto kernel, int warps, size_t smem) -> int {
             RRB_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem)));
@@ -806,8 +817,13 @@ int run_resident_one(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len,
                 as<BatchCounters>(c->s_ctr), as<uint32_t>(c->s_chunk_path), pclip);
             return RRB_OK;
         };
-        if (B->row_shape == 1) rc = rows(k_rows<KCAP_WIDE, 4>, 4, rows_smem_bytes<KCAP_WIDE, 4>());
-        else rc = rows(k_rows<KCAP, ROWS_WARPS>, ROWS_WARPS, rows_smem_bytes<KCAP, ROWS_WARPS>());
+        switch (B->row_shape) {
+            case 1: rc = rows(k_rows<KCAP_WIDE, 4>, 4, rows_smem_bytes<KCAP_WIDE, 4>()); break;
+            case 2: rc = rows(k_rows<KCAP, ROWS_WARPS, 1>, ROWS_WARPS, rows_smem_bytes<KCAP, ROWS_WARPS, 1>()); break;
+            case 3: rc = rows(k_rows<8, 16>, 16, rows_smem_bytes<8, 16>()); break;
+            case 4: rc = rows(k_rows<KCAP_WIDE, 4, 1>, 4, rows_smem_bytes<KCAP_WIDE, 4, 1>()); break;
+            default: rc = rows(k_rows<KCAP, ROWS_WARPS>, ROWS_WARPS, rows_smem_bytes<KCAP, ROWS_WARPS>());
+        }
         if (rc) return rc;
         c->launches += 1;
     }
@@ -1124,11 +1140,12 @@ int run_resident_waves(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_le
 
 int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int rowmap) {
     if (B->trial_epoch != c->tuning_epoch) {
-        // Plan the trials: both row-stage shapes, for the context's tile shape
-        // or, with automatic tiles, for 64x16, 128x16 and 128x32.
+        // Plan the first phase of the trials: the tile shapes (the context's,
+        // or with automatic tiles 64x16, 128x16 and 128x32), row shape 0.
         B->trial_epoch = c->tuning_epoch;
         B->trials.clear();
         B->trial = 0;
+        B->row_trials_planned = false;
         const uint32_t cw = c->tuning.tile_w ? c->tuning.tile_w : 64, ch = c->tuning.tile_h ? c->tuning.tile_h : 16;
         if (c->tuning.auto_tile == 1) {
             // The shape the context last settled on goes first: a batch
@@ -1136,10 +1153,9 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
             uint32_t shapes[3][2] = {{64u, 16u}, {128u, 16u}, {128u, 32u}};
             for (int k = 1; k < 3; ++k)
                 if (shapes[k][0] == c->settled_tw && shapes[k][1] == c->settled_th) std::swap(shapes[0], shapes[k]);
-            for (const auto& t : shapes)
-                for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({t[0], t[1], rs, 0.f});
+            for (const auto& t : shapes) B->trials.push_back({t[0], t[1], 0, 0.f});
         } else {
-            for (uint8_t rs = 0; rs < 2; ++rs) B->trials.push_back({cw, ch, rs, 0.f});
+            B->trials.push_back({cw, ch, 0, 0.f});
         }
     }
     auto settled = [&]() {
@@ -1171,12 +1187,19 @@ int run_resident(rrb_ctx* c, rrb_batch* B, uint8_t* arena, size_t arena_len, int
             size_t best = 0;
             for (size_t k = 1; k < B->trials.size(); ++k)
                 if (B->trials[k].ms < B->trials[best].ms) best = k;
-            B->tile_w = B->trials[best].tw;
-            B->tile_h = B->trials[best].th;
-            B->row_shape = B->trials[best].rs;
-            if (c->tuning.auto_tile == 1) {
-                c->settled_tw = B->tile_w;
-                c->settled_th = B->tile_h;
+            if (!B->row_trials_planned) {
+                // Second phase: the other row shapes with the fastest tile.
+                B->row_trials_planned = true;
+                const rrb_batch::Trial T0 = B->trials[best];
+                for (uint8_t rs = 1; rs < kRowShapes; ++rs) B->trials.push_back({T0.tw, T0.th, rs, 0.f});
+            } else {
+                B->tile_w = B->trials[best].tw;
+                B->tile_h = B->trials[best].th;
+                B->row_shape = B->trials[best].rs;
+                if (c->tuning.auto_tile == 1) {
+                    c->settled_tw = B->tile_w;
+                    c->settled_th = B->tile_h;
+                }
             }
         }
     }

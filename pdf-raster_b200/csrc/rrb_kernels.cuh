@@ -330,8 +330,27 @@ constexpr int CURVE_BIG = 32;
 // Segments per piece slot. SPLIT: a curve with more than CURVE_BIG segments
 // is counted 0 here and appended to big_list (big-curve count in
 // ctr->big_curves) for k_seg_count_big.
+// Register budgets (CTAs per SM the compiler must fit; 0: its own choice)
+// of the thread-per-piece flatten kernels (128 threads) and k_path_bbox (256).
+#ifndef RRB_SEG_CTAS
+#define RRB_SEG_CTAS 0
+#endif
+#ifndef RRB_BBOX_CTAS
+#define RRB_BBOX_CTAS 0
+#endif
+#if RRB_SEG_CTAS > 0
+#define RRB_SEG_BOUNDS __launch_bounds__(128, RRB_SEG_CTAS)
+#else
+#define RRB_SEG_BOUNDS
+#endif
+#if RRB_BBOX_CTAS > 0
+#define RRB_BBOX_BOUNDS __launch_bounds__(256, RRB_BBOX_CTAS)
+#else
+#define RRB_BBOX_BOUNDS
+#endif
+
 template <bool SPLIT>
-__global__ void k_seg_count(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
+__global__ void RRB_SEG_BOUNDS k_seg_count(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, uint32_t* __restrict__ counts,
                             uint32_t* __restrict__ big_list, BatchCounters* __restrict__ ctr) {
     __shared__ double m[6];
@@ -433,7 +452,7 @@ __global__ void RRB_BIG_CURVE_BOUNDS k_seg_count_big(const double* __restrict__ 
 // Edge records per piece slot, at edge_off[slot]. SPLIT: curves with more
 // than CURVE_BIG segments are left to k_seg_write_big.
 template <bool SPLIT>
-__global__ void k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
+__global__ void RRB_SEG_BOUNDS k_seg_write(const double* __restrict__ pts, const uint2* __restrict__ pieces, uint32_t n_slots,
                             const double* __restrict__ mtx, double flat_sq, const uint32_t* __restrict__ edge_off,
                             uint32_t edge_cap, Edge* __restrict__ edges,
                             const uint32_t* __restrict__ slot_clip_hi, const uint32_t* __restrict__ slot_clip_lo) {
@@ -614,7 +633,7 @@ __global__ void k_scan_down(const uint32_t* __restrict__ in, uint32_t* __restric
 // read under the as-shipped row map only) gives per path the pixel rows the
 // shipped driver loop visits when they come from another path's AA range.
 // ---------------------------------------------------------------------------
-__global__ void k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
+__global__ void RRB_BBOX_BOUNDS k_path_bbox(const uint32_t* __restrict__ piece_off, const uint32_t* __restrict__ edge_off,
                             const Edge* __restrict__ edges, uint32_t n_paths, const uint8_t* __restrict__ rule,
                             const uint8_t* __restrict__ gray, const uint8_t* __restrict__ alpha,
                             const uint32_t* __restrict__ path_page, const uint32_t* __restrict__ page_w,
@@ -1161,14 +1180,15 @@ __global__ void k_chunk_paths(const uint32_t* __restrict__ chunk_off, uint32_t n
 // sub-rows of one pixel row; their spans are merged into coverage cells by
 // lane 4k. Pixel rows with a list over KCAP go to k_groups_mid.
 // k_rows' shared memory (dynamic: it exceeds the 48 KB of static shared
-// memory): per warp the three entry lists, two staged edge groups and the
-// span counts.
-template <int KCAP, int WARPS>
+// memory): per warp the three entry lists, GS staged edge groups (32 edge
+// records of 32 bytes each) and the span counts. A block stages
+// WARPS x GS x 32 edges at a time.
+template <int KCAP, int WARPS, int GS = 2>
 constexpr size_t rows_smem_bytes() {
-    return sizeof(int32_t) * WARPS * (3 * KCAP * 32 + 8 * 64 + 32);
+    return sizeof(int32_t) * WARPS * (3 * KCAP * 32 + 8 * 32 * GS + 32);
 }
 
-template <int KCAP, int WARPS = ROWS_WARPS>
+template <int KCAP, int WARPS = ROWS_WARPS, int GS = 2>
 __global__ void __launch_bounds__(WARPS * 32) k_rows(
     const PathInfo* __restrict__ info, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ group_off,
     const Edge* __restrict__ edges, const int32_t* __restrict__ gmin, const int32_t* __restrict__ gmax,
@@ -1180,8 +1200,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_rows(
     auto sx0 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem);
     auto sx1 = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + LIST);
     auto scn = reinterpret_cast<int32_t (*)[KCAP * 32]>(rows_smem + 2 * LIST);
-    auto sedge = reinterpret_cast<Edge (*)[64]>(rows_smem + 3 * LIST);  // 16-byte aligned: LIST is a multiple of 4
-    auto sns = reinterpret_cast<int32_t (*)[32]>(rows_smem + 3 * LIST + WARPS * 8 * 64);
+    auto sedge = reinterpret_cast<Edge (*)[32 * GS]>(rows_smem + 3 * LIST);  // 16-byte aligned: LIST is a multiple of 4
+    auto sns = reinterpret_cast<int32_t (*)[32]>(rows_smem + 3 * LIST + WARPS * 8 * 32 * GS);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t total_chunks = chunk_off[n_paths];
     uint32_t nonterm = 0;
@@ -1194,7 +1214,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_rows(
         const bool valid = r >= P.y0 && r <= chunk_hi;
         const int32_t mask = (P.paint >> 16) & 1 ? 1 : ~0;
         const int32_t aa_width = 4 * static_cast<int32_t>(page_w[P.page]);
-        const int n = gather_row<KCAP, 32, 2>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
+        const int n = gather_row<KCAP, 32, GS>(P, chunk_lo, chunk_hi, r, valid, edges, gmin, gmax, sedge[w], sx0[w],
                                               sx1[w], scn[w], lane);
         const bool overflow = valid && n > KCAP;
         int ns = 0;

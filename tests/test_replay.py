@@ -39,7 +39,7 @@ def test_replays_keep_pixels_and_stats_and_wait_once(backend, oracle, rrb_lib, t
     batch = backend.batch_upload(s.view)
     try:
         stats = []
-        for k in range(7):  # row-shape trials, the chosen shape's first render, then replays
+        for k in range(10):  # row-shape trials, the chosen shape's first render, then replays
             got, st = _render(backend, batch, pages, s.arena_bytes)
             d = np.nonzero(got != exp)[0]
             assert d.size == 0, f"render {k}: {d.size} bytes differ, first at {d[:5]}"
@@ -80,7 +80,8 @@ def test_new_inputs_are_not_replayed(backend, oracle, rrb_lib):
 
 def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
     """With automatic tiles a resident batch renders once with each of 64x16,
-    128x16 and 128x32 under both row-stage shapes, then keeps the fastest pair and
+    128x16 and 128x32 (row shape 0), then with the other row-stage shapes on the
+    fastest of those tiles, then keeps the fastest pair and
     replays it: every render, trials included, gives the oracle's pages."""
     s = rrb_lib.Scene(kind=2, seed=29, n_pages=3, page_scale=0.3, paths_scale=0.1)
     exp = s.blank_arena()
@@ -92,13 +93,14 @@ def test_automatic_tile_trials_keep_pixels(backend, oracle, rrb_lib):
     batch = backend.batch_upload(s.view)
     try:
         seen = set()
-        for k in range(16):
+        for k in range(20):
             got, st = _render(backend, batch, pages, s.arena_bytes)
             assert np.array_equal(got, exp), f"render {k} ({st['tile_w']}x{st['tile_h']}, rows {st['row_shape']})"
             seen.add((st["tile_w"], st["tile_h"], st["row_shape"]))
             if st["trials_left"] == 0 and st["host_syncs"] == 1:
                 break
-        assert {(64, 16, 0), (64, 16, 1), (128, 16, 0), (128, 16, 1), (128, 32, 0), (128, 32, 1)} <= seen
+        assert {(64, 16, 0), (128, 16, 0), (128, 32, 0)} <= seen
+        assert {rs for *_, rs in seen} == {0, 1, 2, 3, 4}  # every row-stage shape ran
         assert st["trials_left"] == 0 and st["host_syncs"] == 1  # settled and replaying
         assert (st["tile_w"], st["tile_h"]) in {(64, 16), (128, 16), (128, 32)}
         # A batch uploaded per call on this context then takes the settled tile shape.
