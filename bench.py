@@ -265,7 +265,11 @@ def run_reference(args, rank, world):
         return
     import rr_oracle
     import rrb
+    from rrb import scenes
     rr_oracle.build()
+    # Inputs from the oracle's build of the workload generator (same source and
+    # flags as the package's): this process maps oracle/ libraries only.
+    scenes.use_library(rr_oracle.SCENES_LIB_PATH)
     if args.workload == "fill_ops":
         print(json.dumps({"impl": "reference", "unavailable": "the fill_ops line times aa_fill_cpu (the "
                                                              "reference's own CPU coverage) as its cpu_baseline"}))
@@ -364,6 +368,8 @@ def run_rrb(args, rank, local, world):
         # A fixed tile shape (profiling runs): no tile trials.
         tw, th = (int(v) for v in args.tile.split("x"))
         backend.set_tuning(tw, th)
+    if args.wave_points:
+        backend.set_tuning(wave_points=args.wave_points, auto_tile=not args.tile)
     tuning = backend.get_tuning()
     pages = backend.alloc_device(scene.arena_bytes)
     scene.view.pages = None
@@ -934,6 +940,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
     ap.add_argument("--tile", default="", help="WxH, a fixed tile shape instead of the trials (profiling runs)")
+    ap.add_argument("--wave-points", type=int, default=0, help="path points per wave of pages (0: the library's)")
     ap.add_argument("--pages", default="", help="a:b, render only pages [a, b) of the batch (profiling runs)")
     ap.add_argument("--serving", action="store_true", help="Poisson request load against the server")
     ap.add_argument("--rates", default="50,200,1000,2000")

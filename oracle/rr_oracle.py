@@ -16,6 +16,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "librr_oracle.so"
+# The workload generator built from the package's scene source into oracle/_build
+# (oracle/Makefile), for the timed CPU reference: it then maps oracle/ libraries only.
+SCENES_LIB_PATH = HERE / "_build" / "librr_scenes.so"
 
 ROWMAP_DOCUMENTED = 0
 ROWMAP_AS_SHIPPED = 1
@@ -58,7 +61,12 @@ class StrokeParams(C.Structure):
 def build(arch: str | None = None) -> Path:
     """Compile the oracle if needed. `arch` overrides -march (default x86-64-v3, portable to any AVX2 host)."""
     srcs = [HERE / n for n in ("rr_oracle.cpp", "rr_oracle.h", "fill_oracle.cpp", "fill_oracle.h", "Makefile")]
-    if LIB_PATH.exists() and LIB_PATH.stat().st_mtime >= max(p.stat().st_mtime for p in srcs):
+    scene_srcs = [HERE.parent / "pdf-raster_b200" / "scenes" / "scene_gen.cpp",
+                  HERE.parent / "pdf-raster_b200" / "csrc" / "path_builder.cpp",
+                  HERE.parent / "pdf-raster_b200" / "csrc" / "path_builder.h",
+                  HERE.parent / "include" / "rrb.h", HERE.parent / "include" / "rrb_scenes.h"]
+    newest = max(p.stat().st_mtime for p in srcs + [q for q in scene_srcs if q.exists()])
+    if all(x.exists() and x.stat().st_mtime >= newest for x in (LIB_PATH, SCENES_LIB_PATH)):
         return LIB_PATH
     env = dict(os.environ)
     cmd = ["make", "-C", str(HERE), f"ARCHFLAGS=-march={arch or 'x86-64-v3'}"]

@@ -52,6 +52,16 @@ SIGNATURES = {
 _LIB = None
 
 
+def use_library(path) -> None:
+    """Generate scenes with another build of the same generator source (the
+    CPU reference's copy under oracle/_build); call before the first scene."""
+    global LIB_PATH
+    path = Path(path).resolve()
+    if _LIB is not None and path != LIB_PATH:
+        raise RuntimeError(f"scene library already loaded from {LIB_PATH}")
+    LIB_PATH = path
+
+
 def lib() -> C.CDLL:
     """Load librrb_scenes.so (building it if needed) and declare its signatures."""
     global _LIB
