@@ -138,6 +138,26 @@ ROW_STAGES = ["12 entries x 8 warps, 512 edges staged per block", "16 entries x 
               "16 entries x 4 warps, 128 edges per block"]
 
 
+L2_BYTES = 126 << 20
+FLUSH_BYTES = 512 << 20
+
+
+def needs_l2_flush(scene) -> bool:
+    """Whether a step's inputs (path points and flags, and the pages) fit in
+    twice the L2: then every timed step starts after an L2 flush."""
+    return 17 * scene.n_pts + scene.pixels < 2 * L2_BYTES
+
+
+def workload_config(desc, scene, rowmap):
+    """The line's `config`: the workload alone, the same in the B200 line and
+    the reference line of one workload (device choices go under `device`)."""
+    inputs = 17 * scene.n_pts + scene.pixels
+    l2 = (f"L2 flushed before every timed step ({FLUSH_BYTES >> 20} MB written; inputs {inputs / 1e6:.0f} MB)"
+          if needs_l2_flush(scene) else f"inputs larger than L2 ({inputs / 1e6:.0f} MB of path points and pages)")
+    return {"workload": desc, "paths": scene.n_paths, "pages": scene.n_pages,
+            "rowmap": ["documented", "as_shipped"][rowmap], "l2": l2}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -315,7 +335,10 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": mpx, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded)", "config": {"workload": desc, "pages_per_step": pages_per_step},
+            "data": "synthetic (seeded generator, seed 0; no public dataset for this path)",
+            "config": (workload_config(desc, scene, args.rowmap) if args.workload != "strokes"
+                       else {"workload": desc}),
+            "pages_per_step": pages_per_step,
             "cpu_baseline": {"value": mpx, "unit": "Mpixel/s", "cores": threads, "kind": "port",
                              "sample": sample_desc,
                              "coverage_tier": ["scalar", "avx2", "avx512_bitalg"][rr_oracle.coverage_tier()]},
@@ -393,16 +416,24 @@ def run_rrb(args, rank, local, world):
     # ---- timed region: resident inputs, per-stage events inside the library
     backend.set_profiling(True)
     stage_acc, launches, step_ms = {}, 0, []
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    # Start and end events per step: an L2 flush (small inputs) runs between
+    # steps, outside the timed spans.
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    flush = (torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+             if needs_l2_flush(full_scene) else None)
     clocks = Clocks(local)
     if dist:
         dist.barrier()
     torch.cuda.synchronize(local)
     clocks.start()
-    ev[0].record(stream)
     for k in range(args.steps):
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xff)
+        ev0[k].record(stream)
         step()
-        ev[k + 1].record(stream)
+        ev1[k].record(stream)
         st = backend.last_batch_stats()
         launches += st["kernel_launches"]
         for name, (ms, nl) in backend.stage_times().items():
@@ -412,8 +443,8 @@ def run_rrb(args, rank, local, world):
     torch.cuda.synchronize(local)
     clk = clocks.stop()
     backend.set_profiling(False)
-    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
+    step_ms = [ev0[k].elapsed_time(ev1[k]) for k in range(args.steps)]
+    total_ms = sum(step_ms)
     if dist:
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -559,12 +590,10 @@ def run_rrb(args, rank, local, world):
             "scaling": "strong" if sharded else "weak",
             "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded generator, seed 0; no public dataset for this path)",
-            "config": {"workload": desc, "paths": full_scene.n_paths, "pages": full_scene.n_pages,
-                       "rowmap": ["documented", "as_shipped"][args.rowmap],
-                       "tile": f"{stats['tile_w']}x{stats['tile_h']} (chosen by trial among 64x16, 128x16 and 128x32)"
+            "config": workload_config(desc, full_scene, args.rowmap),
+            "device": {"tile": f"{stats['tile_w']}x{stats['tile_h']} (chosen by trial among 64x16, 128x16 and 128x32)"
                                if tuning.auto_tile == 1 else f"{stats['tile_w']}x{stats['tile_h']}",
                        "row_stage": ROW_STAGES[int(stats["row_shape"])],
-                       "l2": f"inputs larger than L2 ({16 * scene.n_pts / 1e6:.0f} MB of path points)",
                        "parallelism": (f"pages sharded over {world} GPUs" if sharded
                                        else f"replicas x{world} (the page on every GPU)")},
             "edges_per_s": edges_s, "segments_per_step": stats["segments"],
@@ -714,6 +743,7 @@ def run_fill_ops(args, rank, world):
     rr_oracle.build()
     be = rrb.B200Backend(0)
     stream = torch.cuda.ExternalStream(be.stream, device=torch.device("cuda", 0))
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda:0")
 
     def outline_segs(n_glyphs, size):
         sc = rrb.Scene(1, 7, n_paths=n_glyphs, page_w=size, page_h=size)
@@ -741,14 +771,18 @@ def run_fill_ops(args, rank, world):
             be.wait_page(be.submit_page())
 
         run()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # These inputs fit in L2: every timed call starts after an L2 flush,
+        # outside its events.
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
         torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(reps):
+        for k, (e0, e1) in enumerate(evs):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xff)
+            e0.record(stream)
             run()
-        e1.record(stream)
+            e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
         host = np.empty(w * h, np.uint8)
         t = time.perf_counter()
         for _ in range(reps):
@@ -782,7 +816,8 @@ def run_fill_ops(args, rank, world):
             "value": head["gpu_mpixel_s"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": "48 glyph outlines flattened at 0.1 in a 1024x1024 coverage window; "
-                                   "plus the reference threshold_bench squares 2^8..2^22 px"},
+                                   "plus the reference threshold_bench squares 2^8..2^22 px",
+                       "l2": f"L2 flushed before every timed call ({FLUSH_BYTES >> 20} MB written)"},
             "cpu_baseline": {"value": head["cpu_mpixel_s"], "unit": "Mpixel/s", "cores": 1, "kind": "port",
                              "sample": f"aa_fill_cpu on the first {head['cpu_sample_rows']} rows"},
             "ops": out}
