@@ -221,6 +221,29 @@ int rrb_record_tile_fill(rrb_ctx* ctx, const rrb_tile_fill_params* p);
  * records; *n_records (optional) receives their count. */
 int rrb_record_tile_fill_segs(rrb_ctx* ctx, const rrb_aa_fill_params* p, uint64_t* n_records);
 
+/* GpuBackend::record_scan (crates/gpu/src/backend/mod.rs:340-353; ScanParams
+ * and ScanPhase, params.rs:207-372): one phase of the three-phase exclusive
+ * scan of len_elems u32 in place (u32 sums wrap). Tiles of 1,024 elements
+ * (SCAN_WORKGROUP_SIZE 512 threads x 2): phase 0 scans each tile and writes
+ * its total to block_sums[tile]; phase 1 scans block_sums (at most 1,024
+ * tiles, SCAN_MAX_BLOCKS); phase 2 adds block_sums[tile] to every element of
+ * its tile. Call the three in order inside begin_page/submit_page. The same
+ * invariants as ScanParams::validate: len_elems > 0, data holds len_elems
+ * u32, block_sums holds ceil(len_elems / 1024) u32, and that count is at
+ * most 1,024; else RRB_ERR_INVARIANT. */
+#define RRB_SCAN_WORKGROUP_SIZE 512u
+#define RRB_SCAN_MAX_BLOCKS 1024u
+#define RRB_SCAN_PER_WORKGROUP 0u
+#define RRB_SCAN_BLOCK_SUMS 1u
+#define RRB_SCAN_SCATTER_BLOCK_SUMS 2u
+typedef struct {
+    const rrb_buf* data;        /* device u32 [len_elems], scanned in place */
+    const rrb_buf* block_sums;  /* device u32 [ceil(len_elems / 1024)] */
+    uint32_t len_elems;
+    uint32_t phase;             /* RRB_SCAN_* */
+} rrb_scan_params;
+int rrb_record_scan(rrb_ctx* ctx, const rrb_scan_params* p);
+
 /* Many paths over many pages in one submission (the batched form). All
  * arrays are HOST memory; the backend uploads them and renders every path,
  * in index order per page, into device pages. Paths on different pages are

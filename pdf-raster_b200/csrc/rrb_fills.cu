@@ -513,9 +513,93 @@ int launch_tile_fill(rrb_ctx* c, const TileRec* recs, uint64_t n_recs, const uin
     return RRB_OK;
 }
 
+// record_scan's phases (ScanPhase, crates/gpu/src/backend/params.rs:221-289).
+// A block of SCAN_THREADS threads owns a tile of 2 * SCAN_THREADS u32; thread
+// t holds elements 2t and 2t + 1. The exclusive scan of the pair sums is a
+// warp shuffle scan, then a scan of the warp totals by warp 0; u32 sums wrap.
+constexpr int SCAN_THREADS = static_cast<int>(RRB_SCAN_WORKGROUP_SIZE);
+constexpr uint32_t SCAN_TILE = 2u * RRB_SCAN_WORKGROUP_SIZE;
+
+// Exclusive scan of v over the block; *total receives the block's sum.
+__device__ __forceinline__ uint32_t scan_block_excl(uint32_t v, uint32_t* warp_sums, uint32_t* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        constexpr int NW = SCAN_THREADS / 32;
+        uint32_t x = lane < NW ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
+        }
+        if (lane < NW) warp_sums[lane] = x;  // inclusive over the warps
+    }
+    __syncthreads();
+    *total = warp_sums[SCAN_THREADS / 32 - 1];
+    return (w ? warp_sums[w - 1] : 0u) + incl - v;
+}
+
+// Phase 0 (and phase 1 with tile_sums == nullptr over the block sums): each
+// block scans its tile of data[0, n) in place; tile_sums[block] = its total.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(uint32_t* __restrict__ data, uint32_t n,
+                                                             uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t warp_sums[SCAN_THREADS / 32];
+    const uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * SCAN_TILE + 2u * threadIdx.x;
+    const uint32_t a = i0 < n ? data[i0] : 0u, b = i0 + 1 < n ? data[i0 + 1] : 0u;
+    uint32_t total;
+    const uint32_t excl = scan_block_excl(a + b, warp_sums, &total);
+    if (i0 < n) data[i0] = excl;
+    if (i0 + 1 < n) data[i0 + 1] = excl + a;
+    if (tile_sums && threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Phase 2: block b adds the scanned tile_sums[b] to its tile.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_scatter(uint32_t* __restrict__ data, uint32_t n,
+                                                               const uint32_t* __restrict__ tile_sums) {
+    const uint32_t add = tile_sums[blockIdx.x];
+    const uint64_t i0 = static_cast<uint64_t>(blockIdx.x) * SCAN_TILE + threadIdx.x;
+    if (i0 < n) data[i0] += add;
+    if (i0 + SCAN_THREADS < n) data[i0 + SCAN_THREADS] += add;
+}
+
 }  // namespace
 
 extern "C" {
+
+int rrb_record_scan(rrb_ctx* c, const rrb_scan_params* p) {
+    if (!c || !p) return RRB_ERR_INVARIANT;
+    const rrb_host::DeviceScope dev_scope(rrb_ctx_device(c));
+    int rc;
+    if ((rc = begin(c, dev_scope.status()))) return rc;
+    // ScanParams::validate (crates/gpu/src/backend/params.rs:338-372).
+    if (p->len_elems == 0) return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "len_elems must be > 0");
+    if (!p->data || 4ull * p->len_elems > rrb_device_buffer_len(p->data))
+        return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "data buffer is smaller than len_elems * 4 bytes");
+    const uint32_t blocks = (p->len_elems + SCAN_TILE - 1) / SCAN_TILE;
+    if (blocks > RRB_SCAN_MAX_BLOCKS)
+        return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "block_count exceeds SCAN_MAX_BLOCKS (1024)");
+    if (!p->block_sums || 4ull * blocks > rrb_device_buffer_len(p->block_sums))
+        return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "block_sums buffer is smaller than block_count * 4 bytes");
+    if (p->phase > RRB_SCAN_SCATTER_BLOCK_SUMS) return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "unknown scan phase");
+    if (reinterpret_cast<uintptr_t>(rrb_device_ptr(p->data)) & 3 ||
+        reinterpret_cast<uintptr_t>(rrb_device_ptr(p->block_sums)) & 3)
+        return rrb_ctx_fail(c, RRB_ERR_INVARIANT, "scan buffers must be 4-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(rrb_stream(c));
+    uint32_t* data = static_cast<uint32_t*>(rrb_device_ptr(p->data));
+    uint32_t* sums = static_cast<uint32_t*>(rrb_device_ptr(p->block_sums));
+    if (p->phase == RRB_SCAN_PER_WORKGROUP) k_scan_tiles<<<blocks, SCAN_THREADS, 0, s>>>(data, p->len_elems, sums);
+    else if (p->phase == RRB_SCAN_BLOCK_SUMS) k_scan_tiles<<<1, SCAN_THREADS, 0, s>>>(sums, blocks, nullptr);
+    else k_scan_scatter<<<blocks, SCAN_THREADS, 0, s>>>(data, p->len_elems, sums);
+    FILL_CUDA(c, cudaGetLastError());
+    return RRB_OK;
+}
 
 void rrb_aa_fill_jitter(float* x, float* y) {
     if (x) std::memcpy(x, jitter().x, sizeof jitter().x);

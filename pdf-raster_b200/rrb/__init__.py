@@ -326,6 +326,12 @@ class B200Backend:
         self._chk(lib().rrb_record_tile_fill_segs(self._h, C.byref(p), C.byref(n)))
         return int(n.value)
 
+    def record_scan(self, data: DeviceBuffer, block_sums: DeviceBuffer, len_elems: int, phase: int):
+        """GpuBackend::record_scan: one phase (0 per-tile, 1 block sums, 2 scatter) of the in-place
+        exclusive u32 scan; call 0, 1, 2 in order inside begin_page/submit_page."""
+        p = _abi.ScanParams(data=data.handle, block_sums=block_sums.handle, len_elems=len_elems, phase=phase)
+        self._chk(lib().rrb_record_scan(self._h, C.byref(p)))
+
     def record_path_batch_rgb(self, params: PathBatchParams, path_rgb: np.ndarray):
         """Rgb8 pages (3 bytes per pixel): path p painted with path_rgb[p] = (r, g, b)."""
         rgb = np.ascontiguousarray(path_rgb, np.uint8).reshape(-1)

@@ -78,6 +78,10 @@ class TileFillParams(C.Structure):
                 ("width", C.c_uint32), ("height", C.c_uint32), ("fill_rule", C.c_uint8)]
 
 
+class ScanParams(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("block_sums", C.c_void_p), ("len_elems", C.c_uint32), ("phase", C.c_uint32)]
+
+
 class PathBatchParams(C.Structure):
     _fields_ = [
         ("pts", C.POINTER(C.c_double)),
@@ -205,6 +209,7 @@ SIGNATURES = {
     "rrb_aa_fill_jitter": (None, [C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "rrb_record_tile_fill": (C.c_int, [VP, C.POINTER(TileFillParams)]),
     "rrb_record_tile_fill_segs": (C.c_int, [VP, C.POINTER(AaFillParams), C.POINTER(C.c_uint64)]),
+    "rrb_record_scan": (C.c_int, [VP, C.POINTER(ScanParams)]),
     "rrb_record_path_batch": (C.c_int, [VP, C.POINTER(PathBatchParams)]),
     "rrb_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "rrb_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),

@@ -79,6 +79,7 @@ STRUCTS = {
     "rrb_tile_record": ("TileRecord", ["key", "x_enter", "dxdy", "y0_tile", "y1_tile", "sign", "pad", "pad2"]),
     "rrb_tile_fill_params": ("TileFillParams", ["records", "tile_starts", "tile_counts", "coverage", "width",
                                                 "height", "fill_rule"]),
+    "rrb_scan_params": ("ScanParams", ["data", "block_sums", "len_elems", "phase"]),
     "rrb_stroke_params": ("StrokeParams", ["line_width", "miter_limit", "dash_phase", "dash", "n_dash", "line_cap",
                                            "line_join", "stroke", "reserved"]),
     "rrb_scene_params": ("scenes.SceneParams", ["kind", "seed", "n_pages", "n_paths", "page_w", "page_h",
