@@ -112,13 +112,12 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-# DRAM bytes per flattened segment of the row and flatten kernels on the glyph
-# page: dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of each
-# kernel on the glyph page reduced to 30,000 paths (10,979,156 segments, edge
-# records larger than L2), scaled to a full launch by its segment count.
+# DRAM bytes per flattened segment of the row stage on the glyph page:
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of k_rows on
+# the glyph page reduced to 30,000 paths (10,979,156 segments, edge records
+# larger than L2), scaled to a full launch by its segment count.
 GLYPH_DRAM_BYTES_PER_SEGMENT = {
-    "rows": (386_763_520 + 43_189_504) / 10_979_156,
-    "seg_write": (169_890_304 + 404_720_384) / 10_979_156,
+    "rows": (387_725_568 + 43_464_192) / 10_979_156,
 }
 
 
