@@ -1789,14 +1789,21 @@ __global__ void k_groups_slow(const PathInfo* __restrict__ info, const uint32_t*
 // Tiles of 4,096 pixels or more run RRB_COMP_BIG_THREADS threads per CTA
 // (512: a thread holds 8 pixels, as in the smaller tiles' 256-thread CTAs).
 // The composite is compiled for RRB_COMP_SM_THREADS resident threads per SM,
-// which sets its register budget: 1280 threads (five 256-thread CTAs, 48
-// registers) ran the 64-page mixed batch's composite 5% faster than 1024 (64
-// registers) and 4% faster than 1536 (40), spills included.
+// which sets its register budget. With two path hits' loads in flight, 1280
+// threads (five 256-thread CTAs, 48 registers) ran the 64-page mixed batch's
+// composite 5% faster than 1024 (64 registers) and 4% faster than 1536 (40);
+// with one (a buffer of registers fewer), 1536 threads (six CTAs, 40
+// registers) ran it 3% faster again (53.97 against 55.78 ms).
 #ifndef RRB_COMP_BIG_THREADS
 #define RRB_COMP_BIG_THREADS 512
 #endif
 #ifndef RRB_COMP_SM_THREADS
-#define RRB_COMP_SM_THREADS 1280
+#define RRB_COMP_SM_THREADS 1536
+#endif
+// Path hits whose loads are in flight ahead of the one being blended (1, or
+// 2 with a buffer of registers more).
+#ifndef RRB_COMP_PIPE_DEPTH
+#define RRB_COMP_PIPE_DEPTH 1
 #endif
 __host__ __device__ constexpr int comp_threads(int tw, int th) {
     return tw * th >= 4096 ? RRB_COMP_BIG_THREADS : 256;
@@ -2308,7 +2315,11 @@ __global__ void __launch_bounds__(comp_threads(TW, TH), comp_ctas_per_sm(TW, TH)
             // the boxes and full-tile runs between them, which load nothing.
             // A run of layers covering the whole tile is applied as one 256-entry
             // map (one blend per thread per layer) instead of per pixel.
+#if RRB_COMP_PIPE_DEPTH >= 2
             HitRows<TW, TH> cur, nxt, nxt2;
+#else
+            HitRows<TW, TH> cur, nxt;
+#endif
             const uint32_t p0 = next_set(pathbits, 0);
             uint32_t p1 = p0 < total ? next_set(pathbits, p0 + 1) : total;  // the path hit after the next one
             if (p0 < total) load_hit_index<TW, TH>(hits[p0], rowmap, Y0, H, gidx, runs, cur);
@@ -2402,11 +2413,18 @@ __global__ void __launch_bounds__(comp_threads(TW, TH), comp_ctas_per_sm(TW, TH)
                 // A path hit (k is the pipeline's current one): the index loads
                 // of the path hit after p1 and the cells of p1 go out first.
                 const uint32_t p2 = p1 < total ? next_set(pathbits, p1 + 1) : total;
+#if RRB_COMP_PIPE_DEPTH >= 2
                 if (p2 < total) load_hit_index<TW, TH>(hits[p2], rowmap, Y0, H, gidx, runs, nxt2);
+#endif
                 if (p1 < total) load_hit_cells<TW, TH>(cells, nxt);
                 composite_path_rows<TW, TH, RGB, FEW>(hits[k], cur, X0, cells, gamma, mark, pix);
                 cur = nxt;
+#if RRB_COMP_PIPE_DEPTH >= 2
                 nxt = nxt2;
+#else
+                // One buffer fewer: p2's index loads go out once p1 is current.
+                if (p2 < total) load_hit_index<TW, TH>(hits[p2], rowmap, Y0, H, gidx, runs, nxt);
+#endif
                 p1 = p2;
                 ++k;
             }
