@@ -22,6 +22,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -263,7 +264,11 @@ void worker(rrb_server* s, int wi) {
                 for (size_t k = next.fetch_add(1); k < nb; k = next.fetch_add(1)) copy_req(k);
             };
             std::vector<std::thread> helpers;
-            for (size_t t = 1; t < nt; ++t) helpers.emplace_back(run);
+            try {
+                for (size_t t = 1; t < nt; ++t) helpers.emplace_back(run);
+            } catch (const std::system_error&) {
+                // No thread to spare: the ones started and this one share the rest.
+            }
             run();
             for (std::thread& h : helpers) h.join();
         }
