@@ -304,8 +304,8 @@ def run_reference(args, rank, world):
     else:
         kw, desc = WORKLOADS[args.workload]
         scene = rrb.Scene(**kw)
-    cores = os.cpu_count() or 1
-    threads = max(1, min(cores, args.ref_threads))
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    threads = max(1, min(cores, args.ref_threads) if args.ref_threads > 0 else cores)
     if scene.n_pages > 1:
         # Page-parallel on the host cores: each thread renders the leading
         # paths of its own page (about 2 s of work each per step).
@@ -573,7 +573,8 @@ def run_rrb(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_cpu_baseline and scene.n_pages > 1:
         import rr_oracle
         rr_oracle.build()
-        threads = max(1, min(os.cpu_count() or 1, args.ref_threads))
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        threads = max(1, min(cores, args.ref_threads) if args.ref_threads > 0 else cores)
         sample = PageParallelSample(scene, threads, 2.0)
         secs = sample.step()
         cpu = {"value": sample.credited_px / secs / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port",
@@ -970,7 +971,7 @@ def main():
     ap.add_argument("--rowmap", type=int, default=0)
     ap.add_argument("--plain-sample", type=int, default=2000)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--ref-threads", type=int, default=16)
+    ap.add_argument("--ref-threads", type=int, default=0, help="host threads of the CPU reference (0: every core)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling runs)")
     ap.add_argument("--tile", default="", help="WxH, a fixed tile shape instead of the trials (profiling runs)")
