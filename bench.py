@@ -158,10 +158,18 @@ def workload_config(desc, scene, rowmap):
 
 
 def measured_peak():
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json,
+    `hbm_gbs`), else the recipe's fallback, 6,650 GB/s."""
     p = ROOT / "MEASURED_PEAKS.json"
-    if p.exists():
+    try:
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
+        v = d.get("hbm_gbs")
+        if isinstance(v, dict):  # a burst / sustained pair
+            v = v.get("burst", v.get("value"))
+        if v:
+            return float(v), "measured"
+    except (OSError, ValueError, TypeError, AttributeError):
+        pass
     return 6650.0, "fallback"
 
 
